@@ -1,0 +1,161 @@
+/* voluma_b200.h — C ABI of the B200-native pressure-equation hot path.
+ *
+ * One process per GPU; every call is synchronous with respect to the host unless its
+ * name ends in _device (then it is ordered on the context's stream and reads/writes
+ * device pointers).  No C++ types, no exceptions cross this boundary: every entry point
+ * returns a vlm_status and leaves a message retrievable with vlm_last_error().
+ *
+ * Reference interfaces replaced (paths inside the Voluma project):
+ *   vlm_mesh_register     <- the per-Mesh caches Mesh::cached("GAMG"/"precondFaces")
+ *                            (src/fvm/mesh/Mesh.h:118-122, src/fvm/linalg/GAMG.cpp:204,
+ *                             src/fvm/linalg/LinearSolver.cpp:52-54) and the Mesh arrays
+ *                            owner/neighbour/magSf/nonOrthDeltaCoeffs (Mesh.h:62-73)
+ *   vlm_ldu_solve         <- SolverPerformance solveLdu(const LduSystem&, std::vector<scalar>& x,
+ *                            const SolverControls&)   (src/fvm/linalg/LinearSolver.h:42,
+ *                            LinearSolver.cpp:135-284)
+ *   vlm_amul              <- void amul(const LduSystem&, x, y)  (LinearSolver.h:45, .cpp:121-133)
+ *   vlm_gamg_apply        <- GamgPreconditioner::apply           (src/fvm/linalg/GAMG.h:63, .cpp:445)
+ *   vlm_gamg_levels/_level<- buildHierarchy                      (GAMG.h:57, GAMG.cpp:206-261)
+ *   vlm_laplacian         <- fvm::laplacian(gamma, psi, nonOrthCorr) (src/fvm/discretization/Fvm.h:141-182)
+ *   vlm_grad              <- fvc::grad (Gauss linear / leastSquares) (src/fvm/discretization/Fvc.h:209-291)
+ *   vlm_exact_sum         <- par::ExactSum::add/value            (src/fvm/parallel/Comm.h:42-93, Comm.cpp:107-164)
+ */
+#ifndef VOLUMA_B200_H
+#define VOLUMA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    VLM_OK = 0,
+    VLM_ERR_BAD_ARG = 1,      /* invalid pointer/size/name (reference: std::invalid_argument / runtime_error) */
+    VLM_ERR_CUDA = 2,         /* CUDA runtime failure */
+    VLM_ERR_OOM = 3,          /* device allocation failed / HBM budget exceeded */
+    VLM_ERR_SINGULAR = 4,     /* zero pivot in the coarsest GAMG matrix (GAMG.cpp:336) */
+    VLM_ERR_NONFINITE = 5,    /* Inf/NaN residual */
+    VLM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
+    VLM_ERR_UNSUPPORTED = 7,  /* unknown solver / preconditioner, PCG on asymmetric (LinearSolver.cpp:76,177,280) */
+    VLM_ERR_NO_DEVICE = 8     /* no CUDA device / extension unusable */
+} vlm_status;
+
+typedef struct vlm_ctx vlm_ctx;   /* one per host thread; owns a CUDA stream and scratch */
+typedef struct vlm_mesh vlm_mesh; /* device-resident addressing, geometry and GAMG hierarchy */
+
+/* Mesh description: the arrays of cfd::Mesh (src/fvm/mesh/Mesh.h:54-109), host pointers.
+ * Faces [0, n_internal_faces) are internal (owner < neighbour not required), the rest are
+ * boundary faces grouped by patch.  Geometry pointers may be NULL when only solving:
+ * magSf and ndc are needed for the GAMG agglomeration weights (GAMG.cpp:215); the rest is
+ * needed by vlm_laplacian / vlm_grad. */
+typedef struct {
+    int32_t n_cells;
+    int32_t n_internal_faces;
+    int32_t n_faces;
+    const int32_t* owner;      /* n_faces */
+    const int32_t* neighbour;  /* n_internal_faces */
+    const double* magSf;       /* n_faces */
+    const double* ndc;         /* n_faces, nonOrthDeltaCoeffs */
+    const double* V;           /* n_cells */
+    const double* Sf;          /* 3*n_faces */
+    const double* d;           /* 3*n_faces, owner->neighbour (boundary: owner->face centre) */
+    const double* w;           /* n_faces, linear interpolation weight of the owner */
+    const double* corrVecs;    /* 3*n_faces, n - d*ndc */
+    int32_t two_d;             /* Mesh::twoD() */
+    int32_t empty_dir;         /* Mesh::emptyDir() */
+    int32_t n_patches;
+    const int32_t* patch_start; /* n_patches, face index of each patch's first face */
+    const int32_t* patch_size;  /* n_patches */
+} vlm_mesh_desc;
+
+/* Solver dictionary: SolverControls (src/fvm/linalg/LinearSolver.h:15-23) plus additive keys. */
+typedef struct {
+    char solver[32];          /* "PCG" | "PBiCGStab" | "Jacobi" | "GaussSeidel" | "symGaussSeidel" */
+    char preconditioner[32];  /* "GAMG" | "DIC" | "DILU" | "diagonal" | "none" */
+    double tolerance;
+    double relTol;
+    int32_t maxIter;
+    int32_t minIter;
+    int32_t nSweeps;
+    /* ---- additive keys (zero-initialised struct = reference behaviour) ---- */
+    char smoother[16];        /* GAMG smoother on the device: "" or "mcgs" (multicolour Gauss-Seidel,
+                                 forward colours pre / reversed post) | "jacobi" */
+    char precision[16];       /* "" or "fp64" | "mixed" (FP32 inner PCG+GAMG in FP64 defect correction) */
+    int32_t reproducible;     /* 1: CFD_REPRODUCIBLE semantics: preconditioner -> diagonal,
+                                 GS -> Jacobi, exact (order-independent) global sums */
+    int32_t mergeLevels;      /* GAMG pairwise merges per level; 0 -> 2 (GAMG.cpp:96-99) */
+    double innerRelTol;       /* mixed precision: inner FP32 solve relative tolerance; 0 -> 1e-4 */
+} vlm_solver_ctrl;
+
+/* SolverPerformance (src/fvm/linalg/LinearSolver.h:25-31). */
+typedef struct {
+    double initialResidual;
+    double finalResidual;
+    double residualSum;
+    double normFactor;
+    int32_t iterations;       /* Krylov iterations (mixed: total inner iterations) */
+    int32_t converged;
+    int32_t outerIterations;  /* mixed precision: FP64 defect-correction passes (else 0) */
+    int32_t status;           /* vlm_status of the device solve (NONFINITE, SINGULAR, ...) */
+    char solver[32];
+} vlm_solver_perf;
+
+/* ------------------------------------------------------------------ context / mesh */
+vlm_status vlm_ctx_create(int device, vlm_ctx** out);
+vlm_status vlm_ctx_destroy(vlm_ctx* ctx);
+const char* vlm_last_error(const vlm_ctx* ctx); /* ctx may be NULL: last error of this thread */
+/* Stream the context orders its work on (a cudaStream_t). */
+void* vlm_ctx_stream(vlm_ctx* ctx);
+
+vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* desc, int32_t merge_levels, vlm_mesh** out);
+vlm_status vlm_mesh_release(vlm_mesh* mesh);
+
+/* ------------------------------------------------------------------ linear algebra */
+/* y = A x over the mesh's LDU matrix (host pointers; lower == NULL means symmetric). */
+vlm_status vlm_amul(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
+                    const double* lower, const double* x, double* y);
+
+/* solveLdu: x (in: initial guess, out: solution), host pointers. */
+vlm_status vlm_ldu_solve(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
+                         const double* lower, const double* b, double* x, const vlm_solver_ctrl* ctrl,
+                         vlm_solver_perf* perf);
+/* Same, device pointers, ordered on vlm_ctx_stream(ctx); perf is written after completion. */
+vlm_status vlm_ldu_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
+                                const double* lower, const double* b, double* x, const vlm_solver_ctrl* ctrl,
+                                vlm_solver_perf* perf);
+
+/* One GAMG V-cycle w = M^-1 r with the device smoother named in ctrl (host pointers). */
+vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
+                          const double* lower, const double* r, double* w, const vlm_solver_ctrl* ctrl);
+
+/* Hierarchy introspection (for parity checks): number of levels, then per level sizes
+ * {n, nFaces} and optional copies of l/u (nFaces), agg (n, empty on the coarsest level). */
+vlm_status vlm_gamg_levels(vlm_mesh* mesh, int32_t* n_levels);
+vlm_status vlm_gamg_level(vlm_mesh* mesh, int32_t level, int32_t* sizes, int32_t* l, int32_t* u, int32_t* agg);
+/* Number of colours the device smoother uses on a level. */
+vlm_status vlm_gamg_colours(vlm_mesh* mesh, int32_t level, int32_t* n_colours);
+
+/* ------------------------------------------------------------------ assembly */
+/* fvm::laplacian(gamma, psi, nonOrthCorr) for a scalar field with per-patch BCs
+ * (bc_type[p]: 0 zeroGradient, 1 fixedValue with values bc_values[f - n_internal_faces]).
+ * grad_scheme for the non-orthogonal correction: 0 Gauss linear, 1 leastSquares.
+ * Outputs (host): diag[n_cells], upper[n_internal], source[n_cells],
+ * internal_coeffs[n_boundary], boundary_source[n_boundary], ffc[n_faces], *has_ffc. */
+vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, const double* psi,
+                         const int32_t* bc_type, const double* bc_values, int32_t non_orth_corr,
+                         int32_t grad_scheme, double* diag, double* upper, double* source,
+                         double* internal_coeffs, double* boundary_source, double* ffc, int32_t* has_ffc);
+
+/* fvc::grad of a scalar field, out[3*n_cells]. */
+vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh* mesh, const double* psi, const int32_t* bc_type,
+                    const double* bc_values, int32_t scheme, double* out);
+
+/* ------------------------------------------------------------------ reductions */
+/* Order-independent exact sum of n doubles on the device (host pointer in, host result). */
+vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VOLUMA_B200_H */

@@ -1,0 +1,201 @@
+"""ctypes loader for oracle/_ref/libvlmref.so — the UNMODIFIED reference compiled from its
+own sources (see oracle/Makefile) plus oracle/ref_driver.cpp.
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference arm, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libvlmref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"reference oracle not built: {LIB_PATH} (run make -C oracle)")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_mesh_box.restype = P
+        L.ref_mesh_box.argtypes = [P, P, P, P, C.c_int, P, P, P]
+        L.ref_mesh_free.argtypes = [P]
+        L.ref_mesh_sizes.argtypes = [P, P]
+        L.ref_mesh_get.argtypes = [P, C.c_char_p, P]
+        L.ref_mesh_ncellfaces.argtypes = [P]
+        L.ref_set_reproducible.argtypes = [C.c_int]
+        L.ref_amul.argtypes = [P, P, P, P, P, P]
+        L.ref_solve_ldu.argtypes = [P, P, P, P, P, P, C.c_char_p, C.c_char_p, C.c_double, C.c_double,
+                                    C.c_int, C.c_int, C.c_int, P]
+        L.ref_gamg_nlevels.argtypes = [P]
+        L.ref_gamg_level.argtypes = [P, C.c_int] + [P] * 11
+        L.ref_gamg_meta.argtypes = [P, P, P]
+        L.ref_gamg_apply.argtypes = [P, P, P, P, P, P]
+        L.ref_laplacian.argtypes = [P, P, P, P, P, C.c_int, C.c_int, P, P, P, P, P, P, P]
+        L.ref_grad.argtypes = [P, P, P, P, C.c_int, P]
+        L.ref_pressure_solve.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
+                                         C.c_double, C.c_double, C.c_int, P, P, P]
+        L.ref_exact_sum.restype = C.c_double
+        L.ref_exact_sum.argtypes = [P, C.c_long]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+
+
+class RefMesh:
+    """A reference Mesh built by generateBox + Mesh::build (mesh/RawMesh.cpp:391, mesh/Mesh.cpp:476)."""
+
+    def __init__(self, n, lo=(0, 0, 0), hi=(1, 1, 1), periodic=(0, 0, 0), two_d=False, beta=(0, 0, 0),
+                 points=None, patch_types=None):
+        L = lib()
+        n_ = np.asarray(n, np.int32)
+        lo_ = np.asarray(lo, np.float64)
+        hi_ = np.asarray(hi, np.float64)
+        per = np.asarray(periodic, np.int32)
+        be = np.asarray(beta, np.float64)
+        pts = None if points is None else np.ascontiguousarray(points, np.float64)
+        pt = None if patch_types is None else np.asarray(patch_types, np.int32)
+        self._h = L.ref_mesh_box(_p(n_), _p(lo_), _p(hi_), _p(per), int(two_d), _p(be), _p(pts), _p(pt))
+        if not self._h:
+            raise RuntimeError(L.ref_last_error().decode())
+        s = np.zeros(8, np.int32)
+        L.ref_mesh_sizes(self._h, _p(s))
+        (self.n_cells, self.n_internal_faces, self.n_faces, self.n_patches, two, self.empty_dir,
+         skew) = [int(v) for v in s[:7]]
+        self.two_d = bool(two)
+        self.skewed = bool(skew)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ref_mesh_free(self._h)
+            self._h = None
+
+    def get(self, name):
+        nC, nI, nF, nP = self.n_cells, self.n_internal_faces, self.n_faces, self.n_patches
+        shapes = {"owner": (nF, np.int32), "neighbour": (nI, np.int32), "V": (nC, np.float64),
+                  "magSf": (nF, np.float64), "w": (nF, np.float64), "deltaCoeffs": (nF, np.float64),
+                  "ndc": (nF, np.float64), "C": ((nC, 3), np.float64), "Sf": ((nF, 3), np.float64),
+                  "Cf": ((nF, 3), np.float64), "d": ((nF, 3), np.float64), "corrVecs": ((nF, 3), np.float64),
+                  "skewVecs": ((nF, 3), np.float64), "patchStart": (nP, np.int32), "patchSize": (nP, np.int32),
+                  "cellFaceOffsets": (nC + 1, np.int32),
+                  "cellFaces": (lib().ref_mesh_ncellfaces(self._h), np.int32)}
+        shp, dt = shapes[name]
+        out = np.zeros(shp, dt)
+        _check(lib().ref_mesh_get(self._h, name.encode(), _p(out)))
+        return out
+
+    # ------------------------------------------------------------------ linear algebra
+    def amul(self, diag, upper, lower, x):
+        y = np.zeros(self.n_cells)
+        _check(lib().ref_amul(self._h, _p(np.ascontiguousarray(diag, np.float64)),
+                              _p(np.ascontiguousarray(upper, np.float64)),
+                              None if lower is None else _p(np.ascontiguousarray(lower, np.float64)),
+                              _p(np.ascontiguousarray(x, np.float64)), _p(y)))
+        return y
+
+    def solve(self, diag, upper, lower, b, x0, solver="PCG", precond="diagonal", tol=0.0, rel_tol=1e-8,
+              max_iter=1000, min_iter=0, n_sweeps=1, reproducible=False):
+        """solveLdu (linalg/LinearSolver.cpp:135). Returns (x, perf dict)."""
+        L = lib()
+        L.ref_set_reproducible(1 if reproducible else 0)
+        x = np.ascontiguousarray(x0, np.float64).copy()
+        perf = np.zeros(6)
+        low = None if lower is None else np.ascontiguousarray(lower, np.float64)
+        try:
+            _check(L.ref_solve_ldu(self._h, _p(np.ascontiguousarray(diag, np.float64)),
+                                   _p(np.ascontiguousarray(upper, np.float64)), _p(low),
+                                   _p(np.ascontiguousarray(b, np.float64)), _p(x), solver.encode(),
+                                   precond.encode(), tol, rel_tol, max_iter, min_iter, n_sweeps, _p(perf)))
+        finally:
+            L.ref_set_reproducible(0)
+        return x, dict(initialResidual=perf[0], finalResidual=perf[1], residualSum=perf[2],
+                       normFactor=perf[3], iterations=int(perf[4]), converged=bool(perf[5]))
+
+    def gamg_levels(self):
+        """buildHierarchy (linalg/GAMG.cpp:206) per level: dict of n, l, u, weight, agg, faceMap, faceFlip,
+        off, adjCell, adjFace, adjIsL."""
+        L = lib()
+        out = []
+        for lev in range(L.ref_gamg_nlevels(self._h)):
+            s = np.zeros(4, np.int32)
+            _check(L.ref_gamg_level(self._h, lev, _p(s), *([None] * 10)))
+            n, nf, nagg, nnz = [int(v) for v in s]
+            d = dict(n=n, l=np.zeros(nf, np.int32), u=np.zeros(nf, np.int32), weight=np.zeros(nf),
+                     agg=np.zeros(nagg, np.int32), faceMap=np.zeros(nf if nagg else 0, np.int32),
+                     faceFlip=np.zeros(nf if nagg else 0, np.int8), off=np.zeros(n + 1, np.int32),
+                     adjCell=np.zeros(nnz, np.int32), adjFace=np.zeros(nnz, np.int32),
+                     adjIsL=np.zeros(nnz, np.int8))
+            _check(L.ref_gamg_level(self._h, lev, _p(s), _p(d["l"]), _p(d["u"]), _p(d["weight"]), _p(d["agg"]),
+                                    _p(d["faceMap"]), _p(d["faceFlip"]), _p(d["off"]), _p(d["adjCell"]),
+                                    _p(d["adjFace"]), _p(d["adjIsL"])))
+            out.append(d)
+        return out
+
+    def gamg_apply(self, diag, upper, lower, r):
+        w = np.zeros(self.n_cells)
+        _check(lib().ref_gamg_apply(self._h, _p(np.ascontiguousarray(diag, np.float64)),
+                                    _p(np.ascontiguousarray(upper, np.float64)),
+                                    None if lower is None else _p(np.ascontiguousarray(lower, np.float64)),
+                                    _p(np.ascontiguousarray(r, np.float64)), _p(w)))
+        return w
+
+    # ------------------------------------------------------------------ discretisation
+    def laplacian(self, gamma, psi, bc_type, bc_values=None, non_orth_corr=True, grad_scheme=0):
+        nC, nI, nF = self.n_cells, self.n_internal_faces, self.n_faces
+        nB = nF - nI
+        out = dict(diag=np.zeros(nC), upper=np.zeros(nI), source=np.zeros(nC), internalCoeffs=np.zeros(nB),
+                   boundarySource=np.zeros(nB), ffc=np.zeros(nF))
+        has = np.zeros(1, np.int32)
+        bv = None if bc_values is None else np.ascontiguousarray(bc_values, np.float64)
+        _check(lib().ref_laplacian(self._h, _p(np.ascontiguousarray(gamma, np.float64)),
+                                   _p(np.ascontiguousarray(psi, np.float64)),
+                                   _p(np.ascontiguousarray(bc_type, np.int32)), _p(bv), int(non_orth_corr),
+                                   int(grad_scheme), _p(out["diag"]), _p(out["upper"]), _p(out["source"]),
+                                   _p(out["internalCoeffs"]), _p(out["boundarySource"]), _p(out["ffc"]),
+                                   _p(has)))
+        out["hasFfc"] = bool(has[0])
+        return out
+
+    def grad(self, psi, bc_type, bc_values=None, scheme=0):
+        g = np.zeros((self.n_cells, 3))
+        bv = None if bc_values is None else np.ascontiguousarray(bc_values, np.float64)
+        _check(lib().ref_grad(self._h, _p(np.ascontiguousarray(psi, np.float64)),
+                              _p(np.ascontiguousarray(bc_type, np.int32)), _p(bv), int(scheme), _p(g)))
+        return g
+
+    def pressure_solve(self, gamma, div_phi, p0, ref_cell=0, n_non_orth=0, grad_scheme=1, solver="PCG",
+                       precond="GAMG", tol=0.0, rel_tol=1e-8, max_iter=1000):
+        p = np.ascontiguousarray(p0, np.float64).copy()
+        flux = np.zeros(self.n_faces)
+        perf = np.zeros(6 * (n_non_orth + 1))
+        _check(lib().ref_pressure_solve(self._h, _p(np.ascontiguousarray(gamma, np.float64)),
+                                        _p(np.ascontiguousarray(div_phi, np.float64)), int(ref_cell),
+                                        int(n_non_orth), int(grad_scheme), solver.encode(), precond.encode(),
+                                        tol, rel_tol, max_iter, _p(p), _p(flux), _p(perf)))
+        return p, flux, perf.reshape(-1, 6)
+
+
+def exact_sum(v) -> float:
+    v = np.ascontiguousarray(v, np.float64)
+    return float(lib().ref_exact_sum(_p(v), v.size))

@@ -1,0 +1,268 @@
+"""voluma_b200 — B200-native pressure-equation hot path of Voluma behind its FvMatrix::solve /
+solver-dictionary interface.
+
+The product is the C-ABI library built from voluma_b200/csrc (include/voluma_b200.h).  This
+module is the Python host side over that ABI, with the reference's names:
+
+    SolverControls      <- cfd::SolverControls      (src/fvm/linalg/LinearSolver.h:15-23)
+    SolverPerformance   <- cfd::SolverPerformance   (src/fvm/linalg/LinearSolver.h:25-31)
+    Mesh                <- the cfd::Mesh arrays the solver needs, registered on the device
+    solve_ldu           <- cfd::solveLdu            (src/fvm/linalg/LinearSolver.cpp:135)
+    amul                <- cfd::amul                (src/fvm/linalg/LinearSolver.cpp:121)
+
+Errors follow the reference: an unknown solver/preconditioner or PCG on an asymmetric matrix
+raises (LinearSolver.cpp:76,177,280), a singular coarsest GAMG matrix raises (GAMG.cpp:336),
+non-convergence only clears `converged`.
+"""
+from __future__ import annotations
+
+import atexit
+import ctypes as C
+import weakref
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import VlmError, check, load
+
+__all__ = ["SolverControls", "SolverPerformance", "Context", "Mesh", "solve_ldu", "amul", "VlmError", "load"]
+
+
+@dataclass
+class SolverControls:
+    """The solver dictionary (LinearSolver.h:15-23) plus additive device keys."""
+    solver: str = "PCG"
+    preconditioner: str = "diagonal"
+    tolerance: float = 1e-8
+    relTol: float = 0.0
+    maxIter: int = 1000
+    minIter: int = 0
+    nSweeps: int = 1
+    smoother: str = ""          # GAMG smoother on the device: "" / "mcgs" | "jacobi"
+    precision: str = ""         # "" / "fp64" | "mixed"
+    reproducible: bool = False  # CFD_REPRODUCIBLE semantics
+    mergeLevels: int = 0
+    innerRelTol: float = 0.0
+
+    def to_c(self) -> _ffi.SolverCtrl:
+        c = _ffi.SolverCtrl()
+        c.solver = self.solver.encode()
+        c.preconditioner = self.preconditioner.encode()
+        c.tolerance = self.tolerance
+        c.relTol = self.relTol
+        c.maxIter = self.maxIter
+        c.minIter = self.minIter
+        c.nSweeps = self.nSweeps
+        c.smoother = self.smoother.encode()
+        c.precision = self.precision.encode()
+        c.reproducible = 1 if self.reproducible else 0
+        c.mergeLevels = self.mergeLevels
+        c.innerRelTol = self.innerRelTol
+        return c
+
+
+@dataclass
+class SolverPerformance:
+    solver: str = ""
+    field: str = ""
+    initialResidual: float = 0.0
+    finalResidual: float = 0.0
+    residualSum: float = 0.0
+    normFactor: float = 0.0
+    iterations: int = 0
+    converged: bool = False
+    outerIterations: int = 0
+    status: int = 0
+
+    @classmethod
+    def from_c(cls, p: _ffi.SolverPerf) -> "SolverPerformance":
+        return cls(solver=p.solver.decode(), initialResidual=p.initialResidual, finalResidual=p.finalResidual,
+                   residualSum=p.residualSum, normFactor=p.normFactor, iterations=p.iterations,
+                   converged=bool(p.converged), outerIterations=p.outerIterations, status=p.status)
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One CUDA device + stream (vlm_ctx)."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = C.c_void_p()
+        check(L.vlm_ctx_create(device, C.byref(h)))
+        self._h = h
+        _live.add(self)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream(self) -> int:
+        return load().vlm_ctx_stream(self._h) or 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().vlm_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+_live = weakref.WeakSet()  # meshes/contexts still holding native handles
+
+
+@atexit.register
+def _release_all():
+    # release meshes before contexts while the interpreter (and the CUDA runtime) are intact
+    objs = list(_live)
+    for o in objs:
+        if isinstance(o, Mesh):
+            o.close()
+    for o in objs:
+        o.close()
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class Mesh:
+    """Mesh arrays registered on the device (vlm_mesh_register): addressing, the GAMG
+    agglomeration weights and (optionally) the geometry the assembly kernels read."""
+
+    def __init__(self, n_cells, owner, neighbour, magSf, ndc, n_faces=None, ctx: Context | None = None,
+                 merge_levels: int = 2, geometry: dict | None = None):
+        self.ctx = ctx or default_context()
+        self.owner = np.ascontiguousarray(owner, np.int32)
+        self.neighbour = np.ascontiguousarray(neighbour, np.int32)
+        self.magSf = _f64(magSf)
+        self.ndc = _f64(ndc)
+        self.n_cells = int(n_cells)
+        self.n_internal_faces = int(self.neighbour.size)
+        self.n_faces = int(n_faces if n_faces is not None else self.owner.size)
+        self.geometry = geometry or {}
+        d = _ffi.MeshDesc()
+        d.n_cells = self.n_cells
+        d.n_internal_faces = self.n_internal_faces
+        d.n_faces = self.n_faces
+        d.owner = self.owner.ctypes.data
+        d.neighbour = self.neighbour.ctypes.data
+        d.magSf = self.magSf.ctypes.data
+        d.ndc = self.ndc.ctypes.data
+        self._keep = []
+        for name in ("V", "Sf", "d", "w", "corrVecs"):
+            if name in self.geometry:
+                arr = _f64(self.geometry[name])
+                self._keep.append(arr)
+                setattr(d, name, arr.ctypes.data)
+        if "patch_start" in self.geometry:
+            ps = np.ascontiguousarray(self.geometry["patch_start"], np.int32)
+            pz = np.ascontiguousarray(self.geometry["patch_size"], np.int32)
+            self._keep += [ps, pz]
+            d.n_patches = ps.size
+            d.patch_start = ps.ctypes.data
+            d.patch_size = pz.ctypes.data
+        d.two_d = int(self.geometry.get("two_d", 0))
+        d.empty_dir = int(self.geometry.get("empty_dir", -1))
+        h = C.c_void_p()
+        check(load().vlm_mesh_register(self.ctx.handle, C.byref(d), merge_levels, C.byref(h)), self.ctx.handle)
+        self._h = h
+        _live.add(self)
+
+    @classmethod
+    def from_arrays(cls, m: dict, **kw) -> "Mesh":
+        """From a dict with the cfd::Mesh array names (n_cells, owner, neighbour, magSf, ndc, ...)."""
+        return cls(m["n_cells"], m["owner"], m["neighbour"], m["magSf"], m["ndc"], n_faces=len(m["owner"]),
+                   geometry=m, **kw)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def gamg_levels(self):
+        """The device hierarchy's per-level {n, l, u, agg} (natural numbering)."""
+        L = load()
+        nl = C.c_int32()
+        check(L.vlm_gamg_levels(self._h, C.byref(nl)))
+        out = []
+        for k in range(nl.value):
+            s = np.zeros(3, np.int32)
+            check(L.vlm_gamg_level(self._h, k, _ptr(s), None, None, None))
+            l = np.zeros(s[1], np.int32)
+            u = np.zeros(s[1], np.int32)
+            agg = np.zeros(s[2], np.int32)
+            check(L.vlm_gamg_level(self._h, k, _ptr(s), _ptr(l), _ptr(u), _ptr(agg)))
+            out.append(dict(n=int(s[0]), l=l, u=u, agg=agg))
+        return out
+
+    def colours(self, level):
+        n = C.c_int32()
+        check(load().vlm_gamg_colours(self._h, level, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().vlm_mesh_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_ldu(mesh: Mesh, diag, upper, lower, b, x, ctrl: SolverControls) -> SolverPerformance:
+    """solveLdu (LinearSolver.cpp:135): solves in place into x (float64 numpy array)."""
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+        raise TypeError("x must be a C-contiguous float64 array (solved in place)")
+    diag, upper, b = _f64(diag), _f64(upper), _f64(b)
+    lower = None if lower is None else _f64(lower)
+    c = ctrl.to_c()
+    p = _ffi.SolverPerf()
+    check(load().vlm_ldu_solve(mesh.ctx.handle, mesh.handle, _ptr(diag), _ptr(upper), _ptr(lower), _ptr(b), _ptr(x),
+                               C.byref(c), C.byref(p)), mesh.ctx.handle)
+    return SolverPerformance.from_c(p)
+
+
+def solve_ldu_device(mesh: Mesh, diag_ptr, upper_ptr, lower_ptr, b_ptr, x_ptr, ctrl: SolverControls) -> SolverPerformance:
+    """Device-pointer variant (integers, e.g. torch tensor data_ptr()) ordered on the mesh context's stream."""
+    c = ctrl.to_c()
+    p = _ffi.SolverPerf()
+    check(load().vlm_ldu_solve_device(mesh.ctx.handle, mesh.handle, C.c_void_p(diag_ptr), C.c_void_p(upper_ptr),
+                                      C.c_void_p(lower_ptr) if lower_ptr else None, C.c_void_p(b_ptr),
+                                      C.c_void_p(x_ptr), C.byref(c), C.byref(p)), mesh.ctx.handle)
+    return SolverPerformance.from_c(p)
+
+
+def amul(mesh: Mesh, diag, upper, lower, x):
+    """y = A x (LinearSolver.cpp:121-133)."""
+    y = np.zeros(mesh.n_cells)
+    check(load().vlm_amul(mesh.ctx.handle, mesh.handle, _ptr(_f64(diag)), _ptr(_f64(upper)),
+                          None if lower is None else _ptr(_f64(lower)), _ptr(_f64(x)), _ptr(y)), mesh.ctx.handle)
+    return y
+
+
+def gamg_apply(mesh: Mesh, diag, upper, lower, r, smoother: str = ""):
+    """One device V-cycle w = M^-1 r."""
+    w = np.zeros(mesh.n_cells)
+    c = SolverControls(smoother=smoother).to_c()
+    check(load().vlm_gamg_apply(mesh.ctx.handle, mesh.handle, _ptr(_f64(diag)), _ptr(_f64(upper)),
+                                None if lower is None else _ptr(_f64(lower)), _ptr(_f64(r)), _ptr(w), C.byref(c)),
+          mesh.ctx.handle)
+    return w

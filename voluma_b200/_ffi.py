@@ -1,0 +1,87 @@
+"""ctypes binding of include/voluma_b200.h (the library's C ABI)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libvoluma_b200.so")
+
+STATUS = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "OOM", 4: "SINGULAR", 5: "NONFINITE", 6: "TIMEOUT",
+          7: "UNSUPPORTED", 8: "NO_DEVICE"}
+
+# every entry point include/voluma_b200.h declares
+EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_stream", "vlm_mesh_register",
+           "vlm_mesh_release", "vlm_amul", "vlm_ldu_solve", "vlm_ldu_solve_device", "vlm_gamg_apply",
+           "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum"]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_cells", C.c_int32), ("n_internal_faces", C.c_int32), ("n_faces", C.c_int32),
+                ("owner", C.c_void_p), ("neighbour", C.c_void_p), ("magSf", C.c_void_p), ("ndc", C.c_void_p),
+                ("V", C.c_void_p), ("Sf", C.c_void_p), ("d", C.c_void_p), ("w", C.c_void_p),
+                ("corrVecs", C.c_void_p), ("two_d", C.c_int32), ("empty_dir", C.c_int32), ("n_patches", C.c_int32),
+                ("patch_start", C.c_void_p), ("patch_size", C.c_void_p)]
+
+
+class SolverCtrl(C.Structure):
+    _fields_ = [("solver", C.c_char * 32), ("preconditioner", C.c_char * 32), ("tolerance", C.c_double),
+                ("relTol", C.c_double), ("maxIter", C.c_int32), ("minIter", C.c_int32), ("nSweeps", C.c_int32),
+                ("smoother", C.c_char * 16), ("precision", C.c_char * 16), ("reproducible", C.c_int32),
+                ("mergeLevels", C.c_int32), ("innerRelTol", C.c_double)]
+
+
+class SolverPerf(C.Structure):
+    _fields_ = [("initialResidual", C.c_double), ("finalResidual", C.c_double), ("residualSum", C.c_double),
+                ("normFactor", C.c_double), ("iterations", C.c_int32), ("converged", C.c_int32),
+                ("outerIterations", C.c_int32), ("status", C.c_int32), ("solver", C.c_char * 32)]
+
+
+_lib = None
+
+
+def load():
+    """Loads the native library; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"voluma_b200 native library missing: {LIB_PATH} (run python -m voluma_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    i32 = C.c_int32
+    L.vlm_last_error.restype = C.c_char_p
+    L.vlm_last_error.argtypes = [P]
+    L.vlm_ctx_create.argtypes = [C.c_int, C.POINTER(P)]
+    L.vlm_ctx_destroy.argtypes = [P]
+    L.vlm_ctx_stream.restype = P
+    L.vlm_ctx_stream.argtypes = [P]
+    L.vlm_mesh_register.argtypes = [P, C.POINTER(MeshDesc), i32, C.POINTER(P)]
+    L.vlm_mesh_release.argtypes = [P]
+    L.vlm_amul.argtypes = [P, P, P, P, P, P, P]
+    L.vlm_ldu_solve.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]
+    L.vlm_ldu_solve_device.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]
+    L.vlm_gamg_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
+    L.vlm_gamg_levels.argtypes = [P, C.POINTER(i32)]
+    L.vlm_gamg_level.argtypes = [P, i32, P, P, P, P]
+    L.vlm_gamg_colours.argtypes = [P, i32, C.POINTER(i32)]
+    L.vlm_laplacian.argtypes = [P, P, P, P, P, P, i32, i32, P, P, P, P, P, P, P]
+    L.vlm_grad.argtypes = [P, P, P, P, P, i32, P]
+    L.vlm_exact_sum.argtypes = [P, P, C.c_int64, C.POINTER(C.c_double)]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype if name in ("vlm_last_error", "vlm_ctx_stream") else C.c_int
+    _lib = L
+    return L
+
+
+class VlmError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+def check(rc, ctx=None):
+    if rc != 0:
+        msg = load().vlm_last_error(ctx).decode(errors="replace")
+        raise VlmError(rc, msg)

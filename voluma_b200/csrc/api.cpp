@@ -1,0 +1,274 @@
+// extern "C" boundary (include/voluma_b200.h): status codes in, no exceptions out.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "solver.h"
+#include "voluma_b200.h"
+
+struct vlm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int refs = 1;  // the handle itself + one per registered mesh
+};
+
+struct vlm_mesh {
+    vlm_ctx* ctx = nullptr;
+    int nCells = 0, nInternal = 0, nFaces = 0;
+    std::vector<int32_t> own, nei;
+    std::vector<double> magSf, ndc;
+    std::unique_ptr<vlm::DeviceBatch> batch;
+    // staging for the host-pointer entry points
+    vlm::DBuf<double> diag, upper, lower, b, x;
+};
+
+namespace {
+
+thread_local std::string g_lastError;
+
+vlm_status fail(vlm_ctx* ctx, vlm_status s, const std::string& msg) {
+    g_lastError = msg;
+    if (ctx) ctx->err = msg;
+    return s;
+}
+
+template <class F> vlm_status guarded(vlm_ctx* ctx, F&& f) {
+    try {
+        f();
+        return VLM_OK;
+    } catch (const vlm::Error& e) {
+        return fail(ctx, e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, VLM_ERR_OOM, "host allocation failed");
+    } catch (const std::invalid_argument& e) {
+        return fail(ctx, VLM_ERR_BAD_ARG, e.what());
+    } catch (const std::exception& e) {
+        return fail(ctx, VLM_ERR_CUDA, e.what());
+    }
+}
+
+void setDevice(vlm_ctx* ctx) { VLM_CUDA(cudaSetDevice(ctx->device)); }
+
+// Uploads the host LDU coefficients of a mesh into its staging buffers; returns the device
+// pointers (lower aliases upper when the host lower pointer is NULL).
+void stageCoeffs(vlm_mesh* m, const double* diag, const double* upper, const double* lower, const double** dDiag,
+                 const double** dUpper, const double** dLower) {
+    cudaStream_t s = m->ctx->stream;
+    VLM_REQUIRE(diag && upper, VLM_ERR_BAD_ARG, "diag and upper are required");
+    m->diag.upload(diag, size_t(m->nCells), s);
+    if (m->nInternal > 0)
+        m->upper.upload(upper, size_t(m->nInternal), s);
+    else
+        m->upper.resize(1);
+    *dDiag = m->diag.get();
+    *dUpper = m->upper.get();
+    if (lower && lower != upper) {
+        if (m->nInternal > 0)
+            m->lower.upload(lower, size_t(m->nInternal), s);
+        else
+            m->lower.resize(1);
+        *dLower = m->lower.get();
+    } else {
+        *dLower = m->upper.get();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+vlm_status vlm_ctx_create(int device, vlm_ctx** out) {
+    if (!out) return fail(nullptr, VLM_ERR_BAD_ARG, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(nullptr, VLM_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return fail(nullptr, VLM_ERR_BAD_ARG, "device index out of range");
+    auto* c = new vlm_ctx;
+    c->device = device;
+    vlm_status st = guarded(c, [&] {
+        setDevice(c);
+        VLM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    });
+    if (st != VLM_OK) {
+        delete c;
+        return st;
+    }
+    *out = c;
+    return VLM_OK;
+}
+
+namespace {
+// Drops one reference; the stream is destroyed with the last one, so meshes released after
+// their context handle still find a valid stream.
+void ctxUnref(vlm_ctx* ctx) {
+    if (--ctx->refs > 0) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+}  // namespace
+
+vlm_status vlm_ctx_destroy(vlm_ctx* ctx) {
+    if (!ctx) return VLM_OK;
+    ctxUnref(ctx);
+    return VLM_OK;
+}
+
+const char* vlm_last_error(const vlm_ctx* ctx) { return ctx ? ctx->err.c_str() : g_lastError.c_str(); }
+
+void* vlm_ctx_stream(vlm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* d, int32_t mergeLevels, vlm_mesh** out) {
+    if (!ctx || !d || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        VLM_REQUIRE(d->n_cells > 0 && d->n_internal_faces >= 0 && d->n_faces >= d->n_internal_faces, VLM_ERR_BAD_ARG,
+                    "invalid mesh sizes");
+        VLM_REQUIRE(d->owner && (d->neighbour || d->n_internal_faces == 0), VLM_ERR_BAD_ARG,
+                    "owner/neighbour are required");
+        VLM_REQUIRE(d->magSf && d->ndc, VLM_ERR_BAD_ARG, "magSf and ndc are required (GAMG weights)");
+        setDevice(ctx);
+        auto m = std::make_unique<vlm_mesh>();
+        m->ctx = ctx;
+        m->nCells = d->n_cells;
+        m->nInternal = d->n_internal_faces;
+        m->nFaces = d->n_faces;
+        m->own.assign(d->owner, d->owner + d->n_faces);
+        m->nei.assign(d->neighbour, d->neighbour + d->n_internal_faces);
+        m->magSf.assign(d->magSf, d->magSf + d->n_faces);
+        m->ndc.assign(d->ndc, d->ndc + d->n_faces);
+        vlm::SysTopo t;
+        t.nCells = m->nCells;
+        t.nInternal = m->nInternal;
+        t.own = m->own.data();
+        t.nei = m->nei.data();
+        t.magSf = m->magSf.data();
+        t.ndc = m->ndc.data();
+        m->batch = std::make_unique<vlm::DeviceBatch>(std::vector<vlm::SysTopo>{t}, mergeLevels > 0 ? mergeLevels : 2,
+                                                      ctx->stream);
+        ctx->refs++;
+        *out = m.release();
+    });
+}
+
+vlm_status vlm_mesh_release(vlm_mesh* mesh) {
+    if (!mesh) return VLM_OK;
+    vlm_ctx* ctx = mesh->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete mesh;
+    ctxUnref(ctx);
+    return VLM_OK;
+}
+
+vlm_status vlm_amul(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const double* upper, const double* lower,
+                    const double* x, double* y) {
+    if (!ctx || !m || !x || !y) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        const double *dd, *du, *dl;
+        stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
+        m->x.upload(x, size_t(m->nCells), ctx->stream);
+        m->b.resize(size_t(m->nCells));
+        m->batch->amul(dd, du, dl, m->x.get(), m->b.get());
+        VLM_CUDA(cudaMemcpy(y, m->b.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost));
+    });
+}
+
+vlm_status vlm_ldu_solve_device(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const double* upper,
+                                const double* lower, const double* b, double* x, const vlm_solver_ctrl* ctrl,
+                                vlm_solver_perf* perf) {
+    if (!ctx || !m || !diag || !upper || !b || !x || !ctrl) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        std::vector<vlm_solver_perf> p;
+        m->batch->solve(diag, upper, lower ? lower : upper, b, x, *ctrl, p);
+        if (perf) *perf = p[0];
+    });
+}
+
+vlm_status vlm_ldu_solve(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const double* upper, const double* lower,
+                         const double* b, double* x, const vlm_solver_ctrl* ctrl, vlm_solver_perf* perf) {
+    if (!ctx || !m || !diag || !upper || !b || !x || !ctrl) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        cudaStream_t s = ctx->stream;
+        const double *dd, *du, *dl;
+        stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
+        m->b.upload(b, size_t(m->nCells), s);
+        m->x.upload(x, size_t(m->nCells), s);
+        std::vector<vlm_solver_perf> p;
+        m->batch->solve(dd, du, dl, m->b.get(), m->x.get(), *ctrl, p);
+        VLM_CUDA(cudaMemcpyAsync(x, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+        if (perf) *perf = p[0];
+    });
+}
+
+vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const double* upper, const double* lower,
+                          const double* r, double* w, const vlm_solver_ctrl* ctrl) {
+    if (!ctx || !m || !r || !w) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        const double *dd, *du, *dl;
+        stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
+        m->b.upload(r, size_t(m->nCells), ctx->stream);
+        m->x.resize(size_t(m->nCells));
+        vlm::SmootherKind sm = vlm::SmootherKind::MCGS;
+        if (ctrl && std::string(ctrl->smoother) == "jacobi") sm = vlm::SmootherKind::Jacobi;
+        m->batch->gamgApply(dd, du, dl, m->b.get(), m->x.get(), sm);
+        VLM_CUDA(cudaMemcpy(w, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost));
+    });
+}
+
+vlm_status vlm_gamg_levels(vlm_mesh* m, int32_t* n) {
+    if (!m || !n) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    *n = int32_t(m->batch->plan().H[0].levels.size());
+    return VLM_OK;
+}
+
+vlm_status vlm_gamg_level(vlm_mesh* m, int32_t level, int32_t* sizes, int32_t* l, int32_t* u, int32_t* agg) {
+    if (!m || !sizes) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    const auto& H = m->batch->plan().H[0];
+    if (level < 0 || level >= int32_t(H.levels.size())) return fail(m->ctx, VLM_ERR_BAD_ARG, "level out of range");
+    const auto& L = H.levels[level];
+    sizes[0] = L.n;
+    sizes[1] = int32_t(L.l.size());
+    sizes[2] = int32_t(L.agg.size());
+    if (l) std::copy(L.l.begin(), L.l.end(), l);
+    if (u) std::copy(L.u.begin(), L.u.end(), u);
+    if (agg) std::copy(L.agg.begin(), L.agg.end(), agg);
+    return VLM_OK;
+}
+
+vlm_status vlm_gamg_colours(vlm_mesh* m, int32_t level, int32_t* n) {
+    if (!m || !n) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    if (level < 0 || level >= m->batch->nLevels()) return fail(m->ctx, VLM_ERR_BAD_ARG, "level out of range");
+    *n = m->batch->level(level).maxColours;
+    return VLM_OK;
+}
+
+vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh*, const double*, const double*, const int32_t*, const double*,
+                         int32_t, int32_t, double*, double*, double*, double*, double*, double*, int32_t*) {
+    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_laplacian: not built yet");
+}
+
+vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh*, const double*, const int32_t*, const double*, int32_t, double*) {
+    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_grad: not built yet");
+}
+
+vlm_status vlm_exact_sum(vlm_ctx* ctx, const double*, int64_t, double*) {
+    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_exact_sum: not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,50 @@
+// Plain structs shared by the host orchestration and the device kernels.
+#pragma once
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace vlm {
+
+// Per-system solver state, resident on the device.
+struct SysState {
+    double normFactor, initialResidual, finalResidual, residualSum;
+    double wArA, wArAold, alpha, beta, omega, rho, rhoOld, s0, s1;
+    double innerInit, innerFinal;  // mixed precision inner solve (FP32 L1 norms)
+    int iterations, converged, done, status;
+    int innerIterations, innerDone, outer, pad;
+};
+
+// Solve controls as seen by the device.
+struct DevCtrl {
+    double tolerance, relTol, innerRelTol;
+    int maxIter, minIter, maxInner;
+};
+
+// Double-double accumulator of the compensated reductions.
+struct DD {
+    double hi, lo;
+};
+
+// Reduction context: per-CTA partial slots and per-system completion counters.
+struct RedCtx {
+    DD* partials;           // [slot * NV + q]
+    int* counters;          // per system
+    const int* slotBegin;   // per system
+    const int* slotEnd;
+};
+
+// SELL-32 structure of one level.
+struct Sell {
+    const int32_t* slPtr;
+    const int32_t* rlen;
+    const int32_t* col;
+};
+
+// Coarsest-level solve of one system.
+struct CoarseDev {
+    int rowStart, n, invOffset, sys;
+};
+
+}  // namespace vlm

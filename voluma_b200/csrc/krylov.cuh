@@ -1,0 +1,453 @@
+// Krylov-level kernels: initial residual + normFactor, PCG and PBiCGStab vector updates
+// fused with their global reductions, FP64 defect correction around an FP32 inner solve.
+// Scalar recurrences (alpha, beta, omega, convergence) are evaluated on the device by the
+// CTA that completes a system's reduction, so an iteration needs no host round trip.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace vlm {
+
+// converged() of LinearSolver.cpp:114-117
+__device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, double finalRes, double initRes) {
+    if (iters < c.minIter) return false;
+    return finalRes < c.tolerance || (c.relTol > 0 && finalRes < c.relTol * initRes);
+}
+
+// ------------------------------------------------------------------ initial residual
+// Sum of x (for the normFactor reference value x̄, LinearSolver.cpp:157-159).
+template <class T>
+__global__ void __launch_bounds__(kRowsPerCta) k_sum_x(const Chunk* __restrict__ ch, const T* __restrict__ x, RedCtx R,
+                                                       SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) v[0].hi = (double)x[c.start + threadIdx.x];
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) st[c.sys].s0 = out[0];
+}
+
+// wA = A x, pA = A x̄, r = b - wA; normFactor = Σ|wA-pA|+|b-pA| + 1e-20; residualSum = Σ|r|
+// (LinearSolver.cpp:149-174).  r32 (optional) receives (float)r for the mixed inner solve.
+__global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __restrict__ ch, Sell S,
+                                                               const double* __restrict__ val,
+                                                               const double* __restrict__ diag,
+                                                               const double* __restrict__ x, const double* __restrict__ b,
+                                                               const int32_t* __restrict__ perm, double* __restrict__ r,
+                                                               float* __restrict__ r32, const int32_t* __restrict__ nCells,
+                                                               RedCtx R, SysState* st, const DevCtrl* __restrict__ ctrlp) {
+    const Chunk c = ch[blockIdx.x];
+    const double xRef = st[c.sys].s0 / (double)nCells[c.sys];
+    DD v[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const double wA = row_plus(S, val, x, row, diag[row] * x[row]);
+        // A x̄ with the same entry order as amul on a constant vector
+        const int len = S.rlen[row], base = sell_base(S, row);
+        double pA = diag[row] * xRef;
+        for (int k = 0; k < len; ++k) pA += val[base + (k << 5)] * xRef;
+        const double rr = b[row] - wA;
+        r[row] = rr;
+        if (r32) r32[row] = (float)rr;
+        if (perm[row] >= 0) {
+            v[0].hi = fabs(wA - pA) + fabs(b[row] - pA);
+            v[1].hi = fabs(rr);
+        }
+    }
+    double out[2];
+    if (reduce_to_system<2>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.normFactor = out[0] + 1e-20;
+        s.residualSum = out[1];
+        s.initialResidual = s.residualSum / s.normFactor;
+        s.finalResidual = s.initialResidual;
+        s.iterations = 0;
+        s.outer = 0;
+        s.wArA = kGREAT;
+        s.rho = 0.0;
+        s.alpha = 0.0;
+        s.omega = 0.0;
+        s.innerInit = out[1];
+        if (s.initialResidual < ctrlp->tolerance && ctrlp->minIter <= 0) {
+            s.converged = 1;
+            s.done = 1;
+        }
+        if (!isfinite(s.initialResidual)) {
+            s.status = VLM_ERR_NONFINITE;
+            s.done = 1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ preconditioners
+template <class T>
+__global__ void __launch_bounds__(kRowsPerCta) k_precond_diag(const Chunk* __restrict__ ch, const T* __restrict__ rD,
+                                                              const T* __restrict__ r, T* __restrict__ w,
+                                                              const SysState* st, int flag) {
+    const Chunk c = ch[blockIdx.x];
+    if (sys_idle(st[c.sys], flag) || (int)threadIdx.x >= c.count) return;
+    const int row = c.start + threadIdx.x;
+    w[row] = rD[row] * r[row];
+}
+
+// rD = 1/diag (LinearSolver.cpp:66,78); padding rows: 0
+template <class T>
+__global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* __restrict__ d, T* __restrict__ rD) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rD[i] = valid[i] >= 0 ? T(1) / d[i] : T(0);
+}
+
+// ------------------------------------------------------------------ PCG (LinearSolver.cpp:176-201)
+// wArA = Σ w·r ; beta = wArA / wArAold
+template <class T, int FLAG>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restrict__ ch, const T* __restrict__ w,
+                                                            const T* __restrict__ r, RedCtx R, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (sys_idle(st[c.sys], FLAG)) return;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        v[0].hi = (double)w[row] * (double)r[row];
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
+        s.wArAold = s.wArA;
+        s.wArA = out[0];
+        s.beta = it == 0 ? 0.0 : s.wArA / s.wArAold;
+    }
+}
+
+// p = w (first iteration) or w + beta p
+template <class T, int FLAG>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__ ch, const T* __restrict__ w,
+                                                       T* __restrict__ p, const SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    const SysState& s = st[c.sys];
+    if (sys_idle(s, FLAG) || (int)threadIdx.x >= c.count) return;
+    const int row = c.start + threadIdx.x;
+    const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
+    if (it == 0)
+        p[row] = w[row];
+    else
+        p[row] = w[row] + (T)s.beta * p[row];
+}
+
+// Ap = A p ; wApA = Σ Ap·p ; alpha = wArA / wApA (break when |wApA| < VSMALL)
+template <class T, int FLAG>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
+                                                          const T* __restrict__ diag, const T* __restrict__ p,
+                                                          T* __restrict__ Ap, RedCtx R, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (sys_idle(st[c.sys], FLAG)) return;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const T y = row_plus(S, val, p, row, diag[row] * p[row]);
+        Ap[row] = y;
+        v[0].hi = (double)y * (double)p[row];
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        if (fabs(out[0]) < kVSMALL) {
+            if (FLAG == kFlagDone) {
+                s.done = 1;
+            } else {
+                s.innerDone = 1;
+                s.s1 = 1.0;  // inner breakdown: the outer loop stops after this correction
+            }
+        } else {
+            s.alpha = s.wArA / out[0];
+        }
+    }
+}
+
+// x += alpha p ; r -= alpha Ap ; finalResidual = Σ|r| / normFactor ; convergence
+template <class T, int FLAG>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restrict__ ch, T* __restrict__ x, T* __restrict__ r,
+                                                            const T* __restrict__ p, const T* __restrict__ Ap,
+                                                            const int32_t* __restrict__ perm, RedCtx R, SysState* st,
+                                                            const DevCtrl* __restrict__ ctrlp) {
+    const Chunk c = ch[blockIdx.x];
+    if (sys_idle(st[c.sys], FLAG)) return;
+    const T alpha = (T)st[c.sys].alpha;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        x[row] += alpha * p[row];
+        const T rr = r[row] - alpha * Ap[row];
+        r[row] = rr;
+        v[0].hi = fabs((double)rr);
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        if (FLAG == kFlagDone) {
+            s.finalResidual = out[0] / s.normFactor;
+            s.iterations += 1;
+            if (!isfinite(s.finalResidual)) {
+                s.status = VLM_ERR_NONFINITE;
+                s.done = 1;
+            } else if (s.iterations >= ctrlp->maxIter || dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+                s.done = 1;
+            }
+        } else {
+            s.innerFinal = out[0];
+            s.innerIterations += 1;
+            s.iterations += 1;
+            if (!isfinite(out[0])) {
+                s.status = VLM_ERR_NONFINITE;
+                s.innerDone = 1;
+                s.done = 1;
+            } else if (s.innerIterations >= ctrlp->maxInner || s.iterations >= ctrlp->maxIter ||
+                       s.innerFinal < ctrlp->innerRelTol * s.innerInit) {
+                s.innerDone = 1;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ mixed precision outer loop
+// start of an inner solve: e = 0 is done by a memset; reset the inner recurrences.
+__global__ void k_inner_begin(int nsys, SysState* st) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    SysState& q = st[s];
+    q.innerIterations = 0;
+    q.innerDone = q.done;
+    q.s1 = 0.0;
+    q.wArA = kGREAT;
+}
+
+// x64 += e32 ; then r64 = b - A x64 in a second kernel (neighbours must be updated first)
+__global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
+                                                               const float* __restrict__ e, const SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done || (int)threadIdx.x >= c.count) return;
+    const int row = c.start + threadIdx.x;
+    x[row] += (double)e[row];
+}
+
+// FP64 defect: r = b - A x (exact FP64 matrix), r32 = (float) r, finalResidual = Σ|r| / nf
+__global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __restrict__ ch, Sell S,
+                                                                const double* __restrict__ val,
+                                                                const double* __restrict__ diag,
+                                                                const double* __restrict__ x,
+                                                                const double* __restrict__ b, double* __restrict__ r,
+                                                                float* __restrict__ r32, RedCtx R, SysState* st,
+                                                                const DevCtrl* __restrict__ ctrlp) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const double wA = row_plus(S, val, x, row, diag[row] * x[row]);
+        const double rr = b[row] - wA;
+        r[row] = rr;
+        r32[row] = (float)rr;
+        v[0].hi = fabs(rr);
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.finalResidual = out[0] / s.normFactor;
+        s.innerInit = out[0];
+        s.outer += 1;
+        if (!isfinite(s.finalResidual)) {
+            s.status = VLM_ERR_NONFINITE;
+            s.done = 1;
+        } else if (s.iterations >= ctrlp->maxIter || s.outer >= ctrlp->maxIter || s.s1 != 0.0 ||
+                   dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+            s.done = 1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ PBiCGStab (LinearSolver.cpp:202-237)
+// rho = Σ r0·r ; beta = (rho/rhoOld)(alpha/omega), break on |rhoOld| or |omega| < VSMALL
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restrict__ ch, const double* __restrict__ r0,
+                                                          const double* __restrict__ r, RedCtx R, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        v[0].hi = r0[row] * r[row];
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.rhoOld = s.rho;
+        s.rho = out[0];
+        if (s.iterations > 0) {
+            if (fabs(s.rhoOld) < kVSMALL || fabs(s.omega) < kVSMALL)
+                s.done = 1;
+            else
+                s.beta = (s.rho / s.rhoOld) * (s.alpha / s.omega);
+        }
+    }
+}
+
+// p = r (first) or r + beta (p - omega Ay)
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_p(const Chunk* __restrict__ ch, const double* __restrict__ r,
+                                                        const double* __restrict__ Ay, double* __restrict__ p,
+                                                        const SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    const SysState& s = st[c.sys];
+    if (s.done || (int)threadIdx.x >= c.count) return;
+    const int row = c.start + threadIdx.x;
+    if (s.iterations == 0)
+        p[row] = r[row];
+    else
+        p[row] = r[row] + s.beta * (p[row] - s.omega * Ay[row]);
+}
+
+// Ay = A y ; alpha = rho / Σ r0·Ay (break when < VSMALL)
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __restrict__ ch, Sell S,
+                                                                 const double* __restrict__ val,
+                                                                 const double* __restrict__ diag,
+                                                                 const double* __restrict__ y, double* __restrict__ Ay,
+                                                                 const double* __restrict__ r0, RedCtx R, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const double a = row_plus(S, val, y, row, diag[row] * y[row]);
+        Ay[row] = a;
+        v[0].hi = r0[row] * a;
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        if (fabs(out[0]) < kVSMALL)
+            s.done = 1;
+        else
+            s.alpha = s.rho / out[0];
+    }
+}
+
+// s = r - alpha Ay ; iterations++ ; finalResidual = Σ|s|/nf ; converged -> early exit flag (s0 = 1)
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict__ ch, const double* __restrict__ r,
+                                                        const double* __restrict__ Ay, double* __restrict__ sv, RedCtx R,
+                                                        SysState* st, const DevCtrl* __restrict__ ctrlp) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    const double alpha = st[c.sys].alpha;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const double s = r[row] - alpha * Ay[row];
+        sv[row] = s;
+        v[0].hi = fabs(s);
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.iterations += 1;
+        s.finalResidual = out[0] / s.normFactor;
+        s.s1 = 0.0;
+        if (!isfinite(s.finalResidual)) {
+            s.status = VLM_ERR_NONFINITE;
+            s.done = 1;
+        } else if (dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+            s.s1 = 1.0;  // early exit: x += alpha y, then stop
+        }
+    }
+}
+
+// early exit of LinearSolver.cpp:224-227
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_early(const Chunk* __restrict__ ch, double* __restrict__ x,
+                                                            const double* __restrict__ y, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    SysState& s = st[c.sys];
+    if (s.done || s.s1 == 0.0) return;
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        x[row] += s.alpha * y[row];
+    }
+}
+
+// closes the early exit (separate launch so every CTA above saw s1 before done is set)
+__global__ void k_bicg_early_close(int nsys, SysState* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nsys && !st[i].done && st[i].s1 != 0.0) {
+        st[i].converged = 1;
+        st[i].done = 1;
+    }
+}
+
+// t = A z ; tAtA = Σ t·t ; tAsA = Σ t·s ; omega = tAtA > VSMALL ? tAsA/tAtA : 0
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __restrict__ ch, Sell S,
+                                                                 const double* __restrict__ val,
+                                                                 const double* __restrict__ diag,
+                                                                 const double* __restrict__ z, double* __restrict__ t,
+                                                                 const double* __restrict__ sv, RedCtx R, SysState* st) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    DD v[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        const double a = row_plus(S, val, z, row, diag[row] * z[row]);
+        t[row] = a;
+        v[0].hi = a * a;
+        v[1].hi = a * sv[row];
+    }
+    double out[2];
+    if (reduce_to_system<2>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.omega = out[0] > kVSMALL ? out[1] / out[0] : 0.0;
+    }
+}
+
+// x += alpha y + omega z ; r = s - omega t ; finalResidual = Σ|r| / nf
+__global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __restrict__ ch, double* __restrict__ x,
+                                                             double* __restrict__ r, const double* __restrict__ y,
+                                                             const double* __restrict__ z, const double* __restrict__ sv,
+                                                             const double* __restrict__ t, RedCtx R, SysState* st,
+                                                             const DevCtrl* __restrict__ ctrlp) {
+    const Chunk c = ch[blockIdx.x];
+    if (st[c.sys].done) return;
+    const double alpha = st[c.sys].alpha, omega = st[c.sys].omega;
+    DD v[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) {
+        const int row = c.start + threadIdx.x;
+        x[row] += alpha * y[row] + omega * z[row];
+        const double rr = sv[row] - omega * t[row];
+        r[row] = rr;
+        v[0].hi = fabs(rr);
+    }
+    double out[1];
+    if (reduce_to_system<1>(v, c, R, out)) {
+        SysState& s = st[c.sys];
+        s.finalResidual = out[0] / s.normFactor;
+        if (!isfinite(s.finalResidual)) {
+            s.status = VLM_ERR_NONFINITE;
+            s.done = 1;
+        } else if (s.iterations >= ctrlp->maxIter || dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+            s.done = 1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ plain SpMV (amul)
+__global__ void __launch_bounds__(kRowsPerCta) k_amul(const Chunk* __restrict__ ch, Sell S, const double* __restrict__ val,
+                                                      const double* __restrict__ diag, const double* __restrict__ x,
+                                                      double* __restrict__ y) {
+    const Chunk c = ch[blockIdx.x];
+    if ((int)threadIdx.x >= c.count) return;
+    const int row = c.start + threadIdx.x;
+    y[row] = row_plus(S, val, x, row, diag[row] * x[row]);
+}
+
+// iteration-loop predicate: any system still running
+__global__ void k_any_active(int nsys, const SysState* st, int flag, int* out) {
+    int a = 0;
+    for (int i = threadIdx.x; i < nsys; i += blockDim.x) a |= sys_idle(st[i], flag) ? 0 : 1;
+    a = __syncthreads_or(a);
+    if (threadIdx.x == 0) *out = a;
+}
+
+}  // namespace vlm

@@ -1,0 +1,259 @@
+// Builds the device layout plan of a batch (see plan.h).  Host-only, once per mesh set.
+#include "plan.h"
+
+#include <algorithm>
+#include <numeric>
+#include <stdexcept>
+
+namespace vlm {
+
+namespace {
+
+int pad32(int n) { return (n + kSlice - 1) / kSlice * kSlice; }
+
+void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slot) {
+    for (int s = 0; s < len; s += kRowsPerCta) {
+        Chunk c;
+        c.start = start + s;
+        c.count = std::min(kRowsPerCta, len - s);
+        c.sys = sys;
+        c.slot = slot ? (*slot)++ : 0;
+        out.push_back(c);
+    }
+}
+
+}  // namespace
+
+BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
+    BatchPlan P;
+    const int ns = int(systems.size());
+    if (ns == 0) throw std::invalid_argument("empty batch");
+    P.nsys = ns;
+    P.userCellBase.resize(ns);
+    P.userFaceBase.resize(ns);
+    for (int s = 0; s < ns; ++s) {
+        P.userCellBase[s] = P.userCells;
+        P.userFaceBase[s] = P.userFaces;
+        P.userCells += systems[s].nCells;
+        P.userFaces += systems[s].nInternal;
+    }
+    if (P.userCells >= (int64_t(1) << 31) - 1 || P.userFaces >= (int64_t(1) << 31) - 1)
+        throw std::invalid_argument("batch exceeds 2^31 cells/faces");
+
+    std::vector<Hierarchy> Hin(ns);
+    for (int s = 0; s < ns; ++s) {
+        const SysTopo& t = systems[s];
+        if (t.nCells <= 0) throw std::invalid_argument("system with no cells");
+        Hin[s] = buildHierarchy(t.nCells, t.nInternal, t.own, t.nei, t.magSf, t.ndc, mergeLevels);
+    }
+    P.order.resize(ns);
+    std::iota(P.order.begin(), P.order.end(), 0);
+    std::stable_sort(P.order.begin(), P.order.end(),
+                     [&](int a, int b) { return Hin[a].levels.size() > Hin[b].levels.size(); });
+    P.H.resize(ns);
+    P.nLevels.resize(ns);
+    P.sysCells.resize(ns);
+    for (int b = 0; b < ns; ++b) {
+        P.H[b] = std::move(Hin[P.order[b]]);
+        P.nLevels[b] = int(P.H[b].levels.size());
+        P.sysCells[b] = P.H[b].levels[0].n;
+    }
+    const int Lmax = P.nLevels[0];
+    P.levels.resize(Lmax);
+
+    // ---------------------------------------------------------------- row layout per level
+    // rowOf[k][b][natural] -> solver row
+    std::vector<std::vector<std::vector<int32_t>>> rowOf(Lmax, std::vector<std::vector<int32_t>>(ns));
+    std::vector<std::vector<std::vector<std::pair<int, int>>>> groups(Lmax, std::vector<std::vector<std::pair<int, int>>>(ns));
+    for (int k = 0; k < Lmax; ++k) {
+        LevelPlan& LP = P.levels[k];
+        int row = 0;
+        int present = 0, active = 0;
+        for (int b = 0; b < ns; ++b) {
+            if (P.nLevels[b] > k) present = b + 1;
+            if (P.nLevels[b] - 1 > k) active = b + 1;
+        }
+        LP.sysRow.assign(size_t(present) + 1, 0);
+        LP.sysFace.assign(size_t(present) + 1, 0);
+        int64_t faceCount = 0;
+        for (int b = 0; b < present; ++b) {
+            const HLevel& L = P.H[b].levels[k];
+            LP.sysRow[b] = row;
+            LP.sysFace[b] = k == 0 ? int32_t(P.userFaceBase[P.order[b]]) : int32_t(faceCount);
+            faceCount += int64_t(L.l.size());
+            auto& ro = rowOf[k][b];
+            ro.assign(size_t(L.n), -1);
+            auto place = [&](int i) {
+                ro[i] = row;
+                LP.natural.push_back(i);
+                LP.rowSys.push_back(b);
+                ++row;
+            };
+            auto pad = [&]() {
+                while (row % kSlice) {
+                    LP.natural.push_back(-1);
+                    LP.rowSys.push_back(-1);
+                    ++row;
+                }
+            };
+            if (b < active) {
+                int nc = 0;
+                const std::vector<int> colour = greedyColour(L, &nc);
+                LP.maxColours = std::max(LP.maxColours, nc);
+                std::vector<std::vector<int>> byColour(static_cast<size_t>(nc));
+                for (int i = 0; i < L.n; ++i) byColour[colour[i]].push_back(i);
+                for (int c = 0; c < nc; ++c) {
+                    const int g0 = row;
+                    for (int i : byColour[c]) place(i);
+                    pad();
+                    groups[k][b].push_back({g0, row - g0});
+                }
+            } else {
+                for (int i = 0; i < L.n; ++i) place(i);
+                pad();
+            }
+        }
+        LP.sysRow[present] = row;
+        LP.sysFace[present] = k == 0 ? int32_t(P.userFaces) : int32_t(faceCount);
+        LP.nrows = row;
+        LP.nfaces = k == 0 ? int(P.userFaces) : int(faceCount);
+        LP.nActiveRows = LP.sysRow[active];
+        LP.sysRow.resize(size_t(present) + 1);
+        // chunks
+        int slot = 0;
+        for (int b = 0; b < present; ++b) {
+            const int s0 = LP.sysRow[b], len = LP.sysRow[b + 1] - LP.sysRow[b];
+            if (k == 0) P.sysSlotBegin.push_back(slot);
+            appendChunks(LP.all, s0, len, b, &slot);
+            if (k == 0) P.sysSlotEnd.push_back(slot);
+            if (b < active) appendChunks(LP.active, s0, len, b, nullptr);
+        }
+        if (k == 0) P.nSlots = slot;
+        int nSteps = 0;
+        for (int b = 0; b < active; ++b) nSteps = std::max(nSteps, int(groups[k][b].size()));
+        LP.nSteps = nSteps;
+        LP.fwd.assign(size_t(nSteps), {});
+        LP.rev.assign(size_t(nSteps), {});
+        for (int t = 0; t < nSteps; ++t)
+            for (int b = 0; b < active; ++b) {
+                const auto& g = groups[k][b];
+                const int nc = int(g.size());
+                if (t < nc) {
+                    appendChunks(LP.fwd[t], g[t].first, g[t].second, b, nullptr);
+                    appendChunks(LP.rev[t], g[nc - 1 - t].first, g[nc - 1 - t].second, b, nullptr);
+                }
+            }
+    }
+
+    // ---------------------------------------------------------------- SELL-32 structure
+    for (int k = 0; k < Lmax; ++k) {
+        LevelPlan& LP = P.levels[k];
+        const int nsl = LP.nrows / kSlice;
+        LP.rlen.assign(size_t(LP.nrows), 0);
+        LP.slPtr.assign(size_t(nsl) + 1, 0);
+        for (int r = 0; r < LP.nrows; ++r) {
+            const int b = LP.rowSys[r];
+            if (b < 0) continue;
+            const HLevel& L = P.H[b].levels[k];
+            const int i = LP.natural[r];
+            LP.rlen[r] = L.off[i + 1] - L.off[i];
+        }
+        for (int s = 0; s < nsl; ++s) {
+            int w = 0;
+            for (int q = 0; q < kSlice; ++q) w = std::max(w, LP.rlen[s * kSlice + q]);
+            LP.slPtr[s + 1] = LP.slPtr[s] + w * kSlice;
+        }
+        LP.col.assign(size_t(LP.slPtr[nsl]), 0);
+        LP.src.assign(size_t(LP.slPtr[nsl]), 0);
+        for (int r = 0; r < LP.nrows; ++r) {
+            const int b = LP.rowSys[r];
+            if (b < 0) {
+                continue;
+            }
+            const HLevel& L = P.H[b].levels[k];
+            const int i = LP.natural[r];
+            const int base = LP.slPtr[r / kSlice] + (r % kSlice);
+            const int32_t fb = LP.sysFace[b];
+            const SysTopo& T = systems[P.order[b]];
+            for (int e = L.off[i]; e < L.off[i + 1]; ++e) {
+                const int q = e - L.off[i];
+                const int f = L.adjFace[e];
+                LP.col[size_t(base) + size_t(q) * kSlice] = rowOf[k][b][L.adjCell[e]];
+                bool useUpper;
+                if (k == 0)
+                    useUpper = T.own[f] == i;  // user arrays are owner-oriented
+                else
+                    useUpper = L.adjIsL[e] != 0;
+                const int32_t g = fb + f;
+                LP.src[size_t(base) + size_t(q) * kSlice] = useUpper ? g : ~g;
+            }
+        }
+        // padding rows point at themselves (never read: rlen = 0)
+    }
+
+    // ---------------------------------------------------------------- transfer maps
+    for (int k = 0; k + 1 < Lmax; ++k) {
+        LevelPlan& LP = P.levels[k];
+        const LevelPlan& NP = P.levels[k + 1];
+        LP.agg.assign(size_t(LP.nrows), -1);
+        LP.childPtr.assign(size_t(NP.nrows) + 1, 0);
+        LP.intraPtr.assign(size_t(NP.nrows) + 1, 0);
+        LP.cfacePtr.assign(size_t(NP.nfaces) + 1, 0);
+        std::vector<std::vector<int32_t>> kids(size_t(NP.nrows)), intra(size_t(NP.nrows)),
+            cf(size_t(NP.nfaces));
+        const int activeSys = int(NP.sysRow.size()) - 1;  // systems present on k+1 = active on k
+        for (int b = 0; b < activeSys; ++b) {
+            const HLevel& L = P.H[b].levels[k];
+            const int32_t fb = LP.sysFace[b], nfb = NP.sysFace[b];
+            for (int i = 0; i < L.n; ++i) {
+                const int R = rowOf[k + 1][b][L.agg[i]];
+                LP.agg[rowOf[k][b][i]] = R;
+                kids[R].push_back(rowOf[k][b][i]);
+            }
+            const bool lev0 = k == 0;
+            for (size_t f = 0; f < L.l.size(); ++f) {
+                const int c = L.faceMap[f];
+                const int32_t g = fb + int32_t(f);
+                if (c < 0) {
+                    intra[rowOf[k + 1][b][L.agg[L.l[f]]]].push_back(g);
+                } else {
+                    bool flip = L.faceFlip[f] != 0;
+                    if (lev0 && !P.H[b].ownerIsL[f]) flip = !flip;
+                    cf[size_t(nfb + c)].push_back(int32_t(uint32_t(g) | (flip ? 0x80000000u : 0u)));
+                }
+            }
+        }
+        for (int R = 0; R < NP.nrows; ++R) {
+            LP.childPtr[R + 1] = LP.childPtr[R] + int(kids[R].size());
+            LP.intraPtr[R + 1] = LP.intraPtr[R] + int(intra[R].size());
+        }
+        for (int c = 0; c < NP.nfaces; ++c) LP.cfacePtr[c + 1] = LP.cfacePtr[c] + int(cf[c].size());
+        for (auto& v : kids) LP.child.insert(LP.child.end(), v.begin(), v.end());
+        for (auto& v : intra) LP.intraFace.insert(LP.intraFace.end(), v.begin(), v.end());
+        for (auto& v : cf) LP.cfaceSrc.insert(LP.cfaceSrc.end(), v.begin(), v.end());
+    }
+
+    // ---------------------------------------------------------------- coarse solves, level-0 map
+    P.coarse.resize(ns);
+    int inv = 0;
+    for (int b = 0; b < ns; ++b) {
+        const int Lc = P.nLevels[b] - 1;
+        CoarsePlan c;
+        c.level = Lc;
+        c.rowStart = P.levels[Lc].sysRow[b];
+        c.n = P.H[b].levels[Lc].n;
+        c.invOffset = inv;
+        c.sys = b;
+        inv += c.n * c.n;
+        P.coarse[b] = c;
+    }
+    P.invTotal = inv;
+    const LevelPlan& L0 = P.levels[0];
+    P.perm0.assign(size_t(L0.nrows), -1);
+    for (int r = 0; r < L0.nrows; ++r)
+        if (L0.rowSys[r] >= 0)
+            P.perm0[r] = int32_t(P.userCellBase[P.order[L0.rowSys[r]]] + L0.natural[r]);
+    return P;
+}
+
+}  // namespace vlm

@@ -1,0 +1,621 @@
+// Solve drivers of the device-resident LDU batch: per-solve setup (coefficient
+// materialisation, Galerkin coarsening, coarsest LU), the GAMG V-cycle, PCG / PBiCGStab
+// and the FP64-defect-correction mixed-precision PCG.  Each solve's iteration loop is one
+// CUDA graph launch: a conditional WHILE node whose body is one iteration and whose
+// predicate is set on the device from the per-system convergence flags.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstdio>
+#include <set>
+
+#include "krylov.cuh"
+#include "solver.h"
+
+namespace vlm {
+
+GraphExec::~GraphExec() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+}
+
+static bool eq(const char* a, const char* b) { return std::strcmp(a, b) == 0; }
+
+SolverKind parseSolver(const char* s) {
+    if (eq(s, "PCG")) return SolverKind::PCG;
+    if (eq(s, "PBiCGStab")) return SolverKind::PBiCGStab;
+    if (eq(s, "Jacobi")) return SolverKind::Jacobi;
+    if (eq(s, "GaussSeidel")) return SolverKind::GaussSeidel;
+    if (eq(s, "symGaussSeidel")) return SolverKind::SymGaussSeidel;
+    throw Error(VLM_ERR_UNSUPPORTED, std::string("unknown linear solver ") + s);
+}
+
+PrecondKind parsePrecond(const char* s) {
+    if (eq(s, "none")) return PrecondKind::None;
+    if (eq(s, "diagonal")) return PrecondKind::Diagonal;
+    if (eq(s, "GAMG")) return PrecondKind::GAMG;
+    if (eq(s, "DIC")) return PrecondKind::DIC;
+    if (eq(s, "DILU")) return PrecondKind::DILU;
+    throw Error(VLM_ERR_UNSUPPORTED, std::string("unknown preconditioner ") + s);
+}
+
+namespace {
+
+inline int nblk(int n, int t = 256) { return (n + t - 1) / t; }
+
+// Launch helper: skips empty grids (a zero-block launch is an error).
+#define VLM_LAUNCH(kernel, grid, block, stream, ...)                    \
+    do {                                                                \
+        if ((grid) > 0) kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__); \
+    } while (0)
+
+template <class T> struct LV;
+template <> struct LV<double> {
+    static double* r(DevLevel& L) { return L.r.get(); }
+    static double* x(DevLevel& L) { return L.x.get(); }
+    static double* t(DevLevel& L) { return L.t.get(); }
+    static double* x2(DevLevel& L) { return L.x2.get(); }
+    static const double* val(const DevLevel& L) { return L.val.get(); }
+    static const double* diag(const DevLevel& L) { return L.diag.get(); }
+};
+template <> struct LV<float> {
+    static float* r(DevLevel& L) { return L.r32.get(); }
+    static float* x(DevLevel& L) { return L.x32.get(); }
+    static float* t(DevLevel& L) { return L.t32.get(); }
+    static float* x2(DevLevel& L) { return L.x232.get(); }
+    static const float* val(const DevLevel& L) { return L.val32.get(); }
+    static const float* diag(const DevLevel& L) { return L.diag32.get(); }
+};
+
+__global__ void k_set_cond(cudaGraphConditionalHandle h, int nsys, const SysState* st, int flag) {
+    int a = 0;
+    for (int i = threadIdx.x; i < nsys; i += blockDim.x) a |= sys_idle(st[i], flag) ? 0 : 1;
+    a = __syncthreads_or(a);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, a ? 1u : 0u);
+}
+
+std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
+    size_t n = 0;
+    VLM_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> v(n);
+    if (n) VLM_CUDA(cudaGraphGetNodes(g, v.data(), &n));
+    return v;
+}
+
+}  // namespace
+
+// ====================================================================== construction
+DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
+    : stream_(stream) {
+    plan_ = buildPlan(systems, mergeLevels);
+    const int nL = int(plan_.levels.size());
+    L_.resize(nL);
+    const char* om = std::getenv("VLM_JACOBI_OMEGA");
+    if (om) jacobiOmega_ = std::atof(om);
+    // coarse descriptors grouped by level
+    std::vector<CoarseDev> cds;
+    for (int k = 0; k < nL; ++k) {
+        L_[k].coarse.off = int(cds.size());
+        for (const auto& c : plan_.coarse)
+            if (c.level == k) cds.push_back(CoarseDev{c.rowStart, c.n, c.invOffset, c.sys});
+        L_[k].coarse.n = int(cds.size()) - L_[k].coarse.off;
+    }
+    coarse_.upload(cds, stream_);
+    for (int k = 0; k < nL; ++k) {
+        LevelPlan& P = plan_.levels[k];
+        DevLevel& D = L_[k];
+        D.nrows = P.nrows;
+        D.nfaces = P.nfaces;
+        D.nActiveRows = P.nActiveRows;
+        D.nSteps = P.nSteps;
+        D.maxColours = P.maxColours;
+        D.nent = P.slPtr.back();
+        D.slPtr.upload(P.slPtr, stream_);
+        D.rlen.upload(P.rlen, stream_);
+        D.col.upload(P.col, stream_);
+        D.src.upload(P.src, stream_);
+        std::vector<Chunk> all;
+        auto add = [&](const std::vector<Chunk>& v) {
+            ChunkList l{int(all.size()), int(v.size())};
+            all.insert(all.end(), v.begin(), v.end());
+            return l;
+        };
+        D.active = add(P.active);
+        D.all = add(P.all);
+        for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
+        for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
+        D.chunks.upload(all, stream_);
+        if (k + 1 < nL) {
+            D.agg.upload(P.agg, stream_);
+            D.childPtr.upload(P.childPtr, stream_);
+            D.child.upload(P.child, stream_);
+            D.intraPtr.upload(P.intraPtr, stream_);
+            D.intraFace.upload(P.intraFace, stream_);
+            D.cfacePtr.upload(P.cfacePtr, stream_);
+            D.cfaceSrc.upload(P.cfaceSrc, stream_);
+        }
+        D.diag.resize(size_t(D.nrows));
+        D.val.resize(size_t(std::max(D.nent, 1)));
+        if (k > 0) {
+            D.up.resize(size_t(std::max(D.nfaces, 1)));
+            D.lo.resize(size_t(std::max(D.nfaces, 1)));
+            D.r.resize(size_t(D.nrows));
+            D.x.resize(size_t(D.nrows));
+        }
+        D.t.resize(size_t(D.nrows));
+        D.x2.resize(size_t(D.nrows));
+        // host-side plan data no longer needed on the device path
+        std::vector<int32_t>().swap(P.col);
+        std::vector<int32_t>().swap(P.src);
+    }
+    lu_.resize(size_t(std::max(plan_.invTotal, 1)));
+    inv_.resize(size_t(std::max(plan_.invTotal, 1)));
+    perm0_.upload(plan_.perm0, stream_);
+    sysCells_.upload(plan_.sysCells, stream_);
+    slotBegin_.upload(plan_.sysSlotBegin, stream_);
+    slotEnd_.upload(plan_.sysSlotEnd, stream_);
+    counters_.resize(size_t(plan_.nsys));
+    counters_.zero(stream_);
+    status_.resize(1);
+    partials_.resize(size_t(plan_.nSlots) * 2);
+    st_.resize(size_t(plan_.nsys));
+    st_.zero(stream_);
+    dctrl_.resize(1);
+    anyActive_.resize(1);
+    const int n0 = L_[0].nrows;
+    x_.resize(n0);
+    b_.resize(n0);
+    r_.resize(n0);
+    w_.resize(n0);
+    p_.resize(n0);
+    Ap_.resize(n0);
+    hostState_.resize(size_t(plan_.nsys));
+    VLM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+DeviceBatch::~DeviceBatch() { graphs_.clear(); }
+
+size_t DeviceBatch::deviceBytes() const {
+    size_t b = 0;
+    for (const auto& D : L_)
+        b += D.slPtr.bytes() + D.rlen.bytes() + D.col.bytes() + D.src.bytes() + D.chunks.bytes() + D.agg.bytes() +
+             D.childPtr.bytes() + D.child.bytes() + D.intraPtr.bytes() + D.intraFace.bytes() + D.cfacePtr.bytes() +
+             D.cfaceSrc.bytes() + D.diag.bytes() + D.val.bytes() + D.up.bytes() + D.lo.bytes() + D.diag32.bytes() +
+             D.val32.bytes() + D.r.bytes() + D.x.bytes() + D.t.bytes() + D.x2.bytes() + D.r32.bytes() +
+             D.x32.bytes() + D.t32.bytes() + D.x232.bytes();
+    b += lu_.bytes() + inv_.bytes() + perm0_.bytes() + partials_.bytes();
+    b += x_.bytes() + b_.bytes() + r_.bytes() + w_.bytes() + p_.bytes() + Ap_.bytes() + rD_.bytes() + r0_.bytes() +
+         y_.bytes() + Ay_.bytes() + s_.bytes() + z_.bytes() + t_.bytes();
+    b += e32_.bytes() + r32_.bytes() + w32_.bytes() + p32_.bytes() + Ap32_.bytes() + rD32_.bytes();
+    return b;
+}
+
+void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
+    const size_t n0 = size_t(L_[0].nrows);
+    if (bicg && r0_.size() != n0) {
+        r0_.resize(n0);
+        y_.resize(n0);
+        Ay_.resize(n0);
+        s_.resize(n0);
+        z_.resize(n0);
+        t_.resize(n0);
+    }
+    if (mixed && e32_.size() != n0) {
+        e32_.resize(n0);
+        r32_.resize(n0);
+        w32_.resize(n0);
+        p32_.resize(n0);
+        Ap32_.resize(n0);
+        for (size_t k = 0; k < L_.size(); ++k) {
+            DevLevel& D = L_[k];
+            D.diag32.resize(size_t(D.nrows));
+            D.val32.resize(size_t(std::max(D.nent, 1)));
+            if (k > 0) {
+                D.r32.resize(size_t(D.nrows));
+                D.x32.resize(size_t(D.nrows));
+            }
+            D.t32.resize(size_t(D.nrows));
+            D.x232.resize(size_t(D.nrows));
+        }
+    }
+}
+
+RedCtx DeviceBatch::red() const {
+    return RedCtx{partials_.get(), counters_.get(), slotBegin_.get(), slotEnd_.get()};
+}
+
+// ====================================================================== per-solve setup
+void DeviceBatch::setupMatrix(const double* diag, const double* upper, const double* lower, bool gamg, bool mixed) {
+    cudaStream_t s = stream_;
+    DevLevel& D0 = L_[0];
+    VLM_LAUNCH(k_gather_diag0<double>, nblk(D0.nrows), 256, s, D0.nrows, perm0_.get(), diag, D0.diag.get());
+    if (mixed) VLM_LAUNCH(k_gather_diag0<float>, nblk(D0.nrows), 256, s, D0.nrows, perm0_.get(), diag, D0.diag32.get());
+    VLM_LAUNCH(k_materialize, nblk(D0.nent), 256, s, D0.nent, D0.src.get(), upper, lower, D0.val.get(),
+               mixed ? D0.val32.get() : nullptr);
+    if (!gamg) return;
+    const int nL = int(L_.size());
+    for (int k = 0; k + 1 < nL; ++k) {
+        DevLevel& F = L_[k];
+        DevLevel& C = L_[k + 1];
+        const double* up = k == 0 ? upper : F.up.get();
+        const double* lo = k == 0 ? lower : F.lo.get();
+        VLM_LAUNCH(k_galerkin_diag, nblk(C.nrows), 256, s, C.nrows, F.childPtr.get(), F.child.get(), F.intraPtr.get(),
+                   F.intraFace.get(), F.diag.get(), up, lo, C.diag.get(), mixed ? C.diag32.get() : nullptr);
+        VLM_LAUNCH(k_galerkin_faces, nblk(C.nfaces), 256, s, C.nfaces, F.cfacePtr.get(), F.cfaceSrc.get(), up, lo,
+                   C.up.get(), C.lo.get());
+        VLM_LAUNCH(k_materialize, nblk(C.nent), 256, s, C.nent, C.src.get(), C.up.get(), C.lo.get(), C.val.get(),
+                   mixed ? C.val32.get() : nullptr);
+    }
+    VLM_CUDA(cudaMemsetAsync(status_.get(), 0, sizeof(int), s));
+    for (int k = 0; k < nL; ++k) {
+        DevLevel& D = L_[k];
+        VLM_LAUNCH(k_coarse_factor, D.coarse.n, 128, s, coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
+                   D.diag.get(), lu_.get(), inv_.get(), status_.get());
+    }
+}
+
+// ====================================================================== V-cycle
+template <class T>
+void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag) {
+    DevLevel& D = L_[k];
+    cudaStream_t s = stream_;
+    const Sell S = D.sell();
+    const T* val = LV<T>::val(D);
+    const T* diag = LV<T>::diag(D);
+    const SysState* st = st_.get();
+    if (sm == SmootherKind::MCGS) {
+        if (pre) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
+        for (int sweep = 0; sweep < 2; ++sweep)
+            for (int t = 0; t < D.nSteps; ++t) {
+                const ChunkList& l = pre ? D.fwd[t] : D.rev[t];
+                VLM_LAUNCH(k_smooth_gs<T>, l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, st, flag);
+            }
+    } else {
+        T* x2 = LV<T>::x2(D);
+        const T om = T(jacobiOmega_);
+        if (pre) {
+            VLM_LAUNCH((k_smooth_jacobi<T, true>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r,
+                       (const T*)nullptr, x2, om, st, flag);
+            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+                       om, st, flag);
+        } else {
+            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x, x2,
+                       om, st, flag);
+            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+                       om, st, flag);
+        }
+    }
+}
+
+// GamgPreconditioner::vcycle (GAMG.cpp:403-443) for every system of the batch at once:
+// descend (2 pre-sweeps, residual, restriction) through the levels on which at least one
+// system still smooths, solve every system's coarsest level, then ascend (prolongation,
+// 2 post-sweeps).
+template <class T>
+void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag) {
+    cudaStream_t s = stream_;
+    const int nL = int(L_.size());
+    const SysState* st = st_.get();
+    auto rr = [&](int k) -> const T* { return k == 0 ? r0 : LV<T>::r(L_[k]); };
+    auto xx = [&](int k) -> T* { return k == 0 ? x0 : LV<T>::x(L_[k]); };
+    for (int k = 0; k + 1 < nL; ++k) {
+        DevLevel& D = L_[k];
+        DevLevel& N = L_[k + 1];
+        recordSmooth<T>(k, rr(k), xx(k), sm, true, flag);
+        VLM_LAUNCH(k_residual<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.sell(), LV<T>::val(D), LV<T>::diag(D),
+                   rr(k), xx(k), LV<T>::t(D), st, flag);
+        VLM_LAUNCH(k_restrict<T>, N.all.n, kRowsPerCta, s, N.ch(N.all), D.childPtr.get(), D.child.get(), LV<T>::t(D),
+                   LV<T>::r(N), st, flag);
+    }
+    for (int k = 0; k < nL; ++k) {
+        DevLevel& D = L_[k];
+        VLM_LAUNCH(k_coarse_apply<T>, D.coarse.n, 128, s, coarse_.get() + D.coarse.off, inv_.get(), rr(k), xx(k), st,
+                   flag);
+    }
+    for (int k = nL - 2; k >= 0; --k) {
+        DevLevel& D = L_[k];
+        VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st, flag);
+        recordSmooth<T>(k, rr(k), xx(k), sm, false, flag);
+    }
+}
+
+void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w) {
+    DevLevel& D0 = L_[0];
+    switch (pk) {
+    case PrecondKind::GAMG: recordVcycle<double>(r, w, sm, kFlagDone); break;
+    case PrecondKind::Diagonal:
+        VLM_LAUNCH(k_precond_diag<double>, D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), rD_.get(), r, w, st_.get(),
+                   kFlagDone);
+        break;
+    case PrecondKind::None:
+        VLM_LAUNCH(k_copy_rows<double>, D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), r, w, st_.get(), kFlagDone);
+        break;
+    default: throw Error(VLM_ERR_UNSUPPORTED, "preconditioner not available on the device");
+    }
+}
+
+// ====================================================================== iteration bodies
+void DeviceBatch::recordPcgIter(PrecondKind pk, SmootherKind sm) {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    recordPrecond(pk, sm, r_.get(), w_.get());
+    VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), r_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
+    VLM_LAUNCH((k_pcg_spmv<double, kFlagDone>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), p_.get(),
+               Ap_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_update<double, kFlagDone>), nb, kRowsPerCta, s, ch, x_.get(), r_.get(), p_.get(), Ap_.get(),
+               perm0_.get(), red(), st_.get(), dctrl_.get());
+}
+
+void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    if (pk == PrecondKind::GAMG)
+        recordVcycle<float>(r32_.get(), w32_.get(), sm, kFlagInner);
+    else if (pk == PrecondKind::Diagonal)
+        VLM_LAUNCH(k_precond_diag<float>, nb, kRowsPerCta, s, ch, rD32_.get(), r32_.get(), w32_.get(), st_.get(),
+                   kFlagInner);
+    else
+        throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs the GAMG or diagonal preconditioner");
+    VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
+    VLM_LAUNCH((k_pcg_spmv<float, kFlagInner>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), D0.diag32.get(),
+               p32_.get(), Ap32_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_update<float, kFlagInner>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
+               Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get());
+}
+
+void DeviceBatch::recordBicgIter(PrecondKind pk, SmootherKind sm) {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    SysState* st = st_.get();
+    VLM_LAUNCH(k_bicg_rho, nb, kRowsPerCta, s, ch, r0_.get(), r_.get(), red(), st);
+    VLM_LAUNCH(k_bicg_p, nb, kRowsPerCta, s, ch, r_.get(), Ay_.get(), p_.get(), st);
+    recordPrecond(pk, sm, p_.get(), y_.get());
+    VLM_LAUNCH(k_bicg_spmv_alpha, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), y_.get(), Ay_.get(),
+               r0_.get(), red(), st);
+    VLM_LAUNCH(k_bicg_s, nb, kRowsPerCta, s, ch, r_.get(), Ay_.get(), s_.get(), red(), st, dctrl_.get());
+    VLM_LAUNCH(k_bicg_early, nb, kRowsPerCta, s, ch, x_.get(), y_.get(), st);
+    VLM_LAUNCH(k_bicg_early_close, nblk(plan_.nsys), 256, s, plan_.nsys, st);
+    recordPrecond(pk, sm, s_.get(), z_.get());
+    VLM_LAUNCH(k_bicg_spmv_omega, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), z_.get(), t_.get(),
+               s_.get(), red(), st);
+    VLM_LAUNCH(k_bicg_update, nb, kRowsPerCta, s, ch, x_.get(), r_.get(), y_.get(), z_.get(), s_.get(), t_.get(), red(),
+               st, dctrl_.get());
+}
+
+void DeviceBatch::recordSetCond(cudaGraphConditionalHandle h, int flag) {
+    k_set_cond<<<1, 256, 0, stream_>>>(h, plan_.nsys, st_.get(), flag);
+}
+
+// ====================================================================== graphs
+namespace {
+
+// Stream-captures `body` into graph g after `deps`; returns the new leaf node.
+template <class F>
+cudaGraphNode_t captureInto(cudaStream_t s, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, F&& body) {
+    const auto before = nodesOf(g);
+    const std::set<cudaGraphNode_t> old(before.begin(), before.end());
+    VLM_CUDA(cudaStreamBeginCaptureToGraph(s, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                           cudaStreamCaptureModeRelaxed));
+    try {
+        body();
+    } catch (...) {
+        cudaGraph_t junk;
+        cudaStreamEndCapture(s, &junk);
+        throw;
+    }
+    cudaGraph_t out;
+    VLM_CUDA(cudaStreamEndCapture(s, &out));
+    cudaGraphNode_t leaf = nullptr;
+    for (cudaGraphNode_t n : nodesOf(g)) {
+        if (old.count(n)) continue;
+        size_t nd = 0;
+        VLM_CUDA(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
+        if (nd == 0) leaf = n;
+    }
+    if (!leaf) throw Error(VLM_ERR_CUDA, "graph capture produced no nodes");
+    return leaf;
+}
+
+cudaGraphNode_t addWhile(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    VLM_CUDA(cudaGraphAddNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
+    *body = p.conditional.phGraph_out[0];
+    return node;
+}
+
+}  // namespace
+
+void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
+    VLM_CUDA(cudaGraphCreate(&G.graph, 0));
+    cudaStream_t s = stream_;
+    if (!key.mixed) {
+        cudaGraphConditionalHandle h;
+        VLM_CUDA(cudaGraphConditionalHandleCreate(&h, G.graph, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t pre = captureInto(s, G.graph, {}, [&] { recordSetCond(h, kFlagDone); });
+        cudaGraph_t body;
+        addWhile(G.graph, pre, h, &body);
+        captureInto(s, body, {}, [&] {
+            if (key.solver == SolverKind::PCG)
+                recordPcgIter(key.precond, key.smoother);
+            else
+                recordBicgIter(key.precond, key.smoother);
+            recordSetCond(h, kFlagDone);
+        });
+    } else {
+        cudaGraphConditionalHandle ho;
+        VLM_CUDA(cudaGraphConditionalHandleCreate(&ho, G.graph, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t pre = captureInto(s, G.graph, {}, [&] { recordSetCond(ho, kFlagDone); });
+        cudaGraph_t outer;
+        addWhile(G.graph, pre, ho, &outer);
+        cudaGraphConditionalHandle hi;
+        VLM_CUDA(cudaGraphConditionalHandleCreate(&hi, outer, 0, cudaGraphCondAssignDefault));
+        DevLevel& D0 = L_[0];
+        const Chunk* ch = D0.ch(D0.all);
+        const int nb = D0.all.n;
+        cudaGraphNode_t seg1 = captureInto(s, outer, {}, [&] {
+            VLM_LAUNCH(k_inner_begin, nblk(plan_.nsys), 256, s, plan_.nsys, st_.get());
+            VLM_LAUNCH(k_zero_rows<float>, nb, kRowsPerCta, s, ch, e32_.get(), st_.get(), kFlagInner);
+            recordSetCond(hi, kFlagInner);
+        });
+        cudaGraph_t inner;
+        cudaGraphNode_t w = addWhile(outer, seg1, hi, &inner);
+        captureInto(s, inner, {}, [&] {
+            recordInnerPcgIter(key.precond, key.smoother);
+            recordSetCond(hi, kFlagInner);
+        });
+        captureInto(s, outer, {w}, [&] {
+            VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), e32_.get(), st_.get());
+            VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
+                       b_.get(), r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
+            recordSetCond(ho, kFlagDone);
+        });
+    }
+    VLM_CUDA(cudaGraphInstantiate(&G.exec, G.graph, 0));
+}
+
+GraphExec& DeviceBatch::graphFor(const SolveKey& key) {
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) return *it->second;
+    auto g = std::make_unique<GraphExec>();
+    buildGraph(key, *g);
+    GraphExec& ref = *g;
+    graphs_.emplace(key, std::move(g));
+    return ref;
+}
+
+// ====================================================================== entry points
+void DeviceBatch::solve(const double* diag, const double* upper, const double* lower, const double* b, double* x,
+                        const vlm_solver_ctrl& ctrl, std::vector<vlm_solver_perf>& perfOut) {
+    cudaStream_t s = stream_;
+    SolverKind sk = parseSolver(ctrl.solver);
+    PrecondKind pk = parsePrecond(ctrl.preconditioner);
+    if (ctrl.reproducible) {
+        // CFD_REPRODUCIBLE semantics (LinearSolver.cpp:138-148)
+        if (pk != PrecondKind::None) pk = PrecondKind::Diagonal;
+        if (sk == SolverKind::GaussSeidel || sk == SolverKind::SymGaussSeidel) sk = SolverKind::Jacobi;
+    }
+    const bool symmetric = lower == upper;
+    if (sk == SolverKind::PCG && !symmetric)
+        throw Error(VLM_ERR_UNSUPPORTED, "PCG requires a symmetric matrix; use PBiCGStab");
+    if (sk == SolverKind::PBiCGStab && pk == PrecondKind::DIC) pk = PrecondKind::DILU;
+    if (sk != SolverKind::PCG && sk != SolverKind::PBiCGStab)
+        throw Error(VLM_ERR_UNSUPPORTED, std::string("solver ") + ctrl.solver + " is not available on the device");
+    if (pk == PrecondKind::DIC || pk == PrecondKind::DILU)
+        throw Error(VLM_ERR_UNSUPPORTED, std::string("preconditioner ") + ctrl.preconditioner +
+                                             " is not available on the device");
+    const SmootherKind sm = (ctrl.smoother[0] == 0 || eq(ctrl.smoother, "mcgs")) ? SmootherKind::MCGS
+                            : eq(ctrl.smoother, "jacobi")
+                                ? SmootherKind::Jacobi
+                                : throw Error(VLM_ERR_BAD_ARG, std::string("unknown smoother ") + ctrl.smoother);
+    const bool mixed = eq(ctrl.precision, "mixed");
+    if (!mixed && ctrl.precision[0] != 0 && !eq(ctrl.precision, "fp64"))
+        throw Error(VLM_ERR_BAD_ARG, std::string("unknown precision ") + ctrl.precision);
+    if (mixed && sk != SolverKind::PCG) throw Error(VLM_ERR_UNSUPPORTED, "mixed precision is implemented for PCG");
+    if (mixed && pk == PrecondKind::None) throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs a preconditioner");
+    ensureVectors(mixed, sk == SolverKind::PBiCGStab);
+
+    setupMatrix(diag, upper, lower, pk == PrecondKind::GAMG, mixed);
+    DevLevel& D0 = L_[0];
+    const int n0 = D0.nrows;
+    if (pk == PrecondKind::Diagonal) {
+        if (rD_.size() != size_t(n0)) rD_.resize(n0);
+        VLM_LAUNCH(k_recip_diag<double>, nblk(n0), 256, s, n0, perm0_.get(), D0.diag.get(), rD_.get());
+        if (mixed) {
+            if (rD32_.size() != size_t(n0)) rD32_.resize(n0);
+            VLM_LAUNCH(k_recip_diag<float>, nblk(n0), 256, s, n0, perm0_.get(), D0.diag32.get(), rD32_.get());
+        }
+    }
+    static thread_local DevCtrl hc;  // stays valid until the synchronising copy below
+    hc.tolerance = ctrl.tolerance;
+    hc.relTol = ctrl.relTol;
+    hc.innerRelTol = ctrl.innerRelTol > 0 ? ctrl.innerRelTol : 1e-4;
+    hc.maxIter = ctrl.maxIter;
+    hc.minIter = ctrl.minIter;
+    hc.maxInner = ctrl.maxIter;
+    VLM_CUDA(cudaMemcpyAsync(dctrl_.get(), &hc, sizeof(DevCtrl), cudaMemcpyHostToDevice, s));
+    st_.zero(s);
+    VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
+    VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), b, b_.get());
+    VLM_LAUNCH(k_sum_x<double>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
+    VLM_LAUNCH(k_init_residual, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(),
+               x_.get(), b_.get(), perm0_.get(), r_.get(), mixed ? r32_.get() : nullptr, sysCells_.get(), red(),
+               st_.get(), dctrl_.get());
+    if (sk == SolverKind::PBiCGStab) {
+        VLM_CUDA(cudaMemcpyAsync(r0_.get(), r_.get(), sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+        Ay_.zero(s);
+        p_.zero(s);
+    }
+    GraphExec& G = graphFor(SolveKey{sk, pk, sm, mixed});
+    VLM_CUDA(cudaGraphLaunch(G.exec, s));
+    VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), x_.get(), x);
+    int coarseStatus = 0;
+    VLM_CUDA(cudaMemcpyAsync(hostState_.data(), st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaStreamSynchronize(s));
+    if (pk == PrecondKind::GAMG && coarseStatus == VLM_ERR_SINGULAR)
+        throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+    perfOut.resize(size_t(plan_.nsys));
+    for (int bpos = 0; bpos < plan_.nsys; ++bpos) {
+        const SysState& q = hostState_[bpos];
+        vlm_solver_perf p = {};
+        p.initialResidual = q.initialResidual;
+        p.finalResidual = q.finalResidual;
+        p.residualSum = q.residualSum;
+        p.normFactor = q.normFactor;
+        p.iterations = q.iterations;
+        p.outerIterations = q.outer;
+        p.status = q.status;
+        // converged() evaluated once more at exit (LinearSolver.cpp:283)
+        p.converged = (p.iterations >= ctrl.minIter) &&
+                      (p.finalResidual < ctrl.tolerance ||
+                       (ctrl.relTol > 0 && p.finalResidual < ctrl.relTol * p.initialResidual));
+        std::snprintf(p.solver, sizeof(p.solver), "%s", sk == SolverKind::PCG ? "PCG" : "PBiCGStab");
+        perfOut[size_t(plan_.order[bpos])] = p;
+    }
+}
+
+void DeviceBatch::amul(const double* diag, const double* upper, const double* lower, const double* x, double* y) {
+    cudaStream_t s = stream_;
+    setupMatrix(diag, upper, lower, false, false);
+    DevLevel& D0 = L_[0];
+    const int n0 = D0.nrows;
+    VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
+    VLM_LAUNCH(k_amul, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
+               w_.get());
+    VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), w_.get(), y);
+    VLM_CUDA(cudaStreamSynchronize(s));
+}
+
+void DeviceBatch::gamgApply(const double* diag, const double* upper, const double* lower, const double* r, double* w,
+                            SmootherKind sm) {
+    cudaStream_t s = stream_;
+    setupMatrix(diag, upper, lower, true, false);
+    DevLevel& D0 = L_[0];
+    const int n0 = D0.nrows;
+    st_.zero(s);
+    VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), r, r_.get());
+    recordVcycle<double>(r_.get(), w_.get(), sm, kFlagDone);
+    VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), w_.get(), w);
+    int coarseStatus = 0;
+    VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaStreamSynchronize(s));
+    if (coarseStatus == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+}
+
+template void DeviceBatch::recordVcycle<double>(const double*, double*, SmootherKind, int);
+template void DeviceBatch::recordVcycle<float>(const float*, float*, SmootherKind, int);
+
+}  // namespace vlm

@@ -1,0 +1,122 @@
+// Device-resident batch of LDU systems with GAMG hierarchies, and the solve drivers.
+#pragma once
+
+#include <map>
+#include <tuple>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "devtypes.h"
+#include "plan.h"
+
+namespace vlm {
+
+struct ChunkList {
+    int off = 0, n = 0;
+};
+
+struct DevLevel {
+    int nrows = 0, nfaces = 0, nActiveRows = 0, nSteps = 0, nent = 0, maxColours = 0;
+    DBuf<int32_t> slPtr, rlen, col, src;
+    DBuf<Chunk> chunks;
+    ChunkList active, all;
+    std::vector<ChunkList> fwd, rev;
+    DBuf<int32_t> agg, childPtr, child, intraPtr, intraFace, cfacePtr, cfaceSrc;
+    ChunkList coarse;  // CoarseDev entries whose coarsest level is this one
+    // numeric, per solve
+    DBuf<double> diag, val, up, lo;
+    DBuf<float> diag32, val32;
+    // V-cycle vectors
+    DBuf<double> r, x, t, x2;
+    DBuf<float> r32, x32, t32, x232;
+    Sell sell() const { return Sell{slPtr.get(), rlen.get(), col.get()}; }
+    const Chunk* ch(const ChunkList& l) const { return chunks.get() + l.off; }
+};
+
+enum class SolverKind { PCG, PBiCGStab, Jacobi, GaussSeidel, SymGaussSeidel };
+enum class PrecondKind { None, Diagonal, GAMG, DIC, DILU };
+enum class SmootherKind { MCGS, Jacobi };
+
+struct SolveKey {
+    SolverKind solver;
+    PrecondKind precond;
+    SmootherKind smoother;
+    bool mixed;
+    bool operator<(const SolveKey& o) const {
+        return std::tie(solver, precond, smoother, mixed) < std::tie(o.solver, o.precond, o.smoother, o.mixed);
+    }
+};
+
+struct GraphExec {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GraphExec();
+};
+
+// A batch of systems resident on one device (a single-system mesh is a batch of one).
+class DeviceBatch {
+public:
+    DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream);
+    ~DeviceBatch();
+
+    const BatchPlan& plan() const { return plan_; }
+    int nLevels() const { return int(L_.size()); }
+    const DevLevel& level(int k) const { return L_[k]; }
+    int64_t userCells() const { return plan_.userCells; }
+    int64_t userFaces() const { return plan_.userFaces; }
+
+    // Coefficients: device pointers to user-layout (concatenated, input order) arrays.
+    // lower == upper for symmetric systems.
+    void setupMatrix(const double* diag, const double* upper, const double* lower, bool gamg, bool mixed);
+
+    // Full solve on device pointers (user layout). perfOut: one per input system (input order).
+    void solve(const double* diag, const double* upper, const double* lower, const double* b, double* x,
+               const vlm_solver_ctrl& ctrl, std::vector<vlm_solver_perf>& perfOut);
+
+    // y = A x (user layout device pointers)
+    void amul(const double* diag, const double* upper, const double* lower, const double* x, double* y);
+
+    // One V-cycle w = M^-1 r (user layout device pointers)
+    void gamgApply(const double* diag, const double* upper, const double* lower, const double* r, double* w,
+                   SmootherKind sm);
+
+    cudaStream_t stream() const { return stream_; }
+    size_t deviceBytes() const;
+
+private:
+    template <class T> void recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag);
+    template <class T> void recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag);
+    void recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w);
+    void recordPcgIter(PrecondKind pk, SmootherKind sm);
+    void recordInnerPcgIter(PrecondKind pk, SmootherKind sm);
+    void recordBicgIter(PrecondKind pk, SmootherKind sm);
+    void recordSetCond(cudaGraphConditionalHandle h, int flag);
+    GraphExec& graphFor(const SolveKey& key);
+    void buildGraph(const SolveKey& key, GraphExec& g);
+    void ensureVectors(bool mixed, bool bicg);
+    RedCtx red() const;
+
+    BatchPlan plan_;
+    std::vector<DevLevel> L_;
+    cudaStream_t stream_;
+    DBuf<CoarseDev> coarse_;
+    DBuf<double> lu_, inv_;
+    DBuf<int32_t> perm0_, sysCells_, slotBegin_, slotEnd_, counters_, status_;
+    DBuf<DD> partials_;
+    DBuf<SysState> st_;
+    DBuf<DevCtrl> dctrl_;
+    DBuf<int> anyActive_;
+    // Krylov vectors, level-0 solver order
+    DBuf<double> x_, b_, r_, w_, p_, Ap_, rD_, r0_, y_, Ay_, s_, z_, t_;
+    DBuf<float> e32_, r32_, w32_, p32_, Ap32_, rD32_;
+    std::map<SolveKey, std::unique_ptr<GraphExec>> graphs_;
+    std::vector<SysState> hostState_;
+    double jacobiOmega_ = 1.0;
+};
+
+SolverKind parseSolver(const char* s);
+PrecondKind parsePrecond(const char* s);
+
+}  // namespace vlm
