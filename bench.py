@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the pressure-equation hot path on B200.
+
+Workload (one step = one pressure solve): the 3D Taylor-Green vortex pressure equation on the
+periodic box [0,2pi]^3 with a uniform 128^3 hex mesh (2,097,152 cells, 6,291,456 faces), as the
+PIMPLE corrector assembles it: fvm::laplacian(rAUf, p) with rAUf = dt = 2e-3, minus the divergence
+of a predicted face flux phi = (u_TG + seeded perturbation)_f . S_f, setReference(cell 0), solved
+from p = 0 with PCG + GAMG to relTol 1e-8 (tolerance 0, the reference's normalised L1 residual).
+Synthetic data: the TG field plus 16 seeded Fourier modes (|k| <= 4, amplitude N(0,1)/|k|^2).
+
+Metric: solves/s (whole job, all GPUs) and p50/p99 latency, mixed precision (FP32 inner
+PCG+V-cycles inside FP64 defect correction) vs FP64 GAMG-PCG.  `value` is the mixed-precision
+rate with inputs resident in HBM; `e2e` is the same through the host-pointer C ABI
+(vlm_ldu_solve: H2D of diag/upper/b/x and D2H of x inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 128]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 2e-3
+REL_TOL = 1e-8
+
+
+# ------------------------------------------------------------------------------ workload
+def tg_velocity(C, seed=1234, n_modes=16, amp=0.1):
+    x, y, z = C[:, 0], C[:, 1], C[:, 2]
+    u = np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), np.zeros_like(x)], 1)
+    rng = np.random.default_rng(seed)
+    for _ in range(n_modes):
+        k = rng.integers(-4, 5, size=3)
+        if not k.any():
+            k[0] = 1
+        kk = float(np.sqrt((k * k).sum()))
+        a = rng.standard_normal(3) / kk ** 2
+        ph = rng.uniform(0, 2 * np.pi)
+        u += amp * np.outer(np.cos(C @ k + ph), a)
+    return u
+
+
+def assemble(m):
+    """LDU pressure system from cfd::Mesh arrays: laplacian(rAUf=DT) (Fvm.h:149-154), source +=
+    divPhi*V (FvMatrix.h:93-97 via Fvc.h:294-304), setReference(0) (FvMatrix.h:134-141)."""
+    nC, nI = m["n_cells"], len(m["neighbour"])
+    own, nei = m["owner"][:nI], m["neighbour"]
+    upper = DT * m["magSf"][:nI] * m["ndc"][:nI]
+    diag = np.zeros(nC)
+    np.subtract.at(diag, np.stack([own, nei], 1).ravel(), np.repeat(upper, 2))
+    u = tg_velocity(m["C"])
+    w = m["w"][:nI, None]
+    uf = w * u[own] + (1.0 - w) * u[nei]
+    Sf = m["Sf"][:nI]
+    phi = uf[:, 0] * Sf[:, 0] + uf[:, 1] * Sf[:, 1] + uf[:, 2] * Sf[:, 2]
+    div = np.zeros(nC)
+    np.add.at(div, np.stack([own, nei], 1).ravel(), np.stack([phi, -phi], 1).ravel())
+    b = (div / m["V"]) * m["V"]
+    b[0] += diag[0] * 0.0
+    diag[0] += diag[0]
+    return diag, upper, b
+
+
+def our_mesh(n):
+    from voluma_b200 import mesh as vm
+    return vm.box_mesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+
+
+def ref_mesh_arrays(n):
+    from oracle import ref
+    R = ref.RefMesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+    m = {k: R.get(k) for k in ("owner", "neighbour", "magSf", "ndc", "C", "w", "Sf", "V")}
+    m["n_cells"] = R.n_cells
+    return R, m
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and
+                          s[4 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, n):
+    """dram bytes per launch of `kernel` at n^3 from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
+    try:
+        for line in open(p):
+            f = line.split()
+            if len(f) >= 3 and f[0] == kernel and int(f[1]) == n:
+                return float(f[2])
+    except Exception:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------ reference arm
+def _ref_worker(args):
+    n, nsolves, q = args
+    sys.path.insert(0, ROOT)
+    R, m = ref_mesh_arrays(n)
+    diag, upper, b = assemble(m)
+    R.gamg_levels()  # builds and caches the hierarchy (GAMG.cpp:204) outside the timed solves
+    times, iters = [], []
+    for _ in range(nsolves):
+        t = time.perf_counter()
+        _, perf = R.solve(diag, upper, None, b, np.zeros(m["n_cells"]), "PCG", "GAMG", 0.0, REL_TOL, 1000)
+        times.append(time.perf_counter() - t)
+        iters.append(perf["iterations"])
+    return times, iters
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    base = {"metric": METRIC, "impl": "reference", "unit": "solves/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup}
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvlmref.so was not built (make -C oracle)"}))
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    P = max(1, min(cores, 8, args.steps))
+    per = max(1, math.ceil(args.steps / P))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(P) as pool:
+        res = pool.map(_ref_worker, [(args.n, per, i) for i in range(P)])
+    wall = time.perf_counter() - t0
+    times = [t for r in res for t in r[0]]
+    iters = [i for r in res for i in r[1]]
+    busy = max(sum(r[0]) for r in res)
+    value = len(times) / busy
+    line = dict(base, value=value, ms_per_step=1e3 * busy / per,
+                p50_ms=1e3 * float(np.percentile(times, 50)), p99_ms=1e3 * float(np.percentile(times, 99)),
+                iterations=int(np.median(iters)), dtype="f64", data="synthetic", scaling="weak", vs_baseline=None,
+                config={"workload": f"TGV {args.n}^3 periodic pressure equation, PCG+GAMG relTol 1e-8",
+                        "cells": args.n ** 3, "solves": len(times), "processes": P},
+                cpu_baseline={"value": value, "unit": "solves/s", "cores": P, "kind": "reference",
+                              "sample": f"{len(times)} full solves over {P} single-threaded processes "
+                                        f"(reference solveLdu PCG+GAMG, hierarchy pre-built), wall {wall:.1f}s"},
+                e2e={"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------ our arm
+METRIC = "solves/s & p99 latency at rtol 1e-8, mixed vs FP64 GAMG-PCG on 1 B200"
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import voluma_b200 as vb
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    m = our_mesh(args.n)
+    diag, upper, b = assemble(m)
+    n, nI = m["n_cells"], m["n_internal_faces"]
+    ctx = vb.Context(local)
+    mesh = vb.Mesh.from_arrays(m, ctx=ctx)
+    ext = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    d_diag = torch.from_numpy(diag).to(dev)
+    d_up = torch.from_numpy(upper).to(dev)
+    d_b = torch.from_numpy(b).to(dev)
+    d_x = torch.zeros(n, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def ctrl(prec):
+        return vb.SolverControls("PCG", "GAMG", 0.0, REL_TOL, 1000, smoother=args.smoother,
+                                 precision="mixed" if prec == "mixed" else "")
+
+    def device_solve(prec):
+        with torch.cuda.stream(ext):
+            d_x.zero_()
+        return vb.solve_ldu_device(mesh, d_diag.data_ptr(), d_up.data_ptr(), 0, d_b.data_ptr(), d_x.data_ptr(),
+                                   ctrl(prec))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    modes = {}
+    sampler = ClockSampler(local)
+    for prec in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            device_solve(prec)
+        barrier()
+        if prec == "mixed":
+            sampler.start()
+        l0 = mesh.stats()[0]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        perfs = []
+        for e0, e1 in ev:
+            with torch.cuda.stream(ext):
+                d_x.zero_()
+            e0.record(ext)
+            perfs.append(vb.solve_ldu_device(mesh, d_diag.data_ptr(), d_up.data_ptr(), 0, d_b.data_ptr(),
+                                             d_x.data_ptr(), ctrl(prec)))
+            e1.record(ext)
+        barrier()
+        launches = mesh.stats()[0] - l0
+        ms = np.array([e0.elapsed_time(e1) for e0, e1 in ev])
+        tot = float(ms.sum())
+        if world > 1:
+            t = torch.tensor([tot], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            tot = float(t.item())
+        modes[prec] = dict(value=world * args.steps / (tot / 1e3), ms_per_step=tot / args.steps,
+                           p50_ms=float(np.percentile(ms, 50)), p99_ms=float(np.percentile(ms, 99)),
+                           iterations=int(np.median([p.iterations for p in perfs])),
+                           outer=int(np.median([p.outerIterations for p in perfs])),
+                           final_rel=float(max(p.finalResidual / max(p.initialResidual, 1e-300) for p in perfs)),
+                           converged=all(p.converged for p in perfs), gpu_launches=int(launches))
+    clocks = sampler.stop()
+    x_mixed = d_x.cpu().numpy()
+    device_solve("fp64")
+    x64 = d_x.cpu().numpy()
+    err_vs_fp64 = float(np.linalg.norm(x_mixed - x64) / np.linalg.norm(x64))
+
+    # e2e: host pinned buffers through vlm_ldu_solve (H2D diag/upper/b/x, D2H x inside the timed region)
+    h_diag = torch.from_numpy(diag).pin_memory().numpy()
+    h_up = torch.from_numpy(upper).pin_memory().numpy()
+    h_b = torch.from_numpy(b).pin_memory().numpy()
+    h_x = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        h_x[:] = 0.0
+        vb.solve_ldu(mesh, h_diag, h_up, None, h_b, h_x, ctrl("mixed"))
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        h_x[:] = 0.0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        vb.solve_ldu(mesh, h_diag, h_up, None, h_b, h_x, ctrl("mixed"))
+        e1.record(ext)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    barrier()
+    e2e_tot = float(np.sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_tot = float(t.item())
+
+    # roofline of the dominant kernel (level-0 multicolour GS sweep of the FP32 inner V-cycle),
+    # timed live with CUDA events on the context stream
+    vb.solve_ldu(mesh, h_diag, h_up, None, h_b, h_x, ctrl("mixed"))
+    k_ms, k_bytes = mesh.profile_kernel("smooth32", 20)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    traffic = ncu_traffic("smooth32", args.n)
+    if rank != 0:
+        return
+    mx = modes["mixed"]
+    line = {
+        "metric": METRIC, "value": mx["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic",
+        "p50_ms": mx["p50_ms"], "p99_ms": mx["p99_ms"],
+        "config": {"workload": f"TGV {args.n}^3 periodic pressure equation (laplacian(rAUf) - div(phiHbyA), "
+                               f"setReference), PCG+GAMG relTol 1e-8 from p=0", "cells": n, "faces": nI,
+                   "smoother": args.smoother or "mcgs", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (matrix hierarchy + vectors > 126 MB)"},
+        "modes": {"mixed": mx, "fp64": modes["fp64"],
+                  "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"],
+                  "mixed_rel_l2_vs_fp64": err_vs_fp64},
+        "e2e": {"value": world * args.steps / (e2e_tot / 1e3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(8 * (n + nI + n + n)), "d2h_bytes_per_step": int(8 * n),
+                "p99_ms": float(np.percentile(e2e_ms, 99))},
+        "roofline": {"kernel": "k_smooth_gs<float> level 0 (one full multicolour sweep)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "ms_per_launch": k_ms,
+                     "alg_bytes_per_launch": k_bytes},
+        "clocks": clocks, "gpu_launches": mx["gpu_launches"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.n, diag, upper, b)
+    print(json.dumps(line))
+
+
+def cpu_baseline(n, diag, upper, b):
+    """One reference solve of the same system on one host core (oracle/_ref), else the port."""
+    try:
+        from oracle import ref
+        if ref.available():
+            R = ref.RefMesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+            R.gamg_levels()
+            t = time.perf_counter()
+            _, perf = R.solve(diag, upper, None, b, np.zeros(R.n_cells), "PCG", "GAMG", 0.0, REL_TOL, 1000)
+            dt = time.perf_counter() - t
+            return {"value": 1.0 / dt, "unit": "solves/s", "cores": 1, "kind": "reference",
+                    "sample": f"one full PCG+GAMG solve of the same {n}^3 system by the reference's solveLdu "
+                              f"({perf['iterations']} iterations, {dt:.1f} s; hierarchy pre-built as the "
+                              f"reference caches it on the Mesh)"}
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "solves/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+    return {"value": None, "unit": "solves/s", "cores": 1, "kind": "reference", "sample": "reference not built"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--smoother", default="")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

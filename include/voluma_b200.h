@@ -151,6 +151,29 @@ vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, cons
 vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh* mesh, const double* psi, const int32_t* bc_type,
                     const double* bc_values, int32_t scheme, double* out);
 
+/* Kernel launches executed on this mesh so far and its device memory footprint in bytes. */
+vlm_status vlm_mesh_stats(vlm_mesh* mesh, int64_t* launches, int64_t* device_bytes);
+/* Measurement hook: times `reps` back-to-back launches of one level-0 kernel on the matrix of
+ * the last solve ("amul64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch
+ * is one full multicolour sweep) with CUDA events on the context stream.  Outputs the mean ms per
+ * launch and the algorithmic bytes of one launch (values + int32 addressing, each array once). */
+vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* mesh, const char* kernel, int32_t reps, double* ms,
+                              double* bytes);
+
+/* ------------------------------------------------------------------ host-only topology */
+/* The GAMG agglomeration hierarchy and the smoother colouring the device uses, built on the
+ * host without touching a GPU (buildHierarchy, src/fvm/linalg/GAMG.cpp:206-261).  */
+typedef struct vlm_topology vlm_topology;
+vlm_status vlm_topology_build(int32_t n_cells, int32_t n_internal_faces, const int32_t* owner,
+                              const int32_t* neighbour, const double* magSf, const double* ndc,
+                              int32_t merge_levels, vlm_topology** out);
+vlm_status vlm_topology_levels(const vlm_topology* t, int32_t* n_levels);
+/* sizes: {n, nFaces, len(agg), nColours}; any output may be NULL */
+vlm_status vlm_topology_level(const vlm_topology* t, int32_t level, int32_t* sizes, int32_t* l, int32_t* u,
+                              double* weight, int32_t* agg, int32_t* face_map, int8_t* face_flip,
+                              int32_t* colour);
+vlm_status vlm_topology_destroy(vlm_topology* t);
+
 /* ------------------------------------------------------------------ reductions */
 /* Order-independent exact sum of n doubles on the device (host pointer in, host result). */
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out);

@@ -1,0 +1,256 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the reference's own results.
+
+Tolerances: integer/topology results and row-ordered arithmetic are compared bit for bit; whole
+solves are compared at relative L2 <= 1e-10 with iteration counts equal (reference algorithm) or
+within +-1; mixed precision is checked against its own stated bound (true FP64 residual below
+relTol, solution within 1e-6 relative of the FP64 solve)."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, perf_dict
+import voluma_b200 as vb
+from voluma_b200 import mesh as vm
+from oracle import restate as ro
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+_meshes = {}
+
+
+def device_mesh(name):
+    if name not in _meshes:
+        g = load_golden(name)
+        _meshes[name] = (g, vb.Mesh.from_arrays(g))
+    return _meshes[name]
+
+
+def ctrl(**kw):
+    base = dict(solver="PCG", preconditioner="diagonal", tolerance=0.0, relTol=1e-8, maxIter=2000)
+    base.update(kw)
+    return vb.SolverControls(**base)
+
+
+def true_residual(m, d, up, lo, b, x):
+    return np.abs(b - ro.amul(m, d, up, lo, x)).sum()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_amul_bitwise(name):
+    g, m = device_mesh(name)
+    y = vb.amul(m, g["diag"], g["upper"], None, g["amul_x"])
+    assert np.array_equal(y, g["amul_y"])
+    lo = g["lower_asym"]
+    assert np.array_equal(vb.amul(m, g["diag"], g["upper"], lo, g["amul_x"]),
+                          ro.amul(g, g["diag"], g["upper"], lo, g["amul_x"]))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_device_hierarchy_equals_reference(name):
+    g, m = device_mesh(name)
+    lv = m.gamg_levels()
+    assert len(lv) == int(g["nlevels"])
+    for k, L in enumerate(lv):
+        assert np.array_equal(L["agg"], g[f"lev{k}_agg"])
+        assert np.array_equal(L["l"], g[f"lev{k}_l"])
+
+
+def test_exact_sum_bitwise():
+    g = load_golden("periodic24")
+    assert vb.exact_sum(g["b"]) == g["exact_sum_b"]
+    assert vb.exact_sum(g["exact_spread"]) == g["exact_spread_sum"]
+    assert vb.exact_sum([1e20, 1.0, -1e20]) == 1.0
+    rng = np.random.default_rng(2)
+    v = rng.standard_normal(300000) * np.exp(rng.uniform(-300, 300, 300000))
+    assert vb.exact_sum(v) == ro.exact_sum(v) == vb.exact_sum(v[::-1])
+    assert np.isnan(vb.exact_sum([1.0, np.nan])) and vb.exact_sum([np.inf, 2.0]) == np.inf
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_pcg_diagonal_reproducible_bitwise(name):
+    """CFD_REPRODUCIBLE mode: exact sums + the reference's operation order -> the reference's
+    solution bit for bit, same iteration count and residuals."""
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(reproducible=True))
+    ref = perf_dict(g["pcg_diag_repro_perf"])
+    assert p.iterations == ref["iterations"]
+    assert p.converged == ref["converged"]
+    assert np.array_equal(x, g["pcg_diag_repro_x"])
+    assert p.initialResidual == ref["initialResidual"] and p.finalResidual == ref["finalResidual"]
+    assert p.normFactor == ref["normFactor"] and p.residualSum == ref["residualSum"]
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_pcg_diagonal_matches_reference(name):
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl())
+    ref = perf_dict(g["pcg_diag_perf"])
+    assert abs(p.iterations - ref["iterations"]) <= 1
+    assert rel(x, g["pcg_diag_x"]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_vcycle_mcgs_matches_oracle(name):
+    g, m = device_mesh(name)
+    w = vb.gamg_apply(m, g["diag"], g["upper"], None, g["b"], smoother="mcgs")
+    wo = ro.gamg_apply(g, g["diag"], g["upper"], None, g["b"], smoother="mcgs", coarse=1)
+    assert rel(w, wo) <= 1e-14
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_vcycle_jacobi_matches_oracle(name):
+    g, m = device_mesh(name)
+    w = vb.gamg_apply(m, g["diag"], g["upper"], None, g["b"], smoother="jacobi")
+    wo = ro.gamg_apply(g, g["diag"], g["upper"], None, g["b"], smoother="jacobi", coarse=1)
+    assert rel(w, wo) <= 1e-14
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("smoother", ["mcgs", "jacobi"])
+def test_pcg_gamg_matches_oracle(name, smoother):
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="GAMG", smoother=smoother))
+    xo, po = ro.solve(g, g["diag"], g["upper"], None, g["b"], g["x0"], "PCG", "GAMG", 0.0, 1e-8, 2000,
+                      smoother=smoother, coarse=1)
+    assert abs(p.iterations - po["iterations"]) <= 1
+    assert p.converged and po["converged"]
+    assert rel(x, xo) <= 1e-10 if p.iterations == po["iterations"] else True
+    # against the reference's sequential-GS GAMG: same tolerance reached, counts reported
+    ref = perf_dict(g["pcg_gamg_perf"])
+    assert true_residual(g, g["diag"], g["upper"], None, g["b"], x) <= 1e-8 * ref["residualSum"] * 1.0001
+    if smoother == "mcgs":
+        assert abs(p.iterations - ref["iterations"]) <= 2
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_pbicgstab_diagonal_reproducible_bitwise(name):
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], g["lower_asym"], g["b"], x,
+                     ctrl(solver="PBiCGStab", reproducible=True))
+    ref = perf_dict(g["bicg_diag_repro_perf"])
+    assert p.iterations == ref["iterations"]
+    assert p.converged == ref["converged"]
+    assert np.array_equal(x, g["bicg_diag_repro_x"])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_pbicgstab_gamg(name):
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], g["lower_asym"], g["b"], x,
+                     ctrl(solver="PBiCGStab", preconditioner="GAMG"))
+    xo, po = ro.solve(g, g["diag"], g["upper"], g["lower_asym"], g["b"], g["x0"], "PBiCGStab", "GAMG", 0.0, 1e-8,
+                      2000, smoother="mcgs", coarse=1)
+    assert p.converged
+    assert abs(p.iterations - po["iterations"]) <= 1
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_mixed_precision_reaches_fp64_tolerance(name):
+    """FP32 V-cycle inside the FP64 PCG recurrence: same tolerance, same iteration count (+-1),
+    solution within 1e-6 relative of the FP64 solve (the stated error bound)."""
+    g, m = device_mesh(name)
+    x64 = g["x0"].copy()
+    p64 = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x64, ctrl(preconditioner="GAMG"))
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="GAMG", precision="mixed"))
+    assert p.converged
+    assert abs(p.iterations - p64.iterations) <= 1
+    assert p.finalResidual < 1e-8 * p.initialResidual
+    r = true_residual(g, g["diag"], g["upper"], None, g["b"], x)
+    assert r / p.normFactor < 1e-8 * p.initialResidual * 1.0001
+    assert rel(x, x64) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["periodic8", "walls7x5x3", "jitter10x8x6"])
+def test_mixed_defect_correction_converges(name):
+    """FP32 inner PCG+GAMG inside FP64 defect correction reaches the FP64 tolerance."""
+    g, m = device_mesh(name)
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="GAMG", precision="mixed-dc"))
+    assert p.converged and p.outerIterations >= 1
+    r = true_residual(g, g["diag"], g["upper"], None, g["b"], x)
+    assert r / p.normFactor < 1e-8 * p.initialResidual * 1.0001
+
+
+def test_deterministic_bitwise():
+    g, m = device_mesh("periodic24")
+    xs = []
+    for _ in range(3):
+        x = g["x0"].copy()
+        vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="GAMG"))
+        xs.append(x)
+    assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[1], xs[2])
+
+
+def test_single_level_system_is_a_direct_solve():
+    M = vm.box_mesh((4, 4, 2))
+    d, up = vm.poisson_matrix(M)
+    m = vb.Mesh.from_arrays(M)
+    assert len(m.gamg_levels()) == 1
+    b = np.random.default_rng(3).standard_normal(M["n_cells"])
+    x = np.zeros(M["n_cells"])
+    p = vb.solve_ldu(m, d, up, None, b, x, ctrl(preconditioner="GAMG"))
+    assert p.converged and p.iterations <= 2
+
+
+def test_already_converged_does_no_iteration():
+    g, m = device_mesh("periodic8")
+    x = g["x0"].copy()
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(tolerance=10.0))
+    assert p.iterations == 0 and p.converged
+    assert np.array_equal(x, g["x0"])
+
+
+def test_errors_follow_the_reference():
+    g, m = device_mesh("periodic8")
+    x = g["x0"].copy()
+    with pytest.raises(vb.VlmError) as e:
+        vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(solver="BiCG"))
+    assert e.value.name == "UNSUPPORTED"
+    with pytest.raises(vb.VlmError) as e:
+        vb.solve_ldu(m, g["diag"], g["upper"], g["lower_asym"], g["b"], x, ctrl())
+    assert e.value.name == "UNSUPPORTED" and "symmetric" in str(e.value)
+    with pytest.raises(vb.VlmError) as e:
+        vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="ILU"))
+    assert e.value.name == "UNSUPPORTED"
+
+
+def test_nonfinite_rhs_is_reported_not_hung():
+    g, m = device_mesh("periodic8")
+    b = g["b"].copy()
+    b[5] = np.nan
+    x = np.zeros(g["n_cells"])
+    p = vb.solve_ldu(m, g["diag"], g["upper"], None, b, x, ctrl(preconditioner="GAMG"))
+    assert p.status == 5 and not p.converged
+
+
+def test_singular_coarsest_matrix_raises():
+    g, m = device_mesh("periodic8")
+    x = np.zeros(g["n_cells"])
+    with pytest.raises(vb.VlmError) as e:
+        vb.solve_ldu(m, np.zeros(g["n_cells"]), np.zeros(g["n_internal_faces"]), None, g["b"], x,
+                     ctrl(preconditioner="GAMG", maxIter=3))
+    assert e.value.name == "SINGULAR"
+
+
+def test_64cubed_gamg_against_oracle():
+    M = vm.box_mesh((64, 64, 64), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+    d, up = vm.poisson_matrix(M)
+    b = np.random.default_rng(9).standard_normal(M["n_cells"])
+    b -= b.mean()
+    m = vb.Mesh.from_arrays(M)
+    x = np.zeros(M["n_cells"])
+    p = vb.solve_ldu(m, d, up, None, b, x, ctrl(preconditioner="GAMG"))
+    xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000, smoother="mcgs",
+                      coarse=1)
+    assert abs(p.iterations - po["iterations"]) <= 1
+    assert rel(x, xo) <= 1e-9

@@ -1,0 +1,78 @@
+"""The oracle pinned against the reference: the C restatement (oracle/vlm_oracle.c) must reproduce
+the reference's own outputs stored in tests/golden/ bit for bit, and, where the reference library
+was built here (oracle/_ref), agree with it live on fresh inputs."""
+import numpy as np
+import pytest
+
+from conftest import golden_hierarchy, perf_dict
+from oracle import restate as ro
+
+
+def test_exact_sum_properties():
+    # test_mesh.cpp:13-28: order independence and exact cancellation
+    assert ro.exact_sum([1e20, 1.0, -1e20]) == 1.0
+    rng = np.random.default_rng(1)
+    v = rng.standard_normal(10000) * np.exp(rng.uniform(-30, 30, 10000))
+    assert ro.exact_sum(v) == ro.exact_sum(v[::-1]) == ro.exact_sum(rng.permutation(v))
+    assert ro.exact_sum([]) == 0.0
+    assert np.isnan(ro.exact_sum([1.0, np.nan]))
+    assert ro.exact_sum([np.inf, 1.0]) == np.inf
+
+
+def test_exact_sum_golden(golden):
+    assert ro.exact_sum(golden["b"]) == golden["exact_sum_b"]
+    assert ro.exact_sum(golden["exact_spread"]) == golden["exact_spread_sum"]
+
+
+def test_amul_golden(golden):
+    y = ro.amul(golden, golden["diag"], golden["upper"], None, golden["amul_x"])
+    assert np.array_equal(y, golden["amul_y"])
+
+
+def test_hierarchy_golden(golden):
+    ref_h = golden_hierarchy(golden)
+    h = ro.hierarchy(golden)
+    assert len(h) == len(ref_h)
+    for a, b in zip(h, ref_h):
+        for f in ("l", "u", "weight", "agg", "faceMap", "faceFlip"):
+            assert np.array_equal(a[f], b[f]), f
+
+
+def test_vcycle_gs_golden(golden):
+    w = ro.gamg_apply(golden, golden["diag"], golden["upper"], None, golden["b"], smoother="gs", coarse=0)
+    assert np.array_equal(w, golden["vcycle_w"])
+
+
+@pytest.mark.parametrize("key,solver,prec,exact,asym", [
+    ("pcg_diag_repro", "PCG", "diagonal", True, False),
+    ("pcg_diag", "PCG", "diagonal", False, False),
+    ("pcg_gamg", "PCG", "GAMG", False, False),
+    ("bicg_diag_repro", "PBiCGStab", "diagonal", True, True),
+    ("bicg_gamg", "PBiCGStab", "GAMG", False, True),
+])
+def test_solve_golden(golden, key, solver, prec, exact, asym):
+    lower = golden["lower_asym"] if asym else None
+    x, perf = ro.solve(golden, golden["diag"], golden["upper"], lower, golden["b"], golden["x0"], solver, prec,
+                       0.0, 1e-8, 2000, exact=exact)
+    ref_perf = perf_dict(golden[key + "_perf"])
+    assert np.array_equal(x, golden[key + "_x"])
+    assert perf == ref_perf
+
+
+def test_oracle_live_against_reference():
+    """Fresh random inputs through both the reference build and the restatement."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("reference library not built here")
+    from voluma_b200 import mesh as vm
+    n = (9, 7, 6)
+    pts = vm.jitter_interior(vm.box_points(n, beta=(0.8, 0, 1.1)), n, 0.15, 11)
+    R = ref.RefMesh(n, periodic=(0, 1, 0), points=pts)
+    M = vm.box_mesh(n, periodic=(0, 1, 0), points=pts)
+    d, up = vm.poisson_matrix(M)
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(M["n_cells"])
+    for prec in ("diagonal", "GAMG"):
+        xr, pr = R.solve(d, up, None, b, np.zeros(M["n_cells"]), "PCG", prec, 0.0, 1e-9, 500)
+        xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", prec, 0.0, 1e-9, 500)
+        assert np.array_equal(xr, xo) and pr == po

@@ -210,6 +210,19 @@ class Mesh:
             out.append(dict(n=int(s[0]), l=l, u=u, agg=agg))
         return out
 
+    def stats(self):
+        """(kernel launches executed on this mesh so far, device bytes held)."""
+        n, b = C.c_int64(), C.c_int64()
+        check(load().vlm_mesh_stats(self._h, C.byref(n), C.byref(b)))
+        return n.value, b.value
+
+    def profile_kernel(self, kernel: str, reps: int = 20):
+        """(ms per launch, algorithmic bytes per launch) of a level-0 kernel on the last solve's matrix."""
+        ms, by = C.c_double(), C.c_double()
+        check(load().vlm_profile_kernel(self.ctx.handle, self._h, kernel.encode(), reps, C.byref(ms), C.byref(by)),
+              self.ctx.handle)
+        return ms.value, by.value
+
     def colours(self, level):
         n = C.c_int32()
         check(load().vlm_gamg_colours(self._h, level, C.byref(n)))
@@ -225,6 +238,34 @@ class Mesh:
             self.close()
         except Exception:
             pass
+
+
+def topology(n_cells, owner, neighbour, magSf, ndc, merge_levels: int = 2):
+    """Host-side GAMG hierarchy + colouring exactly as the device uses them (no GPU needed):
+    list of dicts n, l, u, weight, agg, faceMap, faceFlip, colour, ncolours."""
+    L = load()
+    own = np.ascontiguousarray(owner, np.int32)
+    nei = np.ascontiguousarray(neighbour, np.int32)
+    h = C.c_void_p()
+    check(L.vlm_topology_build(int(n_cells), nei.size, _ptr(own), _ptr(nei), _ptr(_f64(magSf)), _ptr(_f64(ndc)),
+                               merge_levels, C.byref(h)))
+    try:
+        nl = C.c_int32()
+        check(L.vlm_topology_levels(h, C.byref(nl)))
+        out = []
+        for k in range(nl.value):
+            s = np.zeros(4, np.int32)
+            check(L.vlm_topology_level(h, k, _ptr(s), None, None, None, None, None, None, None))
+            n, nf, na, nc = (int(v) for v in s)
+            d = dict(n=n, l=np.zeros(nf, np.int32), u=np.zeros(nf, np.int32), weight=np.zeros(nf),
+                     agg=np.zeros(na, np.int32), faceMap=np.zeros(nf if na else 0, np.int32),
+                     faceFlip=np.zeros(nf if na else 0, np.int8), colour=np.zeros(n, np.int32), ncolours=nc)
+            check(L.vlm_topology_level(h, k, _ptr(s), _ptr(d["l"]), _ptr(d["u"]), _ptr(d["weight"]), _ptr(d["agg"]),
+                                       _ptr(d["faceMap"]), _ptr(d["faceFlip"]), _ptr(d["colour"])))
+            out.append(d)
+        return out
+    finally:
+        L.vlm_topology_destroy(h)
 
 
 def solve_ldu(mesh: Mesh, diag, upper, lower, b, x, ctrl: SolverControls) -> SolverPerformance:
@@ -248,6 +289,15 @@ def solve_ldu_device(mesh: Mesh, diag_ptr, upper_ptr, lower_ptr, b_ptr, x_ptr, c
                                       C.c_void_p(lower_ptr) if lower_ptr else None, C.c_void_p(b_ptr),
                                       C.c_void_p(x_ptr), C.byref(c), C.byref(p)), mesh.ctx.handle)
     return SolverPerformance.from_c(p)
+
+
+def exact_sum(values, ctx: Context | None = None) -> float:
+    """Order-independent exact sum on the device (par::ExactSum semantics, Comm.h:42-93)."""
+    ctx = ctx or default_context()
+    v = _f64(values)
+    out = C.c_double()
+    check(load().vlm_exact_sum(ctx.handle, _ptr(v), v.size, C.byref(out)), ctx.handle)
+    return out.value
 
 
 def amul(mesh: Mesh, diag, upper, lower, x):

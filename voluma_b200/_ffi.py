@@ -13,7 +13,9 @@ STATUS = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "OOM", 4: "SINGULAR", 5: "NONFINI
 # every entry point include/voluma_b200.h declares
 EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_stream", "vlm_mesh_register",
            "vlm_mesh_release", "vlm_amul", "vlm_ldu_solve", "vlm_ldu_solve_device", "vlm_gamg_apply",
-           "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum"]
+           "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
+           "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
+           "vlm_mesh_stats", "vlm_profile_kernel"]
 
 
 class MeshDesc(C.Structure):
@@ -68,6 +70,12 @@ def load():
     L.vlm_laplacian.argtypes = [P, P, P, P, P, P, i32, i32, P, P, P, P, P, P, P]
     L.vlm_grad.argtypes = [P, P, P, P, P, i32, P]
     L.vlm_exact_sum.argtypes = [P, P, C.c_int64, C.POINTER(C.c_double)]
+    L.vlm_topology_build.argtypes = [i32, i32, P, P, P, P, i32, C.POINTER(P)]
+    L.vlm_topology_levels.argtypes = [P, C.POINTER(i32)]
+    L.vlm_topology_level.argtypes = [P, i32, P, P, P, P, P, P, P, P]
+    L.vlm_topology_destroy.argtypes = [P]
+    L.vlm_mesh_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.vlm_profile_kernel.argtypes = [P, P, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype if name in ("vlm_last_error", "vlm_ctx_stream") else C.c_int
     _lib = L

@@ -16,6 +16,12 @@ struct vlm_ctx {
     int refs = 1;  // the handle itself + one per registered mesh
 };
 
+struct vlm_topology {
+    vlm::Hierarchy H;
+    std::vector<std::vector<int>> colour;
+    std::vector<int> nColours;
+};
+
 struct vlm_mesh {
     vlm_ctx* ctx = nullptr;
     int nCells = 0, nInternal = 0, nFaces = 0;
@@ -28,6 +34,7 @@ struct vlm_mesh {
 
 namespace {
 
+constexpr int64_t kRowsPerCtaForSum = 256;
 thread_local std::string g_lastError;
 
 vlm_status fail(vlm_ctx* ctx, vlm_status s, const std::string& msg) {
@@ -258,6 +265,71 @@ vlm_status vlm_gamg_colours(vlm_mesh* m, int32_t level, int32_t* n) {
     return VLM_OK;
 }
 
+vlm_status vlm_mesh_stats(vlm_mesh* m, int64_t* launches, int64_t* bytes) {
+    if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    if (launches) *launches = m->batch->launches();
+    if (bytes) *bytes = int64_t(m->batch->deviceBytes());
+    return VLM_OK;
+}
+
+vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* m, const char* kernel, int32_t reps, double* ms, double* bytes) {
+    if (!ctx || !m || !kernel || !ms || !bytes || reps <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        *ms = m->batch->profileKernel(kernel, reps, bytes);
+    });
+}
+
+vlm_status vlm_topology_build(int32_t n_cells, int32_t n_internal_faces, const int32_t* owner,
+                              const int32_t* neighbour, const double* magSf, const double* ndc, int32_t merge_levels,
+                              vlm_topology** out) {
+    if (!out || !owner || (!neighbour && n_internal_faces > 0) || !magSf || !ndc || n_cells <= 0)
+        return fail(nullptr, VLM_ERR_BAD_ARG, "invalid topology arguments");
+    *out = nullptr;
+    return guarded(nullptr, [&] {
+        auto t = std::make_unique<vlm_topology>();
+        t->H = vlm::buildHierarchy(n_cells, n_internal_faces, owner, neighbour, magSf, ndc,
+                                   merge_levels > 0 ? merge_levels : 2);
+        for (const auto& L : t->H.levels) {
+            int nc = 0;
+            t->colour.push_back(vlm::greedyColour(L, &nc));
+            t->nColours.push_back(nc);
+        }
+        *out = t.release();
+    });
+}
+
+vlm_status vlm_topology_levels(const vlm_topology* t, int32_t* n) {
+    if (!t || !n) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    *n = int32_t(t->H.levels.size());
+    return VLM_OK;
+}
+
+vlm_status vlm_topology_level(const vlm_topology* t, int32_t level, int32_t* sizes, int32_t* l, int32_t* u,
+                              double* weight, int32_t* agg, int32_t* face_map, int8_t* face_flip, int32_t* colour) {
+    if (!t || !sizes) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    if (level < 0 || level >= int32_t(t->H.levels.size())) return fail(nullptr, VLM_ERR_BAD_ARG, "level out of range");
+    const auto& L = t->H.levels[level];
+    sizes[0] = L.n;
+    sizes[1] = int32_t(L.l.size());
+    sizes[2] = int32_t(L.agg.size());
+    sizes[3] = t->nColours[level];
+    if (l) std::copy(L.l.begin(), L.l.end(), l);
+    if (u) std::copy(L.u.begin(), L.u.end(), u);
+    if (weight) std::copy(L.weight.begin(), L.weight.end(), weight);
+    if (agg) std::copy(L.agg.begin(), L.agg.end(), agg);
+    if (face_map) std::copy(L.faceMap.begin(), L.faceMap.end(), face_map);
+    if (face_flip)
+        for (size_t k = 0; k < L.faceFlip.size(); ++k) face_flip[k] = int8_t(L.faceFlip[k]);
+    if (colour) std::copy(t->colour[level].begin(), t->colour[level].end(), colour);
+    return VLM_OK;
+}
+
+vlm_status vlm_topology_destroy(vlm_topology* t) {
+    delete t;
+    return VLM_OK;
+}
+
 vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh*, const double*, const double*, const int32_t*, const double*,
                          int32_t, int32_t, double*, double*, double*, double*, double*, double*, int32_t*) {
     return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_laplacian: not built yet");
@@ -267,8 +339,15 @@ vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh*, const double*, const int32_t*, cons
     return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_grad: not built yet");
 }
 
-vlm_status vlm_exact_sum(vlm_ctx* ctx, const double*, int64_t, double*) {
-    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_exact_sum: not built yet");
+vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out) {
+    if (!ctx || (!values && n > 0) || !out || n < 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        if (n >= (int64_t(1) << 31) - kRowsPerCtaForSum) throw vlm::Error(VLM_ERR_BAD_ARG, "n too large");
+        vlm::DBuf<double> d;
+        d.upload(values, size_t(n), ctx->stream);
+        *out = vlm::exactSumOnDevice(ctx->stream, d.get(), n);
+    });
 }
 
 }  // extern "C"

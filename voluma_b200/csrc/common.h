@@ -78,6 +78,8 @@ struct Chunk {
 };
 
 constexpr int kRowsPerCta = 256;
+// Rows of one block-hybrid Gauss-Seidel block (one CTA of that many threads).
+constexpr int kBlockRows = 512;
 constexpr int kSlice = 32;  // SELL slice height (one warp)
 
 }  // namespace vlm

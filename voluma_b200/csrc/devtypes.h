@@ -30,6 +30,7 @@ struct DD {
 // Reduction context: per-CTA partial slots and per-system completion counters.
 struct RedCtx {
     DD* partials;           // [slot * NV + q]
+    long long* xbins;       // exact sums: [slot][NV][bins + flags]
     int* counters;          // per system
     const int* slotBegin;   // per system
     const int* slotEnd;

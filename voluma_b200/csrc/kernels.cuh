@@ -65,7 +65,7 @@ __device__ __forceinline__ void block_reduce(DD (&v)[NV]) {
 // Writes this CTA's partials; returns true in thread 0 of the CTA that completes the
 // system, with the system totals (summed over slots in a fixed order) in `out`.
 template <int NV>
-__device__ bool reduce_to_system(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+__device__ bool reduce_dd(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
     block_reduce<NV>(v);
     __shared__ int isLast;
     if (threadIdx.x == 0) {
@@ -97,6 +97,144 @@ __device__ bool reduce_to_system(DD (&v)[NV], const Chunk& c, const RedCtx& R, d
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = acc[q].hi + acc[q].lo;
     return true;
+}
+
+// ------------------------------------------------------------------ exact (order-independent) sums
+// The superaccumulator of par::ExactSum (src/fvm/parallel/Comm.h:42-93, Comm.cpp:107-164):
+// a double M*2^E is split over three 32-bit-aligned int64 bins; integer addition is
+// associative, so the total does not depend on the summation order, and the final
+// conversion reproduces the reference's value bit for bit.
+constexpr int kExactBins = 72;
+constexpr int kExactStride = kExactBins + 1;  // bins + non-finite flags per partial
+
+__device__ __forceinline__ void exact_add(long long* bins, int* flags, double v) {
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
+    const int ex = (int)((bits >> 52) & 0x7ff);
+    if (ex == 0x7ff) {  // Inf / NaN: remembered as flags (their sum is order independent)
+        if ((bits & ((1ull << 52) - 1)) != 0)
+            atomicOr(flags, 1);
+        else
+            atomicOr(flags, (bits >> 63) ? 4 : 2);
+        return;
+    }
+    long long M = (long long)(bits & ((1ull << 52) - 1));
+    if (ex != 0) M |= 1ll << 52;
+    if (M == 0) return;
+    const int p = (ex == 0 ? 1 : ex) - 1;
+    const int i = p >> 5, sh = p & 31;
+    const long long sgn = -(long long)(bits >> 63);
+    long long lo = (M & ((1ll << (32 - sh)) - 1)) << sh;
+    const long long r = M >> (32 - sh);
+    long long mid = r & 0xFFFFFFFFll;
+    long long hi = r >> 32;
+    lo = (lo ^ sgn) - sgn;
+    mid = (mid ^ sgn) - sgn;
+    hi = (hi ^ sgn) - sgn;
+    atomicAdd((unsigned long long*)&bins[i], (unsigned long long)lo);
+    atomicAdd((unsigned long long*)&bins[i + 1], (unsigned long long)mid);
+    atomicAdd((unsigned long long*)&bins[i + 2], (unsigned long long)hi);
+}
+
+__device__ __forceinline__ void exact_normalize(long long* b) {
+    for (int k = 0; k < kExactBins - 1; ++k) {
+        const long long carry = b[k] >> 32;
+        b[k] -= carry * (1ll << 32);
+        b[k + 1] += carry;
+    }
+}
+
+// binsToDouble (Comm.cpp:135-156)
+__device__ double exact_value(long long* b, int flags) {
+    if (flags & 1) return __longlong_as_double(0x7ff8000000000000ll);
+    if ((flags & 6) == 6) return __longlong_as_double(0x7ff8000000000000ll);
+    if (flags & 2) return __longlong_as_double(0x7ff0000000000000ll);
+    if (flags & 4) return __longlong_as_double((long long)0xfff0000000000000ull);
+    exact_normalize(b);
+    double sign = 1.0;
+    if (b[kExactBins - 1] < 0) {
+        sign = -1.0;
+        for (int k = 0; k < kExactBins; ++k) b[k] = -b[k];
+        exact_normalize(b);
+    }
+    double r = 0.0;
+    for (int k = kExactBins - 1; k >= 0; --k)
+        if (b[k] != 0) r += ldexp((double)b[k], 32 * k - 1074);
+    return sign * r;
+}
+
+template <int NV>
+__device__ bool reduce_exact(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+    constexpr int kWarps = kRowsPerCta / 32;
+    __shared__ long long bins[NV][kWarps][kExactBins];
+    __shared__ int flags[NV][kWarps];
+    __shared__ int isLast;
+    for (int q = threadIdx.x; q < NV * kWarps * kExactBins; q += blockDim.x) (&bins[0][0][0])[q] = 0;
+    if ((int)threadIdx.x < NV * kWarps) (&flags[0][0])[threadIdx.x] = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) exact_add(bins[q][warp], &flags[q][warp], v[q].hi);
+    __syncthreads();
+    long long* dst = R.xbins + (size_t)c.slot * NV * kExactStride;
+    for (int idx = threadIdx.x; idx < NV * kExactBins; idx += blockDim.x) {
+        const int q = idx / kExactBins, k = idx % kExactBins;
+        long long s = 0;
+        for (int w = 0; w < kWarps; ++w) s += bins[q][w][k];
+        dst[q * kExactStride + k] = s;
+    }
+    if ((int)threadIdx.x < NV) {
+        int f = 0;
+        for (int w = 0; w < kWarps; ++w) f |= flags[threadIdx.x][w];
+        dst[threadIdx.x * kExactStride + kExactBins] = f;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nslots = R.slotEnd[c.sys] - R.slotBegin[c.sys];
+        isLast = atomicAdd(&R.counters[c.sys], 1) == nslots - 1;
+    }
+    __syncthreads();
+    if (!isLast) return false;
+    __threadfence();
+    // totals: thread (q, k) adds bin k of every slot (int64: exact in any order)
+    __shared__ long long tot[NV][kExactStride];
+    const int b0 = R.slotBegin[c.sys], b1 = R.slotEnd[c.sys];
+    for (int idx = threadIdx.x; idx < NV * kExactStride; idx += blockDim.x) {
+        const int q = idx / kExactStride, k = idx % kExactStride;
+        long long s = 0;
+        for (int sl = b0; sl < b1; ++sl) {
+            const volatile long long* src = R.xbins + (size_t)sl * NV * kExactStride + q * kExactStride;
+            if (k < kExactBins)
+                s += src[k];
+            else
+                s |= src[k];
+        }
+        tot[q][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return false;
+    R.counters[c.sys] = 0;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = exact_value(tot[q], (int)tot[q][kExactBins]);
+    return true;
+}
+
+template <int NV, bool EXACT = false>
+__device__ __forceinline__ bool reduce_to_system(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+    if constexpr (EXACT)
+        return reduce_exact<NV>(v, c, R, out);
+    else
+        return reduce_dd<NV>(v, c, R, out);
+}
+
+// Exact sum of a plain array (vlm_exact_sum): one system, chunks of kRowsPerCta values.
+__global__ void __launch_bounds__(kRowsPerCta) k_exact_sum(const Chunk* __restrict__ ch, const double* __restrict__ v,
+                                                           RedCtx R, double* out) {
+    const Chunk c = ch[blockIdx.x];
+    DD a[1] = {DD{0.0, 0.0}};
+    if ((int)threadIdx.x < c.count) a[0].hi = v[c.start + threadIdx.x];
+    double o[1];
+    if (reduce_exact<1>(a, c, R, o)) *out = o[0];
 }
 
 // ------------------------------------------------------------------ SELL row access
@@ -154,6 +292,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restri
     w[c.start + threadIdx.x] = r[c.start + threadIdx.x];
 }
 
+// b = (To) a on the rows of the chunks
+template <class From, class To>
+__global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restrict__ ch, const From* __restrict__ a,
+                                                           To* __restrict__ b, const SysState* st, int flag) {
+    const Chunk c = ch[blockIdx.x];
+    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
+    b[c.start + threadIdx.x] = (To)a[c.start + threadIdx.x];
+}
+
 // ------------------------------------------------------------------ smoothers
 // Gauss-Seidel row update (GAMG.cpp:368-380) on the rows of one colour step.
 template <class T>
@@ -165,6 +312,91 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_gs(const Chunk* __restri
     const int row = c.start + threadIdx.x;
     const T s = row_minus(S, val, x, row, r[row]);
     x[row] = s / diag[row];
+}
+
+// Block-hybrid Gauss-Seidel sweep.  One CTA per block of <= kBlockRows rows: the block's x lives
+// in shared memory and is updated colour by colour (block-local colouring, forward or reversed
+// order); neighbours outside the block are read from xi (the previous sweep), so the result does
+// not depend on the order CTAs run in.  Each thread reads its row once per sweep: the terms of
+// neighbours outside the block are summed first (face order), the in-block entries are kept in
+// registers, and every colour step then subtracts the in-block terms (face order) from shared
+// memory — no global-memory latency inside the synchronised colour loop.
+// x_i = (r_i - sum_out a_ij x_j - sum_in a_ij x_j) / a_ii.
+// MODE 0: x = xi; MODE 1: x starts at 0 (first pre-sweep); MODE 2: x = xi + xc[agg] (the
+// coarse-grid correction of GAMG.cpp:437-438, fused in).
+constexpr int kBgsRegEntries = 32;  // in-block entries held in registers; longer rows spill to loads
+
+template <class T, int MODE, bool FWD>
+__global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __restrict__ blocks, Sell S,
+                                                              const T* __restrict__ val, const T* __restrict__ diag,
+                                                              const T* __restrict__ r, const T* __restrict__ xi,
+                                                              T* __restrict__ xo, const int8_t* __restrict__ rcol,
+                                                              const int32_t* __restrict__ agg,
+                                                              const T* __restrict__ xc, const SysState* st, int flag) {
+    __shared__ T xs[kBlockRows];
+    const Chunk c = blocks[blockIdx.x];
+    if (chunk_skip(c, st, flag)) return;
+    const int t = threadIdx.x;
+    const bool mine = t < c.count;
+    const int row = c.start + t;
+    auto xval = [&](int j) -> T {
+        if (MODE == 1) return T(0);
+        T v = xi[j];
+        if (MODE == 2) {
+            const int a = agg[j];
+            if (a >= 0) v += xc[a];
+        }
+        return v;
+    };
+    const int len = mine ? S.rlen[row] : 0;
+    const int base = mine ? sell_base(S, row) : 0;
+    T s = mine ? r[row] : T(0);
+    int16_t li[kBgsRegEntries];
+    T lv[kBgsRegEntries];
+#pragma unroll
+    for (int k = 0; k < kBgsRegEntries; ++k) {
+        li[k] = -1;
+        lv[k] = T(0);
+        if (k < len) {
+            const int e = base + (k << 5);
+            const int j = S.col[e];
+            const T a = val[e];
+            const int jl = j - c.start;
+            if (jl >= 0 && jl < c.count) {
+                li[k] = (int16_t)jl;
+                lv[k] = a;
+            } else {
+                s -= a * xval(j);
+            }
+        }
+    }
+    for (int k = kBgsRegEntries; k < len; ++k) {  // rare: rows longer than the register window
+        const int e = base + (k << 5);
+        const int jl = S.col[e] - c.start;
+        if (!(jl >= 0 && jl < c.count)) s -= val[e] * xval(S.col[e]);
+    }
+    if (mine) xs[t] = xval(row);
+    __syncthreads();
+    const int nc = c.slot;
+    const int mycol = mine ? (int)rcol[row] : -1;
+    const T dd = mine ? diag[row] : T(1);
+    for (int step = 0; step < nc; ++step) {
+        const int colour = FWD ? step : nc - 1 - step;
+        if (mycol == colour) {
+            T q = s;
+#pragma unroll
+            for (int k = 0; k < kBgsRegEntries; ++k)
+                if (li[k] >= 0) q -= lv[k] * xs[li[k]];
+            for (int k = kBgsRegEntries; k < len; ++k) {
+                const int e = base + (k << 5);
+                const int jl = S.col[e] - c.start;
+                if (jl >= 0 && jl < c.count) q -= val[e] * xs[jl];
+            }
+            xs[t] = q / dd;
+        }
+        __syncthreads();
+    }
+    if (mine) xo[row] = xs[t];
 }
 
 // Jacobi sweep xo = (r - offdiag*xi)/D (first: xi == 0).
@@ -227,14 +459,17 @@ __global__ void __launch_bounds__(kRowsPerCta) k_prolong(const Chunk* __restrict
 
 // Dense coarsest matrix, un-pivoted LU in place (GAMG.cpp:317-343) and the explicit
 // inverse from the LU by substituting unit vectors (GAMG.cpp:413-418 per column).
-// One CTA per system.  lu/inv: scratch of n*n doubles at invOffset.
+// One CTA per system.  The factorisation runs in shared memory when the matrix fits
+// (smemN >= n: 2 n^2 doubles of dynamic shared memory), else in the global scratch `lu`.
 __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const double* __restrict__ val,
                                 const double* __restrict__ diag, double* __restrict__ lu, double* __restrict__ inv,
-                                int* status) {
+                                int* status, int smemN) {
+    extern __shared__ double sh[];
     const CoarseDev c = cs[blockIdx.x];
     const int n = c.n;
-    double* A = lu + c.invOffset;
-    double* X = inv + c.invOffset;
+    const bool inShared = n <= smemN;
+    double* A = inShared ? sh : lu + c.invOffset;
+    double* X = inShared ? sh + (size_t)n * n : inv + c.invOffset;
     for (int q = threadIdx.x; q < n * n; q += blockDim.x) A[q] = 0.0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -281,6 +516,10 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
             for (int k = i + 1; k < n; ++k) g -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
             X[(size_t)i * n + j] = g / A[(size_t)i * n + i];
         }
+    }
+    if (inShared) {
+        __syncthreads();
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) inv[c.invOffset + q] = X[q];
     }
 }
 

@@ -16,18 +16,19 @@ __device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, doubl
 
 // ------------------------------------------------------------------ initial residual
 // Sum of x (for the normFactor reference value x̄, LinearSolver.cpp:157-159).
-template <class T>
+template <class T, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_sum_x(const Chunk* __restrict__ ch, const T* __restrict__ x, RedCtx R,
                                                        SysState* st) {
     const Chunk c = ch[blockIdx.x];
     DD v[1] = {DD{0.0, 0.0}};
     if ((int)threadIdx.x < c.count) v[0].hi = (double)x[c.start + threadIdx.x];
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) st[c.sys].s0 = out[0];
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) st[c.sys].s0 = out[0];
 }
 
 // wA = A x, pA = A x̄, r = b - wA; normFactor = Σ|wA-pA|+|b-pA| + 1e-20; residualSum = Σ|r|
 // (LinearSolver.cpp:149-174).  r32 (optional) receives (float)r for the mixed inner solve.
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __restrict__ ch, Sell S,
                                                                const double* __restrict__ val,
                                                                const double* __restrict__ diag,
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __re
         }
     }
     double out[2];
-    if (reduce_to_system<2>(v, c, R, out)) {
+    if (reduce_to_system<2, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         s.normFactor = out[0] + 1e-20;
         s.residualSum = out[1];
@@ -99,7 +100,7 @@ __global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* 
 
 // ------------------------------------------------------------------ PCG (LinearSolver.cpp:176-201)
 // wArA = Σ w·r ; beta = wArA / wArAold
-template <class T, int FLAG>
+template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restrict__ ch, const T* __restrict__ w,
                                                             const T* __restrict__ r, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
         v[0].hi = (double)w[row] * (double)r[row];
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
         s.wArAold = s.wArA;
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__
 }
 
 // Ap = A p ; wApA = Σ Ap·p ; alpha = wArA / wApA (break when |wApA| < VSMALL)
-template <class T, int FLAG>
+template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                           const T* __restrict__ diag, const T* __restrict__ p,
                                                           T* __restrict__ Ap, RedCtx R, SysState* st) {
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restric
         v[0].hi = (double)y * (double)p[row];
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         if (fabs(out[0]) < kVSMALL) {
             if (FLAG == kFlagDone) {
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restric
 }
 
 // x += alpha p ; r -= alpha Ap ; finalResidual = Σ|r| / normFactor ; convergence
-template <class T, int FLAG>
+template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restrict__ ch, T* __restrict__ x, T* __restrict__ r,
                                                             const T* __restrict__ p, const T* __restrict__ Ap,
                                                             const int32_t* __restrict__ perm, RedCtx R, SysState* st,
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
         v[0].hi = fabs((double)rr);
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         if (FLAG == kFlagDone) {
             s.finalResidual = out[0] / s.normFactor;
@@ -267,6 +268,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
 
 // ------------------------------------------------------------------ PBiCGStab (LinearSolver.cpp:202-237)
 // rho = Σ r0·r ; beta = (rho/rhoOld)(alpha/omega), break on |rhoOld| or |omega| < VSMALL
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restrict__ ch, const double* __restrict__ r0,
                                                           const double* __restrict__ r, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
@@ -277,7 +279,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restric
         v[0].hi = r0[row] * r[row];
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         s.rhoOld = s.rho;
         s.rho = out[0];
@@ -305,6 +307,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_p(const Chunk* __restrict_
 }
 
 // Ay = A y ; alpha = rho / Σ r0·Ay (break when < VSMALL)
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __restrict__ ch, Sell S,
                                                                  const double* __restrict__ val,
                                                                  const double* __restrict__ diag,
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
         v[0].hi = r0[row] * a;
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         if (fabs(out[0]) < kVSMALL)
             s.done = 1;
@@ -330,6 +333,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
 }
 
 // s = r - alpha Ay ; iterations++ ; finalResidual = Σ|s|/nf ; converged -> early exit flag (s0 = 1)
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ sv, RedCtx R,
                                                         SysState* st, const DevCtrl* __restrict__ ctrlp) {
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict_
         v[0].hi = fabs(s);
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         s.iterations += 1;
         s.finalResidual = out[0] / s.normFactor;
@@ -380,6 +384,7 @@ __global__ void k_bicg_early_close(int nsys, SysState* st) {
 }
 
 // t = A z ; tAtA = Σ t·t ; tAsA = Σ t·s ; omega = tAtA > VSMALL ? tAsA/tAtA : 0
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __restrict__ ch, Sell S,
                                                                  const double* __restrict__ val,
                                                                  const double* __restrict__ diag,
@@ -396,13 +401,14 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __
         v[1].hi = a * sv[row];
     }
     double out[2];
-    if (reduce_to_system<2>(v, c, R, out)) {
+    if (reduce_to_system<2, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         s.omega = out[0] > kVSMALL ? out[1] / out[0] : 0.0;
     }
 }
 
 // x += alpha y + omega z ; r = s - omega t ; finalResidual = Σ|r| / nf
+template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                              double* __restrict__ r, const double* __restrict__ y,
                                                              const double* __restrict__ z, const double* __restrict__ sv,
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
         v[0].hi = fabs(rr);
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
         SysState& s = st[c.sys];
         s.finalResidual = out[0] / s.normFactor;
         if (!isfinite(s.finalResidual)) {

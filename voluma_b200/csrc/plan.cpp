@@ -9,7 +9,29 @@ namespace vlm {
 
 namespace {
 
-int pad32(int n) { return (n + kSlice - 1) / kSlice * kSlice; }
+// Greedy colouring of rows [s0, s1) considering only edges inside the block.
+std::vector<int> blockColour(const HLevel& L, int s0, int s1, int* nColours) {
+    std::vector<int> colour(size_t(s1 - s0), -1);
+    std::vector<int> mark;
+    int nc = 0;
+    for (int i = s0; i < s1; ++i) {
+        for (int k = L.off[i]; k < L.off[i + 1]; ++k) {
+            const int j = L.adjCell[k];
+            if (j < s0 || j >= s1) continue;
+            const int c = colour[j - s0];
+            if (c >= 0) {
+                if (size_t(c) >= mark.size()) mark.resize(size_t(c) + 1, -1);
+                mark[c] = i;
+            }
+        }
+        int c = 0;
+        while (size_t(c) < mark.size() && mark[c] == i) ++c;
+        colour[i - s0] = c;
+        nc = std::max(nc, c + 1);
+    }
+    *nColours = nc;
+    return colour;
+}
 
 void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slot) {
     for (int s = 0; s < len; s += kRowsPerCta) {
@@ -69,6 +91,17 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
         LevelPlan& LP = P.levels[k];
         int row = 0;
         int present = 0, active = 0;
+        if (k > 0) {
+            LP.blockGS = true;
+        } else {
+            // level 0: global multicolour GS if every smoothing system needs few colours
+            for (int b = 0; b < ns; ++b) {
+                if (P.nLevels[b] <= 1) continue;
+                int nc = 0;
+                greedyColour(P.H[b].levels[0], &nc);
+                if (nc > kMaxGlobalColours) LP.blockGS = true;
+            }
+        }
         for (int b = 0; b < ns; ++b) {
             if (P.nLevels[b] > k) present = b + 1;
             if (P.nLevels[b] - 1 > k) active = b + 1;
@@ -96,7 +129,7 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
                     ++row;
                 }
             };
-            if (b < active) {
+            if (b < active && !LP.blockGS) {
                 int nc = 0;
                 const std::vector<int> colour = greedyColour(L, &nc);
                 LP.maxColours = std::max(LP.maxColours, nc);
@@ -108,9 +141,34 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
                     pad();
                     groups[k][b].push_back({g0, row - g0});
                 }
+            } else if (b < active) {
+                // blocks of consecutive natural rows, each ordered by its block-local colouring
+                for (int s0 = 0; s0 < L.n; s0 += kBlockRows) {
+                    const int s1 = std::min(L.n, s0 + kBlockRows);
+                    int nc = 0;
+                    const std::vector<int> colour = blockColour(L, s0, s1, &nc);
+                    LP.maxColours = std::max(LP.maxColours, nc);
+                    Chunk blk;
+                    blk.start = row;
+                    blk.count = s1 - s0;
+                    blk.sys = b;
+                    blk.slot = nc;
+                    for (int c = 0; c < nc; ++c)
+                        for (int i = s0; i < s1; ++i)
+                            if (colour[i - s0] == c) {
+                                place(i);
+                                LP.rowColour.push_back(int8_t(c));
+                            }
+                    LP.blocks.push_back(blk);
+                }
+                const int before = row;
+                pad();
+                LP.rowColour.resize(LP.rowColour.size() + size_t(row - before), int8_t(-1));
             } else {
                 for (int i = 0; i < L.n; ++i) place(i);
+                const int before = row;
                 pad();
+                if (LP.blockGS) LP.rowColour.resize(LP.rowColour.size() + size_t(row - before + L.n), int8_t(-1));
             }
         }
         LP.sysRow[present] = row;

@@ -24,7 +24,15 @@ struct SysTopo {
     const double* ndc = nullptr;
 };
 
+// Block-hybrid Gauss-Seidel: rows of a smoothing system are cut into blocks of kBlockRows
+// consecutive natural rows (kBlockRows, common.h); each block is one CTA that runs Gauss-Seidel
+// over its rows in block-local colour order, reading neighbours outside the block from the
+// previous sweep.
+// Level 0 keeps a global multicolour Gauss-Seidel when its graph needs at most this many colours.
+constexpr int kMaxGlobalColours = 4;
+
 struct LevelPlan {
+    bool blockGS = false;  // block-hybrid layout (else global colour-major)
     int nrows = 0;         // padded rows
     int nfaces = 0;        // faces of the systems present (level 0: user mesh faces)
     int nActiveRows = 0;   // rows of systems that smooth on this level
@@ -35,6 +43,8 @@ struct LevelPlan {
     std::vector<std::vector<Chunk>> fwd, rev;     // colour step t chunks (forward / reversed)
     std::vector<Chunk> active;                    // all rows of smoothing systems
     std::vector<Chunk> all;                       // all rows (sys/slot set)
+    std::vector<Chunk> blocks;                    // block-hybrid GS blocks (count <= kBlockRows, slot = colours)
+    std::vector<int8_t> rowColour;                // block-local colour of each row (block levels)
     std::vector<int32_t> natural;                 // row -> natural index in its system (-1 padding)
     std::vector<int32_t> rowSys;                  // row -> system (batch order), -1 padding
     std::vector<int32_t> sysRow;                  // system -> first row of its block

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
+#include <functional>
 #include <set>
 
 #include "krylov.cuh"
@@ -43,10 +44,19 @@ namespace {
 
 inline int nblk(int n, int t = 256) { return (n + t - 1) / t; }
 
-// Launch helper: skips empty grids (a zero-block launch is an error).
+// Coarsest matrices up to this order are factorised in shared memory (2 n^2 doubles).
+constexpr int kCoarseSharedN = 80;
+
+// Kernels enqueued (or captured) by this thread; solve() turns captured counts into executed ones.
+thread_local int64_t tl_launches = 0;
+
+// Launch helper: skips empty grids (a zero-block launch is an error) and counts the launch.
 #define VLM_LAUNCH(kernel, grid, block, stream, ...)                    \
     do {                                                                \
-        if ((grid) > 0) kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__); \
+        if ((grid) > 0) {                                               \
+            kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);      \
+            ++tl_launches;                                              \
+        }                                                               \
     } while (0)
 
 template <class T> struct LV;
@@ -88,6 +98,8 @@ std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
 DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
     : stream_(stream) {
     plan_ = buildPlan(systems, mergeLevels);
+    const char* gv = std::getenv("VLM_GRAPH");
+    useGraphs_ = !(gv && gv[0] == '0');
     const int nL = int(plan_.levels.size());
     L_.resize(nL);
     const char* om = std::getenv("VLM_JACOBI_OMEGA");
@@ -104,6 +116,9 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     for (int k = 0; k < nL; ++k) {
         LevelPlan& P = plan_.levels[k];
         DevLevel& D = L_[k];
+        D.blockGS = P.blockGS;
+        if (P.blockGS && P.rowColour.size() != size_t(P.nrows))
+            throw Error(VLM_ERR_BAD_ARG, "internal: block colour layout mismatch");
         D.nrows = P.nrows;
         D.nfaces = P.nfaces;
         D.nActiveRows = P.nActiveRows;
@@ -124,7 +139,9 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         D.all = add(P.all);
         for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
         for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
+        D.blocks = add(P.blocks);
         D.chunks.upload(all, stream_);
+        if (P.blockGS) D.rowColour.upload(P.rowColour, stream_);
         if (k + 1 < nL) {
             D.agg.upload(P.agg, stream_);
             D.childPtr.upload(P.childPtr, stream_);
@@ -144,6 +161,12 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         }
         D.t.resize(size_t(D.nrows));
         D.x2.resize(size_t(D.nrows));
+        D.t.zero(stream_);
+        D.x2.zero(stream_);
+        if (k > 0) {
+            D.r.zero(stream_);
+            D.x.zero(stream_);
+        }
         // host-side plan data no longer needed on the device path
         std::vector<int32_t>().swap(P.col);
         std::vector<int32_t>().swap(P.src);
@@ -163,12 +186,10 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     dctrl_.resize(1);
     anyActive_.resize(1);
     const int n0 = L_[0].nrows;
-    x_.resize(n0);
-    b_.resize(n0);
-    r_.resize(n0);
-    w_.resize(n0);
-    p_.resize(n0);
-    Ap_.resize(n0);
+    for (DBuf<double>* v : {&x_, &b_, &r_, &w_, &p_, &Ap_}) {
+        v->resize(n0);
+        v->zero(stream_);
+    }
     hostState_.resize(size_t(plan_.nsys));
     VLM_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -206,6 +227,11 @@ void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
         w32_.resize(n0);
         p32_.resize(n0);
         Ap32_.resize(n0);
+        e32_.zero(stream_);
+        r32_.zero(stream_);
+        w32_.zero(stream_);
+        p32_.zero(stream_);
+        Ap32_.zero(stream_);
         for (size_t k = 0; k < L_.size(); ++k) {
             DevLevel& D = L_[k];
             D.diag32.resize(size_t(D.nrows));
@@ -213,15 +239,19 @@ void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
             if (k > 0) {
                 D.r32.resize(size_t(D.nrows));
                 D.x32.resize(size_t(D.nrows));
+                D.r32.zero(stream_);
+                D.x32.zero(stream_);
             }
             D.t32.resize(size_t(D.nrows));
             D.x232.resize(size_t(D.nrows));
+            D.t32.zero(stream_);
+            D.x232.zero(stream_);
         }
     }
 }
 
 RedCtx DeviceBatch::red() const {
-    return RedCtx{partials_.get(), counters_.get(), slotBegin_.get(), slotEnd_.get()};
+    return RedCtx{partials_.get(), xbins_.get(), counters_.get(), slotBegin_.get(), slotEnd_.get()};
 }
 
 // ====================================================================== per-solve setup
@@ -249,8 +279,17 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
     VLM_CUDA(cudaMemsetAsync(status_.get(), 0, sizeof(int), s));
     for (int k = 0; k < nL; ++k) {
         DevLevel& D = L_[k];
-        VLM_LAUNCH(k_coarse_factor, D.coarse.n, 128, s, coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
-                   D.diag.get(), lu_.get(), inv_.get(), status_.get());
+        if (D.coarse.n == 0) continue;
+        int nmax = 0;
+        for (const auto& c : plan_.coarse)
+            if (c.level == k) nmax = std::max(nmax, c.n);
+        const int smemN = nmax <= kCoarseSharedN ? nmax : 0;
+        const size_t smem = size_t(2) * smemN * smemN * sizeof(double);
+        if (smem > 48 * 1024)
+            VLM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        k_coarse_factor<<<D.coarse.n, 128, smem, s>>>(coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
+                                                     D.diag.get(), lu_.get(), inv_.get(), status_.get(), smemN);
+        ++tl_launches;
     }
 }
 
@@ -263,7 +302,24 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
     const T* val = LV<T>::val(D);
     const T* diag = LV<T>::diag(D);
     const SysState* st = st_.get();
-    if (sm == SmootherKind::MCGS) {
+    if (sm == SmootherKind::MCGS && D.blockGS) {
+        // block-hybrid GS; pre: from zero, post: prolongation fused into the first sweep
+        T* x2 = LV<T>::x2(D);
+        const int8_t* rc = D.rowColour.get();
+        const int32_t* agg = D.agg.get();
+        const T* xc = k + 1 < int(L_.size()) ? LV<T>::x(L_[k + 1]) : nullptr;
+        if (pre) {
+            VLM_LAUNCH((k_smooth_bgs<T, 1, true>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x, x2,
+                       rc, agg, xc, st, flag);
+            VLM_LAUNCH((k_smooth_bgs<T, 0, true>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x2, x,
+                       rc, agg, xc, st, flag);
+        } else {
+            VLM_LAUNCH((k_smooth_bgs<T, 2, false>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x,
+                       x2, rc, agg, xc, st, flag);
+            VLM_LAUNCH((k_smooth_bgs<T, 0, false>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x2,
+                       x, rc, agg, xc, st, flag);
+        }
+    } else if (sm == SmootherKind::MCGS) {
         if (pre) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
@@ -314,15 +370,28 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag) {
     }
     for (int k = nL - 2; k >= 0; --k) {
         DevLevel& D = L_[k];
-        VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st, flag);
+        if (!(sm == SmootherKind::MCGS && D.blockGS))  // block GS fuses the prolongation into its first sweep
+            VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st,
+                       flag);
         recordSmooth<T>(k, rr(k), xx(k), sm, false, flag);
     }
 }
 
-void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w) {
+void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32) {
     DevLevel& D0 = L_[0];
     switch (pk) {
-    case PrecondKind::GAMG: recordVcycle<double>(r, w, sm, kFlagDone); break;
+    case PrecondKind::GAMG:
+        if (f32) {
+            // FP32 V-cycle inside the FP64 Krylov recurrence
+            VLM_LAUNCH((k_cast_rows<double, float>), D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), r, r32_.get(),
+                       st_.get(), kFlagDone);
+            recordVcycle<float>(r32_.get(), w32_.get(), sm, kFlagDone);
+            VLM_LAUNCH((k_cast_rows<float, double>), D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), w32_.get(), w,
+                       st_.get(), kFlagDone);
+        } else {
+            recordVcycle<double>(r, w, sm, kFlagDone);
+        }
+        break;
     case PrecondKind::Diagonal:
         VLM_LAUNCH(k_precond_diag<double>, D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), rD_.get(), r, w, st_.get(),
                    kFlagDone);
@@ -335,18 +404,63 @@ void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r
 }
 
 // ====================================================================== iteration bodies
-void DeviceBatch::recordPcgIter(PrecondKind pk, SmootherKind sm) {
+void DeviceBatch::recordIter(const SolveKey& key) {
+    const bool f32 = key.prec == Precision::MixedPrecond;
+    if (key.solver == SolverKind::PCG)
+        recordPcgIter(key.precond, key.smoother, f32);
+    else
+        recordBicgIter(key.precond, key.smoother, f32);
+}
+
+// Eager iteration loop (no graph): same kernels launched directly, convergence read back per
+// iteration.  Used when graphs are disabled (VLM_GRAPH=0), e.g. to profile single kernels.
+void DeviceBatch::runEager(const SolveKey& key, int maxIter) {
+    cudaStream_t s = stream_;
+    auto anyActive = [&](int flag) {
+        VLM_CUDA(cudaMemcpyAsync(hostState_.data(), st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+        for (const auto& q : hostState_)
+            if (!(flag == kFlagDone ? q.done : (q.done || q.innerDone))) return true;
+        return false;
+    };
+    const int cap = 4 * (maxIter + 2);
+    if (key.prec != Precision::MixedDC) {
+        for (int it = 0; it < cap && anyActive(kFlagDone); ++it) recordIter(key);
+        return;
+    }
+    DevLevel& D0 = L_[0];
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    for (int o = 0; o < cap && anyActive(kFlagDone); ++o) {
+        VLM_LAUNCH(k_inner_begin, nblk(plan_.nsys), 256, s, plan_.nsys, st_.get());
+        VLM_LAUNCH(k_zero_rows<float>, nb, kRowsPerCta, s, ch, e32_.get(), st_.get(), kFlagInner);
+        for (int it = 0; it < cap && anyActive(kFlagInner); ++it) recordInnerPcgIter(key.precond, key.smoother);
+        VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), e32_.get(), st_.get());
+        VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
+                   b_.get(), r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
+    }
+}
+
+void DeviceBatch::recordPcgIter(PrecondKind pk, SmootherKind sm, bool f32) {
+    if (exact_)
+        recordPcgIterT<true>(pk, sm, f32);
+    else
+        recordPcgIterT<false>(pk, sm, f32);
+}
+
+template <bool EXACT>
+void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
     DevLevel& D0 = L_[0];
     cudaStream_t s = stream_;
     const Chunk* ch = D0.ch(D0.all);
     const int nb = D0.all.n;
-    recordPrecond(pk, sm, r_.get(), w_.get());
-    VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), r_.get(), red(), st_.get());
+    recordPrecond(pk, sm, r_.get(), w_.get(), f32);
+    VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, w_.get(), r_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
-    VLM_LAUNCH((k_pcg_spmv<double, kFlagDone>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), p_.get(),
-               Ap_.get(), red(), st_.get());
-    VLM_LAUNCH((k_pcg_update<double, kFlagDone>), nb, kRowsPerCta, s, ch, x_.get(), r_.get(), p_.get(), Ap_.get(),
-               perm0_.get(), red(), st_.get(), dctrl_.get());
+    VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(),
+               p_.get(), Ap_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_update<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, x_.get(), r_.get(), p_.get(),
+               Ap_.get(), perm0_.get(), red(), st_.get(), dctrl_.get());
 }
 
 void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
@@ -361,37 +475,46 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
                    kFlagInner);
     else
         throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs the GAMG or diagonal preconditioner");
-    VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
+    VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
-    VLM_LAUNCH((k_pcg_spmv<float, kFlagInner>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), D0.diag32.get(),
+    VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), D0.diag32.get(),
                p32_.get(), Ap32_.get(), red(), st_.get());
-    VLM_LAUNCH((k_pcg_update<float, kFlagInner>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
+    VLM_LAUNCH((k_pcg_update<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
                Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get());
 }
 
-void DeviceBatch::recordBicgIter(PrecondKind pk, SmootherKind sm) {
+void DeviceBatch::recordBicgIter(PrecondKind pk, SmootherKind sm, bool f32) {
+    if (exact_)
+        recordBicgIterT<true>(pk, sm, f32);
+    else
+        recordBicgIterT<false>(pk, sm, f32);
+}
+
+template <bool EXACT>
+void DeviceBatch::recordBicgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
     DevLevel& D0 = L_[0];
     cudaStream_t s = stream_;
     const Chunk* ch = D0.ch(D0.all);
     const int nb = D0.all.n;
     SysState* st = st_.get();
-    VLM_LAUNCH(k_bicg_rho, nb, kRowsPerCta, s, ch, r0_.get(), r_.get(), red(), st);
+    VLM_LAUNCH(k_bicg_rho<EXACT>, nb, kRowsPerCta, s, ch, r0_.get(), r_.get(), red(), st);
     VLM_LAUNCH(k_bicg_p, nb, kRowsPerCta, s, ch, r_.get(), Ay_.get(), p_.get(), st);
-    recordPrecond(pk, sm, p_.get(), y_.get());
-    VLM_LAUNCH(k_bicg_spmv_alpha, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), y_.get(), Ay_.get(),
+    recordPrecond(pk, sm, p_.get(), y_.get(), f32);
+    VLM_LAUNCH(k_bicg_spmv_alpha<EXACT>, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), y_.get(), Ay_.get(),
                r0_.get(), red(), st);
-    VLM_LAUNCH(k_bicg_s, nb, kRowsPerCta, s, ch, r_.get(), Ay_.get(), s_.get(), red(), st, dctrl_.get());
+    VLM_LAUNCH(k_bicg_s<EXACT>, nb, kRowsPerCta, s, ch, r_.get(), Ay_.get(), s_.get(), red(), st, dctrl_.get());
     VLM_LAUNCH(k_bicg_early, nb, kRowsPerCta, s, ch, x_.get(), y_.get(), st);
     VLM_LAUNCH(k_bicg_early_close, nblk(plan_.nsys), 256, s, plan_.nsys, st);
-    recordPrecond(pk, sm, s_.get(), z_.get());
-    VLM_LAUNCH(k_bicg_spmv_omega, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), z_.get(), t_.get(),
+    recordPrecond(pk, sm, s_.get(), z_.get(), f32);
+    VLM_LAUNCH(k_bicg_spmv_omega<EXACT>, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), z_.get(), t_.get(),
                s_.get(), red(), st);
-    VLM_LAUNCH(k_bicg_update, nb, kRowsPerCta, s, ch, x_.get(), r_.get(), y_.get(), z_.get(), s_.get(), t_.get(), red(),
+    VLM_LAUNCH(k_bicg_update<EXACT>, nb, kRowsPerCta, s, ch, x_.get(), r_.get(), y_.get(), z_.get(), s_.get(), t_.get(), red(),
                st, dctrl_.get());
 }
 
 void DeviceBatch::recordSetCond(cudaGraphConditionalHandle h, int flag) {
     k_set_cond<<<1, 256, 0, stream_>>>(h, plan_.nsys, st_.get(), flag);
+    ++tl_launches;
 }
 
 // ====================================================================== graphs
@@ -441,23 +564,30 @@ cudaGraphNode_t addWhile(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditiona
 void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
     VLM_CUDA(cudaGraphCreate(&G.graph, 0));
     cudaStream_t s = stream_;
-    if (!key.mixed) {
+    const int64_t saved = tl_launches;
+    int64_t mark = tl_launches;
+    auto segment = [&]() {
+        const int64_t k = tl_launches - mark;
+        mark = tl_launches;
+        return k;
+    };
+    if (key.prec != Precision::MixedDC) {
         cudaGraphConditionalHandle h;
         VLM_CUDA(cudaGraphConditionalHandleCreate(&h, G.graph, 0, cudaGraphCondAssignDefault));
         cudaGraphNode_t pre = captureInto(s, G.graph, {}, [&] { recordSetCond(h, kFlagDone); });
+        G.preK = segment();
         cudaGraph_t body;
         addWhile(G.graph, pre, h, &body);
         captureInto(s, body, {}, [&] {
-            if (key.solver == SolverKind::PCG)
-                recordPcgIter(key.precond, key.smoother);
-            else
-                recordBicgIter(key.precond, key.smoother);
+            recordIter(key);
             recordSetCond(h, kFlagDone);
         });
+        G.bodyK = segment();
     } else {
         cudaGraphConditionalHandle ho;
         VLM_CUDA(cudaGraphConditionalHandleCreate(&ho, G.graph, 0, cudaGraphCondAssignDefault));
         cudaGraphNode_t pre = captureInto(s, G.graph, {}, [&] { recordSetCond(ho, kFlagDone); });
+        G.preK = segment();
         cudaGraph_t outer;
         addWhile(G.graph, pre, ho, &outer);
         cudaGraphConditionalHandle hi;
@@ -470,19 +600,23 @@ void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
             VLM_LAUNCH(k_zero_rows<float>, nb, kRowsPerCta, s, ch, e32_.get(), st_.get(), kFlagInner);
             recordSetCond(hi, kFlagInner);
         });
+        G.bodyK = segment();
         cudaGraph_t inner;
         cudaGraphNode_t w = addWhile(outer, seg1, hi, &inner);
         captureInto(s, inner, {}, [&] {
             recordInnerPcgIter(key.precond, key.smoother);
             recordSetCond(hi, kFlagInner);
         });
+        G.innerK = segment();
         captureInto(s, outer, {w}, [&] {
             VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), e32_.get(), st_.get());
             VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
                        b_.get(), r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
             recordSetCond(ho, kFlagDone);
         });
+        G.bodyK += segment();
     }
+    tl_launches = saved;
     VLM_CUDA(cudaGraphInstantiate(&G.exec, G.graph, 0));
 }
 
@@ -520,12 +654,22 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
                             : eq(ctrl.smoother, "jacobi")
                                 ? SmootherKind::Jacobi
                                 : throw Error(VLM_ERR_BAD_ARG, std::string("unknown smoother ") + ctrl.smoother);
-    const bool mixed = eq(ctrl.precision, "mixed");
-    if (!mixed && ctrl.precision[0] != 0 && !eq(ctrl.precision, "fp64"))
+    Precision prec = Precision::FP64;
+    if (eq(ctrl.precision, "mixed"))
+        prec = Precision::MixedPrecond;
+    else if (eq(ctrl.precision, "mixed-dc"))
+        prec = Precision::MixedDC;
+    else if (ctrl.precision[0] != 0 && !eq(ctrl.precision, "fp64"))
         throw Error(VLM_ERR_BAD_ARG, std::string("unknown precision ") + ctrl.precision);
-    if (mixed && sk != SolverKind::PCG) throw Error(VLM_ERR_UNSUPPORTED, "mixed precision is implemented for PCG");
-    if (mixed && pk == PrecondKind::None) throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs a preconditioner");
+    if (prec == Precision::MixedPrecond && pk != PrecondKind::GAMG) prec = Precision::FP64;  // nothing to lower
+    if (prec == Precision::MixedDC && sk != SolverKind::PCG)
+        throw Error(VLM_ERR_UNSUPPORTED, "defect-correction mixed precision is implemented for PCG");
+    if (prec == Precision::MixedDC && pk == PrecondKind::None)
+        throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs a preconditioner");
+    const bool mixed = prec != Precision::FP64;
+    const bool dc = prec == Precision::MixedDC;
     ensureVectors(mixed, sk == SolverKind::PBiCGStab);
+    const int64_t launch0 = tl_launches;
 
     setupMatrix(diag, upper, lower, pk == PrecondKind::GAMG, mixed);
     DevLevel& D0 = L_[0];
@@ -549,22 +693,54 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     st_.zero(s);
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), b, b_.get());
-    VLM_LAUNCH(k_sum_x<double>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
-    VLM_LAUNCH(k_init_residual, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(),
-               x_.get(), b_.get(), perm0_.get(), r_.get(), mixed ? r32_.get() : nullptr, sysCells_.get(), red(),
-               st_.get(), dctrl_.get());
+    if (exact_) {
+        VLM_LAUNCH((k_sum_x<double, true>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
+        VLM_LAUNCH(k_init_residual<true>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(),
+                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), dc ? r32_.get() : nullptr,
+                   sysCells_.get(), red(), st_.get(), dctrl_.get());
+    } else {
+        VLM_LAUNCH((k_sum_x<double, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
+        VLM_LAUNCH(k_init_residual<false>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(),
+                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), dc ? r32_.get() : nullptr,
+                   sysCells_.get(), red(), st_.get(), dctrl_.get());
+    }
     if (sk == SolverKind::PBiCGStab) {
         VLM_CUDA(cudaMemcpyAsync(r0_.get(), r_.get(), sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
         Ay_.zero(s);
         p_.zero(s);
     }
-    GraphExec& G = graphFor(SolveKey{sk, pk, sm, mixed});
-    VLM_CUDA(cudaGraphLaunch(G.exec, s));
+    exact_ = ctrl.reproducible != 0;
+    if (exact_ && xbins_.size() == 0) {
+        xbins_.resize(size_t(plan_.nSlots) * 2 * 73);
+        xbins_.zero(s);
+    }
+    const SolveKey key{sk, pk, sm, prec, exact_};
+    int64_t eagerLaunches = 0;
+    GraphExec* Gp = nullptr;
+    if (useGraphs_) {
+        Gp = &graphFor(key);
+        VLM_CUDA(cudaGraphLaunch(Gp->exec, s));
+    } else {
+        const int64_t e0 = tl_launches;
+        runEager(key, ctrl.maxIter);
+        eagerLaunches = tl_launches - e0;
+        tl_launches = e0;
+    }
     VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), x_.get(), x);
     int coarseStatus = 0;
     VLM_CUDA(cudaMemcpyAsync(hostState_.data(), st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaStreamSynchronize(s));
+    // executed kernels: the eager setup + the graph's pre-node + one body per loop pass
+    int64_t iters = 0, outers = 0;
+    for (int bpos = 0; bpos < plan_.nsys; ++bpos) {
+        iters = std::max<int64_t>(iters, hostState_[bpos].iterations);
+        outers = std::max<int64_t>(outers, hostState_[bpos].outer);
+    }
+    if (Gp)
+        launches_ += (tl_launches - launch0) + Gp->preK + (dc ? outers * Gp->bodyK + iters * Gp->innerK : iters * Gp->bodyK);
+    else
+        launches_ += (tl_launches - launch0) + eagerLaunches;
     if (pk == PrecondKind::GAMG && coarseStatus == VLM_ERR_SINGULAR)
         throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
     perfOut.resize(size_t(plan_.nsys));
@@ -613,6 +789,77 @@ void DeviceBatch::gamgApply(const double* diag, const double* upper, const doubl
     VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaStreamSynchronize(s));
     if (coarseStatus == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+}
+
+double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n) {
+    if (n <= 0) return 0.0;
+    std::vector<Chunk> ch;
+    for (int64_t q = 0; q < n; q += kRowsPerCta)
+        ch.push_back(Chunk{int32_t(q), int32_t(std::min<int64_t>(kRowsPerCta, n - q)), 0, int32_t(q / kRowsPerCta)});
+    DBuf<Chunk> dch;
+    dch.upload(ch, s);
+    DBuf<long long> bins(ch.size() * 73);
+    DBuf<int> cnt(1), sb(1), se(1);
+    cnt.zero(s);
+    const int zero = 0, nsl = int(ch.size());
+    VLM_CUDA(cudaMemcpyAsync(sb.get(), &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+    VLM_CUDA(cudaMemcpyAsync(se.get(), &nsl, sizeof(int), cudaMemcpyHostToDevice, s));
+    DBuf<double> out(1);
+    RedCtx R{nullptr, bins.get(), cnt.get(), sb.get(), se.get()};
+    VLM_LAUNCH(k_exact_sum, nsl, kRowsPerCta, s, dch.get(), v, R, out.get());
+    double h = 0;
+    VLM_CUDA(cudaMemcpyAsync(&h, out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+double DeviceBatch::profileKernel(const std::string& name, int reps, double* bytesPerLaunch) {
+    cudaStream_t s = stream_;
+    DevLevel& D0 = L_[0];
+    const double N = double(plan_.userCells), F = double(plan_.userFaces);
+    cudaEvent_t e0, e1;
+    VLM_CUDA(cudaEventCreate(&e0));
+    VLM_CUDA(cudaEventCreate(&e1));
+    const bool f32 = name.size() > 2 && name.substr(name.size() - 2) == "32";
+    const double sz = f32 ? 4.0 : 8.0;
+    if (f32 && D0.val32.size() == 0) throw Error(VLM_ERR_BAD_ARG, "run a mixed-precision solve first");
+    std::function<void()> run;
+    if (name == "amul64") {
+        run = [&] { VLM_LAUNCH(k_amul, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), x_.get(), w_.get()); };
+        *bytesPerLaunch = sz * 3 * N + sz * F + 8 * F;
+    } else if (name == "smooth64" || name == "smooth32") {
+        run = [&] {
+            for (int t = 0; t < D0.nSteps; ++t) {
+                if (f32)
+                    VLM_LAUNCH(k_smooth_gs<float>, D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val32.get(), D0.diag32.get(), r32_.get(), w32_.get(), st_.get(), kFlagDone);
+                else
+                    VLM_LAUNCH(k_smooth_gs<double>, D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), st_.get(), kFlagDone);
+            }
+        };
+        *bytesPerLaunch = sz * 4 * N + sz * F + 8 * F;
+    } else if (name == "residual64" || name == "residual32") {
+        run = [&] {
+            if (f32)
+                VLM_LAUNCH(k_residual<float>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), D0.sell(), D0.val32.get(), D0.diag32.get(), r32_.get(), w32_.get(), D0.t32.get(), st_.get(), kFlagDone);
+            else
+                VLM_LAUNCH(k_residual<double>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), D0.t.get(), st_.get(), kFlagDone);
+        };
+        *bytesPerLaunch = sz * 4 * N + sz * F + 8 * F;
+    } else {
+        throw Error(VLM_ERR_BAD_ARG, "unknown kernel " + name);
+    }
+    // st_ flags of a finished solve are 'done': clear them so the kernels do their work
+    st_.zero(s);
+    run();
+    VLM_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < reps; ++i) run();
+    VLM_CUDA(cudaEventRecord(e1, s));
+    VLM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    VLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return double(ms) / reps;
 }
 
 template void DeviceBatch::recordVcycle<double>(const double*, double*, SmootherKind, int);

@@ -18,7 +18,10 @@ struct ChunkList {
 };
 
 struct DevLevel {
+    bool blockGS = false;
     int nrows = 0, nfaces = 0, nActiveRows = 0, nSteps = 0, nent = 0, maxColours = 0;
+    ChunkList blocks;
+    DBuf<int8_t> rowColour;
     DBuf<int32_t> slPtr, rlen, col, src;
     DBuf<Chunk> chunks;
     ChunkList active, all;
@@ -38,20 +41,25 @@ struct DevLevel {
 enum class SolverKind { PCG, PBiCGStab, Jacobi, GaussSeidel, SymGaussSeidel };
 enum class PrecondKind { None, Diagonal, GAMG, DIC, DILU };
 enum class SmootherKind { MCGS, Jacobi };
+// FP64; FP64 Krylov recurrence with an FP32 GAMG V-cycle; FP32 inner PCG in FP64 defect correction
+enum class Precision { FP64, MixedPrecond, MixedDC };
 
 struct SolveKey {
     SolverKind solver;
     PrecondKind precond;
     SmootherKind smoother;
-    bool mixed;
+    Precision prec;
+    bool exact;
     bool operator<(const SolveKey& o) const {
-        return std::tie(solver, precond, smoother, mixed) < std::tie(o.solver, o.precond, o.smoother, o.mixed);
+        return std::tie(solver, precond, smoother, prec, exact) <
+               std::tie(o.solver, o.precond, o.smoother, o.prec, o.exact);
     }
 };
 
 struct GraphExec {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int64_t preK = 0, bodyK = 0, innerK = 0;  // kernels per captured segment
     ~GraphExec();
 };
 
@@ -84,14 +92,23 @@ public:
 
     cudaStream_t stream() const { return stream_; }
     size_t deviceBytes() const;
+    int64_t launches() const { return launches_; }
+    // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
+    // solve); returns ms per launch and the algorithmic bytes one launch moves.
+    double profileKernel(const std::string& name, int reps, double* bytesPerLaunch);
+
 
 private:
     template <class T> void recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag);
     template <class T> void recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag);
-    void recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w);
-    void recordPcgIter(PrecondKind pk, SmootherKind sm);
+    void recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32);
+    void recordIter(const SolveKey& key);
+    void runEager(const SolveKey& key, int maxIter);
+    void recordPcgIter(PrecondKind pk, SmootherKind sm, bool f32);
     void recordInnerPcgIter(PrecondKind pk, SmootherKind sm);
-    void recordBicgIter(PrecondKind pk, SmootherKind sm);
+    void recordBicgIter(PrecondKind pk, SmootherKind sm, bool f32);
+    template <bool EXACT> void recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32);
+    template <bool EXACT> void recordBicgIterT(PrecondKind pk, SmootherKind sm, bool f32);
     void recordSetCond(cudaGraphConditionalHandle h, int flag);
     GraphExec& graphFor(const SolveKey& key);
     void buildGraph(const SolveKey& key, GraphExec& g);
@@ -105,6 +122,8 @@ private:
     DBuf<double> lu_, inv_;
     DBuf<int32_t> perm0_, sysCells_, slotBegin_, slotEnd_, counters_, status_;
     DBuf<DD> partials_;
+    DBuf<long long> xbins_;  // exact-sum partials (reproducible mode)
+    bool exact_ = false;
     DBuf<SysState> st_;
     DBuf<DevCtrl> dctrl_;
     DBuf<int> anyActive_;
@@ -114,7 +133,12 @@ private:
     std::map<SolveKey, std::unique_ptr<GraphExec>> graphs_;
     std::vector<SysState> hostState_;
     double jacobiOmega_ = 1.0;
+    int64_t launches_ = 0;
+    bool useGraphs_ = true;
 };
+
+// Exact (order-independent) sum of n device doubles, ordered on stream s.
+double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n);
 
 SolverKind parseSolver(const char* s);
 PrecondKind parsePrecond(const char* s);
