@@ -79,8 +79,10 @@ typedef struct {
     int32_t minIter;
     int32_t nSweeps;
     /* ---- additive keys (zero-initialised struct = reference behaviour) ---- */
-    char smoother[16];        /* GAMG smoother on the device: "" or "mcgs" (multicolour Gauss-Seidel,
-                                 forward colours pre / reversed post) | "jacobi" */
+    char smoother[16];        /* GAMG smoother on the device: "" or "mcgs-jacobi" (level 0 multicolour
+                                 Gauss-Seidel, forward colours pre / reversed post; Jacobi on the
+                                 coarser levels) | "mcgs" (block-hybrid Gauss-Seidel on the coarser
+                                 levels) | "jacobi" (every level) */
     char precision[16];       /* "" or "fp64" | "mixed" (FP32 inner PCG+GAMG in FP64 defect correction) */
     int32_t reproducible;     /* 1: CFD_REPRODUCIBLE semantics: preconditioner -> diagonal,
                                  GS -> Jacobi, exact (order-independent) global sums */

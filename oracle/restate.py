@@ -11,7 +11,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libvlmoracle.so")
-SMOOTHERS = {"gs": 0, "mcgs": 1, "jacobi": 2}
+SMOOTHERS = {"gs": 0, "mcgs": 1, "jacobi": 2, "mcgs-jacobi": 3}
 
 _lib = None
 

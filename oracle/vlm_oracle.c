@@ -583,7 +583,15 @@ static void gamg_smooth(gamg_t* g, int lev, const double* r, double* x, int forw
     const double* D = g->diag[lev];
     const double* up = g->up[lev];
     const double* lo = g->lo[lev];
-    if (g->opt.smoother == 1 && g->blockGS[lev]) {
+    if (g->opt.smoother == 3 && lev > 0) {
+        double* xo = g->x2[lev];
+        const double om = g->opt.omega;
+        for (int i = 0; i < L->n; ++i) {
+            const double v = row_minus(L, up, lo, x, i, r[i]) / D[i];
+            xo[i] = om == 1.0 ? v : x[i] + om * (v - x[i]);
+        }
+        memcpy(x, xo, sizeof(double) * (size_t)L->n);
+    } else if ((g->opt.smoother == 1 || g->opt.smoother == 3) && g->blockGS[lev]) {
         /* block-hybrid GS: Gauss-Seidel inside each block in block-local colour order; the terms
            of neighbours outside the block (previous sweep) are subtracted first, then the
            in-block terms, each group in face order */
@@ -626,7 +634,7 @@ static void gamg_smooth(gamg_t* g, int lev, const double* r, double* x, int forw
             for (int i = 0; i < L->n; ++i) x[i] = row_minus(L, up, lo, x, i, r[i]) / D[i];
         else
             for (int i = L->n - 1; i >= 0; --i) x[i] = row_minus(L, up, lo, x, i, r[i]) / D[i];
-    } else if (g->opt.smoother == 1) {
+    } else if (g->opt.smoother == 1 || g->opt.smoother == 3) {
         const int nc = g->ncol[lev];
         const int* col = g->colour[lev];
         for (int t = 0; t < nc; ++t) {

@@ -36,7 +36,8 @@ int vo_hier_colour(const vo_hier* h, int lev, int* colour);
  * 1 = the device's Gauss-Seidel schedule: level 0 multicolour GS (forward colours pre, reversed
  *     post) when its greedy colouring has <= 4 colours, block-hybrid GS (512-row blocks,
  *     block-local colours, out-of-block neighbours from the previous sweep) on the other levels,
- * 2 = Jacobi(omega);
+ * 2 = Jacobi(omega) on every level,
+ * 3 = level 0 as in 1, Jacobi(omega) on the coarser levels;
  * coarse 0 = LU substitution (GAMG.cpp:406-420), 1 = explicit inverse from the LU. */
 typedef struct {
     int smoother;

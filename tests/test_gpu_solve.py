@@ -112,7 +112,15 @@ def test_vcycle_jacobi_matches_oracle(name):
 
 
 @pytest.mark.parametrize("name", golden_names())
-@pytest.mark.parametrize("smoother", ["mcgs", "jacobi"])
+def test_vcycle_mcgs_jacobi_matches_oracle(name):
+    g, m = device_mesh(name)
+    w = vb.gamg_apply(m, g["diag"], g["upper"], None, g["b"], smoother="mcgs-jacobi")
+    wo = ro.gamg_apply(g, g["diag"], g["upper"], None, g["b"], smoother="mcgs-jacobi", coarse=1)
+    assert rel(w, wo) <= 1e-14
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("smoother", ["mcgs", "mcgs-jacobi", "jacobi"])
 def test_pcg_gamg_matches_oracle(name, smoother):
     g, m = device_mesh(name)
     x = g["x0"].copy()
@@ -125,8 +133,8 @@ def test_pcg_gamg_matches_oracle(name, smoother):
     # against the reference's sequential-GS GAMG: same tolerance reached, counts reported
     ref = perf_dict(g["pcg_gamg_perf"])
     assert true_residual(g, g["diag"], g["upper"], None, g["b"], x) <= 1e-8 * ref["residualSum"] * 1.0001
-    if smoother == "mcgs":
-        assert abs(p.iterations - ref["iterations"]) <= 2
+    if smoother != "jacobi":
+        assert abs(p.iterations - ref["iterations"]) <= 3
 
 
 @pytest.mark.parametrize("name", golden_names())
@@ -148,7 +156,7 @@ def test_pbicgstab_gamg(name):
     p = vb.solve_ldu(m, g["diag"], g["upper"], g["lower_asym"], g["b"], x,
                      ctrl(solver="PBiCGStab", preconditioner="GAMG"))
     xo, po = ro.solve(g, g["diag"], g["upper"], g["lower_asym"], g["b"], g["x0"], "PBiCGStab", "GAMG", 0.0, 1e-8,
-                      2000, smoother="mcgs", coarse=1)
+                      2000, smoother="mcgs-jacobi", coarse=1)
     assert p.converged
     assert abs(p.iterations - po["iterations"]) <= 1
 
@@ -250,7 +258,7 @@ def test_64cubed_gamg_against_oracle():
     m = vb.Mesh.from_arrays(M)
     x = np.zeros(M["n_cells"])
     p = vb.solve_ldu(m, d, up, None, b, x, ctrl(preconditioner="GAMG"))
-    xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000, smoother="mcgs",
-                      coarse=1)
+    xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000,
+                      smoother="mcgs-jacobi", coarse=1)
     assert abs(p.iterations - po["iterations"]) <= 1
     assert rel(x, xo) <= 1e-9

@@ -39,7 +39,7 @@ class SolverControls:
     maxIter: int = 1000
     minIter: int = 0
     nSweeps: int = 1
-    smoother: str = ""          # GAMG smoother on the device: "" / "mcgs" | "jacobi"
+    smoother: str = ""          # GAMG smoother: "" / "mcgs-jacobi" | "mcgs" | "jacobi"
     precision: str = ""         # "" / "fp64" | "mixed"
     reproducible: bool = False  # CFD_REPRODUCIBLE semantics
     mergeLevels: int = 0

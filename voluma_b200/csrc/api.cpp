@@ -231,8 +231,7 @@ vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const d
         stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
         m->b.upload(r, size_t(m->nCells), ctx->stream);
         m->x.resize(size_t(m->nCells));
-        vlm::SmootherKind sm = vlm::SmootherKind::MCGS;
-        if (ctrl && std::string(ctrl->smoother) == "jacobi") sm = vlm::SmootherKind::Jacobi;
+        const vlm::SmootherKind sm = vlm::parseSmoother(ctrl ? ctrl->smoother : "");
         m->batch->gamgApply(dd, du, dl, m->b.get(), m->x.get(), sm);
         VLM_CUDA(cudaMemcpy(w, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost));
     });

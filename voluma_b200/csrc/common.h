@@ -78,6 +78,8 @@ struct Chunk {
 };
 
 constexpr int kRowsPerCta = 256;
+// Level-0 Krylov kernels give each CTA up to this many rows (4 per thread): fewer partial sums.
+constexpr int kWideRows = 1024;
 // Rows of one block-hybrid Gauss-Seidel block (one CTA of that many threads).
 constexpr int kBlockRows = 512;
 constexpr int kSlice = 32;  // SELL slice height (one warp)

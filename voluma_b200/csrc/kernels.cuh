@@ -83,13 +83,26 @@ __device__ bool reduce_dd(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (
     DD acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = DD{0.0, 0.0};
-    for (int s = b + (int)threadIdx.x; s < e; s += blockDim.x) {
+    // slots s = b + t + 256 m, combined in ascending m; loads issued 4 at a time
+    const double2* P = reinterpret_cast<const double2*>(R.partials);
+    int s = b + (int)threadIdx.x;
+    for (; s + 3 * (int)blockDim.x < e; s += 4 * blockDim.x) {
+        double2 w[4][NV];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) w[u][q] = __ldcg(&P[(size_t)(s + u * blockDim.x) * NV + q]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc[q] = dd_add(acc[q], DD{w[u][q].x, w[u][q].y});
+    }
+    for (; s < e; s += blockDim.x)
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            const volatile double* pp = (const volatile double*)&R.partials[(size_t)s * NV + q];
-            acc[q] = dd_add(acc[q], DD{pp[0], pp[1]});
+            const double2 w = __ldcg(&P[(size_t)s * NV + q]);
+            acc[q] = dd_add(acc[q], DD{w.x, w.y});
         }
-    }
     __syncthreads();  // the shared tree below is reused
     block_reduce<NV>(acc);
     if (threadIdx.x != 0) return false;
@@ -162,18 +175,13 @@ __device__ double exact_value(long long* b, int flags) {
     return sign * r;
 }
 
+// Writes this CTA's exact bins as its partial; the last CTA of the system adds every partial
+// (int64, exact in any order) and converts the total like binsToDouble.
 template <int NV>
-__device__ bool reduce_exact(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+__device__ bool reduce_exact_bins(long long (*bins)[kRowsPerCta / 32][kExactBins], int (*flags)[kRowsPerCta / 32],
+                                  const Chunk& c, const RedCtx& R, double (&out)[NV]) {
     constexpr int kWarps = kRowsPerCta / 32;
-    __shared__ long long bins[NV][kWarps][kExactBins];
-    __shared__ int flags[NV][kWarps];
     __shared__ int isLast;
-    for (int q = threadIdx.x; q < NV * kWarps * kExactBins; q += blockDim.x) (&bins[0][0][0])[q] = 0;
-    if ((int)threadIdx.x < NV * kWarps) (&flags[0][0])[threadIdx.x] = 0;
-    __syncthreads();
-    const int warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; ++q) exact_add(bins[q][warp], &flags[q][warp], v[q].hi);
     __syncthreads();
     long long* dst = R.xbins + (size_t)c.slot * NV * kExactStride;
     for (int idx = threadIdx.x; idx < NV * kExactBins; idx += blockDim.x) {
@@ -196,18 +204,17 @@ __device__ bool reduce_exact(DD (&v)[NV], const Chunk& c, const RedCtx& R, doubl
     __syncthreads();
     if (!isLast) return false;
     __threadfence();
-    // totals: thread (q, k) adds bin k of every slot (int64: exact in any order)
     __shared__ long long tot[NV][kExactStride];
     const int b0 = R.slotBegin[c.sys], b1 = R.slotEnd[c.sys];
     for (int idx = threadIdx.x; idx < NV * kExactStride; idx += blockDim.x) {
         const int q = idx / kExactStride, k = idx % kExactStride;
         long long s = 0;
         for (int sl = b0; sl < b1; ++sl) {
-            const volatile long long* src = R.xbins + (size_t)sl * NV * kExactStride + q * kExactStride;
+            const long long v = __ldcg(R.xbins + (size_t)sl * NV * kExactStride + q * kExactStride + k);
             if (k < kExactBins)
-                s += src[k];
+                s += v;
             else
-                s |= src[k];
+                s |= v;
         }
         tot[q][k] = s;
     }
@@ -219,6 +226,19 @@ __device__ bool reduce_exact(DD (&v)[NV], const Chunk& c, const RedCtx& R, doubl
     return true;
 }
 
+template <int NV>
+__device__ bool reduce_exact(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+    constexpr int kWarps = kRowsPerCta / 32;
+    __shared__ long long bins[NV][kWarps][kExactBins];
+    __shared__ int flags[NV][kWarps];
+    for (int q = threadIdx.x; q < NV * kWarps * kExactBins; q += blockDim.x) (&bins[0][0][0])[q] = 0;
+    if ((int)threadIdx.x < NV * kWarps) (&flags[0][0])[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) exact_add(bins[q][threadIdx.x >> 5], &flags[q][threadIdx.x >> 5], v[q].hi);
+    return reduce_exact_bins<NV>(bins, flags, c, R, out);
+}
+
 template <int NV, bool EXACT = false>
 __device__ __forceinline__ bool reduce_to_system(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
     if constexpr (EXACT)
@@ -226,6 +246,39 @@ __device__ __forceinline__ bool reduce_to_system(DD (&v)[NV], const Chunk& c, co
     else
         return reduce_dd<NV>(v, c, R, out);
 }
+
+// Per-CTA accumulator used by the reduction kernels: add() values (any number per thread),
+// then finish() -> true in the thread that completes the system, with the totals.
+template <int NV, bool EXACT> struct BlockSum;
+
+template <int NV> struct BlockSum<NV, false> {
+    DD v[NV];
+    __device__ void begin() {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q] = DD{0.0, 0.0};
+    }
+    __device__ void add(int q, double x) { v[q] = dd_add(v[q], DD{x, 0.0}); }
+    __device__ bool finish(const Chunk& c, const RedCtx& R, double (&out)[NV]) { return reduce_dd<NV>(v, c, R, out); }
+};
+
+template <int NV> struct BlockSum<NV, true> {
+    static constexpr int kWarps = kRowsPerCta / 32;
+    long long (*bins)[kWarps][kExactBins];
+    int (*flags)[kWarps];
+    __device__ void begin() {
+        __shared__ long long b[NV][kWarps][kExactBins];
+        __shared__ int f[NV][kWarps];
+        bins = b;
+        flags = f;
+        for (int q = threadIdx.x; q < NV * kWarps * kExactBins; q += blockDim.x) (&b[0][0][0])[q] = 0;
+        if ((int)threadIdx.x < NV * kWarps) (&f[0][0])[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    __device__ void add(int q, double x) { exact_add(bins[q][threadIdx.x >> 5], &flags[q][threadIdx.x >> 5], x); }
+    __device__ bool finish(const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+        return reduce_exact_bins<NV>(bins, flags, c, R, out);
+    }
+};
 
 // Exact sum of a plain array (vlm_exact_sum): one system, chunks of kRowsPerCta values.
 __global__ void __launch_bounds__(kRowsPerCta) k_exact_sum(const Chunk* __restrict__ ch, const double* __restrict__ v,
@@ -279,8 +332,8 @@ template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_zero_rows(const Chunk* __restrict__ ch, T* __restrict__ x,
                                                            const SysState* st, int flag) {
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    x[c.start + threadIdx.x] = T(0);
+    if (chunk_skip(c, st, flag)) return;
+    for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) x[row] = T(0);
 }
 
 // w = r on the rows of the chunks (the "none" preconditioner)
@@ -288,8 +341,8 @@ template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restrict__ ch, const T* __restrict__ r,
                                                            T* __restrict__ w, const SysState* st, int flag) {
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    w[c.start + threadIdx.x] = r[c.start + threadIdx.x];
+    if (chunk_skip(c, st, flag)) return;
+    for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) w[row] = r[row];
 }
 
 // b = (To) a on the rows of the chunks
@@ -297,8 +350,8 @@ template <class From, class To>
 __global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restrict__ ch, const From* __restrict__ a,
                                                            To* __restrict__ b, const SysState* st, int flag) {
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    b[c.start + threadIdx.x] = (To)a[c.start + threadIdx.x];
+    if (chunk_skip(c, st, flag)) return;
+    for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) b[row] = (To)a[row];
 }
 
 // ------------------------------------------------------------------ smoothers
@@ -324,7 +377,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_gs(const Chunk* __restri
 // x_i = (r_i - sum_out a_ij x_j - sum_in a_ij x_j) / a_ii.
 // MODE 0: x = xi; MODE 1: x starts at 0 (first pre-sweep); MODE 2: x = xi + xc[agg] (the
 // coarse-grid correction of GAMG.cpp:437-438, fused in).
-constexpr int kBgsRegEntries = 32;  // in-block entries held in registers; longer rows spill to loads
+constexpr int kBgsRegEntries = 24;  // in-block entries held in registers; longer rows spill to loads
 
 template <class T, int MODE, bool FWD>
 __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __restrict__ blocks, Sell S,
@@ -333,7 +386,7 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
                                                               T* __restrict__ xo, const int8_t* __restrict__ rcol,
                                                               const int32_t* __restrict__ agg,
                                                               const T* __restrict__ xc, const SysState* st, int flag) {
-    __shared__ T xs[kBlockRows];
+    __shared__ T xs[kBlockRows + 1];  // xs[kBlockRows] == 0: target of inactive register slots
     const Chunk c = blocks[blockIdx.x];
     if (chunk_skip(c, st, flag)) return;
     const int t = threadIdx.x;
@@ -348,6 +401,7 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
         }
         return v;
     };
+    if (t == 0) xs[kBlockRows] = T(0);
     const int len = mine ? S.rlen[row] : 0;
     const int base = mine ? sell_base(S, row) : 0;
     T s = mine ? r[row] : T(0);
@@ -355,7 +409,7 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
     T lv[kBgsRegEntries];
 #pragma unroll
     for (int k = 0; k < kBgsRegEntries; ++k) {
-        li[k] = -1;
+        li[k] = kBlockRows;  // the zero slot: q -= 0 * 0 leaves q unchanged bit for bit
         lv[k] = T(0);
         if (k < len) {
             const int e = base + (k << 5);
@@ -385,8 +439,7 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
         if (mycol == colour) {
             T q = s;
 #pragma unroll
-            for (int k = 0; k < kBgsRegEntries; ++k)
-                if (li[k] >= 0) q -= lv[k] * xs[li[k]];
+            for (int k = 0; k < kBgsRegEntries; ++k) q -= lv[k] * xs[li[k]];
             for (int k = kBgsRegEntries; k < len; ++k) {
                 const int e = base + (k << 5);
                 const int jl = S.col[e] - c.start;
@@ -399,23 +452,44 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
     if (mine) xo[row] = xs[t];
 }
 
-// Jacobi sweep xo = (r - offdiag*xi)/D (first: xi == 0).
-template <class T, bool FIRST>
+// Jacobi sweep xo = (r - offdiag*xi)/D.  MODE 0: plain; MODE 1: xi == 0 (first pre-sweep);
+// MODE 2: xi + xc[agg] (the coarse-grid correction, GAMG.cpp:437-438, fused in).
+template <class T, int MODE>
 __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
                                                                const T* __restrict__ val, const T* __restrict__ diag,
                                                                const T* __restrict__ r, const T* __restrict__ xi,
-                                                               T* __restrict__ xo, T omega, const SysState* st, int flag) {
+                                                               T* __restrict__ xo, T omega,
+                                                               const int32_t* __restrict__ agg,
+                                                               const T* __restrict__ xc, const SysState* st, int flag) {
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
-    if (FIRST) {
+    if (MODE == 1) {
         const T v = r[row] / diag[row];
         xo[row] = omega == T(1) ? v : omega * v;
         return;
     }
-    const T s = row_minus(S, val, xi, row, r[row]);
+    auto xv = [&](int j) -> T {
+        T v = xi[j];
+        if (MODE == 2) {
+            const int a = agg[j];
+            if (a >= 0) v += xc[a];
+        }
+        return v;
+    };
+    T s = r[row];
+    const int len = S.rlen[row], base = sell_base(S, row);
+    for (int k = 0; k < len; ++k) {
+        const int e = base + (k << 5);
+        s -= val[e] * xv(S.col[e]);
+    }
     const T v = s / diag[row];
-    xo[row] = omega == T(1) ? v : xi[row] + omega * (v - xi[row]);
+    if (omega == T(1)) {
+        xo[row] = v;
+    } else {
+        const T x0 = xv(row);
+        xo[row] = x0 + omega * (v - x0);
+    }
 }
 
 // res = r - A x  (GAMG.cpp:387-401: diagonal first, then the faces in order)

@@ -2,11 +2,16 @@
 // fused with their global reductions, FP64 defect correction around an FP32 inner solve.
 // Scalar recurrences (alpha, beta, omega, convergence) are evaluated on the device by the
 // CTA that completes a system's reduction, so an iteration needs no host round trip.
+//
+// Level-0 chunks may hold up to kWideRows rows: every thread walks rows t, t+256, ... of its
+// chunk and accumulates into a BlockSum (compensated, or exact in reproducible mode).
 #pragma once
 
 #include "kernels.cuh"
 
 namespace vlm {
+
+#define VLM_ROWS(c) for (int row = (c).start + (int)threadIdx.x; row < (c).start + (c).count; row += kRowsPerCta)
 
 // converged() of LinearSolver.cpp:114-117
 __device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, double finalRes, double initRes) {
@@ -20,10 +25,11 @@ template <class T, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_sum_x(const Chunk* __restrict__ ch, const T* __restrict__ x, RedCtx R,
                                                        SysState* st) {
     const Chunk c = ch[blockIdx.x];
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) v[0].hi = (double)x[c.start + threadIdx.x];
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) acc.add(0, (double)x[row]);
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) st[c.sys].s0 = out[0];
+    if (acc.finish(c, R, out)) st[c.sys].s0 = out[0];
 }
 
 // wA = A x, pA = A x̄, r = b - wA; normFactor = Σ|wA-pA|+|b-pA| + 1e-20; residualSum = Σ|r|
@@ -38,9 +44,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __re
                                                                RedCtx R, SysState* st, const DevCtrl* __restrict__ ctrlp) {
     const Chunk c = ch[blockIdx.x];
     const double xRef = st[c.sys].s0 / (double)nCells[c.sys];
-    DD v[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<2, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const double wA = row_plus(S, val, x, row, diag[row] * x[row]);
         // A x̄ with the same entry order as amul on a constant vector
         const int len = S.rlen[row], base = sell_base(S, row);
@@ -50,12 +56,12 @@ __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __re
         r[row] = rr;
         if (r32) r32[row] = (float)rr;
         if (perm[row] >= 0) {
-            v[0].hi = fabs(wA - pA) + fabs(b[row] - pA);
-            v[1].hi = fabs(rr);
+            acc.add(0, fabs(wA - pA) + fabs(b[row] - pA));
+            acc.add(1, fabs(rr));
         }
     }
     double out[2];
-    if (reduce_to_system<2, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.normFactor = out[0] + 1e-20;
         s.residualSum = out[1];
@@ -85,9 +91,8 @@ __global__ void __launch_bounds__(kRowsPerCta) k_precond_diag(const Chunk* __res
                                                               const T* __restrict__ r, T* __restrict__ w,
                                                               const SysState* st, int flag) {
     const Chunk c = ch[blockIdx.x];
-    if (sys_idle(st[c.sys], flag) || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    w[row] = rD[row] * r[row];
+    if (sys_idle(st[c.sys], flag)) return;
+    VLM_ROWS(c) w[row] = rD[row] * r[row];
 }
 
 // rD = 1/diag (LinearSolver.cpp:66,78); padding rows: 0
@@ -105,13 +110,11 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
                                                             const T* __restrict__ r, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
-        v[0].hi = (double)w[row] * (double)r[row];
-    }
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) acc.add(0, (double)w[row] * (double)r[row]);
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
         s.wArAold = s.wArA;
@@ -126,13 +129,14 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__
                                                        T* __restrict__ p, const SysState* st) {
     const Chunk c = ch[blockIdx.x];
     const SysState& s = st[c.sys];
-    if (sys_idle(s, FLAG) || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
+    if (sys_idle(s, FLAG)) return;
     const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
-    if (it == 0)
-        p[row] = w[row];
-    else
-        p[row] = w[row] + (T)s.beta * p[row];
+    const T beta = (T)s.beta;
+    if (it == 0) {
+        VLM_ROWS(c) p[row] = w[row];
+    } else {
+        VLM_ROWS(c) p[row] = w[row] + beta * p[row];
+    }
 }
 
 // Ap = A p ; wApA = Σ Ap·p ; alpha = wArA / wApA (break when |wApA| < VSMALL)
@@ -142,15 +146,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restric
                                                           T* __restrict__ Ap, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const T y = row_plus(S, val, p, row, diag[row] * p[row]);
         Ap[row] = y;
-        v[0].hi = (double)y * (double)p[row];
+        acc.add(0, (double)y * (double)p[row]);
     }
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         if (fabs(out[0]) < kVSMALL) {
             if (FLAG == kFlagDone) {
@@ -174,16 +178,16 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
     const T alpha = (T)st[c.sys].alpha;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         x[row] += alpha * p[row];
         const T rr = r[row] - alpha * Ap[row];
         r[row] = rr;
-        v[0].hi = fabs((double)rr);
+        acc.add(0, fabs((double)rr));
     }
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         if (FLAG == kFlagDone) {
             s.finalResidual = out[0] / s.normFactor;
@@ -191,7 +195,8 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
             if (!isfinite(s.finalResidual)) {
                 s.status = VLM_ERR_NONFINITE;
                 s.done = 1;
-            } else if (s.iterations >= ctrlp->maxIter || dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+            } else if (s.iterations >= ctrlp->maxIter ||
+                       dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
                 s.done = 1;
             }
         } else {
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
 }
 
 // ------------------------------------------------------------------ mixed precision outer loop
-// start of an inner solve: e = 0 is done by a memset; reset the inner recurrences.
+// start of an inner solve: e = 0 is done by a zero kernel; reset the inner recurrences.
 __global__ void k_inner_begin(int nsys, SysState* st) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
@@ -226,9 +231,8 @@ __global__ void k_inner_begin(int nsys, SysState* st) {
 __global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                                const float* __restrict__ e, const SysState* st) {
     const Chunk c = ch[blockIdx.x];
-    if (st[c.sys].done || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    x[row] += (double)e[row];
+    if (st[c.sys].done) return;
+    VLM_ROWS(c) x[row] += (double)e[row];
 }
 
 // FP64 defect: r = b - A x (exact FP64 matrix), r32 = (float) r, finalResidual = Σ|r| / nf
@@ -241,17 +245,17 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
                                                                 const DevCtrl* __restrict__ ctrlp) {
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, false> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const double wA = row_plus(S, val, x, row, diag[row] * x[row]);
         const double rr = b[row] - wA;
         r[row] = rr;
         r32[row] = (float)rr;
-        v[0].hi = fabs(rr);
+        acc.add(0, fabs(rr));
     }
     double out[1];
-    if (reduce_to_system<1>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.finalResidual = out[0] / s.normFactor;
         s.innerInit = out[0];
@@ -273,13 +277,11 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restric
                                                           const double* __restrict__ r, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
-        v[0].hi = r0[row] * r[row];
-    }
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) acc.add(0, r0[row] * r[row]);
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.rhoOld = s.rho;
         s.rho = out[0];
@@ -298,12 +300,13 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_p(const Chunk* __restrict_
                                                         const SysState* st) {
     const Chunk c = ch[blockIdx.x];
     const SysState& s = st[c.sys];
-    if (s.done || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    if (s.iterations == 0)
-        p[row] = r[row];
-    else
-        p[row] = r[row] + s.beta * (p[row] - s.omega * Ay[row]);
+    if (s.done) return;
+    if (s.iterations == 0) {
+        VLM_ROWS(c) p[row] = r[row];
+    } else {
+        const double beta = s.beta, omega = s.omega;
+        VLM_ROWS(c) p[row] = r[row] + beta * (p[row] - omega * Ay[row]);
+    }
 }
 
 // Ay = A y ; alpha = rho / Σ r0·Ay (break when < VSMALL)
@@ -315,15 +318,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
                                                                  const double* __restrict__ r0, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const double a = row_plus(S, val, y, row, diag[row] * y[row]);
         Ay[row] = a;
-        v[0].hi = r0[row] * a;
+        acc.add(0, r0[row] * a);
     }
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         if (fabs(out[0]) < kVSMALL)
             s.done = 1;
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
     }
 }
 
-// s = r - alpha Ay ; iterations++ ; finalResidual = Σ|s|/nf ; converged -> early exit flag (s0 = 1)
+// s = r - alpha Ay ; iterations++ ; finalResidual = Σ|s|/nf ; converged -> early exit flag (s1 = 1)
 template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ sv, RedCtx R,
@@ -340,15 +343,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict_
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const double s = r[row] - alpha * Ay[row];
         sv[row] = s;
-        v[0].hi = fabs(s);
+        acc.add(0, fabs(s));
     }
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.iterations += 1;
         s.finalResidual = out[0] / s.normFactor;
@@ -368,10 +371,8 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_early(const Chunk* __restr
     const Chunk c = ch[blockIdx.x];
     SysState& s = st[c.sys];
     if (s.done || s.s1 == 0.0) return;
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
-        x[row] += s.alpha * y[row];
-    }
+    const double alpha = s.alpha;
+    VLM_ROWS(c) x[row] += alpha * y[row];
 }
 
 // closes the early exit (separate launch so every CTA above saw s1 before done is set)
@@ -392,16 +393,16 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __
                                                                  const double* __restrict__ sv, RedCtx R, SysState* st) {
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
-    DD v[2] = {DD{0.0, 0.0}, DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<2, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         const double a = row_plus(S, val, z, row, diag[row] * z[row]);
         t[row] = a;
-        v[0].hi = a * a;
-        v[1].hi = a * sv[row];
+        acc.add(0, a * a);
+        acc.add(1, a * sv[row]);
     }
     double out[2];
-    if (reduce_to_system<2, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.omega = out[0] > kVSMALL ? out[1] / out[0] : 0.0;
     }
@@ -417,22 +418,23 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha, omega = st[c.sys].omega;
-    DD v[1] = {DD{0.0, 0.0}};
-    if ((int)threadIdx.x < c.count) {
-        const int row = c.start + threadIdx.x;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    VLM_ROWS(c) {
         x[row] += alpha * y[row] + omega * z[row];
         const double rr = sv[row] - omega * t[row];
         r[row] = rr;
-        v[0].hi = fabs(rr);
+        acc.add(0, fabs(rr));
     }
     double out[1];
-    if (reduce_to_system<1, EXACT>(v, c, R, out)) {
+    if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
         s.finalResidual = out[0] / s.normFactor;
         if (!isfinite(s.finalResidual)) {
             s.status = VLM_ERR_NONFINITE;
             s.done = 1;
-        } else if (s.iterations >= ctrlp->maxIter || dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
+        } else if (s.iterations >= ctrlp->maxIter ||
+                   dev_converged(*ctrlp, s.iterations, s.finalResidual, s.initialResidual)) {
             s.done = 1;
         }
     }
@@ -443,17 +445,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_amul(const Chunk* __restrict__ 
                                                       const double* __restrict__ diag, const double* __restrict__ x,
                                                       double* __restrict__ y) {
     const Chunk c = ch[blockIdx.x];
-    if ((int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    y[row] = row_plus(S, val, x, row, diag[row] * x[row]);
-}
-
-// iteration-loop predicate: any system still running
-__global__ void k_any_active(int nsys, const SysState* st, int flag, int* out) {
-    int a = 0;
-    for (int i = threadIdx.x; i < nsys; i += blockDim.x) a |= sys_idle(st[i], flag) ? 0 : 1;
-    a = __syncthreads_or(a);
-    if (threadIdx.x == 0) *out = a;
+    VLM_ROWS(c) y[row] = row_plus(S, val, x, row, diag[row] * x[row]);
 }
 
 }  // namespace vlm

@@ -33,11 +33,11 @@ std::vector<int> blockColour(const HLevel& L, int s0, int s1, int* nColours) {
     return colour;
 }
 
-void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slot) {
-    for (int s = 0; s < len; s += kRowsPerCta) {
+void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slot, int width = kRowsPerCta) {
+    for (int s = 0; s < len; s += width) {
         Chunk c;
         c.start = start + s;
-        c.count = std::min(kRowsPerCta, len - s);
+        c.count = std::min(width, len - s);
         c.sys = sys;
         c.slot = slot ? (*slot)++ : 0;
         out.push_back(c);
@@ -182,7 +182,7 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
         for (int b = 0; b < present; ++b) {
             const int s0 = LP.sysRow[b], len = LP.sysRow[b + 1] - LP.sysRow[b];
             if (k == 0) P.sysSlotBegin.push_back(slot);
-            appendChunks(LP.all, s0, len, b, &slot);
+            appendChunks(LP.all, s0, len, b, &slot, k == 0 ? kWideRows : kRowsPerCta);
             if (k == 0) P.sysSlotEnd.push_back(slot);
             if (b < active) appendChunks(LP.active, s0, len, b, nullptr);
         }

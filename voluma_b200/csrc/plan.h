@@ -42,7 +42,7 @@ struct LevelPlan {
     std::vector<int32_t> slPtr, rlen, col, src;  // src >= 0: upper[src]; src < 0: lower[~src]
     std::vector<std::vector<Chunk>> fwd, rev;     // colour step t chunks (forward / reversed)
     std::vector<Chunk> active;                    // all rows of smoothing systems
-    std::vector<Chunk> all;                       // all rows (sys/slot set)
+    std::vector<Chunk> all;                       // all rows (sys/slot set); level 0: kWideRows per chunk
     std::vector<Chunk> blocks;                    // block-hybrid GS blocks (count <= kBlockRows, slot = colours)
     std::vector<int8_t> rowColour;                // block-local colour of each row (block levels)
     std::vector<int32_t> natural;                 // row -> natural index in its system (-1 padding)

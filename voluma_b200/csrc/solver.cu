@@ -31,6 +31,13 @@ SolverKind parseSolver(const char* s) {
     throw Error(VLM_ERR_UNSUPPORTED, std::string("unknown linear solver ") + s);
 }
 
+SmootherKind parseSmoother(const char* s) {
+    if (s[0] == 0 || eq(s, "mcgs-jacobi")) return SmootherKind::MCGSJacobi;  // default: fastest measured
+    if (eq(s, "mcgs")) return SmootherKind::MCGS;
+    if (eq(s, "jacobi")) return SmootherKind::Jacobi;
+    throw Error(VLM_ERR_BAD_ARG, std::string("unknown smoother ") + s);
+}
+
 PrecondKind parsePrecond(const char* s) {
     if (eq(s, "none")) return PrecondKind::None;
     if (eq(s, "diagonal")) return PrecondKind::Diagonal;
@@ -302,12 +309,27 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
     const T* val = LV<T>::val(D);
     const T* diag = LV<T>::diag(D);
     const SysState* st = st_.get();
-    if (sm == SmootherKind::MCGS && D.blockGS) {
+    T* x2 = LV<T>::x2(D);
+    const int32_t* agg = D.agg.get();
+    const T* xc = k + 1 < int(L_.size()) ? LV<T>::x(L_[k + 1]) : nullptr;
+    const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
+    if (jacobiHere) {
+        // Jacobi; pre: from zero, post: prolongation fused into the first sweep
+        const T om = T(jacobiOmega_);
+        if (pre) {
+            VLM_LAUNCH((k_smooth_jacobi<T, 1>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r,
+                       (const T*)nullptr, x2, om, agg, xc, st, flag);
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+                       om, agg, xc, st, flag);
+        } else {
+            VLM_LAUNCH((k_smooth_jacobi<T, 2>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x, x2,
+                       om, agg, xc, st, flag);
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+                       om, agg, xc, st, flag);
+        }
+    } else if (D.blockGS) {
         // block-hybrid GS; pre: from zero, post: prolongation fused into the first sweep
-        T* x2 = LV<T>::x2(D);
         const int8_t* rc = D.rowColour.get();
-        const int32_t* agg = D.agg.get();
-        const T* xc = k + 1 < int(L_.size()) ? LV<T>::x(L_[k + 1]) : nullptr;
         if (pre) {
             VLM_LAUNCH((k_smooth_bgs<T, 1, true>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x, x2,
                        rc, agg, xc, st, flag);
@@ -319,27 +341,14 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
             VLM_LAUNCH((k_smooth_bgs<T, 0, false>), D.blocks.n, kBlockRows, s, D.ch(D.blocks), S, val, diag, r, x2,
                        x, rc, agg, xc, st, flag);
         }
-    } else if (sm == SmootherKind::MCGS) {
+    } else {
+        // global multicolour GS: forward colours pre-smoothing, reversed colours post-smoothing
         if (pre) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
                 const ChunkList& l = pre ? D.fwd[t] : D.rev[t];
                 VLM_LAUNCH(k_smooth_gs<T>, l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, st, flag);
             }
-    } else {
-        T* x2 = LV<T>::x2(D);
-        const T om = T(jacobiOmega_);
-        if (pre) {
-            VLM_LAUNCH((k_smooth_jacobi<T, true>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r,
-                       (const T*)nullptr, x2, om, st, flag);
-            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
-                       om, st, flag);
-        } else {
-            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x, x2,
-                       om, st, flag);
-            VLM_LAUNCH((k_smooth_jacobi<T, false>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
-                       om, st, flag);
-        }
     }
 }
 
@@ -370,7 +379,8 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag) {
     }
     for (int k = nL - 2; k >= 0; --k) {
         DevLevel& D = L_[k];
-        if (!(sm == SmootherKind::MCGS && D.blockGS))  // block GS fuses the prolongation into its first sweep
+        const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
+        if (!jacobiHere && !D.blockGS)  // block GS and Jacobi fuse the prolongation into their first sweep
             VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st,
                        flag);
         recordSmooth<T>(k, rr(k), xx(k), sm, false, flag);
@@ -650,10 +660,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     if (pk == PrecondKind::DIC || pk == PrecondKind::DILU)
         throw Error(VLM_ERR_UNSUPPORTED, std::string("preconditioner ") + ctrl.preconditioner +
                                              " is not available on the device");
-    const SmootherKind sm = (ctrl.smoother[0] == 0 || eq(ctrl.smoother, "mcgs")) ? SmootherKind::MCGS
-                            : eq(ctrl.smoother, "jacobi")
-                                ? SmootherKind::Jacobi
-                                : throw Error(VLM_ERR_BAD_ARG, std::string("unknown smoother ") + ctrl.smoother);
+    const SmootherKind sm = parseSmoother(ctrl.smoother);
     Precision prec = Precision::FP64;
     if (eq(ctrl.precision, "mixed"))
         prec = Precision::MixedPrecond;

@@ -40,7 +40,9 @@ struct DevLevel {
 
 enum class SolverKind { PCG, PBiCGStab, Jacobi, GaussSeidel, SymGaussSeidel };
 enum class PrecondKind { None, Diagonal, GAMG, DIC, DILU };
-enum class SmootherKind { MCGS, Jacobi };
+// MCGS: level-0 multicolour GS (block-hybrid GS where it needs many colours) + block-hybrid GS on
+// coarser levels; MCGSJacobi: the same level 0 + Jacobi on coarser levels; Jacobi: every level.
+enum class SmootherKind { MCGS, MCGSJacobi, Jacobi };
 // FP64; FP64 Krylov recurrence with an FP32 GAMG V-cycle; FP32 inner PCG in FP64 defect correction
 enum class Precision { FP64, MixedPrecond, MixedDC };
 
@@ -142,5 +144,6 @@ double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n);
 
 SolverKind parseSolver(const char* s);
 PrecondKind parsePrecond(const char* s);
+SmootherKind parseSmoother(const char* s);
 
 }  // namespace vlm
