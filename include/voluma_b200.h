@@ -19,6 +19,10 @@
  *   vlm_laplacian         <- fvm::laplacian(gamma, psi, nonOrthCorr) (src/fvm/discretization/Fvm.h:141-182)
  *   vlm_grad              <- fvc::grad (Gauss linear / leastSquares) (src/fvm/discretization/Fvc.h:209-291)
  *   vlm_exact_sum         <- par::ExactSum::add/value            (src/fvm/parallel/Comm.h:42-93, Comm.cpp:107-164)
+ *   vlm_div               <- fvc::div(mesh, F)                   (src/fvm/discretization/Fvc.h:294-304)
+ *   vlm_pressure_solve    <- the pressure-corrector loop          (src/fvm/solvers/IncompressibleFlow.cpp:322-341)
+ *                            = fvm::laplacian + FvMatrix::operator-= + setReference + FvMatrix::solve + flux
+ *                            (Fvm.h:141-182, FvMatrix.h:93-97,134-175,210-222)
  */
 #ifndef VOLUMA_B200_H
 #define VOLUMA_B200_H
@@ -152,6 +156,28 @@ vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, cons
 /* fvc::grad of a scalar field, out[3*n_cells]. */
 vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh* mesh, const double* psi, const int32_t* bc_type,
                     const double* bc_values, int32_t scheme, double* out);
+
+/* fvc::div of a face flux (src/fvm/discretization/Fvc.h:294-304): out[n_cells] per unit volume. */
+vlm_status vlm_div(vlm_ctx* ctx, vlm_mesh* mesh, const double* face_flux, double* out);
+
+/* The pressure equation of the PISO/SIMPLE corrector (src/fvm/solvers/IncompressibleFlow.cpp:322-341,
+ * projectDivergenceFree :62-71): for each of the n_non_orth+1 passes
+ *     pEqn = fvm::laplacian(gamma, p) [non-orthogonal correction from grad(p)];  pEqn -= div_phi;
+ *     pEqn.setReference(ref_cell, ref_value) (ref_cell < 0: none);  pEqn.solve(ctrl | final_ctrl);
+ * with the GAMG-PCG solve on the device, p's boundary values corrected after each solve, and the
+ * flux of the last pass (pEqn.flux(), n_faces) written to `flux` when not NULL.
+ * gamma: n_faces face diffusivity (rAUf); div_phi: n_cells, per unit volume; p: n_cells in/out;
+ * perf: n_non_orth+1 entries.  Host pointers. */
+vlm_status vlm_pressure_solve(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, const double* div_phi, double* p,
+                              const int32_t* bc_type, const double* bc_values, int32_t ref_cell, double ref_value,
+                              int32_t n_non_orth, int32_t grad_scheme, const vlm_solver_ctrl* ctrl,
+                              const vlm_solver_ctrl* final_ctrl, vlm_solver_perf* perf, double* flux);
+/* Same with device pointers, ordered on vlm_ctx_stream(ctx). */
+vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, const double* div_phi,
+                                     double* p, const int32_t* bc_type, const double* bc_values, int32_t ref_cell,
+                                     double ref_value, int32_t n_non_orth, int32_t grad_scheme,
+                                     const vlm_solver_ctrl* ctrl, const vlm_solver_ctrl* final_ctrl,
+                                     vlm_solver_perf* perf, double* flux);
 
 /* Kernel launches executed on this mesh so far and its device memory footprint in bytes. */
 vlm_status vlm_mesh_stats(vlm_mesh* mesh, int64_t* launches, int64_t* device_bytes);

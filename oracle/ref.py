@@ -185,14 +185,21 @@ class RefMesh:
         return g
 
     def pressure_solve(self, gamma, div_phi, p0, ref_cell=0, n_non_orth=0, grad_scheme=1, solver="PCG",
-                       precond="GAMG", tol=0.0, rel_tol=1e-8, max_iter=1000):
+                       precond="GAMG", tol=0.0, rel_tol=1e-8, max_iter=1000, reproducible=False):
+        """laplacian + (-= divPhi) + setReference + solve, n_non_orth+1 times, with zeroGradient walls
+        (IncompressibleFlow.cpp:62-71). Returns (p, flux of the last pass, perf rows)."""
+        L = lib()
         p = np.ascontiguousarray(p0, np.float64).copy()
         flux = np.zeros(self.n_faces)
         perf = np.zeros(6 * (n_non_orth + 1))
-        _check(lib().ref_pressure_solve(self._h, _p(np.ascontiguousarray(gamma, np.float64)),
+        L.ref_set_reproducible(1 if reproducible else 0)
+        try:
+            _check(L.ref_pressure_solve(self._h, _p(np.ascontiguousarray(gamma, np.float64)),
                                         _p(np.ascontiguousarray(div_phi, np.float64)), int(ref_cell),
                                         int(n_non_orth), int(grad_scheme), solver.encode(), precond.encode(),
                                         tol, rel_tol, max_iter, _p(p), _p(flux), _p(perf)))
+        finally:
+            L.ref_set_reproducible(0)
         return p, flux, perf.reshape(-1, 6)
 
 

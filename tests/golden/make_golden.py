@@ -84,6 +84,28 @@ def make(name, spec):
     for k, L in enumerate(levels):
         for f in ("l", "u", "weight", "agg", "faceMap", "faceFlip"):
             out[f"lev{k}_{f}"] = L[f]
+    # ---- assembly: fvm::laplacian with its non-orthogonal correction, fvc::grad, pressure loop
+    nP = R.n_patches
+    gamma = 0.5 + rng.random(R.n_faces)
+    psi = rng.standard_normal(nC)
+    bct = np.zeros(max(nP, 1), np.int32)
+    if nP:
+        bct[0] = 1  # fixedValue on the first patch, zeroGradient elsewhere
+    bcv = rng.standard_normal(R.n_faces - nI)
+    out.update(lap_gamma=gamma, lap_psi=psi, lap_bctype=bct, lap_bcvalues=bcv)
+    for gs in (0, 1):
+        L = R.laplacian(gamma, psi, bct[:nP] if nP else bct, bcv, non_orth_corr=True, grad_scheme=gs)
+        for k2, v2 in L.items():
+            out[f"lap{gs}_{k2}"] = np.asarray(v2)
+        out[f"grad{gs}"] = R.grad(psi, bct[:nP] if nP else bct, bcv, scheme=gs)
+    divphi = rng.standard_normal(nC)
+    divphi -= (divphi * out["V"]).sum() / out["V"].sum()
+    out["ps_gamma"] = gamma
+    out["ps_divphi"] = divphi
+    p_r, flux_r, perf_r = R.pressure_solve(gamma, divphi, np.zeros(nC), ref_cell=0, n_non_orth=2, grad_scheme=1,
+                                           solver="PCG", precond="diagonal", rel_tol=1e-8, max_iter=3000,
+                                           reproducible=True)
+    out.update(ps_p=p_r, ps_flux=flux_r, ps_perf=perf_r)
     out["exact_sum_b"] = np.array(ref.exact_sum(b))
     spread = rng.standard_normal(4096) * np.exp(rng.uniform(-40, 40, 4096))
     out["exact_spread"] = spread

@@ -25,6 +25,8 @@ _meshes = {}
 def device_mesh(name):
     if name not in _meshes:
         g = load_golden(name)
+        g["patch_start"], g["patch_size"] = g["patchStart"], g["patchSize"]
+        g["two_d"], g["empty_dir"] = int(g["sizes"][4]), int(g["sizes"][5])
         _meshes[name] = (g, vb.Mesh.from_arrays(g))
     return _meshes[name]
 

@@ -291,6 +291,66 @@ def solve_ldu_device(mesh: Mesh, diag_ptr, upper_ptr, lower_ptr, b_ptr, x_ptr, c
     return SolverPerformance.from_c(p)
 
 
+def _bc(mesh: Mesh, bc_type, bc_values):
+    nP = len(mesh.geometry.get("patch_start", []))
+    t = np.zeros(max(nP, 1), np.int32)
+    if bc_type is not None:
+        t[:len(bc_type)] = np.asarray(bc_type, np.int32)
+    v = None if bc_values is None else _f64(bc_values)
+    return t, v
+
+
+def laplacian(mesh: Mesh, gamma, psi, bc_type=None, bc_values=None, non_orth_corr=True, grad_scheme=0):
+    """fvm::laplacian(gamma, psi) (Fvm.h:141-182) of a scalar field: dict of diag, upper, source,
+    internalCoeffs, boundarySource, ffc, hasFfc.  bc_type per patch: 0 zeroGradient, 1 fixedValue."""
+    nC, nI, nF = mesh.n_cells, mesh.n_internal_faces, mesh.n_faces
+    out = dict(diag=np.zeros(nC), upper=np.zeros(nI), source=np.zeros(nC), internalCoeffs=np.zeros(nF - nI),
+               boundarySource=np.zeros(nF - nI), ffc=np.zeros(nF))
+    t, v = _bc(mesh, bc_type, bc_values)
+    has = C.c_int32()
+    check(load().vlm_laplacian(mesh.ctx.handle, mesh.handle, _ptr(_f64(gamma)), _ptr(_f64(psi)), _ptr(t), _ptr(v),
+                               int(non_orth_corr), int(grad_scheme), _ptr(out["diag"]), _ptr(out["upper"]),
+                               _ptr(out["source"]), _ptr(out["internalCoeffs"]), _ptr(out["boundarySource"]),
+                               _ptr(out["ffc"]), C.byref(has)), mesh.ctx.handle)
+    out["hasFfc"] = bool(has.value)
+    return out
+
+
+def grad(mesh: Mesh, psi, bc_type=None, bc_values=None, scheme=0):
+    """fvc::grad of a scalar (Fvc.h:209-291): (n_cells, 3); scheme 0 Gauss linear, 1 least squares."""
+    g = np.zeros((mesh.n_cells, 3))
+    t, v = _bc(mesh, bc_type, bc_values)
+    check(load().vlm_grad(mesh.ctx.handle, mesh.handle, _ptr(_f64(psi)), _ptr(t), _ptr(v), int(scheme), _ptr(g)),
+          mesh.ctx.handle)
+    return g
+
+
+def div(mesh: Mesh, face_flux):
+    """fvc::div (Fvc.h:294-304), per unit volume."""
+    out = np.zeros(mesh.n_cells)
+    check(load().vlm_div(mesh.ctx.handle, mesh.handle, _ptr(_f64(face_flux)), _ptr(out)), mesh.ctx.handle)
+    return out
+
+
+def pressure_solve(mesh: Mesh, gamma, div_phi, p, ctrl: SolverControls, final_ctrl: SolverControls | None = None,
+                   bc_type=None, bc_values=None, ref_cell=0, ref_value=0.0, n_non_orth=0, grad_scheme=1,
+                   want_flux=True):
+    """The pressure-corrector loop (IncompressibleFlow.cpp:322-341) on the device; p is solved in
+    place.  Returns (list of SolverPerformance per pass, face flux of the last pass or None)."""
+    if not (isinstance(p, np.ndarray) and p.dtype == np.float64 and p.flags.c_contiguous):
+        raise TypeError("p must be a C-contiguous float64 array (solved in place)")
+    t, v = _bc(mesh, bc_type, bc_values)
+    perf = (_ffi.SolverPerf * (n_non_orth + 1))()
+    flux = np.zeros(mesh.n_faces) if want_flux else None
+    c = ctrl.to_c()
+    cf = (final_ctrl or ctrl).to_c()
+    check(load().vlm_pressure_solve(mesh.ctx.handle, mesh.handle, _ptr(_f64(gamma)), _ptr(_f64(div_phi)), _ptr(p),
+                                    _ptr(t), _ptr(v), int(-1 if ref_cell is None else ref_cell), float(ref_value),
+                                    int(n_non_orth), int(grad_scheme), C.byref(c), C.byref(cf), perf, _ptr(flux)),
+          mesh.ctx.handle)
+    return [SolverPerformance.from_c(q) for q in perf], flux
+
+
 def exact_sum(values, ctx: Context | None = None) -> float:
     """Order-independent exact sum on the device (par::ExactSum semantics, Comm.h:42-93)."""
     ctx = ctx or default_context()

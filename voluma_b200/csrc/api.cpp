@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "assembly.h"
 #include "solver.h"
 #include "voluma_b200.h"
 
@@ -28,9 +29,19 @@ struct vlm_mesh {
     std::vector<int32_t> own, nei;
     std::vector<double> magSf, ndc;
     std::unique_ptr<vlm::DeviceBatch> batch;
+    std::unique_ptr<vlm::DeviceGeom> geom;  // assembly geometry (when the descriptor carries it)
     // staging for the host-pointer entry points
     vlm::DBuf<double> diag, upper, lower, b, x;
+    // pressure-equation work arrays
+    vlm::DBuf<double> gamma, su, p, pB, pdiag, pupper, psource, ic, bs, ffc, fd, fb, flux, bcv, grad;
 };
+
+namespace {
+vlm::DeviceGeom& geomOf(vlm_mesh* m) {
+    VLM_REQUIRE(m->geom, VLM_ERR_BAD_ARG, "the mesh was registered without geometry (V, Sf, d, w, corrVecs)");
+    return *m->geom;
+}
+}  // namespace
 
 namespace {
 
@@ -163,6 +174,11 @@ vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* d, int32_t merge
         t.ndc = m->ndc.data();
         m->batch = std::make_unique<vlm::DeviceBatch>(std::vector<vlm::SysTopo>{t}, mergeLevels > 0 ? mergeLevels : 2,
                                                       ctx->stream);
+        if (d->V && d->Sf && d->d && d->w && d->corrVecs)
+            m->geom = std::make_unique<vlm::DeviceGeom>(d->n_cells, d->n_internal_faces, d->n_faces, d->owner,
+                                                        d->neighbour, d->magSf, d->ndc, d->V, d->Sf, d->d, d->w,
+                                                        d->corrVecs, d->two_d, d->empty_dir, d->n_patches,
+                                                        d->patch_start, d->patch_size, ctx->stream);
         ctx->refs++;
         *out = m.release();
     });
@@ -329,13 +345,166 @@ vlm_status vlm_topology_destroy(vlm_topology* t) {
     return VLM_OK;
 }
 
-vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh*, const double*, const double*, const int32_t*, const double*,
-                         int32_t, int32_t, double*, double*, double*, double*, double*, double*, int32_t*) {
-    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_laplacian: not built yet");
+namespace {
+
+// Host boundary values -> device (n_boundary doubles), NULL stays NULL.
+const double* stageBC(vlm_mesh* m, const double* bcValues, cudaStream_t s) {
+    const int nB = m->nFaces - m->nInternal;
+    if (!bcValues || nB == 0) return nullptr;
+    m->bcv.upload(bcValues, size_t(nB), s);
+    return m->bcv.get();
 }
 
-vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh*, const double*, const int32_t*, const double*, int32_t, double*) {
-    return fail(ctx, VLM_ERR_UNSUPPORTED, "vlm_grad: not built yet");
+void ensureWork(vlm_mesh* m) {
+    const size_t nC = size_t(m->nCells), nF = size_t(m->nFaces), nI = size_t(std::max(m->nInternal, 1)),
+                 nB = size_t(std::max(m->nFaces - m->nInternal, 1));
+    if (m->pdiag.size() == nC) return;
+    m->gamma.resize(nF);
+    m->su.resize(nC);
+    m->p.resize(nC);
+    m->pB.resize(nB);
+    m->pdiag.resize(nC);
+    m->pupper.resize(nI);
+    m->psource.resize(nC);
+    m->ic.resize(nB);
+    m->bs.resize(nB);
+    m->ffc.resize(nF);
+    m->fd.resize(nC);
+    m->fb.resize(nC);
+    m->flux.resize(nF);
+    m->grad.resize(3 * nC);
+}
+
+// Device-pointer pressure corrector loop; bcv: device boundary values or null.
+void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double* p, const int32_t* bcType,
+                  const double* bcv, int refCell, double refValue, int nNonOrth, int gradScheme,
+                  const vlm_solver_ctrl& ctrl, const vlm_solver_ctrl& finalCtrl, vlm_solver_perf* perf, double* flux) {
+    vlm::DeviceGeom& G = geomOf(m);
+    cudaStream_t s = m->ctx->stream;
+    ensureWork(m);
+    vlm::ScalarBC bc;
+    bc.type = bcType;
+    bc.value = bcv;
+    for (int no = 0; no <= nNonOrth; ++no) {
+        const bool last = no == nNonOrth;
+        G.correctBoundary(p, bc, m->pB.get(), s);
+        bool hasFfc = false;
+        G.laplacian(gamma, p, m->pB.get(), bc, true, gradScheme, m->pdiag.get(), m->pupper.get(), m->psource.get(),
+                    m->ic.get(), m->bs.get(), m->ffc.get(), &hasFfc, s);
+        G.addVolumeSource(m->psource.get(), divPhi, s);
+        if (refCell >= 0) G.setReference(refCell, refValue, m->pdiag.get(), m->psource.get(), s);
+        G.fold(m->pdiag.get(), m->psource.get(), m->ic.get(), m->bs.get(), m->fd.get(), m->fb.get(), s);
+        std::vector<vlm_solver_perf> pf;
+        m->batch->solve(m->fd.get(), m->pupper.get(), m->pupper.get(), m->fb.get(), p, last ? finalCtrl : ctrl, pf);
+        if (perf) perf[no] = pf[0];
+        if (last && flux) G.flux(m->pupper.get(), p, m->ic.get(), m->bs.get(), hasFfc ? m->ffc.get() : nullptr, flux, s);
+    }
+    G.correctBoundary(p, bc, m->pB.get(), s);
+}
+
+}  // namespace
+
+vlm_status vlm_laplacian(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* psi, const int32_t* bcType,
+                         const double* bcValues, int32_t nonOrthCorr, int32_t gradScheme, double* diag, double* upper,
+                         double* source, double* ic, double* bs, double* ffc, int32_t* hasFfc) {
+    if (!ctx || !m || !gamma || !psi || !bcType || !diag || !upper || !source || !ic || !bs || !ffc)
+        return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        vlm::DeviceGeom& G = geomOf(m);
+        cudaStream_t s = ctx->stream;
+        ensureWork(m);
+        m->gamma.upload(gamma, size_t(m->nFaces), s);
+        m->p.upload(psi, size_t(m->nCells), s);
+        vlm::ScalarBC bc;
+        bc.type = bcType;
+        bc.value = stageBC(m, bcValues, s);
+        m->ffc.zero(s);
+        G.correctBoundary(m->p.get(), bc, m->pB.get(), s);
+        bool has = false;
+        G.laplacian(m->gamma.get(), m->p.get(), m->pB.get(), bc, nonOrthCorr != 0, gradScheme, m->pdiag.get(),
+                    m->pupper.get(), m->psource.get(), m->ic.get(), m->bs.get(), m->ffc.get(), &has, s);
+        const size_t nB = size_t(m->nFaces - m->nInternal);
+        VLM_CUDA(cudaMemcpyAsync(diag, m->pdiag.get(), sizeof(double) * m->nCells, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaMemcpyAsync(upper, m->pupper.get(), sizeof(double) * m->nInternal, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaMemcpyAsync(source, m->psource.get(), sizeof(double) * m->nCells, cudaMemcpyDeviceToHost, s));
+        if (nB) {
+            VLM_CUDA(cudaMemcpyAsync(ic, m->ic.get(), sizeof(double) * nB, cudaMemcpyDeviceToHost, s));
+            VLM_CUDA(cudaMemcpyAsync(bs, m->bs.get(), sizeof(double) * nB, cudaMemcpyDeviceToHost, s));
+        }
+        VLM_CUDA(cudaMemcpyAsync(ffc, m->ffc.get(), sizeof(double) * m->nFaces, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+        if (hasFfc) *hasFfc = has ? 1 : 0;
+    });
+}
+
+vlm_status vlm_grad(vlm_ctx* ctx, vlm_mesh* m, const double* psi, const int32_t* bcType, const double* bcValues,
+                    int32_t scheme, double* out) {
+    if (!ctx || !m || !psi || !bcType || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        vlm::DeviceGeom& G = geomOf(m);
+        cudaStream_t s = ctx->stream;
+        ensureWork(m);
+        m->p.upload(psi, size_t(m->nCells), s);
+        vlm::ScalarBC bc;
+        bc.type = bcType;
+        bc.value = stageBC(m, bcValues, s);
+        G.correctBoundary(m->p.get(), bc, m->pB.get(), s);
+        G.grad(m->p.get(), m->pB.get(), bc, scheme, m->grad.get(), s);
+        VLM_CUDA(cudaMemcpyAsync(out, m->grad.get(), sizeof(double) * 3 * m->nCells, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+vlm_status vlm_div(vlm_ctx* ctx, vlm_mesh* m, const double* F, double* out) {
+    if (!ctx || !m || !F || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        vlm::DeviceGeom& G = geomOf(m);
+        cudaStream_t s = ctx->stream;
+        ensureWork(m);
+        m->flux.upload(F, size_t(m->nFaces), s);
+        G.div(m->flux.get(), m->su.get(), s);
+        VLM_CUDA(cudaMemcpyAsync(out, m->su.get(), sizeof(double) * m->nCells, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
+                                     const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
+                                     int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
+                                     const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
+    if (!ctx || !m || !gamma || !divPhi || !p || !bcType || !ctrl || nNonOrth < 0)
+        return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        pressureLoop(m, gamma, divPhi, p, bcType, bcValues, refCell, refValue, nNonOrth, gradScheme, *ctrl,
+                     finalCtrl ? *finalCtrl : *ctrl, perf, flux);
+    });
+}
+
+vlm_status vlm_pressure_solve(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
+                              const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
+                              int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
+                              const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
+    if (!ctx || !m || !gamma || !divPhi || !p || !bcType || !ctrl || nNonOrth < 0)
+        return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        cudaStream_t s = ctx->stream;
+        ensureWork(m);
+        m->gamma.upload(gamma, size_t(m->nFaces), s);
+        m->su.upload(divPhi, size_t(m->nCells), s);
+        m->p.upload(p, size_t(m->nCells), s);
+        const double* bcv = stageBC(m, bcValues, s);
+        pressureLoop(m, m->gamma.get(), m->su.get(), m->p.get(), bcType, bcv, refCell, refValue, nNonOrth, gradScheme,
+                     *ctrl, finalCtrl ? *finalCtrl : *ctrl, perf, flux ? m->flux.get() : nullptr);
+        VLM_CUDA(cudaMemcpyAsync(p, m->p.get(), sizeof(double) * m->nCells, cudaMemcpyDeviceToHost, s));
+        if (flux)
+            VLM_CUDA(cudaMemcpyAsync(flux, m->flux.get(), sizeof(double) * m->nFaces, cudaMemcpyDeviceToHost, s));
+        VLM_CUDA(cudaStreamSynchronize(s));
+    });
 }
 
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out) {

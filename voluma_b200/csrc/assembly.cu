@@ -1,0 +1,424 @@
+// Finite-volume assembly of the pressure equation on the device.
+//
+// Every kernel is a gather: one thread per cell walks the cell's faces in ascending face order
+// (the order in which the reference's face loops update that cell), or one thread per face.
+// With -fmad=false the results equal the reference's face-loop scatters bit for bit; nothing
+// is accumulated with atomics.
+#include <cmath>
+
+#include "assembly.h"
+
+namespace vlm {
+
+namespace {
+
+inline int nblk(int n, int t = 256) { return (n + t - 1) / t; }
+
+struct V3 {
+    double x, y, z;
+};
+
+__device__ __forceinline__ V3 ld3(const double* soa, int n, int i) { return V3{soa[i], soa[n + i], soa[2 * n + i]}; }
+__device__ __forceinline__ double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Boundary constraint of the least-squares gradient (Fvc.h:267-287): value BCs use d and
+// phi_b - phi_P, gradient BCs n (n.d) and g_b (n.d) with n.d >= 0.05|d|.
+struct BFace {
+    V3 de;
+    bool value;
+};
+
+__device__ __forceinline__ BFace lsBoundary(const double* Sf, const double* magSf, const double* d, int nF, int f,
+                                            bool value) {
+    const V3 dd = ld3(d, nF, f);
+    if (value) return BFace{dd, true};
+    const double inv = 1.0 / magSf[f];
+    const V3 n{Sf[f] * inv, Sf[nF + f] * inv, Sf[2 * nF + f] * inv};
+    const double nd = fmax(dot3(n, dd), 0.05 * sqrt(dot3(dd, dd)));
+    return BFace{V3{n.x * nd, n.y * nd, n.z * nd}, false};
+}
+
+// ---------------------------------------------------------------- kernels
+// gs = gamma |S|; upper = gamma |S| ndc  (Fvm.h:150, :176)
+__global__ void k_face_gs(int nF, int nI, const double* __restrict__ gamma, const double* __restrict__ magSf,
+                          const double* __restrict__ ndc, double* __restrict__ gs, double* __restrict__ upper) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const double g = gamma[f] * magSf[f];
+    gs[f] = g;
+    if (f < nI) upper[f] = g * ndc[f];
+}
+
+// boundary coefficients of the laplacian (Fvm.h:171-180) for fixedValue / zeroGradient
+__global__ void k_lap_boundary(int nB, int nI, const double* __restrict__ gs, const double* __restrict__ ndc,
+                               const int32_t* __restrict__ bPatch, const int32_t* __restrict__ bcType,
+                               const double* __restrict__ bcValue, double* __restrict__ ic, double* __restrict__ bs) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB) return;
+    const int f = nI + b;
+    double gic = 0.0, gbc = 0.0;
+    if (bcType[bPatch[b]] == 1) {
+        gic = -ndc[f];
+        gbc = ndc[f] * (bcValue ? bcValue[b] : 0.0);
+    }
+    ic[b] = 0.0 + gs[f] * gic;
+    bs[b] = 0.0 - gs[f] * gbc;
+}
+
+// diag[c] = -Σ upper; source[c] = Σ ∓ffc (Fvm.h:149-168), cell faces in ascending order
+__global__ void k_lap_cells(int nC, int nI, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                            const double* __restrict__ upper, const double* __restrict__ ffc, double* __restrict__ diag,
+                            double* __restrict__ source) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double dg = 0.0, src = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = (int)(e & 0x7fffffffu);
+        if (f >= nI) continue;
+        dg -= upper[f];
+        if (ffc) {
+            if (e >> 31)
+                src += ffc[f];
+            else
+                src -= ffc[f];
+        }
+    }
+    diag[c] = dg;
+    source[c] = src;
+}
+
+// Gauss linear gradient (Fvc.h:216-225)
+__global__ void k_grad_gauss(int nC, int nI, int nF, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                             const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                             const double* __restrict__ w, const double* __restrict__ Sf, const double* __restrict__ V,
+                             const double* __restrict__ psi, const double* __restrict__ psiB, int twoD, int emptyDir,
+                             double* __restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = (int)(e & 0x7fffffffu);
+        double phif;
+        if (f < nI)
+            phif = w[f] * psi[own[f]] + (1.0 - w[f]) * psi[nei[f]];
+        else
+            phif = psiB[f - nI];
+        const double cx = Sf[f] * phif, cy = Sf[nF + f] * phif, cz = Sf[2 * nF + f] * phif;
+        if (e >> 31) {
+            gx -= cx;
+            gy -= cy;
+            gz -= cz;
+        } else {
+            gx += cx;
+            gy += cy;
+            gz += cz;
+        }
+    }
+    const double iv = 1.0 / V[c];
+    gx = gx * iv;
+    gy = gy * iv;
+    gz = gz * iv;
+    if (twoD) {  // finishGrad (Fvc.h:169-181)
+        if (emptyDir == 0) gx = 0.0;
+        if (emptyDir == 1) gy = 0.0;
+        if (emptyDir == 2) gz = 0.0;
+    }
+    g[3 * c] = gx;
+    g[3 * c + 1] = gy;
+    g[3 * c + 2] = gz;
+}
+
+// weighted least-squares gradient (Fvc.h:135-167 with the field boundary constraints :267-287)
+__global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                          const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                          const double* __restrict__ Sf, const double* __restrict__ magSf, const double* __restrict__ d,
+                          const double* __restrict__ psi, const double* __restrict__ psiB,
+                          const int32_t* __restrict__ bPatch, const int32_t* __restrict__ bcType, int twoD,
+                          int emptyDir, double* __restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = (int)((uint32_t)cf[k] & 0x7fffffffu);
+        V3 v;
+        if (f < nI)
+            v = ld3(d, nF, f);
+        else
+            v = lsBoundary(Sf, magSf, d, nF, f, bcType[bPatch[f - nI]] == 1).de;
+        const double s = 1.0 / dot3(v, v);
+        const double o[9] = {v.x * v.x, v.x * v.y, v.x * v.z, v.y * v.x, v.y * v.y, v.y * v.z,
+                             v.z * v.x, v.z * v.y, v.z * v.z};
+#pragma unroll
+        for (int q = 0; q < 9; ++q) a[q] += o[q] * s;
+    }
+    if (twoD) a[4 * emptyDir] += 1.0;
+    // detail::inv (Fvc.h:112-126)
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    double G[9];
+    G[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+    G[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+    G[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+    G[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+    G[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+    G[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+    G[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+    G[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+    G[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = (int)((uint32_t)cf[k] & 0x7fffffffu);
+        V3 v;
+        double dp;
+        if (f < nI) {
+            v = ld3(d, nF, f);
+            dp = psi[nei[f]] - psi[own[f]];
+        } else {
+            const bool value = bcType[bPatch[f - nI]] == 1;
+            const BFace bfc = lsBoundary(Sf, magSf, d, nF, f, value);
+            v = bfc.de;
+            if (value) {
+                dp = psiB[f - nI] - psi[own[f]];
+            } else {
+                // zeroGradient: (gic psi_P + gbc)(n.d) with gic = gbc = 0
+                const double nd = sqrt(dot3(v, v));
+                dp = (0.0 * psi[own[f]] + 0.0) * nd;
+            }
+        }
+        const double wgt = 1.0 / dot3(v, v);
+        const V3 dw{v.x * wgt, v.y * wgt, v.z * wgt};
+        const V3 Gd{G[0] * dw.x + G[1] * dw.y + G[2] * dw.z, G[3] * dw.x + G[4] * dw.y + G[5] * dw.z,
+                    G[6] * dw.x + G[7] * dw.y + G[8] * dw.z};
+        gx += Gd.x * dp;
+        gy += Gd.y * dp;
+        gz += Gd.z * dp;
+    }
+    if (twoD) {
+        if (emptyDir == 0) gx = 0.0;
+        if (emptyDir == 1) gy = 0.0;
+        if (emptyDir == 2) gz = 0.0;
+    }
+    g[3 * c] = gx;
+    g[3 * c + 1] = gy;
+    g[3 * c + 2] = gz;
+}
+
+// explicit non-orthogonal correction flux (Fvm.h:162-165)
+__global__ void k_lap_ffc(int nI, int nF, const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                          const double* __restrict__ w, const double* __restrict__ corr, const double* __restrict__ gs,
+                          const double* __restrict__ g, double* __restrict__ ffc) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    if (f >= nI) {
+        ffc[f] = 0.0;
+        return;
+    }
+    const int o = own[f], n = nei[f];
+    const double wf = w[f], wn = 1.0 - wf;
+    const double gx = wf * g[3 * o] + wn * g[3 * n];
+    const double gy = wf * g[3 * o + 1] + wn * g[3 * n + 1];
+    const double gz = wf * g[3 * o + 2] + wn * g[3 * n + 2];
+    ffc[f] = gs[f] * (corr[f] * gx + corr[nF + f] * gy + corr[2 * nF + f] * gz);
+}
+
+__global__ void k_fold(int nC, int nI, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                       const double* __restrict__ diag, const double* __restrict__ source, const double* __restrict__ ic,
+                       const double* __restrict__ bs, double* __restrict__ d, double* __restrict__ b) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double dd = diag[c], bb = source[c];
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = (int)((uint32_t)cf[k] & 0x7fffffffu);
+        if (f < nI) continue;
+        dd += ic[f - nI];
+        bb += bs[f - nI];
+    }
+    d[c] = dd;
+    b[c] = bb;
+}
+
+__global__ void k_flux(int nF, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                       const double* __restrict__ upper, const double* __restrict__ psi, const double* __restrict__ ic,
+                       const double* __restrict__ bs, const double* __restrict__ ffc, double* __restrict__ F) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    double v;
+    if (f < nI)
+        v = upper[f] * psi[nei[f]] - upper[f] * psi[own[f]];
+    else
+        v = ic[f - nI] * psi[own[f]] - bs[f - nI];
+    if (ffc) v += ffc[f];
+    F[f] = v;
+}
+
+__global__ void k_add_vol_source(int nC, double* __restrict__ source, const double* __restrict__ su,
+                                 const double* __restrict__ V) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nC) source[c] += su[c] * V[c];
+}
+
+__global__ void k_div(int nC, int nI, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                      const double* __restrict__ F, const double* __restrict__ V, double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double r = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = (int)(e & 0x7fffffffu);
+        if (f < nI && (e >> 31))
+            r -= F[f];
+        else
+            r += F[f];
+    }
+    out[c] = r / V[c];
+}
+
+__global__ void k_set_reference(int cell, double value, double* diag, double* source) {
+    source[cell] += diag[cell] * value;
+    diag[cell] += diag[cell];
+}
+
+__global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
+                             const int32_t* __restrict__ bcType, const double* __restrict__ bcValue,
+                             const double* __restrict__ psi, double* __restrict__ psiB) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB) return;
+    psiB[b] = bcType[bPatch[b]] == 1 ? (bcValue ? bcValue[b] : 0.0) : psi[own[nI + b]];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- DeviceGeom
+DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own, const int32_t* nei,
+                       const double* magSf, const double* ndc, const double* V, const double* Sf, const double* d,
+                       const double* w, const double* corrVecs, int twoD, int emptyDir, int nPatches,
+                       const int32_t* patchStart, const int32_t* patchSize, cudaStream_t s)
+    : nC_(nCells), nI_(nInternal), nF_(nFaces), twoD_(twoD), emptyDir_(emptyDir) {
+    VLM_REQUIRE(V && Sf && d && w && corrVecs, VLM_ERR_BAD_ARG, "mesh geometry (V, Sf, d, w, corrVecs) is required");
+    const int nB = nF_ - nI_;
+    // cell -> face list in ascending face order (the order of every reference face loop)
+    std::vector<int32_t> off(size_t(nC_) + 1, 0), list;
+    for (int f = 0; f < nF_; ++f) {
+        off[own[f] + 1]++;
+        if (f < nI_) off[nei[f] + 1]++;
+    }
+    for (int c = 0; c < nC_; ++c) off[c + 1] += off[c];
+    list.resize(size_t(off[nC_]));
+    std::vector<int32_t> pos(off.begin(), off.end() - 1);
+    for (int f = 0; f < nF_; ++f) {
+        list[pos[own[f]]++] = f;
+        if (f < nI_) list[pos[nei[f]]++] = int32_t(uint32_t(f) | 0x80000000u);
+    }
+    cfOff_.upload(off, s);
+    cfList_.upload(list, s);
+    // boundary face -> patch
+    bPatchHost_.assign(size_t(std::max(nB, 1)), 0);
+    for (int p = 0; p < nPatches; ++p) {
+        patchStart_.push_back(patchStart[p]);
+        patchSize_.push_back(patchSize[p]);
+        for (int i = 0; i < patchSize[p]; ++i) {
+            const int b = patchStart[p] + i - nI_;
+            VLM_REQUIRE(b >= 0 && b < nB, VLM_ERR_BAD_ARG, "patch face range outside the boundary faces");
+            bPatchHost_[b] = p;
+        }
+    }
+    bPatch_.upload(bPatchHost_, s);
+    own_.upload(own, size_t(nF_), s);
+    nei_.upload(nei, size_t(std::max(nI_, 1)) * (nI_ > 0), s);
+    if (nI_ == 0) nei_.resize(1);
+    magSf_.upload(magSf, size_t(nF_), s);
+    ndc_.upload(ndc, size_t(nF_), s);
+    V_.upload(V, size_t(nC_), s);
+    w_.upload(w, size_t(nF_), s);
+    auto soa = [&](const double* aos, DBuf<double>& out) {
+        std::vector<double> v(size_t(3) * nF_);
+        for (int f = 0; f < nF_; ++f)
+            for (int q = 0; q < 3; ++q) v[size_t(q) * nF_ + f] = aos[3 * size_t(f) + q];
+        out.upload(v, s);
+    };
+    soa(Sf, Sf_);
+    soa(d, d_);
+    soa(corrVecs, corr_);
+    // the correction is applied when any internal corrVec is non-zero (Fvm.h:156-158)
+    for (int f = 0; f < nI_ && !nonOrth_; ++f) {
+        const double* c = corrVecs + 3 * size_t(f);
+        nonOrth_ = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] > 1e-20;
+    }
+    scratchG_.resize(size_t(3) * nC_);
+    scratchGS_.resize(size_t(nF_));
+    bcType_.resize(size_t(std::max(nPatches, 1)));
+    VLM_CUDA(cudaStreamSynchronize(s));
+}
+
+void DeviceGeom::uploadBCType(const ScalarBC& bc, cudaStream_t s) {
+    std::vector<int32_t> t(bcType_.size(), 0);
+    for (size_t p = 0; p < patchStart_.size(); ++p) t[p] = bc.type ? bc.type[p] : 0;
+    VLM_CUDA(cudaMemcpyAsync(bcType_.get(), t.data(), sizeof(int32_t) * t.size(), cudaMemcpyHostToDevice, s));
+    VLM_CUDA(cudaStreamSynchronize(s));  // t is a local
+}
+
+void DeviceGeom::correctBoundary(const double* psi, const ScalarBC& bc, double* psiB, cudaStream_t s) {
+    uploadBCType(bc, s);
+    const int nB = nBoundary();
+    if (nB > 0)
+        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, psi, psiB);
+}
+
+void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out,
+                      cudaStream_t s) {
+    uploadBCType(bc, s);
+    if (scheme == 1)
+        k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
+                                            Sf_.get(), magSf_.get(), d_.get(), psi, psiB, bPatch_.get(), bcType_.get(),
+                                            twoD_, emptyDir_, out);
+    else
+        k_grad_gauss<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
+                                               w_.get(), Sf_.get(), V_.get(), psi, psiB, twoD_, emptyDir_, out);
+}
+
+void DeviceGeom::laplacian(const double* gamma, const double* psi, const double* psiB, const ScalarBC& bc,
+                           bool nonOrthCorr, int gradScheme, double* diag, double* upper, double* source, double* ic,
+                           double* bs, double* ffc, bool* hasFfc, cudaStream_t s) {
+    uploadBCType(bc, s);
+    double* gs = scratchGS_.get();
+    k_face_gs<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, gamma, magSf_.get(), ndc_.get(), gs, upper);
+    const bool corr = nonOrthCorr && nonOrth_;
+    if (corr) {
+        grad(psi, psiB, bc, gradScheme, scratchG_.get(), s);
+        k_lap_ffc<<<nblk(nF_), 256, 0, s>>>(nI_, nF_, own_.get(), nei_.get(), w_.get(), corr_.get(), gs,
+                                            scratchG_.get(), ffc);
+    }
+    k_lap_cells<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), upper, corr ? ffc : nullptr, diag,
+                                          source);
+    const int nB = nBoundary();
+    if (nB > 0)
+        k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value, ic, bs);
+    if (hasFfc) *hasFfc = corr;
+}
+
+void DeviceGeom::fold(const double* diag, const double* source, const double* ic, const double* bs, double* d,
+                      double* b, cudaStream_t s) {
+    k_fold<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), diag, source, ic, bs, d, b);
+}
+
+void DeviceGeom::flux(const double* upper, const double* psi, const double* ic, const double* bs, const double* ffc,
+                      double* F, cudaStream_t s) {
+    k_flux<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, own_.get(), nei_.get(), upper, psi, ic, bs, ffc, F);
+}
+
+void DeviceGeom::addVolumeSource(double* source, const double* su, cudaStream_t s) {
+    k_add_vol_source<<<nblk(nC_), 256, 0, s>>>(nC_, source, su, V_.get());
+}
+
+void DeviceGeom::div(const double* F, double* out, cudaStream_t s) {
+    k_div<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), F, V_.get(), out);
+}
+
+void DeviceGeom::setReference(int cell, double value, double* diag, double* source, cudaStream_t s) {
+    VLM_REQUIRE(cell >= 0 && cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
+    k_set_reference<<<1, 1, 0, s>>>(cell, value, diag, source);
+}
+
+}  // namespace vlm

@@ -1,0 +1,79 @@
+// Device-resident mesh geometry and the finite-volume assembly kernels of the pressure
+// equation: fvm::laplacian (with explicit non-orthogonal correction), fvc::grad (Gauss linear,
+// weighted least squares), fvc::div, the FvMatrix boundary fold / setReference / flux, and the
+// non-orthogonal-corrector loop of the pressure equation around the GAMG-PCG solve.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "common.h"
+#include "solver.h"
+
+namespace vlm {
+
+// Scalar boundary conditions of one field: per patch 0 = zeroGradient, 1 = fixedValue
+// (values per boundary face, index f - nInternal).
+struct ScalarBC {
+    const int32_t* type = nullptr;  // host, nPatches
+    const double* value = nullptr;  // device, nBoundary (may be null: 0)
+};
+
+class DeviceGeom {
+public:
+    // Host arrays of cfd::Mesh (see vlm_mesh_desc); copied to the device.
+    DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own, const int32_t* nei, const double* magSf,
+               const double* ndc, const double* V, const double* Sf, const double* d, const double* w,
+               const double* corrVecs, int twoD, int emptyDir, int nPatches, const int32_t* patchStart,
+               const int32_t* patchSize, cudaStream_t stream);
+
+    int nCells() const { return nC_; }
+    int nInternal() const { return nI_; }
+    int nFaces() const { return nF_; }
+    int nBoundary() const { return nF_ - nI_; }
+    bool nonOrthogonal() const { return nonOrth_; }
+
+    // fvm::laplacian(gamma, psi) for a scalar field (Fvm.h:141-182).  All pointers device.
+    // gradScheme: 0 Gauss linear, 1 least squares.  ffc may be null when not needed.
+    void laplacian(const double* gamma, const double* psi, const double* psiB, const ScalarBC& bc, bool nonOrthCorr,
+                   int gradScheme, double* diag, double* upper, double* source, double* ic, double* bs, double* ffc,
+                   bool* hasFfc, cudaStream_t s);
+
+    // fvc::grad of a scalar (Fvc.h:209-291): out 3*nCells (x,y,z per cell).  psiB: boundary values.
+    void grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out, cudaStream_t s);
+
+    // zeroGradient / fixedValue boundary values of a scalar field (correctBoundaryConditions)
+    void correctBoundary(const double* psi, const ScalarBC& bc, double* psiB, cudaStream_t s);
+
+    // FvMatrix::solve's fold (FvMatrix.h:154-163): d = diag + Σ ic, b = source + Σ bs
+    void fold(const double* diag, const double* source, const double* ic, const double* bs, double* d, double* b,
+              cudaStream_t s);
+
+    // FvMatrix::flux (FvMatrix.h:210-222), symmetric matrix: F = upper psi_N - upper psi_P (+ffc)
+    void flux(const double* upper, const double* psi, const double* ic, const double* bs, const double* ffc,
+              double* F, cudaStream_t s);
+
+    // source += su * V  (FvMatrix::operator-=(su), FvMatrix.h:93-97)
+    void addVolumeSource(double* source, const double* su, cudaStream_t s);
+
+    // fvc::div(F) (Fvc.h:294-304): per unit volume
+    void div(const double* F, double* out, cudaStream_t s);
+
+    // setReference (FvMatrix.h:134-141) on one cell
+    void setReference(int cell, double value, double* diag, double* source, cudaStream_t s);
+
+    // gather list of one cell's faces: [cfOff[c], cfOff[c+1]) entries f | (cell is neighbour) << 31
+    const int32_t* cellFaceOff() const { return cfOff_.get(); }
+    const int32_t* cellFaces() const { return cfList_.get(); }
+
+private:
+    int nC_, nI_, nF_, twoD_, emptyDir_;
+    bool nonOrth_ = false;
+    std::vector<int32_t> patchStart_, patchSize_, bPatchHost_;
+    DBuf<int32_t> own_, nei_, cfOff_, cfList_, bPatch_, bcType_;
+    DBuf<double> magSf_, ndc_, V_, w_, Sf_, d_, corr_;  // vectors as SoA: [x(nF) y(nF) z(nF)]
+    DBuf<double> scratchG_, scratchGS_;
+    void uploadBCType(const ScalarBC& bc, cudaStream_t s);
+};
+
+}  // namespace vlm
