@@ -115,6 +115,16 @@ const char* vlm_last_error(const vlm_ctx* ctx); /* ctx may be NULL: last error o
 void* vlm_ctx_stream(vlm_ctx* ctx);
 
 vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* desc, int32_t merge_levels, vlm_mesh** out);
+/* A batch of n_systems independent meshes registered as one device object (batched GAMG-PCG:
+ * every kernel of an iteration covers all systems; reductions and convergence stay per system,
+ * so each system's result is bit-identical to solving it alone).  Arrays of every entry point on a
+ * batch concatenate the systems in order: cells, and internal faces (upper/lower) system after
+ * system; face arrays of the assembly calls (gamma, flux) hold every system's internal faces
+ * followed by every system's boundary faces; perf outputs have n_systems entries (per pass). */
+vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t n_systems, const vlm_mesh_desc* descs,
+                                   int32_t merge_levels, vlm_mesh** out);
+vlm_status vlm_mesh_systems(vlm_mesh* mesh, int32_t* n_systems, int64_t* n_cells, int64_t* n_internal_faces,
+                            int64_t* n_faces);
 vlm_status vlm_mesh_release(vlm_mesh* mesh);
 
 /* ------------------------------------------------------------------ linear algebra */
@@ -172,6 +182,13 @@ vlm_status vlm_pressure_solve(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma,
                               const int32_t* bc_type, const double* bc_values, int32_t ref_cell, double ref_value,
                               int32_t n_non_orth, int32_t grad_scheme, const vlm_solver_ctrl* ctrl,
                               const vlm_solver_ctrl* final_ctrl, vlm_solver_perf* perf, double* flux);
+/* Batch form: ref_cells[n_systems] (local cell of each system, -1: none); perf[(n_non_orth+1)*n_systems]
+ * (pass-major); device_pointers selects device (1) or host (0) arrays. */
+vlm_status vlm_pressure_solve_batch(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, const double* div_phi,
+                                    double* p, const int32_t* bc_type, const double* bc_values,
+                                    const int32_t* ref_cells, double ref_value, int32_t n_non_orth,
+                                    int32_t grad_scheme, const vlm_solver_ctrl* ctrl, const vlm_solver_ctrl* final_ctrl,
+                                    vlm_solver_perf* perf, double* flux, int32_t device_pointers);
 /* Same with device pointers, ordered on vlm_ctx_stream(ctx). */
 vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double* gamma, const double* div_phi,
                                      double* p, const int32_t* bc_type, const double* bc_values, int32_t ref_cell,

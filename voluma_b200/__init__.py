@@ -148,6 +148,7 @@ class Mesh:
     def __init__(self, n_cells, owner, neighbour, magSf, ndc, n_faces=None, ctx: Context | None = None,
                  merge_levels: int = 2, geometry: dict | None = None):
         self.ctx = ctx or default_context()
+        self.n_systems = 1
         self.owner = np.ascontiguousarray(owner, np.int32)
         self.neighbour = np.ascontiguousarray(neighbour, np.int32)
         self.magSf = _f64(magSf)
@@ -183,6 +184,51 @@ class Mesh:
         check(load().vlm_mesh_register(self.ctx.handle, C.byref(d), merge_levels, C.byref(h)), self.ctx.handle)
         self._h = h
         _live.add(self)
+
+    @classmethod
+    def batch(cls, meshes: list, ctx: Context | None = None, merge_levels: int = 2) -> "Mesh":
+        """Registers several meshes (dicts with the cfd::Mesh array names) as one device batch.
+        Arrays passed to the batch concatenate the systems: cells and internal faces in system
+        order; assembly face arrays hold all internal faces, then all boundary faces."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        self.n_systems = len(meshes)
+        self._keep = []
+        descs = (_ffi.MeshDesc * len(meshes))()
+        for d, m in zip(descs, meshes):
+            own = np.ascontiguousarray(m["owner"], np.int32)
+            nei = np.ascontiguousarray(m["neighbour"], np.int32)
+            arrs = [own, nei, _f64(m["magSf"]), _f64(m["ndc"])]
+            d.n_cells, d.n_internal_faces, d.n_faces = int(m["n_cells"]), nei.size, own.size
+            d.owner, d.neighbour, d.magSf, d.ndc = (a.ctypes.data for a in arrs)
+            for name in ("V", "Sf", "d", "w", "corrVecs"):
+                if name in m:
+                    a = _f64(m[name])
+                    arrs.append(a)
+                    setattr(d, name, a.ctypes.data)
+            if "patch_start" in m:
+                ps = np.ascontiguousarray(m["patch_start"], np.int32)
+                pz = np.ascontiguousarray(m["patch_size"], np.int32)
+                arrs += [ps, pz]
+                d.n_patches, d.patch_start, d.patch_size = ps.size, ps.ctypes.data, pz.ctypes.data
+            d.two_d = int(m.get("two_d", 0))
+            d.empty_dir = int(m.get("empty_dir", -1))
+            self._keep += arrs
+        h = C.c_void_p()
+        check(load().vlm_mesh_register_batch(self.ctx.handle, len(meshes), descs, merge_levels, C.byref(h)),
+              self.ctx.handle)
+        self._h = h
+        _live.add(self)
+        self._keep = []
+        ns, nc, ni, nf = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().vlm_mesh_systems(h, C.byref(ns), C.byref(nc), C.byref(ni), C.byref(nf)))
+        self.n_cells, self.n_internal_faces, self.n_faces = nc.value, ni.value, nf.value
+        self.geometry = {"patch_start": np.concatenate([np.asarray(m.get("patch_start", []), np.int32)
+                                                        for m in meshes])}
+        self.cell_base = np.cumsum([0] + [int(m["n_cells"]) for m in meshes])
+        self.face_base = np.cumsum([0] + [len(m["neighbour"]) for m in meshes])
+        self.bface_base = np.cumsum([0] + [len(m["owner"]) - len(m["neighbour"]) for m in meshes])
+        return self
 
     @classmethod
     def from_arrays(cls, m: dict, **kw) -> "Mesh":
@@ -275,20 +321,22 @@ def solve_ldu(mesh: Mesh, diag, upper, lower, b, x, ctrl: SolverControls) -> Sol
     diag, upper, b = _f64(diag), _f64(upper), _f64(b)
     lower = None if lower is None else _f64(lower)
     c = ctrl.to_c()
-    p = _ffi.SolverPerf()
+    p = (_ffi.SolverPerf * mesh.n_systems)()
     check(load().vlm_ldu_solve(mesh.ctx.handle, mesh.handle, _ptr(diag), _ptr(upper), _ptr(lower), _ptr(b), _ptr(x),
-                               C.byref(c), C.byref(p)), mesh.ctx.handle)
-    return SolverPerformance.from_c(p)
+                               C.byref(c), p), mesh.ctx.handle)
+    out = [SolverPerformance.from_c(q) for q in p]
+    return out[0] if mesh.n_systems == 1 else out
 
 
 def solve_ldu_device(mesh: Mesh, diag_ptr, upper_ptr, lower_ptr, b_ptr, x_ptr, ctrl: SolverControls) -> SolverPerformance:
     """Device-pointer variant (integers, e.g. torch tensor data_ptr()) ordered on the mesh context's stream."""
     c = ctrl.to_c()
-    p = _ffi.SolverPerf()
+    p = (_ffi.SolverPerf * mesh.n_systems)()
     check(load().vlm_ldu_solve_device(mesh.ctx.handle, mesh.handle, C.c_void_p(diag_ptr), C.c_void_p(upper_ptr),
                                       C.c_void_p(lower_ptr) if lower_ptr else None, C.c_void_p(b_ptr),
-                                      C.c_void_p(x_ptr), C.byref(c), C.byref(p)), mesh.ctx.handle)
-    return SolverPerformance.from_c(p)
+                                      C.c_void_p(x_ptr), C.byref(c), p), mesh.ctx.handle)
+    out = [SolverPerformance.from_c(q) for q in p]
+    return out[0] if mesh.n_systems == 1 else out
 
 
 def _bc(mesh: Mesh, bc_type, bc_values):
@@ -336,19 +384,25 @@ def pressure_solve(mesh: Mesh, gamma, div_phi, p, ctrl: SolverControls, final_ct
                    bc_type=None, bc_values=None, ref_cell=0, ref_value=0.0, n_non_orth=0, grad_scheme=1,
                    want_flux=True):
     """The pressure-corrector loop (IncompressibleFlow.cpp:322-341) on the device; p is solved in
-    place.  Returns (list of SolverPerformance per pass, face flux of the last pass or None)."""
+    place.  ref_cell: one cell (single mesh) or one per system of a batch (-1 / None: none).
+    Returns (performances per pass [per system for a batch], face flux of the last pass or None)."""
     if not (isinstance(p, np.ndarray) and p.dtype == np.float64 and p.flags.c_contiguous):
         raise TypeError("p must be a C-contiguous float64 array (solved in place)")
     t, v = _bc(mesh, bc_type, bc_values)
-    perf = (_ffi.SolverPerf * (n_non_orth + 1))()
+    ns = mesh.n_systems
+    refs = np.full(ns, -1, np.int32)
+    if ref_cell is not None:
+        refs[:] = np.asarray(ref_cell, np.int32)
+    perf = (_ffi.SolverPerf * ((n_non_orth + 1) * ns))()
     flux = np.zeros(mesh.n_faces) if want_flux else None
     c = ctrl.to_c()
     cf = (final_ctrl or ctrl).to_c()
-    check(load().vlm_pressure_solve(mesh.ctx.handle, mesh.handle, _ptr(_f64(gamma)), _ptr(_f64(div_phi)), _ptr(p),
-                                    _ptr(t), _ptr(v), int(-1 if ref_cell is None else ref_cell), float(ref_value),
-                                    int(n_non_orth), int(grad_scheme), C.byref(c), C.byref(cf), perf, _ptr(flux)),
+    check(load().vlm_pressure_solve_batch(mesh.ctx.handle, mesh.handle, _ptr(_f64(gamma)), _ptr(_f64(div_phi)),
+                                          _ptr(p), _ptr(t), _ptr(v), _ptr(refs), float(ref_value), int(n_non_orth),
+                                          int(grad_scheme), C.byref(c), C.byref(cf), perf, _ptr(flux), 0),
           mesh.ctx.handle)
-    return [SolverPerformance.from_c(q) for q in perf], flux
+    rows = [[SolverPerformance.from_c(perf[q * ns + s]) for s in range(ns)] for q in range(n_non_orth + 1)]
+    return ([r[0] for r in rows] if ns == 1 else rows), flux
 
 
 def exact_sum(values, ctx: Context | None = None) -> float:

@@ -1,0 +1,123 @@
+"""Synthetic workloads of the pressure-equation path (host side, numpy).
+
+* tgv_pressure_system(n): the 3D Taylor-Green pressure equation on the periodic [0,2pi]^3 box
+  with an n^3 uniform mesh, as the PIMPLE corrector assembles it (laplacian(rAUf = dt) minus the
+  divergence of a predicted flux, setReference(0)).
+* poisson_batch(...): uneven batch of pressure Poisson systems on graded, jittered unit boxes
+  (Neumann walls + one reference cell; right-hand side = divergence of a random Fourier velocity
+  field with |k| <= 4 and N(0,1)/|k|^2 amplitudes), as projectDivergenceFree solves them.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import mesh as vm
+
+DT = 2e-3
+
+
+def fourier_velocity(X, seed, n_modes=16, kmax=4):
+    """Sum of n_modes random Fourier modes (|k| <= kmax, amplitude N(0,1)/|k|^2) at points X."""
+    rng = np.random.default_rng(seed)
+    u = np.zeros((len(X), 3))
+    for _ in range(n_modes):
+        while True:
+            k = rng.integers(-kmax, kmax + 1, size=3)
+            if k.any() and (k * k).sum() <= kmax * kmax:
+                break
+        kk = float(np.sqrt((k * k).sum()))
+        a = rng.standard_normal(3) / kk ** 2
+        ph = rng.uniform(0, 2 * np.pi)
+        u += np.outer(np.cos(2 * np.pi * (X @ k) + ph), a)
+    return u
+
+
+def face_flux(m, u_face):
+    Sf = m["Sf"]
+    return u_face[:, 0] * Sf[:, 0] + u_face[:, 1] * Sf[:, 1] + u_face[:, 2] * Sf[:, 2]
+
+
+def div_per_volume(m, F):
+    """fvc::div (Fvc.h:294-304) restated for input preparation."""
+    nI = m["n_internal_faces"]
+    r = np.zeros(m["n_cells"])
+    np.add.at(r, np.stack([m["owner"][:nI], m["neighbour"]], 1).ravel(), np.stack([F[:nI], -F[:nI]], 1).ravel())
+    np.add.at(r, m["owner"][nI:], F[nI:])
+    return r / m["V"]
+
+
+def tgv_velocity(C, seed=1234, n_modes=16, amp=0.1):
+    x, y, z = C[:, 0], C[:, 1], C[:, 2]
+    u = np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), np.zeros_like(x)], 1)
+    rng = np.random.default_rng(seed)
+    for _ in range(n_modes):
+        k = rng.integers(-4, 5, size=3)
+        if not k.any():
+            k[0] = 1
+        kk = float(np.sqrt((k * k).sum()))
+        a = rng.standard_normal(3) / kk ** 2
+        ph = rng.uniform(0, 2 * np.pi)
+        u += amp * np.outer(np.cos(C @ k + ph), a)
+    return u
+
+
+def tgv_pressure_system(n=128, m=None):
+    """(mesh, diag, upper, b) of the TGV pressure equation on an n^3 periodic box."""
+    m = m or vm.box_mesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+    nC, nI = m["n_cells"], m["n_internal_faces"]
+    own, nei = m["owner"][:nI], m["neighbour"]
+    upper = DT * m["magSf"][:nI] * m["ndc"][:nI]
+    diag = np.zeros(nC)
+    np.subtract.at(diag, np.stack([own, nei], 1).ravel(), np.repeat(upper, 2))
+    u = tgv_velocity(m["C"])
+    w = m["w"][:nI, None]
+    uf = w * u[own] + (1.0 - w) * u[nei]
+    Sf = m["Sf"][:nI]
+    phi = uf[:, 0] * Sf[:, 0] + uf[:, 1] * Sf[:, 1] + uf[:, 2] * Sf[:, 2]
+    div = np.zeros(nC)
+    np.add.at(div, np.stack([own, nei], 1).ravel(), np.stack([phi, -phi], 1).ravel())
+    b = (div / m["V"]) * m["V"]
+    diag[0] += diag[0]
+    return m, diag, upper, b
+
+
+def graded_jittered_box(n, ratio, jitter, seed):
+    """Unit box n^3 with tanh grading (centre/wall cell-size ratio `ratio`, beta = acosh(sqrt(ratio)))
+    in every direction and interior vertices jittered by U(+-jitter*h)."""
+    beta = math.acosh(math.sqrt(ratio)) if ratio > 1.0 + 1e-12 else 0.0
+    pts = vm.box_points((n, n, n), beta=(beta, beta, beta))
+    if jitter > 0:
+        pts = vm.jitter_interior(pts, (n, n, n), jitter, seed)
+    return vm.box_mesh((n, n, n), points=pts)
+
+
+def poisson_batch(n_systems=256, n_min=16, n_max=96, seed=20261203, jitter=0.2, ratio_max=8.0):
+    """List of (mesh, div_phi) pairs: the pressure Poisson systems of projectDivergenceFree on
+    graded, jittered boxes of uneven sizes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_systems):
+        n = int(rng.integers(n_min, n_max + 1))
+        ratio = float(rng.uniform(1.0, ratio_max))
+        m = graded_jittered_box(n, ratio, jitter, int(rng.integers(1 << 30)))
+        u_f = fourier_velocity(m["Cf"], int(rng.integers(1 << 30)))
+        out.append((m, div_per_volume(m, face_flux(m, u_f))))
+    return out
+
+
+def batch_face_array(meshes, per_mesh):
+    """Concatenates per-mesh face arrays into the batch layout: every mesh's internal faces, then
+    every mesh's boundary faces."""
+    ints = [a[: m["n_internal_faces"]] for m, a in zip(meshes, per_mesh)]
+    bnds = [a[m["n_internal_faces"]:] for m, a in zip(meshes, per_mesh)]
+    return np.concatenate(ints + bnds)
+
+
+def split_batch_faces(meshes, F):
+    nI = [m["n_internal_faces"] for m in meshes]
+    nB = [m["n_faces"] - m["n_internal_faces"] for m in meshes]
+    ib = np.cumsum([0] + nI)
+    bb = sum(nI) + np.cumsum([0] + nB)
+    return [np.concatenate([F[ib[i]:ib[i + 1]], F[bb[i]:bb[i + 1]]]) for i in range(len(meshes))]

@@ -25,9 +25,13 @@ struct vlm_topology {
 
 struct vlm_mesh {
     vlm_ctx* ctx = nullptr;
+    int nsys = 1;
+    // totals of the concatenation: cells and internal faces in system order, then every boundary face
     int nCells = 0, nInternal = 0, nFaces = 0;
-    std::vector<int32_t> own, nei;
-    std::vector<double> magSf, ndc;
+    std::vector<int64_t> cellBase, faceBase, bfaceBase;  // per system
+    std::vector<std::vector<int32_t>> own, nei;          // per system, local numbering (hierarchy input)
+    std::vector<std::vector<double>> magSf, ndc;
+    vlm::DBuf<int32_t> refCells;  // global reference cells of a batch pressure solve
     std::unique_ptr<vlm::DeviceBatch> batch;
     std::unique_ptr<vlm::DeviceGeom> geom;  // assembly geometry (when the descriptor carries it)
     // staging for the host-pointer entry points
@@ -37,6 +41,14 @@ struct vlm_mesh {
 };
 
 namespace {
+// hierarchy of the first system (input order) of a mesh / batch
+const vlm::Hierarchy& hierOf(vlm_mesh* m) {
+    const auto& P = m->batch->plan();
+    for (int b = 0; b < P.nsys; ++b)
+        if (P.order[b] == 0) return P.H[b];
+    return P.H[0];
+}
+
 vlm::DeviceGeom& geomOf(vlm_mesh* m) {
     VLM_REQUIRE(m->geom, VLM_ERR_BAD_ARG, "the mesh was registered without geometry (V, Sf, d, w, corrVecs)");
     return *m->geom;
@@ -146,42 +158,102 @@ const char* vlm_last_error(const vlm_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 void* vlm_ctx_stream(vlm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
-vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* d, int32_t mergeLevels, vlm_mesh** out) {
-    if (!ctx || !d || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_desc* descs, int32_t mergeLevels,
+                                   vlm_mesh** out) {
+    if (!ctx || !descs || !out || nsys <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
     *out = nullptr;
     return guarded(ctx, [&] {
-        VLM_REQUIRE(d->n_cells > 0 && d->n_internal_faces >= 0 && d->n_faces >= d->n_internal_faces, VLM_ERR_BAD_ARG,
-                    "invalid mesh sizes");
-        VLM_REQUIRE(d->owner && (d->neighbour || d->n_internal_faces == 0), VLM_ERR_BAD_ARG,
-                    "owner/neighbour are required");
-        VLM_REQUIRE(d->magSf && d->ndc, VLM_ERR_BAD_ARG, "magSf and ndc are required (GAMG weights)");
+        bool geometry = true;
+        int64_t nC = 0, nI = 0, nF = 0;
+        for (int s = 0; s < nsys; ++s) {
+            const vlm_mesh_desc* d = &descs[s];
+            VLM_REQUIRE(d->n_cells > 0 && d->n_internal_faces >= 0 && d->n_faces >= d->n_internal_faces,
+                        VLM_ERR_BAD_ARG, "invalid mesh sizes");
+            VLM_REQUIRE(d->owner && (d->neighbour || d->n_internal_faces == 0), VLM_ERR_BAD_ARG,
+                        "owner/neighbour are required");
+            VLM_REQUIRE(d->magSf && d->ndc, VLM_ERR_BAD_ARG, "magSf and ndc are required (GAMG weights)");
+            geometry = geometry && d->V && d->Sf && d->d && d->w && d->corrVecs;
+            VLM_REQUIRE(d->two_d == descs[0].two_d && d->empty_dir == descs[0].empty_dir, VLM_ERR_BAD_ARG,
+                        "every system of a batch must have the same 2D/3D setting");
+            nC += d->n_cells;
+            nI += d->n_internal_faces;
+            nF += d->n_faces;
+        }
+        VLM_REQUIRE(nF < (int64_t(1) << 31) - 1, VLM_ERR_BAD_ARG, "batch exceeds 2^31 faces");
         setDevice(ctx);
         auto m = std::make_unique<vlm_mesh>();
         m->ctx = ctx;
-        m->nCells = d->n_cells;
-        m->nInternal = d->n_internal_faces;
-        m->nFaces = d->n_faces;
-        m->own.assign(d->owner, d->owner + d->n_faces);
-        m->nei.assign(d->neighbour, d->neighbour + d->n_internal_faces);
-        m->magSf.assign(d->magSf, d->magSf + d->n_faces);
-        m->ndc.assign(d->ndc, d->ndc + d->n_faces);
-        vlm::SysTopo t;
-        t.nCells = m->nCells;
-        t.nInternal = m->nInternal;
-        t.own = m->own.data();
-        t.nei = m->nei.data();
-        t.magSf = m->magSf.data();
-        t.ndc = m->ndc.data();
-        m->batch = std::make_unique<vlm::DeviceBatch>(std::vector<vlm::SysTopo>{t}, mergeLevels > 0 ? mergeLevels : 2,
-                                                      ctx->stream);
-        if (d->V && d->Sf && d->d && d->w && d->corrVecs)
-            m->geom = std::make_unique<vlm::DeviceGeom>(d->n_cells, d->n_internal_faces, d->n_faces, d->owner,
-                                                        d->neighbour, d->magSf, d->ndc, d->V, d->Sf, d->d, d->w,
-                                                        d->corrVecs, d->two_d, d->empty_dir, d->n_patches,
-                                                        d->patch_start, d->patch_size, ctx->stream);
+        m->nsys = nsys;
+        m->nCells = int(nC);
+        m->nInternal = int(nI);
+        m->nFaces = int(nF);
+        std::vector<vlm::SysTopo> topo(static_cast<size_t>(nsys));
+        int64_t cb = 0, fb = 0, bb = 0;
+        for (int s = 0; s < nsys; ++s) {
+            const vlm_mesh_desc* d = &descs[s];
+            m->cellBase.push_back(cb);
+            m->faceBase.push_back(fb);
+            m->bfaceBase.push_back(bb);
+            m->own.emplace_back(d->owner, d->owner + d->n_faces);
+            m->nei.emplace_back(d->neighbour, d->neighbour + d->n_internal_faces);
+            m->magSf.emplace_back(d->magSf, d->magSf + d->n_faces);
+            m->ndc.emplace_back(d->ndc, d->ndc + d->n_faces);
+            topo[s].nCells = d->n_cells;
+            topo[s].nInternal = d->n_internal_faces;
+            topo[s].own = m->own[s].data();
+            topo[s].nei = m->nei[s].data();
+            topo[s].magSf = m->magSf[s].data();
+            topo[s].ndc = m->ndc[s].data();
+            cb += d->n_cells;
+            fb += d->n_internal_faces;
+            bb += d->n_faces - d->n_internal_faces;
+        }
+        m->batch = std::make_unique<vlm::DeviceBatch>(topo, mergeLevels > 0 ? mergeLevels : 2, ctx->stream);
+        if (geometry) {
+            // the union mesh: every system's internal faces, then every system's boundary faces
+            const size_t F = static_cast<size_t>(nF), NI = static_cast<size_t>(std::max<int64_t>(nI, 1)),
+                         NC = static_cast<size_t>(nC);
+            std::vector<int32_t> own(F), nei(NI), ps, pz;
+            std::vector<double> magSf(F), ndc(F), w(F), V(NC), Sf(3 * F), dd(3 * F), corr(3 * F);
+            auto copyFace = [&](const vlm_mesh_desc* d, int f, int64_t g, int64_t base) {
+                own[g] = int32_t(d->owner[f] + base);
+                magSf[g] = d->magSf[f];
+                ndc[g] = d->ndc[f];
+                w[g] = d->w[f];
+                for (int q = 0; q < 3; ++q) {
+                    Sf[3 * g + q] = d->Sf[3 * f + q];
+                    dd[3 * g + q] = d->d[3 * f + q];
+                    corr[3 * g + q] = d->corrVecs[3 * f + q];
+                }
+            };
+            for (int s = 0; s < nsys; ++s) {
+                const vlm_mesh_desc* d = &descs[s];
+                const int64_t base = m->cellBase[s];
+                for (int c = 0; c < d->n_cells; ++c) V[base + c] = d->V[c];
+                for (int f = 0; f < d->n_internal_faces; ++f) {
+                    copyFace(d, f, m->faceBase[s] + f, base);
+                    nei[m->faceBase[s] + f] = int32_t(d->neighbour[f] + base);
+                }
+                for (int f = d->n_internal_faces; f < d->n_faces; ++f)
+                    copyFace(d, f, nI + m->bfaceBase[s] + (f - d->n_internal_faces), base);
+                for (int p = 0; p < d->n_patches; ++p) {
+                    ps.push_back(int32_t(nI + m->bfaceBase[s] + (d->patch_start[p] - d->n_internal_faces)));
+                    pz.push_back(d->patch_size[p]);
+                }
+            }
+            m->geom = std::make_unique<vlm::DeviceGeom>(int(nC), int(nI), int(nF), own.data(), nei.data(), magSf.data(),
+                                                        ndc.data(), V.data(), Sf.data(), dd.data(), w.data(),
+                                                        corr.data(), descs[0].two_d, descs[0].empty_dir,
+                                                        int(ps.size()), ps.data(), pz.data(), ctx->stream);
+        }
         ctx->refs++;
         *out = m.release();
     });
+}
+
+vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* d, int32_t mergeLevels, vlm_mesh** out) {
+    if (!ctx || !d || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return vlm_mesh_register_batch(ctx, 1, d, mergeLevels, out);
 }
 
 vlm_status vlm_mesh_release(vlm_mesh* mesh) {
@@ -216,7 +288,7 @@ vlm_status vlm_ldu_solve_device(vlm_ctx* ctx, vlm_mesh* m, const double* diag, c
         setDevice(ctx);
         std::vector<vlm_solver_perf> p;
         m->batch->solve(diag, upper, lower ? lower : upper, b, x, *ctrl, p);
-        if (perf) *perf = p[0];
+        if (perf) std::copy(p.begin(), p.end(), perf);
     });
 }
 
@@ -234,7 +306,7 @@ vlm_status vlm_ldu_solve(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const do
         m->batch->solve(dd, du, dl, m->b.get(), m->x.get(), *ctrl, p);
         VLM_CUDA(cudaMemcpyAsync(x, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost, s));
         VLM_CUDA(cudaStreamSynchronize(s));
-        if (perf) *perf = p[0];
+        if (perf) std::copy(p.begin(), p.end(), perf);
     });
 }
 
@@ -255,13 +327,13 @@ vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const d
 
 vlm_status vlm_gamg_levels(vlm_mesh* m, int32_t* n) {
     if (!m || !n) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
-    *n = int32_t(m->batch->plan().H[0].levels.size());
+    *n = int32_t(hierOf(m).levels.size());
     return VLM_OK;
 }
 
 vlm_status vlm_gamg_level(vlm_mesh* m, int32_t level, int32_t* sizes, int32_t* l, int32_t* u, int32_t* agg) {
     if (!m || !sizes) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
-    const auto& H = m->batch->plan().H[0];
+    const auto& H = hierOf(m);
     if (level < 0 || level >= int32_t(H.levels.size())) return fail(m->ctx, VLM_ERR_BAD_ARG, "level out of range");
     const auto& L = H.levels[level];
     sizes[0] = L.n;
@@ -377,11 +449,20 @@ void ensureWork(vlm_mesh* m) {
 
 // Device-pointer pressure corrector loop; bcv: device boundary values or null.
 void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double* p, const int32_t* bcType,
-                  const double* bcv, int refCell, double refValue, int nNonOrth, int gradScheme,
+                  const double* bcv, const int32_t* refCells, double refValue, int nNonOrth, int gradScheme,
                   const vlm_solver_ctrl& ctrl, const vlm_solver_ctrl& finalCtrl, vlm_solver_perf* perf, double* flux) {
     vlm::DeviceGeom& G = geomOf(m);
     cudaStream_t s = m->ctx->stream;
     ensureWork(m);
+    // global reference cells (-1: none)
+    std::vector<int32_t> refs;
+    for (int q = 0; q < m->nsys; ++q) {
+        if (!refCells || refCells[q] < 0) continue;
+        const int64_t cellsOfSystem = (q + 1 < m->nsys ? m->cellBase[q + 1] : int64_t(m->nCells)) - m->cellBase[q];
+        VLM_REQUIRE(refCells[q] < cellsOfSystem, VLM_ERR_BAD_ARG, "reference cell out of range");
+        refs.push_back(int32_t(m->cellBase[q] + refCells[q]));
+    }
+    if (!refs.empty()) m->refCells.upload(refs, s);
     vlm::ScalarBC bc;
     bc.type = bcType;
     bc.value = bcv;
@@ -392,11 +473,12 @@ void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double
         G.laplacian(gamma, p, m->pB.get(), bc, true, gradScheme, m->pdiag.get(), m->pupper.get(), m->psource.get(),
                     m->ic.get(), m->bs.get(), m->ffc.get(), &hasFfc, s);
         G.addVolumeSource(m->psource.get(), divPhi, s);
-        if (refCell >= 0) G.setReference(refCell, refValue, m->pdiag.get(), m->psource.get(), s);
+        if (!refs.empty())
+            G.setReferences(m->refCells.get(), int(refs.size()), refValue, m->pdiag.get(), m->psource.get(), s);
         G.fold(m->pdiag.get(), m->psource.get(), m->ic.get(), m->bs.get(), m->fd.get(), m->fb.get(), s);
         std::vector<vlm_solver_perf> pf;
         m->batch->solve(m->fd.get(), m->pupper.get(), m->pupper.get(), m->fb.get(), p, last ? finalCtrl : ctrl, pf);
-        if (perf) perf[no] = pf[0];
+        if (perf) std::copy(pf.begin(), pf.end(), perf + size_t(no) * m->nsys);
         if (last && flux) G.flux(m->pupper.get(), p, m->ic.get(), m->bs.get(), hasFfc ? m->ffc.get() : nullptr, flux, s);
     }
     G.correctBoundary(p, bc, m->pB.get(), s);
@@ -471,40 +553,66 @@ vlm_status vlm_div(vlm_ctx* ctx, vlm_mesh* m, const double* F, double* out) {
     });
 }
 
-vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
-                                     const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
-                                     int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
-                                     const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
-    if (!ctx || !m || !gamma || !divPhi || !p || !bcType || !ctrl || nNonOrth < 0)
-        return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
-    return guarded(ctx, [&] {
-        setDevice(ctx);
-        pressureLoop(m, gamma, divPhi, p, bcType, bcValues, refCell, refValue, nNonOrth, gradScheme, *ctrl,
-                     finalCtrl ? *finalCtrl : *ctrl, perf, flux);
-    });
-}
-
-vlm_status vlm_pressure_solve(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
-                              const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
-                              int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
-                              const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
+vlm_status vlm_pressure_solve_batch(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
+                                    const int32_t* bcType, const double* bcValues, const int32_t* refCells,
+                                    double refValue, int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
+                                    const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux,
+                                    int32_t devicePointers) {
     if (!ctx || !m || !gamma || !divPhi || !p || !bcType || !ctrl || nNonOrth < 0)
         return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
     return guarded(ctx, [&] {
         setDevice(ctx);
         cudaStream_t s = ctx->stream;
+        if (devicePointers) {
+            vlm::DBuf<double> bcvd;
+            const int nB = m->nFaces - m->nInternal;
+            if (bcValues && nB > 0) {
+                bcvd.resize(size_t(nB));
+                VLM_CUDA(cudaMemcpyAsync(bcvd.get(), bcValues, sizeof(double) * nB, cudaMemcpyDeviceToDevice, s));
+            }
+            pressureLoop(m, gamma, divPhi, p, bcType, bcvd.get(), refCells, refValue, nNonOrth, gradScheme, *ctrl,
+                         finalCtrl ? *finalCtrl : *ctrl, perf, flux);
+            VLM_CUDA(cudaStreamSynchronize(s));
+            return;
+        }
         ensureWork(m);
         m->gamma.upload(gamma, size_t(m->nFaces), s);
         m->su.upload(divPhi, size_t(m->nCells), s);
         m->p.upload(p, size_t(m->nCells), s);
         const double* bcv = stageBC(m, bcValues, s);
-        pressureLoop(m, m->gamma.get(), m->su.get(), m->p.get(), bcType, bcv, refCell, refValue, nNonOrth, gradScheme,
+        pressureLoop(m, m->gamma.get(), m->su.get(), m->p.get(), bcType, bcv, refCells, refValue, nNonOrth, gradScheme,
                      *ctrl, finalCtrl ? *finalCtrl : *ctrl, perf, flux ? m->flux.get() : nullptr);
         VLM_CUDA(cudaMemcpyAsync(p, m->p.get(), sizeof(double) * m->nCells, cudaMemcpyDeviceToHost, s));
         if (flux)
             VLM_CUDA(cudaMemcpyAsync(flux, m->flux.get(), sizeof(double) * m->nFaces, cudaMemcpyDeviceToHost, s));
         VLM_CUDA(cudaStreamSynchronize(s));
     });
+}
+
+vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
+                                     const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
+                                     int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
+                                     const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
+    return vlm_pressure_solve_batch(ctx, m, gamma, divPhi, p, bcType, bcValues, &refCell, refValue, nNonOrth,
+                                    gradScheme, ctrl, finalCtrl, perf, flux, 1);
+}
+
+vlm_status vlm_pressure_solve(vlm_ctx* ctx, vlm_mesh* m, const double* gamma, const double* divPhi, double* p,
+                              const int32_t* bcType, const double* bcValues, int32_t refCell, double refValue,
+                              int32_t nNonOrth, int32_t gradScheme, const vlm_solver_ctrl* ctrl,
+                              const vlm_solver_ctrl* finalCtrl, vlm_solver_perf* perf, double* flux) {
+    return vlm_pressure_solve_batch(ctx, m, gamma, divPhi, p, bcType, bcValues, &refCell, refValue, nNonOrth,
+                                    gradScheme, ctrl, finalCtrl, perf, flux, 0);
+}
+
+vlm_status vlm_mesh_systems(vlm_mesh* m, int32_t* n_systems, int64_t* n_cells, int64_t* n_internal_faces,
+                            int64_t* n_faces) {
+    if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    if (n_systems) *n_systems = m->nsys;
+    if (n_cells) *n_cells = m->nCells;
+    if (n_internal_faces) *n_internal_faces = m->nInternal;
+    if (n_faces) *n_faces = m->nFaces;
+    return VLM_OK;
 }
 
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out) {

@@ -280,6 +280,15 @@ __global__ void k_set_reference(int cell, double value, double* diag, double* so
     diag[cell] += diag[cell];
 }
 
+__global__ void k_set_references(const int32_t* __restrict__ cells, int n, double value, double* diag,
+                                 double* source) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int c = cells[q];
+    source[c] += diag[c] * value;
+    diag[c] += diag[c];
+}
+
 __global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
                              const int32_t* __restrict__ bcType, const double* __restrict__ bcValue,
                              const double* __restrict__ psi, double* __restrict__ psiB) {
@@ -419,6 +428,11 @@ void DeviceGeom::div(const double* F, double* out, cudaStream_t s) {
 void DeviceGeom::setReference(int cell, double value, double* diag, double* source, cudaStream_t s) {
     VLM_REQUIRE(cell >= 0 && cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
     k_set_reference<<<1, 1, 0, s>>>(cell, value, diag, source);
+}
+
+void DeviceGeom::setReferences(const int32_t* cells, int n, double value, double* diag, double* source,
+                               cudaStream_t s) {
+    if (n > 0) k_set_references<<<nblk(n), 256, 0, s>>>(cells, n, value, diag, source);
 }
 
 }  // namespace vlm

@@ -59,8 +59,9 @@ public:
     // fvc::div(F) (Fvc.h:294-304): per unit volume
     void div(const double* F, double* out, cudaStream_t s);
 
-    // setReference (FvMatrix.h:134-141) on one cell
+    // setReference (FvMatrix.h:134-141) on one cell / on n cells (device list of global cells)
     void setReference(int cell, double value, double* diag, double* source, cudaStream_t s);
+    void setReferences(const int32_t* cells, int n, double value, double* diag, double* source, cudaStream_t s);
 
     // gather list of one cell's faces: [cfOff[c], cfOff[c+1]) entries f | (cell is neighbour) << 31
     const int32_t* cellFaceOff() const { return cfOff_.get(); }
