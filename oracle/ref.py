@@ -206,3 +206,45 @@ class RefMesh:
 def exact_sum(v) -> float:
     v = np.ascontiguousarray(v, np.float64)
     return float(lib().ref_exact_sum(_p(v), v.size))
+
+
+# ---------------------------------------------------------------------- drop-in check
+DROPIN_PATH = os.path.join(HERE, "_ref", "libvlmdropin.so")
+_dropin = None
+
+
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_PATH)
+
+
+def dropin_pressure_solve(n, gamma, div_phi, p0, lo=(0, 0, 0), hi=(1, 1, 1), periodic=(0, 0, 0), points=None,
+                          ref_cell=0, n_non_orth=0, grad_scheme=1, solver="PCG", precond="GAMG", tol=0.0,
+                          rel_tol=1e-8, max_iter=1000, reproducible=False, smoother="", precision=""):
+    """The reference's pressure loop (laplacian, -= divPhi, setReference, FvMatrix::solve) with its
+    solveLdu calls redirected to the GPU library (oracle/dropin_driver.cpp).  Returns
+    (p, flux, perf rows, number of solveLdu calls that reached the GPU)."""
+    global _dropin
+    if _dropin is None:
+        L = C.CDLL(DROPIN_PATH)
+        P = C.c_void_p
+        L.dropin_last_error.restype = C.c_char_p
+        L.dropin_pressure_solve.argtypes = [P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
+                                            C.c_double, C.c_double, C.c_int, C.c_int, C.c_char_p, C.c_char_p, P, P,
+                                            P]
+        _dropin = L
+    L = _dropin
+    before = L.dropin_calls()
+    p = np.ascontiguousarray(p0, np.float64).copy()
+    nF = len(gamma)
+    flux = np.zeros(nF)
+    perf = np.zeros(6 * (n_non_orth + 1))
+    pts = None if points is None else np.ascontiguousarray(points, np.float64)
+    rc = L.dropin_pressure_solve(_p(np.asarray(n, np.int32)), _p(np.asarray(lo, np.float64)),
+                                 _p(np.asarray(hi, np.float64)), _p(np.asarray(periodic, np.int32)), _p(pts),
+                                 _p(np.ascontiguousarray(gamma, np.float64)),
+                                 _p(np.ascontiguousarray(div_phi, np.float64)), int(ref_cell), int(n_non_orth),
+                                 int(grad_scheme), solver.encode(), precond.encode(), tol, rel_tol, max_iter,
+                                 int(reproducible), smoother.encode(), precision.encode(), _p(p), _p(flux), _p(perf))
+    if rc != 0:
+        raise RuntimeError(L.dropin_last_error().decode())
+    return p, flux, perf.reshape(-1, 6), L.dropin_calls() - before
