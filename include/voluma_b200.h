@@ -223,6 +223,17 @@ vlm_status vlm_topology_destroy(vlm_topology* t);
 /* Order-independent exact sum of n doubles on the device (host pointer in, host result). */
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out);
 
+/* Exact sum that allocates no device memory.  No counterpart in the reference.  For callers that
+ * cannot call cudaMalloc where they need the sum (device memory owned by their own pool or fixed
+ * budget; loops where an allocate/free pair would synchronise the device).  values and out are
+ * device pointers; the work is ordered on `stream` (a cudaStream_t, NULL = default stream) and the
+ * call returns before it completes.  Scratch: one fixed 299,016-byte __device__ array per device,
+ * held until the process exits and shared by all calls; calls that overlap on the GPU race on it,
+ * so order them on one stream.  The first call on a device looks the array up and clears it
+ * (make that first call before any stream capture).  n <= 2^31-1, else VLM_ERR_BAD_ARG; the
+ * message is available from vlm_last_error(NULL). */
+vlm_status vlm_exact_sum_noalloc(const double* values, int64_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
-           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch"]
+           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc"]
 
 
 class MeshDesc(C.Structure):
@@ -80,6 +80,7 @@ def load():
                                      C.POINTER(SolverCtrl), P, P]
     L.vlm_pressure_solve_device.argtypes = L.vlm_pressure_solve.argtypes
     L.vlm_mesh_register_batch.argtypes = [P, i32, P, i32, C.POINTER(P)]
+    L.vlm_exact_sum_noalloc.argtypes = [P, C.c_int64, P, P]
     L.vlm_mesh_systems.argtypes = [P, P, P, P, P]
     L.vlm_pressure_solve_batch.argtypes = [P, P, P, P, P, P, P, P, C.c_double, i32, i32, C.POINTER(SolverCtrl),
                                            C.POINTER(SolverCtrl), P, P, i32]

@@ -60,6 +60,12 @@ namespace {
 constexpr int64_t kRowsPerCtaForSum = 256;
 thread_local std::string g_lastError;
 
+}  // namespace
+
+void vlm::setThreadError(const std::string& msg) { g_lastError = msg; }
+
+namespace {
+
 vlm_status fail(vlm_ctx* ctx, vlm_status s, const std::string& msg) {
     g_lastError = msg;
     if (ctx) ctx->err = msg;

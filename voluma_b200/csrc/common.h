@@ -71,6 +71,9 @@ private:
     size_t n_ = 0;
 };
 
+// Records the message vlm_last_error(NULL) returns on this thread.
+void setThreadError(const std::string& msg);
+
 // Row chunk handed to one CTA of a row kernel: rows [start, start+count), count <= 256.
 // sys/slot are used by reduction kernels (system index; partial-sum slot).
 struct Chunk {
