@@ -200,8 +200,10 @@ vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double*
 vlm_status vlm_mesh_stats(vlm_mesh* mesh, int64_t* launches, int64_t* device_bytes);
 /* Measurement hook: times `reps` back-to-back launches of one level-0 kernel on the matrix of
  * the last solve ("amul64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch
- * is one full multicolour sweep) with CUDA events on the context stream.  Outputs the mean ms per
- * launch and the algorithmic bytes of one launch (values + int32 addressing, each array once). */
+ * is one full multicolour sweep; "vcycle32" / "vcycle32_notail" one FP32 V-cycle with / without
+ * the single-CTA coarse tail, "tail32" the tail alone, bytes 0) with CUDA events on the context
+ * stream, from a fixed state (right-hand side b, zero iterate).  Outputs the mean ms per launch
+ * and the algorithmic bytes of one launch (values + int32 addressing, each array once). */
 vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* mesh, const char* kernel, int32_t reps, double* ms,
                               double* bytes);
 

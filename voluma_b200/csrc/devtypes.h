@@ -48,4 +48,27 @@ struct CoarseDev {
     int rowStart, n, invOffset, sys;
 };
 
+// Arrays of one level as the coarse-tail kernel sees them (one table per precision).
+template <class T>
+struct TailLevel {
+    Sell S;
+    const T* val;
+    const T* diag;
+    T* r;                   // null on level 0 (the V-cycle's own input is passed instead)
+    T* x;                   // null on level 0 (the V-cycle's own output)
+    T* x2;                  // Jacobi ping-pong vector
+    const int32_t* agg;     // row -> next-level row (-1: padding)
+    const int32_t* cptr;    // next-level row -> its children on this level
+    const int32_t* child;
+};
+
+// One system's part of the coarse tail: levels first..coarsest of the V-cycle run in one
+// thread-block cluster.
+constexpr int kTailMaxLevels = 32;
+struct TailSys {
+    int sys, first, coarsest;  // batch position; first tail level; coarsest level
+    int coarseN, invOffset;
+    int rowStart[kTailMaxLevels], rowCount[kTailMaxLevels];
+};
+
 }  // namespace vlm

@@ -19,6 +19,17 @@
 
 namespace vlm {
 
+// ------------------------------------------------------------------ programmatic dependent launch
+// Every kernel of the solver is launched with programmatic stream serialisation: the next kernel
+// may start (its CTAs become resident) while this one drains, and each kernel waits at entry until
+// its predecessor has completed and its writes are visible (griddepcontrol.wait returns at once
+// when the launch had no programmatic predecessor).  It then lets its own successor launch.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 constexpr double kVSMALL = 1.0e-300;  // core/Types.h VSMALL
 constexpr double kGREAT = 1.0e15;     // core/Types.h GREAT
 
@@ -221,6 +232,7 @@ template <int NV> struct BlockSum<NV, true> {
 // Exact sum of a plain array (vlm_exact_sum): one system, chunks of kRowsPerCta values.
 __global__ void __launch_bounds__(kRowsPerCta) k_exact_sum(const Chunk* __restrict__ ch, const double* __restrict__ v,
                                                            RedCtx R, double* out) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     DD a[1] = {DD{0.0, 0.0}};
     if ((int)threadIdx.x < c.count) a[0].hi = v[c.start + threadIdx.x];
@@ -230,28 +242,64 @@ __global__ void __launch_bounds__(kRowsPerCta) k_exact_sum(const Chunk* __restri
 
 // ------------------------------------------------------------------ SELL row access
 
-__device__ __forceinline__ int sell_base(const Sell& S, int row) { return S.slPtr[row >> 5] + (row & 31); }
+__device__ __forceinline__ int sell_base(const Sell& S, int row) { return __ldg(S.slPtr + (row >> 5)) + (row & 31); }
 
-template <class T>
-__device__ __forceinline__ T row_minus(const Sell& S, const T* __restrict__ val, const T* __restrict__ x, int row, T s) {
-    const int len = S.rlen[row];
+// s -= (MINUS) or += a_row,e * X(col_e) over the row's entries in entry order.  The loads are issued
+// in batches of kRowBatch (all column indices and values, then all gathers, then the arithmetic in
+// order), so a row costs two memory round trips instead of two per entry; the arithmetic and its
+// order are those of the plain entry loop.
+constexpr int kRowBatch = 8;
+
+// The matrix (structure and values) is read-only in every kernel that walks rows, so it is read
+// through the non-coherent cache; how X is read is the caller's choice (xf).
+template <bool MINUS, class T, class XF, int B = kRowBatch>
+__device__ __forceinline__ T row_accumulate(const Sell& S, const T* __restrict__ val, XF xf, int row, T s) {
+    const int len = __ldg(S.rlen + row);
     const int base = sell_base(S, row);
-    for (int k = 0; k < len; ++k) {
-        const int e = base + (k << 5);
-        s -= val[e] * x[S.col[e]];
+    if (B == 1) {
+        for (int k = 0; k < len; ++k) {
+            const int e = base + (k << 5);
+            if (MINUS)
+                s -= __ldg(val + e) * xf(__ldg(S.col + e));
+            else
+                s += __ldg(val + e) * xf(__ldg(S.col + e));
+        }
+        return s;
+    }
+    for (int k0 = 0; k0 < len; k0 += B) {
+        int cj[B];
+        T a[B], xv[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q)
+            if (k0 + q < len) {
+                const int e = base + ((k0 + q) << 5);
+                cj[q] = __ldg(S.col + e);
+                a[q] = __ldg(val + e);
+            }
+#pragma unroll
+        for (int q = 0; q < B; ++q)
+            if (k0 + q < len) xv[q] = xf(cj[q]);
+#pragma unroll
+        for (int q = 0; q < B; ++q)
+            if (k0 + q < len) {
+                if (MINUS)
+                    s -= a[q] * xv[q];
+                else
+                    s += a[q] * xv[q];
+            }
     }
     return s;
 }
 
+// x must not be written by the running kernel (it is read through the non-coherent cache).
+template <class T>
+__device__ __forceinline__ T row_minus(const Sell& S, const T* __restrict__ val, const T* __restrict__ x, int row, T s) {
+    return row_accumulate<true>(S, val, [&](int j) { return __ldg(x + j); }, row, s);
+}
+
 template <class T>
 __device__ __forceinline__ T row_plus(const Sell& S, const T* __restrict__ val, const T* __restrict__ x, int row, T s) {
-    const int len = S.rlen[row];
-    const int base = sell_base(S, row);
-    for (int k = 0; k < len; ++k) {
-        const int e = base + (k << 5);
-        s += val[e] * x[S.col[e]];
-    }
-    return s;
+    return row_accumulate<false>(S, val, [&](int j) { return __ldg(x + j); }, row, s);
 }
 
 // Which SysState flag a kernel honours: the outer "done" or the inner-solve "innerDone".
@@ -269,6 +317,7 @@ __device__ __forceinline__ bool chunk_skip(const Chunk& c, const SysState* st, i
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_zero_rows(const Chunk* __restrict__ ch, T* __restrict__ x,
                                                            const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) x[row] = T(0);
@@ -278,6 +327,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_zero_rows(const Chunk* __restri
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restrict__ ch, const T* __restrict__ r,
                                                            T* __restrict__ w, const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) w[row] = r[row];
@@ -287,21 +337,41 @@ __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restri
 template <class From, class To>
 __global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restrict__ ch, const From* __restrict__ a,
                                                            To* __restrict__ b, const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) b[row] = (To)a[row];
 }
 
 // ------------------------------------------------------------------ smoothers
-// Gauss-Seidel row update (GAMG.cpp:368-380) on the rows of one colour step.
-template <class T>
+// Gauss-Seidel row update (GAMG.cpp:368-380) on the rows of one colour step.  Neighbours belong to
+// other colours and are not written by this launch.
+// MODE 0: plain.  MODE 1: first colour of a sweep from x = 0 (every neighbour is still zero:
+// x = r / D without reading the row).  MODE 2: first colour of the first post-sweep of a
+// two-colour level; the neighbours (the other colour, not yet swept) get the coarse-grid
+// correction x + xc[agg] (GAMG.cpp:437-438) on the fly, which replaces the separate prolongation.
+template <class T, int MODE = 0>
 __global__ void __launch_bounds__(kRowsPerCta) k_smooth_gs(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                            const T* __restrict__ diag, const T* __restrict__ r, T* x,
+                                                           const int32_t* __restrict__ agg, const T* __restrict__ xc,
                                                            const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
-    const T s = row_minus(S, val, x, row, r[row]);
+    if (MODE == 1) {
+        x[row] = r[row] / diag[row];
+        return;
+    }
+    auto xf = [&](int j) -> T {
+        T v = __ldg(x + j);
+        if (MODE == 2) {
+            const int a = __ldg(agg + j);
+            if (a >= 0) v += __ldg(xc + a);
+        }
+        return v;
+    };
+    const T s = row_accumulate<true>(S, val, xf, row, r[row]);
     x[row] = s / diag[row];
 }
 
@@ -324,6 +394,7 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
                                                               T* __restrict__ xo, const int8_t* __restrict__ rcol,
                                                               const int32_t* __restrict__ agg,
                                                               const T* __restrict__ xc, const SysState* st, int flag) {
+    pdl_entry();
     __shared__ T xs[kBlockRows + 1];  // xs[kBlockRows] == 0: target of inactive register slots
     const Chunk c = blocks[blockIdx.x];
     if (chunk_skip(c, st, flag)) return;
@@ -399,6 +470,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __re
                                                                T* __restrict__ xo, T omega,
                                                                const int32_t* __restrict__ agg,
                                                                const T* __restrict__ xc, const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
@@ -408,19 +480,14 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __re
         return;
     }
     auto xv = [&](int j) -> T {
-        T v = xi[j];
+        T v = __ldg(xi + j);
         if (MODE == 2) {
-            const int a = agg[j];
-            if (a >= 0) v += xc[a];
+            const int a = __ldg(agg + j);
+            if (a >= 0) v += __ldg(xc + a);
         }
         return v;
     };
-    T s = r[row];
-    const int len = S.rlen[row], base = sell_base(S, row);
-    for (int k = 0; k < len; ++k) {
-        const int e = base + (k << 5);
-        s -= val[e] * xv(S.col[e]);
-    }
+    const T s = row_accumulate<true>(S, val, xv, row, r[row]);
     const T v = s / diag[row];
     if (omega == T(1)) {
         xo[row] = v;
@@ -436,6 +503,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_residual(const Chunk* __restric
                                                           const T* __restrict__ diag, const T* __restrict__ r,
                                                           const T* __restrict__ x, T* __restrict__ res,
                                                           const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
@@ -448,6 +516,7 @@ template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_restrict(const Chunk* __restrict__ ch, const int32_t* __restrict__ cptr,
                                                           const int32_t* __restrict__ child, const T* __restrict__ res,
                                                           T* __restrict__ rc, const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int R = c.start + threadIdx.x;
@@ -460,6 +529,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_restrict(const Chunk* __restric
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_prolong(const Chunk* __restrict__ ch, const int32_t* __restrict__ agg,
                                                          const T* __restrict__ xc, T* __restrict__ x, const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
@@ -476,6 +546,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_prolong(const Chunk* __restrict
 __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const double* __restrict__ val,
                                 const double* __restrict__ diag, double* __restrict__ lu, double* __restrict__ inv,
                                 int* status, int smemN) {
+    pdl_entry();
     extern __shared__ double sh[];
     const CoarseDev c = cs[blockIdx.x];
     const int n = c.n;
@@ -539,6 +610,7 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
 template <class T>
 __global__ void k_coarse_apply(const CoarseDev* __restrict__ cs, const double* __restrict__ inv, const T* __restrict__ r,
                                T* __restrict__ x, const SysState* st, int flag) {
+    pdl_entry();
     const CoarseDev c = cs[blockIdx.x];
     if (st != nullptr && sys_idle(st[c.sys], flag)) return;
     const double* X = inv + c.invOffset;
@@ -549,10 +621,128 @@ __global__ void k_coarse_apply(const CoarseDev* __restrict__ cs, const double* _
     }
 }
 
+// ------------------------------------------------------------------ coarse tail of the V-cycle
+// Levels first..coarsest of one system (GAMG.cpp:403-443 with Jacobi smoothing) in ONE CTA: the
+// levels at the bottom of the hierarchy are a few thousand rows or fewer, too small to fill the
+// GPU, and as separate launches their cost is launch latency.  One CTA per system runs them with
+// __syncthreads() in place of the kernel boundaries; the matrix stays in the SM's L1 across the
+// phases and the vectors are coherent inside the CTA.  Every row is computed with the same
+// operations in the same order as k_smooth_jacobi / k_residual / k_restrict / k_coarse_apply, so
+// the result is bit-identical to the per-level launch sequence.
+constexpr int kTailThreads = 1024;
+constexpr int kTailBatch = 4;      // entries in flight per row (64 registers at 1024 threads)
+constexpr int kTailMaxRows = 1024;  // levels at most this many rows (padded) go to the tail
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* __restrict__ tsys,
+                                                                 const TailLevel<T>* __restrict__ lev,
+                                                                 const double* __restrict__ inv, const T* r0, T* x0,
+                                                                 T omega, const SysState* st, int flag) {
+    pdl_entry();
+    const TailSys& ts = tsys[blockIdx.x];
+    if (st != nullptr && sys_idle(st[ts.sys], flag)) return;  // uniform over the CTA
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int c = ts.coarsest;
+    auto rOf = [&](int k) -> const T* { return k == 0 ? r0 : lev[k].r; };
+    auto xOf = [&](int k) -> T* { return k == 0 ? x0 : lev[k].x; };
+
+    for (int k = ts.first; k < c; ++k) {
+        const TailLevel<T>& L = lev[k];
+        const T* r = rOf(k);
+        T* x = xOf(k);
+        const int a0 = ts.rowStart[k], a1 = a0 + ts.rowCount[k];
+        // two pre-sweeps from zero; the first sweep's value of a neighbour is recomputed where
+        // the second sweep needs it (MODE 1 then MODE 0 of k_smooth_jacobi)
+        auto first = [&](int j) -> T {
+            const T v = r[j] / __ldg(L.diag + j);
+            return omega == T(1) ? v : omega * v;
+        };
+        for (int i = a0 + tid; i < a1; i += nthr) {
+            const T s = row_accumulate<true, T, decltype(first), kTailBatch>(L.S, L.val, first, i, r[i]);
+            const T v = s / __ldg(L.diag + i);
+            if (omega == T(1)) {
+                x[i] = v;
+            } else {
+                const T xv = first(i);
+                x[i] = xv + omega * (v - xv);
+            }
+        }
+        __syncthreads();
+        // residual of each child computed where its aggregate sums it (k_residual + k_restrict)
+        T* rn = lev[k + 1].r;
+        auto xr = [&](int j) -> T { return x[j]; };
+        const int b0 = ts.rowStart[k + 1], b1 = b0 + ts.rowCount[k + 1];
+        for (int R = b0 + tid; R < b1; R += nthr) {
+            T s = T(0);
+            const int q1 = __ldg(L.cptr + R + 1);
+            for (int q = __ldg(L.cptr + R); q < q1; ++q) {
+                const int i = __ldg(L.child + q);
+                const T t = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
+                                                                               r[i] - __ldg(L.diag + i) * x[i]);
+                s += t;
+            }
+            rn[R] = s;
+        }
+        __syncthreads();
+    }
+    {
+        // coarsest level: x = inv * r (k_coarse_apply)
+        const T* r = rOf(c);
+        T* x = xOf(c);
+        const int n = ts.coarseN, rs = ts.rowStart[c];
+        const double* X = inv + ts.invOffset;
+        for (int i = tid; i < n; i += nthr) {
+            double g = 0.0;
+            for (int j = 0; j < n; ++j) g += __ldg(X + (size_t)i * n + j) * (double)r[rs + j];
+            x[rs + i] = (T)g;
+        }
+    }
+    for (int k = c - 1; k >= ts.first; --k) {
+        __syncthreads();
+        const TailLevel<T>& L = lev[k];
+        const T* r = rOf(k);
+        T* x = xOf(k);
+        const T* xc = xOf(k + 1);
+        T* x2 = L.x2;
+        const int a0 = ts.rowStart[k], a1 = a0 + ts.rowCount[k];
+        // post-sweep 1 with the coarse-grid correction fused in (MODE 2), into x2
+        auto xv = [&](int j) -> T {
+            T v = x[j];
+            const int a = __ldg(L.agg + j);
+            if (a >= 0) v += xc[a];
+            return v;
+        };
+        for (int i = a0 + tid; i < a1; i += nthr) {
+            const T s = row_accumulate<true, T, decltype(xv), kTailBatch>(L.S, L.val, xv, i, r[i]);
+            const T v = s / __ldg(L.diag + i);
+            if (omega == T(1)) {
+                x2[i] = v;
+            } else {
+                const T x0v = xv(i);
+                x2[i] = x0v + omega * (v - x0v);
+            }
+        }
+        __syncthreads();
+        // post-sweep 2 (MODE 0), back into x
+        for (int i = a0 + tid; i < a1; i += nthr) {
+            auto x2f = [&](int j) -> T { return x2[j]; };
+            const T s = row_accumulate<true, T, decltype(x2f), kTailBatch>(L.S, L.val, x2f, i, r[i]);
+            const T v = s / __ldg(L.diag + i);
+            if (omega == T(1)) {
+                x[i] = v;
+            } else {
+                const T x0v = x2[i];
+                x[i] = x0v + omega * (v - x0v);
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ per-solve setup
 // Level-0 diagonal in solver order (padding rows get 1 so smoothers leave them at 0).
 template <class T>
 __global__ void k_gather_diag0(int n, const int32_t* __restrict__ perm, const double* __restrict__ d, T* __restrict__ out) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p = perm[i];
@@ -562,6 +752,7 @@ __global__ void k_gather_diag0(int n, const int32_t* __restrict__ perm, const do
 // Entry values from LDU face coefficients: src >= 0 -> upper[src], else lower[~src].
 __global__ void k_materialize(int nent, const int32_t* __restrict__ src, const double* __restrict__ upper,
                               const double* __restrict__ lower, double* __restrict__ val, float* __restrict__ val32) {
+    pdl_entry();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nent) return;
     const int s = src[e];
@@ -576,6 +767,7 @@ __global__ void k_galerkin_diag(int nrows, const int32_t* __restrict__ cptr, con
                                 const int32_t* __restrict__ iptr, const int32_t* __restrict__ iface,
                                 const double* __restrict__ dfine, const double* __restrict__ up,
                                 const double* __restrict__ lo, double* __restrict__ dc, float* __restrict__ dc32) {
+    pdl_entry();
     const int R = blockIdx.x * blockDim.x + threadIdx.x;
     if (R >= nrows) return;
     double s;
@@ -597,6 +789,7 @@ __global__ void k_galerkin_diag(int nrows, const int32_t* __restrict__ cptr, con
 __global__ void k_galerkin_faces(int nfaces, const int32_t* __restrict__ fptr, const int32_t* __restrict__ fsrc,
                                  const double* __restrict__ up, const double* __restrict__ lo, double* __restrict__ cu,
                                  double* __restrict__ cl) {
+    pdl_entry();
     const int F = blockIdx.x * blockDim.x + threadIdx.x;
     if (F >= nfaces) return;
     double su = 0.0, sl = 0.0;
@@ -618,6 +811,7 @@ __global__ void k_galerkin_faces(int nfaces, const int32_t* __restrict__ fptr, c
 // Permute a user vector into solver order (padding -> 0) and back.
 template <class T>
 __global__ void k_to_solver(int n, const int32_t* __restrict__ perm, const double* __restrict__ u, T* __restrict__ v) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p = perm[i];
@@ -625,6 +819,7 @@ __global__ void k_to_solver(int n, const int32_t* __restrict__ perm, const doubl
 }
 
 __global__ void k_from_solver(int n, const int32_t* __restrict__ perm, const double* __restrict__ v, double* __restrict__ u) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p = perm[i];
@@ -632,6 +827,7 @@ __global__ void k_from_solver(int n, const int32_t* __restrict__ perm, const dou
 }
 
 __global__ void k_cast_f64_to_f32(int n, const double* __restrict__ a, float* __restrict__ b) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];
 }

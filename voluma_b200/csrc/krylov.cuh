@@ -24,6 +24,7 @@ __device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, doubl
 template <class T, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_sum_x(const Chunk* __restrict__ ch, const T* __restrict__ x, RedCtx R,
                                                        SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     BlockSum<1, EXACT> acc;
     acc.begin();
@@ -42,6 +43,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __re
                                                                const int32_t* __restrict__ perm, double* __restrict__ r,
                                                                float* __restrict__ r32, const int32_t* __restrict__ nCells,
                                                                RedCtx R, SysState* st, const DevCtrl* __restrict__ ctrlp) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     const double xRef = st[c.sys].s0 / (double)nCells[c.sys];
     BlockSum<2, EXACT> acc;
@@ -90,6 +92,7 @@ template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_precond_diag(const Chunk* __restrict__ ch, const T* __restrict__ rD,
                                                               const T* __restrict__ r, T* __restrict__ w,
                                                               const SysState* st, int flag) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], flag)) return;
     VLM_ROWS(c) w[row] = rD[row] * r[row];
@@ -98,6 +101,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_precond_diag(const Chunk* __res
 // rD = 1/diag (LinearSolver.cpp:66,78); padding rows: 0
 template <class T>
 __global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* __restrict__ d, T* __restrict__ rD) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     rD[i] = valid[i] >= 0 ? T(1) / d[i] : T(0);
@@ -105,9 +109,12 @@ __global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* 
 
 // ------------------------------------------------------------------ PCG (LinearSolver.cpp:176-201)
 // wArA = Σ w·r ; beta = wArA / wArAold
-template <class T, int FLAG, bool EXACT>
-__global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restrict__ ch, const T* __restrict__ w,
+// W: type of the preconditioned residual w (float when an FP32 V-cycle produced it; widening it
+// here gives the same doubles a separate cast would).
+template <class T, int FLAG, bool EXACT, class W = T>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restrict__ ch, const W* __restrict__ w,
                                                             const T* __restrict__ r, RedCtx R, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
@@ -124,18 +131,19 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
 }
 
 // p = w (first iteration) or w + beta p
-template <class T, int FLAG>
-__global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__ ch, const T* __restrict__ w,
+template <class T, int FLAG, class W = T>
+__global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__ ch, const W* __restrict__ w,
                                                        T* __restrict__ p, const SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     const SysState& s = st[c.sys];
     if (sys_idle(s, FLAG)) return;
     const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
     const T beta = (T)s.beta;
     if (it == 0) {
-        VLM_ROWS(c) p[row] = w[row];
+        VLM_ROWS(c) p[row] = (T)w[row];
     } else {
-        VLM_ROWS(c) p[row] = w[row] + beta * p[row];
+        VLM_ROWS(c) p[row] = (T)w[row] + beta * p[row];
     }
 }
 
@@ -144,6 +152,7 @@ template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                           const T* __restrict__ diag, const T* __restrict__ p,
                                                           T* __restrict__ Ap, RedCtx R, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
@@ -169,12 +178,14 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restric
     }
 }
 
-// x += alpha p ; r -= alpha Ap ; finalResidual = Σ|r| / normFactor ; convergence
+// x += alpha p ; r -= alpha Ap ; finalResidual = Σ|r| / normFactor ; convergence.
+// r32 (optional): FP32 copy of the new r, the next FP32 V-cycle's input.
 template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restrict__ ch, T* __restrict__ x, T* __restrict__ r,
                                                             const T* __restrict__ p, const T* __restrict__ Ap,
                                                             const int32_t* __restrict__ perm, RedCtx R, SysState* st,
-                                                            const DevCtrl* __restrict__ ctrlp) {
+                                                            const DevCtrl* __restrict__ ctrlp, float* __restrict__ r32) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (sys_idle(st[c.sys], FLAG)) return;
     const T alpha = (T)st[c.sys].alpha;
@@ -184,6 +195,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
         x[row] += alpha * p[row];
         const T rr = r[row] - alpha * Ap[row];
         r[row] = rr;
+        if (r32 != nullptr) r32[row] = (float)rr;
         acc.add(0, fabs((double)rr));
     }
     double out[1];
@@ -218,6 +230,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
 // ------------------------------------------------------------------ mixed precision outer loop
 // start of an inner solve: e = 0 is done by a zero kernel; reset the inner recurrences.
 __global__ void k_inner_begin(int nsys, SysState* st) {
+    pdl_entry();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
     SysState& q = st[s];
@@ -230,6 +243,7 @@ __global__ void k_inner_begin(int nsys, SysState* st) {
 // x64 += e32 ; then r64 = b - A x64 in a second kernel (neighbours must be updated first)
 __global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                                const float* __restrict__ e, const SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     VLM_ROWS(c) x[row] += (double)e[row];
@@ -243,6 +257,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
                                                                 const double* __restrict__ b, double* __restrict__ r,
                                                                 float* __restrict__ r32, RedCtx R, SysState* st,
                                                                 const DevCtrl* __restrict__ ctrlp) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     BlockSum<1, false> acc;
@@ -275,6 +290,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
 template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restrict__ ch, const double* __restrict__ r0,
                                                           const double* __restrict__ r, RedCtx R, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     BlockSum<1, EXACT> acc;
@@ -298,6 +314,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restric
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_p(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ p,
                                                         const SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     const SysState& s = st[c.sys];
     if (s.done) return;
@@ -316,6 +333,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
                                                                  const double* __restrict__ diag,
                                                                  const double* __restrict__ y, double* __restrict__ Ay,
                                                                  const double* __restrict__ r0, RedCtx R, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     BlockSum<1, EXACT> acc;
@@ -340,6 +358,7 @@ template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ sv, RedCtx R,
                                                         SysState* st, const DevCtrl* __restrict__ ctrlp) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha;
@@ -368,6 +387,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict_
 // early exit of LinearSolver.cpp:224-227
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_early(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                             const double* __restrict__ y, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     SysState& s = st[c.sys];
     if (s.done || s.s1 == 0.0) return;
@@ -377,6 +397,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_early(const Chunk* __restr
 
 // closes the early exit (separate launch so every CTA above saw s1 before done is set)
 __global__ void k_bicg_early_close(int nsys, SysState* st) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nsys && !st[i].done && st[i].s1 != 0.0) {
         st[i].converged = 1;
@@ -391,6 +412,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __
                                                                  const double* __restrict__ diag,
                                                                  const double* __restrict__ z, double* __restrict__ t,
                                                                  const double* __restrict__ sv, RedCtx R, SysState* st) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     BlockSum<2, EXACT> acc;
@@ -415,6 +437,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
                                                              const double* __restrict__ z, const double* __restrict__ sv,
                                                              const double* __restrict__ t, RedCtx R, SysState* st,
                                                              const DevCtrl* __restrict__ ctrlp) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha, omega = st[c.sys].omega;
@@ -444,6 +467,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
 __global__ void __launch_bounds__(kRowsPerCta) k_amul(const Chunk* __restrict__ ch, Sell S, const double* __restrict__ val,
                                                       const double* __restrict__ diag, const double* __restrict__ x,
                                                       double* __restrict__ y) {
+    pdl_entry();
     const Chunk c = ch[blockIdx.x];
     VLM_ROWS(c) y[row] = row_plus(S, val, x, row, diag[row] * x[row]);
 }

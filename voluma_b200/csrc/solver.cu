@@ -6,9 +6,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <cstdio>
 #include <functional>
 #include <set>
+#include <utility>
 
 #include "krylov.cuh"
 #include "solver.h"
@@ -58,10 +60,38 @@ constexpr int kCoarseSharedN = 80;
 thread_local int64_t tl_launches = 0;
 
 // Launch helper: skips empty grids (a zero-block launch is an error) and counts the launch.
+// Programmatic dependent launch for the solver kernels launched directly on a stream (VLM_PDL=0
+// turns it off).  Inside the captured solve graphs it measured no faster, so graph capture
+// records plain launches.
+thread_local bool tl_capturing = false;
+
+bool pdlEnabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("VLM_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on && !tl_capturing;
+}
+
+template <class... Exp, class... Act>
+void launchK(void (*kernel)(Exp...), int grid, int block, cudaStream_t s, Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdlEnabled() ? 1 : 0;
+    VLM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
+}
+
 #define VLM_LAUNCH(kernel, grid, block, stream, ...)                    \
     do {                                                                \
         if ((grid) > 0) {                                               \
-            kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);      \
+            launchK(kernel, (grid), (block), (stream), __VA_ARGS__);    \
             ++tl_launches;                                              \
         }                                                               \
     } while (0)
@@ -107,6 +137,7 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     plan_ = buildPlan(systems, mergeLevels);
     const char* gv = std::getenv("VLM_GRAPH");
     useGraphs_ = !(gv && gv[0] == '0');
+
     const int nL = int(plan_.levels.size());
     L_.resize(nL);
     const char* om = std::getenv("VLM_JACOBI_OMEGA");
@@ -120,6 +151,7 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         L_[k].coarse.n = int(cds.size()) - L_[k].coarse.off;
     }
     coarse_.upload(cds, stream_);
+    planTail();
     for (int k = 0; k < nL; ++k) {
         LevelPlan& P = plan_.levels[k];
         DevLevel& D = L_[k];
@@ -144,6 +176,17 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         };
         D.active = add(P.active);
         D.all = add(P.all);
+        if (tailOn_) {
+            // coarse-tail mode: rows still smoothed by per-level launches, and the rows the last
+            // of those restrictions writes (systems whose tail starts at or below this level)
+            std::vector<Chunk> head, in;
+            for (const Chunk& c : P.active)
+                if (tailFirst_[c.sys] > k) head.push_back(c);
+            for (const Chunk& c : P.all)
+                if (k > 0 && tailFirst_[c.sys] >= k) in.push_back(c);
+            D.headActive = add(head);
+            D.headIn = add(in);
+        }
         for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
         for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
         D.blocks = add(P.blocks);
@@ -198,10 +241,32 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         v->zero(stream_);
     }
     hostState_.resize(size_t(plan_.nsys));
+    if (tailOn_) buildTailTable<double>(tail64_);
     VLM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 DeviceBatch::~DeviceBatch() { graphs_.clear(); }
+
+template <class T>
+void DeviceBatch::buildTailTable(DBuf<TailLevel<T>>& out) {
+    const int nL = int(L_.size());
+    std::vector<TailLevel<T>> tab(static_cast<size_t>(nL));
+    for (int k = 0; k < nL; ++k) {
+        DevLevel& D = L_[k];
+        TailLevel<T>& t = tab[k];
+        t.S = D.sell();
+        t.val = LV<T>::val(D);
+        t.diag = LV<T>::diag(D);
+        t.r = k > 0 ? LV<T>::r(D) : nullptr;
+        t.x = k > 0 ? LV<T>::x(D) : nullptr;
+        t.x2 = LV<T>::x2(D);
+        t.agg = D.agg.get();
+        t.cptr = D.childPtr.get();
+        t.child = D.child.get();
+    }
+    out.upload(tab, stream_);
+    VLM_CUDA(cudaStreamSynchronize(stream_));  // the host table is a local
+}
 
 size_t DeviceBatch::deviceBytes() const {
     size_t b = 0;
@@ -254,6 +319,7 @@ void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
             D.t32.zero(stream_);
             D.x232.zero(stream_);
         }
+        if (tailOn_) buildTailTable<float>(tail32_);
     }
 }
 
@@ -302,7 +368,7 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
 
 // ====================================================================== V-cycle
 template <class T>
-void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag) {
+void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag, bool head) {
     DevLevel& D = L_[k];
     cudaStream_t s = stream_;
     const Sell S = D.sell();
@@ -316,15 +382,16 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
     if (jacobiHere) {
         // Jacobi; pre: from zero, post: prolongation fused into the first sweep
         const T om = T(jacobiOmega_);
+        const ChunkList& rows = head ? D.headActive : D.active;
         if (pre) {
-            VLM_LAUNCH((k_smooth_jacobi<T, 1>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r,
+            VLM_LAUNCH((k_smooth_jacobi<T, 1>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r,
                        (const T*)nullptr, x2, om, agg, xc, st, flag);
-            VLM_LAUNCH((k_smooth_jacobi<T, 0>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         } else {
-            VLM_LAUNCH((k_smooth_jacobi<T, 2>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x, x2,
+            VLM_LAUNCH((k_smooth_jacobi<T, 2>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
                        om, agg, xc, st, flag);
-            VLM_LAUNCH((k_smooth_jacobi<T, 0>), D.active.n, kRowsPerCta, s, D.ch(D.active), S, val, diag, r, x2, x,
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         }
     } else if (D.blockGS) {
@@ -342,12 +409,24 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
                        x, rc, agg, xc, st, flag);
         }
     } else {
-        // global multicolour GS: forward colours pre-smoothing, reversed colours post-smoothing
-        if (pre) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
+        // global multicolour GS: forward colours pre-smoothing, reversed colours post-smoothing.
+        // Two colours: the pre-smoothing's first colour sees only zeros (x = r/D, no zeroing
+        // needed) and the post-smoothing's first colour applies the prolongation to the
+        // neighbours it reads (no separate prolongation).
+        const bool two = D.nSteps == 2;
+        if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
                 const ChunkList& l = pre ? D.fwd[t] : D.rev[t];
-                VLM_LAUNCH(k_smooth_gs<T>, l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, st, flag);
+                if (two && sweep == 0 && t == 0 && pre)
+                    VLM_LAUNCH((k_smooth_gs<T, 1>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
+                               flag);
+                else if (two && sweep == 0 && t == 0)
+                    VLM_LAUNCH((k_smooth_gs<T, 2>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
+                               flag);
+                else
+                    VLM_LAUNCH((k_smooth_gs<T, 0>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
+                               flag);
             }
     }
 }
@@ -357,34 +436,95 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
 // system still smooths, solve every system's coarsest level, then ascend (prolongation,
 // 2 post-sweeps).
 template <class T>
-void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag) {
+void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bool allowTail) {
     cudaStream_t s = stream_;
     const int nL = int(L_.size());
     const SysState* st = st_.get();
     auto rr = [&](int k) -> const T* { return k == 0 ? r0 : LV<T>::r(L_[k]); };
     auto xx = [&](int k) -> T* { return k == 0 ? x0 : LV<T>::x(L_[k]); };
-    for (int k = 0; k + 1 < nL; ++k) {
+    // Jacobi coarse levels: each system's levels from tailFirst_ down run in one cluster launch
+    const bool tail = allowTail && tailOn_ && sm != SmootherKind::MCGS;
+    const int headEnd = tail ? tailMaxFirst_ : nL - 1;
+    for (int k = 0; k < headEnd; ++k) {
         DevLevel& D = L_[k];
         DevLevel& N = L_[k + 1];
-        recordSmooth<T>(k, rr(k), xx(k), sm, true, flag);
-        VLM_LAUNCH(k_residual<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.sell(), LV<T>::val(D), LV<T>::diag(D),
+        const ChunkList& rows = tail ? D.headActive : D.active;
+        const ChunkList& next = tail ? N.headIn : N.all;
+        recordSmooth<T>(k, rr(k), xx(k), sm, true, flag, tail);
+        VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
                    rr(k), xx(k), LV<T>::t(D), st, flag);
-        VLM_LAUNCH(k_restrict<T>, N.all.n, kRowsPerCta, s, N.ch(N.all), D.childPtr.get(), D.child.get(), LV<T>::t(D),
+        VLM_LAUNCH(k_restrict<T>, next.n, kRowsPerCta, s, N.ch(next), D.childPtr.get(), D.child.get(), LV<T>::t(D),
                    LV<T>::r(N), st, flag);
     }
-    for (int k = 0; k < nL; ++k) {
-        DevLevel& D = L_[k];
-        VLM_LAUNCH(k_coarse_apply<T>, D.coarse.n, 128, s, coarse_.get() + D.coarse.off, inv_.get(), rr(k), xx(k), st,
-                   flag);
+    if (tail) {
+        recordTail<T>(r0, x0, flag);
+    } else {
+        for (int k = 0; k < nL; ++k) {
+            DevLevel& D = L_[k];
+            VLM_LAUNCH(k_coarse_apply<T>, D.coarse.n, 128, s, coarse_.get() + D.coarse.off, inv_.get(), rr(k), xx(k),
+                       st, flag);
+        }
     }
-    for (int k = nL - 2; k >= 0; --k) {
+    for (int k = headEnd - 1; k >= 0; --k) {
         DevLevel& D = L_[k];
         const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
-        if (!jacobiHere && !D.blockGS)  // block GS and Jacobi fuse the prolongation into their first sweep
+        // block GS, Jacobi and two-colour GS fuse the prolongation into their first sweep
+        if (!jacobiHere && !D.blockGS && D.nSteps != 2)
             VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st,
                        flag);
-        recordSmooth<T>(k, rr(k), xx(k), sm, false, flag);
+        recordSmooth<T>(k, rr(k), xx(k), sm, false, flag, tail);
     }
+}
+
+template <class T>
+void DeviceBatch::recordTail(const T* r0, T* x0, int flag) {
+    const TailLevel<T>* tab = std::is_same<T, float>::value ? (const TailLevel<T>*)tail32_.get()
+                                                             : (const TailLevel<T>*)tail64_.get();
+    if (!tab) throw Error(VLM_ERR_CUDA, "internal: coarse-tail table missing");
+    VLM_LAUNCH(k_vcycle_tail<T>, int(tailSys_.size()), kTailThreads, stream_, (const TailSys*)tailSys_.get(), tab,
+               (const double*)inv_.get(), r0, x0, T(jacobiOmega_), (const SysState*)st_.get(), flag);
+}
+
+// Per system: the first level of the single-CTA tail = the first level (below level 0) whose
+// padded row count is at most kTailMaxRows (VLM_TAIL_ROWS overrides; VLM_TAIL=0 disables), else
+// the coarsest level alone.
+void DeviceBatch::planTail() {
+    const char* tv = std::getenv("VLM_TAIL");
+    if (tv && tv[0] == '0') return;
+    const int ns = plan_.nsys;
+    if (ns == 0) return;
+    int64_t maxRows = kTailMaxRows;
+    if (const char* mr = std::getenv("VLM_TAIL_ROWS")) maxRows = std::atoll(mr);
+    tailFirst_.assign(size_t(ns), 0);
+    std::vector<TailSys> ts(static_cast<size_t>(ns));
+    tailMaxFirst_ = 0;
+    for (int b = 0; b < ns; ++b) {
+        const int c = plan_.nLevels[b] - 1;
+        if (c >= kTailMaxLevels) throw Error(VLM_ERR_UNSUPPORTED, "GAMG hierarchy deeper than the coarse tail supports");
+        int first = c;
+        for (int k = 1; k < c; ++k)
+            if (int64_t(plan_.levels[k].sysRow[b + 1] - plan_.levels[k].sysRow[b]) <= maxRows) {
+                first = k;
+                break;
+            }
+        tailFirst_[b] = first;
+        tailMaxFirst_ = std::max(tailMaxFirst_, first);
+        TailSys& t = ts[b];
+        std::memset(&t, 0, sizeof t);
+        t.sys = b;
+        t.first = first;
+        t.coarsest = c;
+        const CoarsePlan& cp = plan_.coarse[b];
+        t.coarseN = cp.n;
+        t.invOffset = cp.invOffset;
+        for (int k = 0; k <= c; ++k) {
+            t.rowStart[k] = plan_.levels[k].sysRow[b];
+            t.rowCount[k] = plan_.levels[k].sysRow[b + 1] - plan_.levels[k].sysRow[b];
+        }
+        if (cp.rowStart != t.rowStart[c]) throw Error(VLM_ERR_CUDA, "internal: coarse-tail row mismatch");
+    }
+    tailSys_.upload(ts, stream_);
+    tailOn_ = true;
 }
 
 void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32) {
@@ -464,13 +604,24 @@ void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
     cudaStream_t s = stream_;
     const Chunk* ch = D0.ch(D0.all);
     const int nb = D0.all.n;
-    recordPrecond(pk, sm, r_.get(), w_.get(), f32);
-    VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, w_.get(), r_.get(), red(), st_.get());
-    VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
+    const bool v32 = f32 && pk == PrecondKind::GAMG;
+    if (v32) {
+        // FP32 V-cycle on r32 (written by the previous update / the initial residual); its FP32
+        // output feeds the dot and the direction update directly
+        recordVcycle<float>(r32_.get(), w32_.get(), sm, kFlagDone);
+        VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone, EXACT, float>), nb, kRowsPerCta, s, ch, w32_.get(), r_.get(), red(),
+                   st_.get());
+        VLM_LAUNCH((k_pcg_p<double, kFlagDone, float>), nb, kRowsPerCta, s, ch, w32_.get(), p_.get(), st_.get());
+    } else {
+        recordPrecond(pk, sm, r_.get(), w_.get(), f32);
+        VLM_LAUNCH((k_pcg_dot_wr<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, w_.get(), r_.get(), red(),
+                   st_.get());
+        VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
+    }
     VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(),
                p_.get(), Ap_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_update<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, x_.get(), r_.get(), p_.get(),
-               Ap_.get(), perm0_.get(), red(), st_.get(), dctrl_.get());
+               Ap_.get(), perm0_.get(), red(), st_.get(), dctrl_.get(), v32 ? r32_.get() : (float*)nullptr);
 }
 
 void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
@@ -490,7 +641,7 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
     VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), D0.diag32.get(),
                p32_.get(), Ap32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_update<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
-               Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get());
+               Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get(), (float*)nullptr);
 }
 
 void DeviceBatch::recordBicgIter(PrecondKind pk, SmootherKind sm, bool f32) {
@@ -572,6 +723,10 @@ cudaGraphNode_t addWhile(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditiona
 }  // namespace
 
 void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
+    struct CaptureScope {
+        CaptureScope() { tl_capturing = true; }
+        ~CaptureScope() { tl_capturing = false; }
+    } scope;
     VLM_CUDA(cudaGraphCreate(&G.graph, 0));
     cudaStream_t s = stream_;
     const int64_t saved = tl_launches;
@@ -700,26 +855,28 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     st_.zero(s);
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), b, b_.get());
+    exact_ = ctrl.reproducible != 0;
+    if (exact_ && xbins_.size() == 0) {
+        xbins_.resize(size_t(plan_.nSlots) * 2 * 73);
+        xbins_.zero(s);
+    }
+    // FP32 copy of the initial residual: the inner solve's RHS (mixed-dc) or the first FP32 V-cycle's input
+    const bool r32first = dc || (prec == Precision::MixedPrecond && sk == SolverKind::PCG && pk == PrecondKind::GAMG);
     if (exact_) {
         VLM_LAUNCH((k_sum_x<double, true>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
         VLM_LAUNCH(k_init_residual<true>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(),
-                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), dc ? r32_.get() : nullptr,
+                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), r32first ? r32_.get() : nullptr,
                    sysCells_.get(), red(), st_.get(), dctrl_.get());
     } else {
         VLM_LAUNCH((k_sum_x<double, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), x_.get(), red(), st_.get());
         VLM_LAUNCH(k_init_residual<false>, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(),
-                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), dc ? r32_.get() : nullptr,
+                   D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), r32first ? r32_.get() : nullptr,
                    sysCells_.get(), red(), st_.get(), dctrl_.get());
     }
     if (sk == SolverKind::PBiCGStab) {
         VLM_CUDA(cudaMemcpyAsync(r0_.get(), r_.get(), sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
         Ay_.zero(s);
         p_.zero(s);
-    }
-    exact_ = ctrl.reproducible != 0;
-    if (exact_ && xbins_.size() == 0) {
-        xbins_.resize(size_t(plan_.nSlots) * 2 * 73);
-        xbins_.zero(s);
     }
     const SolveKey key{sk, pk, sm, prec, exact_};
     int64_t eagerLaunches = 0;
@@ -838,12 +995,22 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
         run = [&] {
             for (int t = 0; t < D0.nSteps; ++t) {
                 if (f32)
-                    VLM_LAUNCH(k_smooth_gs<float>, D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val32.get(), D0.diag32.get(), r32_.get(), w32_.get(), st_.get(), kFlagDone);
+                    VLM_LAUNCH((k_smooth_gs<float, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val32.get(), D0.diag32.get(), r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr, st_.get(), kFlagDone);
                 else
-                    VLM_LAUNCH(k_smooth_gs<double>, D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), st_.get(), kFlagDone);
+                    VLM_LAUNCH((k_smooth_gs<double, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), (const int32_t*)nullptr, (const double*)nullptr, st_.get(), kFlagDone);
             }
         };
         *bytesPerLaunch = sz * 4 * N + sz * F + 8 * F;
+    } else if (name == "vcycle32" || name == "vcycle32_notail" || name == "tail32") {
+        const bool allow = name != "vcycle32_notail";
+        run = [&, allow, name] {
+            if (name == "tail32") {
+                if (tailOn_) recordTail<float>(r32_.get(), w32_.get(), kFlagDone);
+            } else {
+                recordVcycle<float>(r32_.get(), w32_.get(), SmootherKind::MCGSJacobi, kFlagDone, allow);
+            }
+        };
+        *bytesPerLaunch = 0;
     } else if (name == "residual64" || name == "residual32") {
         run = [&] {
             if (f32)
@@ -855,8 +1022,16 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
     } else {
         throw Error(VLM_ERR_BAD_ARG, "unknown kernel " + name);
     }
-    // st_ flags of a finished solve are 'done': clear them so the kernels do their work
+    // st_ flags of a finished solve are 'done': clear them so the kernels do their work.  The
+    // vectors are reset to one fixed state (right-hand side b, zero iterate) so the timing does
+    // not depend on what the last solve left in them.
     st_.zero(s);
+    if (r32_.size() == size_t(D0.nrows))
+        VLM_LAUNCH((k_cast_rows<double, float>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), b_.get(), r32_.get(),
+                   st_.get(), kFlagDone);
+    VLM_CUDA(cudaMemcpyAsync(r_.get(), b_.get(), sizeof(double) * size_t(D0.nrows), cudaMemcpyDeviceToDevice, s));
+    w_.zero(s);
+    if (w32_.size() == size_t(D0.nrows)) w32_.zero(s);
     run();
     VLM_CUDA(cudaEventRecord(e0, s));
     for (int i = 0; i < reps; ++i) run();
@@ -869,7 +1044,7 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
     return double(ms) / reps;
 }
 
-template void DeviceBatch::recordVcycle<double>(const double*, double*, SmootherKind, int);
-template void DeviceBatch::recordVcycle<float>(const float*, float*, SmootherKind, int);
+template void DeviceBatch::recordVcycle<double>(const double*, double*, SmootherKind, int, bool);
+template void DeviceBatch::recordVcycle<float>(const float*, float*, SmootherKind, int, bool);
 
 }  // namespace vlm

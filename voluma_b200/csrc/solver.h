@@ -25,6 +25,7 @@ struct DevLevel {
     DBuf<int32_t> slPtr, rlen, col, src;
     DBuf<Chunk> chunks;
     ChunkList active, all;
+    ChunkList headActive, headIn;  // coarse-tail mode: rows above each system's tail / restricted into
     std::vector<ChunkList> fwd, rev;
     DBuf<int32_t> agg, childPtr, child, intraPtr, intraFace, cfacePtr, cfaceSrc;
     ChunkList coarse;  // CoarseDev entries whose coarsest level is this one
@@ -101,8 +102,11 @@ public:
 
 
 private:
-    template <class T> void recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag);
-    template <class T> void recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag);
+    template <class T> void recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bool allowTail = true);
+    template <class T> void recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag, bool head);
+    template <class T> void recordTail(const T* r0, T* x0, int flag);
+    template <class T> void buildTailTable(DBuf<TailLevel<T>>& out);
+    void planTail();
     void recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32);
     void recordIter(const SolveKey& key);
     void runEager(const SolveKey& key, int maxIter);
@@ -135,8 +139,16 @@ private:
     std::map<SolveKey, std::unique_ptr<GraphExec>> graphs_;
     std::vector<SysState> hostState_;
     double jacobiOmega_ = 1.0;
+    // coarse tail: levels tailFirst_[b].. of system b run in one CTA (Jacobi coarse levels)
+    bool tailOn_ = false;
+    int tailMaxFirst_ = 0;      // head levels: k < tailMaxFirst_
+    std::vector<int> tailFirst_;
+    DBuf<TailSys> tailSys_;
+    DBuf<TailLevel<double>> tail64_;
+    DBuf<TailLevel<float>> tail32_;
     int64_t launches_ = 0;
     bool useGraphs_ = true;
+
 };
 
 // Exact (order-independent) sum of n device doubles, ordered on stream s.
