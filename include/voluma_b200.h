@@ -15,6 +15,8 @@
  *                            LinearSolver.cpp:135-284)
  *   vlm_amul              <- void amul(const LduSystem&, x, y)  (LinearSolver.h:45, .cpp:121-133)
  *   vlm_gamg_apply        <- GamgPreconditioner::apply           (src/fvm/linalg/GAMG.h:63, .cpp:445)
+ *   vlm_precond_apply     <- Preconditioner ctor + apply (none/diagonal/DIC/DILU/GAMG)
+ *                            (src/fvm/linalg/LinearSolver.cpp:56-107)
  *   vlm_gamg_levels/_level<- buildHierarchy                      (GAMG.h:57, GAMG.cpp:206-261)
  *   vlm_laplacian         <- fvm::laplacian(gamma, psi, nonOrthCorr) (src/fvm/discretization/Fvm.h:141-182)
  *   vlm_grad              <- fvc::grad (Gauss linear / leastSquares) (src/fvm/discretization/Fvc.h:209-291)
@@ -144,6 +146,12 @@ vlm_status vlm_ldu_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag
 /* One GAMG V-cycle w = M^-1 r with the device smoother named in ctrl (host pointers). */
 vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
                           const double* lower, const double* r, double* w, const vlm_solver_ctrl* ctrl);
+
+/* w = M^-1 r with the preconditioner named in ctrl->preconditioner: "none", "diagonal", "DIC",
+ * "DILU" (natural-order factorisation and sweeps, level-scheduled on the device) or "GAMG"
+ * (= vlm_gamg_apply).  Host pointers. */
+vlm_status vlm_precond_apply(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,
+                             const double* lower, const double* r, double* w, const vlm_solver_ctrl* ctrl);
 
 /* Hierarchy introspection (for parity checks): number of levels, then per level sizes
  * {n, nFaces} and optional copies of l/u (nFaces), agg (n, empty on the coarsest level). */

@@ -43,6 +43,9 @@ def lib():
         L.vo_gamg_apply.argtypes = [C.c_int, C.c_int, P, P, P, P, P, P, P, P, P, C.POINTER(GamgOpts)]
         L.vo_solve.argtypes = [C.c_int, C.c_int, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_char_p, C.c_double,
                                C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(GamgOpts), P]
+        L.vo_solve_ex.argtypes = [C.c_int, C.c_int, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_char_p, C.c_double,
+                                  C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(GamgOpts), P]
+        L.vo_precond_apply.argtypes = [C.c_int, C.c_int, P, P, P, P, P, C.c_char_p, P, P]
         _lib = L
     return _lib
 
@@ -116,17 +119,28 @@ def gamg_apply(m, diag, upper, lower, r, smoother="gs", omega=1.0, coarse=0, mer
 
 
 def solve(m, diag, upper, lower, b, x0, solver="PCG", precond="diagonal", tol=0.0, rel_tol=1e-8, max_iter=1000,
-          min_iter=0, exact=False, smoother="gs", omega=1.0, coarse=0, merge=2):
-    """solveLdu restated. Returns (x, perf dict)."""
+          min_iter=0, exact=False, smoother="gs", omega=1.0, coarse=0, merge=2, n_sweeps=1):
+    """solveLdu restated (PCG, PBiCGStab, GaussSeidel, symGaussSeidel, Jacobi). Returns (x, perf dict)."""
     nI = len(m["neighbour"])
     x = np.ascontiguousarray(x0, np.float64).copy()
     perf = np.zeros(6)
     o = opts(smoother, omega, coarse, merge)
-    st = lib().vo_solve(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(m["magSf"])),
-                        _p(_d(m["ndc"])), _p(_d(diag)), _p(_d(upper)), _p(_d(lower)), _p(_d(b)), _p(x),
-                        solver.encode(), precond.encode(), tol, rel_tol, max_iter, min_iter, int(exact), C.byref(o),
-                        _p(perf))
+    st = lib().vo_solve_ex(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(m["magSf"])),
+                           _p(_d(m["ndc"])), _p(_d(diag)), _p(_d(upper)), _p(_d(lower)), _p(_d(b)), _p(x),
+                           solver.encode(), precond.encode(), tol, rel_tol, max_iter, min_iter, n_sweeps, int(exact),
+                           C.byref(o), _p(perf))
     if st:
         raise RuntimeError(f"oracle solve status {st}")
     return x, dict(initialResidual=perf[0], finalResidual=perf[1], residualSum=perf[2], normFactor=perf[3],
                    iterations=int(perf[4]), converged=bool(perf[5]))
+
+
+def precond_apply(m, diag, upper, lower, r, precond="DILU"):
+    """w = M^-1 r for none / diagonal / DIC / DILU (Preconditioner, linalg/LinearSolver.cpp:56-107)."""
+    nI = len(m["neighbour"])
+    w = np.zeros(m["n_cells"])
+    st = lib().vo_precond_apply(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(diag)),
+                                _p(_d(upper)), _p(_d(lower)), precond.encode(), _p(_d(r)), _p(w))
+    if st:
+        raise RuntimeError(f"oracle precond_apply status {st}")
+    return w

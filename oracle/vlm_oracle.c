@@ -715,13 +715,112 @@ int vo_gamg_apply(int n, int nf, const int* own, const int* nei, const double* m
     return st;
 }
 
+/* ======================================================================= DIC / DILU */
+/* Faces of the DIC/DILU sweeps (LinearSolver.cpp:28-50): internal faces between two distinct
+ * cells, (l, u) = (min, max), sorted by (u, l, face). */
+typedef struct {
+    int n, m;
+    int *face, *l, *u;
+    unsigned char* ownerIsL;
+    double* rD;
+} dilu_t;
+
+static int cmp_ulf(const void* a, const void* b) {
+    const int* x = (const int*)a;
+    const int* y = (const int*)b;
+    for (int q = 0; q < 3; ++q)
+        if (x[q] != y[q]) return x[q] < y[q] ? -1 : 1;
+    return 0;
+}
+
+/* LinearSolver.cpp:66-77: rD[u] -= A_lu A_ul / rD[l] over the sorted faces, then rD = 1 / rD */
+static void dilu_init(dilu_t* P, int n, int nf, const int* own, const int* nei, const double* diag,
+                      const double* upper, const double* lower) {
+    int* t = (int*)malloc(sizeof(int) * 3 * (size_t)(nf > 0 ? nf : 1));
+    int m = 0;
+    for (int f = 0; f < nf; ++f) {
+        const int o = own[f], q = nei[f];
+        if (o >= n || q >= n || o == q) continue;
+        t[3 * m] = o > q ? o : q;
+        t[3 * m + 1] = o < q ? o : q;
+        t[3 * m + 2] = f;
+        ++m;
+    }
+    qsort(t, (size_t)m, sizeof(int) * 3, cmp_ulf);
+    P->n = n;
+    P->m = m;
+    P->face = (int*)malloc(sizeof(int) * (size_t)(m + 1));
+    P->l = (int*)malloc(sizeof(int) * (size_t)(m + 1));
+    P->u = (int*)malloc(sizeof(int) * (size_t)(m + 1));
+    P->ownerIsL = (unsigned char*)malloc((size_t)(m + 1));
+    P->rD = (double*)malloc(sizeof(double) * (size_t)(n + 1));
+    for (int k = 0; k < m; ++k) {
+        P->u[k] = t[3 * k];
+        P->l[k] = t[3 * k + 1];
+        P->face[k] = t[3 * k + 2];
+        P->ownerIsL[k] = own[P->face[k]] == P->l[k];
+    }
+    free(t);
+    for (int c = 0; c < n; ++c) P->rD[c] = diag[c];
+    for (int k = 0; k < m; ++k) {
+        const int f = P->face[k];
+        const double Alu = P->ownerIsL[k] ? upper[f] : lower[f];
+        const double Aul = P->ownerIsL[k] ? lower[f] : upper[f];
+        P->rD[P->u[k]] -= Alu * Aul / P->rD[P->l[k]];
+    }
+    for (int c = 0; c < n; ++c) P->rD[c] = 1.0 / P->rD[c];
+}
+
+/* LinearSolver.cpp:87-106: w = rD r, forward and backward substitution over the sorted faces */
+static void dilu_apply(const dilu_t* P, const double* upper, const double* lower, const double* r, double* w) {
+    for (int c = 0; c < P->n; ++c) w[c] = P->rD[c] * r[c];
+    for (int k = 0; k < P->m; ++k) {
+        const int f = P->face[k];
+        const double Aul = P->ownerIsL[k] ? lower[f] : upper[f];
+        w[P->u[k]] -= P->rD[P->u[k]] * Aul * w[P->l[k]];
+    }
+    for (int k = P->m; k-- > 0;) {
+        const int f = P->face[k];
+        const double Alu = P->ownerIsL[k] ? upper[f] : lower[f];
+        w[P->l[k]] -= P->rD[P->l[k]] * Alu * w[P->u[k]];
+    }
+}
+
+static void dilu_free(dilu_t* P) {
+    free(P->face);
+    free(P->l);
+    free(P->u);
+    free(P->ownerIsL);
+    free(P->rD);
+}
+
+int vo_precond_apply(int n, int nf, const int* own, const int* nei, const double* diag, const double* upper,
+                     const double* lower, const char* precond, const double* r, double* w) {
+    if (!lower) lower = upper;
+    if (strcmp(precond, "none") == 0) {
+        memcpy(w, r, sizeof(double) * (size_t)n);
+    } else if (strcmp(precond, "diagonal") == 0) {
+        for (int c = 0; c < n; ++c) w[c] = 1.0 / diag[c] * r[c];
+    } else if (strcmp(precond, "DIC") == 0 || strcmp(precond, "DILU") == 0) {
+        dilu_t P;
+        dilu_init(&P, n, nf, own, nei, diag, upper, lower);
+        dilu_apply(&P, upper, lower, r, w);
+        dilu_free(&P);
+    } else {
+        return 7;
+    }
+    return 0;
+}
+
 /* ======================================================================= solveLdu */
 typedef struct {
-    int kind; /* 0 none, 1 diagonal, 2 GAMG */
+    int kind; /* 0 none, 1 diagonal, 2 GAMG, 3 DIC/DILU */
     int n;
     double* rD;
     gamg_t g;
     vo_hier* H;
+    dilu_t d;
+    const double *up, *lo;
 } prec_t;
 
 static void prec_apply(prec_t* P, const double* r, double* w) {
@@ -729,6 +828,8 @@ static void prec_apply(prec_t* P, const double* r, double* w) {
         memcpy(w, r, sizeof(double) * (size_t)P->n);
     } else if (P->kind == 1) {
         for (int c = 0; c < P->n; ++c) w[c] = P->rD[c] * r[c];
+    } else if (P->kind == 3) {
+        dilu_apply(&P->d, P->up, P->lo, r, w);
     } else {
         gamg_vcycle(&P->g, 0, r, P->g.xb[0]);
         memcpy(w, P->g.xb[0], sizeof(double) * (size_t)P->n);
@@ -740,25 +841,62 @@ static int converged(double tol, double relTol, int minIter, int iters, double f
     return fin < tol || (relTol > 0 && fin < relTol * init);
 }
 
+/* sweepCell of LinearSolver.cpp:245-259: the cell's faces in cellFaces order (ascending face,
+ * a face listed twice when both its sides are the cell, Mesh.cpp:630-641) */
+static double sweep_cell(int c, const int* cfOff, const int* cf, const int* own, const int* nei, const double* diag,
+                         const double* upper, const double* lower, const double* b, const double* xs) {
+    double r = b[c];
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = cf[k];
+        if (own[f] == c && nei[f] == c)
+            r -= (upper[f] + lower[f]) * xs[c];
+        else if (own[f] == c)
+            r -= upper[f] * xs[nei[f]];
+        else
+            r -= lower[f] * xs[own[f]];
+    }
+    return r / diag[c];
+}
+
 int vo_solve(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
              const double* diag, const double* upper, const double* lower, const double* b, double* x,
              const char* solver, const char* precond, double tol, double relTol, int maxIter, int minIter,
              int exactSums, const vo_gamg_opts* opt, double* perf) {
+    return vo_solve_ex(n, nf, own, nei, magSf, ndc, diag, upper, lower, b, x, solver, precond, tol, relTol, maxIter,
+                       minIter, 1, exactSums, opt, perf);
+}
+
+int vo_solve_ex(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
+                const double* diag, const double* upper, const double* lower, const double* b, double* x,
+                const char* solver, const char* precond, double tol, double relTol, int maxIter, int minIter,
+                int nSweeps, int exactSums, const vo_gamg_opts* opt, double* perf) {
     const int sym = lower == NULL || lower == upper;
     if (!lower) lower = upper;
     const int pcg = strcmp(solver, "PCG") == 0;
     const int bicg = strcmp(solver, "PBiCGStab") == 0;
-    if (!pcg && !bicg) return 7;
+    int gs = strcmp(solver, "GaussSeidel") == 0, sgs = strcmp(solver, "symGaussSeidel") == 0;
+    int jac = strcmp(solver, "Jacobi") == 0;
+    if (!pcg && !bicg && !gs && !sgs && !jac) return 7;
     if (pcg && !sym) return 7;
+    if (exactSums && (gs || sgs)) { /* CFD_REPRODUCIBLE swap, LinearSolver.cpp:141 */
+        gs = sgs = 0;
+        jac = 1;
+    }
+    const int relax = gs || sgs || jac;
+    if (relax && nSweeps < 1) return 1;
     prec_t P;
     memset(&P, 0, sizeof P);
     P.n = n;
-    if (strcmp(precond, "none") == 0)
+    P.up = upper;
+    P.lo = lower;
+    if (relax || strcmp(precond, "none") == 0)
         P.kind = 0;
     else if (strcmp(precond, "diagonal") == 0)
         P.kind = 1;
     else if (strcmp(precond, "GAMG") == 0)
         P.kind = 2;
+    else if (strcmp(precond, "DIC") == 0 || strcmp(precond, "DILU") == 0)
+        P.kind = 3;
     else
         return 7;
     if (exactSums && P.kind != 0) P.kind = 1; /* CFD_REPRODUCIBLE swap, LinearSolver.cpp:138-148 */
@@ -789,8 +927,48 @@ int vo_solve(int n, int nf, const int* own, const int* nei, const double* magSf,
         } else if (P.kind == 2) {
             P.H = vo_hier_build(n, nf, own, nei, magSf, ndc, opt->mergeLevels ? opt->mergeLevels : 2, 64);
             status = gamg_init(&P.g, P.H, diag, upper, lower, opt);
+        } else if (P.kind == 3) {
+            dilu_init(&P.d, n, nf, own, nei, diag, upper, lower);
         }
-        if (status == 0 && pcg) {
+        if (status == 0 && relax) {
+            /* LinearSolver.cpp:238-278 */
+            int* cfOff = (int*)calloc((size_t)n + 1, sizeof(int));
+            for (int f = 0; f < nf; ++f) {
+                if (own[f] < n) ++cfOff[own[f] + 1];
+                if (nei[f] < n) ++cfOff[nei[f] + 1];
+            }
+            for (int c = 0; c < n; ++c) cfOff[c + 1] += cfOff[c];
+            int* cf = (int*)malloc(sizeof(int) * (size_t)(cfOff[n] + 1));
+            int* fill = (int*)malloc(sizeof(int) * (size_t)(n + 1));
+            for (int c = 0; c < n; ++c) fill[c] = cfOff[c];
+            for (int f = 0; f < nf; ++f) {
+                if (own[f] < n) cf[fill[own[f]]++] = f;
+                if (nei[f] < n) cf[fill[nei[f]]++] = f;
+            }
+            double* xOld = (double*)malloc(sizeof(double) * (size_t)(n + 1));
+            do {
+                for (int sw = 0; sw < nSweeps; ++sw) {
+                    if (jac) {
+                        memcpy(xOld, x, sizeof(double) * (size_t)n);
+                        for (int c = 0; c < n; ++c)
+                            x[c] = sweep_cell(c, cfOff, cf, own, nei, diag, upper, lower, b, xOld);
+                    } else {
+                        for (int c = 0; c < n; ++c) x[c] = sweep_cell(c, cfOff, cf, own, nei, diag, upper, lower, b, x);
+                        if (sgs)
+                            for (int c = n; c-- > 0;)
+                                x[c] = sweep_cell(c, cfOff, cf, own, nei, diag, upper, lower, b, x);
+                    }
+                }
+                it += nSweeps;
+                vo_amul(n, nf, own, nei, diag, upper, lower, x, wA);
+                for (int c = 0; c < n; ++c) rA[c] = b[c] - wA[c];
+                fin = gSumMag(rA, n, exactSums) / normFactor;
+            } while (it < maxIter && !converged(tol, relTol, minIter, it, fin, init));
+            free(cfOff);
+            free(cf);
+            free(fill);
+            free(xOld);
+        } else if (status == 0 && pcg) {
             double* w = (double*)calloc((size_t)n + 1, sizeof(double));
             double* p = (double*)calloc((size_t)n + 1, sizeof(double));
             double wArA = GREAT, wArAold;
@@ -871,6 +1049,7 @@ int vo_solve(int n, int nf, const int* own, const int* nei, const double* magSf,
             gamg_free(&P.g);
             vo_hier_free(P.H);
         }
+        if (P.kind == 3) dilu_free(&P.d);
         free(P.rD);
     }
     perf[0] = init;

@@ -61,6 +61,18 @@ int vo_solve(int n, int nf, const int* own, const int* nei, const double* magSf,
              const char* solver, const char* precond, double tol, double relTol, int maxIter, int minIter,
              int exactSums, const vo_gamg_opts* opt, double* perf);
 
+/* vo_solve with the relaxation solvers GaussSeidel / symGaussSeidel / Jacobi (nSweeps sweeps per
+ * residual evaluation, LinearSolver.cpp:238-278) and the DIC / DILU preconditioners
+ * (LinearSolver.cpp:56-107).  Returns 1 for nSweeps < 1 with a relaxation solver. */
+int vo_solve_ex(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
+                const double* diag, const double* upper, const double* lower, const double* b, double* x,
+                const char* solver, const char* precond, double tol, double relTol, int maxIter, int minIter,
+                int nSweeps, int exactSums, const vo_gamg_opts* opt, double* perf);
+
+/* w = M^-1 r for "none", "diagonal", "DIC", "DILU" (Preconditioner, LinearSolver.cpp:56-107). */
+int vo_precond_apply(int n, int nf, const int* own, const int* nei, const double* diag, const double* upper,
+                     const double* lower, const char* precond, const double* r, double* w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,7 +4,8 @@ Run in a checkout where the reference sources are present:  make -C oracle && py
 tests/golden/make_golden.py.  Every array comes from the unmodified reference compiled from its
 own sources (oracle/_ref/libvlmref.so through oracle/ref_driver.cpp): generateBox + Mesh::build
 meshes, the LDU pressure matrix of fvm::laplacian(1, p) + setReference(0), and the results of
-solveLdu (PCG/diagonal in CFD_REPRODUCIBLE mode and plain, PCG/GAMG, PBiCGStab/diagonal),
+solveLdu (PCG/diagonal in CFD_REPRODUCIBLE mode and plain, PCG/GAMG, PBiCGStab/diagonal,
+PBiCGStab/DILU, PCG/DIC, GaussSeidel, symGaussSeidel, Jacobi),
 one GamgPreconditioner::apply, buildHierarchy, amul and ExactSum.  The fixtures are small
 (each case < 0.5 MB) so the CPU tests load them in milliseconds.
 """
@@ -75,6 +76,19 @@ def make(name, spec):
     }
     for key, (d, u, l, solver, prec, repro) in runs.items():
         x, perf = R.solve(d, u, l, b, x0, solver, prec, 0.0, 1e-8, 2000, reproducible=repro)
+        out[key + "_x"] = x
+        out[key + "_perf"] = np.array([perf["initialResidual"], perf["finalResidual"], perf["residualSum"],
+                                       perf["normFactor"], perf["iterations"], perf["converged"]])
+    # DIC / DILU and the relaxation solvers (LinearSolver.cpp:56-112, 238-278)
+    runs2 = {
+        "bicg_dilu": (lower, "PBiCGStab", "DILU", 1e-8, 2000, 1),
+        "pcg_dic": (None, "PCG", "DIC", 1e-8, 2000, 1),
+        "gs": (None, "GaussSeidel", "none", 1e-3, 300, 2),
+        "sgs": (lower, "symGaussSeidel", "none", 1e-3, 300, 1),
+        "jac": (None, "Jacobi", "none", 1e-3, 300, 3),
+    }
+    for key, (l, solver, prec, rtol, mx, nsw) in runs2.items():
+        x, perf = R.solve(diag, upper, l, b, x0, solver, prec, 0.0, rtol, mx, n_sweeps=nsw)
         out[key + "_x"] = x
         out[key + "_perf"] = np.array([perf["initialResidual"], perf["finalResidual"], perf["residualSum"],
                                        perf["normFactor"], perf["iterations"], perf["converged"]])

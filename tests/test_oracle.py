@@ -59,6 +59,35 @@ def test_solve_golden(golden, key, solver, prec, exact, asym):
     assert perf == ref_perf
 
 
+@pytest.mark.parametrize("key,solver,prec,asym,rtol,max_iter,sweeps", [
+    ("bicg_dilu", "PBiCGStab", "DILU", True, 1e-8, 2000, 1),
+    ("pcg_dic", "PCG", "DIC", False, 1e-8, 2000, 1),
+    ("gs", "GaussSeidel", "none", False, 1e-3, 300, 2),
+    ("sgs", "symGaussSeidel", "none", True, 1e-3, 300, 1),
+    ("jac", "Jacobi", "none", False, 1e-3, 300, 3),
+])
+def test_dilu_and_relaxation_golden(golden, key, solver, prec, asym, rtol, max_iter, sweeps):
+    """DIC/DILU (LinearSolver.cpp:56-107) and GaussSeidel/symGaussSeidel/Jacobi (:238-278) restated:
+    the reference's solutions, residuals and iteration counts bit for bit."""
+    lower = golden["lower_asym"] if asym else None
+    x, perf = ro.solve(golden, golden["diag"], golden["upper"], lower, golden["b"], golden["x0"], solver, prec,
+                       0.0, rtol, max_iter, n_sweeps=sweeps)
+    assert np.array_equal(x, golden[key + "_x"])
+    assert perf == perf_dict(golden[key + "_perf"])
+
+
+def test_precond_apply_properties(golden):
+    """DILU on a symmetric matrix is DIC; M^-1 applied to M-products: w = M^-1 r is linear."""
+    g = golden
+    r = g["b"]
+    w1 = ro.precond_apply(g, g["diag"], g["upper"], None, r, "DIC")
+    assert np.array_equal(w1, ro.precond_apply(g, g["diag"], g["upper"], g["upper"], r, "DILU"))
+    w2 = ro.precond_apply(g, g["diag"], g["upper"], None, 2.0 * r, "DIC")
+    assert np.allclose(w2, 2.0 * w1, rtol=1e-13, atol=0)
+    wd = ro.precond_apply(g, g["diag"], g["upper"], None, r, "diagonal")
+    assert np.array_equal(wd, 1.0 / g["diag"] * r)
+
+
 def test_oracle_live_against_reference():
     """Fresh random inputs through both the reference build and the restatement."""
     ref = pytest.importorskip("oracle.ref")

@@ -422,6 +422,16 @@ def amul(mesh: Mesh, diag, upper, lower, x):
     return y
 
 
+def precond_apply(mesh: Mesh, diag, upper, lower, r, preconditioner: str = "DILU", smoother: str = ""):
+    """w = M^-1 r (Preconditioner ctor + apply, LinearSolver.cpp:56-107): none, diagonal, DIC, DILU, GAMG."""
+    w = np.zeros(mesh.n_cells)
+    c = SolverControls(preconditioner=preconditioner, smoother=smoother).to_c()
+    check(load().vlm_precond_apply(mesh.ctx.handle, mesh.handle, _ptr(_f64(diag)), _ptr(_f64(upper)),
+                                   None if lower is None else _ptr(_f64(lower)), _ptr(_f64(r)), _ptr(w), C.byref(c)),
+          mesh.ctx.handle)
+    return w
+
+
 def gamg_apply(mesh: Mesh, diag, upper, lower, r, smoother: str = ""):
     """One device V-cycle w = M^-1 r."""
     w = np.zeros(mesh.n_cells)

@@ -16,7 +16,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
-           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc"]
+           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply"]
 
 
 class MeshDesc(C.Structure):
@@ -65,6 +65,7 @@ def load():
     L.vlm_ldu_solve.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]
     L.vlm_ldu_solve_device.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]
     L.vlm_gamg_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
+    L.vlm_precond_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
     L.vlm_gamg_levels.argtypes = [P, C.POINTER(i32)]
     L.vlm_gamg_level.argtypes = [P, i32, P, P, P, P]
     L.vlm_gamg_colours.argtypes = [P, i32, C.POINTER(i32)]

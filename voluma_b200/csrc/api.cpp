@@ -331,6 +331,20 @@ vlm_status vlm_gamg_apply(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const d
     });
 }
 
+vlm_status vlm_precond_apply(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const double* upper, const double* lower,
+                             const double* r, double* w, const vlm_solver_ctrl* ctrl) {
+    if (!ctx || !m || !r || !w || !ctrl) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        const double *dd, *du, *dl;
+        stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
+        m->b.upload(r, size_t(m->nCells), ctx->stream);
+        m->x.resize(size_t(m->nCells));
+        m->batch->precondApply(dd, du, dl, m->b.get(), m->x.get(), *ctrl);
+        VLM_CUDA(cudaMemcpy(w, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost));
+    });
+}
+
 vlm_status vlm_gamg_levels(vlm_mesh* m, int32_t* n) {
     if (!m || !n) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
     *n = int32_t(hierOf(m).levels.size());

@@ -1,0 +1,42 @@
+// Level schedule of the DIC/DILU preconditioner (LinearSolver.cpp:28-112) on the device.
+//
+// The reference factorises and applies DILU in natural cell order over the faces sorted by
+// (upper cell, lower cell): rD[u] -= A_lu A_ul / rD[l], then a forward sweep
+// w[u] -= rD[u] A_ul w[l] and a backward sweep w[l] -= rD[l] A_lu w[u].  Each is a recurrence
+// along the natural-order dependency graph (l -> u for every face), so rows can be updated in
+// parallel exactly when they sit on the same level of that graph: level[u] = 1 + max level[l]
+// over its lower neighbours.  Inside a row the terms are applied in the reference's order
+// (forward: lower neighbours by ascending (l, face); backward: upper neighbours by descending
+// (u, face)), so the device result is the reference's, bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "plan.h"
+
+namespace vlm {
+
+// One system's part of the schedule (batch position `sys`): levels [levBegin, levBegin + nLev) of
+// the concatenated level table.
+struct DiluSys {
+    int sys, levBegin, nLev, pad;
+};
+
+struct DiluPlan {
+    // per level-0 row (solver order): lower neighbours (forward order) and upper neighbours
+    // (backward order); face = user face index | ownerIsL << 31
+    std::vector<int32_t> loPtr, loCol, loFace;
+    std::vector<int32_t> upPtr, upCol, upFace;
+    // level schedule: levPtr[levBegin + t] .. levPtr[levBegin + t + 1] index levRows (solver rows);
+    // padding rows are on level 0 of their system
+    std::vector<int32_t> levPtr, levRows;
+    std::vector<DiluSys> sys;
+    int maxWidth = 0;  // widest level over all systems
+    int maxLevels = 0;
+};
+
+// systems: input order; P: the batch plan (solver order, perm0).
+DiluPlan buildDiluPlan(const std::vector<SysTopo>& systems, const BatchPlan& P);
+
+}  // namespace vlm

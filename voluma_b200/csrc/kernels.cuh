@@ -472,13 +472,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __re
                                                                const T* __restrict__ xc, const SysState* st, int flag) {
     pdl_entry();
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    if (MODE == 1) {
-        const T v = r[row] / diag[row];
-        xo[row] = omega == T(1) ? v : omega * v;
-        return;
-    }
+    if (chunk_skip(c, st, flag)) return;
     auto xv = [&](int j) -> T {
         T v = __ldg(xi + j);
         if (MODE == 2) {
@@ -487,13 +481,21 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __re
         }
         return v;
     };
-    const T s = row_accumulate<true>(S, val, xv, row, r[row]);
-    const T v = s / diag[row];
-    if (omega == T(1)) {
-        xo[row] = v;
-    } else {
-        const T x0 = xv(row);
-        xo[row] = x0 + omega * (v - x0);
+    // chunks of up to kRowsPerCta rows (one pass), or wider level-0 chunks (strided)
+    for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) {
+        if (MODE == 1) {
+            const T v = r[row] / diag[row];
+            xo[row] = omega == T(1) ? v : omega * v;
+            continue;
+        }
+        const T s = row_accumulate<true>(S, val, xv, row, r[row]);
+        const T v = s / diag[row];
+        if (omega == T(1)) {
+            xo[row] = v;
+        } else {
+            const T x0 = xv(row);
+            xo[row] = x0 + omega * (v - x0);
+        }
     }
 }
 

@@ -12,10 +12,22 @@
 #include <set>
 #include <utility>
 
+#include "dilu.cuh"
 #include "krylov.cuh"
 #include "solver.h"
 
 namespace vlm {
+
+// Device copy of the level schedule (dilu.h) and the per-solve DIC/DILU arrays.
+struct DiluDev {
+    DBuf<int32_t> loPtr, loCol, loFace, upPtr, upCol, upFace, levPtr, levRows;
+    DBuf<DiluSys> sys;
+    DBuf<double> loAul, loAlu, upAlu, rD;
+    DBuf<DiluBar> bars;
+    DBuf<int> err;
+    int G = 1, groups = 0, nFaces = 0;
+};
+
 
 GraphExec::~GraphExec() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -133,7 +145,7 @@ std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
 
 // ====================================================================== construction
 DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
-    : stream_(stream) {
+    : stream_(stream), topo_(systems) {
     plan_ = buildPlan(systems, mergeLevels);
     const char* gv = std::getenv("VLM_GRAPH");
     useGraphs_ = !(gv && gv[0] == '0');
@@ -330,6 +342,8 @@ RedCtx DeviceBatch::red() const {
 // ====================================================================== per-solve setup
 void DeviceBatch::setupMatrix(const double* diag, const double* upper, const double* lower, bool gamg, bool mixed) {
     cudaStream_t s = stream_;
+    curUpper_ = upper;
+    curLower_ = lower;
     DevLevel& D0 = L_[0];
     VLM_LAUNCH(k_gather_diag0<double>, nblk(D0.nrows), 256, s, D0.nrows, perm0_.get(), diag, D0.diag.get());
     if (mixed) VLM_LAUNCH(k_gather_diag0<float>, nblk(D0.nrows), 256, s, D0.nrows, perm0_.get(), diag, D0.diag32.get());
@@ -549,6 +563,8 @@ void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r
     case PrecondKind::None:
         VLM_LAUNCH(k_copy_rows<double>, D0.all.n, kRowsPerCta, stream_, D0.ch(D0.all), r, w, st_.get(), kFlagDone);
         break;
+    case PrecondKind::DIC:
+    case PrecondKind::DILU: recordDiluApply(r, w); break;
     default: throw Error(VLM_ERR_UNSUPPORTED, "preconditioner not available on the device");
     }
 }
@@ -558,8 +574,10 @@ void DeviceBatch::recordIter(const SolveKey& key) {
     const bool f32 = key.prec == Precision::MixedPrecond;
     if (key.solver == SolverKind::PCG)
         recordPcgIter(key.precond, key.smoother, f32);
-    else
+    else if (key.solver == SolverKind::PBiCGStab)
         recordBicgIter(key.precond, key.smoother, f32);
+    else
+        recordRelaxIter(key);
 }
 
 // Eager iteration loop (no graph): same kernels launched directly, convergence read back per
@@ -671,6 +689,133 @@ void DeviceBatch::recordBicgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
                s_.get(), red(), st);
     VLM_LAUNCH(k_bicg_update<EXACT>, nb, kRowsPerCta, s, ch, x_.get(), r_.get(), y_.get(), z_.get(), s_.get(), t_.get(), red(),
                st, dctrl_.get());
+}
+
+// ====================================================================== level-scheduled paths
+void DeviceBatch::ensureDilu() {
+    if (dilu_) return;
+    const DiluPlan P = buildDiluPlan(topo_, plan_);
+    auto D = std::make_unique<DiluDev>();
+    cudaStream_t s = stream_;
+    D->loPtr.upload(P.loPtr, s);
+    D->loCol.upload(P.loCol, s);
+    D->loFace.upload(P.loFace, s);
+    D->upPtr.upload(P.upPtr, s);
+    D->upCol.upload(P.upCol, s);
+    D->upFace.upload(P.upFace, s);
+    D->levPtr.upload(P.levPtr, s);
+    D->levRows.upload(P.levRows, s);
+    D->sys.upload(P.sys, s);
+    D->nFaces = int(P.loCol.size());
+    const size_t nf = size_t(std::max(D->nFaces, 1));
+    D->loAul.resize(nf);
+    D->loAlu.resize(nf);
+    D->upAlu.resize(nf);
+    D->rD.resize(size_t(L_[0].nrows));
+    D->groups = int(P.sys.size());
+    // one CTA per system; a single wide system gets a co-resident group of CTAs
+    D->G = 1;
+    if (D->groups == 1 && P.maxWidth > 2 * kDiluThreads) {
+        int dev = 0, sms = 0, per = 0;
+        VLM_CUDA(cudaGetDevice(&dev));
+        VLM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dilu_apply, kDiluThreads, 0));
+        int perF = 0, perG = 0;
+        VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perF, k_dilu_factor, kDiluThreads, 0));
+        VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perG, k_gs_sweep, kDiluThreads, 0));
+        const int resident = sms * std::max(1, std::min(per, std::min(perF, perG)));
+        D->G = std::max(1, std::min({(P.maxWidth + kDiluThreads - 1) / kDiluThreads, resident, sms}));
+    }
+    D->bars.resize(size_t(D->groups));
+    D->bars.zero(s);
+    D->err.resize(1);
+    D->err.zero(s);
+    VLM_CUDA(cudaStreamSynchronize(s));
+    dilu_ = std::move(D);
+}
+
+namespace {
+// Launch of a level-scheduled kernel: groups x G CTAs, cooperative when a group spans CTAs.
+template <class... Exp, class... Act>
+void launchLevels(void (*kernel)(Exp...), int groups, int G, cudaStream_t s, Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(groups * G));
+    cfg.blockDim = dim3(unsigned(kDiluThreads));
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = G > 1 ? 1 : 0;
+    VLM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
+    ++tl_launches;
+}
+}  // namespace
+
+void DeviceBatch::diluFactor(const double* upper, const double* lower) {
+    DiluDev& Dd = *dilu_;
+    cudaStream_t s = stream_;
+    VLM_LAUNCH(k_dilu_values, nblk(Dd.nFaces), 256, s, Dd.nFaces, (const int32_t*)Dd.loFace.get(),
+               (const int32_t*)Dd.upFace.get(), upper, lower, Dd.loAul.get(), Dd.loAlu.get(), Dd.upAlu.get());
+    launchLevels(k_dilu_factor, Dd.groups, Dd.G, s, (const DiluSys*)Dd.sys.get(), Dd.G, (const int32_t*)Dd.levPtr.get(),
+                 (const int32_t*)Dd.levRows.get(), (const int32_t*)Dd.loPtr.get(), (const int32_t*)Dd.loCol.get(),
+                 (const double*)Dd.loAlu.get(), (const double*)Dd.loAul.get(), (const double*)L_[0].diag.get(),
+                 Dd.rD.get(), Dd.bars.get(), Dd.err.get());
+}
+
+// A group barrier of a level-scheduled kernel that gave up leaves its status here.
+void DeviceBatch::checkLevelError() {
+    int e = 0;
+    VLM_CUDA(cudaMemcpy(&e, dilu_->err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+        dilu_->err.zero(stream_);
+        dilu_->bars.zero(stream_);
+        VLM_CUDA(cudaStreamSynchronize(stream_));
+        throw Error(VLM_ERR_TIMEOUT, "level-scheduled sweep: a group barrier wait gave up");
+    }
+}
+
+void DeviceBatch::recordDiluApply(const double* r, double* w) {
+    DiluDev& D = *dilu_;
+    launchLevels(k_dilu_apply, D.groups, D.G, stream_, (const DiluSys*)D.sys.get(), D.G, (const int32_t*)D.levPtr.get(),
+                 (const int32_t*)D.levRows.get(), (const int32_t*)D.loPtr.get(), (const int32_t*)D.loCol.get(),
+                 (const double*)D.loAul.get(), (const int32_t*)D.upPtr.get(), (const int32_t*)D.upCol.get(),
+                 (const double*)D.upAlu.get(), (const double*)D.rD.get(), r, w, D.bars.get(), D.err.get(),
+                 (const SysState*)st_.get(), int(kFlagDone));
+}
+
+// Gauss-Seidel / symmetric Gauss-Seidel / Jacobi: nSweeps sweeps, then the residual and the
+// convergence test (LinearSolver.cpp:238-278)
+void DeviceBatch::recordRelaxIter(const SolveKey& key) {
+    if (exact_)
+        recordRelaxIterT<true>(key);
+    else
+        recordRelaxIterT<false>(key);
+}
+
+template <bool EXACT>
+void DeviceBatch::recordRelaxIterT(const SolveKey& key) {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    for (int sw = 0; sw < key.nSweeps; ++sw) {
+        if (key.solver == SolverKind::Jacobi) {
+            VLM_LAUNCH((k_smooth_jacobi<double, 0>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(),
+                       b_.get(), x_.get(), w_.get(), 1.0, (const int32_t*)nullptr, (const double*)nullptr, st_.get(),
+                       kFlagDone);
+            VLM_LAUNCH(k_copy_rows<double>, nb, kRowsPerCta, s, ch, w_.get(), x_.get(), st_.get(), kFlagDone);
+        } else {
+            DiluDev& D = *dilu_;
+            for (int dir = 0; dir < (key.solver == SolverKind::SymGaussSeidel ? 2 : 1); ++dir)
+                launchLevels(k_gs_sweep, D.groups, D.G, s, (const DiluSys*)D.sys.get(), D.G,
+                             (const int32_t*)D.levPtr.get(), (const int32_t*)D.levRows.get(), D0.sell(),
+                             (const double*)D0.val.get(), (const double*)D0.diag.get(), (const double*)b_.get(),
+                             x_.get(), dir, D.bars.get(), D.err.get(), (const SysState*)st_.get(), int(kFlagDone));
+        }
+    }
+    VLM_LAUNCH(k_relax_residual<EXACT>, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
+               b_.get(), perm0_.get(), key.nSweeps, red(), st_.get(), dctrl_.get());
 }
 
 void DeviceBatch::recordSetCond(cudaGraphConditionalHandle h, int flag) {
@@ -810,11 +955,16 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     if (sk == SolverKind::PCG && !symmetric)
         throw Error(VLM_ERR_UNSUPPORTED, "PCG requires a symmetric matrix; use PBiCGStab");
     if (sk == SolverKind::PBiCGStab && pk == PrecondKind::DIC) pk = PrecondKind::DILU;
-    if (sk != SolverKind::PCG && sk != SolverKind::PBiCGStab)
-        throw Error(VLM_ERR_UNSUPPORTED, std::string("solver ") + ctrl.solver + " is not available on the device");
-    if (pk == PrecondKind::DIC || pk == PrecondKind::DILU)
-        throw Error(VLM_ERR_UNSUPPORTED, std::string("preconditioner ") + ctrl.preconditioner +
-                                             " is not available on the device");
+    const bool relax = sk != SolverKind::PCG && sk != SolverKind::PBiCGStab;
+    if (relax) {
+        // the relaxation solvers use no preconditioner; nSweeps < 1 would never advance the
+        // iteration count (LinearSolver.cpp:260-277)
+        pk = PrecondKind::None;
+        if (ctrl.nSweeps < 1) throw Error(VLM_ERR_BAD_ARG, "nSweeps must be at least 1 for the relaxation solvers");
+    }
+    const bool levelSchedule = pk == PrecondKind::DIC || pk == PrecondKind::DILU || sk == SolverKind::GaussSeidel ||
+                               sk == SolverKind::SymGaussSeidel;
+    if (levelSchedule) ensureDilu();
     const SmootherKind sm = parseSmoother(ctrl.smoother);
     Precision prec = Precision::FP64;
     if (eq(ctrl.precision, "mixed"))
@@ -836,6 +986,8 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     setupMatrix(diag, upper, lower, pk == PrecondKind::GAMG, mixed);
     DevLevel& D0 = L_[0];
     const int n0 = D0.nrows;
+    // DIC/DILU factorisation per solve (the coefficients change), before the iteration loop
+    if (pk == PrecondKind::DIC || pk == PrecondKind::DILU) diluFactor(upper, lower);
     if (pk == PrecondKind::Diagonal) {
         if (rD_.size() != size_t(n0)) rD_.resize(n0);
         VLM_LAUNCH(k_recip_diag<double>, nblk(n0), 256, s, n0, perm0_.get(), D0.diag.get(), rD_.get());
@@ -878,7 +1030,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
         Ay_.zero(s);
         p_.zero(s);
     }
-    const SolveKey key{sk, pk, sm, prec, exact_};
+    const SolveKey key{sk, pk, sm, prec, exact_, relax ? ctrl.nSweeps : 0};
     int64_t eagerLaunches = 0;
     GraphExec* Gp = nullptr;
     if (useGraphs_) {
@@ -907,6 +1059,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
         launches_ += (tl_launches - launch0) + eagerLaunches;
     if (pk == PrecondKind::GAMG && coarseStatus == VLM_ERR_SINGULAR)
         throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+    if (levelSchedule) checkLevelError();
     perfOut.resize(size_t(plan_.nsys));
     for (int bpos = 0; bpos < plan_.nsys; ++bpos) {
         const SysState& q = hostState_[bpos];
@@ -953,6 +1106,36 @@ void DeviceBatch::gamgApply(const double* diag, const double* upper, const doubl
     VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaStreamSynchronize(s));
     if (coarseStatus == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+}
+
+void DeviceBatch::precondApply(const double* diag, const double* upper, const double* lower, const double* r,
+                               double* w, const vlm_solver_ctrl& ctrl) {
+    const PrecondKind pk = parsePrecond(ctrl.preconditioner);
+    if (pk == PrecondKind::GAMG) {
+        gamgApply(diag, upper, lower, r, w, parseSmoother(ctrl.smoother));
+        return;
+    }
+    cudaStream_t s = stream_;
+    const bool dilu = pk == PrecondKind::DIC || pk == PrecondKind::DILU;
+    if (dilu) ensureDilu();
+    setupMatrix(diag, upper, lower, false, false);
+    DevLevel& D0 = L_[0];
+    const int n0 = D0.nrows;
+    st_.zero(s);
+    VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), r, r_.get());
+    if (dilu) {
+        diluFactor(upper, lower);
+        recordDiluApply(r_.get(), w_.get());
+    } else if (pk == PrecondKind::Diagonal) {
+        if (rD_.size() != size_t(n0)) rD_.resize(n0);
+        VLM_LAUNCH(k_recip_diag<double>, nblk(n0), 256, s, n0, perm0_.get(), D0.diag.get(), rD_.get());
+        recordPrecond(pk, SmootherKind::MCGSJacobi, r_.get(), w_.get(), false);
+    } else {
+        recordPrecond(pk, SmootherKind::MCGSJacobi, r_.get(), w_.get(), false);
+    }
+    VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), w_.get(), w);
+    VLM_CUDA(cudaStreamSynchronize(s));
+    if (dilu) checkLevelError();
 }
 
 double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n) {

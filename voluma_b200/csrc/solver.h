@@ -53,11 +53,14 @@ struct SolveKey {
     SmootherKind smoother;
     Precision prec;
     bool exact;
+    int nSweeps;  // relaxation solvers: sweeps per residual evaluation (0 for Krylov solvers)
     bool operator<(const SolveKey& o) const {
-        return std::tie(solver, precond, smoother, prec, exact) <
-               std::tie(o.solver, o.precond, o.smoother, o.prec, o.exact);
+        return std::tie(solver, precond, smoother, prec, exact, nSweeps) <
+               std::tie(o.solver, o.precond, o.smoother, o.prec, o.exact, o.nSweeps);
     }
 };
+
+struct DiluDev;  // device copy of the DIC/DILU / Gauss-Seidel level schedule (solver.cu)
 
 struct GraphExec {
     cudaGraph_t graph = nullptr;
@@ -93,6 +96,10 @@ public:
     void gamgApply(const double* diag, const double* upper, const double* lower, const double* r, double* w,
                    SmootherKind sm);
 
+    // w = M^-1 r for the preconditioner named in ctrl (user layout device pointers)
+    void precondApply(const double* diag, const double* upper, const double* lower, const double* r, double* w,
+                      const vlm_solver_ctrl& ctrl);
+
     cudaStream_t stream() const { return stream_; }
     size_t deviceBytes() const;
     int64_t launches() const { return launches_; }
@@ -107,6 +114,12 @@ private:
     template <class T> void recordTail(const T* r0, T* x0, int flag);
     template <class T> void buildTailTable(DBuf<TailLevel<T>>& out);
     void planTail();
+    void ensureDilu();
+    void recordDiluApply(const double* r, double* w);
+    void diluFactor(const double* upper, const double* lower);
+    void checkLevelError();
+    void recordRelaxIter(const SolveKey& key);
+    template <bool EXACT> void recordRelaxIterT(const SolveKey& key);
     void recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32);
     void recordIter(const SolveKey& key);
     void runEager(const SolveKey& key, int maxIter);
@@ -144,6 +157,10 @@ private:
     int tailMaxFirst_ = 0;      // head levels: k < tailMaxFirst_
     std::vector<int> tailFirst_;
     DBuf<TailSys> tailSys_;
+    std::vector<SysTopo> topo_;          // host topology (owned by the caller for the batch's lifetime)
+    std::unique_ptr<DiluDev> dilu_;      // built on the first DIC/DILU/Gauss-Seidel solve
+    const double* curUpper_ = nullptr;   // face coefficients of the current solve (device, user layout)
+    const double* curLower_ = nullptr;
     DBuf<TailLevel<double>> tail64_;
     DBuf<TailLevel<float>> tail32_;
     int64_t launches_ = 0;
