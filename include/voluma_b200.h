@@ -15,6 +15,7 @@
  *                            LinearSolver.cpp:135-284)
  *   vlm_amul              <- void amul(const LduSystem&, x, y)  (LinearSolver.h:45, .cpp:121-133)
  *   vlm_gamg_apply        <- GamgPreconditioner::apply           (src/fvm/linalg/GAMG.h:63, .cpp:445)
+ *   vlm_flow_*            <- IncompressibleFlow::initialize / step (src/fvm/solvers/IncompressibleFlow.cpp)
  *   vlm_precond_apply     <- Preconditioner ctor + apply (none/diagonal/DIC/DILU/GAMG)
  *                            (src/fvm/linalg/LinearSolver.cpp:56-107)
  *   vlm_gamg_levels/_level<- buildHierarchy                      (GAMG.h:57, GAMG.cpp:206-261)
@@ -73,6 +74,8 @@ typedef struct {
     int32_t n_patches;
     const int32_t* patch_start; /* n_patches, face index of each patch's first face */
     const int32_t* patch_size;  /* n_patches */
+    const double* C;            /* 3*n_cells cell centres (optional: linearUpwind / LUST momentum) */
+    const double* Cf;           /* 3*n_faces face centres (optional, with C) */
 } vlm_mesh_desc;
 
 /* Solver dictionary: SolverControls (src/fvm/linalg/LinearSolver.h:15-23) plus additive keys. */
@@ -232,6 +235,48 @@ vlm_status vlm_topology_destroy(vlm_topology* t);
 /* ------------------------------------------------------------------ reductions */
 /* Order-independent exact sum of n doubles on the device (host pointer in, host result). */
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out);
+
+/* ------------------------------------------------------------------ incompressible step */
+/* IncompressibleFlow::step (src/fvm/solvers/IncompressibleFlow.cpp:138-370) on the device, for laminar
+ * flow: momentum assembly (fvm::ddt + fvm::div(phi, U) - fvm::laplacian(nu, U), Fvm.h:18-182),
+ * FvMatrix::relax (FvMatrix.h:111-131), the momentum predictor, A/H/HbyA and the Rhie-Chow flux
+ * phiHbyA (IncompressibleFlow.cpp:244-292), the pressure equation with its non-orthogonal correctors,
+ * the explicit pressure relaxation and U = HbyA - rAU grad p.  The mesh must be a single system
+ * registered with geometry (and C / Cf for linearUpwind or LUST); it must outlive the flow.
+ * Boundary conditions per patch: 0 zeroGradient, 1 fixedValue (noSlip = fixedValue 0).
+ * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
+ * reference's fields bit for bit. */
+typedef struct vlm_flow vlm_flow;
+
+typedef struct {
+    double nu;                   /* kinematic viscosity */
+    int32_t steady;              /* 1: SIMPLE (steadyState) */
+    int32_t div_scheme;          /* 0 upwind, 1 linear, 2 linearUpwind, 3 LUST (Schemes.h:13-40) */
+    int32_t ddt_scheme;          /* 0 steadyState, 1 Euler, 2 backward */
+    int32_t n_outer, n_corr, n_non_orth_corr, momentum_predictor; /* PimpleControls */
+    double alpha_u, alpha_p;
+    int32_t p_ref_cell;
+    double p_ref_value;
+    vlm_solver_ctrl U, p, p_final;
+} vlm_flow_ctrl;
+
+typedef struct {
+    double UInitialResidual, pInitialResidual, continuityError; /* StepInfo */
+    int32_t iterations;          /* linear-solver iterations of the step */
+} vlm_step_info;
+
+vlm_status vlm_flow_create(vlm_ctx* ctx, vlm_mesh* mesh, const vlm_flow_ctrl* ctrl, const int32_t* u_type,
+                           const double* u_value, const int32_t* p_type, const double* p_value, vlm_flow** out);
+/* IncompressibleFlow::initialize from host fields: U 3 per cell (NULL: keep), p per cell (NULL: keep). */
+vlm_status vlm_flow_set_state(vlm_flow* flow, const double* U, const double* p);
+/* One IncompressibleFlow::step(dt) (dt ignored when steady). */
+vlm_status vlm_flow_step(vlm_flow* flow, double dt, vlm_step_info* info);
+/* The steady loop of fvmFlow (apps/fvmFlow/fvmFlow.cpp:611-640): steps until U and p residuals are
+ * below residual_tol (from the second iteration) or max_iter; *iterations = steps taken. */
+vlm_status vlm_flow_run_steady(vlm_flow* flow, int32_t max_iter, double residual_tol, int32_t* iterations,
+                               vlm_step_info* last);
+vlm_status vlm_flow_get_state(vlm_flow* flow, double* U, double* p, double* phi);
+vlm_status vlm_flow_destroy(vlm_flow* flow);
 
 /* Exact sum that allocates no device memory.  No counterpart in the reference.  For callers that
  * cannot call cudaMalloc where they need the sum (device memory owned by their own pool or fixed

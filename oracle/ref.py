@@ -50,6 +50,8 @@ def lib():
                                          C.c_double, C.c_double, C.c_int, P, P, P]
         L.ref_exact_sum.restype = C.c_double
         L.ref_exact_sum.argtypes = [P, C.c_long]
+        L.ref_flow_run.argtypes = [P, C.POINTER(RefFlowSpec), C.c_int, C.c_double, P, P, P, P]
+        L.ref_flow_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -61,6 +63,29 @@ def _p(a):
 def _check(rc):
     if rc != 0:
         raise RuntimeError(lib().ref_last_error().decode())
+
+
+class RefSolverCtl(C.Structure):
+    _fields_ = [("solver", C.c_char * 32), ("preconditioner", C.c_char * 32), ("tolerance", C.c_double),
+                ("relTol", C.c_double), ("maxIter", C.c_int), ("minIter", C.c_int), ("nSweeps", C.c_int)]
+
+
+class RefFlowSpec(C.Structure):
+    _fields_ = [("nu", C.c_double), ("steady", C.c_int), ("divScheme", C.c_int), ("ddtScheme", C.c_int),
+                ("nOuter", C.c_int), ("nCorr", C.c_int), ("nNonOrthCorr", C.c_int), ("momentumPredictor", C.c_int),
+                ("alphaU", C.c_double), ("alphaP", C.c_double), ("nPatches", C.c_int), ("uType", C.c_void_p),
+                ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
+                ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
+                ("reproducible", C.c_int)]
+
+
+def _solver_ctl(d):
+    c = RefSolverCtl()
+    c.solver = d["solver"].encode()
+    c.preconditioner = d["preconditioner"].encode()
+    c.tolerance, c.relTol = d["tolerance"], d["relTol"]
+    c.maxIter, c.minIter, c.nSweeps = d["maxIter"], d.get("minIter", 0), d.get("nSweeps", 1)
+    return c
 
 
 class RefMesh:
@@ -104,6 +129,33 @@ class RefMesh:
         out = np.zeros(shp, dt)
         _check(lib().ref_mesh_get(self._h, name.encode(), _p(out)))
         return out
+
+    # ------------------------------------------------------------------ incompressible step
+    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False):
+        """n_steps of IncompressibleFlow::step(dt) (solvers/IncompressibleFlow.cpp:138-370) with the case
+        settings of `case` (a dict, voluma_b200.cases.flow_case layout).  Returns U (n,3), p, phi, and the
+        per-step history [UInitialResidual, pInitialResidual, continuityError, linear iterations]."""
+        nC = self.n_cells
+        Uc = np.zeros((nC, 3)) if U is None else np.ascontiguousarray(U, np.float64).reshape(nC, 3).copy()
+        pc = np.zeros(nC) if p is None else np.ascontiguousarray(p, np.float64).copy()
+        phi = np.zeros(self.n_faces)
+        hist = np.zeros((n_steps, 4))
+        keep = [np.ascontiguousarray(case["u_type"], np.int32), np.ascontiguousarray(case["u_value"], np.float64),
+                np.ascontiguousarray(case["p_type"], np.int32), np.ascontiguousarray(case["p_value"], np.float64)]
+        sp = RefFlowSpec()
+        sp.nu = case["nu"]
+        sp.steady, sp.divScheme, sp.ddtScheme = int(case["steady"]), case["div_scheme"], case["ddt_scheme"]
+        sp.nOuter, sp.nCorr, sp.nNonOrthCorr = case["n_outer"], case["n_corr"], case["n_non_orth_corr"]
+        sp.momentumPredictor = int(case["momentum_predictor"])
+        sp.alphaU, sp.alphaP = case["alpha_u"], case["alpha_p"]
+        sp.nPatches = self.n_patches
+        sp.uType, sp.uValue, sp.pType, sp.pValue = (_p(a) for a in keep)
+        sp.U, sp.p, sp.pFinal = (_solver_ctl(case[k]) for k in ("U", "p", "pFinal"))
+        sp.pRefCell, sp.pRefValue = case["p_ref_cell"], case["p_ref_value"]
+        sp.reproducible = int(reproducible)
+        if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist)) != 0:
+            raise RuntimeError(lib().ref_flow_error().decode())
+        return Uc, pc, phi, hist
 
     # ------------------------------------------------------------------ linear algebra
     def amul(self, diag, upper, lower, x):

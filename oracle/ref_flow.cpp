@@ -1,0 +1,141 @@
+// Test-infrastructure driver: the reference's own incompressible step (solvers/IncompressibleFlow.cpp,
+// IncompressibleFlow::step) on a mesh built by ref_driver.cpp, with boundary conditions set through
+// the reference's public VolField API the way CaseSetup.cpp:300-430 sets them (fixedValue/noSlip,
+// zeroGradient) and the controls fvmFlow.cpp:141-178 derives from a case file.  It only marshals
+// arrays and settings; every number comes from the unmodified reference.
+
+#include "fvm/solvers/IncompressibleFlow.h"
+#include "fvm/parallel/Comm.h"
+
+#include <cstring>
+#include <exception>
+#include <string>
+
+using namespace cfd;
+
+struct RefMesh {
+    MeshPtr mesh;
+};
+
+extern "C" {
+
+// One linear-solver dictionary (SolverControls, LinearSolver.h:15-23).
+struct RefSolverCtl {
+    char solver[32];
+    char preconditioner[32];
+    double tolerance, relTol;
+    int maxIter, minIter, nSweeps;
+};
+
+// Case settings: scheme codes follow Schemes.h (div: 0 upwind, 1 linear, 2 linearUpwind, 3 LUST;
+// ddt: 0 steadyState, 1 Euler, 2 backward); per patch (mesh patch order) U/p boundary type
+// 0 zeroGradient, 1 fixedValue with the given value.
+struct RefFlowSpec {
+    double nu;
+    int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
+    double alphaU, alphaP;
+    int nPatches;
+    const int* uType;
+    const double* uValue;  // 3 per patch
+    const int* pType;
+    const double* pValue;  // 1 per patch
+    RefSolverCtl U, p, pFinal;
+    int pRefCell;
+    double pRefValue;
+    int reproducible;
+};
+
+int ref_flow_run(const RefMesh* r, const RefFlowSpec* spec, int nSteps, double dt, double* U, double* p,
+                 double* phi, double* hist);
+const char* ref_flow_error();
+}
+
+namespace {
+thread_local std::string g_flowErr;
+
+SolverControls toCtl(const RefSolverCtl& c) {
+    SolverControls s;
+    s.solver = c.solver;
+    s.preconditioner = c.preconditioner;
+    s.tolerance = c.tolerance;
+    s.relTol = c.relTol;
+    s.maxIter = c.maxIter;
+    s.minIter = c.minIter;
+    s.nSweeps = c.nSweeps;
+    return s;
+}
+}  // namespace
+
+const char* ref_flow_error() { return g_flowErr.c_str(); }
+
+// Runs nSteps of IncompressibleFlow::step(dt) from the given U (3 per cell) and p (per cell).
+// Outputs U, p, phi (nFaces) and per step hist[4*k..]: UInitialResidual, pInitialResidual,
+// continuityError, total linear-solver iterations.
+int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt, double* U, double* p, double* phi,
+                 double* hist) {
+    try {
+        par::setReproducible(sp->reproducible != 0);
+        const Mesh& m = *r->mesh;
+        IncompressibleFlow flow(r->mesh, sp->nu);
+        PimpleControls& c = flow.controls;
+        c.steady = sp->steady != 0;
+        c.nOuter = sp->nOuter;
+        c.nCorr = sp->nCorr;
+        c.nNonOrthCorr = sp->nNonOrthCorr;
+        c.momentumPredictor = sp->momentumPredictor != 0;
+        c.alphaU = sp->alphaU;
+        c.alphaP = sp->alphaP;
+        c.UControls = toCtl(sp->U);
+        c.pControls = toCtl(sp->p);
+        c.pFinalControls = toCtl(sp->pFinal);
+        c.pRefCell = sp->pRefCell;
+        c.pRefValue = sp->pRefValue;
+        static const char* div[4] = {"upwind", "linear", "linearUpwind", "LUST"};
+        flow.divScheme = ConvectionScheme::parse(div[sp->divScheme]);
+        flow.ddtScheme = sp->ddtScheme == 0 ? DdtScheme::Steady : sp->ddtScheme == 1 ? DdtScheme::Euler
+                                                                                      : DdtScheme::Backward;
+        if (sp->nPatches != int(m.patches().size())) throw std::runtime_error("patch count mismatch");
+        for (int q = 0; q < sp->nPatches; ++q) {
+            const std::string name = m.patches()[q].name;
+            if (m.patches()[q].type == PatchType::Empty || m.patches()[q].type == PatchType::Cyclic) continue;
+            if (sp->uType[q] == 1)
+                flow.U().fixedValue(name, Vec3{sp->uValue[3 * q], sp->uValue[3 * q + 1], sp->uValue[3 * q + 2]});
+            else
+                flow.U().zeroGradient(name);
+            if (sp->pType[q] == 1)
+                flow.p().fixedValue(name, sp->pValue[q]);
+            else
+                flow.p().zeroGradient(name);
+        }
+        const label nC = m.nCells();
+        for (label k = 0; k < nC; ++k) {
+            flow.U()[k] = Vec3{U[3 * k], U[3 * k + 1], U[3 * k + 2]};
+            flow.p()[k] = p[k];
+        }
+        for (int s = 0; s < nSteps; ++s) {
+            const StepInfo info = flow.step(dt);
+            double its = 0;
+            for (const auto& pf : info.perf) its += pf.iterations;
+            if (hist) {
+                hist[4 * s] = info.UInitialResidual;
+                hist[4 * s + 1] = info.pInitialResidual;
+                hist[4 * s + 2] = info.continuityError;
+                hist[4 * s + 3] = its;
+            }
+        }
+        for (label k = 0; k < nC; ++k) {
+            U[3 * k] = flow.U()[k].x;
+            U[3 * k + 1] = flow.U()[k].y;
+            U[3 * k + 2] = flow.U()[k].z;
+            p[k] = flow.p()[k];
+        }
+        if (phi)
+            for (label f = 0; f < m.nFaces(); ++f) phi[f] = flow.phi()[f];
+        par::setReproducible(false);
+        return 0;
+    } catch (const std::exception& e) {
+        g_flowErr = e.what();
+        par::setReproducible(false);
+        return 1;
+    }
+}

@@ -127,9 +127,10 @@ _live = weakref.WeakSet()  # meshes/contexts still holding native handles
 def _release_all():
     # release meshes before contexts while the interpreter (and the CUDA runtime) are intact
     objs = list(_live)
-    for o in objs:
-        if isinstance(o, Mesh):
-            o.close()
+    for kind in ("Flow", "Mesh"):  # flows before their meshes, meshes before their contexts
+        for o in objs:
+            if type(o).__name__ == kind:
+                o.close()
     for o in objs:
         o.close()
 
@@ -166,7 +167,7 @@ class Mesh:
         d.magSf = self.magSf.ctypes.data
         d.ndc = self.ndc.ctypes.data
         self._keep = []
-        for name in ("V", "Sf", "d", "w", "corrVecs"):
+        for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
             if name in self.geometry:
                 arr = _f64(self.geometry[name])
                 self._keep.append(arr)
@@ -201,7 +202,7 @@ class Mesh:
             arrs = [own, nei, _f64(m["magSf"]), _f64(m["ndc"])]
             d.n_cells, d.n_internal_faces, d.n_faces = int(m["n_cells"]), nei.size, own.size
             d.owner, d.neighbour, d.magSf, d.ndc = (a.ctypes.data for a in arrs)
-            for name in ("V", "Sf", "d", "w", "corrVecs"):
+            for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
                 if name in m:
                     a = _f64(m[name])
                     arrs.append(a)
@@ -440,3 +441,77 @@ def gamg_apply(mesh: Mesh, diag, upper, lower, r, smoother: str = ""):
                                 None if lower is None else _ptr(_f64(lower)), _ptr(_f64(r)), _ptr(w), C.byref(c)),
           mesh.ctx.handle)
     return w
+
+
+# ------------------------------------------------------------------ incompressible step
+def _flow_ctrl(case: dict) -> _ffi.FlowCtrl:
+    c = _ffi.FlowCtrl()
+    c.nu = case["nu"]
+    c.steady = int(case["steady"])
+    c.div_scheme, c.ddt_scheme = case["div_scheme"], case["ddt_scheme"]
+    c.n_outer, c.n_corr, c.n_non_orth_corr = case["n_outer"], case["n_corr"], case["n_non_orth_corr"]
+    c.momentum_predictor = int(case["momentum_predictor"])
+    c.alpha_u, c.alpha_p = case["alpha_u"], case["alpha_p"]
+    c.p_ref_cell, c.p_ref_value = case["p_ref_cell"], case["p_ref_value"]
+    repro = bool(case.get("reproducible", False))
+    for name, key in (("U", "U"), ("p", "p"), ("p_final", "pFinal")):
+        d = case[key]
+        sc = SolverControls(d["solver"], d["preconditioner"], d["tolerance"], d["relTol"], d["maxIter"],
+                            d.get("minIter", 0), d.get("nSweeps", 1), reproducible=repro,
+                            smoother=d.get("smoother", ""), precision=d.get("precision", ""))
+        setattr(c, name, sc.to_c())
+    return c
+
+
+class Flow:
+    """IncompressibleFlow (solvers/IncompressibleFlow.h) on the device for a registered single-system mesh
+    with geometry.  `case`: dict with nu, steady, div_scheme, ddt_scheme, n_outer, n_corr,
+    n_non_orth_corr, momentum_predictor, alpha_u, alpha_p, p_ref_cell, p_ref_value, U / p / pFinal solver
+    dictionaries, per-patch u_type / u_value / p_type / p_value and optionally reproducible
+    (voluma_b200.cases.lid_cavity builds one)."""
+
+    def __init__(self, mesh: Mesh, case: dict):
+        self.mesh = mesh
+        self.n_cells = mesh.n_cells
+        self.n_faces = mesh.n_faces
+        self._keep = [np.ascontiguousarray(case["u_type"], np.int32), _f64(case["u_value"]),
+                      np.ascontiguousarray(case["p_type"], np.int32), _f64(case["p_value"])]
+        c = _flow_ctrl(case)
+        h = C.c_void_p()
+        check(load().vlm_flow_create(mesh.ctx.handle, mesh.handle, C.byref(c), *(a.ctypes.data for a in self._keep),
+                                     C.byref(h)), mesh.ctx.handle)
+        self._h = h
+        _live.add(self)
+
+    def set_state(self, U=None, p=None):
+        Ua = None if U is None else _f64(U).reshape(-1)
+        pa = None if p is None else _f64(p)
+        check(load().vlm_flow_set_state(self._h, None if Ua is None else Ua.ctypes.data,
+                                        None if pa is None else pa.ctypes.data), self.mesh.ctx.handle)
+
+    def step(self, dt=1.0) -> dict:
+        i = _ffi.StepInfo()
+        check(load().vlm_flow_step(self._h, dt, C.byref(i)), self.mesh.ctx.handle)
+        return dict(UInitialResidual=i.UInitialResidual, pInitialResidual=i.pInitialResidual,
+                    continuityError=i.continuityError, iterations=i.iterations)
+
+    def run_steady(self, max_iter=5000, residual_tol=1e-6):
+        it = C.c_int32()
+        i = _ffi.StepInfo()
+        check(load().vlm_flow_run_steady(self._h, max_iter, residual_tol, C.byref(it), C.byref(i)),
+              self.mesh.ctx.handle)
+        return it.value, dict(UInitialResidual=i.UInitialResidual, pInitialResidual=i.pInitialResidual,
+                              continuityError=i.continuityError, iterations=i.iterations)
+
+    def state(self):
+        U = np.zeros((self.n_cells, 3))
+        p = np.zeros(self.n_cells)
+        phi = np.zeros(self.n_faces)
+        check(load().vlm_flow_get_state(self._h, U.ctypes.data, p.ctypes.data, phi.ctypes.data),
+              self.mesh.ctx.handle)
+        return U, p, phi
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().vlm_flow_destroy(self._h)
+            self._h = None

@@ -16,7 +16,8 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
-           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply"]
+           "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
+           "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy"]
 
 
 class MeshDesc(C.Structure):
@@ -24,7 +25,7 @@ class MeshDesc(C.Structure):
                 ("owner", C.c_void_p), ("neighbour", C.c_void_p), ("magSf", C.c_void_p), ("ndc", C.c_void_p),
                 ("V", C.c_void_p), ("Sf", C.c_void_p), ("d", C.c_void_p), ("w", C.c_void_p),
                 ("corrVecs", C.c_void_p), ("two_d", C.c_int32), ("empty_dir", C.c_int32), ("n_patches", C.c_int32),
-                ("patch_start", C.c_void_p), ("patch_size", C.c_void_p)]
+                ("patch_start", C.c_void_p), ("patch_size", C.c_void_p), ("C", C.c_void_p), ("Cf", C.c_void_p)]
 
 
 class SolverCtrl(C.Structure):
@@ -38,6 +39,19 @@ class SolverPerf(C.Structure):
     _fields_ = [("initialResidual", C.c_double), ("finalResidual", C.c_double), ("residualSum", C.c_double),
                 ("normFactor", C.c_double), ("iterations", C.c_int32), ("converged", C.c_int32),
                 ("outerIterations", C.c_int32), ("status", C.c_int32), ("solver", C.c_char * 32)]
+
+
+class FlowCtrl(C.Structure):
+    _fields_ = [("nu", C.c_double), ("steady", C.c_int32), ("div_scheme", C.c_int32), ("ddt_scheme", C.c_int32),
+                ("n_outer", C.c_int32), ("n_corr", C.c_int32), ("n_non_orth_corr", C.c_int32),
+                ("momentum_predictor", C.c_int32), ("alpha_u", C.c_double), ("alpha_p", C.c_double),
+                ("p_ref_cell", C.c_int32), ("p_ref_value", C.c_double), ("U", SolverCtrl), ("p", SolverCtrl),
+                ("p_final", SolverCtrl)]
+
+
+class StepInfo(C.Structure):
+    _fields_ = [("UInitialResidual", C.c_double), ("pInitialResidual", C.c_double),
+                ("continuityError", C.c_double), ("iterations", C.c_int32)]
 
 
 _lib = None
@@ -66,6 +80,12 @@ def load():
     L.vlm_ldu_solve_device.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]
     L.vlm_gamg_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
     L.vlm_precond_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
+    L.vlm_flow_create.argtypes = [P, P, C.POINTER(FlowCtrl), P, P, P, P, C.POINTER(P)]
+    L.vlm_flow_set_state.argtypes = [P, P, P]
+    L.vlm_flow_step.argtypes = [P, C.c_double, C.POINTER(StepInfo)]
+    L.vlm_flow_run_steady.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_int32), C.POINTER(StepInfo)]
+    L.vlm_flow_get_state.argtypes = [P, P, P, P]
+    L.vlm_flow_destroy.argtypes = [P]
     L.vlm_gamg_levels.argtypes = [P, C.POINTER(i32)]
     L.vlm_gamg_level.argtypes = [P, i32, P, P, P, P]
     L.vlm_gamg_colours.argtypes = [P, i32, C.POINTER(i32)]

@@ -121,3 +121,50 @@ def split_batch_faces(meshes, F):
     ib = np.cumsum([0] + nI)
     bb = sum(nI) + np.cumsum([0] + nB)
     return [np.concatenate([F[ib[i]:ib[i + 1]], F[bb[i]:bb[i + 1]]]) for i in range(len(meshes))]
+
+
+# ------------------------------------------------------------------ incompressible cases
+def _ctl(solver, precond, tol, rel_tol, max_iter):
+    return dict(solver=solver, preconditioner=precond, tolerance=tol, relTol=rel_tol, maxIter=max_iter, minIter=0,
+                nSweeps=1)
+
+
+def lid_cavity(n=64, Re=100.0, lid=1.0):
+    """The lid-driven cavity of cases/cavity/case.json: generateBox n = (n, n, 1), hi = (1, 1, 0.1), twoD,
+    walls on xMin/xMax/yMin/yMax with yMax the moving lid, nu = lid/Re; steady SIMPLE with the fvmFlow
+    steady defaults (fvmFlow.cpp:141-178: linearUpwind, alphaU 0.7, alphaP 0.3, nCorr 1,
+    U {PBiCGStab, DILU, 1e-10, relTol 0.1}, p {PCG, GAMG, 1e-10, relTol 0.05}).
+    Returns (mesh dict, case dict); the case's boundary arrays follow the mesh's patch order."""
+    from . import mesh as vm
+    m = vm.box_mesh((n, n, 1), hi=(1.0, 1.0, 0.1), two_d=True)
+    nP = len(m["patch_start"])
+    u_type = np.ones(nP, np.int32)               # noSlip / fixedValue everywhere
+    u_value = np.zeros((nP, 3))
+    cf_y = [m["Cf"][m["patch_start"][q]:m["patch_start"][q] + m["patch_size"][q], 1] for q in range(nP)]
+    lid_patch = int(np.argmax([c.mean() for c in cf_y]))
+    u_value[lid_patch] = (lid, 0.0, 0.0)
+    case = dict(nu=lid / Re, steady=True, div_scheme=2, ddt_scheme=0, n_outer=1, n_corr=1, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=0.7, alpha_p=0.3, u_type=u_type, u_value=u_value.ravel(),
+                p_type=np.zeros(nP, np.int32), p_value=np.zeros(nP), U=_ctl("PBiCGStab", "DILU", 1e-10, 0.1, 1000),
+                p=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000), pFinal=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000),
+                p_ref_cell=0, p_ref_value=0.0, lid_patch=lid_patch)
+    return m, case
+
+
+def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
+    """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
+    U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient
+    defaults: backward ddt, linear divergence, nOuter 1, nCorr 2, U {PBiCGStab, DILU, 1e-8},
+    p {PCG, GAMG, 1e-8, relTol 0.01}, pFinal {PCG, GAMG, 1e-8}.  Returns (mesh, case, U0)."""
+    from . import mesh as vm
+    m = vm.box_mesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+    C = m["C"]
+    U0 = u0 * np.stack([np.sin(C[:, 0]) * np.cos(C[:, 1]) * np.cos(C[:, 2]),
+                        -np.cos(C[:, 0]) * np.sin(C[:, 1]) * np.cos(C[:, 2]), np.zeros(len(C))], 1)
+    nP = max(len(m["patch_start"]), 1)
+    case = dict(nu=nu, steady=False, div_scheme=1, ddt_scheme=2, n_outer=1, n_corr=2, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=1.0, alpha_p=1.0, u_type=np.zeros(nP, np.int32),
+                u_value=np.zeros(3 * nP), p_type=np.zeros(nP, np.int32), p_value=np.zeros(nP),
+                U=_ctl("PBiCGStab", "DILU", 1e-8, 0.0, 1000), p=_ctl("PCG", "GAMG", 1e-8, 0.01, 2000),
+                pFinal=_ctl("PCG", "GAMG", 1e-8, 0.0, 2000), p_ref_cell=0, p_ref_value=0.0)
+    return m, case, U0

@@ -1,12 +1,15 @@
 // extern "C" boundary (include/voluma_b200.h): status codes in, no exceptions out.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "assembly.h"
+#include "flow.h"
 #include "solver.h"
 #include "voluma_b200.h"
 
@@ -221,6 +224,9 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
                          NC = static_cast<size_t>(nC);
             std::vector<int32_t> own(F), nei(NI), ps, pz;
             std::vector<double> magSf(F), ndc(F), w(F), V(NC), Sf(3 * F), dd(3 * F), corr(3 * F);
+            bool centres = true;  // cell / face centres (optional)
+            for (int s = 0; s < nsys; ++s) centres = centres && descs[s].C && descs[s].Cf;
+            std::vector<double> Cc(centres ? 3 * NC : 0), Cfc(centres ? 3 * F : 0);
             auto copyFace = [&](const vlm_mesh_desc* d, int f, int64_t g, int64_t base) {
                 own[g] = int32_t(d->owner[f] + base);
                 magSf[g] = d->magSf[f];
@@ -230,12 +236,17 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
                     Sf[3 * g + q] = d->Sf[3 * f + q];
                     dd[3 * g + q] = d->d[3 * f + q];
                     corr[3 * g + q] = d->corrVecs[3 * f + q];
+                    if (centres) Cfc[3 * g + q] = d->Cf[3 * f + q];
                 }
             };
             for (int s = 0; s < nsys; ++s) {
                 const vlm_mesh_desc* d = &descs[s];
                 const int64_t base = m->cellBase[s];
-                for (int c = 0; c < d->n_cells; ++c) V[base + c] = d->V[c];
+                for (int c = 0; c < d->n_cells; ++c) {
+                    V[base + c] = d->V[c];
+                    if (centres)
+                        for (int q = 0; q < 3; ++q) Cc[3 * (base + c) + q] = d->C[3 * c + q];
+                }
                 for (int f = 0; f < d->n_internal_faces; ++f) {
                     copyFace(d, f, m->faceBase[s] + f, base);
                     nei[m->faceBase[s] + f] = int32_t(d->neighbour[f] + base);
@@ -250,7 +261,9 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
             m->geom = std::make_unique<vlm::DeviceGeom>(int(nC), int(nI), int(nF), own.data(), nei.data(), magSf.data(),
                                                         ndc.data(), V.data(), Sf.data(), dd.data(), w.data(),
                                                         corr.data(), descs[0].two_d, descs[0].empty_dir,
-                                                        int(ps.size()), ps.data(), pz.data(), ctx->stream);
+                                                        int(ps.size()), ps.data(), pz.data(),
+                                                        centres ? Cc.data() : nullptr, centres ? Cfc.data() : nullptr,
+                                                        ctx->stream);
         }
         ctx->refs++;
         *out = m.release();
@@ -647,3 +660,80 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
 }
 
 }  // extern "C"
+
+// ====================================================================== incompressible step
+struct vlm_flow {
+    vlm_mesh* mesh = nullptr;
+    std::unique_ptr<vlm::DeviceFlow> flow;
+};
+
+extern "C" {
+
+vlm_status vlm_flow_create(vlm_ctx* ctx, vlm_mesh* m, const vlm_flow_ctrl* ctrl, const int32_t* uType,
+                           const double* uValue, const int32_t* pType, const double* pValue, vlm_flow** out) {
+    if (!ctx || !m || !ctrl || !out || !uType || !uValue || !pType || !pValue)
+        return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        auto f = std::make_unique<vlm_flow>();
+        f->mesh = m;
+        f->flow = std::make_unique<vlm::DeviceFlow>(*m->batch, geomOf(m), *ctrl, uType, uValue, pType, pValue,
+                                                    ctx->stream);
+        *out = f.release();
+    });
+}
+
+vlm_status vlm_flow_set_state(vlm_flow* f, const double* U, const double* p) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->setState(U, p);
+    });
+}
+
+vlm_status vlm_flow_step(vlm_flow* f, double dt, vlm_step_info* info) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        const vlm_step_info i = f->flow->step(dt);
+        if (info) *info = i;
+    });
+}
+
+vlm_status vlm_flow_run_steady(vlm_flow* f, int32_t maxIter, double tol, int32_t* iterations, vlm_step_info* last) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        vlm_step_info i;
+        std::memset(&i, 0, sizeof i);
+        int it = 0;
+        for (it = 1; it <= maxIter; ++it) {
+            i = f->flow->step(1.0);
+            VLM_REQUIRE(std::isfinite(i.UInitialResidual) && std::isfinite(i.pInitialResidual) &&
+                            std::isfinite(i.continuityError),
+                        VLM_ERR_NONFINITE, "solution diverged (non-finite residual) at iteration " + std::to_string(it));
+            if (it > 1 && i.UInitialResidual < tol && i.pInitialResidual < tol) break;
+        }
+        if (iterations) *iterations = std::min(it, maxIter);
+        if (last) *last = i;
+    });
+}
+
+vlm_status vlm_flow_get_state(vlm_flow* f, double* U, double* p, double* phi) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->getState(U, p, phi);
+    });
+}
+
+vlm_status vlm_flow_destroy(vlm_flow* f) {
+    if (!f) return VLM_OK;
+    cudaSetDevice(f->mesh->ctx->device);
+    cudaStreamSynchronize(f->mesh->ctx->stream);
+    delete f;
+    return VLM_OK;
+}
+
+}  // extern "C"
+

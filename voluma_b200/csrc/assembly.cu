@@ -303,7 +303,8 @@ __global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, co
 DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own, const int32_t* nei,
                        const double* magSf, const double* ndc, const double* V, const double* Sf, const double* d,
                        const double* w, const double* corrVecs, int twoD, int emptyDir, int nPatches,
-                       const int32_t* patchStart, const int32_t* patchSize, cudaStream_t s)
+                       const int32_t* patchStart, const int32_t* patchSize, const double* C, const double* Cf,
+                       cudaStream_t s)
     : nC_(nCells), nI_(nInternal), nF_(nFaces), twoD_(twoD), emptyDir_(emptyDir) {
     VLM_REQUIRE(V && Sf && d && w && corrVecs, VLM_ERR_BAD_ARG, "mesh geometry (V, Sf, d, w, corrVecs) is required");
     const int nB = nF_ - nI_;
@@ -350,6 +351,13 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
     soa(Sf, Sf_);
     soa(d, d_);
     soa(corrVecs, corr_);
+    if (C && Cf) {
+        soa(Cf, Cf_);
+        std::vector<double> v(size_t(3) * nC_);
+        for (int c = 0; c < nC_; ++c)
+            for (int q = 0; q < 3; ++q) v[size_t(q) * nC_ + c] = C[3 * size_t(c) + q];
+        C_.upload(v, s);
+    }
     // the correction is applied when any internal corrVec is non-zero (Fvm.h:156-158)
     for (int f = 0; f < nI_ && !nonOrth_; ++f) {
         const double* c = corrVecs + 3 * size_t(f);

@@ -25,7 +25,7 @@ public:
     DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own, const int32_t* nei, const double* magSf,
                const double* ndc, const double* V, const double* Sf, const double* d, const double* w,
                const double* corrVecs, int twoD, int emptyDir, int nPatches, const int32_t* patchStart,
-               const int32_t* patchSize, cudaStream_t stream);
+               const int32_t* patchSize, const double* C, const double* Cf, cudaStream_t stream);
 
     int nCells() const { return nC_; }
     int nInternal() const { return nI_; }
@@ -67,12 +67,32 @@ public:
     const int32_t* cellFaceOff() const { return cfOff_.get(); }
     const int32_t* cellFaces() const { return cfList_.get(); }
 
+    // raw device arrays (vectors SoA: [x(n) y(n) z(n)]) for the momentum kernels
+    const int32_t* own() const { return own_.get(); }
+    const int32_t* nei() const { return nei_.get(); }
+    const int32_t* bPatch() const { return bPatch_.get(); }
+    const double* magSf() const { return magSf_.get(); }
+    const double* ndc() const { return ndc_.get(); }
+    const double* V() const { return V_.get(); }
+    const double* w() const { return w_.get(); }
+    const double* Sf() const { return Sf_.get(); }
+    const double* d() const { return d_.get(); }
+    const double* corr() const { return corr_.get(); }
+    const double* C() const { return C_.size() ? C_.get() : nullptr; }
+    const double* Cf() const { return Cf_.size() ? Cf_.get() : nullptr; }
+    int twoD() const { return twoD_; }
+    int emptyDir() const { return emptyDir_; }
+    int nPatches() const { return int(patchStart_.size()); }
+    const std::vector<int32_t>& patchStart() const { return patchStart_; }
+    const std::vector<int32_t>& patchSize() const { return patchSize_; }
+
 private:
     int nC_, nI_, nF_, twoD_, emptyDir_;
     bool nonOrth_ = false;
     std::vector<int32_t> patchStart_, patchSize_, bPatchHost_;
     DBuf<int32_t> own_, nei_, cfOff_, cfList_, bPatch_, bcType_;
     DBuf<double> magSf_, ndc_, V_, w_, Sf_, d_, corr_;  // vectors as SoA: [x(nF) y(nF) z(nF)]
+    DBuf<double> C_, Cf_;                               // SoA; empty when not registered
     DBuf<double> scratchG_, scratchGS_;
     void uploadBCType(const ScalarBC& bc, cudaStream_t s);
 };

@@ -1,0 +1,655 @@
+// Device incompressible step (see flow.h).  Every kernel names the reference loop it restates;
+// floating-point expressions keep the reference's operand order (the library is built with
+// -fmad=false, so a*b+c rounds twice, as in the reference's -ffp-contract=off build).
+#include "flow.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace vlm {
+namespace {
+
+inline int nblk(int64_t n, int b = 256) { return int((n + b - 1) / b); }
+
+enum : int { kUpwind = 0, kLinear = 1, kLinearUpwind = 2, kLUST = 3 };
+
+// ---------------------------------------------------------------- boundary values of U
+// correctBoundaryConditions (VolField.h:96-103) for fixedValue (value) and zeroGradient (cell value)
+__global__ void k_u_boundary(int nB, int nI, int nC, const int32_t* __restrict__ own,
+                             const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                             const double* __restrict__ uValue, const double* __restrict__ U, double* __restrict__ Ub) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB) return;
+    const int q = bPatch[b];
+    const int c = own[nI + b];
+    for (int k = 0; k < 3; ++k) Ub[k * nB + b] = uType[q] == 1 ? uValue[3 * q + k] : U[k * nC + c];
+}
+
+// ---------------------------------------------------------------- fvc::grad of U (Gauss linear)
+// Fvc.h:214-225 + finishGrad (Fvc.h:169-181): G_ij = sum S_i phi_j / V, row `emptyDir` zero in 2D.
+// Output SoA: component (3i + j) at [(3i + j) * nC + c].
+__global__ void k_grad_tensor(int nC, int nI, int nB, int nF, const int32_t* __restrict__ cfOff,
+                              const int32_t* __restrict__ cf, const int32_t* __restrict__ own,
+                              const int32_t* __restrict__ nei, const double* __restrict__ w,
+                              const double* __restrict__ Sf, const double* __restrict__ V,
+                              const double* __restrict__ U, const double* __restrict__ Ub, int twoD, int emptyDir,
+                              double* __restrict__ G) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double g[9];
+    for (int m = 0; m < 9; ++m) g[m] = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = int(e & 0x7fffffffu);
+        double phif[3];
+        if (f < nI) {
+            const double wf = w[f], wn = 1.0 - wf;
+            for (int j = 0; j < 3; ++j) phif[j] = U[j * nC + own[f]] * wf + U[j * nC + nei[f]] * wn;
+        } else {
+            for (int j = 0; j < 3; ++j) phif[j] = Ub[j * nB + (f - nI)];
+        }
+        const double S[3] = {Sf[f], Sf[nF + f], Sf[2 * nF + f]};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const double t = S[i] * phif[j];
+                if (e >> 31)
+                    g[3 * i + j] -= t;
+                else
+                    g[3 * i + j] += t;
+            }
+    }
+    const double iv = 1.0 / V[c];
+    for (int m = 0; m < 9; ++m) g[m] = g[m] * iv;
+    if (twoD)
+        for (int j = 0; j < 3; ++j) g[3 * emptyDir + j] = 0.0;
+    for (int m = 0; m < 9; ++m) G[size_t(m) * nC + c] = g[m];
+}
+
+// v . T (Types.h: dot(Vec3, Tensor)) with T read from the SoA gradient of cell c
+__device__ __forceinline__ void vec_dot_tensor(const double v[3], const double* __restrict__ G, int nC, int c,
+                                               double out[3]) {
+    for (int j = 0; j < 3; ++j)
+        out[j] = v[0] * G[size_t(j) * nC + c] + v[1] * G[size_t(3 + j) * nC + c] + v[2] * G[size_t(6 + j) * nC + c];
+}
+
+// ---------------------------------------------------------------- momentum operators, internal faces
+// fvm::div(phi, U) (Fvm.h:74-123) and fvm::laplacian(nu, U) (Fvm.h:143-168) per internal face, and
+// the combined off-diagonals of UEqn = ddt + div - laplacian (FvMatrix.h:52-79, addOffDiag).
+__global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                            const double* __restrict__ w, const double* __restrict__ magSf,
+                            const double* __restrict__ ndc, const double* __restrict__ d,
+                            const double* __restrict__ corr, const double* __restrict__ C,
+                            const double* __restrict__ Cf, const double* __restrict__ phi, double nu, int scheme,
+                            int nonOrth, const double* __restrict__ G, double* __restrict__ loDiv,
+                            double* __restrict__ upDiv, double* __restrict__ lapUp, double* __restrict__ upper,
+                            double* __restrict__ lower, double* __restrict__ cDiv, double* __restrict__ ffc) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nI) return;
+    const double F = phi[f];
+    const double wUp = F >= 0 ? 1.0 : 0.0;
+    double wf;
+    if (scheme == kUpwind || scheme == kLinearUpwind)
+        wf = wUp;
+    else if (scheme == kLinear)
+        wf = w[f];
+    else
+        wf = 0.75 * w[f] + 0.25 * wUp;
+    const double lo = -wf * F;
+    const double up = lo + F;
+    const double lap = nu * magSf[f] * ndc[f];
+    loDiv[f] = lo;
+    upDiv[f] = up;
+    lapUp[f] = lap;
+    double u = 0.0, l = 0.0;
+    l += 1.0 * lo;
+    u += 1.0 * up;
+    l += -1.0 * lap;
+    u += -1.0 * lap;
+    upper[f] = u;
+    lower[f] = l;
+    const int o = own[f], n = nei[f];
+    // linearUpwind / LUST: explicit gradient correction (Fvm.h:106-116)
+    double cc[3] = {0.0, 0.0, 0.0};
+    if (scheme == kLinearUpwind || scheme == kLUST) {
+        const double fac = scheme == kLUST ? 0.25 : 1.0;
+        double v[3], corrv[3];
+        if (F >= 0) {
+            for (int k = 0; k < 3; ++k) v[k] = Cf[size_t(k) * nF + f] - C[size_t(k) * nC + o];
+            vec_dot_tensor(v, G, nC, o, corrv);
+        } else {
+            for (int k = 0; k < 3; ++k) v[k] = Cf[size_t(k) * nF + f] - (C[size_t(k) * nC + o] + d[size_t(k) * nF + f]);
+            vec_dot_tensor(v, G, nC, n, corrv);
+        }
+        const double s = fac * F;
+        for (int k = 0; k < 3; ++k) cc[k] = corrv[k] * s;
+    }
+    for (int k = 0; k < 3; ++k) cDiv[size_t(k) * nI + f] = cc[k];
+    // non-orthogonal correction of the laplacian (Fvm.h:155-167)
+    double fc[3] = {0.0, 0.0, 0.0};
+    if (nonOrth) {
+        const double wo = w[f], wn = 1.0 - wo;
+        double gf[9];
+        for (int m = 0; m < 9; ++m) gf[m] = G[size_t(m) * nC + o] * wo + G[size_t(m) * nC + n] * wn;
+        const double cv[3] = {corr[f], corr[nF + f], corr[2 * nF + f]};
+        const double s = nu * magSf[f];
+        for (int j = 0; j < 3; ++j) fc[j] = (cv[0] * gf[j] + cv[1] * gf[3 + j] + cv[2] * gf[6 + j]) * s;
+    }
+    for (int k = 0; k < 3; ++k) ffc[size_t(k) * nI + f] = fc[k];
+}
+
+// ---------------------------------------------------------------- momentum operators, boundary faces
+// div: internalCoeffs += F vic, boundarySource -= F vbc (Fvm.h:117-126); laplacian: += gs gic,
+// -= gs gbc (Fvm.h:169-178); fixedValue: vic 0, vbc U_b, gic -dc, gbc dc U_b; zeroGradient: vic 1,
+// others 0 (BoundaryCondition.h:104-130).  UEqn = (0 + div) - laplacian.
+__global__ void k_mom_bfaces(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                             const double* __restrict__ uValue, const double* __restrict__ magSf,
+                             const double* __restrict__ ndc, const double* __restrict__ phi, double nu,
+                             double* __restrict__ ic, double* __restrict__ bs) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB) return;
+    const int f = nI + b, q = bPatch[b];
+    const bool fixedValue = uType[q] == 1;
+    const double F = phi[f], dc = ndc[f], gs = nu * magSf[f];
+    for (int k = 0; k < 3; ++k) {
+        const double val = fixedValue ? uValue[3 * q + k] : 0.0;
+        const double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
+        const double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
+        double icDiv = 0.0, bsDiv = 0.0, icLap = 0.0, bsLap = 0.0;
+        icDiv += vic * F;
+        bsDiv -= vbc * F;
+        icLap += gic * gs;
+        bsLap -= gbc * gs;
+        double i = 0.0, s = 0.0;
+        i += icDiv;
+        s += bsDiv;
+        i -= icLap;
+        s -= bsLap;
+        ic[size_t(k) * nB + b] = i;
+        bs[size_t(k) * nB + b] = s;
+    }
+}
+
+// ---------------------------------------------------------------- momentum operators, cells
+// diag and source of ddt (Fvm.h:18-31), div and laplacian accumulated per operator in face order,
+// then UEqn = ddt; UEqn += div; UEqn -= laplacian (FvMatrix.h:52-79)
+__global__ void k_mom_cells(int nC, int nI, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                            const double* __restrict__ loDiv, const double* __restrict__ upDiv,
+                            const double* __restrict__ lapUp, const double* __restrict__ cDiv,
+                            const double* __restrict__ ffc, const double* __restrict__ V, int transient, double kc,
+                            double kc0, double kc00, const double* __restrict__ U0, const double* __restrict__ U00,
+                            double* __restrict__ diag, double* __restrict__ src) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double dDiv = 0.0, dLap = 0.0, sDiv[3] = {0.0, 0.0, 0.0}, sLap[3] = {0.0, 0.0, 0.0};
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = int(e & 0x7fffffffu);
+        if (f >= nI) continue;
+        if (e >> 31) {
+            dDiv -= upDiv[f];
+            dLap -= lapUp[f];
+            for (int q = 0; q < 3; ++q) {
+                sDiv[q] += cDiv[size_t(q) * nI + f];
+                sLap[q] += ffc[size_t(q) * nI + f];
+            }
+        } else {
+            dDiv -= loDiv[f];
+            dLap -= lapUp[f];
+            for (int q = 0; q < 3; ++q) {
+                sDiv[q] -= cDiv[size_t(q) * nI + f];
+                sLap[q] -= ffc[size_t(q) * nI + f];
+            }
+        }
+    }
+    double dg = 0.0, s[3] = {0.0, 0.0, 0.0};
+    if (transient) {
+        const double Vc = V[c];
+        dg += kc * Vc;
+        for (int q = 0; q < 3; ++q) {
+            const double t = U0[size_t(q) * nC + c] * kc0 - U00[size_t(q) * nC + c] * kc00;
+            s[q] += t * Vc;
+        }
+    }
+    dg += dDiv;
+    dg -= dLap;
+    diag[c] = dg;
+    for (int q = 0; q < 3; ++q) {
+        s[q] += sDiv[q];
+        s[q] -= sLap[q];
+        src[size_t(q) * nC + c] = s[q];
+    }
+}
+
+// ---------------------------------------------------------------- FvMatrix::relax (FvMatrix.h:111-131)
+__global__ void k_mom_relax(int nC, int nI, int nB, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                            const double* __restrict__ upper, const double* __restrict__ lower,
+                            const double* __restrict__ ic, const double* __restrict__ U, double alpha,
+                            double* __restrict__ diag, double* __restrict__ src) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double sumOff = 0.0, bD = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = int(e & 0x7fffffffu);
+        if (f < nI) {
+            sumOff += (e >> 31) ? fabs(lower[f]) : fabs(upper[f]);
+        } else {
+            const int b = f - nI;
+            double m = ic[b];
+            const double y = ic[size_t(nB) + b], z = ic[size_t(2) * nB + b];
+            if (m < y) m = y;
+            if (m < z) m = z;
+            bD += m;
+        }
+    }
+    const double Dfull = diag[c] + bD;
+    const double aD = fabs(Dfull);
+    const double D = aD < sumOff ? sumOff : aD;
+    const double dD = D / alpha - Dfull;
+    diag[c] += dD;
+    for (int q = 0; q < 3; ++q) src[size_t(q) * nC + c] += U[size_t(q) * nC + c] * dD;
+}
+
+// M = UEqn - (-grad p): source += (-grad p) V  (FvMatrix.h:89-97); gp: 3 per cell
+__global__ void k_mom_gradp(int nC, const double* __restrict__ src, const double* __restrict__ gp,
+                            const double* __restrict__ V, double* __restrict__ msrc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    for (int q = 0; q < 3; ++q) msrc[size_t(q) * nC + c] = src[size_t(q) * nC + c] + (-gp[3 * c + q]) * V[c];
+}
+
+// A (FvMatrix.h:178-187), rAU = 1/A, H (FvMatrix.h:189-206), HbyA = rAU H
+__global__ void k_mom_AH(int nC, int nI, int nB, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
+                         const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
+                         const double* __restrict__ diag, const double* __restrict__ upper,
+                         const double* __restrict__ lower, const double* __restrict__ ic, const double* __restrict__ bs,
+                         const double* __restrict__ src, const double* __restrict__ U, const double* __restrict__ V,
+                         double* __restrict__ rAU, double* __restrict__ HbyA) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double a = diag[c];
+    double h[3] = {src[c], src[size_t(nC) + c], src[size_t(2) * nC + c]};
+    const int k0 = cfOff[c], k1 = cfOff[c + 1];
+    // internal faces first (all of them precede the boundary faces in the cell's ascending list)
+    for (int k = k0; k < k1; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = int(e & 0x7fffffffu);
+        if (f >= nI) continue;
+        if (e >> 31) {
+            const double lf = lower[f];
+            const int o = own[f];
+            for (int q = 0; q < 3; ++q) h[q] -= U[size_t(q) * nC + o] * lf;
+        } else {
+            const double uf = upper[f];
+            const int n = nei[f];
+            for (int q = 0; q < 3; ++q) h[q] -= U[size_t(q) * nC + n] * uf;
+        }
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int f = int((uint32_t)cf[k] & 0x7fffffffu);
+        if (f < nI) continue;
+        const int b = f - nI;
+        const double icv[3] = {ic[b], ic[size_t(nB) + b], ic[size_t(2) * nB + b]};
+        const double av = (icv[0] + icv[1] + icv[2]) / 3.0;
+        a += av;
+        for (int q = 0; q < 3; ++q) {
+            h[q] += bs[size_t(q) * nB + b];
+            h[q] -= (icv[q] - av) * U[size_t(q) * nC + c];
+        }
+    }
+    a /= V[c];
+    const double r = 1.0 / a;
+    rAU[c] = r;
+    for (int q = 0; q < 3; ++q) HbyA[size_t(q) * nC + c] = (h[q] / V[c]) * r;
+}
+
+// rAUf = interpolate(rAU) (Fvc.h:24-32) and phiHbyA (IncompressibleFlow.cpp:258-281)
+__global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __restrict__ own,
+                           const int32_t* __restrict__ nei, const double* __restrict__ w, const double* __restrict__ Sf,
+                           const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                           const double* __restrict__ rAU, const double* __restrict__ HbyA,
+                           const double* __restrict__ Ub, double* __restrict__ rAUf, double* __restrict__ phiHbyA) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const double S[3] = {Sf[f], Sf[nF + f], Sf[2 * nF + f]};
+    const int o = own[f];
+    if (f < nI) {
+        const int n = nei[f];
+        const double wf = w[f], wn = 1.0 - wf;
+        rAUf[f] = wf * rAU[o] + wn * rAU[n];
+        double Hf[3];
+        for (int q = 0; q < 3; ++q) Hf[q] = HbyA[size_t(q) * nC + o] * wf + HbyA[size_t(q) * nC + n] * wn;
+        phiHbyA[f] = Hf[0] * S[0] + Hf[1] * S[1] + Hf[2] * S[2];
+    } else {
+        const int b = f - nI;
+        rAUf[f] = rAU[o];
+        if (uType[bPatch[b]] == 1)
+            phiHbyA[f] = Ub[b] * S[0] + Ub[size_t(nB) + b] * S[1] + Ub[size_t(2) * nB + b] * S[2];
+        else
+            phiHbyA[f] = HbyA[o] * S[0] + HbyA[size_t(nC) + o] * S[1] + HbyA[size_t(2) * nC + o] * S[2];
+    }
+}
+
+// phi = phiHbyA - flux (IncompressibleFlow.cpp:337-340)
+__global__ void k_phi_update(int nF, const double* __restrict__ phiHbyA, const double* __restrict__ F,
+                             double* __restrict__ phi) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < nF) phi[f] = phiHbyA[f] - F[f];
+}
+
+// p = pPrev + alphaP (p - pPrev) (IncompressibleFlow.cpp:345-348)
+__global__ void k_p_relax(int nC, const double* __restrict__ pPrev, double alpha, double* __restrict__ p) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nC) p[c] = pPrev[c] + alpha * (p[c] - pPrev[c]);
+}
+
+// U = HbyA - rAU grad p, empty direction zeroed (IncompressibleFlow.cpp:355-360)
+__global__ void k_u_correct(int nC, const double* __restrict__ HbyA, const double* __restrict__ rAU,
+                            const double* __restrict__ gp, int twoD, int emptyDir, double* __restrict__ U) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    for (int q = 0; q < 3; ++q) U[size_t(q) * nC + c] = HbyA[size_t(q) * nC + c] - gp[3 * c + q] * rAU[c];
+    if (twoD) U[size_t(emptyDir) * nC + c] = 0.0;
+}
+
+// phi = U_f . S_f with boundary faces at the boundary value (Fvc.h:103-109, initialize)
+__global__ void k_flux_u(int nF, int nI, int nB, int nC, const int32_t* __restrict__ own,
+                         const int32_t* __restrict__ nei, const double* __restrict__ w, const double* __restrict__ Sf,
+                         const double* __restrict__ U, const double* __restrict__ Ub, double* __restrict__ phi) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    double Uf[3];
+    if (f < nI) {
+        const double wf = w[f], wn = 1.0 - wf;
+        for (int q = 0; q < 3; ++q) Uf[q] = U[size_t(q) * nC + own[f]] * wf + U[size_t(q) * nC + nei[f]] * wn;
+    } else {
+        for (int q = 0; q < 3; ++q) Uf[q] = Ub[size_t(q) * nB + (f - nI)];
+    }
+    phi[f] = Uf[0] * Sf[f] + Uf[1] * Sf[nF + f] + Uf[2] * Sf[2 * nF + f];
+}
+
+// max |div phi| (the values are non-negative: the IEEE bit patterns order like the numbers)
+__global__ void k_max_abs(int n, const double* __restrict__ v, unsigned long long* __restrict__ out) {
+    unsigned long long m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = fabs(v[i]);
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(a);
+        if (bits > m) m = bits;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_down_sync(0xffffffffu, m, o);
+        if (t > m) m = t;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// U: SoA <-> AoS (3 per cell)
+__global__ void k_soa_from_aos(int n, const double* __restrict__ a, double* __restrict__ s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        for (int q = 0; q < 3; ++q) s[size_t(q) * n + i] = a[3 * size_t(i) + q];
+}
+__global__ void k_aos_from_soa(int n, const double* __restrict__ s, double* __restrict__ a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        for (int q = 0; q < 3; ++q) a[3 * size_t(i) + q] = s[size_t(q) * n + i];
+}
+
+}  // namespace
+
+// ====================================================================== DeviceFlow
+DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl& ctrl, const int32_t* uType,
+                       const double* uValue, const int32_t* pType, const double* pValue, cudaStream_t s)
+    : batch_(batch), G_(geom), ctrl_(ctrl), s_(s) {
+    nC_ = G_.nCells();
+    nI_ = G_.nInternal();
+    nF_ = G_.nFaces();
+    nB_ = G_.nBoundary();
+    const int nP = G_.nPatches();
+    VLM_REQUIRE(batch_.plan().nsys == 1, VLM_ERR_UNSUPPORTED, "the device flow step runs on a single-system mesh");
+    VLM_REQUIRE(ctrl_.div_scheme >= 0 && ctrl_.div_scheme <= 3, VLM_ERR_BAD_ARG, "unknown divergence scheme");
+    VLM_REQUIRE(ctrl_.ddt_scheme >= 0 && ctrl_.ddt_scheme <= 2, VLM_ERR_BAD_ARG, "unknown ddt scheme");
+    VLM_REQUIRE(!ctrl_.steady || ctrl_.ddt_scheme == 0 || true, VLM_ERR_BAD_ARG, "");
+    VLM_REQUIRE(ctrl_.nu > 0, VLM_ERR_BAD_ARG, "nu must be positive");
+    VLM_REQUIRE(ctrl_.n_corr >= 1 && ctrl_.n_outer >= 1 && ctrl_.n_non_orth_corr >= 0, VLM_ERR_BAD_ARG,
+                "nOuter, nCorr must be >= 1 and nNonOrthCorr >= 0");
+    if (ctrl_.div_scheme == kLinearUpwind || ctrl_.div_scheme == kLUST)
+        VLM_REQUIRE(G_.C() && G_.Cf(), VLM_ERR_BAD_ARG,
+                    "linearUpwind / LUST need the cell and face centres (vlm_mesh_desc.C, .Cf)");
+    uTypeHost_.assign(uType, uType + nP);
+    pTypeHost_.assign(pType, pType + nP);
+    for (int q = 0; q < nP; ++q) {
+        VLM_REQUIRE(uType[q] == 0 || uType[q] == 1, VLM_ERR_BAD_ARG, "U boundary type must be 0 or 1");
+        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1, VLM_ERR_BAD_ARG, "p boundary type must be 0 or 1");
+    }
+    // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
+    needRef_ = true;
+    for (int q = 0; q < nP; ++q)
+        if (pType[q] == 1 && G_.patchSize()[q] > 0) needRef_ = false;
+    if (needRef_)
+        VLM_REQUIRE(ctrl_.p_ref_cell >= 0 && ctrl_.p_ref_cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
+    for (int k = 0; k < 3; ++k)
+        if (!G_.twoD() || k != G_.emptyDir()) solved_.push_back(k);  // Mesh.cpp:642-644
+    uType_.upload(uTypeHost_, s_);
+    uValue_.upload(uValue, size_t(3) * std::max(nP, 1), s_);
+    std::vector<double> pv(size_t(std::max(nB_, 1)), 0.0);
+    for (int q = 0; q < nP; ++q)
+        for (int i = 0; i < G_.patchSize()[q]; ++i) pv[size_t(G_.patchStart()[q] - nI_ + i)] = pValue[q];
+    pValueB_.upload(pv, s_);
+    const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1)), FI = size_t(std::max(nI_, 1)), F = size_t(nF_);
+    for (DBuf<double>* b : {&U_, &U0_, &U00_, &src_, &msrc_, &HbyA_}) b->resize(3 * N);
+    for (DBuf<double>* b : {&Ub_, &ic_, &bs_}) b->resize(3 * B);
+    for (DBuf<double>* b : {&p_, &diag_, &rAU_, &divPhi_, &pPrev_, &fd_, &fb_, &pdiag_, &psrc_}) b->resize(N);
+    for (DBuf<double>* b : {&pB_, &pic_, &pbs_}) b->resize(B);
+    for (DBuf<double>* b : {&upper_, &lower_, &loDiv_, &upDiv_, &lapUp_}) b->resize(FI);
+    for (DBuf<double>* b : {&cDiv_, &ffc_}) b->resize(3 * FI);
+    for (DBuf<double>* b : {&phi_, &rAUf_, &phiHbyA_, &pffc_, &pflux_}) b->resize(F);
+    pupper_.resize(FI);
+    gU_.resize(9 * N);
+    gP_.resize(3 * N);
+    cont_.resize(1);
+    for (DBuf<double>* b : {&U_, &U0_, &U00_, &p_, &phi_, &pffc_}) b->zero(s_);
+}
+
+void DeviceFlow::boundaryU() {
+    if (nB_ > 0)
+        k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, G_.own(), G_.bPatch(), uType_.get(), uValue_.get(),
+                                                U_.get(), Ub_.get());
+}
+
+void DeviceFlow::boundaryP() {
+    ScalarBC bc;
+    bc.type = pTypeHost_.data();
+    bc.value = pValueB_.get();
+    G_.correctBoundary(p_.get(), bc, pB_.get(), s_);
+}
+
+void DeviceFlow::gradU() {
+    k_grad_tensor<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, nF_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
+                                            G_.w(), G_.Sf(), G_.V(), U_.get(), Ub_.get(), G_.twoD(), G_.emptyDir(),
+                                            gU_.get());
+}
+
+void DeviceFlow::setState(const double* U, const double* p) {
+    if (U) {
+        DBuf<double> tmp;
+        tmp.upload(U, size_t(3) * nC_, s_);
+        k_soa_from_aos<<<nblk(nC_), 256, 0, s_>>>(nC_, tmp.get(), U_.get());
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    }
+    if (p) p_.upload(p, size_t(nC_), s_);
+    boundaryU();
+    boundaryP();
+    k_flux_u<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), U_.get(), Ub_.get(),
+                                       phi_.get());
+    rAU_.zero(s_);
+    VLM_CUDA(cudaGetLastError());
+    VLM_CUDA(cudaStreamSynchronize(s_));
+    initialized_ = true;
+}
+
+void DeviceFlow::getState(double* U, double* p, double* phi) {
+    if (U) {
+        DBuf<double> tmp(size_t(3) * nC_);
+        k_aos_from_soa<<<nblk(nC_), 256, 0, s_>>>(nC_, U_.get(), tmp.get());
+        VLM_CUDA(cudaMemcpyAsync(U, tmp.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    }
+    if (p) VLM_CUDA(cudaMemcpyAsync(p, p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToHost, s_));
+    if (phi) VLM_CUDA(cudaMemcpyAsync(phi, phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToHost, s_));
+    VLM_CUDA(cudaStreamSynchronize(s_));
+}
+
+// UEqn = ddt + div(phi, U) - laplacian(nu, U), relaxed by aU (IncompressibleFlow.cpp:176-198)
+void DeviceFlow::assembleMomentum(double aU) {
+    const bool needG = ctrl_.div_scheme == kLinearUpwind || ctrl_.div_scheme == kLUST || G_.nonOrthogonal();
+    if (needG) gradU();
+    if (nI_ > 0)
+        k_mom_faces<<<nblk(nI_), 256, 0, s_>>>(nI_, nC_, nF_, G_.own(), G_.nei(), G_.w(), G_.magSf(), G_.ndc(), G_.d(),
+                                              G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, ctrl_.div_scheme,
+                                              G_.nonOrthogonal() ? 1 : 0, gU_.get(), loDiv_.get(), upDiv_.get(),
+                                              lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get());
+    if (nB_ > 0)
+        k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), uValue_.get(), G_.magSf(),
+                                               G_.ndc(), phi_.get(), ctrl_.nu, ic_.get(), bs_.get());
+    // ddt coefficients (Schemes.h:70-86)
+    double kc = 0, kc0 = 0, kc00 = 0;
+    const bool transient = !ctrl_.steady;
+    if (transient) {
+        const double rDt = 1.0 / dt_;
+        if (ctrl_.ddt_scheme == 2 && nOld_ >= 2 && dt0_ > 0) {
+            const double ct = 1.0 + dt_ / (dt_ + dt0_);
+            const double ct00 = dt_ * dt_ / (dt0_ * (dt_ + dt0_));
+            kc = ct * rDt;
+            kc0 = (ct + ct00) * rDt;
+            kc00 = ct00 * rDt;
+        } else {
+            kc = kc0 = rDt;
+        }
+    }
+    k_mom_cells<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, G_.cellFaceOff(), G_.cellFaces(), loDiv_.get(), upDiv_.get(),
+                                          lapUp_.get(), cDiv_.get(), ffc_.get(), G_.V(), transient ? 1 : 0, kc, kc0,
+                                          kc00, U0_.get(), nOld_ >= 2 ? U00_.get() : U0_.get(), diag_.get(),
+                                          src_.get());
+    if (aU < 1.0)
+        k_mom_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), upper_.get(),
+                                              lower_.get(), ic_.get(), U_.get(), aU, diag_.get(), src_.get());
+    VLM_CUDA(cudaGetLastError());
+}
+
+// Momentum predictor: M = UEqn + grad p, one solve per solved component (FvMatrix.h:144-175)
+void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
+    ScalarBC pbc;
+    pbc.type = pTypeHost_.data();
+    pbc.value = pValueB_.get();
+    G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+    k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get());
+    double r = 0, nf = 0;
+    const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
+    for (int k : solved_) {
+        G_.fold(diag_.get(), msrc_.get() + k * N, ic_.get() + k * B, bs_.get() + k * B, fd_.get(), fb_.get(), s_);
+        std::vector<vlm_solver_perf> pf;
+        batch_.solve(fd_.get(), upper_.get(), lower_.get(), fb_.get(), U_.get() + k * N, ctrl_.U, pf);
+        info.iterations += pf[0].iterations;
+        r = std::max(r, pf[0].residualSum);
+        nf = std::max(nf, pf[0].normFactor);
+    }
+    boundaryU();
+    if (first) info.UInitialResidual = r / (nf + 1e-30);
+}
+
+// One pressure correction (IncompressibleFlow.cpp:244-362)
+void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info) {
+    k_mom_AH<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
+                                       diag_.get(), upper_.get(), lower_.get(), ic_.get(), bs_.get(), src_.get(),
+                                       U_.get(), G_.V(), rAU_.get(), HbyA_.get());
+    k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
+                                         uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(), rAUf_.get(),
+                                         phiHbyA_.get());
+    G_.div(phiHbyA_.get(), divPhi_.get(), s_);
+    if (ctrl_.steady) VLM_CUDA(cudaMemcpyAsync(pPrev_.get(), p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToDevice, s_));
+    ScalarBC pbc;
+    pbc.type = pTypeHost_.data();
+    pbc.value = pValueB_.get();
+    const int nNO = ctrl_.n_non_orth_corr;
+    for (int no = 0; no <= nNO; ++no) {
+        const bool finalNO = no == nNO;
+        bool hasFfc = false;
+        G_.laplacian(rAUf_.get(), p_.get(), pB_.get(), pbc, true, 0, pdiag_.get(), pupper_.get(), psrc_.get(),
+                     pic_.get(), pbs_.get(), pffc_.get(), &hasFfc, s_);
+        G_.addVolumeSource(psrc_.get(), divPhi_.get(), s_);
+        if (needRef_) G_.setReference(ctrl_.p_ref_cell, ctrl_.p_ref_value, pdiag_.get(), psrc_.get(), s_);
+        G_.fold(pdiag_.get(), psrc_.get(), pic_.get(), pbs_.get(), fd_.get(), fb_.get(), s_);
+        std::vector<vlm_solver_perf> pf;
+        batch_.solve(fd_.get(), pupper_.get(), pupper_.get(), fb_.get(), p_.get(),
+                     (finalCorr && finalNO) ? ctrl_.p_final : ctrl_.p, pf);
+        info.iterations += pf[0].iterations;
+        if (first && no == 0) {
+            // monitored pressure residual with a normalisation floor (IncompressibleFlow.cpp:320-327)
+            if (pNormSteps_ < 5) {
+                pNormRef_ = std::max(pNormRef_, pf[0].normFactor);
+                ++pNormSteps_;
+            }
+            info.pInitialResidual = pf[0].residualSum / (std::max(pf[0].normFactor, pNormRef_) + 1e-30);
+        }
+        boundaryP();
+        if (finalNO) {
+            G_.flux(pupper_.get(), p_.get(), pic_.get(), pbs_.get(), hasFfc ? pffc_.get() : nullptr, pflux_.get(), s_);
+            k_phi_update<<<nblk(nF_), 256, 0, s_>>>(nF_, phiHbyA_.get(), pflux_.get(), phi_.get());
+        }
+    }
+    if (ctrl_.steady && ctrl_.alpha_p < 1.0) {
+        k_p_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, pPrev_.get(), ctrl_.alpha_p, p_.get());
+        boundaryP();
+    }
+    G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+    k_u_correct<<<nblk(nC_), 256, 0, s_>>>(nC_, HbyA_.get(), rAU_.get(), gP_.get(), G_.twoD(), G_.emptyDir(),
+                                          U_.get());
+    boundaryU();
+    VLM_CUDA(cudaGetLastError());
+}
+
+vlm_step_info DeviceFlow::step(double dt) {
+    if (!initialized_) setState(nullptr, nullptr);
+    vlm_step_info info;
+    std::memset(&info, 0, sizeof info);
+    const bool steady = ctrl_.steady != 0;
+    if (!steady) {
+        VLM_REQUIRE(dt > 0, VLM_ERR_BAD_ARG, "dt must be positive");
+        dt0_ = timeIndex_ > 0 ? dt_ : -1.0;
+        dt_ = dt;
+        time_ += dt;
+        ++timeIndex_;
+        // VolField::storeOld (VolField.h:114-118)
+        if (nOld_ >= 1)
+            VLM_CUDA(cudaMemcpyAsync(U00_.get(), U0_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
+        VLM_CUDA(cudaMemcpyAsync(U0_.get(), U_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
+        nOld_ = std::min(nOld_ + 1, 2);
+    } else {
+        time_ += 1.0;
+        ++timeIndex_;
+    }
+    boundaryU();
+    boundaryP();
+    for (int outer = 0; outer < ctrl_.n_outer; ++outer) {
+        const bool finalOuter = outer == ctrl_.n_outer - 1;
+        const double aU = steady ? ctrl_.alpha_u : (finalOuter ? 1.0 : ctrl_.alpha_u);
+        assembleMomentum(aU);
+        if (ctrl_.momentum_predictor) solveMomentum(info, outer == 0);
+        for (int corr = 0; corr < ctrl_.n_corr; ++corr)
+            correctPressure(finalOuter && corr == ctrl_.n_corr - 1, outer == 0 && corr == 0, info);
+    }
+    // continuity error: max |div phi| (IncompressibleFlow.cpp:367-370)
+    G_.div(phi_.get(), divPhi_.get(), s_);
+    cont_.zero(s_);
+    k_max_abs<<<std::min(nblk(nC_), 1184), 256, 0, s_>>>(nC_, divPhi_.get(), (unsigned long long*)cont_.get());
+    VLM_CUDA(cudaMemcpyAsync(&info.continuityError, cont_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
+    VLM_CUDA(cudaStreamSynchronize(s_));
+    VLM_CUDA(cudaGetLastError());
+    return info;
+}
+
+}  // namespace vlm

@@ -1,0 +1,80 @@
+// Device-resident incompressible step: IncompressibleFlow::step (solvers/IncompressibleFlow.cpp:138-370)
+// for laminar flow on a mesh whose geometry is registered on the device.
+//
+// One step: momentum assembly (fvm::ddt + fvm::div(phi, U) - fvm::laplacian(nu, U), Fvm.h:18-182),
+// implicit under-relaxation (FvMatrix::relax, FvMatrix.h:111-131), the momentum predictor (one
+// PBiCGStab/DILU solve per solved component), then nCorr pressure corrections: A, H, HbyA, rAUf and
+// the face flux phiHbyA (Rhie-Chow, IncompressibleFlow.cpp:244-292), the pressure equation with its
+// non-orthogonal correctors (GAMG-PCG), phi = phiHbyA - flux, the explicit pressure relaxation
+// (steady) and U = HbyA - rAU grad p.  Every array stays on the device; the host reads only the
+// solver performance records and the step's residual figures.
+//
+// Every kernel restates one loop of the reference with its accumulation order (per cell: its faces
+// in ascending face order; per boundary face: the order of the patch), so in CFD_REPRODUCIBLE mode
+// (exact sums, diagonal preconditioning) a step reproduces the reference's fields bit for bit.
+//
+// Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
+// linear / linearUpwind / LUST, Gauss linear gradients, fixedValue and zeroGradient boundary
+// conditions for U and p, empty (2D) directions and cyclic (internal) faces.  Not supported (an
+// UNSUPPORTED status): skewed meshes, turbulence, body forces, momentum forcing, ddtPhiCoeff.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "assembly.h"
+#include "solver.h"
+#include "voluma_b200.h"
+
+namespace vlm {
+
+class DeviceFlow {
+public:
+    // uType/pType: per patch 0 zeroGradient, 1 fixedValue; uValue 3 per patch, pValue 1 per patch.
+    DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl& ctrl, const int32_t* uType,
+               const double* uValue, const int32_t* pType, const double* pValue, cudaStream_t stream);
+
+    // IncompressibleFlow::initialize (IncompressibleFlow.cpp:32-40) from host fields (U: 3 per cell)
+    void setState(const double* U, const double* p);
+    // IncompressibleFlow::step(dt)
+    vlm_step_info step(double dt);
+    // fields to host (any pointer may be null)
+    void getState(double* U, double* p, double* phi);
+
+private:
+    void boundaryU();
+    void boundaryP();
+    void gradU();
+    void assembleMomentum(double aU);
+    void solveMomentum(vlm_step_info& info, bool first);
+    void correctPressure(bool finalCorr, bool first, vlm_step_info& info);
+
+    DeviceBatch& batch_;
+    DeviceGeom& G_;
+    vlm_flow_ctrl ctrl_;
+    cudaStream_t s_;
+    int nC_, nI_, nF_, nB_;
+    bool needRef_ = false;
+    std::vector<int32_t> uTypeHost_, pTypeHost_;
+    std::vector<int> solved_;
+    DBuf<int32_t> uType_;
+    DBuf<double> uValue_, pValueB_;
+    // fields (vectors SoA: component k at [k * n])
+    DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_;
+    // momentum matrix: UEqn (diag, upper, lower, source, internalCoeffs, boundarySource)
+    DBuf<double> diag_, upper_, lower_, src_, ic_, bs_;
+    // face terms of the operators and their per-cell sums
+    DBuf<double> loDiv_, upDiv_, lapUp_, cDiv_, ffc_;
+    // momentum predictor and pressure correction
+    DBuf<double> gU_, gP_, msrc_, rAU_, HbyA_, rAUf_, phiHbyA_, divPhi_, pPrev_, fd_, fb_;
+    DBuf<double> pdiag_, pupper_, psrc_, pic_, pbs_, pffc_, pflux_;
+    DBuf<double> cont_;  // continuity error (max, as ordered bits)
+    // time state (Schemes.h TimeState) and the pressure-residual normalisation of the step
+    double time_ = 0, dt_ = 1, dt0_ = -1;
+    int timeIndex_ = 0, nOld_ = 0;
+    double pNormRef_ = 0;
+    int pNormSteps_ = 0;
+    bool initialized_ = false;
+};
+
+}  // namespace vlm
