@@ -59,7 +59,10 @@ DiluPlan buildDiluPlan(const std::vector<SysTopo>& systems, const BatchPlan& P) 
         ds.sys = b;
         ds.levBegin = int(D.levPtr.size()) - 1;
         ds.nLev = nLev;
+        ds.rowBegin = L0.sysRow[b];
+        ds.rowCount = L0.sysRow[b + 1] - L0.sysRow[b];
         ds.pad = 0;
+        D.maxRows = std::max(D.maxRows, ds.rowCount);
         for (auto& v : byLevel) {
             std::sort(v.begin(), v.end());
             D.maxWidth = std::max(D.maxWidth, int(v.size()));

@@ -137,6 +137,121 @@ __global__ void __launch_bounds__(kDiluThreads) k_dilu_apply(const DiluSys* __re
     }
 }
 
+// ---------------------------------------------------------------- shared-memory variants
+// One CTA per system whose level-0 vector fits in shared memory and whose levels are at most one
+// row per thread.  The swept vector lives in shared memory, and each thread loads its row of the
+// NEXT level (row index, scalars and the first kDiluPre coefficients) before the barrier that ends
+// the current level, so a level costs a barrier and shared-memory reads, not an L2 round trip.
+// Same arithmetic in the same order as k_dilu_factor / k_dilu_apply.
+constexpr int kDiluPre = 4;
+
+struct DiluRow {
+    int c, k0, k1;
+    double a, b;                      // apply: rD[c], r[c]; factor: diag[c]
+    int col[kDiluPre];
+    double v0[kDiluPre], v1[kDiluPre];  // apply: A_ul (fwd) / A_lu (bwd); factor: A_lu, A_ul
+};
+
+__device__ __forceinline__ void dilu_row_load(const DiluSys& d, int t, int tid, const int32_t* __restrict__ levPtr,
+                                              const int32_t* __restrict__ levRows, const int32_t* __restrict__ ptr,
+                                              const int32_t* __restrict__ col, const double* __restrict__ c0,
+                                              const double* __restrict__ c1, const double* __restrict__ sa,
+                                              const double* __restrict__ sb, DiluRow& p) {
+    p.c = -1;
+    if (t < 0 || t >= d.nLev) return;
+    const int idx = levPtr[d.levBegin + t] + tid;
+    if (idx >= levPtr[d.levBegin + t + 1]) return;
+    p.c = levRows[idx];
+    p.a = sa[p.c];
+    p.b = sb ? sb[p.c] : 0.0;
+    p.k0 = ptr[p.c];
+    p.k1 = ptr[p.c + 1];
+#pragma unroll
+    for (int q = 0; q < kDiluPre; ++q)
+        if (p.k0 + q < p.k1) {
+            p.col[q] = col[p.k0 + q];
+            p.v0[q] = c0[p.k0 + q];
+            p.v1[q] = c1 ? c1[p.k0 + q] : 0.0;
+        }
+}
+
+__global__ void __launch_bounds__(kDiluThreads) k_dilu_factor_smem(const DiluSys* __restrict__ ds,
+                                                                   const int32_t* __restrict__ levPtr,
+                                                                   const int32_t* __restrict__ levRows,
+                                                                   const int32_t* __restrict__ loPtr,
+                                                                   const int32_t* __restrict__ loCol,
+                                                                   const double* __restrict__ loAlu,
+                                                                   const double* __restrict__ loAul,
+                                                                   const double* __restrict__ diag,
+                                                                   double* __restrict__ rD) {
+    extern __shared__ double sh[];
+    const DiluSys d = ds[blockIdx.x];
+    const int base = d.rowBegin, tid = threadIdx.x;
+    DiluRow cur, nxt;
+    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, cur);
+    for (int t = 0; t < d.nLev; ++t) {
+        dilu_row_load(d, t + 1, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, nxt);
+        if (cur.c >= 0) {
+            double v = cur.a;
+            const int np = min(cur.k1 - cur.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) v -= cur.v0[q] * cur.v1[q] / sh[cur.col[q] - base];
+            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) v -= loAlu[k] * loAul[k] / sh[loCol[k] - base];
+            sh[cur.c - base] = v;
+        }
+        __syncthreads();
+        cur = nxt;
+    }
+    for (int i = tid; i < d.rowCount; i += blockDim.x) rD[base + i] = 1.0 / sh[i];
+}
+
+__global__ void __launch_bounds__(kDiluThreads) k_dilu_apply_smem(const DiluSys* __restrict__ ds,
+                                                                  const int32_t* __restrict__ levPtr,
+                                                                  const int32_t* __restrict__ levRows,
+                                                                  const int32_t* __restrict__ loPtr,
+                                                                  const int32_t* __restrict__ loCol,
+                                                                  const double* __restrict__ loAul,
+                                                                  const int32_t* __restrict__ upPtr,
+                                                                  const int32_t* __restrict__ upCol,
+                                                                  const double* __restrict__ upAlu,
+                                                                  const double* __restrict__ rD, const double* r,
+                                                                  double* w, const SysState* st, int flag) {
+    pdl_entry();
+    extern __shared__ double sh[];
+    const DiluSys d = ds[blockIdx.x];
+    if (st != nullptr && sys_idle(st[d.sys], flag)) return;
+    const int base = d.rowBegin, tid = threadIdx.x;
+    DiluRow cur, nxt;
+    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, cur);
+    for (int t = 0; t < d.nLev; ++t) {
+        dilu_row_load(d, t + 1, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, nxt);
+        if (cur.c >= 0) {
+            const double rd = cur.a;
+            double wc = rd * cur.b;
+            const int np = min(cur.k1 - cur.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) wc -= rd * cur.v0[q] * sh[cur.col[q] - base];
+            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) wc -= rd * loAul[k] * sh[loCol[k] - base];
+            sh[cur.c - base] = wc;
+        }
+        __syncthreads();
+        cur = nxt;
+    }
+    dilu_row_load(d, d.nLev - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, cur);
+    for (int t = d.nLev - 1; t >= 0; --t) {
+        dilu_row_load(d, t - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, nxt);
+        if (cur.c >= 0) {
+            const double rd = cur.a;
+            double wc = sh[cur.c - base];
+            const int np = min(cur.k1 - cur.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) wc -= rd * cur.v0[q] * sh[cur.col[q] - base];
+            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) wc -= rd * upAlu[k] * sh[upCol[k] - base];
+            sh[cur.c - base] = wc;
+        }
+        __syncthreads();
+        cur = nxt;
+    }
+    for (int i = tid; i < d.rowCount; i += blockDim.x) w[base + i] = sh[i];
+}
+
 // Gauss-Seidel sweep in natural order (forward) or reversed (backward), in place:
 // x[c] = (b[c] - sum over the row's entries in face order of a * x) / D[c], where the lower
 // neighbours already hold this sweep's value (LinearSolver.cpp:245-275, sweepCell)

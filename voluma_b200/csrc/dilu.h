@@ -20,7 +20,7 @@ namespace vlm {
 // One system's part of the schedule (batch position `sys`): levels [levBegin, levBegin + nLev) of
 // the concatenated level table.
 struct DiluSys {
-    int sys, levBegin, nLev, pad;
+    int sys, levBegin, nLev, rowBegin, rowCount, pad;  // rows [rowBegin, rowBegin + rowCount) of level 0
 };
 
 struct DiluPlan {
@@ -34,6 +34,7 @@ struct DiluPlan {
     std::vector<DiluSys> sys;
     int maxWidth = 0;  // widest level over all systems
     int maxLevels = 0;
+    int maxRows = 0;   // largest system (level-0 rows incl. padding)
 };
 
 // systems: input order; P: the batch plan (solver order, perm0).

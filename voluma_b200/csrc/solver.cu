@@ -26,6 +26,7 @@ struct DiluDev {
     DBuf<DiluBar> bars;
     DBuf<int> err;
     int G = 1, groups = 0, nFaces = 0;
+    size_t smem = 0;  // > 0: shared-memory sweeps with this many bytes per CTA
 };
 
 
@@ -372,10 +373,16 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
             if (c.level == k) nmax = std::max(nmax, c.n);
         const int smemN = nmax <= kCoarseSharedN ? nmax : 0;
         const size_t smem = size_t(2) * smemN * smemN * sizeof(double);
-        if (smem > 48 * 1024)
-            VLM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        // the opt-in limit is per function and shared by every mesh: raised once to the ceiling
+        static const bool raised = [] {
+            VLM_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(size_t(2) * kCoarseSharedN * kCoarseSharedN * sizeof(double))));
+            return true;
+        }();
+        (void)raised;
         k_coarse_factor<<<D.coarse.n, 128, smem, s>>>(coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
                                                      D.diag.get(), lu_.get(), inv_.get(), status_.get(), smemN);
+        VLM_CUDA(cudaGetLastError());
         ++tl_launches;
     }
 }
@@ -726,6 +733,22 @@ void DeviceBatch::ensureDilu() {
         const int resident = sms * std::max(1, std::min(per, std::min(perF, perG)));
         D->G = std::max(1, std::min({(P.maxWidth + kDiluThreads - 1) / kDiluThreads, resident, sms}));
     }
+    // shared-memory sweeps: one CTA per system, every level at most one row per thread, the vector
+    // of the largest system within the opt-in shared memory
+    // (the kernels' opt-in limit is a per-function setting shared by every mesh: it is raised once to
+    // the ceiling, never to one mesh's size)
+    constexpr size_t kDiluSmemMax = 200 * 1024;
+    if (D->G == 1 && P.maxWidth <= kDiluThreads && size_t(P.maxRows) * sizeof(double) <= kDiluSmemMax) {
+        static const bool raised = [] {
+            VLM_CUDA(cudaFuncSetAttribute(k_dilu_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(kDiluSmemMax)));
+            VLM_CUDA(cudaFuncSetAttribute(k_dilu_apply_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(kDiluSmemMax)));
+            return true;
+        }();
+        (void)raised;
+        D->smem = std::max<size_t>(size_t(P.maxRows) * sizeof(double), 8);
+    }
     D->bars.resize(size_t(D->groups));
     D->bars.zero(s);
     D->err.resize(1);
@@ -757,6 +780,14 @@ void DeviceBatch::diluFactor(const double* upper, const double* lower) {
     cudaStream_t s = stream_;
     VLM_LAUNCH(k_dilu_values, nblk(Dd.nFaces), 256, s, Dd.nFaces, (const int32_t*)Dd.loFace.get(),
                (const int32_t*)Dd.upFace.get(), upper, lower, Dd.loAul.get(), Dd.loAlu.get(), Dd.upAlu.get());
+    if (Dd.smem) {
+        k_dilu_factor_smem<<<Dd.groups, kDiluThreads, Dd.smem, s>>>(Dd.sys.get(), Dd.levPtr.get(), Dd.levRows.get(),
+                                                                    Dd.loPtr.get(), Dd.loCol.get(), Dd.loAlu.get(),
+                                                                    Dd.loAul.get(), L_[0].diag.get(), Dd.rD.get());
+        VLM_CUDA(cudaGetLastError());
+        ++tl_launches;
+        return;
+    }
     launchLevels(k_dilu_factor, Dd.groups, Dd.G, s, (const DiluSys*)Dd.sys.get(), Dd.G, (const int32_t*)Dd.levPtr.get(),
                  (const int32_t*)Dd.levRows.get(), (const int32_t*)Dd.loPtr.get(), (const int32_t*)Dd.loCol.get(),
                  (const double*)Dd.loAlu.get(), (const double*)Dd.loAul.get(), (const double*)L_[0].diag.get(),
@@ -777,6 +808,14 @@ void DeviceBatch::checkLevelError() {
 
 void DeviceBatch::recordDiluApply(const double* r, double* w) {
     DiluDev& D = *dilu_;
+    if (D.smem) {
+        k_dilu_apply_smem<<<D.groups, kDiluThreads, D.smem, stream_>>>(
+            D.sys.get(), D.levPtr.get(), D.levRows.get(), D.loPtr.get(), D.loCol.get(), D.loAul.get(), D.upPtr.get(),
+            D.upCol.get(), D.upAlu.get(), D.rD.get(), r, w, st_.get(), kFlagDone);
+        VLM_CUDA(cudaGetLastError());
+        ++tl_launches;
+        return;
+    }
     launchLevels(k_dilu_apply, D.groups, D.G, stream_, (const DiluSys*)D.sys.get(), D.G, (const int32_t*)D.levPtr.get(),
                  (const int32_t*)D.levRows.get(), (const int32_t*)D.loPtr.get(), (const int32_t*)D.loCol.get(),
                  (const double*)D.loAul.get(), (const int32_t*)D.upPtr.get(), (const int32_t*)D.upCol.get(),
