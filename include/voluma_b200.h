@@ -278,6 +278,51 @@ vlm_status vlm_flow_run_steady(vlm_flow* flow, int32_t max_iter, double residual
 vlm_status vlm_flow_get_state(vlm_flow* flow, double* U, double* p, double* phi);
 vlm_status vlm_flow_destroy(vlm_flow* flow);
 
+/* ------------------------------------------------------------------ serving */
+/* Continuous batching of incompressible solves on one device (no counterpart in the reference,
+ * which runs one case per process): requests are admitted in arrival order when a slot is free and
+ * their device-memory estimate fits in the unused HBM budget, run concurrently on their own
+ * streams, keep all their state on the device until they finish, and give the same result alone
+ * and in any mix. */
+typedef struct vlm_server vlm_server;
+
+typedef struct {
+    const vlm_mesh_desc* mesh;  /* with geometry; copied at submission */
+    const vlm_flow_ctrl* ctrl;  /* copied; ctrl->steady selects the steady loop or n_steps of dt */
+    const int32_t* u_type;      /* per patch (copied) */
+    const double* u_value;
+    const int32_t* p_type;
+    const double* p_value;
+    const double* U0;           /* initial fields, 3 per cell / per cell (NULL: zero) */
+    const double* p0;
+    int32_t n_steps;            /* transient */
+    double dt;
+    int32_t max_iter;           /* steady: SIMPLE iteration cap */
+    double residual_tol;        /* steady: convergence tolerance (fvmFlow residualTol) */
+    double arrival;             /* server clock (s) at which the request arrives */
+    int64_t device_bytes;       /* admission estimate (0: vlm_flow_request_bytes) */
+} vlm_flow_request;
+
+typedef struct {
+    int64_t id;
+    int32_t status;             /* VLM_OK, VLM_ERR_OOM (larger than the budget), or the failing call's status */
+    int32_t iterations;         /* SIMPLE iterations / transient steps */
+    double arrival, admitted, finished; /* server clock (s) */
+    double UInitialResidual, pInitialResidual, continuityError; /* last step */
+    int64_t device_bytes;       /* admission estimate used */
+} vlm_flow_result;
+
+int64_t vlm_flow_request_bytes(int32_t n_cells, int32_t n_faces);
+vlm_status vlm_server_create(int32_t device, int64_t hbm_budget, int32_t max_active, vlm_server** out);
+double vlm_server_clock(vlm_server* server);
+vlm_status vlm_server_submit(vlm_server* server, const vlm_flow_request* request, int64_t* id);
+/* Finished results in completion order (waits up to timeout seconds when none is ready). */
+vlm_status vlm_server_collect(vlm_server* server, vlm_flow_result* out, int32_t capacity, int32_t* n, double timeout);
+/* Final U (3 per cell), p and phi of a finished request (any pointer may be NULL). */
+vlm_status vlm_server_result_fields(vlm_server* server, int64_t id, double* U, double* p, double* phi);
+/* Stops admitting, finishes the requests already running, frees everything. */
+vlm_status vlm_server_destroy(vlm_server* server);
+
 /* Exact sum that allocates no device memory.  No counterpart in the reference.  For callers that
  * cannot call cudaMalloc where they need the sum (device memory owned by their own pool or fixed
  * budget; loops where an allocate/free pair would synchronise the device).  values and out are

@@ -127,7 +127,7 @@ _live = weakref.WeakSet()  # meshes/contexts still holding native handles
 def _release_all():
     # release meshes before contexts while the interpreter (and the CUDA runtime) are intact
     objs = list(_live)
-    for kind in ("Flow", "Mesh"):  # flows before their meshes, meshes before their contexts
+    for kind in ("Server", "Flow", "Mesh"):  # servers and flows before meshes, meshes before contexts
         for o in objs:
             if type(o).__name__ == kind:
                 o.close()
@@ -515,3 +515,82 @@ class Flow:
         if getattr(self, "_h", None):
             load().vlm_flow_destroy(self._h)
             self._h = None
+
+
+# ------------------------------------------------------------------ serving
+class Server:
+    """Continuous-batching server of incompressible solves on one device (vlm_server_*): requests are
+    admitted in arrival order as slots and HBM budget free up and run concurrently, each on its own
+    stream; results come back with their arrival / admission / completion times."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 64 << 30, max_active: int = 4):
+        h = C.c_void_p()
+        check(load().vlm_server_create(device, int(hbm_budget), int(max_active), C.byref(h)))
+        self._h = h
+        self._keep = {}
+        _live.add(self)
+
+    def clock(self) -> float:
+        return load().vlm_server_clock(self._h)
+
+    def submit(self, mesh: dict, case: dict, arrival: float = 0.0, max_iter: int = 5000, residual_tol: float = 1e-6,
+               n_steps: int = 0, dt: float = 1.0, U0=None, p0=None, device_bytes: int = 0) -> int:
+        """mesh: cfd::Mesh arrays with geometry (voluma_b200.mesh.box_mesh); case: Flow case dict."""
+        arrs = {}
+        d = _ffi.MeshDesc()
+        own = np.ascontiguousarray(mesh["owner"], np.int32)
+        nei = np.ascontiguousarray(mesh["neighbour"], np.int32)
+        arrs.update(own=own, nei=nei)
+        d.n_cells, d.n_internal_faces, d.n_faces = int(mesh["n_cells"]), nei.size, own.size
+        d.owner, d.neighbour = own.ctypes.data, nei.ctypes.data
+        for name in ("magSf", "ndc", "V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
+            if name in mesh:
+                a = _f64(mesh[name])
+                arrs[name] = a
+                setattr(d, name, a.ctypes.data)
+        ps = np.ascontiguousarray(mesh["patch_start"], np.int32)
+        pz = np.ascontiguousarray(mesh["patch_size"], np.int32)
+        arrs.update(ps=ps, pz=pz)
+        d.n_patches, d.patch_start, d.patch_size = ps.size, ps.ctypes.data, pz.ctypes.data
+        d.two_d, d.empty_dir = int(mesh.get("two_d", 0)), int(mesh.get("empty_dir", -1))
+        ctrl = _flow_ctrl(case)
+        bc = [np.ascontiguousarray(case["u_type"], np.int32), _f64(case["u_value"]),
+              np.ascontiguousarray(case["p_type"], np.int32), _f64(case["p_value"])]
+        r = _ffi.FlowRequest()
+        r.mesh, r.ctrl = C.addressof(d), C.addressof(ctrl)
+        r.u_type, r.u_value, r.p_type, r.p_value = (a.ctypes.data for a in bc)
+        if U0 is not None:
+            arrs["U0"] = _f64(U0).reshape(-1)
+            r.U0 = arrs["U0"].ctypes.data
+        if p0 is not None:
+            arrs["p0"] = _f64(p0)
+            r.p0 = arrs["p0"].ctypes.data
+        r.n_steps, r.dt, r.max_iter, r.residual_tol = int(n_steps), float(dt), int(max_iter), float(residual_tol)
+        r.arrival, r.device_bytes = float(arrival), int(device_bytes)
+        rid = C.c_int64()
+        check(load().vlm_server_submit(self._h, C.byref(r), C.byref(rid)))  # copies everything
+        self._keep[rid.value] = (int(mesh["n_cells"]), own.size)
+        return rid.value
+
+    def collect(self, timeout: float = 0.0, capacity: int = 256) -> list:
+        out = (_ffi.FlowResult * capacity)()
+        n = C.c_int32()
+        check(load().vlm_server_collect(self._h, out, capacity, C.byref(n), float(timeout)))
+        return [dict(id=q.id, status=q.status, iterations=q.iterations, arrival=q.arrival, admitted=q.admitted,
+                     finished=q.finished, UInitialResidual=q.UInitialResidual, pInitialResidual=q.pInitialResidual,
+                     continuityError=q.continuityError, device_bytes=q.device_bytes) for q in out[:n.value]]
+
+    def fields(self, rid: int):
+        nC, nF = self._keep[rid]
+        U, p, phi = np.zeros((nC, 3)), np.zeros(nC), np.zeros(nF)
+        check(load().vlm_server_result_fields(self._h, rid, U.ctypes.data, p.ctypes.data, phi.ctypes.data))
+        return U, p, phi
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().vlm_server_destroy(self._h)
+            self._h = None
+
+
+def request_bytes(n_cells: int, n_faces: int) -> int:
+    return int(load().vlm_flow_request_bytes(int(n_cells), int(n_faces)))

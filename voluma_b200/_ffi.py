@@ -17,7 +17,9 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
-           "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy"]
+           "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy",
+           "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
+           "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy"]
 
 
 class MeshDesc(C.Structure):
@@ -54,6 +56,19 @@ class StepInfo(C.Structure):
                 ("continuityError", C.c_double), ("iterations", C.c_int32)]
 
 
+class FlowRequest(C.Structure):
+    _fields_ = [("mesh", C.c_void_p), ("ctrl", C.c_void_p), ("u_type", C.c_void_p), ("u_value", C.c_void_p),
+                ("p_type", C.c_void_p), ("p_value", C.c_void_p), ("U0", C.c_void_p), ("p0", C.c_void_p),
+                ("n_steps", C.c_int32), ("dt", C.c_double), ("max_iter", C.c_int32), ("residual_tol", C.c_double),
+                ("arrival", C.c_double), ("device_bytes", C.c_int64)]
+
+
+class FlowResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("iterations", C.c_int32), ("arrival", C.c_double),
+                ("admitted", C.c_double), ("finished", C.c_double), ("UInitialResidual", C.c_double),
+                ("pInitialResidual", C.c_double), ("continuityError", C.c_double), ("device_bytes", C.c_int64)]
+
+
 _lib = None
 
 
@@ -86,6 +101,15 @@ def load():
     L.vlm_flow_run_steady.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_int32), C.POINTER(StepInfo)]
     L.vlm_flow_get_state.argtypes = [P, P, P, P]
     L.vlm_flow_destroy.argtypes = [P]
+    L.vlm_flow_request_bytes.restype = C.c_int64
+    L.vlm_flow_request_bytes.argtypes = [C.c_int32, C.c_int32]
+    L.vlm_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.POINTER(P)]
+    L.vlm_server_clock.restype = C.c_double
+    L.vlm_server_clock.argtypes = [P]
+    L.vlm_server_submit.argtypes = [P, C.POINTER(FlowRequest), C.POINTER(C.c_int64)]
+    L.vlm_server_collect.argtypes = [P, C.POINTER(FlowResult), C.c_int32, C.POINTER(C.c_int32), C.c_double]
+    L.vlm_server_result_fields.argtypes = [P, C.c_int64, P, P, P]
+    L.vlm_server_destroy.argtypes = [P]
     L.vlm_gamg_levels.argtypes = [P, C.POINTER(i32)]
     L.vlm_gamg_level.argtypes = [P, i32, P, P, P, P]
     L.vlm_gamg_colours.argtypes = [P, i32, C.POINTER(i32)]
@@ -108,7 +132,8 @@ def load():
     L.vlm_mesh_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.vlm_profile_kernel.argtypes = [P, P, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     for name in EXPORTS:
-        getattr(L, name).restype = getattr(L, name).restype if name in ("vlm_last_error", "vlm_ctx_stream") else C.c_int
+        keep = ("vlm_last_error", "vlm_ctx_stream", "vlm_flow_request_bytes", "vlm_server_clock")
+        getattr(L, name).restype = getattr(L, name).restype if name in keep else C.c_int
     _lib = L
     return L
 

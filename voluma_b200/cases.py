@@ -168,3 +168,15 @@ def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
                 U=_ctl("PBiCGStab", "DILU", 1e-8, 0.0, 1000), p=_ctl("PCG", "GAMG", 1e-8, 0.01, 2000),
                 pFinal=_ctl("PCG", "GAMG", 1e-8, 0.0, 2000), p_ref_cell=0, p_ref_value=0.0)
     return m, case, U0
+
+
+def serving_trace(n_requests=32, rate_hz=2.0, seed=20261203, n_range=(32, 256), re_range=(100.0, 1000.0)):
+    """Serving stream of steady lid-cavity solves: Poisson arrivals of the given rate (seeded),
+    mesh N x N with N uniform in n_range (inclusive), Re uniform in re_range.
+    Returns a list of dicts (arrival s, n, Re)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n_requests))
+    t -= t[0]
+    ns = rng.integers(n_range[0], n_range[1] + 1, n_requests)
+    res = rng.uniform(re_range[0], re_range[1], n_requests)
+    return [dict(arrival=float(a), n=int(n), Re=float(r)) for a, n, r in zip(t, ns, res)]
