@@ -8,12 +8,16 @@ of a predicted face flux phi = (u_TG + seeded perturbation)_f . S_f, setReferenc
 from p = 0 with PCG + GAMG to relTol 1e-8 (tolerance 0, the reference's normalised L1 residual).
 Synthetic data: the TG field plus 16 seeded Fourier modes (|k| <= 4, amplitude N(0,1)/|k|^2).
 
-Metric: solves/s (whole job, all GPUs) and p50/p99 latency, mixed precision (FP32 inner
-PCG+V-cycles inside FP64 defect correction) vs FP64 GAMG-PCG.  `value` is the mixed-precision
-rate with inputs resident in HBM; `e2e` is the same through the host-pointer C ABI
-(vlm_ldu_solve: H2D of diag/upper/b/x and D2H of x inside the timed region).
+Metric: solves/s (whole job, all GPUs) and p50/p99 latency, mixed precision (FP32 GAMG V-cycle
+inside the FP64 PCG recurrence) vs FP64 GAMG-PCG.  `value` is the mixed-precision rate with inputs
+resident in HBM; `e2e` is the same through the host-pointer C ABI (vlm_ldu_solve: H2D of
+diag/upper/b/x and D2H of x inside the timed region).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 128]
+
+--workload serving: a seeded Poisson trace of steady lid-cavity solves through the serving runtime
+(vlm_server_*), mixed-precision vs FP64 pressure, solves/s and p50/p99 latency; --impl reference
+replays the trace through the reference's own incompressible solver in host worker processes.
 """
 from __future__ import annotations
 
@@ -199,6 +203,143 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------------ serving workload
+SERVE_METRIC = "serving: steady lid-cavity SIMPLE solves/s and p50/p99 latency (residualTol 1e-6)"
+
+
+def serve_trace(args):
+    from voluma_b200 import cases
+    return cases.serving_trace(args.requests, args.rate, seed=20261203, n_range=(args.nmin, args.nmax),
+                               re_range=(args.remin, args.remax))
+
+
+def serve_config(args, world):
+    return {"workload": f"Poisson arrivals ({args.rate}/s) of steady 2D lid-driven cavity solves, N^2 cells with N "
+                        f"uniform in {{{args.nmin}..{args.nmax}}}, Re uniform in [{args.remin}, {args.remax}], lid U=1, "
+                        f"SIMPLE (linearUpwind, alphaU 0.7, alphaP 0.3, PBiCGStab/DILU U, PCG/GAMG p) to residualTol "
+                        f"1e-6; trace seed 20261203",
+            "requests": args.requests, "rate_hz": args.rate, "n_range": [args.nmin, args.nmax],
+            "re_range": [args.remin, args.remax], "max_active": args.max_active, "hbm_budget_gb": args.hbm_gb,
+            "parallelism": f"replicas{world}", "latency": "arrival to completion, server clock (wall)",
+            "l2": "each request's working set is small; requests overlap on the device"}
+
+
+def _serve_ref_worker(q):
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    from voluma_b200 import cases
+    m, case = cases.lid_cavity(q["n"], q["Re"])
+    t = time.perf_counter()
+    R = ref.RefMesh((q["n"], q["n"], 1), hi=(1.0, 1.0, 0.1), two_d=True)
+    _, _, _, hist = R.flow_run(case, 20000, residual_tol=1e-6)
+    return time.perf_counter() - t, len(hist)
+
+
+def run_serving_reference(args, rank, world):
+    """The same trace replayed on the host: the reference's IncompressibleFlow (generateBox + Mesh::build +
+    the steady loop) in `procs` single-threaded worker processes, FIFO by arrival."""
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvlmref.so was not built (make -C oracle)"}))
+        return
+    import multiprocessing as mp
+    trace = serve_trace(args)
+    P = max(1, min(os.cpu_count() or 1, 8))
+    with mp.get_context("spawn").Pool(P) as pool:
+        res = pool.map(_serve_ref_worker, trace, chunksize=1)
+    # FIFO schedule of the measured durations over P workers
+    free = [0.0] * P
+    lat, fin = [], []
+    for q, (dur, _) in zip(trace, res):
+        k = int(np.argmin(free))
+        start = max(q["arrival"], free[k])
+        free[k] = start + dur
+        fin.append(free[k])
+        lat.append(free[k] - q["arrival"])
+    span = max(fin) - trace[0]["arrival"]
+    value = len(trace) / span
+    line = {"metric": SERVE_METRIC, "impl": "reference", "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": len(trace), "warmup": 0, "ms_per_step": 1e3 * span / len(trace), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "iterations_median": int(np.median([r[1] for r in res])), "config": serve_config(args, 1),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": P, "kind": "reference",
+                             "sample": f"the full {len(trace)}-request trace, {P} single-threaded worker processes"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_serving(args, rank, world, local):
+    import voluma_b200 as vb
+    from voluma_b200 import cases
+    trace = serve_trace(args)[rank::world]  # replicas: requests dealt round-robin to the ranks
+    meshes = {}
+    built = []
+    for q in trace:
+        if q["n"] not in meshes:
+            meshes[q["n"]] = cases.lid_cavity(q["n"], 100.0)
+        m, case = meshes[q["n"]]
+        c = dict(case, nu=1.0 / q["Re"])
+        built.append((q, m, c))
+    modes = {}
+    sampler = ClockSampler(local)
+    for prec in ("mixed", "fp64"):
+        s = vb.Server(device=local, hbm_budget=int(args.hbm_gb * (1 << 30)), max_active=args.max_active)
+        # warm-up requests (untimed): contexts, graphs, first launches
+        wm, wc = cases.lid_cavity(32, 100.0)
+        for _ in range(args.warmup):
+            s.submit(wm, wc, max_iter=50, residual_tol=1e-12)
+        got = 0
+        while got < args.warmup:
+            got += len(s.collect(timeout=1.0))
+        if prec == "mixed":
+            sampler.start()
+        t0 = s.clock() + 0.05
+        for q, m, c in built:
+            cc = dict(c)
+            if prec == "mixed":
+                cc = dict(c, p=dict(c["p"], precision="mixed"), pFinal=dict(c["pFinal"], precision="mixed"))
+            s.submit(m, cc, arrival=t0 + q["arrival"], max_iter=20000, residual_tol=1e-6)
+        res = []
+        while len(res) < len(built):
+            res += s.collect(timeout=1.0)
+        if prec == "mixed":
+            clocks = sampler.stop()
+        s.close()
+        ok = [r for r in res if r["status"] == 0]
+        lat = [r["finished"] - r["arrival"] for r in ok]
+        span = max(r["finished"] for r in ok) - min(r["arrival"] for r in ok)
+        modes[prec] = dict(value=len(ok) / span, ms_per_step=1e3 * span / max(len(ok), 1),
+                           p50_ms=1e3 * float(np.percentile(lat, 50)), p99_ms=1e3 * float(np.percentile(lat, 99)),
+                           iterations_median=int(np.median([r["iterations"] for r in ok])),
+                           failed=len(res) - len(ok), gpu_launches=int(sum(r["launches"] for r in ok)),
+                           span_s=span)
+    if world > 1:
+        import torch
+        t = torch.tensor([modes["mixed"]["span_s"]], device=torch.device("cuda", local), dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        modes["mixed"]["value"] = args.requests / float(t.item())
+    if rank != 0:
+        return
+    mx = modes["mixed"]
+    h2d = sum(8 * m["n_cells"] * 3 + 8 * 12 * m["n_faces"] for _, m, _ in built) // max(len(built), 1)
+    d2h = sum(8 * (4 * m["n_cells"] + m["n_faces"]) for _, m, _ in built) // max(len(built), 1)
+    line = {"metric": SERVE_METRIC, "value": mx["value"], "unit": "solves/s", "n_gpus": world,
+            "steps": args.requests, "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic",
+            "p50_ms": mx["p50_ms"], "p99_ms": mx["p99_ms"], "config": serve_config(args, world),
+            "modes": {"mixed": mx, "fp64": modes["fp64"],
+                      "speedup_mixed_vs_fp64": modes["fp64"]["span_s"] / mx["span_s"]},
+            "e2e": {"value": mx["value"], "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "note": "latency and throughput are end to end through vlm_server_* with host meshes: "
+                            "registration (GAMG hierarchy), H2D, every SIMPLE step, D2H of U, p, phi"},
+            "clocks": clocks, "gpu_launches": mx["gpu_launches"]}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------------------ our arm
 METRIC = "solves/s & p99 latency at rtol 1e-8, mixed vs FP64 GAMG-PCG on 1 B200"
 
@@ -362,12 +503,21 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--smoother", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving"])
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--nmin", type=int, default=32)
+    ap.add_argument("--nmax", type=int, default=96)
+    ap.add_argument("--remin", type=float, default=100.0)
+    ap.add_argument("--remax", type=float, default=400.0)
+    ap.add_argument("--max-active", type=int, default=8)
+    ap.add_argument("--hbm-gb", type=float, default=64.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        (run_serving_reference if args.workload == "serving" else run_reference)(args, rank, world)
         return
     if world > 1:
         import datetime
@@ -376,7 +526,7 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local)
+        (run_serving if args.workload == "serving" else run_ours)(args, rank, world, local)
     finally:
         if world > 1:
             import torch

@@ -263,6 +263,7 @@ typedef struct {
 typedef struct {
     double UInitialResidual, pInitialResidual, continuityError; /* StepInfo */
     int32_t iterations;          /* linear-solver iterations of the step */
+    int32_t launches;            /* kernels the step ran (graph kernel nodes included) */
 } vlm_step_info;
 
 vlm_status vlm_flow_create(vlm_ctx* ctx, vlm_mesh* mesh, const vlm_flow_ctrl* ctrl, const int32_t* u_type,
@@ -275,6 +276,8 @@ vlm_status vlm_flow_step(vlm_flow* flow, double dt, vlm_step_info* info);
  * below residual_tol (from the second iteration) or max_iter; *iterations = steps taken. */
 vlm_status vlm_flow_run_steady(vlm_flow* flow, int32_t max_iter, double residual_tol, int32_t* iterations,
                                vlm_step_info* last);
+/* Kernels run by the flow so far (all steps). */
+int64_t vlm_flow_launches(vlm_flow* flow);
 vlm_status vlm_flow_get_state(vlm_flow* flow, double* U, double* p, double* phi);
 vlm_status vlm_flow_destroy(vlm_flow* flow);
 
@@ -310,6 +313,7 @@ typedef struct {
     double arrival, admitted, finished; /* server clock (s) */
     double UInitialResidual, pInitialResidual, continuityError; /* last step */
     int64_t device_bytes;       /* admission estimate used */
+    int64_t launches;           /* kernels run for this request */
 } vlm_flow_result;
 
 int64_t vlm_flow_request_bytes(int32_t n_cells, int32_t n_faces);

@@ -50,7 +50,7 @@ def lib():
                                          C.c_double, C.c_double, C.c_int, P, P, P]
         L.ref_exact_sum.restype = C.c_double
         L.ref_exact_sum.argtypes = [P, C.c_long]
-        L.ref_flow_run.argtypes = [P, C.POINTER(RefFlowSpec), C.c_int, C.c_double, P, P, P, P]
+        L.ref_flow_run.argtypes = [P, C.POINTER(RefFlowSpec), C.c_int, C.c_double, P, P, P, P, C.POINTER(C.c_int)]
         L.ref_flow_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -76,7 +76,7 @@ class RefFlowSpec(C.Structure):
                 ("alphaU", C.c_double), ("alphaP", C.c_double), ("nPatches", C.c_int), ("uType", C.c_void_p),
                 ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
-                ("reproducible", C.c_int)]
+                ("reproducible", C.c_int), ("residualTol", C.c_double)]
 
 
 def _solver_ctl(d):
@@ -131,10 +131,11 @@ class RefMesh:
         return out
 
     # ------------------------------------------------------------------ incompressible step
-    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False):
+    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False, residual_tol=0.0):
         """n_steps of IncompressibleFlow::step(dt) (solvers/IncompressibleFlow.cpp:138-370) with the case
-        settings of `case` (a dict, voluma_b200.cases.flow_case layout).  Returns U (n,3), p, phi, and the
-        per-step history [UInitialResidual, pInitialResidual, continuityError, linear iterations]."""
+        settings of `case` (a dict, voluma_b200.cases.lid_cavity layout).  residual_tol > 0 stops at
+        convergence like fvmFlow's steady loop.  Returns U (n,3), p, phi, and the per-step history
+        [UInitialResidual, pInitialResidual, continuityError, linear iterations] of the steps run."""
         nC = self.n_cells
         Uc = np.zeros((nC, 3)) if U is None else np.ascontiguousarray(U, np.float64).reshape(nC, 3).copy()
         pc = np.zeros(nC) if p is None else np.ascontiguousarray(p, np.float64).copy()
@@ -153,9 +154,11 @@ class RefMesh:
         sp.U, sp.p, sp.pFinal = (_solver_ctl(case[k]) for k in ("U", "p", "pFinal"))
         sp.pRefCell, sp.pRefValue = case["p_ref_cell"], case["p_ref_value"]
         sp.reproducible = int(reproducible)
-        if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist)) != 0:
+        sp.residualTol = residual_tol
+        ran = C.c_int()
+        if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist), C.byref(ran)) != 0:
             raise RuntimeError(lib().ref_flow_error().decode())
-        return Uc, pc, phi, hist
+        return Uc, pc, phi, hist[:ran.value]
 
     # ------------------------------------------------------------------ linear algebra
     def amul(self, diag, upper, lower, x):

@@ -43,10 +43,11 @@ struct RefFlowSpec {
     int pRefCell;
     double pRefValue;
     int reproducible;
+    double residualTol;  // > 0: stop once U and p residuals are below it (from step 2, fvmFlow.cpp:611-625)
 };
 
 int ref_flow_run(const RefMesh* r, const RefFlowSpec* spec, int nSteps, double dt, double* U, double* p,
-                 double* phi, double* hist);
+                 double* phi, double* hist, int* stepsRun);
 const char* ref_flow_error();
 }
 
@@ -72,7 +73,7 @@ const char* ref_flow_error() { return g_flowErr.c_str(); }
 // Outputs U, p, phi (nFaces) and per step hist[4*k..]: UInitialResidual, pInitialResidual,
 // continuityError, total linear-solver iterations.
 int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt, double* U, double* p, double* phi,
-                 double* hist) {
+                 double* hist, int* stepsRun) {
     try {
         par::setReproducible(sp->reproducible != 0);
         const Mesh& m = *r->mesh;
@@ -112,7 +113,8 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
             flow.U()[k] = Vec3{U[3 * k], U[3 * k + 1], U[3 * k + 2]};
             flow.p()[k] = p[k];
         }
-        for (int s = 0; s < nSteps; ++s) {
+        int s = 0;
+        for (s = 0; s < nSteps; ++s) {
             const StepInfo info = flow.step(dt);
             double its = 0;
             for (const auto& pf : info.perf) its += pf.iterations;
@@ -122,7 +124,13 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
                 hist[4 * s + 2] = info.continuityError;
                 hist[4 * s + 3] = its;
             }
+            if (sp->residualTol > 0 && s > 0 && info.UInitialResidual < sp->residualTol &&
+                info.pInitialResidual < sp->residualTol) {
+                ++s;
+                break;
+            }
         }
+        if (stepsRun) *stepsRun = s;
         for (label k = 0; k < nC; ++k) {
             U[3 * k] = flow.U()[k].x;
             U[3 * k + 1] = flow.U()[k].y;

@@ -493,7 +493,10 @@ class Flow:
         i = _ffi.StepInfo()
         check(load().vlm_flow_step(self._h, dt, C.byref(i)), self.mesh.ctx.handle)
         return dict(UInitialResidual=i.UInitialResidual, pInitialResidual=i.pInitialResidual,
-                    continuityError=i.continuityError, iterations=i.iterations)
+                    continuityError=i.continuityError, iterations=i.iterations, launches=i.launches)
+
+    def launches(self) -> int:
+        return int(load().vlm_flow_launches(self._h))
 
     def run_steady(self, max_iter=5000, residual_tol=1e-6):
         it = C.c_int32()
@@ -578,7 +581,8 @@ class Server:
         check(load().vlm_server_collect(self._h, out, capacity, C.byref(n), float(timeout)))
         return [dict(id=q.id, status=q.status, iterations=q.iterations, arrival=q.arrival, admitted=q.admitted,
                      finished=q.finished, UInitialResidual=q.UInitialResidual, pInitialResidual=q.pInitialResidual,
-                     continuityError=q.continuityError, device_bytes=q.device_bytes) for q in out[:n.value]]
+                     continuityError=q.continuityError, device_bytes=q.device_bytes, launches=q.launches)
+                for q in out[:n.value]]
 
     def fields(self, rid: int):
         nC, nF = self._keep[rid]

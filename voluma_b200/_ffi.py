@@ -17,7 +17,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
-           "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy",
+           "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
            "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
            "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy"]
 
@@ -53,7 +53,7 @@ class FlowCtrl(C.Structure):
 
 class StepInfo(C.Structure):
     _fields_ = [("UInitialResidual", C.c_double), ("pInitialResidual", C.c_double),
-                ("continuityError", C.c_double), ("iterations", C.c_int32)]
+                ("continuityError", C.c_double), ("iterations", C.c_int32), ("launches", C.c_int32)]
 
 
 class FlowRequest(C.Structure):
@@ -66,7 +66,8 @@ class FlowRequest(C.Structure):
 class FlowResult(C.Structure):
     _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("iterations", C.c_int32), ("arrival", C.c_double),
                 ("admitted", C.c_double), ("finished", C.c_double), ("UInitialResidual", C.c_double),
-                ("pInitialResidual", C.c_double), ("continuityError", C.c_double), ("device_bytes", C.c_int64)]
+                ("pInitialResidual", C.c_double), ("continuityError", C.c_double), ("device_bytes", C.c_int64),
+                ("launches", C.c_int64)]
 
 
 _lib = None
@@ -101,6 +102,8 @@ def load():
     L.vlm_flow_run_steady.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_int32), C.POINTER(StepInfo)]
     L.vlm_flow_get_state.argtypes = [P, P, P, P]
     L.vlm_flow_destroy.argtypes = [P]
+    L.vlm_flow_launches.restype = C.c_int64
+    L.vlm_flow_launches.argtypes = [P]
     L.vlm_flow_request_bytes.restype = C.c_int64
     L.vlm_flow_request_bytes.argtypes = [C.c_int32, C.c_int32]
     L.vlm_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.POINTER(P)]
@@ -132,7 +135,7 @@ def load():
     L.vlm_mesh_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.vlm_profile_kernel.argtypes = [P, P, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     for name in EXPORTS:
-        keep = ("vlm_last_error", "vlm_ctx_stream", "vlm_flow_request_bytes", "vlm_server_clock")
+        keep = ("vlm_last_error", "vlm_ctx_stream", "vlm_flow_request_bytes", "vlm_server_clock", "vlm_flow_launches")
         getattr(L, name).restype = getattr(L, name).restype if name in keep else C.c_int
     _lib = L
     return L

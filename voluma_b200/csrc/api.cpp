@@ -727,6 +727,8 @@ vlm_status vlm_flow_get_state(vlm_flow* f, double* U, double* p, double* phi) {
     });
 }
 
+int64_t vlm_flow_launches(vlm_flow* f) { return f ? f->flow->launches() : 0; }
+
 vlm_status vlm_flow_destroy(vlm_flow* f) {
     if (!f) return VLM_OK;
     cudaSetDevice(f->mesh->ctx->device);

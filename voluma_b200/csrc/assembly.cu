@@ -369,18 +369,22 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
     VLM_CUDA(cudaStreamSynchronize(s));
 }
 
+// The device copy of the patch types is refreshed only when they change (a host-to-device copy
+// from pageable memory waits for the stream, which would stall every assembly call).
 void DeviceGeom::uploadBCType(const ScalarBC& bc, cudaStream_t s) {
     std::vector<int32_t> t(bcType_.size(), 0);
     for (size_t p = 0; p < patchStart_.size(); ++p) t[p] = bc.type ? bc.type[p] : 0;
+    if (t == bcTypeHost_) return;
     VLM_CUDA(cudaMemcpyAsync(bcType_.get(), t.data(), sizeof(int32_t) * t.size(), cudaMemcpyHostToDevice, s));
     VLM_CUDA(cudaStreamSynchronize(s));  // t is a local
+    bcTypeHost_ = std::move(t);
 }
 
 void DeviceGeom::correctBoundary(const double* psi, const ScalarBC& bc, double* psiB, cudaStream_t s) {
     uploadBCType(bc, s);
     const int nB = nBoundary();
     if (nB > 0)
-        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, psi, psiB);
+        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, psi, psiB), ++launches_;
 }
 
 void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out,
@@ -389,10 +393,10 @@ void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc,
     if (scheme == 1)
         k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                             Sf_.get(), magSf_.get(), d_.get(), psi, psiB, bPatch_.get(), bcType_.get(),
-                                            twoD_, emptyDir_, out);
+                                            twoD_, emptyDir_, out), ++launches_;
     else
         k_grad_gauss<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
-                                               w_.get(), Sf_.get(), V_.get(), psi, psiB, twoD_, emptyDir_, out);
+                                               w_.get(), Sf_.get(), V_.get(), psi, psiB, twoD_, emptyDir_, out), ++launches_;
 }
 
 void DeviceGeom::laplacian(const double* gamma, const double* psi, const double* psiB, const ScalarBC& bc,
@@ -400,47 +404,47 @@ void DeviceGeom::laplacian(const double* gamma, const double* psi, const double*
                            double* bs, double* ffc, bool* hasFfc, cudaStream_t s) {
     uploadBCType(bc, s);
     double* gs = scratchGS_.get();
-    k_face_gs<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, gamma, magSf_.get(), ndc_.get(), gs, upper);
+    k_face_gs<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, gamma, magSf_.get(), ndc_.get(), gs, upper), ++launches_;
     const bool corr = nonOrthCorr && nonOrth_;
     if (corr) {
         grad(psi, psiB, bc, gradScheme, scratchG_.get(), s);
         k_lap_ffc<<<nblk(nF_), 256, 0, s>>>(nI_, nF_, own_.get(), nei_.get(), w_.get(), corr_.get(), gs,
-                                            scratchG_.get(), ffc);
+                                            scratchG_.get(), ffc), ++launches_;
     }
     k_lap_cells<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), upper, corr ? ffc : nullptr, diag,
-                                          source);
+                                          source), ++launches_;
     const int nB = nBoundary();
     if (nB > 0)
-        k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value, ic, bs);
+        k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value, ic, bs), ++launches_;
     if (hasFfc) *hasFfc = corr;
 }
 
 void DeviceGeom::fold(const double* diag, const double* source, const double* ic, const double* bs, double* d,
                       double* b, cudaStream_t s) {
-    k_fold<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), diag, source, ic, bs, d, b);
+    k_fold<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), diag, source, ic, bs, d, b), ++launches_;
 }
 
 void DeviceGeom::flux(const double* upper, const double* psi, const double* ic, const double* bs, const double* ffc,
                       double* F, cudaStream_t s) {
-    k_flux<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, own_.get(), nei_.get(), upper, psi, ic, bs, ffc, F);
+    k_flux<<<nblk(nF_), 256, 0, s>>>(nF_, nI_, own_.get(), nei_.get(), upper, psi, ic, bs, ffc, F), ++launches_;
 }
 
 void DeviceGeom::addVolumeSource(double* source, const double* su, cudaStream_t s) {
-    k_add_vol_source<<<nblk(nC_), 256, 0, s>>>(nC_, source, su, V_.get());
+    k_add_vol_source<<<nblk(nC_), 256, 0, s>>>(nC_, source, su, V_.get()), ++launches_;
 }
 
 void DeviceGeom::div(const double* F, double* out, cudaStream_t s) {
-    k_div<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), F, V_.get(), out);
+    k_div<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, cfOff_.get(), cfList_.get(), F, V_.get(), out), ++launches_;
 }
 
 void DeviceGeom::setReference(int cell, double value, double* diag, double* source, cudaStream_t s) {
     VLM_REQUIRE(cell >= 0 && cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
-    k_set_reference<<<1, 1, 0, s>>>(cell, value, diag, source);
+    k_set_reference<<<1, 1, 0, s>>>(cell, value, diag, source), ++launches_;
 }
 
 void DeviceGeom::setReferences(const int32_t* cells, int n, double value, double* diag, double* source,
                                cudaStream_t s) {
-    if (n > 0) k_set_references<<<nblk(n), 256, 0, s>>>(cells, n, value, diag, source);
+    if (n > 0) k_set_references<<<nblk(n), 256, 0, s>>>(cells, n, value, diag, source), ++launches_;
 }
 
 }  // namespace vlm

@@ -81,6 +81,7 @@ public:
     const double* C() const { return C_.size() ? C_.get() : nullptr; }
     const double* Cf() const { return Cf_.size() ? Cf_.get() : nullptr; }
     int twoD() const { return twoD_; }
+    int64_t launches() const { return launches_; }  // kernels launched by the methods above
     int emptyDir() const { return emptyDir_; }
     int nPatches() const { return int(patchStart_.size()); }
     const std::vector<int32_t>& patchStart() const { return patchStart_; }
@@ -91,8 +92,10 @@ private:
     bool nonOrth_ = false;
     std::vector<int32_t> patchStart_, patchSize_, bPatchHost_;
     DBuf<int32_t> own_, nei_, cfOff_, cfList_, bPatch_, bcType_;
+    std::vector<int32_t> bcTypeHost_;  // the patch types last copied to bcType_
     DBuf<double> magSf_, ndc_, V_, w_, Sf_, d_, corr_;  // vectors as SoA: [x(nF) y(nF) z(nF)]
     DBuf<double> C_, Cf_;                               // SoA; empty when not registered
+    int64_t launches_ = 0;
     DBuf<double> scratchG_, scratchGS_;
     void uploadBCType(const ScalarBC& bc, cudaStream_t s);
 };

@@ -69,6 +69,10 @@ struct TailSys {
     int sys, first, coarsest;  // batch position; first tail level; coarsest level
     int coarseN, invOffset;
     int rowStart[kTailMaxLevels], rowCount[kTailMaxLevels];
+    // level 0 in the tail (first == 0) with global multicolour Gauss-Seidel: the system's colour
+    // groups (padded row ranges) and whether the batch runs the two-colour fused schedule
+    int nColours, two;
+    int grpStart[4], grpCount[4];
 };
 
 }  // namespace vlm

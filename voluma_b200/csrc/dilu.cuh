@@ -139,9 +139,9 @@ __global__ void __launch_bounds__(kDiluThreads) k_dilu_apply(const DiluSys* __re
 
 // ---------------------------------------------------------------- shared-memory variants
 // One CTA per system whose level-0 vector fits in shared memory and whose levels are at most one
-// row per thread.  The swept vector lives in shared memory, and each thread loads its row of the
-// NEXT level (row index, scalars and the first kDiluPre coefficients) before the barrier that ends
-// the current level, so a level costs a barrier and shared-memory reads, not an L2 round trip.
+// row per thread.  The swept vector lives in shared memory, and each thread loads its rows of the
+// next three levels (row index, scalars and the first kDiluPre coefficients) ahead of the barriers,
+// so a level costs a barrier and shared-memory reads, not an L2 round trip.
 // Same arithmetic in the same order as k_dilu_factor / k_dilu_apply.
 constexpr int kDiluPre = 4;
 
@@ -187,19 +187,23 @@ __global__ void __launch_bounds__(kDiluThreads) k_dilu_factor_smem(const DiluSys
     extern __shared__ double sh[];
     const DiluSys d = ds[blockIdx.x];
     const int base = d.rowBegin, tid = threadIdx.x;
-    DiluRow cur, nxt;
-    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, cur);
+    DiluRow r0, r1, r2, r3;  // levels t .. t+3 in flight
+    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r0);
+    dilu_row_load(d, 1, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r1);
+    dilu_row_load(d, 2, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r2);
     for (int t = 0; t < d.nLev; ++t) {
-        dilu_row_load(d, t + 1, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, nxt);
-        if (cur.c >= 0) {
-            double v = cur.a;
-            const int np = min(cur.k1 - cur.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) v -= cur.v0[q] * cur.v1[q] / sh[cur.col[q] - base];
-            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) v -= loAlu[k] * loAul[k] / sh[loCol[k] - base];
-            sh[cur.c - base] = v;
+        dilu_row_load(d, t + 3, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r3);
+        if (r0.c >= 0) {
+            double v = r0.a;
+            const int np = min(r0.k1 - r0.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) v -= r0.v0[q] * r0.v1[q] / sh[r0.col[q] - base];
+            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) v -= loAlu[k] * loAul[k] / sh[loCol[k] - base];
+            sh[r0.c - base] = v;
         }
         __syncthreads();
-        cur = nxt;
+        r0 = r1;
+        r1 = r2;
+        r2 = r3;
     }
     for (int i = tid; i < d.rowCount; i += blockDim.x) rD[base + i] = 1.0 / sh[i];
 }
@@ -220,34 +224,43 @@ __global__ void __launch_bounds__(kDiluThreads) k_dilu_apply_smem(const DiluSys*
     const DiluSys d = ds[blockIdx.x];
     if (st != nullptr && sys_idle(st[d.sys], flag)) return;
     const int base = d.rowBegin, tid = threadIdx.x;
-    DiluRow cur, nxt;
-    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, cur);
+    DiluRow r0, r1, r2, r3;  // levels t .. t+3 in flight
+    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r0);
+    dilu_row_load(d, 1, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r1);
+    dilu_row_load(d, 2, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r2);
     for (int t = 0; t < d.nLev; ++t) {
-        dilu_row_load(d, t + 1, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, nxt);
-        if (cur.c >= 0) {
-            const double rd = cur.a;
-            double wc = rd * cur.b;
-            const int np = min(cur.k1 - cur.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) wc -= rd * cur.v0[q] * sh[cur.col[q] - base];
-            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) wc -= rd * loAul[k] * sh[loCol[k] - base];
-            sh[cur.c - base] = wc;
+        dilu_row_load(d, t + 3, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r3);
+        if (r0.c >= 0) {
+            const double rd = r0.a;
+            double wc = rd * r0.b;
+            const int np = min(r0.k1 - r0.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) wc -= rd * r0.v0[q] * sh[r0.col[q] - base];
+            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) wc -= rd * loAul[k] * sh[loCol[k] - base];
+            sh[r0.c - base] = wc;
         }
         __syncthreads();
-        cur = nxt;
+        r0 = r1;
+        r1 = r2;
+        r2 = r3;
     }
-    dilu_row_load(d, d.nLev - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, cur);
-    for (int t = d.nLev - 1; t >= 0; --t) {
-        dilu_row_load(d, t - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, nxt);
-        if (cur.c >= 0) {
-            const double rd = cur.a;
-            double wc = sh[cur.c - base];
-            const int np = min(cur.k1 - cur.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) wc -= rd * cur.v0[q] * sh[cur.col[q] - base];
-            for (int k = cur.k0 + kDiluPre; k < cur.k1; ++k) wc -= rd * upAlu[k] * sh[upCol[k] - base];
-            sh[cur.c - base] = wc;
+    const int L = d.nLev - 1;
+    dilu_row_load(d, L, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r0);
+    dilu_row_load(d, L - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r1);
+    dilu_row_load(d, L - 2, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r2);
+    for (int t = L; t >= 0; --t) {
+        dilu_row_load(d, t - 3, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r3);
+        if (r0.c >= 0) {
+            const double rd = r0.a;
+            double wc = sh[r0.c - base];
+            const int np = min(r0.k1 - r0.k0, kDiluPre);
+            for (int q = 0; q < np; ++q) wc -= rd * r0.v0[q] * sh[r0.col[q] - base];
+            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) wc -= rd * upAlu[k] * sh[upCol[k] - base];
+            sh[r0.c - base] = wc;
         }
         __syncthreads();
-        cur = nxt;
+        r0 = r1;
+        r1 = r2;
+        r2 = r3;
     }
     for (int i = tid; i < d.rowCount; i += blockDim.x) w[base + i] = sh[i];
 }

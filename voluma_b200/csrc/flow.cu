@@ -451,13 +451,26 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     gU_.resize(9 * N);
     gP_.resize(3 * N);
     cont_.resize(1);
+    const int maxSolves = ctrl_.n_outer * (3 + ctrl_.n_corr * (ctrl_.n_non_orth_corr + 1));
+    solveState_.resize(size_t(maxSolves));
+    solveStatus_.resize(size_t(2) * maxSolves);
     for (DBuf<double>* b : {&U_, &U0_, &U00_, &p_, &phi_, &pffc_}) b->zero(s_);
+}
+
+// Next record slot of this step; the solve writes its SysState and status words there.
+int DeviceFlow::solveSlot(bool momentum, bool monitoredP) {
+    const int k = nSolves_++;
+    VLM_REQUIRE(size_t(k) < solveState_.size(), VLM_ERR_CUDA, "internal: solve records exhausted");
+    if (momentum) uSolves_.push_back(k);
+    if (monitoredP) pSolve_ = k;
+    batch_.deferNextSolve(solveState_.get() + k, solveStatus_.get() + 2 * k);
+    return k;
 }
 
 void DeviceFlow::boundaryU() {
     if (nB_ > 0)
         k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, G_.own(), G_.bPatch(), uType_.get(), uValue_.get(),
-                                                U_.get(), Ub_.get());
+                                                U_.get(), Ub_.get()), ++launches_;
 }
 
 void DeviceFlow::boundaryP() {
@@ -470,21 +483,21 @@ void DeviceFlow::boundaryP() {
 void DeviceFlow::gradU() {
     k_grad_tensor<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, nF_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
                                             G_.w(), G_.Sf(), G_.V(), U_.get(), Ub_.get(), G_.twoD(), G_.emptyDir(),
-                                            gU_.get());
+                                            gU_.get()), ++launches_;
 }
 
 void DeviceFlow::setState(const double* U, const double* p) {
     if (U) {
         DBuf<double> tmp;
         tmp.upload(U, size_t(3) * nC_, s_);
-        k_soa_from_aos<<<nblk(nC_), 256, 0, s_>>>(nC_, tmp.get(), U_.get());
+        k_soa_from_aos<<<nblk(nC_), 256, 0, s_>>>(nC_, tmp.get(), U_.get()), ++launches_;
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
     if (p) p_.upload(p, size_t(nC_), s_);
     boundaryU();
     boundaryP();
     k_flux_u<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), U_.get(), Ub_.get(),
-                                       phi_.get());
+                                       phi_.get()), ++launches_;
     rAU_.zero(s_);
     VLM_CUDA(cudaGetLastError());
     VLM_CUDA(cudaStreamSynchronize(s_));
@@ -494,7 +507,7 @@ void DeviceFlow::setState(const double* U, const double* p) {
 void DeviceFlow::getState(double* U, double* p, double* phi) {
     if (U) {
         DBuf<double> tmp(size_t(3) * nC_);
-        k_aos_from_soa<<<nblk(nC_), 256, 0, s_>>>(nC_, U_.get(), tmp.get());
+        k_aos_from_soa<<<nblk(nC_), 256, 0, s_>>>(nC_, U_.get(), tmp.get()), ++launches_;
         VLM_CUDA(cudaMemcpyAsync(U, tmp.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToHost, s_));
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
@@ -511,10 +524,10 @@ void DeviceFlow::assembleMomentum(double aU) {
         k_mom_faces<<<nblk(nI_), 256, 0, s_>>>(nI_, nC_, nF_, G_.own(), G_.nei(), G_.w(), G_.magSf(), G_.ndc(), G_.d(),
                                               G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, ctrl_.div_scheme,
                                               G_.nonOrthogonal() ? 1 : 0, gU_.get(), loDiv_.get(), upDiv_.get(),
-                                              lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get());
+                                              lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), uValue_.get(), G_.magSf(),
-                                               G_.ndc(), phi_.get(), ctrl_.nu, ic_.get(), bs_.get());
+                                               G_.ndc(), phi_.get(), ctrl_.nu, ic_.get(), bs_.get()), ++launches_;
     // ddt coefficients (Schemes.h:70-86)
     double kc = 0, kc0 = 0, kc00 = 0;
     const bool transient = !ctrl_.steady;
@@ -533,10 +546,10 @@ void DeviceFlow::assembleMomentum(double aU) {
     k_mom_cells<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, G_.cellFaceOff(), G_.cellFaces(), loDiv_.get(), upDiv_.get(),
                                           lapUp_.get(), cDiv_.get(), ffc_.get(), G_.V(), transient ? 1 : 0, kc, kc0,
                                           kc00, U0_.get(), nOld_ >= 2 ? U00_.get() : U0_.get(), diag_.get(),
-                                          src_.get());
+                                          src_.get()), ++launches_;
     if (aU < 1.0)
         k_mom_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), upper_.get(),
-                                              lower_.get(), ic_.get(), U_.get(), aU, diag_.get(), src_.get());
+                                              lower_.get(), ic_.get(), U_.get(), aU, diag_.get(), src_.get()), ++launches_;
     VLM_CUDA(cudaGetLastError());
 }
 
@@ -546,29 +559,27 @@ void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     pbc.type = pTypeHost_.data();
     pbc.value = pValueB_.get();
     G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
-    k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get());
-    double r = 0, nf = 0;
+    k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get()), ++launches_;
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
     for (int k : solved_) {
         G_.fold(diag_.get(), msrc_.get() + k * N, ic_.get() + k * B, bs_.get() + k * B, fd_.get(), fb_.get(), s_);
         std::vector<vlm_solver_perf> pf;
+        solveSlot(first, false);
         batch_.solve(fd_.get(), upper_.get(), lower_.get(), fb_.get(), U_.get() + k * N, ctrl_.U, pf);
-        info.iterations += pf[0].iterations;
-        r = std::max(r, pf[0].residualSum);
-        nf = std::max(nf, pf[0].normFactor);
+        solveLaunches_.push_back(batch_.lastDeferred());
     }
+    (void)info;
     boundaryU();
-    if (first) info.UInitialResidual = r / (nf + 1e-30);
 }
 
 // One pressure correction (IncompressibleFlow.cpp:244-362)
 void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info) {
     k_mom_AH<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
                                        diag_.get(), upper_.get(), lower_.get(), ic_.get(), bs_.get(), src_.get(),
-                                       U_.get(), G_.V(), rAU_.get(), HbyA_.get());
+                                       U_.get(), G_.V(), rAU_.get(), HbyA_.get()), ++launches_;
     k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
                                          uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(), rAUf_.get(),
-                                         phiHbyA_.get());
+                                         phiHbyA_.get()), ++launches_;
     G_.div(phiHbyA_.get(), divPhi_.get(), s_);
     if (ctrl_.steady) VLM_CUDA(cudaMemcpyAsync(pPrev_.get(), p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToDevice, s_));
     ScalarBC pbc;
@@ -584,30 +595,23 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
         if (needRef_) G_.setReference(ctrl_.p_ref_cell, ctrl_.p_ref_value, pdiag_.get(), psrc_.get(), s_);
         G_.fold(pdiag_.get(), psrc_.get(), pic_.get(), pbs_.get(), fd_.get(), fb_.get(), s_);
         std::vector<vlm_solver_perf> pf;
+        solveSlot(false, first && no == 0);
         batch_.solve(fd_.get(), pupper_.get(), pupper_.get(), fb_.get(), p_.get(),
                      (finalCorr && finalNO) ? ctrl_.p_final : ctrl_.p, pf);
-        info.iterations += pf[0].iterations;
-        if (first && no == 0) {
-            // monitored pressure residual with a normalisation floor (IncompressibleFlow.cpp:320-327)
-            if (pNormSteps_ < 5) {
-                pNormRef_ = std::max(pNormRef_, pf[0].normFactor);
-                ++pNormSteps_;
-            }
-            info.pInitialResidual = pf[0].residualSum / (std::max(pf[0].normFactor, pNormRef_) + 1e-30);
-        }
+        solveLaunches_.push_back(batch_.lastDeferred());
         boundaryP();
         if (finalNO) {
             G_.flux(pupper_.get(), p_.get(), pic_.get(), pbs_.get(), hasFfc ? pffc_.get() : nullptr, pflux_.get(), s_);
-            k_phi_update<<<nblk(nF_), 256, 0, s_>>>(nF_, phiHbyA_.get(), pflux_.get(), phi_.get());
+            k_phi_update<<<nblk(nF_), 256, 0, s_>>>(nF_, phiHbyA_.get(), pflux_.get(), phi_.get()), ++launches_;
         }
     }
     if (ctrl_.steady && ctrl_.alpha_p < 1.0) {
-        k_p_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, pPrev_.get(), ctrl_.alpha_p, p_.get());
+        k_p_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, pPrev_.get(), ctrl_.alpha_p, p_.get()), ++launches_;
         boundaryP();
     }
     G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
     k_u_correct<<<nblk(nC_), 256, 0, s_>>>(nC_, HbyA_.get(), rAU_.get(), gP_.get(), G_.twoD(), G_.emptyDir(),
-                                          U_.get());
+                                          U_.get()), ++launches_;
     boundaryU();
     VLM_CUDA(cudaGetLastError());
 }
@@ -634,6 +638,11 @@ vlm_step_info DeviceFlow::step(double dt) {
     }
     boundaryU();
     boundaryP();
+    nSolves_ = 0;
+    uSolves_.clear();
+    solveLaunches_.clear();
+    pSolve_ = -1;
+    const int64_t own0 = launches_, geom0 = G_.launches();
     for (int outer = 0; outer < ctrl_.n_outer; ++outer) {
         const bool finalOuter = outer == ctrl_.n_outer - 1;
         const double aU = steady ? ctrl_.alpha_u : (finalOuter ? 1.0 : ctrl_.alpha_u);
@@ -645,10 +654,50 @@ vlm_step_info DeviceFlow::step(double dt) {
     // continuity error: max |div phi| (IncompressibleFlow.cpp:367-370)
     G_.div(phi_.get(), divPhi_.get(), s_);
     cont_.zero(s_);
-    k_max_abs<<<std::min(nblk(nC_), 1184), 256, 0, s_>>>(nC_, divPhi_.get(), (unsigned long long*)cont_.get());
+    k_max_abs<<<std::min(nblk(nC_), 1184), 256, 0, s_>>>(nC_, divPhi_.get(), (unsigned long long*)cont_.get()), ++launches_;
     VLM_CUDA(cudaMemcpyAsync(&info.continuityError, cont_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
+    // the step's solver records, read once
+    std::vector<SysState> st(static_cast<size_t>(nSolves_));
+    std::vector<int> status(static_cast<size_t>(2 * nSolves_));
+    if (nSolves_ > 0) {
+        VLM_CUDA(cudaMemcpyAsync(st.data(), solveState_.get(), sizeof(SysState) * nSolves_, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaMemcpyAsync(status.data(), solveStatus_.get(), sizeof(int) * 2 * nSolves_, cudaMemcpyDeviceToHost,
+                                 s_));
+    }
     VLM_CUDA(cudaStreamSynchronize(s_));
     VLM_CUDA(cudaGetLastError());
+    for (int k = 0; k < nSolves_; ++k) {
+        if (status[2 * k + 1] != 0) {
+            batch_.clearLevelError();
+            throw Error(VLM_ERR_TIMEOUT, "level-scheduled sweep: a group barrier wait gave up");
+        }
+        if (status[2 * k] == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+        info.iterations += st[k].iterations;
+    }
+    int64_t launched = (launches_ - own0) + (G_.launches() - geom0);
+    for (int k = 0; k < nSolves_ && k < int(solveLaunches_.size()); ++k) {
+        const auto& c = solveLaunches_[k];
+        launched += c.eager + c.pre + int64_t(st[k].iterations) * c.body;
+    }
+    info.launches = int32_t(launched);
+    total_ += launched;
+    // monitored residuals (IncompressibleFlow.cpp:205-213, 320-327)
+    if (!uSolves_.empty()) {
+        double r = 0, nf = 0;
+        for (int k : uSolves_) {
+            r = std::max(r, st[k].residualSum);
+            nf = std::max(nf, st[k].normFactor);
+        }
+        info.UInitialResidual = r / (nf + 1e-30);
+    }
+    if (pSolve_ >= 0) {
+        const SysState& q = st[pSolve_];
+        if (pNormSteps_ < 5) {
+            pNormRef_ = std::max(pNormRef_, q.normFactor);
+            ++pNormSteps_;
+        }
+        info.pInitialResidual = q.residualSum / (std::max(q.normFactor, pNormRef_) + 1e-30);
+    }
     return info;
 }
 

@@ -40,6 +40,8 @@ public:
     vlm_step_info step(double dt);
     // fields to host (any pointer may be null)
     void getState(double* U, double* p, double* phi);
+    // kernels run by this flow so far (its own, the geometry's and the solves', graph nodes included)
+    int64_t launches() const { return total_; }
 
 private:
     void boundaryU();
@@ -69,6 +71,15 @@ private:
     DBuf<double> gU_, gP_, msrc_, rAU_, HbyA_, rAUf_, phiHbyA_, divPhi_, pPrev_, fd_, fb_;
     DBuf<double> pdiag_, pupper_, psrc_, pic_, pbs_, pffc_, pflux_;
     DBuf<double> cont_;  // continuity error (max, as ordered bits)
+    // solver records of the step's solves, read once at the end of the step
+    DBuf<SysState> solveState_;
+    DBuf<int> solveStatus_;
+    int nSolves_ = 0;
+    std::vector<int> uSolves_;  // record indices of the first outer pass's momentum solves
+    int pSolve_ = -1;           // record index of the monitored pressure solve
+    int solveSlot(bool momentum, bool monitoredP);
+    std::vector<DeviceBatch::LaunchCount> solveLaunches_;  // per record, set after its solve
+    int64_t launches_ = 0, total_ = 0;
     // time state (Schemes.h TimeState) and the pressure-residual normalisation of the step
     double time_ = 0, dt_ = 1, dt0_ = -1;
     int timeIndex_ = 0, nOld_ = 0;

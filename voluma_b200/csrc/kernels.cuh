@@ -634,12 +634,13 @@ __global__ void k_coarse_apply(const CoarseDev* __restrict__ cs, const double* _
 constexpr int kTailThreads = 1024;
 constexpr int kTailBatch = 4;      // entries in flight per row (64 registers at 1024 threads)
 constexpr int kTailMaxRows = 1024;  // levels at most this many rows (padded) go to the tail
+constexpr int kTailFullRows = 8192; // systems at most this many level-0 rows run the whole V-cycle there
 
 template <class T>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* __restrict__ tsys,
                                                                  const TailLevel<T>* __restrict__ lev,
                                                                  const double* __restrict__ inv, const T* r0, T* x0,
-                                                                 T omega, const SysState* st, int flag) {
+                                                                 T omega, const SysState* st, int flag, int jacobi0) {
     pdl_entry();
     const TailSys& ts = tsys[blockIdx.x];
     if (st != nullptr && sys_idle(st[ts.sys], flag)) return;  // uniform over the CTA
@@ -648,11 +649,43 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
     auto rOf = [&](int k) -> const T* { return k == 0 ? r0 : lev[k].r; };
     auto xOf = [&](int k) -> T* { return k == 0 ? x0 : lev[k].x; };
 
+    // level 0 with global multicolour Gauss-Seidel (k_smooth_gs colour steps, k_zero_rows, k_prolong)
+    auto gsRows = [&](const TailLevel<T>& L, const T* r, T* x, int g0, int g1, int mode, const T* xc) {
+        for (int i = g0 + tid; i < g1; i += nthr) {
+            if (mode == 1) {
+                x[i] = r[i] / __ldg(L.diag + i);
+                continue;
+            }
+            auto xf = [&](int j) -> T {
+                T v = x[j];
+                if (mode == 2) {
+                    const int a = __ldg(L.agg + j);
+                    if (a >= 0) v += xc[a];
+                }
+                return v;
+            };
+            const T s = row_accumulate<true, T, decltype(xf), kTailBatch>(L.S, L.val, xf, i, r[i]);
+            x[i] = s / __ldg(L.diag + i);
+        }
+    };
     for (int k = ts.first; k < c; ++k) {
         const TailLevel<T>& L = lev[k];
         const T* r = rOf(k);
         T* x = xOf(k);
         const int a0 = ts.rowStart[k], a1 = a0 + ts.rowCount[k];
+        if (k == 0 && !jacobi0) {
+            const int nc = ts.nColours;
+            if (!ts.two) {
+                for (int i = a0 + tid; i < a1; i += nthr) x[i] = T(0);
+                __syncthreads();
+            }
+            for (int sweep = 0; sweep < 2; ++sweep)
+                for (int t = 0; t < nc; ++t) {
+                    gsRows(L, r, x, ts.grpStart[t], ts.grpStart[t] + ts.grpCount[t],
+                           (ts.two && sweep == 0 && t == 0) ? 1 : 0, nullptr);
+                    __syncthreads();
+                }
+        } else {
         // two pre-sweeps from zero; the first sweep's value of a neighbour is recomputed where
         // the second sweep needs it (MODE 1 then MODE 0 of k_smooth_jacobi)
         auto first = [&](int j) -> T {
@@ -670,6 +703,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
             }
         }
         __syncthreads();
+        }
         // residual of each child computed where its aggregate sums it (k_residual + k_restrict)
         T* rn = lev[k + 1].r;
         auto xr = [&](int j) -> T { return x[j]; };
@@ -707,6 +741,25 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
         const T* xc = xOf(k + 1);
         T* x2 = L.x2;
         const int a0 = ts.rowStart[k], a1 = a0 + ts.rowCount[k];
+        if (k == 0 && !jacobi0) {
+            // post-smoothing: colours reversed; two colours fuse the prolongation into the first step
+            const int nc = ts.nColours;
+            if (!ts.two) {
+                for (int i = a0 + tid; i < a1; i += nthr) {
+                    const int a = __ldg(L.agg + i);
+                    if (a >= 0) x[i] += xc[a];
+                }
+                __syncthreads();
+            }
+            for (int sweep = 0; sweep < 2; ++sweep)
+                for (int t = 0; t < nc; ++t) {
+                    const int q = nc - 1 - t;
+                    gsRows(L, r, x, ts.grpStart[q], ts.grpStart[q] + ts.grpCount[q],
+                           (ts.two && sweep == 0 && t == 0) ? 2 : 0, xc);
+                    if (sweep + 1 < 2 || t + 1 < nc) __syncthreads();
+                }
+            continue;
+        }
         // post-sweep 1 with the coarse-grid correction fused in (MODE 2), into x2
         auto xv = [&](int j) -> T {
             T v = x[j];

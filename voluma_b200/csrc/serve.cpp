@@ -189,6 +189,7 @@ struct vlm_server {
             d.phi.resize(size_t(q.nFaces));
             st = vlm_flow_get_state(flow, d.U.data(), d.p.data(), d.phi.data());
         }
+        if (flow) d.r.launches = vlm_flow_launches(flow);
         d.r.UInitialResidual = info.UInitialResidual;
         d.r.pInitialResidual = info.pInitialResidual;
         d.r.continuityError = info.continuityError;

@@ -26,7 +26,8 @@ struct DiluDev {
     DBuf<DiluBar> bars;
     DBuf<int> err;
     int G = 1, groups = 0, nFaces = 0;
-    size_t smem = 0;  // > 0: shared-memory sweeps with this many bytes per CTA
+    size_t smem = 0;   // > 0: shared-memory sweeps with this many bytes per CTA
+    int threads = 0;   // their CTA size: the widest level rounded up to whole warps (cheap barriers)
 };
 
 
@@ -134,6 +135,11 @@ __global__ void k_set_cond(cudaGraphConditionalHandle h, int nsys, const SysStat
     if (threadIdx.x == 0) cudaGraphSetConditional(h, a ? 1u : 0u);
 }
 
+__global__ void k_set_ctrl(DevCtrl* out, DevCtrl v) {
+    pdl_entry();
+    *out = v;
+}
+
 std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
     size_t n = 0;
     VLM_CUDA(cudaGraphGetNodes(g, nullptr, &n));
@@ -199,6 +205,15 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
                 if (k > 0 && tailFirst_[c.sys] >= k) in.push_back(c);
             D.headActive = add(head);
             D.headIn = add(in);
+            for (int t = 0; t < P.nSteps; ++t) {
+                std::vector<Chunk> hf, hr;
+                for (const Chunk& c : P.fwd[t])
+                    if (tailFirst_[c.sys] > k) hf.push_back(c);
+                for (const Chunk& c : P.rev[t])
+                    if (tailFirst_[c.sys] > k) hr.push_back(c);
+                D.headFwd.push_back(add(hf));
+                D.headRev.push_back(add(hr));
+            }
         }
         for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
         for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
@@ -435,10 +450,11 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
         // needed) and the post-smoothing's first colour applies the prolongation to the
         // neighbours it reads (no separate prolongation).
         const bool two = D.nSteps == 2;
-        if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), x, st, flag);
+        const ChunkList& rows = head ? D.headActive : D.active;
+        if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, rows.n, kRowsPerCta, s, D.ch(rows), x, st, flag);
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
-                const ChunkList& l = pre ? D.fwd[t] : D.rev[t];
+                const ChunkList& l = head ? (pre ? D.headFwd[t] : D.headRev[t]) : (pre ? D.fwd[t] : D.rev[t]);
                 if (two && sweep == 0 && t == 0 && pre)
                     VLM_LAUNCH((k_smooth_gs<T, 1>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
                                flag);
@@ -478,7 +494,7 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
                    LV<T>::r(N), st, flag);
     }
     if (tail) {
-        recordTail<T>(r0, x0, flag);
+        recordTail<T>(r0, x0, flag, sm == SmootherKind::Jacobi);
     } else {
         for (int k = 0; k < nL; ++k) {
             DevLevel& D = L_[k];
@@ -490,20 +506,21 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
         DevLevel& D = L_[k];
         const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
         // block GS, Jacobi and two-colour GS fuse the prolongation into their first sweep
-        if (!jacobiHere && !D.blockGS && D.nSteps != 2)
-            VLM_LAUNCH(k_prolong<T>, D.active.n, kRowsPerCta, s, D.ch(D.active), D.agg.get(), xx(k + 1), xx(k), st,
-                       flag);
+        if (!jacobiHere && !D.blockGS && D.nSteps != 2) {
+            const ChunkList& rows = tail ? D.headActive : D.active;
+            VLM_LAUNCH(k_prolong<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.agg.get(), xx(k + 1), xx(k), st, flag);
+        }
         recordSmooth<T>(k, rr(k), xx(k), sm, false, flag, tail);
     }
 }
 
 template <class T>
-void DeviceBatch::recordTail(const T* r0, T* x0, int flag) {
+void DeviceBatch::recordTail(const T* r0, T* x0, int flag, bool jacobi0) {
     const TailLevel<T>* tab = std::is_same<T, float>::value ? (const TailLevel<T>*)tail32_.get()
                                                              : (const TailLevel<T>*)tail64_.get();
     if (!tab) throw Error(VLM_ERR_CUDA, "internal: coarse-tail table missing");
     VLM_LAUNCH(k_vcycle_tail<T>, int(tailSys_.size()), kTailThreads, stream_, (const TailSys*)tailSys_.get(), tab,
-               (const double*)inv_.get(), r0, x0, T(jacobiOmega_), (const SysState*)st_.get(), flag);
+               (const double*)inv_.get(), r0, x0, T(jacobiOmega_), (const SysState*)st_.get(), flag, jacobi0 ? 1 : 0);
 }
 
 // Per system: the first level of the single-CTA tail = the first level (below level 0) whose
@@ -514,8 +531,10 @@ void DeviceBatch::planTail() {
     if (tv && tv[0] == '0') return;
     const int ns = plan_.nsys;
     if (ns == 0) return;
-    int64_t maxRows = kTailMaxRows;
+    int64_t maxRows = kTailMaxRows, fullRows = kTailFullRows;
     if (const char* mr = std::getenv("VLM_TAIL_ROWS")) maxRows = std::atoll(mr);
+    if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) fullRows = std::atoll(fr);
+    const LevelPlan& L0 = plan_.levels[0];
     tailFirst_.assign(size_t(ns), 0);
     std::vector<TailSys> ts(static_cast<size_t>(ns));
     tailMaxFirst_ = 0;
@@ -523,11 +542,15 @@ void DeviceBatch::planTail() {
         const int c = plan_.nLevels[b] - 1;
         if (c >= kTailMaxLevels) throw Error(VLM_ERR_UNSUPPORTED, "GAMG hierarchy deeper than the coarse tail supports");
         int first = c;
-        for (int k = 1; k < c; ++k)
-            if (int64_t(plan_.levels[k].sysRow[b + 1] - plan_.levels[k].sysRow[b]) <= maxRows) {
-                first = k;
-                break;
-            }
+        const int64_t rows0 = plan_.levels[0].sysRow[b + 1] - plan_.levels[0].sysRow[b];
+        if (c > 0 && rows0 <= fullRows && !plan_.levels[0].blockGS)
+            first = 0;  // the whole V-cycle of a small system in one CTA
+        else
+            for (int k = 1; k < c; ++k)
+                if (int64_t(plan_.levels[k].sysRow[b + 1] - plan_.levels[k].sysRow[b]) <= maxRows) {
+                    first = k;
+                    break;
+                }
         tailFirst_[b] = first;
         tailMaxFirst_ = std::max(tailMaxFirst_, first);
         TailSys& t = ts[b];
@@ -542,6 +565,22 @@ void DeviceBatch::planTail() {
             t.rowStart[k] = plan_.levels[k].sysRow[b];
             t.rowCount[k] = plan_.levels[k].sysRow[b + 1] - plan_.levels[k].sysRow[b];
         }
+        // level-0 colour groups of this system (the chunks of the colour steps)
+        t.two = L0.nSteps == 2 ? 1 : 0;
+        t.nColours = 0;
+        for (int q = 0; q < L0.nSteps && q < 4; ++q) {
+            int s0 = -1, cnt = 0;
+            for (const Chunk& ch : L0.fwd[q])
+                if (ch.sys == b) {
+                    if (s0 < 0) s0 = ch.start;
+                    cnt += ch.count;
+                }
+            if (s0 < 0) break;
+            t.grpStart[q] = s0;
+            t.grpCount[q] = cnt;
+            t.nColours = q + 1;
+        }
+        if (first == 0 && L0.nSteps > 4) first = c;  // (never: level 0 is block-hybrid beyond 4 colours)
         if (cp.rowStart != t.rowStart[c]) throw Error(VLM_ERR_CUDA, "internal: coarse-tail row mismatch");
     }
     tailSys_.upload(ts, stream_);
@@ -748,6 +787,7 @@ void DeviceBatch::ensureDilu() {
         }();
         (void)raised;
         D->smem = std::max<size_t>(size_t(P.maxRows) * sizeof(double), 8);
+        D->threads = std::max(32, (P.maxWidth + 31) / 32 * 32);
     }
     D->bars.resize(size_t(D->groups));
     D->bars.zero(s);
@@ -781,7 +821,7 @@ void DeviceBatch::diluFactor(const double* upper, const double* lower) {
     VLM_LAUNCH(k_dilu_values, nblk(Dd.nFaces), 256, s, Dd.nFaces, (const int32_t*)Dd.loFace.get(),
                (const int32_t*)Dd.upFace.get(), upper, lower, Dd.loAul.get(), Dd.loAlu.get(), Dd.upAlu.get());
     if (Dd.smem) {
-        k_dilu_factor_smem<<<Dd.groups, kDiluThreads, Dd.smem, s>>>(Dd.sys.get(), Dd.levPtr.get(), Dd.levRows.get(),
+        k_dilu_factor_smem<<<Dd.groups, Dd.threads, Dd.smem, s>>>(Dd.sys.get(), Dd.levPtr.get(), Dd.levRows.get(),
                                                                     Dd.loPtr.get(), Dd.loCol.get(), Dd.loAlu.get(),
                                                                     Dd.loAul.get(), L_[0].diag.get(), Dd.rD.get());
         VLM_CUDA(cudaGetLastError());
@@ -792,6 +832,12 @@ void DeviceBatch::diluFactor(const double* upper, const double* lower) {
                  (const int32_t*)Dd.levRows.get(), (const int32_t*)Dd.loPtr.get(), (const int32_t*)Dd.loCol.get(),
                  (const double*)Dd.loAlu.get(), (const double*)Dd.loAul.get(), (const double*)L_[0].diag.get(),
                  Dd.rD.get(), Dd.bars.get(), Dd.err.get());
+}
+
+void DeviceBatch::clearLevelError() {
+    if (!dilu_) return;
+    dilu_->err.zero(stream_);
+    dilu_->bars.zero(stream_);
 }
 
 // A group barrier of a level-scheduled kernel that gave up leaves its status here.
@@ -809,7 +855,7 @@ void DeviceBatch::checkLevelError() {
 void DeviceBatch::recordDiluApply(const double* r, double* w) {
     DiluDev& D = *dilu_;
     if (D.smem) {
-        k_dilu_apply_smem<<<D.groups, kDiluThreads, D.smem, stream_>>>(
+        k_dilu_apply_smem<<<D.groups, D.threads, D.smem, stream_>>>(
             D.sys.get(), D.levPtr.get(), D.levRows.get(), D.loPtr.get(), D.loCol.get(), D.loAul.get(), D.upPtr.get(),
             D.upCol.get(), D.upAlu.get(), D.rD.get(), r, w, st_.get(), kFlagDone);
         VLM_CUDA(cudaGetLastError());
@@ -1035,14 +1081,16 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
             VLM_LAUNCH(k_recip_diag<float>, nblk(n0), 256, s, n0, perm0_.get(), D0.diag32.get(), rD32_.get());
         }
     }
-    static thread_local DevCtrl hc;  // stays valid until the synchronising copy below
+    // the controls travel as kernel arguments: a copy from pageable host memory would wait for
+    // the stream and stop the host from running ahead
+    DevCtrl hc;
     hc.tolerance = ctrl.tolerance;
     hc.relTol = ctrl.relTol;
     hc.innerRelTol = ctrl.innerRelTol > 0 ? ctrl.innerRelTol : 1e-4;
     hc.maxIter = ctrl.maxIter;
     hc.minIter = ctrl.minIter;
     hc.maxInner = ctrl.maxIter;
-    VLM_CUDA(cudaMemcpyAsync(dctrl_.get(), &hc, sizeof(DevCtrl), cudaMemcpyHostToDevice, s));
+    VLM_LAUNCH(k_set_ctrl, 1, 1, s, dctrl_.get(), hc);
     st_.zero(s);
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), b, b_.get());
@@ -1082,6 +1130,22 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
         tl_launches = e0;
     }
     VLM_LAUNCH(k_from_solver, nblk(n0), 256, s, n0, perm0_.get(), x_.get(), x);
+    if (deferState_) {
+        SysState* so = deferState_;
+        int* sto = deferStatus_;
+        deferState_ = nullptr;
+        deferStatus_ = nullptr;
+        lastDeferred_.eager = (tl_launches - launch0) + eagerLaunches;
+        lastDeferred_.pre = Gp ? Gp->preK : 0;
+        lastDeferred_.body = Gp ? Gp->bodyK : 0;
+        VLM_CUDA(cudaMemcpyAsync(so, st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToDevice, s));
+        VLM_CUDA(cudaMemcpyAsync(sto, status_.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
+        if (levelSchedule)
+            VLM_CUDA(cudaMemcpyAsync(sto + 1, dilu_->err.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
+        else
+            VLM_CUDA(cudaMemsetAsync(sto + 1, 0, sizeof(int), s));
+        return;
+    }
     int coarseStatus = 0;
     VLM_CUDA(cudaMemcpyAsync(hostState_.data(), st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaMemcpyAsync(&coarseStatus, status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1227,7 +1291,7 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
         const bool allow = name != "vcycle32_notail";
         run = [&, allow, name] {
             if (name == "tail32") {
-                if (tailOn_) recordTail<float>(r32_.get(), w32_.get(), kFlagDone);
+                if (tailOn_) recordTail<float>(r32_.get(), w32_.get(), kFlagDone, false);
             } else {
                 recordVcycle<float>(r32_.get(), w32_.get(), SmootherKind::MCGSJacobi, kFlagDone, allow);
             }

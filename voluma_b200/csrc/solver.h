@@ -26,6 +26,7 @@ struct DevLevel {
     DBuf<Chunk> chunks;
     ChunkList active, all;
     ChunkList headActive, headIn;  // coarse-tail mode: rows above each system's tail / restricted into
+    std::vector<ChunkList> headFwd, headRev;  // coarse-tail mode: colour steps of the systems above the tail
     std::vector<ChunkList> fwd, rev;
     DBuf<int32_t> agg, childPtr, child, intraPtr, intraFace, cfacePtr, cfaceSrc;
     ChunkList coarse;  // CoarseDev entries whose coarsest level is this one
@@ -89,6 +90,22 @@ public:
     void solve(const double* diag, const double* upper, const double* lower, const double* b, double* x,
                const vlm_solver_ctrl& ctrl, std::vector<vlm_solver_perf>& perfOut);
 
+    // The next solve() only enqueues its work: its final solver state (one SysState per system) and
+    // its status words (coarsest-matrix status, level-schedule barrier status) are copied, on the
+    // stream, to these device locations, and solve() returns without waiting or filling perfOut.
+    void deferNextSolve(SysState* stateOut, int* statusOut) {
+        deferState_ = stateOut;
+        deferStatus_ = statusOut;
+    }
+    // Clears a level-schedule barrier error left by a deferred solve.
+    void clearLevelError();
+    // Launch counts of the last deferred solve: kernels launched directly, and (graph mode) the
+    // kernel nodes of the loop's entry and of one loop pass; launches = eager + pre + its * body.
+    struct LaunchCount {
+        int64_t eager = 0, pre = 0, body = 0;
+    };
+    LaunchCount lastDeferred() const { return lastDeferred_; }
+
     // y = A x (user layout device pointers)
     void amul(const double* diag, const double* upper, const double* lower, const double* x, double* y);
 
@@ -111,7 +128,7 @@ public:
 private:
     template <class T> void recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bool allowTail = true);
     template <class T> void recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pre, int flag, bool head);
-    template <class T> void recordTail(const T* r0, T* x0, int flag);
+    template <class T> void recordTail(const T* r0, T* x0, int flag, bool jacobi0);
     template <class T> void buildTailTable(DBuf<TailLevel<T>>& out);
     void planTail();
     void ensureDilu();
@@ -159,6 +176,9 @@ private:
     DBuf<TailSys> tailSys_;
     std::vector<SysTopo> topo_;          // host topology (owned by the caller for the batch's lifetime)
     std::unique_ptr<DiluDev> dilu_;      // built on the first DIC/DILU/Gauss-Seidel solve
+    SysState* deferState_ = nullptr;     // deferNextSolve targets (one-shot)
+    LaunchCount lastDeferred_;
+    int* deferStatus_ = nullptr;
     const double* curUpper_ = nullptr;   // face coefficients of the current solve (device, user layout)
     const double* curLower_ = nullptr;
     DBuf<TailLevel<double>> tail64_;
