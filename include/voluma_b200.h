@@ -281,6 +281,34 @@ int64_t vlm_flow_launches(vlm_flow* flow);
 vlm_status vlm_flow_get_state(vlm_flow* flow, double* U, double* p, double* phi);
 vlm_status vlm_flow_destroy(vlm_flow* flow);
 
+/* Turbulence model and momentum forcing of a flow: the LES Smagorinsky model with optional Van
+ * Driest damping (TurbulenceModel::correct, TurbulenceModel.cpp:226-250; LESModel::correctModel,
+ * LESModels.cpp:64-153; Smagorinsky::nutCell, LESModels.cpp:274-287) and the momentum forcing of
+ * IncompressibleFlow (MomentumForcing, IncompressibleFlow.h:40-47; the source terms at
+ * IncompressibleFlow.cpp:186-202 and applyForcingCorrection, :115-142).  Set before the first step
+ * (vlm_flow_set_model replaces IncompressibleFlow.updateTurbulence and .forcing). */
+typedef struct vlm_flow_model {
+    int32_t les;               /* 0 laminar, 1 Smagorinsky */
+    double Cs;                 /* Smagorinsky constant (coeffs.Cs, 0.17) */
+    int32_t van_driest;        /* damp the filter width near walls (vanDriest) */
+    double Aplus, Cdelta;      /* Van Driest constants (coeffs.Aplus 26, coeffs.Cdelta 0.158) */
+    double kappa;              /* von Karman constant (coeffs.kappa 0.41) */
+    double delta_coeff;        /* filter width = delta_coeff * cbrt(V) (coeffs.deltaCoeff 1) */
+    double nut_max_ratio;      /* nu_t is limited to nut_max_ratio * nu (nutMaxRatio 1e5) */
+    double depth;              /* 2D meshes: extent in the empty direction (filter width sqrt(V / depth)) */
+    const int32_t* wall_patch; /* per mesh patch: 1 = wall (PatchType::Wall), else 0; may be NULL (no walls) */
+    int32_t forcing;           /* 0 none, 1 constant body force, 2 mean velocity */
+    double force[3];           /* constant: force per unit mass */
+    double Ubar[3];            /* mean velocity: target volume-averaged velocity */
+    double relaxation;         /* mean velocity: gain of the pressure-gradient update (1) */
+    double grad_p;             /* mean velocity: initial driving pressure gradient (0) */
+} vlm_flow_model;
+
+vlm_status vlm_flow_set_model(vlm_flow* flow, const vlm_flow_model* model);
+/* nu_t per cell (nCells, of the last step's last outer pass) and the mean-velocity driving pressure
+ * gradient; either pointer may be NULL. */
+vlm_status vlm_flow_get_model_state(vlm_flow* flow, double* nut, double* grad_p);
+
 /* ------------------------------------------------------------------ serving */
 /* Continuous batching of incompressible solves on one device (no counterpart in the reference,
  * which runs one case per process): requests are admitted in arrival order when a slot is free and

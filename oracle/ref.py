@@ -7,6 +7,7 @@ baseline / reference arm, never by the product package.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 
 import numpy as np
@@ -51,6 +52,8 @@ def lib():
         L.ref_exact_sum.restype = C.c_double
         L.ref_exact_sum.argtypes = [P, C.c_long]
         L.ref_flow_run.argtypes = [P, C.POINTER(RefFlowSpec), C.c_int, C.c_double, P, P, P, P, C.POINTER(C.c_int)]
+        L.ref_flow_run_model.argtypes = [P, C.POINTER(RefFlowSpec), C.POINTER(RefModelSpec), C.c_int, C.c_double,
+                                         P, P, P, P, C.POINTER(C.c_int), P, P]
         L.ref_flow_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -77,6 +80,38 @@ class RefFlowSpec(C.Structure):
                 ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
                 ("reproducible", C.c_int), ("residualTol", C.c_double)]
+
+
+class RefModelSpec(C.Structure):
+    _fields_ = [("turbulence", C.c_char_p), ("forcing", C.c_int), ("force", C.c_double * 3),
+                ("Ubar", C.c_double * 3), ("relaxation", C.c_double), ("gradP", C.c_double)]
+
+
+def _model_spec(model):
+    """RefModelSpec of a Flow.set_model dict: the turbulence dictionary as the reference's case files
+    write it ("model", "vanDriest", "coeffs"; LESModels.cpp:17-60, 274-281) and the forcing."""
+    les = model.get("les", "laminar")
+    les = {0: "laminar", 1: "Smagorinsky"}.get(les, les)
+    turb = None
+    if les != "laminar":
+        coeffs = {k: model[k] for k in ("Cs", "Aplus", "Cdelta", "kappa") if k in model}
+        if "delta_coeff" in model:
+            coeffs["deltaCoeff"] = model["delta_coeff"]
+        d = {"model": les, "vanDriest": bool(model.get("van_driest", False)), "coeffs": coeffs}
+        if "nut_max_ratio" in model:
+            d["nutMaxRatio"] = model["nut_max_ratio"]
+        turb = json.dumps(d).encode()
+    ms = RefModelSpec()
+    ms.turbulence = turb
+    fo = model.get("forcing", "none")
+    ms.forcing = {"none": 0, "constant": 1, "meanVelocity": 2}[fo] if isinstance(fo, str) else int(fo)
+    for k, v in enumerate(model.get("force", (0.0, 0.0, 0.0))):
+        ms.force[k] = v
+    for k, v in enumerate(model.get("Ubar", (0.0, 0.0, 0.0))):
+        ms.Ubar[k] = v
+    ms.relaxation = model.get("relaxation", 1.0)
+    ms.gradP = model.get("grad_p", 0.0)
+    return ms, turb
 
 
 def _solver_ctl(d):
@@ -131,11 +166,14 @@ class RefMesh:
         return out
 
     # ------------------------------------------------------------------ incompressible step
-    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False, residual_tol=0.0):
+    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False, residual_tol=0.0, model=None):
         """n_steps of IncompressibleFlow::step(dt) (solvers/IncompressibleFlow.cpp:138-370) with the case
         settings of `case` (a dict, voluma_b200.cases.lid_cavity layout).  residual_tol > 0 stops at
         convergence like fvmFlow's steady loop.  Returns U (n,3), p, phi, and the per-step history
-        [UInitialResidual, pInitialResidual, continuityError, linear iterations] of the steps run."""
+        [UInitialResidual, pInitialResidual, continuityError, linear iterations] of the steps run.
+        `model` (the Flow.set_model dict) adds the reference's turbulence model, built from the equivalent
+        "turbulence" case dictionary by TurbulenceModel::create, and the momentum forcing; the run then
+        also returns nu_t per cell and the final forcing gradP."""
         nC = self.n_cells
         Uc = np.zeros((nC, 3)) if U is None else np.ascontiguousarray(U, np.float64).reshape(nC, 3).copy()
         pc = np.zeros(nC) if p is None else np.ascontiguousarray(p, np.float64).copy()
@@ -156,9 +194,18 @@ class RefMesh:
         sp.reproducible = int(reproducible)
         sp.residualTol = residual_tol
         ran = C.c_int()
-        if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist), C.byref(ran)) != 0:
+        if model is None:
+            if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist),
+                                  C.byref(ran)) != 0:
+                raise RuntimeError(lib().ref_flow_error().decode())
+            return Uc, pc, phi, hist[:ran.value]
+        ms, turb = _model_spec(model)
+        nut = np.zeros(nC)
+        gp = np.zeros(1)
+        if lib().ref_flow_run_model(self._h, C.byref(sp), C.byref(ms), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist),
+                                    C.byref(ran), _p(nut), _p(gp)) != 0:
             raise RuntimeError(lib().ref_flow_error().decode())
-        return Uc, pc, phi, hist[:ran.value]
+        return Uc, pc, phi, hist[:ran.value], nut, float(gp[0])
 
     # ------------------------------------------------------------------ linear algebra
     def amul(self, diag, upper, lower, x):

@@ -5,10 +5,13 @@
 // arrays and settings; every number comes from the unmodified reference.
 
 #include "fvm/solvers/IncompressibleFlow.h"
+#include "fvm/core/Json.h"
+#include "fvm/models/TurbulenceModel.h"
 #include "fvm/parallel/Comm.h"
 
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <string>
 
 using namespace cfd;
@@ -46,8 +49,21 @@ struct RefFlowSpec {
     double residualTol;  // > 0: stop once U and p residuals are below it (from step 2, fvmFlow.cpp:611-625)
 };
 
+// Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
+// `turbulence` is the case's "turbulence" dictionary as JSON text (NULL: laminar); forcing 0 none,
+// 1 constant (force), 2 meanVelocity (Ubar, relaxation; gradP is the initial driving gradient).
+struct RefModelSpec {
+    const char* turbulence;
+    int forcing;
+    double force[3], Ubar[3];
+    double relaxation, gradP;
+};
+
 int ref_flow_run(const RefMesh* r, const RefFlowSpec* spec, int nSteps, double dt, double* U, double* p,
                  double* phi, double* hist, int* stepsRun);
+// ref_flow_run with a turbulence model / forcing; also returns nu_t per cell and the final gradP.
+int ref_flow_run_model(const RefMesh* r, const RefFlowSpec* spec, const RefModelSpec* model, int nSteps, double dt,
+                       double* U, double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP);
 const char* ref_flow_error();
 }
 
@@ -69,11 +85,12 @@ SolverControls toCtl(const RefSolverCtl& c) {
 
 const char* ref_flow_error() { return g_flowErr.c_str(); }
 
+namespace {
 // Runs nSteps of IncompressibleFlow::step(dt) from the given U (3 per cell) and p (per cell).
 // Outputs U, p, phi (nFaces) and per step hist[4*k..]: UInitialResidual, pInitialResidual,
 // continuityError, total linear-solver iterations.
-int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt, double* U, double* p, double* phi,
-                 double* hist, int* stepsRun) {
+int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, int nSteps, double dt, double* U,
+            double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP) {
     try {
         par::setReproducible(sp->reproducible != 0);
         const Mesh& m = *r->mesh;
@@ -108,6 +125,20 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
             else
                 flow.p().zeroGradient(name);
         }
+        // the turbulence model keeps references to its dictionaries: they live as long as the run
+        const Json empty = Json::parse("{}");
+        const Json turb = Json::parse(model && model->turbulence ? model->turbulence : "{}");
+        std::unique_ptr<TurbulenceModel> tm;
+        if (model && model->turbulence) tm = TurbulenceModel::create(flow, turb, empty, empty);
+        if (model && model->forcing == 1) {
+            flow.forcing.mode = MomentumForcing::Mode::Constant;
+            flow.forcing.force = Vec3{model->force[0], model->force[1], model->force[2]};
+        } else if (model && model->forcing == 2) {
+            flow.forcing.mode = MomentumForcing::Mode::MeanVelocity;
+            flow.forcing.Ubar = Vec3{model->Ubar[0], model->Ubar[1], model->Ubar[2]};
+            flow.forcing.relaxation = model->relaxation;
+            flow.forcing.gradP = model->gradP;
+        }
         const label nC = m.nCells();
         for (label k = 0; k < nC; ++k) {
             flow.U()[k] = Vec3{U[3 * k], U[3 * k + 1], U[3 * k + 2]};
@@ -139,6 +170,9 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
         }
         if (phi)
             for (label f = 0; f < m.nFaces(); ++f) phi[f] = flow.phi()[f];
+        if (nut)
+            for (label k = 0; k < nC; ++k) nut[k] = flow.nut().empty() ? 0.0 : flow.nut()[k];
+        if (gradP) *gradP = flow.forcing.gradP;
         par::setReproducible(false);
         return 0;
     } catch (const std::exception& e) {
@@ -146,4 +180,15 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
         par::setReproducible(false);
         return 1;
     }
+}
+}  // namespace
+
+int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt, double* U, double* p, double* phi,
+                 double* hist, int* stepsRun) {
+    return runFlow(r, sp, nullptr, nSteps, dt, U, p, phi, hist, stepsRun, nullptr, nullptr);
+}
+
+int ref_flow_run_model(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, int nSteps, double dt,
+                       double* U, double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP) {
+    return runFlow(r, sp, model, nSteps, dt, U, p, phi, hist, stepsRun, nut, gradP);
 }

@@ -539,9 +539,11 @@ static int gamg_init(gamg_t* g, const vo_hier* H, const double* diag, const doub
                 for (int k = 0; k < i; ++k) v -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
                 X[(size_t)i * n + j] = v;
             }
+            /* U back substitution with the upper terms in descending k (the device kernel's
+               right-looking order) */
             for (int i = n - 1; i >= 0; --i) {
                 double v = X[(size_t)i * n + j];
-                for (int k = i + 1; k < n; ++k) v -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
+                for (int k = n - 1; k > i; --k) v -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
                 X[(size_t)i * n + j] = v / A[(size_t)i * n + i];
             }
         }

@@ -498,6 +498,42 @@ class Flow:
     def launches(self) -> int:
         return int(load().vlm_flow_launches(self._h))
 
+    def set_model(self, model: dict):
+        """Turbulence model and momentum forcing (vlm_flow_model), before the first step.  `model`: les
+        ("laminar" or "Smagorinsky"), Cs, van_driest, Aplus, Cdelta, kappa, delta_coeff, nut_max_ratio,
+        depth (2D), wall_patch (per patch 0/1), forcing ("none", "constant", "meanVelocity"), force, Ubar,
+        relaxation, grad_p; missing keys take the reference's defaults."""
+        mdl = _ffi.FlowModel()
+        les = model.get("les", "laminar")
+        mdl.les = {"laminar": 0, "Smagorinsky": 1}[les] if isinstance(les, str) else int(les)
+        mdl.Cs = model.get("Cs", 0.17)
+        mdl.van_driest = int(bool(model.get("van_driest", False)))
+        mdl.Aplus = model.get("Aplus", 26.0)
+        mdl.Cdelta = model.get("Cdelta", 0.158)
+        mdl.kappa = model.get("kappa", 0.41)
+        mdl.delta_coeff = model.get("delta_coeff", 1.0)
+        mdl.nut_max_ratio = model.get("nut_max_ratio", 1e5)
+        mdl.depth = model.get("depth", 0.0)
+        wp = model.get("wall_patch")
+        self._wall = None if wp is None else np.ascontiguousarray(wp, np.int32)
+        mdl.wall_patch = None if self._wall is None else self._wall.ctypes.data
+        fo = model.get("forcing", "none")
+        mdl.forcing = {"none": 0, "constant": 1, "meanVelocity": 2}[fo] if isinstance(fo, str) else int(fo)
+        for k, v in enumerate(model.get("force", (0.0, 0.0, 0.0))):
+            mdl.force[k] = v
+        for k, v in enumerate(model.get("Ubar", (0.0, 0.0, 0.0))):
+            mdl.Ubar[k] = v
+        mdl.relaxation = model.get("relaxation", 1.0)
+        mdl.grad_p = model.get("grad_p", 0.0)
+        check(load().vlm_flow_set_model(self._h, C.byref(mdl)), self.mesh.ctx.handle)
+
+    def model_state(self):
+        """(nu_t per cell, mean-velocity driving pressure gradient)."""
+        nut = np.zeros(self.n_cells)
+        gp = np.zeros(1)
+        check(load().vlm_flow_get_model_state(self._h, nut.ctypes.data, gp.ctypes.data), self.mesh.ctx.handle)
+        return nut, float(gp[0])
+
     def run_steady(self, max_iter=5000, residual_tol=1e-6):
         it = C.c_int32()
         i = _ffi.StepInfo()

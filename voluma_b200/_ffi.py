@@ -19,7 +19,8 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
            "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
            "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
-           "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy"]
+           "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy", "vlm_flow_set_model",
+           "vlm_flow_get_model_state"]
 
 
 class MeshDesc(C.Structure):
@@ -54,6 +55,14 @@ class FlowCtrl(C.Structure):
 class StepInfo(C.Structure):
     _fields_ = [("UInitialResidual", C.c_double), ("pInitialResidual", C.c_double),
                 ("continuityError", C.c_double), ("iterations", C.c_int32), ("launches", C.c_int32)]
+
+
+class FlowModel(C.Structure):
+    _fields_ = [("les", C.c_int32), ("Cs", C.c_double), ("van_driest", C.c_int32), ("Aplus", C.c_double),
+                ("Cdelta", C.c_double), ("kappa", C.c_double), ("delta_coeff", C.c_double),
+                ("nut_max_ratio", C.c_double), ("depth", C.c_double), ("wall_patch", C.c_void_p),
+                ("forcing", C.c_int32), ("force", C.c_double * 3), ("Ubar", C.c_double * 3),
+                ("relaxation", C.c_double), ("grad_p", C.c_double)]
 
 
 class FlowRequest(C.Structure):
@@ -102,6 +111,8 @@ def load():
     L.vlm_flow_run_steady.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_int32), C.POINTER(StepInfo)]
     L.vlm_flow_get_state.argtypes = [P, P, P, P]
     L.vlm_flow_destroy.argtypes = [P]
+    L.vlm_flow_set_model.argtypes = [P, C.POINTER(FlowModel)]
+    L.vlm_flow_get_model_state.argtypes = [P, P, P]
     L.vlm_flow_launches.restype = C.c_int64
     L.vlm_flow_launches.argtypes = [P]
     L.vlm_flow_request_bytes.restype = C.c_int64

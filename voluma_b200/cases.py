@@ -170,6 +170,57 @@ def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     return m, case, U0
 
 
+def channel_beta(ny, y1, height=2.0):
+    """tanh grading parameter beta of a two-sided stretched wall-normal direction of ny cells whose
+    first cell is y1 high (bisection on tanhStretch, RawMesh.cpp:387-389)."""
+    def first(beta):
+        t = 2.0 / ny - 1.0
+        return 0.5 * height * (1.0 + math.tanh(beta * t) / math.tanh(beta))
+    lo, hi = 1e-6, 20.0
+    if first(lo) <= y1:
+        return 0.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if first(mid) > y1:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def channel(n=(256, 192, 128), Re_b=6875.0, Re_tau=395.0, y_plus1=1.0, ubar=1.0, noise=0.1, seed=20261203,
+            les=True, van_driest=True, beta=None):
+    """Periodic channel 2pi x 2 x pi (x streamwise and z spanwise periodic, walls at yMin / yMax,
+    half-height 1), tanh-graded in y so that the first cell has y+ ~ y_plus1 at Re_tau; nu = ubar / Re_b
+    (Re_b 6875 <-> Re_tau ~ 395, the reference's channel395 case); mean-velocity forcing to Ubar =
+    (ubar, 0, 0) (fvmFlow.cpp:182-194); Smagorinsky LES with Van Driest damping (LESModels.cpp); the
+    fvmFlow transient defaults (backward, linear, nOuter 1, nCorr 2; U {PBiCGStab, DILU, 1e-8},
+    p {PCG, GAMG, 1e-8, relTol 0.01}, pFinal relTol 0).  Initial field: the laminar profile
+    1.5 ubar (1 - (y - 1)^2) plus a seeded uniform perturbation of +-noise*ubar in every component.
+    Returns (mesh, case, model, U0, dt) with dt at a Courant number of ~0.5."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    if beta is None:
+        beta = channel_beta(ny, y_plus1 / Re_tau)
+    m = vm.box_mesh((nx, ny, nz), hi=(2 * np.pi, 2.0, np.pi), periodic=(True, False, True), beta=(0.0, beta, 0.0))
+    nP = len(m["patch_start"])
+    walls = np.array([1 if m["patch_names"][q] in ("yMin", "yMax") else 0 for q in range(nP)], np.int32)
+    case = dict(nu=ubar / Re_b, steady=False, div_scheme=1, ddt_scheme=2, n_outer=1, n_corr=2, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=1.0, alpha_p=1.0, u_type=walls.copy(), u_value=np.zeros(3 * nP),
+                p_type=np.zeros(nP, np.int32), p_value=np.zeros(nP),
+                U=_ctl("PBiCGStab", "DILU", 1e-8, 0.0, 1000), p=_ctl("PCG", "GAMG", 1e-8, 0.01, 2000),
+                pFinal=_ctl("PCG", "GAMG", 1e-8, 0.0, 2000), p_ref_cell=0, p_ref_value=0.0)
+    model = dict(les="Smagorinsky" if les else "laminar", van_driest=bool(van_driest), wall_patch=walls,
+                 forcing="meanVelocity", Ubar=(ubar, 0.0, 0.0))
+    y = m["C"][:, 1]
+    rng = np.random.default_rng(seed)
+    U0 = np.zeros((m["n_cells"], 3))
+    U0[:, 0] = 1.5 * ubar * (1.0 - (y - 1.0) ** 2)
+    U0 += noise * ubar * rng.uniform(-1.0, 1.0, size=U0.shape)
+    dt = 0.5 * (2 * np.pi / nx) / (1.5 * ubar + noise * ubar)
+    return m, case, model, U0, dt
+
+
 def serving_trace(n_requests=32, rate_hz=2.0, seed=20261203, n_range=(32, 256), re_range=(100.0, 1000.0)):
     """Serving stream of steady lid-cavity solves: Poisson arrivals of the given rate (seeded),
     mesh N x N with N uniform in n_range (inclusive), Re uniform in re_range.

@@ -729,6 +729,22 @@ vlm_status vlm_flow_get_state(vlm_flow* f, double* U, double* p, double* phi) {
 
 int64_t vlm_flow_launches(vlm_flow* f) { return f ? f->flow->launches() : 0; }
 
+vlm_status vlm_flow_set_model(vlm_flow* f, const vlm_flow_model* model) {
+    if (!f || !model) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->setModel(*model);
+    });
+}
+
+vlm_status vlm_flow_get_model_state(vlm_flow* f, double* nut, double* gradP) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->modelState(nut, gradP);
+    });
+}
+
 vlm_status vlm_flow_destroy(vlm_flow* f) {
     if (!f) return VLM_OK;
     cudaSetDevice(f->mesh->ctx->device);

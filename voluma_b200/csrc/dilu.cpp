@@ -61,14 +61,46 @@ DiluPlan buildDiluPlan(const std::vector<SysTopo>& systems, const BatchPlan& P) 
         ds.nLev = nLev;
         ds.rowBegin = L0.sysRow[b];
         ds.rowCount = L0.sysRow[b + 1] - L0.sysRow[b];
-        ds.pad = 0;
+        ds.slotBegin = int(D.levRows.size());
+        ds.loBegin = int(D.sLoCol.size());
+        ds.upBegin = int(D.sUpCol.size());
         D.maxRows = std::max(D.maxRows, ds.rowCount);
         for (auto& v : byLevel) {
             std::sort(v.begin(), v.end());
-            D.maxWidth = std::max(D.maxWidth, int(v.size()));
+            const int width = int(v.size());
+            D.maxWidth = std::max(D.maxWidth, width);
+            DiluLevel lv;
+            lv.s0 = int(D.levRows.size());
+            lv.width = width;
+            lv.mlo = lv.mup = 0;
+            for (int r : v) {
+                lv.mlo = std::max(lv.mlo, int(lo[r].size()));
+                lv.mup = std::max(lv.mup, int(up[r].size()));
+                D.slotRow.push_back(r - ds.rowBegin);
+            }
+            D.maxEnt = std::max({D.maxEnt, lv.mlo, lv.mup});
+            lv.lo = int(D.sLoCol.size());
+            for (int j = 0; j < lv.mlo; ++j)
+                for (int r : v) {
+                    const bool has = j < int(lo[r].size());
+                    D.sLoCol.push_back(has ? lo[r][j][1] - ds.rowBegin : -1);
+                    D.sLoFace.push_back(has ? lo[r][j][2] : 0);
+                }
+            lv.up = int(D.sUpCol.size());
+            for (int j = 0; j < lv.mup; ++j)
+                for (int r : v) {
+                    const int nu = int(up[r].size());
+                    const bool has = j < nu;  // backward order: descending (u, f)
+                    D.sUpCol.push_back(has ? up[r][nu - 1 - j][1] - ds.rowBegin : -1);
+                    D.sUpFace.push_back(has ? up[r][nu - 1 - j][2] : 0);
+                }
+            D.lev.push_back(lv);
             D.levRows.insert(D.levRows.end(), v.begin(), v.end());
             D.levPtr.push_back(int32_t(D.levRows.size()));
         }
+        ds.slotEnd = int(D.levRows.size());
+        ds.loEnd = int(D.sLoCol.size());
+        ds.upEnd = int(D.sUpCol.size());
         D.maxLevels = std::max(D.maxLevels, nLev);
         D.sys.push_back(ds);
     }

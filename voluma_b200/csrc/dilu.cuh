@@ -137,132 +137,217 @@ __global__ void __launch_bounds__(kDiluThreads) k_dilu_apply(const DiluSys* __re
     }
 }
 
-// ---------------------------------------------------------------- shared-memory variants
+// ---------------------------------------------------------------- shared-memory (streamed) variants
 // One CTA per system whose level-0 vector fits in shared memory and whose levels are at most one
-// row per thread.  The swept vector lives in shared memory, and each thread loads its rows of the
-// next three levels (row index, scalars and the first kDiluPre coefficients) ahead of the barriers,
-// so a level costs a barrier and shared-memory reads, not an L2 round trip.
-// Same arithmetic in the same order as k_dilu_factor / k_dilu_apply.
-constexpr int kDiluPre = 4;
+// row per thread.  The swept vector lives in shared memory.  The schedule is streamed (dilu.h,
+// DiluLevel): each level's rows, scalars and entries are contiguous in global memory, and cp.async
+// copies them into a ring of kDiluRing shared-memory stages, kDiluRing - 1 levels ahead of the
+// sweep, so a level costs one barrier and shared-memory reads instead of a chain of L2 round trips.
+//
+// The factor's A_lu * A_ul is formed once per factorisation (the product the reference's
+// rD[u] -= A_lu A_ul / rD[l] forms first); every other operation is the reference's, in its order,
+// so the results are those of k_dilu_factor / k_dilu_apply bit for bit.
+constexpr int kDiluRing = 8;
 
-struct DiluRow {
-    int c, k0, k1;
-    double a, b;                      // apply: rD[c], r[c]; factor: diag[c]
-    int col[kDiluPre];
-    double v0[kDiluPre], v1[kDiluPre];  // apply: A_ul (fwd) / A_lu (bwd); factor: A_lu, A_ul
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(unsigned(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(unsigned(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__host__ __device__ constexpr size_t dilu_align16(size_t b) { return (b + 15) / 16 * 16; }
+
+// One ring stage for levels of at most W slots and M entries per slot: a[W] (slot scalar),
+// v[M * W] (entry coefficient), row[W], col[M * W].
+__host__ __device__ constexpr size_t dilu_stage_bytes(int W, int M) {
+    return dilu_align16(size_t(W) * (M + 1) * (sizeof(double) + sizeof(int32_t)));
+}
+
+// Shared memory of a streamed kernel: the vector, the level table and the ring.
+__host__ __device__ constexpr size_t dilu_stream_smem(int rows, int levels, int W, int M) {
+    return dilu_align16(size_t(rows) * sizeof(double)) + dilu_align16(size_t(levels) * sizeof(DiluLevel)) +
+           kDiluRing * dilu_stage_bytes(W, M);
+}
+
+struct DiluStage {
+    double *a, *v;
+    int32_t *row, *col;
+    __device__ DiluStage(char* base, int W, int M) {
+        a = reinterpret_cast<double*>(base);
+        v = a + W;
+        row = reinterpret_cast<int32_t*>(v + size_t(M) * W);
+        col = row + W;
+    }
 };
 
-__device__ __forceinline__ void dilu_row_load(const DiluSys& d, int t, int tid, const int32_t* __restrict__ levPtr,
-                                              const int32_t* __restrict__ levRows, const int32_t* __restrict__ ptr,
-                                              const int32_t* __restrict__ col, const double* __restrict__ c0,
-                                              const double* __restrict__ c1, const double* __restrict__ sa,
-                                              const double* __restrict__ sb, DiluRow& p) {
-    p.c = -1;
-    if (t < 0 || t >= d.nLev) return;
-    const int idx = levPtr[d.levBegin + t] + tid;
-    if (idx >= levPtr[d.levBegin + t + 1]) return;
-    p.c = levRows[idx];
-    p.a = sa[p.c];
-    p.b = sb ? sb[p.c] : 0.0;
-    p.k0 = ptr[p.c];
-    p.k1 = ptr[p.c + 1];
-#pragma unroll
-    for (int q = 0; q < kDiluPre; ++q)
-        if (p.k0 + q < p.k1) {
-            p.col[q] = col[p.k0 + q];
-            p.v0[q] = c0[p.k0 + q];
-            p.v1[q] = c1 ? c1[p.k0 + q] : 0.0;
-        }
-}
-
-__global__ void __launch_bounds__(kDiluThreads) k_dilu_factor_smem(const DiluSys* __restrict__ ds,
-                                                                   const int32_t* __restrict__ levPtr,
-                                                                   const int32_t* __restrict__ levRows,
-                                                                   const int32_t* __restrict__ loPtr,
-                                                                   const int32_t* __restrict__ loCol,
-                                                                   const double* __restrict__ loAlu,
-                                                                   const double* __restrict__ loAul,
-                                                                   const double* __restrict__ diag,
-                                                                   double* __restrict__ rD) {
-    extern __shared__ double sh[];
-    const DiluSys d = ds[blockIdx.x];
-    const int base = d.rowBegin, tid = threadIdx.x;
-    DiluRow r0, r1, r2, r3;  // levels t .. t+3 in flight
-    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r0);
-    dilu_row_load(d, 1, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r1);
-    dilu_row_load(d, 2, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r2);
-    for (int t = 0; t < d.nLev; ++t) {
-        dilu_row_load(d, t + 3, tid, levPtr, levRows, loPtr, loCol, loAlu, loAul, diag, nullptr, r3);
-        if (r0.c >= 0) {
-            double v = r0.a;
-            const int np = min(r0.k1 - r0.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) v -= r0.v0[q] * r0.v1[q] / sh[r0.col[q] - base];
-            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) v -= loAlu[k] * loAul[k] / sh[loCol[k] - base];
-            sh[r0.c - base] = v;
-        }
-        __syncthreads();
-        r0 = r1;
-        r1 = r2;
-        r2 = r3;
+// Starts the copies of one level's slots (rows and, if sa, one scalar per slot) and its m entries per
+// slot (columns and coefficients) into a stage.
+__device__ __forceinline__ void dilu_stage_issue(const DiluStage& S, const DiluLevel& L, int ent, int m,
+                                                 const int32_t* __restrict__ slotRow, const double* __restrict__ sa,
+                                                 const int32_t* __restrict__ col, const double* __restrict__ v) {
+    const int tid = threadIdx.x;
+    if (tid < L.width) {
+        cp_async4(S.row + tid, slotRow + L.s0 + tid);
+        if (sa != nullptr) cp_async8(S.a + tid, sa + L.s0 + tid);
     }
-    for (int i = tid; i < d.rowCount; i += blockDim.x) rD[base + i] = 1.0 / sh[i];
+    const int n = m * L.width;
+    for (int k = tid; k < n; k += blockDim.x) {
+        cp_async4(S.col + k, col + ent + k);
+        cp_async8(S.v + k, v + ent + k);
+    }
 }
 
-__global__ void __launch_bounds__(kDiluThreads) k_dilu_apply_smem(const DiluSys* __restrict__ ds,
-                                                                  const int32_t* __restrict__ levPtr,
-                                                                  const int32_t* __restrict__ levRows,
-                                                                  const int32_t* __restrict__ loPtr,
-                                                                  const int32_t* __restrict__ loCol,
-                                                                  const double* __restrict__ loAul,
-                                                                  const int32_t* __restrict__ upPtr,
-                                                                  const int32_t* __restrict__ upCol,
-                                                                  const double* __restrict__ upAlu,
-                                                                  const double* __restrict__ rD, const double* r,
-                                                                  double* w, const SysState* st, int flag) {
+// Streamed sweep over levels t = 0 .. nLev-1 (or reversed) of one system: before level t is
+// processed, the copies of level t + kDiluRing - 1 are started into the stage level t - 1 used.
+// body(stage, level) runs for every slot thread of the level.
+template <bool LOWER, bool REVERSE, class Body>
+__device__ __forceinline__ void dilu_stream(const DiluLevel* lt, int nLev, char* ring, int W, int M,
+                                            const int32_t* __restrict__ slotRow, const double* __restrict__ sa,
+                                            const int32_t* __restrict__ col, const double* __restrict__ v,
+                                            Body body) {
+    const size_t SB = dilu_stage_bytes(W, M);
+    auto issue = [&](int q) {
+        if (q < nLev) {
+            const DiluLevel& L = lt[REVERSE ? nLev - 1 - q : q];
+            dilu_stage_issue(DiluStage(ring + size_t(q % kDiluRing) * SB, W, M), L, LOWER ? L.lo : L.up,
+                             LOWER ? L.mlo : L.mup, slotRow, sa, col, v);
+        }
+        cp_async_commit();
+    };
+    for (int q = 0; q < kDiluRing - 1; ++q) issue(q);
+    for (int q = 0; q < nLev; ++q) {
+        cp_async_wait<kDiluRing - 2>();
+        __syncthreads();  // level q staged by every thread; level q - 1's vector writes visible
+        issue(q + kDiluRing - 1);
+        const DiluLevel& L = lt[REVERSE ? nLev - 1 - q : q];
+        if (threadIdx.x < L.width) body(DiluStage(ring + size_t(q % kDiluRing) * SB, W, M), L);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+// Shared memory of a streamed kernel: the vector sh[rowCount] (filled from src by cp.async), the
+// level table and the ring.  Both copies are waited for before the function returns.
+__device__ __forceinline__ char* dilu_stream_setup(char* smem, const DiluSys& d, const DiluLevel* __restrict__ lev,
+                                                   const double* __restrict__ src, double*& sh, DiluLevel*& lt) {
+    sh = reinterpret_cast<double*>(smem);
+    lt = reinterpret_cast<DiluLevel*>(smem + dilu_align16(size_t(d.rowCount) * sizeof(double)));
+    const int32_t* lg = reinterpret_cast<const int32_t*>(lev + d.levBegin);
+    int32_t* ls = reinterpret_cast<int32_t*>(lt);
+    const int nw = d.nLev * int(sizeof(DiluLevel) / sizeof(int32_t));
+    for (int i = threadIdx.x; i < nw; i += blockDim.x) cp_async4(ls + i, lg + i);
+    for (int i = threadIdx.x; i < d.rowCount; i += blockDim.x) cp_async8(sh + i, src + d.rowBegin + i);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    return reinterpret_cast<char*>(lt) + dilu_align16(size_t(d.nLev) * sizeof(DiluLevel));
+}
+
+// Per-solve coefficients of the streamed schedule: prod = A_lu A_ul and coefLo = A_ul per lower
+// entry, coefUp = A_lu per upper entry.
+__global__ void k_dilu_stream_values(int nLo, int nUp, const int32_t* __restrict__ loCol,
+                                     const int32_t* __restrict__ loFace, const int32_t* __restrict__ upCol,
+                                     const int32_t* __restrict__ upFace, const double* __restrict__ upper,
+                                     const double* __restrict__ lower, double* __restrict__ prod,
+                                     double* __restrict__ coefLo, double* __restrict__ coefUp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nLo) {
+        double p = 0.0, c = 0.0;
+        if (loCol[k] >= 0) {
+            const int32_t a = loFace[k];
+            const int fa = a & 0x7fffffff;
+            const double aul = a < 0 ? lower[fa] : upper[fa];
+            const double alu = a < 0 ? upper[fa] : lower[fa];
+            p = alu * aul;
+            c = aul;
+        }
+        prod[k] = p;
+        coefLo[k] = c;
+    } else if (k - nLo < nUp) {
+        const int q = k - nLo;
+        double c = 0.0;
+        if (upCol[q] >= 0) {
+            const int32_t b = upFace[q];
+            const int fb = b & 0x7fffffff;
+            c = b < 0 ? upper[fb] : lower[fb];
+        }
+        coefUp[q] = c;
+    }
+}
+
+// rD = D - sum_l A_lu A_ul / rD[l] in level order; rDs[slot] = 1 / rD[row] as each level completes.
+__global__ void __launch_bounds__(kDiluThreads) k_dilu_factor_stream(
+    const DiluSys* __restrict__ ds, const DiluLevel* __restrict__ lev, int W, int M,
+    const int32_t* __restrict__ slotRow, const int32_t* __restrict__ loCol, const double* __restrict__ prod,
+    const double* __restrict__ diag, double* __restrict__ rDs) {
+    extern __shared__ __align__(16) char dsm[];
+    const DiluSys d = ds[blockIdx.x];
+    double* sh;
+    DiluLevel* lt;
+    char* ring = dilu_stream_setup(dsm, d, lev, diag, sh, lt);
+    dilu_stream<true, false>(lt, d.nLev, ring, W, M, slotRow, nullptr, loCol, prod,
+                             [&](const DiluStage& S, const DiluLevel& L) {
+                                 const int q = threadIdx.x, c = S.row[q];
+                                 double v = sh[c];
+                                 for (int j = 0; j < L.mlo; ++j) {
+                                     const int l = S.col[j * L.width + q];
+                                     if (l < 0) break;
+                                     v -= S.v[j * L.width + q] / sh[l];
+                                 }
+                                 sh[c] = v;
+                                 rDs[L.s0 + q] = 1.0 / v;
+                             });
+}
+
+// w = M^-1 r: forward w[u] = rD[u] r[u] - sum rD[u] A_ul w[l], backward w[l] -= sum rD[l] A_lu w[u]
+// (each product formed left to right, as the reference's expressions do)
+__global__ void __launch_bounds__(kDiluThreads) k_dilu_apply_stream(
+    const DiluSys* __restrict__ ds, const DiluLevel* __restrict__ lev, int W, int M,
+    const int32_t* __restrict__ slotRow, const double* __restrict__ rDs, const int32_t* __restrict__ loCol,
+    const double* __restrict__ coefLo, const int32_t* __restrict__ upCol, const double* __restrict__ coefUp,
+    const double* r, double* w, const SysState* st, int flag) {
     pdl_entry();
-    extern __shared__ double sh[];
+    extern __shared__ __align__(16) char dsm[];
     const DiluSys d = ds[blockIdx.x];
     if (st != nullptr && sys_idle(st[d.sys], flag)) return;
-    const int base = d.rowBegin, tid = threadIdx.x;
-    DiluRow r0, r1, r2, r3;  // levels t .. t+3 in flight
-    dilu_row_load(d, 0, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r0);
-    dilu_row_load(d, 1, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r1);
-    dilu_row_load(d, 2, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r2);
-    for (int t = 0; t < d.nLev; ++t) {
-        dilu_row_load(d, t + 3, tid, levPtr, levRows, loPtr, loCol, loAul, nullptr, rD, r, r3);
-        if (r0.c >= 0) {
-            const double rd = r0.a;
-            double wc = rd * r0.b;
-            const int np = min(r0.k1 - r0.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) wc -= rd * r0.v0[q] * sh[r0.col[q] - base];
-            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) wc -= rd * loAul[k] * sh[loCol[k] - base];
-            sh[r0.c - base] = wc;
-        }
-        __syncthreads();
-        r0 = r1;
-        r1 = r2;
-        r2 = r3;
-    }
-    const int L = d.nLev - 1;
-    dilu_row_load(d, L, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r0);
-    dilu_row_load(d, L - 1, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r1);
-    dilu_row_load(d, L - 2, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r2);
-    for (int t = L; t >= 0; --t) {
-        dilu_row_load(d, t - 3, tid, levPtr, levRows, upPtr, upCol, upAlu, nullptr, rD, nullptr, r3);
-        if (r0.c >= 0) {
-            const double rd = r0.a;
-            double wc = sh[r0.c - base];
-            const int np = min(r0.k1 - r0.k0, kDiluPre);
-            for (int q = 0; q < np; ++q) wc -= rd * r0.v0[q] * sh[r0.col[q] - base];
-            for (int k = r0.k0 + kDiluPre; k < r0.k1; ++k) wc -= rd * upAlu[k] * sh[upCol[k] - base];
-            sh[r0.c - base] = wc;
-        }
-        __syncthreads();
-        r0 = r1;
-        r1 = r2;
-        r2 = r3;
-    }
-    for (int i = tid; i < d.rowCount; i += blockDim.x) w[base + i] = sh[i];
+    double* sh;
+    DiluLevel* lt;
+    char* ring = dilu_stream_setup(dsm, d, lev, r, sh, lt);
+    dilu_stream<true, false>(lt, d.nLev, ring, W, M, slotRow, rDs, loCol, coefLo,
+                             [&](const DiluStage& S, const DiluLevel& L) {
+                                 const int q = threadIdx.x, c = S.row[q];
+                                 const double rd = S.a[q];
+                                 double wc = rd * sh[c];
+                                 for (int j = 0; j < L.mlo; ++j) {
+                                     const int l = S.col[j * L.width + q];
+                                     if (l < 0) break;
+                                     wc -= rd * S.v[j * L.width + q] * sh[l];
+                                 }
+                                 sh[c] = wc;
+                             });
+    dilu_stream<false, true>(lt, d.nLev, ring, W, M, slotRow, rDs, upCol, coefUp,
+                             [&](const DiluStage& S, const DiluLevel& L) {
+                                 const int q = threadIdx.x, c = S.row[q];
+                                 const double rd = S.a[q];
+                                 double wc = sh[c];
+                                 for (int j = 0; j < L.mup; ++j) {
+                                     const int u = S.col[j * L.width + q];
+                                     if (u < 0) break;
+                                     wc -= rd * S.v[j * L.width + q] * sh[u];
+                                 }
+                                 sh[c] = wc;
+                             });
+    for (int i = threadIdx.x; i < d.rowCount; i += blockDim.x) w[d.rowBegin + i] = sh[i];
 }
 
 // Gauss-Seidel sweep in natural order (forward) or reversed (backward), in place:

@@ -20,7 +20,18 @@ namespace vlm {
 // One system's part of the schedule (batch position `sys`): levels [levBegin, levBegin + nLev) of
 // the concatenated level table.
 struct DiluSys {
-    int sys, levBegin, nLev, rowBegin, rowCount, pad;  // rows [rowBegin, rowBegin + rowCount) of level 0
+    int sys, levBegin, nLev, rowBegin, rowCount;  // rows [rowBegin, rowBegin + rowCount) of level 0
+    int slotBegin, slotEnd;                       // its slots: levRows[slotBegin .. slotEnd)
+    int loBegin, loEnd, upBegin, upEnd;           // its entries of the streamed schedule
+};
+
+// One level of the streamed schedule: slots [s0, s0 + width) of levRows; entry j of slot s0 + q at
+// lo + j * width + q (j < mlo, lower neighbours in forward order) and up + j * width + q (j < mup,
+// upper neighbours in backward order).  A row with fewer entries pads its column with -1.  A level's
+// rows, scalars and entries are contiguous, so a CTA can stream them into shared memory levels ahead
+// of the sweep without looking anything up.
+struct DiluLevel {
+    int s0, width, lo, mlo, up, mup;
 };
 
 struct DiluPlan {
@@ -32,6 +43,12 @@ struct DiluPlan {
     // padding rows are on level 0 of their system
     std::vector<int32_t> levPtr, levRows;
     std::vector<DiluSys> sys;
+    // streamed schedule (per level of levPtr): slot -> row - rowBegin, entries (local column or -1,
+    // face as loFace)
+    std::vector<DiluLevel> lev;
+    std::vector<int32_t> slotRow;
+    std::vector<int32_t> sLoCol, sLoFace, sUpCol, sUpFace;
+    int maxEnt = 0;    // largest mlo / mup of any level
     int maxWidth = 0;  // widest level over all systems
     int maxLevels = 0;
     int maxRows = 0;   // largest system (level-0 rows incl. padding)

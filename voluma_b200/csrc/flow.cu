@@ -82,8 +82,9 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
                             const double* __restrict__ w, const double* __restrict__ magSf,
                             const double* __restrict__ ndc, const double* __restrict__ d,
                             const double* __restrict__ corr, const double* __restrict__ C,
-                            const double* __restrict__ Cf, const double* __restrict__ phi, double nu, int scheme,
-                            int nonOrth, const double* __restrict__ G, double* __restrict__ loDiv,
+                            const double* __restrict__ Cf, const double* __restrict__ phi, double nu,
+                            const double* __restrict__ nuF, int scheme, int nonOrth, const double* __restrict__ G,
+                            double* __restrict__ loDiv,
                             double* __restrict__ upDiv, double* __restrict__ lapUp, double* __restrict__ upper,
                             double* __restrict__ lower, double* __restrict__ cDiv, double* __restrict__ ffc) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,7 +100,9 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
         wf = 0.75 * w[f] + 0.25 * wUp;
     const double lo = -wf * F;
     const double up = lo + F;
-    const double lap = nu * magSf[f] * ndc[f];
+    // laplacian(nu_eff, U) with the face values nuF (turbulence model) or the uniform nu
+    const double gam = nuF ? nuF[f] : nu;
+    const double lap = gam * magSf[f] * ndc[f];
     loDiv[f] = lo;
     upDiv[f] = up;
     lapUp[f] = lap;
@@ -134,7 +137,7 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
         double gf[9];
         for (int m = 0; m < 9; ++m) gf[m] = G[size_t(m) * nC + o] * wo + G[size_t(m) * nC + n] * wn;
         const double cv[3] = {corr[f], corr[nF + f], corr[2 * nF + f]};
-        const double s = nu * magSf[f];
+        const double s = gam * magSf[f];
         for (int j = 0; j < 3; ++j) fc[j] = (cv[0] * gf[j] + cv[1] * gf[3 + j] + cv[2] * gf[6 + j]) * s;
     }
     for (int k = 0; k < 3; ++k) ffc[size_t(k) * nI + f] = fc[k];
@@ -147,12 +150,12 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
 __global__ void k_mom_bfaces(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                              const double* __restrict__ uValue, const double* __restrict__ magSf,
                              const double* __restrict__ ndc, const double* __restrict__ phi, double nu,
-                             double* __restrict__ ic, double* __restrict__ bs) {
+                             const double* __restrict__ nuF, double* __restrict__ ic, double* __restrict__ bs) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int f = nI + b, q = bPatch[b];
     const bool fixedValue = uType[q] == 1;
-    const double F = phi[f], dc = ndc[f], gs = nu * magSf[f];
+    const double F = phi[f], dc = ndc[f], gs = (nuF ? nuF[f] : nu) * magSf[f];
     for (int k = 0; k < 3; ++k) {
         const double val = fixedValue ? uValue[3 * q + k] : 0.0;
         const double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
@@ -517,17 +520,18 @@ void DeviceFlow::getState(double* U, double* p, double* phi) {
 }
 
 // UEqn = ddt + div(phi, U) - laplacian(nu, U), relaxed by aU (IncompressibleFlow.cpp:176-198)
-void DeviceFlow::assembleMomentum(double aU) {
+void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
     const bool needG = ctrl_.div_scheme == kLinearUpwind || ctrl_.div_scheme == kLUST || G_.nonOrthogonal();
-    if (needG) gradU();
+    if (needG && !haveGradU) gradU();
+    const double* nuF = les_ ? nuF_.get() : nullptr;
     if (nI_ > 0)
         k_mom_faces<<<nblk(nI_), 256, 0, s_>>>(nI_, nC_, nF_, G_.own(), G_.nei(), G_.w(), G_.magSf(), G_.ndc(), G_.d(),
-                                              G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, ctrl_.div_scheme,
+                                              G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, nuF, ctrl_.div_scheme,
                                               G_.nonOrthogonal() ? 1 : 0, gU_.get(), loDiv_.get(), upDiv_.get(),
                                               lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), uValue_.get(), G_.magSf(),
-                                               G_.ndc(), phi_.get(), ctrl_.nu, ic_.get(), bs_.get()), ++launches_;
+                                               G_.ndc(), phi_.get(), ctrl_.nu, nuF, ic_.get(), bs_.get()), ++launches_;
     // ddt coefficients (Schemes.h:70-86)
     double kc = 0, kc0 = 0, kc00 = 0;
     const bool transient = !ctrl_.steady;
@@ -547,6 +551,7 @@ void DeviceFlow::assembleMomentum(double aU) {
                                           lapUp_.get(), cDiv_.get(), ffc_.get(), G_.V(), transient ? 1 : 0, kc, kc0,
                                           kc00, U0_.get(), nOld_ >= 2 ? U00_.get() : U0_.get(), diag_.get(),
                                           src_.get()), ++launches_;
+    if (les_ || forcing_ != 0) explicitSources();
     if (aU < 1.0)
         k_mom_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), upper_.get(),
                                               lower_.get(), ic_.get(), U_.get(), aU, diag_.get(), src_.get()), ++launches_;
@@ -646,10 +651,16 @@ vlm_step_info DeviceFlow::step(double dt) {
     for (int outer = 0; outer < ctrl_.n_outer; ++outer) {
         const bool finalOuter = outer == ctrl_.n_outer - 1;
         const double aU = steady ? ctrl_.alpha_u : (finalOuter ? 1.0 : ctrl_.alpha_u);
-        assembleMomentum(aU);
+        // updateGradU + updateTurbulence at the start of every outer pass (IncompressibleFlow.cpp:176-179)
+        if (les_) {
+            gradU();
+            lesCorrect();
+        }
+        assembleMomentum(aU, les_);
         if (ctrl_.momentum_predictor) solveMomentum(info, outer == 0);
         for (int corr = 0; corr < ctrl_.n_corr; ++corr)
             correctPressure(finalOuter && corr == ctrl_.n_corr - 1, outer == 0 && corr == 0, info);
+        if (forcing_ == 2) forcingCorrection(aU);
     }
     // continuity error: max |div phi| (IncompressibleFlow.cpp:367-370)
     G_.div(phi_.get(), divPhi_.get(), s_);

@@ -15,8 +15,10 @@
 //
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
 // linear / linearUpwind / LUST, Gauss linear gradients, fixedValue and zeroGradient boundary
-// conditions for U and p, empty (2D) directions and cyclic (internal) faces.  Not supported (an
-// UNSUPPORTED status): skewed meshes, turbulence, body forces, momentum forcing, ddtPhiCoeff.
+// conditions for U and p, empty (2D) directions and cyclic (internal) faces, the LES Smagorinsky model
+// with Van Driest damping and constant / mean-velocity momentum forcing (flow_les.cu).  Not supported
+// (an UNSUPPORTED status): skewed meshes, other turbulence models, wall models, buoyancy body forces,
+// ddtPhiCoeff.
 #pragma once
 
 #include <cstdint>
@@ -42,12 +44,21 @@ public:
     void getState(double* U, double* p, double* phi);
     // kernels run by this flow so far (its own, the geometry's and the solves', graph nodes included)
     int64_t launches() const { return total_; }
+    // turbulence model and momentum forcing (flow_les.cu); before the first step
+    void setModel(const vlm_flow_model& model);
+    void modelState(double* nut, double* gradP);
 
 private:
     void boundaryU();
     void boundaryP();
     void gradU();
-    void assembleMomentum(double aU);
+    void assembleMomentum(double aU, bool haveGradU);
+    // TurbulenceModel::correct for the LES model: wall shear, filter width, nu_t, face nu_eff
+    void lesCorrect();
+    // the explicit momentum sources after fvm::laplacian: div(nu_eff dev2(T(grad U))) and the forcing
+    void explicitSources();
+    // IncompressibleFlow::applyForcingCorrection (mean-velocity forcing)
+    void forcingCorrection(double aU);
     void solveMomentum(vlm_step_info& info, bool first);
     void correctPressure(bool finalCorr, bool first, vlm_step_info& info);
 
@@ -86,6 +97,19 @@ private:
     double pNormRef_ = 0;
     int pNormSteps_ = 0;
     bool initialized_ = false;
+
+    // turbulence model and forcing (flow_les.cu)
+    bool les_ = false, vanDriest_ = false, exactSums_ = false;
+    int forcing_ = 0, nWall_ = 0;
+    double CsCs_ = 0, kOverC_ = 0, Aplus_ = 26, nutMax_ = 0;
+    double force_[3] = {0, 0, 0}, Ubar_[3] = {0, 0, 0}, dir_[3] = {0, 0, 0};
+    double magUbar_ = 0, relax_ = 1, totalVolume_ = 0;
+    DBuf<int32_t> wallFace_, wallCell_, nearest_, wallB_;
+    DBuf<double> wallN_, wallY_, uTau_, delta0_, yWall_, nut_, nuEffC_, nuF_, devF_;
+    DBuf<double> forceState_;          // gradP, dU, rAUave
+    DBuf<double> forcePart_;           // per-CTA partial sums (plain)
+    DBuf<long long> forceBins_;        // per-CTA partial sums (exact)
+    DBuf<unsigned long long> forceCount_;
 };
 
 }  // namespace vlm

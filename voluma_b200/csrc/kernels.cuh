@@ -567,43 +567,49 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
         }
     }
     __syncthreads();
-    __shared__ int singular;
-    if (threadIdx.x == 0) singular = 0;
-    __syncthreads();
+    // LU without pivoting, one pivot at a time: multipliers of column k, then the trailing block
+    // element-parallel (each element receives its updates in the order k = 0, 1, ...)
+    const int nt = blockDim.x;
     for (int k = 0; k < n; ++k) {
         const double piv = A[(size_t)k * n + k];
-        if (fabs(piv) < kVSMALL) {
-            if (threadIdx.x == 0) singular = 1;
-            break;
+        if (fabs(piv) < kVSMALL) {  // uniform: every thread reads the same pivot
+            if (threadIdx.x == 0) atomicExch(status, (int)VLM_ERR_SINGULAR);
+            return;
         }
-        for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) {
-            const double fct = A[(size_t)i * n + k] / piv;
-            A[(size_t)i * n + k] = fct;
-            if (fct == 0.0) continue;
-            for (int j = k + 1; j < n; ++j) A[(size_t)i * n + j] -= fct * A[(size_t)k * n + j];
+        for (int i = k + 1 + threadIdx.x; i < n; i += nt) A[(size_t)i * n + k] /= piv;
+        __syncthreads();
+        const int m = n - k - 1;
+        for (int q = threadIdx.x; q < m * m; q += nt) {
+            const int i = k + 1 + q / m, j = k + 1 + q % m;
+            const double fct = A[(size_t)i * n + k];
+            if (fct != 0.0) A[(size_t)i * n + j] -= fct * A[(size_t)k * n + j];
         }
         __syncthreads();
     }
+    // inverse = U^-1 L^-1, all columns at once.  Forward (unit L): X = I, then for k ascending
+    // X[i][j] -= L[i][k] X[k][j] for i > k (X[k][j] = 0 for j > k, so j <= k).
+    for (int q = threadIdx.x; q < n * n; q += nt) X[q] = (q / n == q % n) ? 1.0 : 0.0;
     __syncthreads();
-    if (singular) {
-        if (threadIdx.x == 0) atomicExch(status, (int)VLM_ERR_SINGULAR);
-        return;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1, w = k + 1;
+        for (int q = threadIdx.x; q < m * w; q += nt) {
+            const int i = k + 1 + q / w, j = q % w;
+            X[(size_t)i * n + j] -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
+        }
+        __syncthreads();
     }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        // column j of the inverse: solve L U g = e_j
-        for (int i = 0; i < n; ++i) {
-            double g = i == j ? 1.0 : 0.0;
-            for (int k = 0; k < i; ++k) g -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
-            X[(size_t)i * n + j] = g;
+    // backward (U): for k descending, X[k][:] /= U[k][k], then X[i][j] -= U[i][k] X[k][j] for i < k
+    for (int k = n - 1; k >= 0; --k) {
+        const double ukk = A[(size_t)k * n + k];
+        for (int j = threadIdx.x; j < n; j += nt) X[(size_t)k * n + j] /= ukk;
+        __syncthreads();
+        for (int q = threadIdx.x; q < k * n; q += nt) {
+            const int i = q / n, j = q % n;
+            X[(size_t)i * n + j] -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
         }
-        for (int i = n - 1; i >= 0; --i) {
-            double g = X[(size_t)i * n + j];
-            for (int k = i + 1; k < n; ++k) g -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
-            X[(size_t)i * n + j] = g / A[(size_t)i * n + i];
-        }
+        __syncthreads();
     }
     if (inShared) {
-        __syncthreads();
         for (int q = threadIdx.x; q < n * n; q += blockDim.x) inv[c.invOffset + q] = X[q];
     }
 }
@@ -634,7 +640,7 @@ __global__ void k_coarse_apply(const CoarseDev* __restrict__ cs, const double* _
 constexpr int kTailThreads = 1024;
 constexpr int kTailBatch = 4;      // entries in flight per row (64 registers at 1024 threads)
 constexpr int kTailMaxRows = 1024;  // levels at most this many rows (padded) go to the tail
-constexpr int kTailFullRows = 8192; // systems at most this many level-0 rows run the whole V-cycle there
+constexpr int kTailFullRows = 2048;  // systems at most this many level-0 rows run the whole V-cycle there
 
 template <class T>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* __restrict__ tsys,

@@ -26,6 +26,11 @@ struct DiluDev {
     DBuf<DiluBar> bars;
     DBuf<int> err;
     int G = 1, groups = 0, nFaces = 0;
+    // streamed shared-memory sweeps (dilu.h DiluLevel): used when smem > 0
+    DBuf<DiluLevel> lev;
+    DBuf<int32_t> slotRow, sLoCol, sLoFace, sUpCol, sUpFace;
+    DBuf<double> prod, coefLo, coefUp, rDs;
+    int W = 0, M = 0, nLoS = 0, nUpS = 0;
     size_t smem = 0;   // > 0: shared-memory sweeps with this many bytes per CTA
     int threads = 0;   // their CTA size: the widest level rounded up to whole warps (cheap barriers)
 };
@@ -395,7 +400,7 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
             return true;
         }();
         (void)raised;
-        k_coarse_factor<<<D.coarse.n, 128, smem, s>>>(coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
+        k_coarse_factor<<<D.coarse.n, 512, smem, s>>>(coarse_.get() + D.coarse.off, D.sell(), D.val.get(),
                                                      D.diag.get(), lu_.get(), inv_.get(), status_.get(), smemN);
         VLM_CUDA(cudaGetLastError());
         ++tl_launches;
@@ -777,17 +782,33 @@ void DeviceBatch::ensureDilu() {
     // (the kernels' opt-in limit is a per-function setting shared by every mesh: it is raised once to
     // the ceiling, never to one mesh's size)
     constexpr size_t kDiluSmemMax = 200 * 1024;
-    if (D->G == 1 && P.maxWidth <= kDiluThreads && size_t(P.maxRows) * sizeof(double) <= kDiluSmemMax) {
+    const int W = std::max(1, P.maxWidth), M = std::max(1, P.maxEnt);
+    const size_t streamSmem = dilu_stream_smem(P.maxRows, P.maxLevels, W, M);
+    if (D->G == 1 && P.maxWidth <= kDiluThreads && streamSmem <= kDiluSmemMax) {
         static const bool raised = [] {
-            VLM_CUDA(cudaFuncSetAttribute(k_dilu_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            VLM_CUDA(cudaFuncSetAttribute(k_dilu_factor_stream, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(kDiluSmemMax)));
-            VLM_CUDA(cudaFuncSetAttribute(k_dilu_apply_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            VLM_CUDA(cudaFuncSetAttribute(k_dilu_apply_stream, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(kDiluSmemMax)));
             return true;
         }();
         (void)raised;
-        D->smem = std::max<size_t>(size_t(P.maxRows) * sizeof(double), 8);
+        D->smem = streamSmem;
         D->threads = std::max(32, (P.maxWidth + 31) / 32 * 32);
+        D->W = W;
+        D->M = M;
+        D->lev.upload(P.lev, s);
+        D->slotRow.upload(P.slotRow, s);
+        D->sLoCol.upload(P.sLoCol, s);
+        D->sLoFace.upload(P.sLoFace, s);
+        D->sUpCol.upload(P.sUpCol, s);
+        D->sUpFace.upload(P.sUpFace, s);
+        D->nLoS = int(P.sLoCol.size());
+        D->nUpS = int(P.sUpCol.size());
+        D->prod.resize(size_t(std::max(D->nLoS, 1)));
+        D->coefLo.resize(size_t(std::max(D->nLoS, 1)));
+        D->coefUp.resize(size_t(std::max(D->nUpS, 1)));
+        D->rDs.resize(std::max<size_t>(P.slotRow.size(), 1));
     }
     D->bars.resize(size_t(D->groups));
     D->bars.zero(s);
@@ -818,16 +839,19 @@ void launchLevels(void (*kernel)(Exp...), int groups, int G, cudaStream_t s, Act
 void DeviceBatch::diluFactor(const double* upper, const double* lower) {
     DiluDev& Dd = *dilu_;
     cudaStream_t s = stream_;
-    VLM_LAUNCH(k_dilu_values, nblk(Dd.nFaces), 256, s, Dd.nFaces, (const int32_t*)Dd.loFace.get(),
-               (const int32_t*)Dd.upFace.get(), upper, lower, Dd.loAul.get(), Dd.loAlu.get(), Dd.upAlu.get());
     if (Dd.smem) {
-        k_dilu_factor_smem<<<Dd.groups, Dd.threads, Dd.smem, s>>>(Dd.sys.get(), Dd.levPtr.get(), Dd.levRows.get(),
-                                                                    Dd.loPtr.get(), Dd.loCol.get(), Dd.loAlu.get(),
-                                                                    Dd.loAul.get(), L_[0].diag.get(), Dd.rD.get());
+        VLM_LAUNCH(k_dilu_stream_values, nblk(std::max(1, Dd.nLoS + Dd.nUpS)), 256, s, Dd.nLoS, Dd.nUpS,
+                   (const int32_t*)Dd.sLoCol.get(), (const int32_t*)Dd.sLoFace.get(), (const int32_t*)Dd.sUpCol.get(),
+                   (const int32_t*)Dd.sUpFace.get(), upper, lower, Dd.prod.get(), Dd.coefLo.get(), Dd.coefUp.get());
+        k_dilu_factor_stream<<<Dd.groups, Dd.threads, Dd.smem, s>>>(Dd.sys.get(), Dd.lev.get(), Dd.W, Dd.M,
+                                                                      Dd.slotRow.get(), Dd.sLoCol.get(), Dd.prod.get(),
+                                                                      L_[0].diag.get(), Dd.rDs.get());
         VLM_CUDA(cudaGetLastError());
         ++tl_launches;
         return;
     }
+    VLM_LAUNCH(k_dilu_values, nblk(Dd.nFaces), 256, s, Dd.nFaces, (const int32_t*)Dd.loFace.get(),
+               (const int32_t*)Dd.upFace.get(), upper, lower, Dd.loAul.get(), Dd.loAlu.get(), Dd.upAlu.get());
     launchLevels(k_dilu_factor, Dd.groups, Dd.G, s, (const DiluSys*)Dd.sys.get(), Dd.G, (const int32_t*)Dd.levPtr.get(),
                  (const int32_t*)Dd.levRows.get(), (const int32_t*)Dd.loPtr.get(), (const int32_t*)Dd.loCol.get(),
                  (const double*)Dd.loAlu.get(), (const double*)Dd.loAul.get(), (const double*)L_[0].diag.get(),
@@ -855,9 +879,9 @@ void DeviceBatch::checkLevelError() {
 void DeviceBatch::recordDiluApply(const double* r, double* w) {
     DiluDev& D = *dilu_;
     if (D.smem) {
-        k_dilu_apply_smem<<<D.groups, D.threads, D.smem, stream_>>>(
-            D.sys.get(), D.levPtr.get(), D.levRows.get(), D.loPtr.get(), D.loCol.get(), D.loAul.get(), D.upPtr.get(),
-            D.upCol.get(), D.upAlu.get(), D.rD.get(), r, w, st_.get(), kFlagDone);
+        k_dilu_apply_stream<<<D.groups, D.threads, D.smem, stream_>>>(
+            D.sys.get(), D.lev.get(), D.W, D.M, D.slotRow.get(), D.rDs.get(), D.sLoCol.get(), D.coefLo.get(),
+            D.sUpCol.get(), D.coefUp.get(), r, w, st_.get(), kFlagDone);
         VLM_CUDA(cudaGetLastError());
         ++tl_launches;
         return;
