@@ -18,6 +18,10 @@ diag/upper/b/x and D2H of x inside the timed region).
 --workload serving: a seeded Poisson trace of steady lid-cavity solves through the serving runtime
 (vlm_server_*), mixed-precision vs FP64 pressure, solves/s and p50/p99 latency; --impl reference
 replays the trace through the reference's own incompressible solver in host worker processes.
+
+--workload channel [--channel 256x192x128]: the Re_tau 395 LES channel (Smagorinsky + Van Driest,
+mean-velocity forcing), PIMPLE steps/s with mixed vs FP64 pressure; --impl reference times the
+reference's own LES step on a 96x72x48 sample and scales it by cells.
 """
 from __future__ import annotations
 
@@ -340,6 +344,142 @@ def run_serving(args, rank, world, local):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------------ channel LES workload
+CHAN_METRIC = "channel Re_tau 395 LES: PIMPLE steps/s (Smagorinsky + Van Driest, mean-velocity forcing)"
+CHAN_REF_SAMPLE = (96, 72, 48)
+
+
+def chan_shape(args):
+    return tuple(int(v) for v in args.channel.split("x"))
+
+
+def chan_config(args, world, n):
+    return {"workload": f"periodic channel 2pi x 2 x pi, {n[0]}x{n[1]}x{n[2]} hex ({n[0] * n[1] * n[2]} cells), "
+                        f"tanh wall grading (first cell y+ ~ 1 at Re_tau 395), nu = 1/6875 (Re_b 6875), "
+                        f"mean-velocity forcing to Ubar = (1,0,0), Smagorinsky LES with Van Driest damping, "
+                        f"PIMPLE backward/linear nOuter 1 nCorr 2, U PBiCGStab/DILU 1e-8, p PCG/GAMG 1e-8 "
+                        f"(relTol 0.01, final 0); laminar profile + 10% seeded noise, dt at Courant ~0.5",
+            "cells": n[0] * n[1] * n[2], "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (the 6.3M-cell step touches ~GBs)"}
+
+
+def _chan_ref_step_time(n, steps):
+    """Seconds per step of the reference's own LES channel step (IncompressibleFlow + TurbulenceModel,
+    single-threaded) on an n-cell channel, excluding the first step."""
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    from voluma_b200 import cases
+    m, case, model, U0, dt = cases.channel(n)
+    beta = cases.channel_beta(n[1], 1.0 / 395.0)
+    R = ref.RefMesh(n, hi=(2 * np.pi, 2.0, np.pi), periodic=(1, 0, 1), beta=(0, beta, 0),
+                    patch_types=[0, 0, 1, 1, 0, 0])
+    t0 = time.perf_counter()
+    R.flow_run(case, 1, dt=dt, U=U0, model=model)
+    t1 = time.perf_counter()
+    R.flow_run(case, 1 + steps, dt=dt, U=U0, model=model)
+    t2 = time.perf_counter()
+    return ((t2 - t1) - (t1 - t0)) / steps
+
+
+def run_channel_reference(args, rank, world):
+    """The reference's LES step timed on a bounded sample (a 96x72x48 channel, the same case), scaled to the
+    configured channel by cells: steps/s = (cell-steps/s of the sample) / cells."""
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvlmref.so was not built (make -C oracle)"}))
+        return
+    n = chan_shape(args)
+    cells = n[0] * n[1] * n[2]
+    ns = CHAN_REF_SAMPLE
+    per = _chan_ref_step_time(ns, 2)
+    value = (ns[0] * ns[1] * ns[2] / per) / cells
+    sample = f"2 LES channel steps on {ns[0]}x{ns[1]}x{ns[2]} cells (after one untimed step), 1 thread, scaled by cells"
+    line = {"metric": CHAN_METRIC, "impl": "reference", "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": 2, "warmup": 1, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": chan_config(args, 1, n),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_channel(args, rank, world, local):
+    import torch
+    import voluma_b200 as vb
+    from voluma_b200 import cases
+    torch.cuda.set_device(local)
+    n = chan_shape(args)
+    m, case0, model, U0, dt = cases.channel(n, seed=20261203 + rank)
+    mesh = vb.Mesh.from_arrays(m, ctx=vb.Context(local))
+    st = torch.cuda.ExternalStream(mesh.ctx.stream())
+    modes = {}
+    sampler = ClockSampler(local)
+    clocks = None
+    for prec in ("mixed", "fp64"):
+        case = dict(case0, p=dict(case0["p"], precision=prec), pFinal=dict(case0["pFinal"], precision=prec))
+        fl = vb.Flow(mesh, case)
+        fl.set_model(model)
+        fl.set_state(U0, None)
+        for _ in range(args.warmup):
+            fl.step(dt)
+        l0 = fl.launches()
+        if prec == "mixed":
+            sampler.start()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its = 0
+        for _ in range(args.steps):
+            its += fl.step(dt)["iterations"]
+        e1.record(st)
+        torch.cuda.synchronize(local)
+        dev_s = e0.elapsed_time(e1) / 1e3
+        launches = fl.launches() - l0
+        # end to end: every step also reads U and p back to the host
+        t = time.perf_counter()
+        for _ in range(max(2, args.steps // 2)):
+            fl.step(dt)
+            fl.state()
+        e2e_s = (time.perf_counter() - t) / max(2, args.steps // 2)
+        if prec == "mixed":
+            clocks = sampler.stop()
+        fl.close()
+        if world > 1:
+            tt = torch.tensor([dev_s], device=torch.device("cuda", local), dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            dev_s = float(tt.item())
+        modes[prec] = dict(value=world * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
+                           iterations_per_step=its / args.steps, e2e_steps_per_s=world / e2e_s,
+                           gpu_launches=int(launches))
+    if rank != 0:
+        return
+    mx = modes["mixed"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            ns = CHAN_REF_SAMPLE
+            per = _chan_ref_step_time(ns, 2)
+            cpu = {"value": (ns[0] * ns[1] * ns[2] / per) / (n[0] * n[1] * n[2]), "unit": "steps/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"2 LES channel steps on {ns[0]}x{ns[1]}x{ns[2]} cells, 1 thread, scaled by cells"}
+    nC = n[0] * n[1] * n[2]
+    line = {"metric": CHAN_METRIC, "value": mx["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (pressure V-cycle f32 in mixed)", "data": "synthetic",
+            "config": chan_config(args, world, n),
+            "modes": {"mixed": mx, "fp64": modes["fp64"],
+                      "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"]},
+            "e2e": {"value": mx["e2e_steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * 4 * nC,
+                    "note": "vlm_flow_step plus vlm_flow_get_state of U and p every step; the state stays resident"},
+            "roofline": None, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": mx["gpu_launches"]}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------------------ our arm
 METRIC = "solves/s & p99 latency at rtol 1e-8, mixed vs FP64 GAMG-PCG on 1 B200"
 
@@ -503,7 +643,8 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--smoother", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving"])
+    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving", "channel"])
+    ap.add_argument("--channel", default="256x192x128")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--nmin", type=int, default=32)
@@ -517,7 +658,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        (run_serving_reference if args.workload == "serving" else run_reference)(args, rank, world)
+        {"serving": run_serving_reference, "channel": run_channel_reference}.get(args.workload, run_reference)(
+            args, rank, world)
         return
     if world > 1:
         import datetime
@@ -526,7 +668,7 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        (run_serving if args.workload == "serving" else run_ours)(args, rank, world, local)
+        {"serving": run_serving, "channel": run_channel}.get(args.workload, run_ours)(args, rank, world, local)
     finally:
         if world > 1:
             import torch
