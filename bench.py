@@ -19,6 +19,10 @@ diag/upper/b/x and D2H of x inside the timed region).
 (vlm_server_*), mixed-precision vs FP64 pressure, solves/s and p50/p99 latency; --impl reference
 replays the trace through the reference's own incompressible solver in host worker processes.
 
+--workload batch [--systems 256]: config 3, a batch of uneven graded, jittered Poisson systems solved
+in one batched pressure corrector (nNonOrthCorr 2, FP32 V-cycles in FP64 PCG), systems/s; the
+reference arm times the reference's pressure loop on the batch's first --ref-systems systems.
+
 --workload channel [--channel 256x192x128]: the Re_tau 395 LES channel (Smagorinsky + Van Driest,
 mean-velocity forcing), PIMPLE steps/s with mixed vs FP64 pressure; --impl reference times the
 reference's own LES step on a 96x72x48 sample and scales it by cells.
@@ -480,6 +484,189 @@ def run_channel(args, rank, world, local):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------------ batch workload (config 3)
+BATCH_METRIC = ("batch of Poisson systems: systems solved/s (laplacian with LS non-orthogonal correction, "
+                "nNonOrthCorr 2, PCG+GAMG relTol 1e-8, FP32 V-cycles in FP64 PCG)")
+BATCH_SEED = 20261203
+BATCH_NON_ORTH = 2
+
+
+def batch_params(args, rank=0):
+    from voluma_b200 import cases
+    return cases.poisson_batch_params(args.systems, 16, 96, seed=BATCH_SEED + rank, jitter=0.2, ratio_max=8.0)
+
+
+def batch_config(args, world, cells):
+    return {"workload": f"{args.systems} pressure Poisson systems (projectDivergenceFree): box meshes n^3, n uniform "
+                        f"in [16, 96], tanh grading ratio U[1, 8], interior vertices jittered U(+-0.2h), Neumann "
+                        f"walls + reference cell 0, RHS = div of 16 seeded Fourier modes (|k| <= 4, N(0,1)/|k|^2); "
+                        f"laplacian(1, p) with least-squares non-orthogonal correction, nNonOrthCorr "
+                        f"{BATCH_NON_ORTH}, PCG+GAMG relTol 1e-8 from p = 0; seed {BATCH_SEED}",
+            "systems": args.systems, "cells": int(cells), "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (the batch holds ~1e8 cells)"}
+
+
+def _batch_ref_worker(q):
+    """One system through the reference's own pressure loop (laplacian + setReference + solveLdu,
+    nNonOrthCorr + 1 passes), single-threaded: (seconds, cells)."""
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    from voluma_b200 import cases
+    from voluma_b200 import mesh as vm
+    m, div = cases.poisson_system(q)
+    n = q["n"]
+    beta = math.acosh(math.sqrt(q["ratio"])) if q["ratio"] > 1.0 + 1e-12 else 0.0
+    pts = vm.jitter_interior(vm.box_points((n, n, n), beta=(beta, beta, beta)), (n, n, n), q["jitter"], q["mesh_seed"])
+    R = ref.RefMesh((n, n, n), beta=(beta, beta, beta), points=pts)
+    t = time.perf_counter()
+    R.pressure_solve(np.ones(m["n_faces"]), div, np.zeros(m["n_cells"]), ref_cell=0, n_non_orth=BATCH_NON_ORTH,
+                     grad_scheme=1, rel_tol=1e-8, max_iter=1000)
+    return time.perf_counter() - t, m["n_cells"]
+
+
+def batch_reference_sample(args):
+    """The reference on a bounded sample of the batch: its first `--ref-systems` systems, one
+    single-threaded worker process per system (up to 16 concurrently); returns (systems/s at the
+    batch's mean system size, cores, sample text)."""
+    import multiprocessing as mp
+    params = batch_params(args)
+    sample = params[:args.ref_systems]
+    P = max(1, min(os.cpu_count() or 1, 16, len(sample)))
+    t = time.perf_counter()
+    with mp.get_context("spawn").Pool(P) as pool:
+        res = pool.map(_batch_ref_worker, sample, chunksize=1)
+    wall = time.perf_counter() - t  # includes mesh generation in the workers: conservative
+    solve_cells = sum(c for _, c in res)
+    mean_cells = float(np.mean([q["n"] ** 3 for q in params]))
+    busy = sum(d for d, _ in res)
+    value = (solve_cells / busy) * P / mean_cells
+    text = (f"the batch's first {len(sample)} systems ({solve_cells} cells), reference pressure loop per system in "
+            f"{P} single-threaded processes; systems/s = cells solved per busy core-second x {P} cores / mean cells "
+            f"per system of the full batch ({mean_cells:.0f}); wall {wall:.1f} s")
+    return value, P, text
+
+
+def run_batch_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvlmref.so was not built (make -C oracle)"}))
+        return
+    value, P, text = batch_reference_sample(args)
+    cells = sum(q["n"] ** 3 for q in batch_params(args))
+    line = {"metric": BATCH_METRIC, "impl": "reference", "value": value, "unit": "systems/s", "n_gpus": args.gpus,
+            "steps": args.ref_systems, "warmup": 0, "ms_per_step": 1e3 * args.systems / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": batch_config(args, 1, cells),
+            "cpu_baseline": {"value": value, "unit": "systems/s", "cores": P, "kind": "reference", "sample": text},
+            "e2e": {"value": value, "unit": "systems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_batch(args, rank, world, local):
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    import voluma_b200 as vb
+    from voluma_b200 import cases
+    params = batch_params(args, rank)
+    keep = ("n_cells", "n_internal_faces", "n_faces", "owner", "neighbour", "magSf", "ndc", "V", "Sf", "d", "w",
+            "corrVecs", "patch_start", "patch_size", "two_d", "empty_dir")
+
+    def gen(q):  # only the arrays the registration reads: the batch's host copy stays ~half the size
+        m, d = cases.poisson_system(q)
+        return {k: m[k] for k in keep if k in m}, d
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max(1, min(32, os.cpu_count() or 1))) as ex:
+        systems = list(ex.map(gen, params))
+    t_gen = time.perf_counter() - t0
+    meshes = [m for m, _ in systems]
+    torch.cuda.set_device(local)
+    ctx = vb.Context(local)
+    t0 = time.perf_counter()
+    B = vb.Mesh.batch(meshes, ctx=ctx)
+    t_reg = time.perf_counter() - t0
+    gamma_h = cases.batch_face_array(meshes, [np.ones(m["n_faces"]) for m in meshes])
+    div_h = np.concatenate([d for _, d in systems])
+    del systems
+    dev = torch.device("cuda", local)
+    st = torch.cuda.ExternalStream(ctx.stream())
+    with torch.cuda.stream(st):
+        gamma = torch.from_numpy(gamma_h).to(dev)
+        div = torch.from_numpy(div_h).to(dev)
+        p = torch.zeros(B.n_cells, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(local)
+    refs = [0] * len(meshes)
+    modes = {}
+    sampler = ClockSampler(local)
+    clocks = None
+    for prec in ("mixed", "fp64"):
+        ctrl = vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000, precision="" if prec == "fp64" else prec)
+
+        def one():
+            with torch.cuda.stream(st):
+                p.zero_()
+            return vb.pressure_solve_device(B, gamma.data_ptr(), div.data_ptr(), p.data_ptr(), ctrl, ref_cell=refs,
+                                            n_non_orth=BATCH_NON_ORTH, grad_scheme=1)
+        for _ in range(args.warmup):
+            perf = one()
+        its = [[r.iterations for r in row] for row in perf]
+        if prec == "mixed":
+            sampler.start()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            perf = one()
+        e1.record(st)
+        torch.cuda.synchronize(local)
+        dev_s = e0.elapsed_time(e1) / 1e3
+        ok = all(r.converged for row in perf for r in row)
+        if prec == "mixed":
+            clocks = sampler.stop()
+        if world > 1:
+            tt = torch.tensor([dev_s], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            dev_s = float(tt.item())
+        modes[prec] = dict(value=world * args.systems * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
+                           all_converged=bool(ok), iterations_max=int(max(max(r) for r in its)),
+                           iterations_median=int(np.median([x for r in its for x in r])))
+    # end to end through the host-pointer corrector (H2D gamma, div, p; D2H p and the face flux)
+    ctrl = vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000, precision="mixed")
+    ph = np.zeros(B.n_cells)
+    t = time.perf_counter()
+    ne = max(1, args.steps // 2)
+    for _ in range(ne):
+        ph[:] = 0.0
+        vb.pressure_solve(B, gamma_h, div_h, ph, ctrl, ref_cell=refs, n_non_orth=BATCH_NON_ORTH, grad_scheme=1)
+    e2e = world * args.systems * ne / (time.perf_counter() - t)
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            v, P, text = batch_reference_sample(args)
+            cpu = {"value": v, "unit": "systems/s", "cores": P, "kind": "reference", "sample": text}
+    mx = modes["mixed"]
+    nC, nF = B.n_cells, B.n_faces
+    line = {"metric": BATCH_METRIC, "value": mx["value"], "unit": "systems/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic",
+            "config": batch_config(args, world, nC),
+            "modes": {"mixed": mx, "fp64": modes["fp64"],
+                      "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"]},
+            "setup_s": {"generate": t_gen, "register": t_reg},
+            "e2e": {"value": e2e, "unit": "systems/s", "h2d_bytes_per_step": int(8 * (nF + 2 * nC)),
+                    "d2h_bytes_per_step": int(8 * (nC + nF)),
+                    "note": "vlm_pressure_solve_batch with host arrays: H2D gamma, divPhi, p; D2H p and flux"},
+            "roofline": None, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": None}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------------------ our arm
 METRIC = "solves/s & p99 latency at rtol 1e-8, mixed vs FP64 GAMG-PCG on 1 B200"
 
@@ -643,7 +830,9 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--smoother", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving", "channel"])
+    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving", "channel", "batch"])
+    ap.add_argument("--systems", type=int, default=256)
+    ap.add_argument("--ref-systems", type=int, default=16)
     ap.add_argument("--channel", default="256x192x128")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=4.0)
@@ -658,7 +847,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        {"serving": run_serving_reference, "channel": run_channel_reference}.get(args.workload, run_reference)(
+        {"serving": run_serving_reference, "channel": run_channel_reference,
+         "batch": run_batch_reference}.get(args.workload, run_reference)(
             args, rank, world)
         return
     if world > 1:
@@ -668,7 +858,8 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        {"serving": run_serving, "channel": run_channel}.get(args.workload, run_ours)(args, rank, world, local)
+        {"serving": run_serving, "channel": run_channel, "batch": run_batch}.get(args.workload, run_ours)(
+            args, rank, world, local)
     finally:
         if world > 1:
             import torch

@@ -406,6 +406,26 @@ def pressure_solve(mesh: Mesh, gamma, div_phi, p, ctrl: SolverControls, final_ct
     return ([r[0] for r in rows] if ns == 1 else rows), flux
 
 
+def pressure_solve_device(mesh: Mesh, gamma_ptr: int, div_ptr: int, p_ptr: int, ctrl: SolverControls,
+                          final_ctrl: SolverControls | None = None, ref_cell=0, n_non_orth=0, grad_scheme=1,
+                          flux_ptr: int | None = None):
+    """pressure_solve on device pointers (gamma, div_phi, p, flux: device addresses of float64 arrays in
+    the batch layout, ordered on the mesh context's stream); zeroGradient on every patch."""
+    t, v = _bc(mesh, None, None)
+    ns = mesh.n_systems
+    refs = np.full(ns, -1, np.int32)
+    if ref_cell is not None:
+        refs[:] = np.asarray(ref_cell, np.int32)
+    perf = (_ffi.SolverPerf * ((n_non_orth + 1) * ns))()
+    c = ctrl.to_c()
+    cf = (final_ctrl or ctrl).to_c()
+    check(load().vlm_pressure_solve_batch(mesh.ctx.handle, mesh.handle, C.c_void_p(gamma_ptr), C.c_void_p(div_ptr),
+                                          C.c_void_p(p_ptr), _ptr(t), _ptr(v), _ptr(refs), 0.0, int(n_non_orth),
+                                          int(grad_scheme), C.byref(c), C.byref(cf), perf,
+                                          None if flux_ptr is None else C.c_void_p(flux_ptr), 1), mesh.ctx.handle)
+    return [[SolverPerformance.from_c(perf[q * ns + s]) for s in range(ns)] for q in range(n_non_orth + 1)]
+
+
 def exact_sum(values, ctx: Context | None = None) -> float:
     """Order-independent exact sum on the device (par::ExactSum semantics, Comm.h:42-93)."""
     ctx = ctx or default_context()

@@ -93,18 +93,30 @@ def graded_jittered_box(n, ratio, jitter, seed):
     return vm.box_mesh((n, n, n), points=pts)
 
 
+def poisson_batch_params(n_systems=256, n_min=16, n_max=96, seed=20261203, jitter=0.2, ratio_max=8.0):
+    """The seeded draws of poisson_batch, one dict per system (n, ratio, jitter, mesh seed, field seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_systems):
+        n = int(rng.integers(n_min, n_max + 1))
+        ratio = float(rng.uniform(1.0, ratio_max))
+        mesh_seed = int(rng.integers(1 << 30))
+        field_seed = int(rng.integers(1 << 30))
+        out.append(dict(n=n, ratio=ratio, jitter=jitter, mesh_seed=mesh_seed, field_seed=field_seed))
+    return out
+
+
+def poisson_system(q):
+    """(mesh, div_phi) of one poisson_batch_params entry."""
+    m = graded_jittered_box(q["n"], q["ratio"], q["jitter"], q["mesh_seed"])
+    u_f = fourier_velocity(m["Cf"], q["field_seed"])
+    return m, div_per_volume(m, face_flux(m, u_f))
+
+
 def poisson_batch(n_systems=256, n_min=16, n_max=96, seed=20261203, jitter=0.2, ratio_max=8.0):
     """List of (mesh, div_phi) pairs: the pressure Poisson systems of projectDivergenceFree on
     graded, jittered boxes of uneven sizes."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for s in range(n_systems):
-        n = int(rng.integers(n_min, n_max + 1))
-        ratio = float(rng.uniform(1.0, ratio_max))
-        m = graded_jittered_box(n, ratio, jitter, int(rng.integers(1 << 30)))
-        u_f = fourier_velocity(m["Cf"], int(rng.integers(1 << 30)))
-        out.append((m, div_per_volume(m, face_flux(m, u_f))))
-    return out
+    return [poisson_system(q) for q in poisson_batch_params(n_systems, n_min, n_max, seed, jitter, ratio_max)]
 
 
 def batch_face_array(meshes, per_mesh):

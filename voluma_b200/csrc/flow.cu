@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace vlm {
@@ -457,7 +458,17 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     const int maxSolves = ctrl_.n_outer * (3 + ctrl_.n_corr * (ctrl_.n_non_orth_corr + 1));
     solveState_.resize(size_t(maxSolves));
     solveStatus_.resize(size_t(2) * maxSolves);
+    VLM_CUDA(cudaHostAlloc(&pinned_, sizeof(double) + sizeof(SysState) * maxSolves + sizeof(int) * 2 * maxSolves,
+                           cudaHostAllocDefault));
     for (DBuf<double>* b : {&U_, &U0_, &U00_, &p_, &phi_, &pffc_}) b->zero(s_);
+    // VLM_FLOW_GRAPH=0: every step enqueued kernel by kernel (the captured steps' default is on)
+    const char* fg = std::getenv("VLM_FLOW_GRAPH");
+    graphOn_ = !(fg && fg[0] == '0');
+}
+
+DeviceFlow::~DeviceFlow() {
+    stepGraphs_.clear();
+    if (pinned_) cudaFreeHost(pinned_);
 }
 
 // Next record slot of this step; the solve writes its SysState and status words there.
@@ -621,33 +632,24 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     VLM_CUDA(cudaGetLastError());
 }
 
-vlm_step_info DeviceFlow::step(double dt) {
-    if (!initialized_) setState(nullptr, nullptr);
+// The device work of one step (everything the host enqueues between the time-state update and the
+// read-back of the step's records); records its bookkeeping in nSolves_, uSolves_, pSolve_,
+// solveLaunches_.
+void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
     vlm_step_info info;
     std::memset(&info, 0, sizeof info);
     const bool steady = ctrl_.steady != 0;
-    if (!steady) {
-        VLM_REQUIRE(dt > 0, VLM_ERR_BAD_ARG, "dt must be positive");
-        dt0_ = timeIndex_ > 0 ? dt_ : -1.0;
-        dt_ = dt;
-        time_ += dt;
-        ++timeIndex_;
-        // VolField::storeOld (VolField.h:114-118)
-        if (nOld_ >= 1)
-            VLM_CUDA(cudaMemcpyAsync(U00_.get(), U0_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
+    // VolField::storeOld (VolField.h:114-118)
+    if (copyOldOld)
+        VLM_CUDA(cudaMemcpyAsync(U00_.get(), U0_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
+    if (copyOld)
         VLM_CUDA(cudaMemcpyAsync(U0_.get(), U_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
-        nOld_ = std::min(nOld_ + 1, 2);
-    } else {
-        time_ += 1.0;
-        ++timeIndex_;
-    }
     boundaryU();
     boundaryP();
     nSolves_ = 0;
     uSolves_.clear();
     solveLaunches_.clear();
     pSolve_ = -1;
-    const int64_t own0 = launches_, geom0 = G_.launches();
     for (int outer = 0; outer < ctrl_.n_outer; ++outer) {
         const bool finalOuter = outer == ctrl_.n_outer - 1;
         const double aU = steady ? ctrl_.alpha_u : (finalOuter ? 1.0 : ctrl_.alpha_u);
@@ -666,17 +668,99 @@ vlm_step_info DeviceFlow::step(double dt) {
     G_.div(phi_.get(), divPhi_.get(), s_);
     cont_.zero(s_);
     k_max_abs<<<std::min(nblk(nC_), 1184), 256, 0, s_>>>(nC_, divPhi_.get(), (unsigned long long*)cont_.get()), ++launches_;
-    VLM_CUDA(cudaMemcpyAsync(&info.continuityError, cont_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
-    // the step's solver records, read once
-    std::vector<SysState> st(static_cast<size_t>(nSolves_));
-    std::vector<int> status(static_cast<size_t>(2 * nSolves_));
+}
+
+// One step's device work captured into a graph (the solves' iteration loops embedded as conditional
+// nodes); returns null when the capture is not possible, and the step then runs directly.
+DeviceFlow::StepGraph* DeviceFlow::stepGraph(bool copyOld, bool copyOldOld) {
+    const StepKey key{ctrl_.steady != 0, dt_, dt0_, copyOld, copyOldOld};
+    for (auto& g : stepGraphs_)
+        if (g->key == key) return g.get();
+    auto g = std::make_unique<StepGraph>();
+    g->key = key;
+    const int64_t own0 = launches_, geom0 = G_.launches();
+    VLM_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeRelaxed));
+    batch_.beginEmbedding();
+    try {
+        stepWork(copyOld, copyOldOld);
+    } catch (...) {
+        batch_.endEmbedding();
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(s_, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        cudaGetLastError();
+        graphOn_ = false;
+        return nullptr;
+    }
+    batch_.endEmbedding();
+    VLM_CUDA(cudaStreamEndCapture(s_, &g->graph));
+    VLM_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    g->ownLaunches = (launches_ - own0) + (G_.launches() - geom0);
+    g->nSolves = nSolves_;
+    g->uSolves = uSolves_;
+    g->pSolve = pSolve_;
+    g->solveLaunches = solveLaunches_;
+    stepGraphs_.push_back(std::move(g));
+    return stepGraphs_.back().get();
+}
+
+DeviceFlow::StepGraph::~StepGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+}
+
+vlm_step_info DeviceFlow::step(double dt) {
+    if (!initialized_) setState(nullptr, nullptr);
+    vlm_step_info info;
+    std::memset(&info, 0, sizeof info);
+    const bool steady = ctrl_.steady != 0;
+    bool copyOld = false, copyOldOld = false;
+    if (!steady) {
+        VLM_REQUIRE(dt > 0, VLM_ERR_BAD_ARG, "dt must be positive");
+        dt0_ = timeIndex_ > 0 ? dt_ : -1.0;
+        dt_ = dt;
+        time_ += dt;
+        ++timeIndex_;
+        copyOldOld = nOld_ >= 1;
+        copyOld = true;
+        nOld_ = std::min(nOld_ + 1, 2);
+    } else {
+        time_ += 1.0;
+        ++timeIndex_;
+    }
+    // The first step runs directly (it creates every lazily built resource); later steps replay one
+    // captured graph per (steady, dt, old-time-level) configuration: one launch per step.
+    StepGraph* sg = nullptr;
+    if (graphOn_ && stepsRun_ >= 1 && batch_.embeddable()) sg = stepGraph(copyOld, copyOldOld);
+    int64_t stepOwn = 0;
+    if (sg) {
+        VLM_CUDA(cudaGraphLaunch(sg->exec, s_));
+        nSolves_ = sg->nSolves;
+        uSolves_ = sg->uSolves;
+        pSolve_ = sg->pSolve;
+        solveLaunches_ = sg->solveLaunches;
+        stepOwn = sg->ownLaunches;
+    } else {
+        const int64_t own0 = launches_, geom0 = G_.launches();
+        stepWork(copyOld, copyOldOld);
+        stepOwn = (launches_ - own0) + (G_.launches() - geom0);
+    }
+    ++stepsRun_;
+    // the step's continuity error and solver records, read once into pinned memory (a copy into
+    // pageable memory would block in the driver until the stream drains, serialising concurrent flows)
+    double* hCont = reinterpret_cast<double*>(pinned_);
+    SysState* hSt = reinterpret_cast<SysState*>(hCont + 1);
+    int* hStatus = reinterpret_cast<int*>(hSt + solveState_.size());
+    VLM_CUDA(cudaMemcpyAsync(hCont, cont_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
     if (nSolves_ > 0) {
-        VLM_CUDA(cudaMemcpyAsync(st.data(), solveState_.get(), sizeof(SysState) * nSolves_, cudaMemcpyDeviceToHost, s_));
-        VLM_CUDA(cudaMemcpyAsync(status.data(), solveStatus_.get(), sizeof(int) * 2 * nSolves_, cudaMemcpyDeviceToHost,
-                                 s_));
+        VLM_CUDA(cudaMemcpyAsync(hSt, solveState_.get(), sizeof(SysState) * nSolves_, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaMemcpyAsync(hStatus, solveStatus_.get(), sizeof(int) * 2 * nSolves_, cudaMemcpyDeviceToHost, s_));
     }
     VLM_CUDA(cudaStreamSynchronize(s_));
     VLM_CUDA(cudaGetLastError());
+    info.continuityError = *hCont;
+    const std::vector<SysState> st(hSt, hSt + nSolves_);
+    const std::vector<int> status(hStatus, hStatus + 2 * nSolves_);
     for (int k = 0; k < nSolves_; ++k) {
         if (status[2 * k + 1] != 0) {
             batch_.clearLevelError();
@@ -685,7 +769,7 @@ vlm_step_info DeviceFlow::step(double dt) {
         if (status[2 * k] == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
         info.iterations += st[k].iterations;
     }
-    int64_t launched = (launches_ - own0) + (G_.launches() - geom0);
+    int64_t launched = stepOwn;
     for (int k = 0; k < nSolves_ && k < int(solveLaunches_.size()); ++k) {
         const auto& c = solveLaunches_[k];
         launched += c.eager + c.pre + int64_t(st[k].iterations) * c.body;

@@ -22,6 +22,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "assembly.h"
@@ -35,6 +36,9 @@ public:
     // uType/pType: per patch 0 zeroGradient, 1 fixedValue; uValue 3 per patch, pValue 1 per patch.
     DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl& ctrl, const int32_t* uType,
                const double* uValue, const int32_t* pType, const double* pValue, cudaStream_t stream);
+    ~DeviceFlow();
+    DeviceFlow(const DeviceFlow&) = delete;
+    DeviceFlow& operator=(const DeviceFlow&) = delete;
 
     // IncompressibleFlow::initialize (IncompressibleFlow.cpp:32-40) from host fields (U: 3 per cell)
     void setState(const double* U, const double* p);
@@ -61,6 +65,36 @@ private:
     void forcingCorrection(double aU);
     void solveMomentum(vlm_step_info& info, bool first);
     void correctPressure(bool finalCorr, bool first, vlm_step_info& info);
+    void stepWork(bool copyOld, bool copyOldOld);
+
+    // captured steps: one graph per (steady, dt, dt0, old-time copies) configuration
+    struct StepKey {
+        bool steady;
+        double dt, dt0;
+        bool copyOld, copyOldOld;
+        bool operator==(const StepKey& o) const {
+            return steady == o.steady && dt == o.dt && dt0 == o.dt0 && copyOld == o.copyOld &&
+                   copyOldOld == o.copyOldOld;
+        }
+    };
+    struct StepGraph {
+        StepKey key{};
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int64_t ownLaunches = 0;
+        int nSolves = 0, pSolve = -1;
+        std::vector<int> uSolves;
+        std::vector<DeviceBatch::LaunchCount> solveLaunches;
+        StepGraph() = default;
+        StepGraph(const StepGraph&) = delete;
+        StepGraph& operator=(const StepGraph&) = delete;
+        ~StepGraph();
+    };
+    StepGraph* stepGraph(bool copyOld, bool copyOldOld);
+    std::vector<std::unique_ptr<StepGraph>> stepGraphs_;
+    bool graphOn_ = true;
+    int64_t stepsRun_ = 0;
+    void* pinned_ = nullptr;  // per-step read-back: continuity error, solver records, status words
 
     DeviceBatch& batch_;
     DeviceGeom& G_;

@@ -2,8 +2,12 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 namespace vlm {
 
@@ -63,10 +67,35 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
         throw std::invalid_argument("batch exceeds 2^31 cells/faces");
 
     std::vector<Hierarchy> Hin(ns);
-    for (int s = 0; s < ns; ++s) {
-        const SysTopo& t = systems[s];
-        if (t.nCells <= 0) throw std::invalid_argument("system with no cells");
-        Hin[s] = buildHierarchy(t.nCells, t.nInternal, t.own, t.nei, t.magSf, t.ndc, mergeLevels);
+    for (int s = 0; s < ns; ++s)
+        if (systems[s].nCells <= 0) throw std::invalid_argument("system with no cells");
+    // the systems' hierarchies are independent: built by a pool of host threads, each taking the
+    // next system (largest first keeps the pool busy to the end)
+    {
+        std::vector<int> byCells(ns);
+        std::iota(byCells.begin(), byCells.end(), 0);
+        std::stable_sort(byCells.begin(), byCells.end(),
+                         [&](int a, int b) { return systems[a].nCells > systems[b].nCells; });
+        std::atomic<int> next{0};
+        std::exception_ptr err;
+        std::mutex errMutex;
+        auto work = [&] {
+            for (int q = next++; q < ns; q = next++) {
+                const SysTopo& t = systems[byCells[q]];
+                try {
+                    Hin[byCells[q]] = buildHierarchy(t.nCells, t.nInternal, t.own, t.nei, t.magSf, t.ndc, mergeLevels);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lock(errMutex);
+                    if (!err) err = std::current_exception();
+                }
+            }
+        };
+        const int nt = std::max(1, std::min(ns, int(std::min(32u, std::max(1u, std::thread::hardware_concurrency())))));
+        std::vector<std::thread> pool;
+        for (int k = 1; k < nt; ++k) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        if (err) std::rethrow_exception(err);
     }
     P.order.resize(ns);
     std::iota(P.order.begin(), P.order.end(), 0);

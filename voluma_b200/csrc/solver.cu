@@ -278,7 +278,32 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     VLM_CUDA(cudaStreamSynchronize(stream_));
 }
 
-DeviceBatch::~DeviceBatch() { graphs_.clear(); }
+DeviceBatch::~DeviceBatch() {
+    graphs_.clear();
+    if (side_) cudaStreamDestroy(side_);
+}
+
+// Temporarily points the batch's recording stream elsewhere (every record function launches on
+// stream_): used to capture graph bodies on the side stream while stream_ is being captured.
+struct StreamSwap {
+    DeviceBatch* b;
+    cudaStream_t old;
+    StreamSwap(DeviceBatch* batch, cudaStream_t s) : b(batch), old(batch->stream_) { b->stream_ = s; }
+    ~StreamSwap() { b->stream_ = old; }
+};
+
+void DeviceBatch::beginEmbedding() {
+    if (!side_) VLM_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    embedding_ = true;
+    tl_capturing = true;
+}
+
+void DeviceBatch::endEmbedding() {
+    embedding_ = false;
+    tl_capturing = false;
+}
+
+bool DeviceBatch::embeddable() const { return useGraphs_ && !(dilu_ && dilu_->G > 1); }
 
 template <class T>
 void DeviceBatch::buildTailTable(DBuf<TailLevel<T>>& out) {
@@ -978,9 +1003,13 @@ cudaGraphNode_t addWhile(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditiona
 
 void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
     struct CaptureScope {
-        CaptureScope() { tl_capturing = true; }
-        ~CaptureScope() { tl_capturing = false; }
+        bool was;
+        CaptureScope() : was(tl_capturing) { tl_capturing = true; }
+        ~CaptureScope() { tl_capturing = was; }
     } scope;
+    // while stream_ is itself being captured, the solve's graph is recorded on the side stream
+    std::unique_ptr<StreamSwap> swap;
+    if (embedding_) swap = std::make_unique<StreamSwap>(this, side_);
     VLM_CUDA(cudaGraphCreate(&G.graph, 0));
     cudaStream_t s = stream_;
     const int64_t saved = tl_launches;
@@ -1037,6 +1066,38 @@ void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
     }
     tl_launches = saved;
     VLM_CUDA(cudaGraphInstantiate(&G.exec, G.graph, 0));
+}
+
+// The solve's loop inside the graph the caller is capturing on stream_: the entry kernel that sets
+// the loop condition, a WHILE node after the capture's current dependencies, and the loop body
+// captured into the node's body graph on the side stream (the same nodes buildGraph records).
+void DeviceBatch::embedSolve(const SolveKey& key) {
+    VLM_REQUIRE(key.prec != Precision::MixedDC, VLM_ERR_UNSUPPORTED,
+                "defect-correction solves are not embedded in a captured step");
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    VLM_CUDA(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &cg, &deps, &nd));
+    VLM_REQUIRE(cs == cudaStreamCaptureStatusActive, VLM_ERR_CUDA, "internal: embedding without a capture");
+    cudaGraphConditionalHandle h;
+    VLM_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+    recordSetCond(h, kFlagDone);
+    VLM_CUDA(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t w;
+    VLM_CUDA(cudaGraphAddNode(&w, cg, deps, nd, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    VLM_CUDA(cudaStreamUpdateCaptureDependencies(stream_, &w, 1, cudaStreamSetCaptureDependencies));
+    StreamSwap swap(this, side_);
+    captureInto(side_, body, {}, [&] {
+        recordIter(key);
+        recordSetCond(h, kFlagDone);
+    });
 }
 
 GraphExec& DeviceBatch::graphFor(const SolveKey& key) {
@@ -1146,7 +1207,10 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     GraphExec* Gp = nullptr;
     if (useGraphs_) {
         Gp = &graphFor(key);
-        VLM_CUDA(cudaGraphLaunch(Gp->exec, s));
+        if (embedding_)
+            embedSolve(key);
+        else
+            VLM_CUDA(cudaGraphLaunch(Gp->exec, s));
     } else {
         const int64_t e0 = tl_launches;
         runEager(key, ctrl.maxIter);

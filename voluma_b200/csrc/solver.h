@@ -118,6 +118,13 @@ public:
                       const vlm_solver_ctrl& ctrl);
 
     cudaStream_t stream() const { return stream_; }
+    // While the caller captures the batch's stream into its own graph, solve() adds its iteration loop
+    // to that graph (a conditional WHILE node whose body is captured on a side stream) instead of
+    // launching the solve's graph.  Only valid after every solve key has run once outside a capture.
+    void beginEmbedding();
+    void endEmbedding();
+    // Whether solves can be embedded in a captured graph (graph mode, no cooperative launches).
+    bool embeddable() const;
     size_t deviceBytes() const;
     int64_t launches() const { return launches_; }
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
@@ -146,6 +153,7 @@ private:
     template <bool EXACT> void recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32);
     template <bool EXACT> void recordBicgIterT(PrecondKind pk, SmootherKind sm, bool f32);
     void recordSetCond(cudaGraphConditionalHandle h, int flag);
+    void embedSolve(const SolveKey& key);
     GraphExec& graphFor(const SolveKey& key);
     void buildGraph(const SolveKey& key, GraphExec& g);
     void ensureVectors(bool mixed, bool bicg);
@@ -185,7 +193,10 @@ private:
     DBuf<TailLevel<float>> tail32_;
     int64_t launches_ = 0;
     bool useGraphs_ = true;
+    bool embedding_ = false;
+    cudaStream_t side_ = nullptr;        // captures loop bodies while stream_ is being captured
 
+    friend struct StreamSwap;
 };
 
 // Exact (order-independent) sum of n device doubles, ordered on stream s.
