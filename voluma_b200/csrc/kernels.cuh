@@ -350,8 +350,11 @@ __global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restri
 // x = r / D without reading the row).  MODE 2: first colour of the first post-sweep of a
 // two-colour level; the neighbours (the other colour, not yet swept) get the coarse-grid
 // correction x + xc[agg] (GAMG.cpp:437-438) on the fly, which replaces the separate prolongation.
+// The colour step is bound by the latency of its three dependent loads per row (structure, entries,
+// gathers): the more rows in flight per SM the better.  Batches of 6 entries (one batch for the
+// rows of a hex mesh) fit 32 registers in FP32, so 8 CTAs of 256 threads stay resident.
 template <class T, int MODE = 0>
-__global__ void __launch_bounds__(kRowsPerCta) k_smooth_gs(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 8 : 6) k_smooth_gs(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                            const T* __restrict__ diag, const T* __restrict__ r, T* x,
                                                            const int32_t* __restrict__ agg, const T* __restrict__ xc,
                                                            const SysState* st, int flag) {
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_gs(const Chunk* __restri
         }
         return v;
     };
-    const T s = row_accumulate<true>(S, val, xf, row, r[row]);
+    const T s = row_accumulate<true, T, decltype(xf), 6>(S, val, xf, row, r[row]);
     x[row] = s / diag[row];
 }
 
@@ -463,8 +466,10 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
 
 // Jacobi sweep xo = (r - offdiag*xi)/D.  MODE 0: plain; MODE 1: xi == 0 (first pre-sweep);
 // MODE 2: xi + xc[agg] (the coarse-grid correction, GAMG.cpp:437-438, fused in).
+// FP32: 48 registers, 5 resident CTAs per SM (measured faster than 4 at 56 registers on the coarse
+// levels, whose rows of 11-19 entries take two or three batches); FP64 keeps the compiler's choice.
 template <class T, int MODE>
-__global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
                                                                const T* __restrict__ val, const T* __restrict__ diag,
                                                                const T* __restrict__ r, const T* __restrict__ xi,
                                                                T* __restrict__ xo, T omega,
@@ -501,7 +506,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_smooth_jacobi(const Chunk* __re
 
 // res = r - A x  (GAMG.cpp:387-401: diagonal first, then the faces in order)
 template <class T>
-__global__ void __launch_bounds__(kRowsPerCta) k_residual(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_residual(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                           const T* __restrict__ diag, const T* __restrict__ r,
                                                           const T* __restrict__ x, T* __restrict__ res,
                                                           const SysState* st, int flag) {
