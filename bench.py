@@ -47,6 +47,28 @@ DT = 2e-3
 REL_TOL = 1e-8
 
 
+# ------------------------------------------------------------------------------ replicas (N > 1)
+def max_over_ranks(value, world, device=None):
+    """The largest of one float per rank (a multi-GPU time is the slowest rank's); every rank takes
+    this collective in the same order.  device: the tensor's device (CUDA for NCCL, None for gloo)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def deal(items, rank, world):
+    """Replica sharding: item i goes to rank i mod world (no item twice, none lost)."""
+    return list(items)[rank::world]
+
+
+def aggregate_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of `world` replicas that each processed units_per_rank in (max) seconds."""
+    return world * units_per_rank / seconds
+
+
 # ------------------------------------------------------------------------------ workload
 def tg_velocity(C, seed=1234, n_modes=16, amp=0.1):
     x, y, z = C[:, 0], C[:, 1], C[:, 2]
@@ -282,7 +304,7 @@ def run_serving_reference(args, rank, world):
 def run_serving(args, rank, world, local):
     import voluma_b200 as vb
     from voluma_b200 import cases
-    trace = serve_trace(args)[rank::world]  # replicas: requests dealt round-robin to the ranks
+    trace = deal(serve_trace(args), rank, world)  # replicas: requests dealt round-robin to the ranks
     meshes = {}
     built = []
     for q in trace:
@@ -326,9 +348,8 @@ def run_serving(args, rank, world, local):
                            span_s=span)
     if world > 1:
         import torch
-        t = torch.tensor([modes["mixed"]["span_s"]], device=torch.device("cuda", local), dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        modes["mixed"]["value"] = args.requests / float(t.item())
+        span = max_over_ranks(modes["mixed"]["span_s"], world, torch.device("cuda", local))
+        modes["mixed"]["value"] = args.requests / span
     if rank != 0:
         return
     mx = modes["mixed"]
@@ -447,15 +468,12 @@ def run_channel(args, rank, world, local):
         for _ in range(max(2, args.steps // 2)):
             fl.step(dt)
             fl.state()
-        e2e_s = (time.perf_counter() - t) / max(2, args.steps // 2)
+        e2e_s = max_over_ranks((time.perf_counter() - t) / max(2, args.steps // 2), world, torch.device("cuda", local))
         if prec == "mixed":
             clocks = sampler.stop()
         fl.close()
-        if world > 1:
-            tt = torch.tensor([dev_s], device=torch.device("cuda", local), dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            dev_s = float(tt.item())
-        modes[prec] = dict(value=world * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
+        dev_s = max_over_ranks(dev_s, world, torch.device("cuda", local))
+        modes[prec] = dict(value=aggregate_rate(args.steps, world, dev_s), ms_per_step=1e3 * dev_s / args.steps,
                            iterations_per_step=its / args.steps, e2e_steps_per_s=world / e2e_s,
                            gpu_launches=int(launches))
     if rank != 0:
@@ -626,11 +644,9 @@ def run_batch(args, rank, world, local):
         ok = all(r.converged for row in perf for r in row)
         if prec == "mixed":
             clocks = sampler.stop()
-        if world > 1:
-            tt = torch.tensor([dev_s], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            dev_s = float(tt.item())
-        modes[prec] = dict(value=world * args.systems * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
+        dev_s = max_over_ranks(dev_s, world, dev)
+        modes[prec] = dict(value=aggregate_rate(args.systems * args.steps, world, dev_s),
+                           ms_per_step=1e3 * dev_s / args.steps,
                            all_converged=bool(ok), iterations_max=int(max(max(r) for r in its)),
                            iterations_median=int(np.median([x for r in its for x in r])))
     # end to end through the host-pointer corrector (H2D gamma, div, p; D2H p and the face flux)
@@ -641,7 +657,7 @@ def run_batch(args, rank, world, local):
     for _ in range(ne):
         ph[:] = 0.0
         vb.pressure_solve(B, gamma_h, div_h, ph, ctrl, ref_cell=refs, n_non_orth=BATCH_NON_ORTH, grad_scheme=1)
-    e2e = world * args.systems * ne / (time.perf_counter() - t)
+    e2e = aggregate_rate(args.systems * ne, world, max_over_ranks(time.perf_counter() - t, world, dev))
     if rank != 0:
         return
     cpu = None
@@ -725,11 +741,8 @@ def run_ours(args, rank, world, local):
         launches = mesh.stats()[0] - l0
         ms = np.array([e0.elapsed_time(e1) for e0, e1 in ev])
         tot = float(ms.sum())
-        if world > 1:
-            t = torch.tensor([tot], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            tot = float(t.item())
-        modes[prec] = dict(value=world * args.steps / (tot / 1e3), ms_per_step=tot / args.steps,
+        tot = max_over_ranks(tot, world, dev)
+        modes[prec] = dict(value=aggregate_rate(args.steps, world, tot / 1e3), ms_per_step=tot / args.steps,
                            p50_ms=float(np.percentile(ms, 50)), p99_ms=float(np.percentile(ms, 99)),
                            iterations=int(np.median([p.iterations for p in perfs])),
                            outer=int(np.median([p.outerIterations for p in perfs])),
@@ -760,11 +773,7 @@ def run_ours(args, rank, world, local):
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     barrier()
-    e2e_tot = float(np.sum(e2e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_tot], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_tot = float(t.item())
+    e2e_tot = max_over_ranks(float(np.sum(e2e_ms)), world, dev)
 
     # roofline of the dominant kernel (level-0 multicolour GS sweep of the FP32 inner V-cycle),
     # timed live with CUDA events on the context stream
