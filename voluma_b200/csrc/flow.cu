@@ -472,13 +472,44 @@ DeviceFlow::~DeviceFlow() {
 }
 
 // Next record slot of this step; the solve writes its SysState and status words there.
-int DeviceFlow::solveSlot(bool momentum, bool monitoredP) {
-    const int k = nSolves_++;
-    VLM_REQUIRE(size_t(k) < solveState_.size(), VLM_ERR_CUDA, "internal: solve records exhausted");
-    if (momentum) uSolves_.push_back(k);
+// Next record slot(s) of this step: a solve of `group` systems writes one SysState per system into
+// consecutive slots and its status words into the first slot's.
+int DeviceFlow::solveSlot(bool momentum, bool monitoredP, int group) {
+    const int k = nSolves_;
+    nSolves_ += group;
+    VLM_REQUIRE(size_t(nSolves_) <= solveState_.size(), VLM_ERR_CUDA, "internal: solve records exhausted");
+    for (int j = 0; j < group; ++j) {
+        if (momentum) uSolves_.push_back(k + j);
+        solveGroup_.push_back(j == 0 ? group : 0);
+    }
     if (monitoredP) pSolve_ = k;
-    batch_.deferNextSolve(solveState_.get() + k, solveStatus_.get() + 2 * k);
+    if (group > 1)
+        VLM_CUDA(cudaMemsetAsync(solveStatus_.get() + 2 * (k + 1), 0, sizeof(int) * 2 * (group - 1), s_));
+    (group > 1 ? *uBatch_ : batch_).deferNextSolve(solveState_.get() + k, solveStatus_.get() + 2 * k);
     return k;
+}
+
+// The solved velocity components as one batch (one system per component, the same topology): one
+// set of launches for all components and their level-scheduled sweeps side by side, each system's
+// result the one it would have alone.  Used when every component's sweeps fit one CTA in shared
+// memory; larger meshes keep the component-by-component solves (their sweeps span the GPU).
+bool DeviceFlow::componentBatch() {
+    if (uBatchTried_) return uBatch_ != nullptr;
+    uBatchTried_ = true;
+    const int nc = int(solved_.size());
+    const char* cb = std::getenv("VLM_COMPONENT_BATCH");
+    if (nc < 2 || (cb && cb[0] == '0') || nC_ > 25000 || batch_.topology().size() != 1) return false;
+    auto b = std::make_unique<DeviceBatch>(std::vector<SysTopo>(size_t(nc), batch_.topology()[0]),
+                                           batch_.mergeLevels(), s_);
+    if (!b->levelScheduleInSharedMemory(ctrl_.U)) return false;
+    const size_t N = size_t(nC_), FI = size_t(std::max(nI_, 1));
+    fdU_.resize(nc * N);
+    fbU_.resize(nc * N);
+    upU_.resize(nc * FI);
+    loU_.resize(nc * FI);
+    xU_.resize(nc * N);
+    uBatch_ = std::move(b);
+    return true;
 }
 
 void DeviceFlow::boundaryU() {
@@ -577,12 +608,44 @@ void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
     k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get()), ++launches_;
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
-    for (int k : solved_) {
-        G_.fold(diag_.get(), msrc_.get() + k * N, ic_.get() + k * B, bs_.get() + k * B, fd_.get(), fb_.get(), s_);
+    if (componentBatch()) {
+        const int nc = int(solved_.size());
+        const size_t FI = size_t(std::max(nI_, 1));
+        bool contiguous = true;
+        for (int i = 0; i < nc; ++i) contiguous = contiguous && solved_[i] == solved_[0] + i;
+        for (int i = 0; i < nc; ++i) {
+            const int k = solved_[i];
+            G_.fold(diag_.get(), msrc_.get() + k * N, ic_.get() + k * B, bs_.get() + k * B, fdU_.get() + i * N,
+                    fbU_.get() + i * N, s_);
+            if (nI_ > 0) {
+                VLM_CUDA(cudaMemcpyAsync(upU_.get() + i * FI, upper_.get(), sizeof(double) * nI_,
+                                         cudaMemcpyDeviceToDevice, s_));
+                VLM_CUDA(cudaMemcpyAsync(loU_.get() + i * FI, lower_.get(), sizeof(double) * nI_,
+                                         cudaMemcpyDeviceToDevice, s_));
+            }
+            if (!contiguous)
+                VLM_CUDA(cudaMemcpyAsync(xU_.get() + i * N, U_.get() + k * N, sizeof(double) * N,
+                                         cudaMemcpyDeviceToDevice, s_));
+        }
+        double* x = contiguous ? U_.get() + solved_[0] * N : xU_.get();
         std::vector<vlm_solver_perf> pf;
-        solveSlot(first, false);
-        batch_.solve(fd_.get(), upper_.get(), lower_.get(), fb_.get(), U_.get() + k * N, ctrl_.U, pf);
-        solveLaunches_.push_back(batch_.lastDeferred());
+        solveSlot(first, false, nc);
+        uBatch_->solve(fdU_.get(), upU_.get(), loU_.get(), fbU_.get(), x, ctrl_.U, pf);
+        solveLaunches_.push_back(uBatch_->lastDeferred());
+        for (int i = 1; i < nc; ++i) solveLaunches_.push_back(DeviceBatch::LaunchCount{});
+        if (!contiguous)
+            for (int i = 0; i < nc; ++i)
+                VLM_CUDA(cudaMemcpyAsync(U_.get() + solved_[i] * N, xU_.get() + i * N, sizeof(double) * N,
+                                         cudaMemcpyDeviceToDevice, s_));
+    } else {
+        for (int k : solved_) {
+            G_.fold(diag_.get(), msrc_.get() + k * N, ic_.get() + k * B, bs_.get() + k * B, fd_.get(), fb_.get(),
+                    s_);
+            std::vector<vlm_solver_perf> pf;
+            solveSlot(first, false);
+            batch_.solve(fd_.get(), upper_.get(), lower_.get(), fb_.get(), U_.get() + k * N, ctrl_.U, pf);
+            solveLaunches_.push_back(batch_.lastDeferred());
+        }
     }
     (void)info;
     boundaryU();
@@ -649,6 +712,7 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
     nSolves_ = 0;
     uSolves_.clear();
     solveLaunches_.clear();
+    solveGroup_.clear();
     pSolve_ = -1;
     for (int outer = 0; outer < ctrl_.n_outer; ++outer) {
         const bool finalOuter = outer == ctrl_.n_outer - 1;
@@ -681,10 +745,12 @@ DeviceFlow::StepGraph* DeviceFlow::stepGraph(bool copyOld, bool copyOldOld) {
     const int64_t own0 = launches_, geom0 = G_.launches();
     VLM_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeRelaxed));
     batch_.beginEmbedding();
+    if (uBatch_) uBatch_->beginEmbedding();
     try {
         stepWork(copyOld, copyOldOld);
     } catch (...) {
         batch_.endEmbedding();
+        if (uBatch_) uBatch_->endEmbedding();
         cudaGraph_t junk = nullptr;
         cudaStreamEndCapture(s_, &junk);
         if (junk) cudaGraphDestroy(junk);
@@ -693,6 +759,7 @@ DeviceFlow::StepGraph* DeviceFlow::stepGraph(bool copyOld, bool copyOldOld) {
         return nullptr;
     }
     batch_.endEmbedding();
+    if (uBatch_) uBatch_->endEmbedding();
     VLM_CUDA(cudaStreamEndCapture(s_, &g->graph));
     VLM_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
     g->ownLaunches = (launches_ - own0) + (G_.launches() - geom0);
@@ -700,6 +767,7 @@ DeviceFlow::StepGraph* DeviceFlow::stepGraph(bool copyOld, bool copyOldOld) {
     g->uSolves = uSolves_;
     g->pSolve = pSolve_;
     g->solveLaunches = solveLaunches_;
+    g->solveGroup = solveGroup_;
     stepGraphs_.push_back(std::move(g));
     return stepGraphs_.back().get();
 }
@@ -731,7 +799,8 @@ vlm_step_info DeviceFlow::step(double dt) {
     // The first step runs directly (it creates every lazily built resource); later steps replay one
     // captured graph per (steady, dt, old-time-level) configuration: one launch per step.
     StepGraph* sg = nullptr;
-    if (graphOn_ && stepsRun_ >= 1 && batch_.embeddable()) sg = stepGraph(copyOld, copyOldOld);
+    if (graphOn_ && stepsRun_ >= 1 && batch_.embeddable() && (!uBatch_ || uBatch_->embeddable()))
+        sg = stepGraph(copyOld, copyOldOld);
     int64_t stepOwn = 0;
     if (sg) {
         VLM_CUDA(cudaGraphLaunch(sg->exec, s_));
@@ -739,6 +808,7 @@ vlm_step_info DeviceFlow::step(double dt) {
         uSolves_ = sg->uSolves;
         pSolve_ = sg->pSolve;
         solveLaunches_ = sg->solveLaunches;
+        solveGroup_ = sg->solveGroup;
         stepOwn = sg->ownLaunches;
     } else {
         const int64_t own0 = launches_, geom0 = G_.launches();
@@ -764,6 +834,7 @@ vlm_step_info DeviceFlow::step(double dt) {
     for (int k = 0; k < nSolves_; ++k) {
         if (status[2 * k + 1] != 0) {
             batch_.clearLevelError();
+            if (uBatch_) uBatch_->clearLevelError();
             throw Error(VLM_ERR_TIMEOUT, "level-scheduled sweep: a group barrier wait gave up");
         }
         if (status[2 * k] == VLM_ERR_SINGULAR) throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
@@ -772,7 +843,11 @@ vlm_step_info DeviceFlow::step(double dt) {
     int64_t launched = stepOwn;
     for (int k = 0; k < nSolves_ && k < int(solveLaunches_.size()); ++k) {
         const auto& c = solveLaunches_[k];
-        launched += c.eager + c.pre + int64_t(st[k].iterations) * c.body;
+        // a batched solve loops until its last system is done
+        int its = st[k].iterations;
+        const int g = k < int(solveGroup_.size()) ? solveGroup_[k] : 1;
+        for (int j = 1; j < g && k + j < nSolves_; ++j) its = std::max(its, st[k + j].iterations);
+        launched += c.eager + c.pre + int64_t(its) * c.body;
     }
     info.launches = int32_t(launched);
     total_ += launched;

@@ -85,6 +85,7 @@ private:
         int nSolves = 0, pSolve = -1;
         std::vector<int> uSolves;
         std::vector<DeviceBatch::LaunchCount> solveLaunches;
+        std::vector<int> solveGroup;
         StepGraph() = default;
         StepGraph(const StepGraph&) = delete;
         StepGraph& operator=(const StepGraph&) = delete;
@@ -122,7 +123,13 @@ private:
     int nSolves_ = 0;
     std::vector<int> uSolves_;  // record indices of the first outer pass's momentum solves
     int pSolve_ = -1;           // record index of the monitored pressure solve
-    int solveSlot(bool momentum, bool monitoredP);
+    int solveSlot(bool momentum, bool monitoredP, int group = 1);
+    std::vector<int> solveGroup_;  // per record: systems of the solve that wrote it (0: a later system's)
+    // momentum components solved together: one batch of the mesh once per solved component
+    bool componentBatch();
+    std::unique_ptr<DeviceBatch> uBatch_;
+    bool uBatchTried_ = false;
+    DBuf<double> fdU_, fbU_, upU_, loU_, xU_;
     std::vector<DeviceBatch::LaunchCount> solveLaunches_;  // per record, set after its solve
     int64_t launches_ = 0, total_ = 0;
     // time state (Schemes.h TimeState) and the pressure-residual normalisation of the step

@@ -157,7 +157,7 @@ std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
 
 // ====================================================================== construction
 DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
-    : stream_(stream), topo_(systems) {
+    : stream_(stream), topo_(systems), mergeLevels_(mergeLevels) {
     plan_ = buildPlan(systems, mergeLevels);
     const char* gv = std::getenv("VLM_GRAPH");
     useGraphs_ = !(gv && gv[0] == '0');
@@ -304,6 +304,20 @@ void DeviceBatch::endEmbedding() {
 }
 
 bool DeviceBatch::embeddable() const { return useGraphs_ && !(dilu_ && dilu_->G > 1); }
+
+bool DeviceBatch::levelScheduleInSharedMemory(const vlm_solver_ctrl& ctrl) {
+    PrecondKind pk = parsePrecond(ctrl.preconditioner);
+    SolverKind sk = parseSolver(ctrl.solver);
+    if (ctrl.reproducible) {
+        if (pk != PrecondKind::None) pk = PrecondKind::Diagonal;
+        if (sk == SolverKind::GaussSeidel || sk == SolverKind::SymGaussSeidel) sk = SolverKind::Jacobi;
+    }
+    const bool levels = pk == PrecondKind::DIC || pk == PrecondKind::DILU || sk == SolverKind::GaussSeidel ||
+                        sk == SolverKind::SymGaussSeidel;
+    if (!levels) return true;
+    ensureDilu();
+    return dilu_->smem > 0;
+}
 
 template <class T>
 void DeviceBatch::buildTailTable(DBuf<TailLevel<T>>& out) {

@@ -125,6 +125,11 @@ public:
     void endEmbedding();
     // Whether solves can be embedded in a captured graph (graph mode, no cooperative launches).
     bool embeddable() const;
+    // Whether a solve with these controls keeps every system's level-scheduled sweeps (DIC / DILU /
+    // Gauss-Seidel) in one CTA each (builds the level schedule on first use); true without them.
+    bool levelScheduleInSharedMemory(const vlm_solver_ctrl& ctrl);
+    const std::vector<SysTopo>& topology() const { return topo_; }
+    int mergeLevels() const { return mergeLevels_; }
     size_t deviceBytes() const;
     int64_t launches() const { return launches_; }
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
@@ -183,6 +188,7 @@ private:
     std::vector<int> tailFirst_;
     DBuf<TailSys> tailSys_;
     std::vector<SysTopo> topo_;          // host topology (owned by the caller for the batch's lifetime)
+    int mergeLevels_ = 2;
     std::unique_ptr<DiluDev> dilu_;      // built on the first DIC/DILU/Gauss-Seidel solve
     SysState* deferState_ = nullptr;     // deferNextSolve targets (one-shot)
     LaunchCount lastDeferred_;
