@@ -305,6 +305,16 @@ typedef struct vlm_flow_model {
 } vlm_flow_model;
 
 vlm_status vlm_flow_set_model(vlm_flow* flow, const vlm_flow_model* model);
+
+/* Restart snapshot in the reference's format (restart::write / restart::read, io/Restart.cpp:105-190):
+ * a directory with one binary file per array (U.bin, p.bin, phi.bin, the old time levels U_0 / U_00 /
+ * phi_0 / phi_00 when the flow has them, nut.bin with a turbulence model; each an 8-byte magic
+ * "CFDRST01", the count and the number of components, then the doubles in cell or face order) and
+ * state.txt (time, dt, dt0, timeIndex, nOldTimes, gradP).  Files written by either side are read by
+ * the other.  Set the model (vlm_flow_set_model) before reading; *found is 0 when dir has no
+ * state.txt (nothing read).  A file that does not match the mesh is BAD_ARG. */
+vlm_status vlm_flow_write_restart(vlm_flow* flow, const char* dir);
+vlm_status vlm_flow_read_restart(vlm_flow* flow, const char* dir, int32_t* found);
 /* nu_t per cell (nCells, of the last step's last outer pass) and the mean-velocity driving pressure
  * gradient; either pointer may be NULL. */
 vlm_status vlm_flow_get_model_state(vlm_flow* flow, double* nut, double* grad_p);

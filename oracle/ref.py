@@ -54,6 +54,8 @@ def lib():
         L.ref_flow_run.argtypes = [P, C.POINTER(RefFlowSpec), C.c_int, C.c_double, P, P, P, P, C.POINTER(C.c_int)]
         L.ref_flow_run_model.argtypes = [P, C.POINTER(RefFlowSpec), C.POINTER(RefModelSpec), C.c_int, C.c_double,
                                          P, P, P, P, C.POINTER(C.c_int), P, P]
+        L.ref_flow_run_restart.argtypes = [P, C.POINTER(RefFlowSpec), C.POINTER(RefModelSpec), C.c_char_p,
+                                           C.c_char_p, C.c_int, C.c_double, P, P, P, P, C.POINTER(C.c_int), P, P]
         L.ref_flow_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -166,14 +168,17 @@ class RefMesh:
         return out
 
     # ------------------------------------------------------------------ incompressible step
-    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False, residual_tol=0.0, model=None):
+    def flow_run(self, case, n_steps, dt=1.0, U=None, p=None, reproducible=False, residual_tol=0.0, model=None,
+                 read_restart=None, write_restart=None):
         """n_steps of IncompressibleFlow::step(dt) (solvers/IncompressibleFlow.cpp:138-370) with the case
         settings of `case` (a dict, voluma_b200.cases.lid_cavity layout).  residual_tol > 0 stops at
         convergence like fvmFlow's steady loop.  Returns U (n,3), p, phi, and the per-step history
         [UInitialResidual, pInitialResidual, continuityError, linear iterations] of the steps run.
         `model` (the Flow.set_model dict) adds the reference's turbulence model, built from the equivalent
         "turbulence" case dictionary by TurbulenceModel::create, and the momentum forcing; the run then
-        also returns nu_t per cell and the final forcing gradP."""
+        also returns nu_t per cell and the final forcing gradP.  read_restart / write_restart: directories
+        the run continues from (restart::read) and ends by writing (restart::write); either implies the
+        model form of the return."""
         nC = self.n_cells
         Uc = np.zeros((nC, 3)) if U is None else np.ascontiguousarray(U, np.float64).reshape(nC, 3).copy()
         pc = np.zeros(nC) if p is None else np.ascontiguousarray(p, np.float64).copy()
@@ -194,6 +199,16 @@ class RefMesh:
         sp.reproducible = int(reproducible)
         sp.residualTol = residual_tol
         ran = C.c_int()
+        if read_restart is not None or write_restart is not None:
+            ms, turb = _model_spec(model or {})
+            nut = np.zeros(nC)
+            gp = np.zeros(1)
+            rd = None if read_restart is None else os.fspath(read_restart).encode()
+            wd = None if write_restart is None else os.fspath(write_restart).encode()
+            if lib().ref_flow_run_restart(self._h, C.byref(sp), C.byref(ms), rd, wd, n_steps, dt, _p(Uc), _p(pc),
+                                          _p(phi), _p(hist), C.byref(ran), _p(nut), _p(gp)) != 0:
+                raise RuntimeError(lib().ref_flow_error().decode())
+            return Uc, pc, phi, hist[:ran.value], nut, float(gp[0])
         if model is None:
             if lib().ref_flow_run(self._h, C.byref(sp), n_steps, dt, _p(Uc), _p(pc), _p(phi), _p(hist),
                                   C.byref(ran)) != 0:

@@ -6,6 +6,7 @@
 
 #include "fvm/solvers/IncompressibleFlow.h"
 #include "fvm/core/Json.h"
+#include "fvm/io/Restart.h"
 #include "fvm/models/TurbulenceModel.h"
 #include "fvm/parallel/Comm.h"
 
@@ -61,6 +62,11 @@ struct RefModelSpec {
 
 int ref_flow_run(const RefMesh* r, const RefFlowSpec* spec, int nSteps, double dt, double* U, double* p,
                  double* phi, double* hist, int* stepsRun);
+// ref_flow_run_model that first continues from a restart directory (restart::read, when readDir is
+// not NULL) and ends by writing one (restart::write, when writeDir is not NULL).
+int ref_flow_run_restart(const RefMesh* r, const RefFlowSpec* spec, const RefModelSpec* model, const char* readDir,
+                         const char* writeDir, int nSteps, double dt, double* U, double* p, double* phi, double* hist,
+                         int* stepsRun, double* nut, double* gradP);
 // ref_flow_run with a turbulence model / forcing; also returns nu_t per cell and the final gradP.
 int ref_flow_run_model(const RefMesh* r, const RefFlowSpec* spec, const RefModelSpec* model, int nSteps, double dt,
                        double* U, double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP);
@@ -90,7 +96,8 @@ namespace {
 // Outputs U, p, phi (nFaces) and per step hist[4*k..]: UInitialResidual, pInitialResidual,
 // continuityError, total linear-solver iterations.
 int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, int nSteps, double dt, double* U,
-            double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP) {
+            double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP,
+            const char* readDir = nullptr, const char* writeDir = nullptr) {
     try {
         par::setReproducible(sp->reproducible != 0);
         const Mesh& m = *r->mesh;
@@ -144,6 +151,7 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
             flow.U()[k] = Vec3{U[3 * k], U[3 * k + 1], U[3 * k + 2]};
             flow.p()[k] = p[k];
         }
+        if (readDir && !restart::read(readDir, flow)) throw std::runtime_error("no restart state in " + std::string(readDir));
         int s = 0;
         for (s = 0; s < nSteps; ++s) {
             const StepInfo info = flow.step(dt);
@@ -162,6 +170,7 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
             }
         }
         if (stepsRun) *stepsRun = s;
+        if (writeDir) restart::write(writeDir, flow);
         for (label k = 0; k < nC; ++k) {
             U[3 * k] = flow.U()[k].x;
             U[3 * k + 1] = flow.U()[k].y;
@@ -191,4 +200,10 @@ int ref_flow_run(const RefMesh* r, const RefFlowSpec* sp, int nSteps, double dt,
 int ref_flow_run_model(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, int nSteps, double dt,
                        double* U, double* p, double* phi, double* hist, int* stepsRun, double* nut, double* gradP) {
     return runFlow(r, sp, model, nSteps, dt, U, p, phi, hist, stepsRun, nut, gradP);
+}
+
+int ref_flow_run_restart(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, const char* readDir,
+                         const char* writeDir, int nSteps, double dt, double* U, double* p, double* phi, double* hist,
+                         int* stepsRun, double* nut, double* gradP) {
+    return runFlow(r, sp, model, nSteps, dt, U, p, phi, hist, stepsRun, nut, gradP, readDir, writeDir);
 }

@@ -17,6 +17,7 @@ non-convergence only clears `converged`.
 from __future__ import annotations
 
 import atexit
+import os
 import ctypes as C
 import weakref
 from dataclasses import dataclass
@@ -546,6 +547,18 @@ class Flow:
         mdl.relaxation = model.get("relaxation", 1.0)
         mdl.grad_p = model.get("grad_p", 0.0)
         check(load().vlm_flow_set_model(self._h, C.byref(mdl)), self.mesh.ctx.handle)
+
+    def write_restart(self, directory: str):
+        """The flow's state in the reference's restart directory format (restart::write)."""
+        check(load().vlm_flow_write_restart(self._h, os.fspath(directory).encode()), self.mesh.ctx.handle)
+
+    def read_restart(self, directory: str) -> bool:
+        """Continue from a restart directory (restart::read); False when it has no state.txt.  Set
+        the model first."""
+        found = C.c_int32()
+        check(load().vlm_flow_read_restart(self._h, os.fspath(directory).encode(), C.byref(found)),
+              self.mesh.ctx.handle)
+        return bool(found.value)
 
     def model_state(self):
         """(nu_t per cell, mean-velocity driving pressure gradient)."""

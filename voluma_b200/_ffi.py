@@ -20,7 +20,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
            "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
            "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy", "vlm_flow_set_model",
-           "vlm_flow_get_model_state"]
+           "vlm_flow_get_model_state", "vlm_flow_write_restart", "vlm_flow_read_restart"]
 
 
 class MeshDesc(C.Structure):
@@ -113,6 +113,8 @@ def load():
     L.vlm_flow_destroy.argtypes = [P]
     L.vlm_flow_set_model.argtypes = [P, C.POINTER(FlowModel)]
     L.vlm_flow_get_model_state.argtypes = [P, P, P]
+    L.vlm_flow_write_restart.argtypes = [P, C.c_char_p]
+    L.vlm_flow_read_restart.argtypes = [P, C.c_char_p, C.POINTER(C.c_int32)]
     L.vlm_flow_launches.restype = C.c_int64
     L.vlm_flow_launches.argtypes = [P]
     L.vlm_flow_request_bytes.restype = C.c_int64

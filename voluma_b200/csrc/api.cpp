@@ -737,6 +737,23 @@ vlm_status vlm_flow_set_model(vlm_flow* f, const vlm_flow_model* model) {
     });
 }
 
+vlm_status vlm_flow_write_restart(vlm_flow* f, const char* dir) {
+    if (!f || !dir) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->writeRestart(dir);
+    });
+}
+
+vlm_status vlm_flow_read_restart(vlm_flow* f, const char* dir, int32_t* found) {
+    if (!f || !dir) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        const bool ok = f->flow->readRestart(dir);
+        if (found) *found = ok ? 1 : 0;
+    });
+}
+
 vlm_status vlm_flow_get_model_state(vlm_flow* f, double* nut, double* gradP) {
     if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
     return guarded(f->mesh->ctx, [&] {

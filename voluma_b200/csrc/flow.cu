@@ -9,6 +9,11 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <map>
+#include <string>
 
 namespace vlm {
 namespace {
@@ -450,7 +455,7 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     for (DBuf<double>* b : {&pB_, &pic_, &pbs_}) b->resize(B);
     for (DBuf<double>* b : {&upper_, &lower_, &loDiv_, &upDiv_, &lapUp_}) b->resize(FI);
     for (DBuf<double>* b : {&cDiv_, &ffc_}) b->resize(3 * FI);
-    for (DBuf<double>* b : {&phi_, &rAUf_, &phiHbyA_, &pffc_, &pflux_}) b->resize(F);
+    for (DBuf<double>* b : {&phi_, &rAUf_, &phiHbyA_, &pffc_, &pflux_, &phiOld_, &phiOldOld_}) b->resize(F);
     pupper_.resize(FI);
     gU_.resize(9 * N);
     gP_.resize(3 * N);
@@ -460,7 +465,7 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     solveStatus_.resize(size_t(2) * maxSolves);
     VLM_CUDA(cudaHostAlloc(&pinned_, sizeof(double) + sizeof(SysState) * maxSolves + sizeof(int) * 2 * maxSolves,
                            cudaHostAllocDefault));
-    for (DBuf<double>* b : {&U_, &U0_, &U00_, &p_, &phi_, &pffc_}) b->zero(s_);
+    for (DBuf<double>* b : {&U_, &U0_, &U00_, &p_, &phi_, &pffc_, &phiOld_, &phiOldOld_}) b->zero(s_);
     // VLM_FLOW_GRAPH=0: every step enqueued kernel by kernel (the captured steps' default is on)
     const char* fg = std::getenv("VLM_FLOW_GRAPH");
     graphOn_ = !(fg && fg[0] == '0');
@@ -559,6 +564,134 @@ void DeviceFlow::getState(double* U, double* p, double* phi) {
     if (p) VLM_CUDA(cudaMemcpyAsync(p, p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToHost, s_));
     if (phi) VLM_CUDA(cudaMemcpyAsync(phi, phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToHost, s_));
     VLM_CUDA(cudaStreamSynchronize(s_));
+}
+
+// ---------------------------------------------------------------- restart (io/Restart.cpp)
+namespace {
+constexpr uint64_t kRestartMagic = 0x4346445253543031ull;  // "CFDRST01"
+
+// writeGlobal (Restart.cpp:15-22): magic, count, components, then the doubles
+void writeRestartArray(const std::string& file, const std::vector<double>& g, uint64_t n, int nc) {
+    std::ofstream os(file, std::ios::binary);
+    VLM_REQUIRE(bool(os), VLM_ERR_BAD_ARG, "cannot write " + file);
+    const uint64_t h[3] = {kRestartMagic, n, uint64_t(nc)};
+    os.write(reinterpret_cast<const char*>(h), sizeof(h));
+    os.write(reinterpret_cast<const char*>(g.data()), std::streamsize(g.size() * sizeof(double)));
+    VLM_REQUIRE(bool(os), VLM_ERR_BAD_ARG, "cannot write " + file);
+}
+
+// readGlobal (Restart.cpp:25-43): false when the file is absent, an error when it does not fit
+bool readRestartArray(const std::string& file, uint64_t n, int nc, std::vector<double>& g) {
+    std::ifstream is(file, std::ios::binary);
+    if (!is) return false;
+    uint64_t h[3] = {0, 0, 0};
+    is.read(reinterpret_cast<char*>(h), sizeof(h));
+    VLM_REQUIRE(h[0] == kRestartMagic && h[1] == n && h[2] == uint64_t(nc), VLM_ERR_BAD_ARG,
+                "restart file " + file + " does not match the mesh");
+    g.resize(size_t(n) * size_t(nc));
+    is.read(reinterpret_cast<char*>(g.data()), std::streamsize(g.size() * sizeof(double)));
+    VLM_REQUIRE(bool(is), VLM_ERR_BAD_ARG, "restart file " + file + " is truncated");
+    return true;
+}
+}  // namespace
+
+// restart::write (Restart.cpp:105-132): cell arrays in cell order (vectors as 3 doubles per cell),
+// face arrays in face order (one rank: the global orders), and the time / forcing state as text
+void DeviceFlow::writeRestart(const std::string& dir) {
+    std::filesystem::create_directories(dir);
+    const size_t N = size_t(nC_), F = size_t(nF_);
+    auto cellVec = [&](const DBuf<double>& soa) {
+        DBuf<double> tmp(3 * N);
+        k_aos_from_soa<<<nblk(nC_), 256, 0, s_>>>(nC_, soa.get(), tmp.get()), ++launches_;
+        std::vector<double> h(3 * N);
+        VLM_CUDA(cudaMemcpyAsync(h.data(), tmp.get(), sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+        return h;
+    };
+    auto plain = [&](const double* d, size_t n) {
+        std::vector<double> h(n);
+        VLM_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+        return h;
+    };
+    writeRestartArray(dir + "/U.bin", cellVec(U_), N, 3);
+    writeRestartArray(dir + "/p.bin", plain(p_.get(), N), N, 1);
+    writeRestartArray(dir + "/phi.bin", plain(phi_.get(), F), F, 1);
+    if (nOld_ >= 1) {
+        writeRestartArray(dir + "/U_0.bin", cellVec(U0_), N, 3);
+        writeRestartArray(dir + "/phi_0.bin", plain(phiOld_.get(), F), F, 1);
+    }
+    if (nOld_ >= 2) {
+        writeRestartArray(dir + "/U_00.bin", cellVec(U00_), N, 3);
+        writeRestartArray(dir + "/phi_00.bin", plain(phiOldOld_.get(), F), F, 1);
+    }
+    if (les_) writeRestartArray(dir + "/nut.bin", plain(nut_.get(), N), N, 1);
+    double gradP = 0.0;
+    if (forcing_ == 2) gradP = plain(forceState_.get(), 1)[0];
+    std::ofstream os(dir + "/state.txt");
+    VLM_REQUIRE(bool(os), VLM_ERR_BAD_ARG, "cannot write " + dir + "/state.txt");
+    os << std::setprecision(17);
+    os << "time " << time_ << "\ndt " << dt_ << "\ndt0 " << dt0_ << "\ntimeIndex " << timeIndex_ << "\nnOldTimes "
+       << nOld_ << "\ngradP " << gradP << '\n';
+    VLM_REQUIRE(bool(os), VLM_ERR_BAD_ARG, "cannot write " + dir + "/state.txt");
+}
+
+// restart::read (Restart.cpp:134-190) followed by markRestarted (IncompressibleFlow.cpp:41-47)
+bool DeviceFlow::readRestart(const std::string& dir) {
+    std::ifstream st(dir + "/state.txt");
+    if (!st) return false;
+    std::map<std::string, double> kv;
+    {
+        std::string k;
+        double v;
+        while (st >> k >> v) kv[k] = v;
+    }
+    const size_t N = size_t(nC_), F = size_t(nF_);
+    std::vector<double> g;
+    auto cellVec = [&](const std::string& f, DBuf<double>& soa) {
+        if (!readRestartArray(f, N, 3, g)) return;
+        DBuf<double> tmp;
+        tmp.upload(g, s_);
+        k_soa_from_aos<<<nblk(nC_), 256, 0, s_>>>(nC_, tmp.get(), soa.get()), ++launches_;
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    };
+    auto plain = [&](const std::string& f, DBuf<double>& d, size_t n) {
+        if (!readRestartArray(f, n, 1, g)) return;
+        VLM_CUDA(cudaMemcpyAsync(d.get(), g.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    };
+    cellVec(dir + "/U.bin", U_);
+    plain(dir + "/p.bin", p_, N);
+    plain(dir + "/phi.bin", phi_, F);
+    const int nOld = int(kv["nOldTimes"]);
+    if (nOld >= 1) {
+        U0_.zero(s_);
+        phiOld_.zero(s_);
+        cellVec(dir + "/U_0.bin", U0_);
+        plain(dir + "/phi_0.bin", phiOld_, F);
+    }
+    if (nOld >= 2) {
+        U00_.zero(s_);
+        phiOldOld_.zero(s_);
+        cellVec(dir + "/U_00.bin", U00_);
+        plain(dir + "/phi_00.bin", phiOldOld_, F);
+    }
+    nOld_ = nOld;
+    if (les_) plain(dir + "/nut.bin", nut_, N);
+    time_ = kv["time"];
+    dt_ = kv["dt"];
+    dt0_ = kv["dt0"];
+    timeIndex_ = int(kv["timeIndex"]);
+    if (forcing_ == 2) {
+        const double gp = kv["gradP"];
+        VLM_CUDA(cudaMemcpyAsync(forceState_.get(), &gp, sizeof(double), cudaMemcpyHostToDevice, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    }
+    boundaryU();
+    boundaryP();
+    VLM_CUDA(cudaStreamSynchronize(s_));
+    initialized_ = true;
+    return true;
 }
 
 // UEqn = ddt + div(phi, U) - laplacian(nu, U), relaxed by aU (IncompressibleFlow.cpp:176-198)
@@ -702,11 +835,15 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
     vlm_step_info info;
     std::memset(&info, 0, sizeof info);
     const bool steady = ctrl_.steady != 0;
-    // VolField::storeOld (VolField.h:114-118)
-    if (copyOldOld)
+    // VolField::storeOld (VolField.h:114-118) and phiOldOld = phiOld, phiOld = phi (IncompressibleFlow.cpp:150-152)
+    if (copyOldOld) {
         VLM_CUDA(cudaMemcpyAsync(U00_.get(), U0_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
-    if (copyOld)
+        VLM_CUDA(cudaMemcpyAsync(phiOldOld_.get(), phiOld_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToDevice, s_));
+    }
+    if (copyOld) {
         VLM_CUDA(cudaMemcpyAsync(U0_.get(), U_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
+        VLM_CUDA(cudaMemcpyAsync(phiOld_.get(), phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToDevice, s_));
+    }
     boundaryU();
     boundaryP();
     nSolves_ = 0;

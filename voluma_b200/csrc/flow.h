@@ -23,6 +23,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "assembly.h"
@@ -51,6 +52,10 @@ public:
     // turbulence model and momentum forcing (flow_les.cu); before the first step
     void setModel(const vlm_flow_model& model);
     void modelState(double* nut, double* gradP);
+    // restart::write / restart::read (io/Restart.cpp): the flow's state in the reference's restart
+    // directory format; readRestart returns false when the directory has no state.txt
+    void writeRestart(const std::string& dir);
+    bool readRestart(const std::string& dir);
 
 private:
     void boundaryU();
@@ -108,7 +113,7 @@ private:
     DBuf<int32_t> uType_;
     DBuf<double> uValue_, pValueB_;
     // fields (vectors SoA: component k at [k * n])
-    DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_;
+    DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_, phiOld_, phiOldOld_;
     // momentum matrix: UEqn (diag, upper, lower, source, internalCoeffs, boundarySource)
     DBuf<double> diag_, upper_, lower_, src_, ic_, bs_;
     // face terms of the operators and their per-cell sums
