@@ -251,13 +251,15 @@ typedef struct vlm_flow vlm_flow;
 typedef struct {
     double nu;                   /* kinematic viscosity */
     int32_t steady;              /* 1: SIMPLE (steadyState) */
-    int32_t div_scheme;          /* 0 upwind, 1 linear, 2 linearUpwind, 3 LUST (Schemes.h:13-40) */
+    int32_t div_scheme;          /* 0 upwind, 1 linear, 2 linearUpwind, 3 LUST, 4 limitedLinear (k = div_coeff),
+                                    5 vanLeer, 6 MUSCL, 7 minmod (Schemes.h:15-39, Fvm.h:47-72) */
     int32_t ddt_scheme;          /* 0 steadyState, 1 Euler, 2 backward */
     int32_t n_outer, n_corr, n_non_orth_corr, momentum_predictor; /* PimpleControls */
     double alpha_u, alpha_p;
     int32_t p_ref_cell;
     double p_ref_value;
     vlm_solver_ctrl U, p, p_final;
+    double div_coeff;            /* limitedLinear's k ("limitedLinear k"); 0 -> 1 */
 } vlm_flow_ctrl;
 
 typedef struct {

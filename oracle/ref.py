@@ -81,7 +81,7 @@ class RefFlowSpec(C.Structure):
                 ("alphaU", C.c_double), ("alphaP", C.c_double), ("nPatches", C.c_int), ("uType", C.c_void_p),
                 ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
-                ("reproducible", C.c_int), ("residualTol", C.c_double)]
+                ("reproducible", C.c_int), ("residualTol", C.c_double), ("divK", C.c_double)]
 
 
 class RefModelSpec(C.Structure):
@@ -198,6 +198,7 @@ class RefMesh:
         sp.pRefCell, sp.pRefValue = case["p_ref_cell"], case["p_ref_value"]
         sp.reproducible = int(reproducible)
         sp.residualTol = residual_tol
+        sp.divK = case.get("div_coeff", 1.0)
         ran = C.c_int()
         if read_restart is not None or write_restart is not None:
             ms, turb = _model_spec(model or {})

@@ -12,7 +12,9 @@
 
 #include <cstring>
 #include <exception>
+#include <iomanip>
 #include <memory>
+#include <sstream>
 #include <string>
 
 using namespace cfd;
@@ -31,7 +33,8 @@ struct RefSolverCtl {
     int maxIter, minIter, nSweeps;
 };
 
-// Case settings: scheme codes follow Schemes.h (div: 0 upwind, 1 linear, 2 linearUpwind, 3 LUST;
+// Case settings: scheme codes follow Schemes.h (div: 0 upwind, 1 linear, 2 linearUpwind, 3 LUST,
+// 4 limitedLinear divK, 5 vanLeer, 6 MUSCL, 7 minmod;
 // ddt: 0 steadyState, 1 Euler, 2 backward); per patch (mesh patch order) U/p boundary type
 // 0 zeroGradient, 1 fixedValue with the given value.
 struct RefFlowSpec {
@@ -48,6 +51,7 @@ struct RefFlowSpec {
     double pRefValue;
     int reproducible;
     double residualTol;  // > 0: stop once U and p residuals are below it (from step 2, fvmFlow.cpp:611-625)
+    double divK;         // limitedLinear's k
 };
 
 // Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
@@ -115,8 +119,16 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
         c.pFinalControls = toCtl(sp->pFinal);
         c.pRefCell = sp->pRefCell;
         c.pRefValue = sp->pRefValue;
-        static const char* div[4] = {"upwind", "linear", "linearUpwind", "LUST"};
-        flow.divScheme = ConvectionScheme::parse(div[sp->divScheme]);
+        static const char* div[8] = {"upwind", "linear",  "linearUpwind", "LUST",
+                                     "limitedLinear", "vanLeer", "MUSCL", "minmod"};
+        if (sp->divScheme < 0 || sp->divScheme > 7) throw std::runtime_error("unknown divergence scheme code");
+        std::string scheme = div[sp->divScheme];
+        if (sp->divScheme == 4) {
+            std::ostringstream os;
+            os << std::setprecision(17) << scheme << ' ' << sp->divK;
+            scheme = os.str();
+        }
+        flow.divScheme = ConvectionScheme::parse(scheme);
         flow.ddtScheme = sp->ddtScheme == 0 ? DdtScheme::Steady : sp->ddtScheme == 1 ? DdtScheme::Euler
                                                                                       : DdtScheme::Backward;
         if (sp->nPatches != int(m.patches().size())) throw std::runtime_error("patch count mismatch");

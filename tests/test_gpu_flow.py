@@ -108,7 +108,7 @@ def test_cavity32_converges_like_reference(gold):
 def test_flow_rejects_bad_settings():
     m, case = cases.lid_cavity(8, 100.0)
     mesh = vb.Mesh.from_arrays(m)
-    bad = dict(case, div_scheme=7)
+    bad = dict(case, div_scheme=9)
     with pytest.raises(vb.VlmError) as e:
         vb.Flow(mesh, bad)
     assert e.value.name == "BAD_ARG"

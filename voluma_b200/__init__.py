@@ -474,6 +474,7 @@ def _flow_ctrl(case: dict) -> _ffi.FlowCtrl:
     c.momentum_predictor = int(case["momentum_predictor"])
     c.alpha_u, c.alpha_p = case["alpha_u"], case["alpha_p"]
     c.p_ref_cell, c.p_ref_value = case["p_ref_cell"], case["p_ref_value"]
+    c.div_coeff = case.get("div_coeff", 1.0)
     repro = bool(case.get("reproducible", False))
     for name, key in (("U", "U"), ("p", "p"), ("p_final", "pFinal")):
         d = case[key]

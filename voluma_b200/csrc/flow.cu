@@ -20,7 +20,21 @@ namespace {
 
 inline int nblk(int64_t n, int b = 256) { return int((n + b - 1) / b); }
 
-enum : int { kUpwind = 0, kLinear = 1, kLinearUpwind = 2, kLUST = 3 };
+enum : int { kUpwind = 0, kLinear = 1, kLinearUpwind = 2, kLUST = 3, kLimitedLinear = 4, kVanLeer = 5, kMUSCL = 6,
+             kMinmod = 7 };
+
+// the TVD limiters of detail::limiter (Fvm.h:63-72); std::min / std::max as the reference evaluates them
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double tvd_limiter(int scheme, double k, double r) {
+    switch (scheme) {
+    case kVanLeer: return (r + fabs(r)) / (1.0 + fabs(r));
+    case kMinmod: return dmax(dmin(r, 1.0), 0.0);
+    case kMUSCL: return dmax(dmin(dmin(2.0 * r, 0.5 * r + 0.5), 2.0), 0.0);
+    case kLimitedLinear: return dmax(dmin(2.0 / dmax(k, 1.0e-15) * r, 1.0), 0.0);
+    default: return 1.0;
+    }
+}
 
 // ---------------------------------------------------------------- boundary values of U
 // correctBoundaryConditions (VolField.h:96-103) for fixedValue (value) and zeroGradient (cell value)
@@ -89,8 +103,8 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
                             const double* __restrict__ ndc, const double* __restrict__ d,
                             const double* __restrict__ corr, const double* __restrict__ C,
                             const double* __restrict__ Cf, const double* __restrict__ phi, double nu,
-                            const double* __restrict__ nuF, int scheme, int nonOrth, const double* __restrict__ G,
-                            double* __restrict__ loDiv,
+                            const double* __restrict__ nuF, int scheme, double limK, const double* __restrict__ U,
+                            int nonOrth, const double* __restrict__ G, double* __restrict__ loDiv,
                             double* __restrict__ upDiv, double* __restrict__ lapUp, double* __restrict__ upper,
                             double* __restrict__ lower, double* __restrict__ cDiv, double* __restrict__ ffc) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -98,12 +112,29 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
     const double F = phi[f];
     const double wUp = F >= 0 ? 1.0 : 0.0;
     double wf;
-    if (scheme == kUpwind || scheme == kLinearUpwind)
+    if (scheme == kUpwind || scheme == kLinearUpwind) {
         wf = wUp;
-    else if (scheme == kLinear)
+    } else if (scheme == kLinear) {
         wf = w[f];
-    else
+    } else if (scheme == kLUST) {
         wf = 0.75 * w[f] + 0.25 * wUp;
+    } else {
+        // limiterR for a vector field (Fvm.h:55-61): r from (phiN - phiP) . (d . grad upwind)
+        const int o = own[f], n = nei[f];
+        double gradf[3], gradcf[3];
+        for (int k = 0; k < 3; ++k) gradf[k] = U[size_t(k) * nC + n] - U[size_t(k) * nC + o];
+        const double dv[3] = {d[f], d[nF + f], d[2 * size_t(nF) + f]};
+        vec_dot_tensor(dv, G, nC, F > 0 ? o : n, gradcf);
+        const double a = gradf[0] * gradcf[0] + gradf[1] * gradcf[1] + gradf[2] * gradcf[2];
+        const double b = gradf[0] * gradf[0] + gradf[1] * gradf[1] + gradf[2] * gradf[2];
+        double r;
+        if (fabs(a) >= 1000.0 * b)
+            r = 2.0 * 1000.0 * (a >= 0 ? 1 : -1) - 1.0;
+        else
+            r = 2.0 * (a / b) - 1.0;
+        const double lim = tvd_limiter(scheme, limK, r);
+        wf = lim * w[f] + (1.0 - lim) * wUp;
+    }
     const double lo = -wf * F;
     const double up = lo + F;
     // laplacian(nu_eff, U) with the face values nuF (turbulence model) or the uniform nu
@@ -419,7 +450,8 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     nB_ = G_.nBoundary();
     const int nP = G_.nPatches();
     VLM_REQUIRE(batch_.plan().nsys == 1, VLM_ERR_UNSUPPORTED, "the device flow step runs on a single-system mesh");
-    VLM_REQUIRE(ctrl_.div_scheme >= 0 && ctrl_.div_scheme <= 3, VLM_ERR_BAD_ARG, "unknown divergence scheme");
+    VLM_REQUIRE(ctrl_.div_scheme >= 0 && ctrl_.div_scheme <= 7, VLM_ERR_BAD_ARG, "unknown divergence scheme");
+    if (ctrl_.div_coeff == 0) ctrl_.div_coeff = 1.0;
     VLM_REQUIRE(ctrl_.ddt_scheme >= 0 && ctrl_.ddt_scheme <= 2, VLM_ERR_BAD_ARG, "unknown ddt scheme");
     VLM_REQUIRE(!ctrl_.steady || ctrl_.ddt_scheme == 0 || true, VLM_ERR_BAD_ARG, "");
     VLM_REQUIRE(ctrl_.nu > 0, VLM_ERR_BAD_ARG, "nu must be positive");
@@ -696,13 +728,14 @@ bool DeviceFlow::readRestart(const std::string& dir) {
 
 // UEqn = ddt + div(phi, U) - laplacian(nu, U), relaxed by aU (IncompressibleFlow.cpp:176-198)
 void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
-    const bool needG = ctrl_.div_scheme == kLinearUpwind || ctrl_.div_scheme == kLUST || G_.nonOrthogonal();
+    const bool needG = ctrl_.div_scheme >= kLinearUpwind || G_.nonOrthogonal();
     if (needG && !haveGradU) gradU();
     const double* nuF = les_ ? nuF_.get() : nullptr;
     if (nI_ > 0)
         k_mom_faces<<<nblk(nI_), 256, 0, s_>>>(nI_, nC_, nF_, G_.own(), G_.nei(), G_.w(), G_.magSf(), G_.ndc(), G_.d(),
                                               G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, nuF, ctrl_.div_scheme,
-                                              G_.nonOrthogonal() ? 1 : 0, gU_.get(), loDiv_.get(), upDiv_.get(),
+                                              ctrl_.div_coeff, U_.get(), G_.nonOrthogonal() ? 1 : 0, gU_.get(),
+                                              loDiv_.get(), upDiv_.get(),
                                               lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), uValue_.get(), G_.magSf(),

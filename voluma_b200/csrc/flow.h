@@ -14,7 +14,7 @@
 // (exact sums, diagonal preconditioning) a step reproduces the reference's fields bit for bit.
 //
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
-// linear / linearUpwind / LUST, Gauss linear gradients, fixedValue and zeroGradient boundary
+// linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients, fixedValue and zeroGradient boundary
 // conditions for U and p, empty (2D) directions and cyclic (internal) faces, the LES Smagorinsky model
 // with Van Driest damping and constant / mean-velocity momentum forcing (flow_les.cu).  Not supported
 // (an UNSUPPORTED status): skewed meshes, other turbulence models, wall models, buoyancy body forces,
