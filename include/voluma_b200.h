@@ -243,7 +243,9 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * phiHbyA (IncompressibleFlow.cpp:244-292), the pressure equation with its non-orthogonal correctors,
  * the explicit pressure relaxation and U = HbyA - rAU grad p.  The mesh must be a single system
  * registered with geometry (and C / Cf for linearUpwind or LUST); it must outlive the flow.
- * Boundary conditions per patch: 0 zeroGradient, 1 fixedValue (noSlip = fixedValue 0).
+ * Boundary conditions per patch: 0 zeroGradient, 1 fixedValue (noSlip = fixedValue 0), 2 symmetry
+ * (slip plane, SymmetryBC of field/BoundaryCondition.h:194-205: U_b = U_P - (n.U_P) n with the
+ * normal part implicit and zero flux; for p the same as zeroGradient).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
  * reference's fields bit for bit. */
 typedef struct vlm_flow vlm_flow;

@@ -137,10 +137,14 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
             if (m.patches()[q].type == PatchType::Empty || m.patches()[q].type == PatchType::Cyclic) continue;
             if (sp->uType[q] == 1)
                 flow.U().fixedValue(name, Vec3{sp->uValue[3 * q], sp->uValue[3 * q + 1], sp->uValue[3 * q + 2]});
+            else if (sp->uType[q] == 2)
+                flow.U().set<SymmetryBC<Vec3>>(name);
             else
                 flow.U().zeroGradient(name);
             if (sp->pType[q] == 1)
                 flow.p().fixedValue(name, sp->pValue[q]);
+            else if (sp->pType[q] == 2)
+                flow.p().set<SymmetryBC<scalar>>(name);
             else
                 flow.p().zeroGradient(name);
         }

@@ -1,0 +1,55 @@
+"""Generates tests/golden/flow_bc_cases.npz from the reference itself: IncompressibleFlow::step with
+symmetry (slip) planes for U and p (SymmetryBC, field/BoundaryCondition.h:194-205 and
+field/VolField.h:156-191), compiled into oracle/_ref/libvlmref.so and driven by oracle/ref_flow.cpp, in
+CFD_REPRODUCIBLE mode:
+  * slip2d: the 16 x 16 sheared slip cavity (leaning slip walls, one non-orthogonal corrector),
+    6 SIMPLE steps;
+  * slip2d_flat: the same without shear, 4 SIMPLE steps;
+  * slip3d: the 8 x 8 x 6 sheared slip cavity (slip x and z walls), transient Euler with nCorr 2,
+    3 steps of dt 0.05;
+  * slip2d_default: slip2d in the reference's default (non-reproducible) mode.
+Run where the reference sources are present:
+    make -C oracle && python tests/golden/make_bc_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import ref  # noqa: E402
+from voluma_b200 import cases  # noqa: E402
+
+
+def transient(case):
+    return dict(case, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0)
+
+
+CASES = {
+    # tag: (n, shear, case transform, steps, dt)
+    "slip2d": ((16, 16, 1), 0.3, dict, 6, 1.0),
+    "slip2d_flat": ((16, 16, 1), 0.0, dict, 4, 1.0),
+    "slip3d": ((8, 8, 6), 0.3, transient, 3, 0.05),
+}
+
+
+def main():
+    out = {}
+    for tag, (n, shear, tf, steps, dt) in CASES.items():
+        m, case, pts = cases.slip_cavity(n, shear)
+        R = ref.RefMesh(n, points=pts, two_d=n[2] == 1)
+        U, p, phi, hist = R.flow_run(tf(case), steps, dt=dt, reproducible=True)
+        out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
+    # the reference's default mode (DILU, GAMG with Gauss-Seidel) for the loose default-mode comparison
+    m, case, pts = cases.slip_cavity((16, 16, 1), 0.3)
+    R = ref.RefMesh((16, 16, 1), points=pts, two_d=True)
+    U, p, phi, hist = R.flow_run(case, 6)
+    out.update(slip2d_default_U=U, slip2d_default_p=p, slip2d_default_phi=phi, slip2d_default_hist=hist)
+    np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
+    print(sorted(out))
+
+
+if __name__ == "__main__":
+    main()

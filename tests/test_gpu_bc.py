@@ -1,0 +1,97 @@
+"""Symmetry (slip) planes for U and p in the device incompressible step (SymmetryBC,
+BoundaryCondition.h:194-205, VolField.h:156-191: u_b = u - (n.u) n, per-component implicit normal part,
+fixesFlux) against the reference's own IncompressibleFlow::step in CFD_REPRODUCIBLE mode (fixtures
+tests/golden/flow_bc_cases.npz, made by make_bc_golden.py): fields and residual histories bit for bit,
+on sheared meshes whose slip walls lean (normals off the axes)."""
+import os
+
+import numpy as np
+import pytest
+
+import voluma_b200 as vb
+from voluma_b200 import cases
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "flow_bc_cases.npz")
+
+
+def transient(case):
+    return dict(case, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0)
+
+
+CASES = {
+    "slip2d": ((16, 16, 1), 0.3, dict, 6, 1.0),
+    "slip2d_flat": ((16, 16, 1), 0.0, dict, 4, 1.0),
+    "slip3d": ((8, 8, 6), 0.3, transient, 3, 0.05),
+}
+
+
+@pytest.fixture(scope="module")
+def gold():
+    z = np.load(GOLD)
+    return {k: z[k] for k in z.files}
+
+
+def slip_faces(m):
+    names = list(m["patch_names"])
+    idx = []
+    for q, nm in enumerate(names):
+        if nm in ("xMin", "xMax", "zMin", "zMax"):
+            s = int(m["patch_start"][q])
+            idx.extend(range(s, s + int(m["patch_size"][q])))
+    return np.array(idx, np.int64)
+
+
+def test_golden_slip_walls_carry_no_flux(gold):
+    # the reference's own fields: the flux through every slip face is zero to rounding
+    for tag, (n, shear, _, _, _) in CASES.items():
+        m, _, _ = cases.slip_cavity(n, shear)
+        phi = gold[f"{tag}_phi"]
+        f = slip_faces(m)
+        assert f.size > 0
+        assert np.abs(phi[f]).max() < 1e-15 * max(1.0, np.abs(phi).max())
+
+
+def test_slip_case_types():
+    m, case, pts = cases.slip_cavity((8, 8, 6), 0.3)
+    assert not m["skewed"]
+    names = list(m["patch_names"])
+    assert [int(case["u_type"][names.index(k)]) for k in ("xMin", "zMax", "yMin", "yMax")] == [2, 2, 1, 1]
+    assert [int(case["p_type"][names.index(k)]) for k in ("xMax", "zMin", "yMin")] == [2, 2, 0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", sorted(CASES))
+def test_slip_cavity_bitwise(gold, tag):
+    n, shear, tf, steps, dt = CASES[tag]
+    m, case, _ = cases.slip_cavity(n, shear)
+    case = dict(tf(case), reproducible=True)
+    fl = vb.Flow(vb.Mesh.from_arrays(m), case)
+    fl.set_state(None, None)
+    hist = []
+    for _ in range(steps):
+        i = fl.step(dt)
+        hist.append([i["UInitialResidual"], i["pInitialResidual"], i["continuityError"]])
+    U, p, phi = fl.state()
+    fl.close()
+    assert np.array_equal(np.array(hist), gold[f"{tag}_hist"][:, :3])
+    assert np.array_equal(U, gold[f"{tag}_U"])
+    assert np.array_equal(p, gold[f"{tag}_p"])
+    assert np.array_equal(phi, gold[f"{tag}_phi"])
+
+
+@pytest.mark.gpu
+def test_slip_cavity_default_mode_close(gold):
+    # default (fast) mode against the reference's default mode: the device's parallel DILU and GAMG
+    # smoothers change the iterates within the solver tolerances (U relTol 0.1, p relTol 0.05 per
+    # outer iteration; measured 1.1e-3 of max |U| after 6 iterations)
+    n, shear, tf, steps, dt = CASES["slip2d"]
+    m, case, _ = cases.slip_cavity(n, shear)
+    fl = vb.Flow(vb.Mesh.from_arrays(m), case)
+    fl.set_state(None, None)
+    for _ in range(steps):
+        fl.step(dt)
+    U, p, phi = fl.state()
+    fl.close()
+    ref = gold["slip2d_default_U"]
+    assert np.abs(U - ref).max() < 5e-3 * np.abs(ref).max()
+    assert np.abs(phi[slip_faces(m)]).max() < 1e-15

@@ -163,6 +163,35 @@ def lid_cavity(n=64, Re=100.0, lid=1.0):
     return m, case
 
 
+def slip_cavity(n=(16, 16, 1), shear=0.3, Re=100.0, lid=1.0):
+    """A lid-driven cavity with slip side walls: the unit box (0.1 deep when nz = 1, two-dimensional)
+    sheared by x += shear * y, so that every cell is a parallelogram (non-orthogonal, not skewed) and
+    the xMin / xMax walls lean; those walls and, in 3D, zMin / zMax are symmetry planes for U and p
+    (SymmetryBC, BoundaryCondition.h:194-205); yMin is a no-slip wall and yMax the lid moving at
+    (lid, 0, 0); nu = lid / Re.  Steady SIMPLE with the lid-cavity settings and one non-orthogonal
+    corrector.  Returns (mesh, case, points); `points` is the vertex array in generateBox order."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    two_d = nz == 1
+    hi = (1.0, 1.0, 0.1 if two_d else 1.0)
+    pts = vm.box_points((nx, ny, nz), hi=hi)
+    pts[:, 0] += shear * pts[:, 1]
+    m = vm.box_mesh((nx, ny, nz), points=pts, two_d=two_d)
+    names = list(m["patch_names"])
+    nP = len(names)
+    slip = ("xMin", "xMax", "zMin", "zMax")
+    u_type = np.array([2 if nm in slip else 1 for nm in names], np.int32)
+    p_type = np.array([2 if nm in slip else 0 for nm in names], np.int32)
+    u_value = np.zeros((nP, 3))
+    u_value[names.index("yMax")] = (lid, 0.0, 0.0)
+    case = dict(nu=lid / Re, steady=True, div_scheme=2, ddt_scheme=0, n_outer=1, n_corr=1, n_non_orth_corr=1,
+                momentum_predictor=True, alpha_u=0.7, alpha_p=0.3, u_type=u_type, u_value=u_value.ravel(),
+                p_type=p_type, p_value=np.zeros(nP), U=_ctl("PBiCGStab", "DILU", 1e-10, 0.1, 1000),
+                p=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000), pFinal=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000),
+                p_ref_cell=0, p_ref_value=0.0)
+    return m, case, pts
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

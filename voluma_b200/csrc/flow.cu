@@ -38,13 +38,26 @@ __device__ __forceinline__ double tvd_limiter(int scheme, double k, double r) {
 
 // ---------------------------------------------------------------- boundary values of U
 // correctBoundaryConditions (VolField.h:96-103) for fixedValue (value) and zeroGradient (cell value)
-__global__ void k_u_boundary(int nB, int nI, int nC, const int32_t* __restrict__ own,
+// U boundary values (VolField::correctBoundaryConditions): fixedValue the value; zeroGradient the
+// owner's; symmetry u - (n.u) n with n = S_f / |S_f| (SymmetryBC<Vec3>::evaluate, VolField.h:164-170)
+__global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __restrict__ own,
                              const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
-                             const double* __restrict__ uValue, const double* __restrict__ U, double* __restrict__ Ub) {
+                             const double* __restrict__ uValue, const double* __restrict__ Sf,
+                             const double* __restrict__ magSf, const double* __restrict__ U,
+                             double* __restrict__ Ub) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int q = bPatch[b];
     const int c = own[nI + b];
+    if (uType[q] == 2) {
+        const int f = nI + b;
+        const double A = magSf[f];
+        const double n[3] = {Sf[f] / A, Sf[nF + f] / A, Sf[2 * size_t(nF) + f] / A};
+        const double u[3] = {U[c], U[size_t(nC) + c], U[2 * size_t(nC) + c]};
+        const double dnu = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+        for (int k = 0; k < 3; ++k) Ub[k * nB + b] = u[k] - dnu * n[k];
+        return;
+    }
     for (int k = 0; k < 3; ++k) Ub[k * nB + b] = uType[q] == 1 ? uValue[3 * q + k] : U[k * nC + c];
 }
 
@@ -184,19 +197,40 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
 // div: internalCoeffs += F vic, boundarySource -= F vbc (Fvm.h:117-126); laplacian: += gs gic,
 // -= gs gbc (Fvm.h:169-178); fixedValue: vic 0, vbc U_b, gic -dc, gbc dc U_b; zeroGradient: vic 1,
 // others 0 (BoundaryCondition.h:104-130).  UEqn = (0 + div) - laplacian.
-__global__ void k_mom_bfaces(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
-                             const double* __restrict__ uValue, const double* __restrict__ magSf,
-                             const double* __restrict__ ndc, const double* __restrict__ phi, double nu,
-                             const double* __restrict__ nuF, double* __restrict__ ic, double* __restrict__ bs) {
+__global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __restrict__ own,
+                             const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                             const double* __restrict__ uValue, const double* __restrict__ Sf,
+                             const double* __restrict__ magSf, const double* __restrict__ ndc,
+                             const double* __restrict__ phi, double nu, const double* __restrict__ nuF,
+                             const double* __restrict__ U, double* __restrict__ ic, double* __restrict__ bs) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int f = nI + b, q = bPatch[b];
-    const bool fixedValue = uType[q] == 1;
+    const bool fixedValue = uType[q] == 1, symmetry = uType[q] == 2;
     const double F = phi[f], dc = ndc[f], gs = (nuF ? nuF[f] : nu) * magSf[f];
+    // symmetry (SymmetryBC<Vec3>, VolField.h:174-191): vic = 1 - n^2, vbc = ub - vic u,
+    // gic = -dc n^2, gbc = -dc (n.u) n - gic u, per component
+    double n[3] = {0.0, 0.0, 0.0}, u[3] = {0.0, 0.0, 0.0}, dnu = 0.0;
+    if (symmetry) {
+        const double A = magSf[f];
+        const int c = own[f];
+        for (int k = 0; k < 3; ++k) {
+            n[k] = Sf[size_t(k) * nF + f] / A;
+            u[k] = U[size_t(k) * nC + c];
+        }
+        dnu = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+    }
     for (int k = 0; k < 3; ++k) {
         const double val = fixedValue ? uValue[3 * q + k] : 0.0;
-        const double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
-        const double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
+        double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
+        double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
+        if (symmetry) {
+            const double nn = n[k] * n[k];
+            vic = 1.0 - nn;
+            vbc = (u[k] - dnu * n[k]) - vic * u[k];
+            gic = -dc * nn;
+            gbc = (-dc * dnu) * n[k] - gic * u[k];
+        }
         double icDiv = 0.0, bsDiv = 0.0, icLap = 0.0, bsLap = 0.0;
         icDiv += vic * F;
         bsDiv -= vbc * F;
@@ -366,7 +400,7 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     } else {
         const int b = f - nI;
         rAUf[f] = rAU[o];
-        if (uType[bPatch[b]] == 1)
+        if (uType[bPatch[b]] != 0)  // fixesFlux: fixedValue and symmetry (BoundaryCondition.h:76, 203)
             phiHbyA[f] = Ub[b] * S[0] + Ub[size_t(nB) + b] * S[1] + Ub[size_t(2) * nB + b] * S[2];
         else
             phiHbyA[f] = HbyA[o] * S[0] + HbyA[size_t(nC) + o] * S[1] + HbyA[size_t(2) * nC + o] * S[2];
@@ -463,8 +497,8 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     uTypeHost_.assign(uType, uType + nP);
     pTypeHost_.assign(pType, pType + nP);
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE(uType[q] == 0 || uType[q] == 1, VLM_ERR_BAD_ARG, "U boundary type must be 0 or 1");
-        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1, VLM_ERR_BAD_ARG, "p boundary type must be 0 or 1");
+        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 2, VLM_ERR_BAD_ARG, "U boundary type must be 0, 1 or 2");
+        VLM_REQUIRE(pType[q] >= 0 && pType[q] <= 2, VLM_ERR_BAD_ARG, "p boundary type must be 0, 1 or 2");
     }
     // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
     needRef_ = true;
@@ -551,8 +585,8 @@ bool DeviceFlow::componentBatch() {
 
 void DeviceFlow::boundaryU() {
     if (nB_ > 0)
-        k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, G_.own(), G_.bPatch(), uType_.get(), uValue_.get(),
-                                                U_.get(), Ub_.get()), ++launches_;
+        k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
+                                                uValue_.get(), G_.Sf(), G_.magSf(), U_.get(), Ub_.get()), ++launches_;
 }
 
 void DeviceFlow::boundaryP() {
@@ -738,8 +772,9 @@ void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
                                               loDiv_.get(), upDiv_.get(),
                                               lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get()), ++launches_;
     if (nB_ > 0)
-        k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), uValue_.get(), G_.magSf(),
-                                               G_.ndc(), phi_.get(), ctrl_.nu, nuF, ic_.get(), bs_.get()), ++launches_;
+        k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
+                                               uValue_.get(), G_.Sf(), G_.magSf(), G_.ndc(), phi_.get(), ctrl_.nu,
+                                               nuF, U_.get(), ic_.get(), bs_.get()), ++launches_;
     // ddt coefficients (Schemes.h:70-86)
     double kc = 0, kc0 = 0, kc00 = 0;
     const bool transient = !ctrl_.steady;
