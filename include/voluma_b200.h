@@ -76,6 +76,9 @@ typedef struct {
     const int32_t* patch_size;  /* n_patches */
     const double* C;            /* 3*n_cells cell centres (optional: linearUpwind / LUST momentum) */
     const double* Cf;           /* 3*n_faces face centres (optional, with C) */
+    const double* skewVecs;     /* 3*n_faces, x_f - x'_f (Mesh::skewVecs); optional: NULL = not skewed.  The
+                                   device flow step applies the reference's skew corrections when
+                                   max |skewVecs|/|d| over internal faces exceeds 1e-8 (Mesh.cpp:596, 617-621) */
 } vlm_mesh_desc;
 
 /* Solver dictionary: SolverControls (src/fvm/linalg/LinearSolver.h:15-23) plus additive keys. */

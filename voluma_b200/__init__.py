@@ -168,7 +168,7 @@ class Mesh:
         d.magSf = self.magSf.ctypes.data
         d.ndc = self.ndc.ctypes.data
         self._keep = []
-        for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
+        for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf", "skewVecs"):
             if name in self.geometry:
                 arr = _f64(self.geometry[name])
                 self._keep.append(arr)
@@ -203,7 +203,7 @@ class Mesh:
             arrs = [own, nei, _f64(m["magSf"]), _f64(m["ndc"])]
             d.n_cells, d.n_internal_faces, d.n_faces = int(m["n_cells"]), nei.size, own.size
             d.owner, d.neighbour, d.magSf, d.ndc = (a.ctypes.data for a in arrs)
-            for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
+            for name in ("V", "Sf", "d", "w", "corrVecs", "C", "Cf", "skewVecs"):
                 if name in m:
                     a = _f64(m[name])
                     arrs.append(a)
@@ -616,7 +616,7 @@ class Server:
         arrs.update(own=own, nei=nei)
         d.n_cells, d.n_internal_faces, d.n_faces = int(mesh["n_cells"]), nei.size, own.size
         d.owner, d.neighbour = own.ctypes.data, nei.ctypes.data
-        for name in ("magSf", "ndc", "V", "Sf", "d", "w", "corrVecs", "C", "Cf"):
+        for name in ("magSf", "ndc", "V", "Sf", "d", "w", "corrVecs", "C", "Cf", "skewVecs"):
             if name in mesh:
                 a = _f64(mesh[name])
                 arrs[name] = a

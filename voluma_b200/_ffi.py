@@ -28,7 +28,8 @@ class MeshDesc(C.Structure):
                 ("owner", C.c_void_p), ("neighbour", C.c_void_p), ("magSf", C.c_void_p), ("ndc", C.c_void_p),
                 ("V", C.c_void_p), ("Sf", C.c_void_p), ("d", C.c_void_p), ("w", C.c_void_p),
                 ("corrVecs", C.c_void_p), ("two_d", C.c_int32), ("empty_dir", C.c_int32), ("n_patches", C.c_int32),
-                ("patch_start", C.c_void_p), ("patch_size", C.c_void_p), ("C", C.c_void_p), ("Cf", C.c_void_p)]
+                ("patch_start", C.c_void_p), ("patch_size", C.c_void_p), ("C", C.c_void_p), ("Cf", C.c_void_p),
+                ("skewVecs", C.c_void_p)]
 
 
 class SolverCtrl(C.Structure):

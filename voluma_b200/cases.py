@@ -192,6 +192,31 @@ def slip_cavity(n=(16, 16, 1), shear=0.3, Re=100.0, lid=1.0):
     return m, case, pts
 
 
+def skewed_cavity(n=(16, 16, 1), jitter=0.2, seed=20261203, Re=100.0, lid=1.0):
+    """The lid-driven cavity on a jittered box: interior vertices moved by U(+-jitter h) (boundary
+    vertices stay), so that the mesh is non-orthogonal and skewed (Mesh::skewed: the linear
+    interpolation point of a face is off its centre) and the step takes the reference's skew
+    corrections.  The unit box is 0.1 deep and two-dimensional when nz = 1; no-slip walls, the yMax
+    lid at (lid, 0, 0), nu = lid / Re; the lid-cavity SIMPLE settings with one non-orthogonal
+    corrector.  Returns (mesh, case, points); `points` is the vertex array in generateBox order."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    two_d = nz == 1
+    hi = (1.0, 1.0, 0.1 if two_d else 1.0)
+    pts = vm.jitter_interior(vm.box_points((nx, ny, nz), hi=hi), (nx, ny, nz), jitter, seed)
+    m = vm.box_mesh((nx, ny, nz), points=pts, two_d=two_d)
+    names = list(m["patch_names"])
+    nP = len(names)
+    u_value = np.zeros((nP, 3))
+    u_value[names.index("yMax")] = (lid, 0.0, 0.0)
+    case = dict(nu=lid / Re, steady=True, div_scheme=2, ddt_scheme=0, n_outer=1, n_corr=1, n_non_orth_corr=1,
+                momentum_predictor=True, alpha_u=0.7, alpha_p=0.3, u_type=np.ones(nP, np.int32),
+                u_value=u_value.ravel(), p_type=np.zeros(nP, np.int32), p_value=np.zeros(nP),
+                U=_ctl("PBiCGStab", "DILU", 1e-10, 0.1, 1000), p=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000),
+                pFinal=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000), p_ref_cell=0, p_ref_value=0.0)
+    return m, case, pts
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

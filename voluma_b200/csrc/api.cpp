@@ -227,6 +227,9 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
             bool centres = true;  // cell / face centres (optional)
             for (int s = 0; s < nsys; ++s) centres = centres && descs[s].C && descs[s].Cf;
             std::vector<double> Cc(centres ? 3 * NC : 0), Cfc(centres ? 3 * F : 0);
+            bool skews = true;  // skew vectors (optional)
+            for (int s = 0; s < nsys; ++s) skews = skews && descs[s].skewVecs;
+            std::vector<double> skv(skews ? 3 * F : 0);
             auto copyFace = [&](const vlm_mesh_desc* d, int f, int64_t g, int64_t base) {
                 own[g] = int32_t(d->owner[f] + base);
                 magSf[g] = d->magSf[f];
@@ -237,6 +240,7 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
                     dd[3 * g + q] = d->d[3 * f + q];
                     corr[3 * g + q] = d->corrVecs[3 * f + q];
                     if (centres) Cfc[3 * g + q] = d->Cf[3 * f + q];
+                    if (skews) skv[3 * g + q] = d->skewVecs[3 * f + q];
                 }
             };
             for (int s = 0; s < nsys; ++s) {
@@ -263,7 +267,7 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
                                                         corr.data(), descs[0].two_d, descs[0].empty_dir,
                                                         int(ps.size()), ps.data(), pz.data(),
                                                         centres ? Cc.data() : nullptr, centres ? Cfc.data() : nullptr,
-                                                        ctx->stream);
+                                                        skews ? skv.data() : nullptr, ctx->stream);
         }
         ctx->refs++;
         *out = m.release();

@@ -4,6 +4,7 @@
 // (the order in which the reference's face loops update that cell), or one thread per face.
 // With -fmad=false the results equal the reference's face-loop scatters bit for bit; nothing
 // is accumulated with atomics.
+#include <algorithm>
 #include <cmath>
 
 #include "assembly.h"
@@ -304,7 +305,7 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
                        const double* magSf, const double* ndc, const double* V, const double* Sf, const double* d,
                        const double* w, const double* corrVecs, int twoD, int emptyDir, int nPatches,
                        const int32_t* patchStart, const int32_t* patchSize, const double* C, const double* Cf,
-                       cudaStream_t s)
+                       const double* skewVecs, cudaStream_t s)
     : nC_(nCells), nI_(nInternal), nF_(nFaces), twoD_(twoD), emptyDir_(emptyDir) {
     VLM_REQUIRE(V && Sf && d && w && corrVecs, VLM_ERR_BAD_ARG, "mesh geometry (V, Sf, d, w, corrVecs) is required");
     const int nB = nF_ - nI_;
@@ -357,6 +358,19 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
         for (int c = 0; c < nC_; ++c)
             for (int q = 0; q < 3; ++q) v[size_t(q) * nC_ + c] = C[3 * size_t(c) + q];
         C_.upload(v, s);
+    }
+    // Mesh::skewed (Mesh.cpp:596, 617-621): max |x_f - x'_f| / |d| over internal faces above 1e-8
+    if (skewVecs) {
+        double skewMax = 0.0;
+        for (int f = 0; f < nI_; ++f) {
+            const double* k = skewVecs + 3 * size_t(f);
+            const double* dd = d + 3 * size_t(f);
+            const double sk = std::sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]) /
+                              std::sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+            skewMax = std::max(skewMax, sk);
+        }
+        skewed_ = skewMax > 1e-8;
+        if (skewed_) soa(skewVecs, skew_);
     }
     // the correction is applied when any internal corrVec is non-zero (Fvm.h:156-158)
     for (int f = 0; f < nI_ && !nonOrth_; ++f) {

@@ -25,13 +25,15 @@ public:
     DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own, const int32_t* nei, const double* magSf,
                const double* ndc, const double* V, const double* Sf, const double* d, const double* w,
                const double* corrVecs, int twoD, int emptyDir, int nPatches, const int32_t* patchStart,
-               const int32_t* patchSize, const double* C, const double* Cf, cudaStream_t stream);
+               const int32_t* patchSize, const double* C, const double* Cf, const double* skewVecs,
+               cudaStream_t stream);
 
     int nCells() const { return nC_; }
     int nInternal() const { return nI_; }
     int nFaces() const { return nF_; }
     int nBoundary() const { return nF_ - nI_; }
     bool nonOrthogonal() const { return nonOrth_; }
+    bool skewed() const { return skewed_; }  // Mesh::skewed(); skew() is then the SoA x_f - x'_f
 
     // fvm::laplacian(gamma, psi) for a scalar field (Fvm.h:141-182).  All pointers device.
     // gradScheme: 0 Gauss linear, 1 least squares.  ffc may be null when not needed.
@@ -80,6 +82,7 @@ public:
     const double* corr() const { return corr_.get(); }
     const double* C() const { return C_.size() ? C_.get() : nullptr; }
     const double* Cf() const { return Cf_.size() ? Cf_.get() : nullptr; }
+    const double* skew() const { return skew_.size() ? skew_.get() : nullptr; }
     int twoD() const { return twoD_; }
     int64_t launches() const { return launches_; }  // kernels launched by the methods above
     int emptyDir() const { return emptyDir_; }
@@ -89,12 +92,12 @@ public:
 
 private:
     int nC_, nI_, nF_, twoD_, emptyDir_;
-    bool nonOrth_ = false;
+    bool nonOrth_ = false, skewed_ = false;
     std::vector<int32_t> patchStart_, patchSize_, bPatchHost_;
     DBuf<int32_t> own_, nei_, cfOff_, cfList_, bPatch_, bcType_;
     std::vector<int32_t> bcTypeHost_;  // the patch types last copied to bcType_
     DBuf<double> magSf_, ndc_, V_, w_, Sf_, d_, corr_;  // vectors as SoA: [x(nF) y(nF) z(nF)]
-    DBuf<double> C_, Cf_;                               // SoA; empty when not registered
+    DBuf<double> C_, Cf_, skew_;                        // SoA; empty when not registered (skew_: not skewed)
     int64_t launches_ = 0;
     DBuf<double> scratchG_, scratchGS_;
     void uploadBCType(const ScalarBC& bc, cudaStream_t s);

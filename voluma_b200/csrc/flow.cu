@@ -117,9 +117,10 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
                             const double* __restrict__ corr, const double* __restrict__ C,
                             const double* __restrict__ Cf, const double* __restrict__ phi, double nu,
                             const double* __restrict__ nuF, int scheme, double limK, const double* __restrict__ U,
-                            int nonOrth, const double* __restrict__ G, double* __restrict__ loDiv,
-                            double* __restrict__ upDiv, double* __restrict__ lapUp, double* __restrict__ upper,
-                            double* __restrict__ lower, double* __restrict__ cDiv, double* __restrict__ ffc) {
+                            int nonOrth, const double* __restrict__ G, const double* __restrict__ skew,
+                            double* __restrict__ loDiv, double* __restrict__ upDiv, double* __restrict__ lapUp,
+                            double* __restrict__ upper, double* __restrict__ lower, double* __restrict__ cDiv,
+                            double* __restrict__ cSkew, double* __restrict__ ffc) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nI) return;
     const double F = phi[f];
@@ -180,6 +181,16 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
         for (int k = 0; k < 3; ++k) cc[k] = corrv[k] * s;
     }
     for (int k = 0; k < 3; ++k) cDiv[size_t(k) * nI + f] = cc[k];
+    // skewed mesh, linear / LUST: explicit skew correction of the linear part (Fvm.h:83, 119-123)
+    if (skew && (scheme == kLinear || scheme == kLUST)) {
+        const double fac = scheme == kLUST ? 0.75 : 1.0;
+        const double wo = w[f], wn = 1.0 - wo;
+        double gf[9];
+        for (int m = 0; m < 9; ++m) gf[m] = G[size_t(m) * nC + o] * wo + G[size_t(m) * nC + n] * wn;
+        const double sv[3] = {skew[f], skew[nF + f], skew[2 * size_t(nF) + f]};
+        const double s = fac * F;
+        for (int j = 0; j < 3; ++j) cSkew[size_t(j) * nI + f] = (sv[0] * gf[j] + sv[1] * gf[3 + j] + sv[2] * gf[6 + j]) * s;
+    }
     // non-orthogonal correction of the laplacian (Fvm.h:155-167)
     double fc[3] = {0.0, 0.0, 0.0};
     if (nonOrth) {
@@ -252,7 +263,8 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
 __global__ void k_mom_cells(int nC, int nI, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
                             const double* __restrict__ loDiv, const double* __restrict__ upDiv,
                             const double* __restrict__ lapUp, const double* __restrict__ cDiv,
-                            const double* __restrict__ ffc, const double* __restrict__ V, int transient, double kc,
+                            const double* __restrict__ cSkew, const double* __restrict__ ffc,
+                            const double* __restrict__ V, int transient, double kc,
                             double kc0, double kc00, const double* __restrict__ U0, const double* __restrict__ U00,
                             double* __restrict__ diag, double* __restrict__ src) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,6 +279,7 @@ __global__ void k_mom_cells(int nC, int nI, const int32_t* __restrict__ cfOff, c
             dLap -= lapUp[f];
             for (int q = 0; q < 3; ++q) {
                 sDiv[q] += cDiv[size_t(q) * nI + f];
+                if (cSkew) sDiv[q] += cSkew[size_t(q) * nI + f];
                 sLap[q] += ffc[size_t(q) * nI + f];
             }
         } else {
@@ -274,6 +287,7 @@ __global__ void k_mom_cells(int nC, int nI, const int32_t* __restrict__ cfOff, c
             dLap -= lapUp[f];
             for (int q = 0; q < 3; ++q) {
                 sDiv[q] -= cDiv[size_t(q) * nI + f];
+                if (cSkew) sDiv[q] -= cSkew[size_t(q) * nI + f];
                 sLap[q] -= ffc[size_t(q) * nI + f];
             }
         }
@@ -380,12 +394,99 @@ __global__ void k_mom_AH(int nC, int nI, int nB, const int32_t* __restrict__ cfO
     for (int q = 0; q < 3; ++q) HbyA[size_t(q) * nC + c] = (h[q] / V[c]) * r;
 }
 
+// fvc::gradLS (Fvc.h:135-167, 186-205) of an NC-component cell array psi (SoA): boundary faces of the
+// patches with fix[p] != 0 constrain by value (d, bVal - psi_P), the others by a zero normal gradient
+// (n max(n.d, 0.05|d|), 0); weights 1/|d|^2; the empty direction zeroed in 2D.  Out: SoA rows
+// 3 i + j = d psi_j / dx_i (Tensor(i, j) of outer(G d, dpsi)); row i for NC = 1.
+template <int NC>
+__global__ void k_grad_ls_cells(int nC, int nI, int nF, int nB, const int32_t* __restrict__ cfOff,
+                                const int32_t* __restrict__ cf, const int32_t* __restrict__ own,
+                                const int32_t* __restrict__ nei, const double* __restrict__ Sf,
+                                const double* __restrict__ magSf, const double* __restrict__ d,
+                                const double* __restrict__ psi, const double* __restrict__ bVal,
+                                const int32_t* __restrict__ bPatch, const int32_t* __restrict__ fix, int twoD,
+                                int emptyDir, double* __restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    auto faceVec = [&](int f, double v[3]) -> bool {
+        v[0] = d[f];
+        v[1] = d[nF + f];
+        v[2] = d[2 * size_t(nF) + f];
+        if (f < nI || (fix && fix[bPatch[f - nI]] != 0)) return true;
+        const double inv = 1.0 / magSf[f];
+        const double n[3] = {Sf[f] * inv, Sf[nF + f] * inv, Sf[2 * size_t(nF) + f] * inv};
+        const double nd = fmax(n[0] * v[0] + n[1] * v[1] + n[2] * v[2], 0.05 * sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+        for (int k = 0; k < 3; ++k) v[k] = n[k] * nd;
+        return false;
+    };
+    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = int((uint32_t)cf[k] & 0x7fffffffu);
+        double v[3];
+        faceVec(f, v);
+        const double s = 1.0 / (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double o[9] = {v[0] * v[0], v[0] * v[1], v[0] * v[2], v[1] * v[0], v[1] * v[1],
+                             v[1] * v[2], v[2] * v[0], v[2] * v[1], v[2] * v[2]};
+        for (int q = 0; q < 9; ++q) a[q] += o[q] * s;
+    }
+    if (twoD) a[4 * emptyDir] += 1.0;
+    // detail::inv (Fvc.h:112-126)
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    double G[9];
+    G[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+    G[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+    G[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+    G[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+    G[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+    G[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+    G[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+    G[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+    G[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+    double acc[3 * NC];
+    for (int q = 0; q < 3 * NC; ++q) acc[q] = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = int((uint32_t)cf[k] & 0x7fffffffu);
+        double v[3], dp[NC];
+        const bool value = faceVec(f, v);
+        if (f < nI) {
+            for (int j = 0; j < NC; ++j) dp[j] = psi[size_t(j) * nC + nei[f]] - psi[size_t(j) * nC + own[f]];
+        } else if (value) {
+            for (int j = 0; j < NC; ++j) dp[j] = bVal[size_t(j) * nB + (f - nI)] - psi[size_t(j) * nC + c];
+        } else {
+            for (int j = 0; j < NC; ++j) dp[j] = 0.0;
+        }
+        const double wgt = 1.0 / (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double dw[3] = {v[0] * wgt, v[1] * wgt, v[2] * wgt};
+        const double Gd[3] = {G[0] * dw[0] + G[1] * dw[1] + G[2] * dw[2], G[3] * dw[0] + G[4] * dw[1] + G[5] * dw[2],
+                              G[6] * dw[0] + G[7] * dw[1] + G[8] * dw[2]};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < NC; ++j) acc[i * NC + j] += Gd[i] * dp[j];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < NC; ++j)
+            g[size_t(i * NC + j) * nC + c] = (twoD && i == emptyDir) ? 0.0 : acc[i * NC + j];
+}
+
+// HbyA boundary values of the skew-corrected Rhie-Chow flux on fixes-flux faces: U_b + rAU_P grad p_P
+// (IncompressibleFlow.cpp:262-272); gp: 3 per cell
+__global__ void k_hbya_bval(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
+                            const int32_t* __restrict__ uType, const double* __restrict__ Ub,
+                            const double* __restrict__ rAU, const double* __restrict__ gp, double* __restrict__ hB) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB || uType[bPatch[b]] == 0) return;
+    const int o = own[nI + b];
+    for (int j = 0; j < 3; ++j) hB[size_t(j) * nB + b] = Ub[size_t(j) * nB + b] + rAU[o] * gp[3 * size_t(o) + j];
+}
+
 // rAUf = interpolate(rAU) (Fvc.h:24-32) and phiHbyA (IncompressibleFlow.cpp:258-281)
 __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __restrict__ own,
                            const int32_t* __restrict__ nei, const double* __restrict__ w, const double* __restrict__ Sf,
                            const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                            const double* __restrict__ rAU, const double* __restrict__ HbyA,
-                           const double* __restrict__ Ub, double* __restrict__ rAUf, double* __restrict__ phiHbyA) {
+                           const double* __restrict__ Ub, const double* __restrict__ skew,
+                           const double* __restrict__ gR, const double* __restrict__ gH, double* __restrict__ rAUf,
+                           double* __restrict__ phiHbyA) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nF) return;
     const double S[3] = {Sf[f], Sf[nF + f], Sf[2 * nF + f]};
@@ -393,9 +494,20 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     if (f < nI) {
         const int n = nei[f];
         const double wf = w[f], wn = 1.0 - wf;
-        rAUf[f] = wf * rAU[o] + wn * rAU[n];
+        double r = wf * rAU[o] + wn * rAU[n];
         double Hf[3];
         for (int q = 0; q < 3; ++q) Hf[q] = HbyA[size_t(q) * nC + o] * wf + HbyA[size_t(q) * nC + n] * wn;
+        if (skew) {
+            // skewed mesh: rAUf and HbyA_f with (x_f - x'_f) . grad_f (Fvc.h:73-82; IncompressibleFlow.cpp:252-282)
+            const double sv[3] = {skew[f], skew[nF + f], skew[2 * size_t(nF) + f]};
+            double gr[3];
+            for (int i = 0; i < 3; ++i) gr[i] = wf * gR[size_t(i) * nC + o] + wn * gR[size_t(i) * nC + n];
+            r += sv[0] * gr[0] + sv[1] * gr[1] + sv[2] * gr[2];
+            double gf[9];
+            for (int m = 0; m < 9; ++m) gf[m] = wf * gH[size_t(m) * nC + o] + wn * gH[size_t(m) * nC + n];
+            for (int j = 0; j < 3; ++j) Hf[j] += sv[0] * gf[j] + sv[1] * gf[3 + j] + sv[2] * gf[6 + j];
+        }
+        rAUf[f] = r;
         phiHbyA[f] = Hf[0] * S[0] + Hf[1] * S[1] + Hf[2] * S[2];
     } else {
         const int b = f - nI;
@@ -432,13 +544,21 @@ __global__ void k_u_correct(int nC, const double* __restrict__ HbyA, const doubl
 // phi = U_f . S_f with boundary faces at the boundary value (Fvc.h:103-109, initialize)
 __global__ void k_flux_u(int nF, int nI, int nB, int nC, const int32_t* __restrict__ own,
                          const int32_t* __restrict__ nei, const double* __restrict__ w, const double* __restrict__ Sf,
-                         const double* __restrict__ U, const double* __restrict__ Ub, double* __restrict__ phi) {
+                         const double* __restrict__ U, const double* __restrict__ Ub, const double* __restrict__ skew,
+                         const double* __restrict__ G, double* __restrict__ phi) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nF) return;
     double Uf[3];
     if (f < nI) {
+        const int o = own[f], n = nei[f];
         const double wf = w[f], wn = 1.0 - wf;
-        for (int q = 0; q < 3; ++q) Uf[q] = U[size_t(q) * nC + own[f]] * wf + U[size_t(q) * nC + nei[f]] * wn;
+        for (int q = 0; q < 3; ++q) Uf[q] = U[size_t(q) * nC + o] * wf + U[size_t(q) * nC + n] * wn;
+        if (skew) {  // skewed mesh: fvc::flux(U, grad U) (Fvc.h:84-95, IncompressibleFlow.cpp:36)
+            const double sv[3] = {skew[f], skew[nF + f], skew[2 * size_t(nF) + f]};
+            double gf[9];
+            for (int m = 0; m < 9; ++m) gf[m] = wf * G[size_t(m) * nC + o] + wn * G[size_t(m) * nC + n];
+            for (int j = 0; j < 3; ++j) Uf[j] += sv[0] * gf[j] + sv[1] * gf[3 + j] + sv[2] * gf[6 + j];
+        }
     } else {
         for (int q = 0; q < 3; ++q) Uf[q] = Ub[size_t(q) * nB + (f - nI)];
     }
@@ -526,6 +646,12 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     gU_.resize(9 * N);
     gP_.resize(3 * N);
     cont_.resize(1);
+    if (G_.skewed()) {
+        cSkew_.resize(3 * FI);
+        gR_.resize(3 * N);
+        gH_.resize(9 * N);
+        hB_.resize(3 * size_t(std::max(nB_, 1)));
+    }
     const int maxSolves = ctrl_.n_outer * (3 + ctrl_.n_corr * (ctrl_.n_non_orth_corr + 1));
     solveState_.resize(size_t(maxSolves));
     solveStatus_.resize(size_t(2) * maxSolves);
@@ -612,8 +738,9 @@ void DeviceFlow::setState(const double* U, const double* p) {
     if (p) p_.upload(p, size_t(nC_), s_);
     boundaryU();
     boundaryP();
+    if (G_.skewed()) gradU();
     k_flux_u<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), U_.get(), Ub_.get(),
-                                       phi_.get()), ++launches_;
+                                       G_.skewed() ? G_.skew() : nullptr, gU_.get(), phi_.get()), ++launches_;
     rAU_.zero(s_);
     VLM_CUDA(cudaGetLastError());
     VLM_CUDA(cudaStreamSynchronize(s_));
@@ -762,15 +889,18 @@ bool DeviceFlow::readRestart(const std::string& dir) {
 
 // UEqn = ddt + div(phi, U) - laplacian(nu, U), relaxed by aU (IncompressibleFlow.cpp:176-198)
 void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
-    const bool needG = ctrl_.div_scheme >= kLinearUpwind || G_.nonOrthogonal();
+    // skewed mesh: linear and LUST add an explicit skew correction from grad U (Fvm.h:83-84)
+    const bool skewLin = G_.skewed() && (ctrl_.div_scheme == kLinear || ctrl_.div_scheme == kLUST);
+    const bool needG = ctrl_.div_scheme >= kLinearUpwind || G_.nonOrthogonal() || skewLin;
     if (needG && !haveGradU) gradU();
     const double* nuF = les_ ? nuF_.get() : nullptr;
     if (nI_ > 0)
         k_mom_faces<<<nblk(nI_), 256, 0, s_>>>(nI_, nC_, nF_, G_.own(), G_.nei(), G_.w(), G_.magSf(), G_.ndc(), G_.d(),
                                               G_.corr(), G_.C(), G_.Cf(), phi_.get(), ctrl_.nu, nuF, ctrl_.div_scheme,
                                               ctrl_.div_coeff, U_.get(), G_.nonOrthogonal() ? 1 : 0, gU_.get(),
-                                              loDiv_.get(), upDiv_.get(),
-                                              lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(), ffc_.get()), ++launches_;
+                                              skewLin ? G_.skew() : nullptr, loDiv_.get(), upDiv_.get(),
+                                              lapUp_.get(), upper_.get(), lower_.get(), cDiv_.get(),
+                                              skewLin ? cSkew_.get() : nullptr, ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
                                                uValue_.get(), G_.Sf(), G_.magSf(), G_.ndc(), phi_.get(), ctrl_.nu,
@@ -791,7 +921,8 @@ void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
         }
     }
     k_mom_cells<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, G_.cellFaceOff(), G_.cellFaces(), loDiv_.get(), upDiv_.get(),
-                                          lapUp_.get(), cDiv_.get(), ffc_.get(), G_.V(), transient ? 1 : 0, kc, kc0,
+                                          lapUp_.get(), cDiv_.get(), skewLin && nI_ > 0 ? cSkew_.get() : nullptr,
+                                          ffc_.get(), G_.V(), transient ? 1 : 0, kc, kc0,
                                           kc00, U0_.get(), nOld_ >= 2 ? U00_.get() : U0_.get(), diag_.get(),
                                           src_.get()), ++launches_;
     if (les_ || forcing_ != 0) explicitSources();
@@ -857,14 +988,32 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     k_mom_AH<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
                                        diag_.get(), upper_.get(), lower_.get(), ic_.get(), bs_.get(), src_.get(),
                                        U_.get(), G_.V(), rAU_.get(), HbyA_.get()), ++launches_;
-    k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
-                                         uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(), rAUf_.get(),
-                                         phiHbyA_.get()), ++launches_;
-    G_.div(phiHbyA_.get(), divPhi_.get(), s_);
-    if (ctrl_.steady) VLM_CUDA(cudaMemcpyAsync(pPrev_.get(), p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToDevice, s_));
     ScalarBC pbc;
     pbc.type = pTypeHost_.data();
     pbc.value = pValueB_.get();
+    const bool skewed = G_.skewed();
+    if (skewed) {
+        // skewed mesh (IncompressibleFlow.cpp:252-275): grad rAU by least squares with zero-gradient
+        // boundaries; grad HbyA by least squares with the fixes-flux faces at U_b + rAU_P grad p_P
+        G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+        if (nB_ > 0)
+            k_hbya_bval<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.own(), G_.bPatch(), uType_.get(), Ub_.get(),
+                                                  rAU_.get(), gP_.get(), hB_.get()), ++launches_;
+        k_grad_ls_cells<1><<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
+                                                     G_.nei(), G_.Sf(), G_.magSf(), G_.d(), rAU_.get(), nullptr,
+                                                     G_.bPatch(), nullptr, G_.twoD(), G_.emptyDir(), gR_.get()),
+            ++launches_;
+        k_grad_ls_cells<3><<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
+                                                     G_.nei(), G_.Sf(), G_.magSf(), G_.d(), HbyA_.get(), hB_.get(),
+                                                     G_.bPatch(), uType_.get(), G_.twoD(), G_.emptyDir(), gH_.get()),
+            ++launches_;
+    }
+    k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
+                                         uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(),
+                                         skewed ? G_.skew() : nullptr, gR_.get(), gH_.get(), rAUf_.get(),
+                                         phiHbyA_.get()), ++launches_;
+    G_.div(phiHbyA_.get(), divPhi_.get(), s_);
+    if (ctrl_.steady) VLM_CUDA(cudaMemcpyAsync(pPrev_.get(), p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToDevice, s_));
     const int nNO = ctrl_.n_non_orth_corr;
     for (int no = 0; no <= nNO; ++no) {
         const bool finalNO = no == nNO;

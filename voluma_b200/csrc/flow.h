@@ -122,6 +122,8 @@ private:
     DBuf<double> gU_, gP_, msrc_, rAU_, HbyA_, rAUf_, phiHbyA_, divPhi_, pPrev_, fd_, fb_;
     DBuf<double> pdiag_, pupper_, psrc_, pic_, pbs_, pffc_, pflux_;
     DBuf<double> cont_;  // continuity error (max, as ordered bits)
+    // skewed meshes: div skew correction, least-squares gradients of rAU / HbyA, HbyA boundary values
+    DBuf<double> cSkew_, gR_, gH_, hB_;
     // solver records of the step's solves, read once at the end of the step
     DBuf<SysState> solveState_;
     DBuf<int> solveStatus_;

@@ -35,7 +35,7 @@ struct Request {
     int64_t id = 0;
     int32_t nCells = 0, nInternal = 0, nFaces = 0, nPatches = 0, twoD = 0, emptyDir = 0;
     std::vector<int32_t> own, nei, patchStart, patchSize, uType, pType;
-    std::vector<double> magSf, ndc, V, Sf, d, w, corr, C, Cf, uValue, pValue, U0, p0;
+    std::vector<double> magSf, ndc, V, Sf, d, w, corr, C, Cf, skew, uValue, pValue, U0, p0;
     vlm_flow_ctrl ctrl{};
     int32_t steady = 1, nSteps = 0, maxIter = 0;
     double dt = 1.0, tol = 1e-6, arrival = 0;
@@ -166,6 +166,7 @@ struct vlm_server {
         m.patch_size = q.patchSize.data();
         m.C = q.C.empty() ? nullptr : q.C.data();
         m.Cf = q.Cf.empty() ? nullptr : q.Cf.data();
+        m.skewVecs = q.skew.empty() ? nullptr : q.skew.data();
         vlm_mesh* mesh = nullptr;
         vlm_flow* flow = nullptr;
         vlm_status st = vlm_mesh_register(ctx, &m, 0, &mesh);
@@ -255,6 +256,7 @@ vlm_status vlm_server_submit(vlm_server* s, const vlm_flow_request* r, int64_t* 
     q->corr = copyOf(m.corrVecs, 3 * nF);
     q->C = copyOf(m.C, 3 * nC);
     q->Cf = copyOf(m.Cf, 3 * nF);
+    q->skew = copyOf(m.skewVecs, 3 * nF);
     q->patchStart = copyOf(m.patch_start, nP);
     q->patchSize = copyOf(m.patch_size, nP);
     const size_t nPb = std::max<size_t>(nP, 1);
