@@ -63,3 +63,24 @@ def test_context_without_device_fails_cleanly():
         raise AssertionError("expected NO_DEVICE")
     except vb.VlmError as e:
         assert e.name in ("NO_DEVICE", "CUDA")
+
+
+def test_topology_matches_reference_on_skewed_meshes():
+    """The library's agglomeration (coarse faces numbered by first occurrence without hashing)
+    against the reference's own buildHierarchy on jittered graded meshes, 3D with a periodic
+    direction and 2D."""
+    import pytest
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("reference library not built here")
+    from voluma_b200 import mesh as vm
+    for n, per, two_d, seed in (((13, 11, 9), (0, 1, 0), False, 3), ((41, 29, 1), (0, 0, 0), True, 4)):
+        pts = vm.jitter_interior(vm.box_points(n, beta=(0.7, 0.0, 0.9 if not two_d else 0.0)), n, 0.2, seed)
+        M = vm.box_mesh(n, periodic=per, points=pts, two_d=two_d)
+        R = ref.RefMesh(n, periodic=per, points=pts, two_d=two_d)
+        t = vb.topology(M["n_cells"], M["owner"], M["neighbour"], M["magSf"], M["ndc"])
+        h = R.gamg_levels()
+        assert len(t) == len(h)
+        for a, b in zip(t, h):
+            for f in ("l", "u", "weight", "agg", "faceMap", "faceFlip"):
+                assert np.array_equal(a[f], b[f].astype(a[f].dtype)), f

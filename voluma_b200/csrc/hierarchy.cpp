@@ -10,7 +10,6 @@
 
 #include <algorithm>
 #include <stdexcept>
-#include <unordered_map>
 
 namespace vlm {
 
@@ -77,26 +76,51 @@ HLevel pairPass(HLevel& L) {
     }
     HLevel C;
     C.n = nAgg;
-    const size_t nf = L.l.size();
-    L.faceMap.assign(nf, -1);
-    L.faceFlip.assign(nf, 0);
-    std::unordered_map<uint64_t, int> seen;
-    seen.reserve(nf);
-    for (size_t f = 0; f < nf; ++f) {
+    const int nf = int(L.l.size());
+    L.faceMap.assign(size_t(nf), -1);
+    L.faceFlip.assign(size_t(nf), 0);
+    // Coarse faces are numbered by the first fine face (in face order) that joins their aggregate
+    // pair.  That first face (the pair's leader) is found without hashing: the fine faces are
+    // bucketed by their lower aggregate (a stable counting sort, so each bucket is in face order)
+    // and each bucket is scanned with a per-aggregate marker of the last bucket that saw it.
+    std::vector<int> start(size_t(nAgg) + 1, 0);
+    for (int f = 0; f < nf; ++f) {
+        const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
+        if (a != b) start[size_t(a < b ? a : b) + 1]++;
+    }
+    for (int c = 0; c < nAgg; ++c) start[c + 1] += start[c];
+    std::vector<int> bucket(static_cast<size_t>(start[nAgg]));
+    {
+        std::vector<int> pos(start.begin(), start.end() - 1);
+        for (int f = 0; f < nf; ++f) {
+            const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
+            if (a != b) bucket[pos[a < b ? a : b]++] = f;
+        }
+    }
+    std::vector<int> leader(size_t(nf), -1), markLo(size_t(nAgg), -1), markFace(size_t(nAgg), -1);
+    for (int lo = 0; lo < nAgg; ++lo)
+        for (int k = start[lo]; k < start[lo + 1]; ++k) {
+            const int f = bucket[k];
+            const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
+            const int hi = a < b ? b : a;
+            if (markLo[hi] != lo) {
+                markLo[hi] = lo;
+                markFace[hi] = f;
+            }
+            leader[f] = markFace[hi];
+        }
+    for (int f = 0; f < nf; ++f) {
         const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
         if (a == b) continue;
         const int lo = a < b ? a : b, hi = a < b ? b : a;
-        const uint64_t key = (uint64_t(uint32_t(lo)) << 32) | uint64_t(uint32_t(hi));
-        auto it = seen.find(key);
         int cf;
-        if (it == seen.end()) {
+        if (leader[f] == f) {
             cf = int(C.l.size());
-            seen.emplace(key, cf);
             C.l.push_back(lo);
             C.u.push_back(hi);
             C.weight.push_back(0.0);
         } else {
-            cf = it->second;
+            cf = L.faceMap[leader[f]];  // the leader precedes f and is numbered already
         }
         L.faceMap[f] = cf;
         L.faceFlip[f] = char(a != lo);
