@@ -135,6 +135,29 @@ vlm_status vlm_mesh_systems(vlm_mesh* mesh, int32_t* n_systems, int64_t* n_cells
                             int64_t* n_faces);
 vlm_status vlm_mesh_release(vlm_mesh* mesh);
 
+/* ------------------------------------------------------------------ device-side box mesh setup */
+/* generateBox (src/fvm/mesh/RawMesh.cpp:391-502, BoxSpec) and the serial Mesh::build geometry
+ * (src/fvm/mesh/Mesh.cpp:21-48, 135-153, 239-320, 600-626) computed by kernels on the context's
+ * device; the arrays equal the reference's bit for bit.  They come back in host memory as a
+ * vlm_mesh_desc (with C, Cf and skewVecs) to pass to vlm_mesh_register; the box owns them. */
+typedef struct {
+    int32_t n[3];          /* cells per direction */
+    double lo[3];
+    double hi[3];
+    int32_t periodic[3];   /* cyclic pairs merged into internal faces */
+    int32_t two_d;         /* n[2] == 1; the z sides become empty and are dropped */
+    double beta[3];        /* tanhStretch grading per direction (RawMesh.cpp:387-389); 0 = uniform */
+    const double* points;  /* optional: (n0+1)(n1+1)(n2+1)*3 vertex coordinates in generateBox order
+                              (host); NULL = the graded box from lo, hi, beta */
+} vlm_box_spec;
+typedef struct vlm_box vlm_box;
+vlm_status vlm_box_create(vlm_ctx* ctx, const vlm_box_spec* spec, vlm_box** out);
+/* desc: pointers into the box's arrays (valid until vlm_box_destroy); patches in side order */
+vlm_status vlm_box_desc(const vlm_box* box, vlm_mesh_desc* desc);
+/* per patch of the desc, its box side: 0 xMin, 1 xMax, 2 yMin, 3 yMax, 4 zMin, 5 zMax */
+vlm_status vlm_box_patch_sides(const vlm_box* box, int32_t* sides);
+vlm_status vlm_box_destroy(vlm_box* box);
+
 /* ------------------------------------------------------------------ linear algebra */
 /* y = A x over the mesh's LDU matrix (host pointers; lower == NULL means symmetric). */
 vlm_status vlm_amul(vlm_ctx* ctx, vlm_mesh* mesh, const double* diag, const double* upper,

@@ -288,6 +288,64 @@ class Mesh:
             pass
 
 
+_BOX_SIDES = ("xMin", "xMax", "yMin", "yMax", "zMin", "zMax")
+
+
+def box_mesh_device(n, lo=(0, 0, 0), hi=(1, 1, 1), periodic=(False, False, False), two_d=False, beta=(0, 0, 0),
+                    points=None, ctx: Context | None = None) -> dict:
+    """generateBox + Mesh::build computed on the device (vlm_box_create): the same dict as
+    voluma_b200.mesh.box_mesh (the cfd::Mesh array names, patches in side order), bit-identical."""
+    ctx = ctx or default_context()
+    L = load()
+    s = _ffi.BoxSpec()
+    for q in range(3):
+        s.n[q] = int(n[q])
+        s.lo[q] = float(lo[q])
+        s.hi[q] = float(hi[q])
+        s.periodic[q] = int(bool(periodic[q]))
+        s.beta[q] = float(beta[q]) if beta[q] else 0.0
+    s.two_d = int(bool(two_d))
+    pts = None
+    if points is not None:
+        pts = _f64(points).reshape(-1)
+        if pts.size != 3 * (int(n[0]) + 1) * (int(n[1]) + 1) * (int(n[2]) + 1):
+            raise ValueError("points must hold (nx+1)(ny+1)(nz+1) vertices")
+        s.points = pts.ctypes.data
+    h = C.c_void_p()
+    check(L.vlm_box_create(ctx.handle, C.byref(s), C.byref(h)), ctx.handle)
+    try:
+        d = _ffi.MeshDesc()
+        check(L.vlm_box_desc(h, C.byref(d)))
+        nC, nI, nF, nP = d.n_cells, d.n_internal_faces, d.n_faces, d.n_patches
+
+        def arr(ptr, n_, dt, shape=None):
+            a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), (n_,)).copy()
+            return a if shape is None else a.reshape(shape)
+
+        sides = np.zeros(max(nP, 1), np.int32)
+        check(L.vlm_box_patch_sides(h, sides.ctypes.data))
+        m = dict(n_cells=nC, n_internal_faces=nI, n_faces=nF, owner=arr(d.owner, nF, np.int32),
+                 neighbour=arr(d.neighbour, nI, np.int32) if nI else np.zeros(0, np.int32),
+                 V=arr(d.V, nC, np.float64), C=arr(d.C, 3 * nC, np.float64, (nC, 3)),
+                 Sf=arr(d.Sf, 3 * nF, np.float64, (nF, 3)), magSf=arr(d.magSf, nF, np.float64),
+                 Cf=arr(d.Cf, 3 * nF, np.float64, (nF, 3)), d=arr(d.d, 3 * nF, np.float64, (nF, 3)),
+                 w=arr(d.w, nF, np.float64), ndc=arr(d.ndc, nF, np.float64),
+                 corrVecs=arr(d.corrVecs, 3 * nF, np.float64, (nF, 3)),
+                 skewVecs=arr(d.skewVecs, 3 * nF, np.float64, (nF, 3)),
+                 patch_start=arr(d.patch_start, nP, np.int32) if nP else np.zeros(0, np.int32),
+                 patch_size=arr(d.patch_size, nP, np.int32) if nP else np.zeros(0, np.int32),
+                 patch_names=[_BOX_SIDES[int(q)] for q in sides[:nP]], two_d=bool(d.two_d),
+                 empty_dir=int(d.empty_dir), shape=tuple(int(v) for v in n),
+                 periodic=tuple(bool(p) for p in periodic))
+    finally:
+        L.vlm_box_destroy(h)
+    sk = m["skewVecs"][:nI]
+    dd = m["d"][:nI]
+    m["skewed"] = bool(nI and (np.sqrt((sk * sk).sum(1)) / np.sqrt((dd * dd).sum(1))).max() > 1e-8)
+    m["deltaCoeffs"] = 1.0 / np.sqrt((m["d"] * m["d"]).sum(1))
+    return m
+
+
 def topology(n_cells, owner, neighbour, magSf, ndc, merge_levels: int = 2):
     """Host-side GAMG hierarchy + colouring exactly as the device uses them (no GPU needed):
     list of dicts n, l, u, weight, agg, faceMap, faceFlip, colour, ncolours."""

@@ -20,7 +20,8 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
            "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
            "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy", "vlm_flow_set_model",
-           "vlm_flow_get_model_state", "vlm_flow_write_restart", "vlm_flow_read_restart"]
+           "vlm_flow_get_model_state", "vlm_flow_write_restart", "vlm_flow_read_restart", "vlm_box_create",
+           "vlm_box_desc", "vlm_box_patch_sides", "vlm_box_destroy"]
 
 
 class MeshDesc(C.Structure):
@@ -30,6 +31,11 @@ class MeshDesc(C.Structure):
                 ("corrVecs", C.c_void_p), ("two_d", C.c_int32), ("empty_dir", C.c_int32), ("n_patches", C.c_int32),
                 ("patch_start", C.c_void_p), ("patch_size", C.c_void_p), ("C", C.c_void_p), ("Cf", C.c_void_p),
                 ("skewVecs", C.c_void_p)]
+
+
+class BoxSpec(C.Structure):
+    _fields_ = [("n", C.c_int32 * 3), ("lo", C.c_double * 3), ("hi", C.c_double * 3), ("periodic", C.c_int32 * 3),
+                ("two_d", C.c_int32), ("beta", C.c_double * 3), ("points", C.c_void_p)]
 
 
 class SolverCtrl(C.Structure):
@@ -147,6 +153,10 @@ def load():
     L.vlm_pressure_solve_batch.argtypes = [P, P, P, P, P, P, P, P, C.c_double, i32, i32, C.POINTER(SolverCtrl),
                                            C.POINTER(SolverCtrl), P, P, i32]
     L.vlm_mesh_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.vlm_box_create.argtypes = [P, C.POINTER(BoxSpec), C.POINTER(P)]
+    L.vlm_box_desc.argtypes = [P, C.POINTER(MeshDesc)]
+    L.vlm_box_patch_sides.argtypes = [P, P]
+    L.vlm_box_destroy.argtypes = [P]
     L.vlm_profile_kernel.argtypes = [P, P, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     for name in EXPORTS:
         keep = ("vlm_last_error", "vlm_ctx_stream", "vlm_flow_request_bytes", "vlm_server_clock", "vlm_flow_launches")

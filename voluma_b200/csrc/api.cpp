@@ -1,6 +1,7 @@
 // extern "C" boundary (include/voluma_b200.h): status codes in, no exceptions out.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -10,6 +11,7 @@
 
 #include "assembly.h"
 #include "flow.h"
+#include "meshgen.h"
 #include "solver.h"
 #include "voluma_b200.h"
 
@@ -649,6 +651,59 @@ vlm_status vlm_mesh_systems(vlm_mesh* m, int32_t* n_systems, int64_t* n_cells, i
     if (n_cells) *n_cells = m->nCells;
     if (n_internal_faces) *n_internal_faces = m->nInternal;
     if (n_faces) *n_faces = m->nFaces;
+    return VLM_OK;
+}
+
+struct vlm_box {
+    vlm::BoxMesh m;
+};
+
+vlm_status vlm_box_create(vlm_ctx* ctx, const vlm_box_spec* spec, vlm_box** out) {
+    if (!ctx || !spec || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        auto b = std::make_unique<vlm_box>();
+        b->m = vlm::buildBoxMesh(*spec, ctx->stream);
+        *out = b.release();
+    });
+}
+
+vlm_status vlm_box_desc(const vlm_box* box, vlm_mesh_desc* d) {
+    if (!box || !d) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    const vlm::BoxMesh& m = box->m;
+    std::memset(d, 0, sizeof *d);
+    d->n_cells = m.nCells;
+    d->n_internal_faces = m.nInternal;
+    d->n_faces = m.nFaces;
+    d->owner = m.owner.data();
+    d->neighbour = m.neighbour.data();
+    d->magSf = m.magSf.data();
+    d->ndc = m.ndc.data();
+    d->V = m.V.data();
+    d->Sf = m.Sf.data();
+    d->d = m.d.data();
+    d->w = m.w.data();
+    d->corrVecs = m.corrVecs.data();
+    d->two_d = m.twoD;
+    d->empty_dir = m.emptyDir;
+    d->n_patches = int32_t(m.patchStart.size());
+    d->patch_start = m.patchStart.data();
+    d->patch_size = m.patchSize.data();
+    d->C = m.C.data();
+    d->Cf = m.Cf.data();
+    d->skewVecs = m.skewVecs.data();
+    return VLM_OK;
+}
+
+vlm_status vlm_box_patch_sides(const vlm_box* box, int32_t* sides) {
+    if (!box || !sides) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    std::copy(box->m.patchSide.begin(), box->m.patchSide.end(), sides);
+    return VLM_OK;
+}
+
+vlm_status vlm_box_destroy(vlm_box* box) {
+    delete box;
     return VLM_OK;
 }
 

@@ -14,11 +14,12 @@
 // (exact sums, diagonal preconditioning) a step reproduces the reference's fields bit for bit.
 //
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
-// linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients, fixedValue and zeroGradient boundary
-// conditions for U and p, empty (2D) directions and cyclic (internal) faces, the LES Smagorinsky model
-// with Van Driest damping and constant / mean-velocity momentum forcing (flow_les.cu).  Not supported
-// (an UNSUPPORTED status): skewed meshes, other turbulence models, wall models, buoyancy body forces,
-// ddtPhiCoeff.
+// linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients,
+// fixedValue, zeroGradient and symmetry boundary conditions for U and p, empty (2D) directions and
+// cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
+// Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
+// constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
+// wall models, buoyancy body forces, ddtPhiCoeff, the leastSquares / GaussSkew gradient schemes.
 #pragma once
 
 #include <cstdint>
