@@ -83,34 +83,43 @@ HLevel pairPass(HLevel& L) {
     // pair.  That first face (the pair's leader) is found without hashing: the fine faces are
     // bucketed by their lower aggregate (a stable counting sort, so each bucket is in face order)
     // and each bucket is scanned with a per-aggregate marker of the last bucket that saw it.
+    std::vector<int> fa(static_cast<size_t>(nf)), fb(static_cast<size_t>(nf));  // each face's two aggregates
     std::vector<int> start(size_t(nAgg) + 1, 0);
     for (int f = 0; f < nf; ++f) {
         const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
+        fa[f] = a;
+        fb[f] = b;
         if (a != b) start[size_t(a < b ? a : b) + 1]++;
     }
     for (int c = 0; c < nAgg; ++c) start[c + 1] += start[c];
-    std::vector<int> bucket(static_cast<size_t>(start[nAgg]));
+    std::vector<int> bucketFace(static_cast<size_t>(start[nAgg])), bucketHi(static_cast<size_t>(start[nAgg]));
     {
         std::vector<int> pos(start.begin(), start.end() - 1);
         for (int f = 0; f < nf; ++f) {
-            const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
-            if (a != b) bucket[pos[a < b ? a : b]++] = f;
+            const int a = fa[f], b = fb[f];
+            if (a == b) continue;
+            const int k = pos[a < b ? a : b]++;
+            bucketFace[k] = f;
+            bucketHi[k] = a < b ? b : a;
         }
     }
     std::vector<int> leader(size_t(nf), -1), markLo(size_t(nAgg), -1), markFace(size_t(nAgg), -1);
+    size_t nCoarseFaces = 0;
     for (int lo = 0; lo < nAgg; ++lo)
         for (int k = start[lo]; k < start[lo + 1]; ++k) {
-            const int f = bucket[k];
-            const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
-            const int hi = a < b ? b : a;
+            const int f = bucketFace[k], hi = bucketHi[k];
             if (markLo[hi] != lo) {
                 markLo[hi] = lo;
                 markFace[hi] = f;
+                ++nCoarseFaces;
             }
             leader[f] = markFace[hi];
         }
+    C.l.reserve(nCoarseFaces);
+    C.u.reserve(nCoarseFaces);
+    C.weight.reserve(nCoarseFaces);
     for (int f = 0; f < nf; ++f) {
-        const int a = L.agg[L.l[f]], b = L.agg[L.u[f]];
+        const int a = fa[f], b = fb[f];
         if (a == b) continue;
         const int lo = a < b ? a : b, hi = a < b ? b : a;
         int cf;
@@ -138,6 +147,9 @@ Hierarchy buildHierarchy(int nCells, int nInternal, const int32_t* own, const in
     HLevel L0;
     L0.n = nCells;
     L0.l.reserve(size_t(nInternal));
+    L0.u.reserve(size_t(nInternal));
+    L0.weight.reserve(size_t(nInternal));
+    H.ownerIsL.reserve(size_t(nInternal));
     for (int f = 0; f < nInternal; ++f) {
         const int o = own[f], n = nei[f];
         if (o < 0 || n < 0 || o >= nCells || n >= nCells || o == n)
