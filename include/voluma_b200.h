@@ -271,7 +271,10 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * registered with geometry (and C / Cf for linearUpwind or LUST); it must outlive the flow.
  * Boundary conditions per patch: 0 zeroGradient, 1 fixedValue (noSlip = fixedValue 0), 2 symmetry
  * (slip plane, SymmetryBC of field/BoundaryCondition.h:194-205: U_b = U_P - (n.U_P) n with the
- * normal part implicit and zero flux; for p the same as zeroGradient).
+ * normal part implicit and zero flux; for p the same as zeroGradient), and for U 3 inletOutlet
+ * (InletOutletBC, BoundaryCondition.h:263-287: inlet value u_value where the face flux at the start
+ * of the step is inflow, zeroGradient elsewhere; the flux is not fixed).  Patch values are uniform;
+ * vlm_flow_set_boundary_values sets them face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
  * reference's fields bit for bit. */
 typedef struct vlm_flow vlm_flow;
@@ -300,6 +303,10 @@ vlm_status vlm_flow_create(vlm_ctx* ctx, vlm_mesh* mesh, const vlm_flow_ctrl* ct
                            const double* u_value, const int32_t* p_type, const double* p_value, vlm_flow** out);
 /* IncompressibleFlow::initialize from host fields: U 3 per cell (NULL: keep), p per cell (NULL: keep). */
 vlm_status vlm_flow_set_state(vlm_flow* flow, const double* U, const double* p);
+/* Face-by-face boundary values (FixedValueBC::values, InletOutletBC refValue): u_face 3 per boundary
+ * face (index f - n_internal_faces) for the fixedValue and inletOutlet U patches, p_face 1 per
+ * boundary face for the fixedValue p patches; faces of other patches are ignored; NULL keeps. */
+vlm_status vlm_flow_set_boundary_values(vlm_flow* flow, const double* u_face, const double* p_face);
 /* One IncompressibleFlow::step(dt) (dt ignored when steady). */
 vlm_status vlm_flow_step(vlm_flow* flow, double dt, vlm_step_info* info);
 /* The steady loop of fvmFlow (apps/fvmFlow/fvmFlow.cpp:611-640): steps until U and p residuals are

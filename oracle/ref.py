@@ -81,7 +81,8 @@ class RefFlowSpec(C.Structure):
                 ("alphaU", C.c_double), ("alphaP", C.c_double), ("nPatches", C.c_int), ("uType", C.c_void_p),
                 ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
-                ("reproducible", C.c_int), ("residualTol", C.c_double), ("divK", C.c_double)]
+                ("reproducible", C.c_int), ("residualTol", C.c_double), ("divK", C.c_double),
+                ("uFace", C.c_void_p), ("pFace", C.c_void_p)]
 
 
 class RefModelSpec(C.Structure):
@@ -199,6 +200,12 @@ class RefMesh:
         sp.reproducible = int(reproducible)
         sp.residualTol = residual_tol
         sp.divK = case.get("div_coeff", 1.0)
+        if case.get("u_face") is not None:  # face-by-face values (boundary faces in mesh order)
+            keep.append(np.ascontiguousarray(case["u_face"], np.float64).reshape(-1))
+            sp.uFace = _p(keep[-1])
+        if case.get("p_face") is not None:
+            keep.append(np.ascontiguousarray(case["p_face"], np.float64).reshape(-1))
+            sp.pFace = _p(keep[-1])
         ran = C.c_int()
         if read_restart is not None or write_restart is not None:
             ms, turb = _model_spec(model or {})

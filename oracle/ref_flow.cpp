@@ -36,7 +36,8 @@ struct RefSolverCtl {
 // Case settings: scheme codes follow Schemes.h (div: 0 upwind, 1 linear, 2 linearUpwind, 3 LUST,
 // 4 limitedLinear divK, 5 vanLeer, 6 MUSCL, 7 minmod;
 // ddt: 0 steadyState, 1 Euler, 2 backward); per patch (mesh patch order) U/p boundary type
-// 0 zeroGradient, 1 fixedValue with the given value.
+// 0 zeroGradient, 1 fixedValue with the given value, 2 symmetry, 3 inletOutlet with the given inlet
+// value (InletOutletBC on the flow's BCContext); uFace / pFace override the values face by face.
 struct RefFlowSpec {
     double nu;
     int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
@@ -52,6 +53,8 @@ struct RefFlowSpec {
     int reproducible;
     double residualTol;  // > 0: stop once U and p residuals are below it (from step 2, fvmFlow.cpp:611-625)
     double divK;         // limitedLinear's k
+    const double* uFace; // optional, 3 per boundary face: values of the fixedValue / inletOutlet U faces
+    const double* pFace; // optional, 1 per boundary face: values of the fixedValue p faces
 };
 
 // Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
@@ -132,21 +135,40 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
         flow.ddtScheme = sp->ddtScheme == 0 ? DdtScheme::Steady : sp->ddtScheme == 1 ? DdtScheme::Euler
                                                                                       : DdtScheme::Backward;
         if (sp->nPatches != int(m.patches().size())) throw std::runtime_error("patch count mismatch");
+        const label nI = m.nInternalFaces();
         for (int q = 0; q < sp->nPatches; ++q) {
             const std::string name = m.patches()[q].name;
             if (m.patches()[q].type == PatchType::Empty || m.patches()[q].type == PatchType::Cyclic) continue;
-            if (sp->uType[q] == 1)
-                flow.U().fixedValue(name, Vec3{sp->uValue[3 * q], sp->uValue[3 * q + 1], sp->uValue[3 * q + 2]});
-            else if (sp->uType[q] == 2)
+            const label start = m.patches()[q].start, size = m.patches()[q].size;
+            const Vec3 uv{sp->uValue[3 * q], sp->uValue[3 * q + 1], sp->uValue[3 * q + 2]};
+            auto uFace = [&](label i) {
+                const double* v = sp->uFace + 3 * (start - nI + i);
+                return Vec3{v[0], v[1], v[2]};
+            };
+            if (sp->uType[q] == 1) {
+                auto& bc = flow.U().set<FixedValueBC<Vec3>>(name, uv);
+                if (sp->uFace)
+                    for (label i = 0; i < size; ++i) bc.values()[i] = uFace(i);
+            } else if (sp->uType[q] == 2) {
                 flow.U().set<SymmetryBC<Vec3>>(name);
-            else
+            } else if (sp->uType[q] == 3) {
+                auto& bc = flow.U().set<InletOutletBC<Vec3>>(name, &flow.context(), uv);
+                if (sp->uFace)
+                    for (label i = 0; i < size; ++i) bc.refValue()[i] = uFace(i);
+            } else {
                 flow.U().zeroGradient(name);
-            if (sp->pType[q] == 1)
-                flow.p().fixedValue(name, sp->pValue[q]);
-            else if (sp->pType[q] == 2)
+            }
+            if (sp->pType[q] == 1) {
+                auto& bc = flow.p().set<FixedValueBC<scalar>>(name, sp->pValue[q]);
+                if (sp->pFace)
+                    for (label i = 0; i < size; ++i) bc.values()[i] = sp->pFace[start - nI + i];
+            } else if (sp->pType[q] == 2) {
                 flow.p().set<SymmetryBC<scalar>>(name);
-            else
+            } else if (sp->pType[q] == 3) {
+                flow.p().set<InletOutletBC<scalar>>(name, &flow.context(), sp->pValue[q]);
+            } else {
                 flow.p().zeroGradient(name);
+            }
         }
         // the turbulence model keeps references to its dictionaries: they live as long as the run
         const Json empty = Json::parse("{}");

@@ -7,7 +7,11 @@ CFD_REPRODUCIBLE mode:
   * slip2d_flat: the same without shear, 4 SIMPLE steps;
   * slip3d: the 8 x 8 x 6 sheared slip cavity (slip x and z walls), transient Euler with nCorr 2,
     3 steps of dt 0.05;
-  * slip2d_default: slip2d in the reference's default (non-reproducible) mode.
+  * slip2d_default: slip2d in the reference's default (non-reproducible) mode;
+  * inlet / inlet_backflow / inlet_transient: the 40 x 10 inlet-outlet channel (parabolic fixedValue
+    inlet given face by face, inletOutlet outlet, InletOutletBC BoundaryCondition.h:263-287), steady
+    SIMPLE 6 steps from U = (1, 0, 0) and from a field with backflow at the outlet, and transient
+    Euler (nCorr 2, 3 steps of dt 0.02) from the backflow field.
 Run where the reference sources are present:
     make -C oracle && python tests/golden/make_bc_golden.py
 """
@@ -35,6 +39,15 @@ CASES = {
 }
 
 
+INLET = {
+    # tag: (backflow, case transform, steps, dt)
+    "inlet": (0.0, dict, 6, 1.0),
+    "inlet_backflow": (0.5, dict, 6, 1.0),
+    "inlet_transient": (0.5, lambda c: dict(c, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0), 3,
+                        0.02),
+}
+
+
 def main():
     out = {}
     for tag, (n, shear, tf, steps, dt) in CASES.items():
@@ -47,6 +60,11 @@ def main():
     R = ref.RefMesh((16, 16, 1), points=pts, two_d=True)
     U, p, phi, hist = R.flow_run(case, 6)
     out.update(slip2d_default_U=U, slip2d_default_p=p, slip2d_default_phi=phi, slip2d_default_hist=hist)
+    for tag, (backflow, tf, steps, dt) in INLET.items():
+        m, case, U0 = cases.channel_inlet((40, 10, 1), backflow=backflow)
+        R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
+        U, p, phi, hist = R.flow_run(tf(case), steps, dt=dt, U=U0, reproducible=True)
+        out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))
 

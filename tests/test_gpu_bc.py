@@ -95,3 +95,54 @@ def test_slip_cavity_default_mode_close(gold):
     ref = gold["slip2d_default_U"]
     assert np.abs(U - ref).max() < 5e-3 * np.abs(ref).max()
     assert np.abs(phi[slip_faces(m)]).max() < 1e-15
+
+
+INLET = {
+    "inlet": (0.0, dict, 6, 1.0),
+    "inlet_backflow": (0.5, dict, 6, 1.0),
+    "inlet_transient": (0.5, lambda c: dict(c, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0), 3,
+                        0.02),
+}
+
+
+def test_inlet_case_layout():
+    m, case, U0 = cases.channel_inlet((40, 10, 1), backflow=0.5)
+    names = list(m["patch_names"])
+    assert int(case["u_type"][names.index("xMax")]) == 3 and int(case["p_type"][names.index("xMax")]) == 1
+    nI = m["n_internal_faces"]
+    q = names.index("xMin")
+    f = np.arange(m["patch_start"][q], m["patch_start"][q] + m["patch_size"][q]) - nI
+    assert case["u_face"][f, 0].min() > 0 and np.abs(case["u_face"][f, 1:]).max() == 0
+    assert (U0[:, 0] < 0).any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", sorted(INLET))
+def test_inlet_outlet_channel_bitwise(gold, tag):
+    # fixedValue inlet given face by face (vlm_flow_set_boundary_values) and an inletOutlet outlet whose
+    # inflow faces (backflow) switch to the inlet value
+    backflow, tf, steps, dt = INLET[tag]
+    m, case, U0 = cases.channel_inlet((40, 10, 1), backflow=backflow)
+    fl = vb.Flow(vb.Mesh.from_arrays(m), dict(tf(case), reproducible=True))
+    fl.set_state(U0, None)
+    hist = []
+    for _ in range(steps):
+        i = fl.step(dt)
+        hist.append([i["UInitialResidual"], i["pInitialResidual"], i["continuityError"]])
+    U, p, phi = fl.state()
+    fl.close()
+    assert np.array_equal(np.array(hist), gold[f"{tag}_hist"][:, :3])
+    assert np.array_equal(U, gold[f"{tag}_U"])
+    assert np.array_equal(p, gold[f"{tag}_p"])
+    assert np.array_equal(phi, gold[f"{tag}_phi"])
+
+
+@pytest.mark.gpu
+def test_flow_rejects_unknown_boundary_types():
+    m, case, _ = cases.channel_inlet((8, 4, 1))
+    bad = dict(case, u_type=np.full(len(case["u_type"]), 4, np.int32))
+    with pytest.raises(vb.VlmError):
+        vb.Flow(vb.Mesh.from_arrays(m), bad)
+    bad = dict(case, p_type=np.full(len(case["p_type"]), 3, np.int32))
+    with pytest.raises(vb.VlmError):
+        vb.Flow(vb.Mesh.from_arrays(m), bad)

@@ -547,8 +547,9 @@ class Flow:
     """IncompressibleFlow (solvers/IncompressibleFlow.h) on the device for a registered single-system mesh
     with geometry.  `case`: dict with nu, steady, div_scheme, ddt_scheme, n_outer, n_corr,
     n_non_orth_corr, momentum_predictor, alpha_u, alpha_p, p_ref_cell, p_ref_value, U / p / pFinal solver
-    dictionaries, per-patch u_type / u_value / p_type / p_value and optionally reproducible
-    (voluma_b200.cases.lid_cavity builds one)."""
+    dictionaries, per-patch u_type / u_value / p_type / p_value and optionally reproducible and the
+    face-by-face boundary values u_face / p_face (set_boundary_values) (voluma_b200.cases.lid_cavity
+    builds one)."""
 
     def __init__(self, mesh: Mesh, case: dict):
         self.mesh = mesh
@@ -562,12 +563,22 @@ class Flow:
                                      C.byref(h)), mesh.ctx.handle)
         self._h = h
         _live.add(self)
+        if case.get("u_face") is not None or case.get("p_face") is not None:
+            self.set_boundary_values(case.get("u_face"), case.get("p_face"))
 
     def set_state(self, U=None, p=None):
         Ua = None if U is None else _f64(U).reshape(-1)
         pa = None if p is None else _f64(p)
         check(load().vlm_flow_set_state(self._h, None if Ua is None else Ua.ctypes.data,
                                         None if pa is None else pa.ctypes.data), self.mesh.ctx.handle)
+
+    def set_boundary_values(self, u_face=None, p_face=None):
+        """Face-by-face values of the fixedValue / inletOutlet U patches (n_boundary x 3) and of the
+        fixedValue p patches (n_boundary), boundary faces in mesh order (vlm_flow_set_boundary_values)."""
+        ua = None if u_face is None else _f64(u_face).reshape(-1)
+        pa = None if p_face is None else _f64(p_face).reshape(-1)
+        check(load().vlm_flow_set_boundary_values(self._h, None if ua is None else ua.ctypes.data,
+                                                  None if pa is None else pa.ctypes.data), self.mesh.ctx.handle)
 
     def step(self, dt=1.0) -> dict:
         i = _ffi.StepInfo()

@@ -21,7 +21,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_flow_request_bytes", "vlm_server_create", "vlm_server_clock", "vlm_server_submit",
            "vlm_server_collect", "vlm_server_result_fields", "vlm_server_destroy", "vlm_flow_set_model",
            "vlm_flow_get_model_state", "vlm_flow_write_restart", "vlm_flow_read_restart", "vlm_box_create",
-           "vlm_box_desc", "vlm_box_patch_sides", "vlm_box_destroy"]
+           "vlm_box_desc", "vlm_box_patch_sides", "vlm_box_destroy", "vlm_flow_set_boundary_values"]
 
 
 class MeshDesc(C.Structure):
@@ -114,6 +114,7 @@ def load():
     L.vlm_precond_apply.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl)]
     L.vlm_flow_create.argtypes = [P, P, C.POINTER(FlowCtrl), P, P, P, P, C.POINTER(P)]
     L.vlm_flow_set_state.argtypes = [P, P, P]
+    L.vlm_flow_set_boundary_values.argtypes = [P, P, P]
     L.vlm_flow_step.argtypes = [P, C.c_double, C.POINTER(StepInfo)]
     L.vlm_flow_run_steady.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_int32), C.POINTER(StepInfo)]
     L.vlm_flow_get_state.argtypes = [P, P, P, P]

@@ -217,6 +217,41 @@ def skewed_cavity(n=(16, 16, 1), jitter=0.2, seed=20261203, Re=100.0, lid=1.0):
     return m, case, pts
 
 
+def channel_inlet(n=(80, 20, 1), ubulk=1.0, nu=0.05, backflow=0.0):
+    """The plane channel with an inlet and an outlet of the reference's cases/channelInlet/parabolic.json:
+    the 2D box 4 x 1 (0.1 deep), walls yMin / yMax (no slip), the xMin inlet with the parabolic profile
+    u = 1.5 ubulk (1 - s^2), s = (y - 0.5) / 0.5, given face by face (u_face) and zeroGradient p, the
+    xMax outlet with inletOutlet U (inlet value 0) and fixedValue p = 0; nu 0.05 (Re_h = 20), steady
+    SIMPLE with linear divergence.  Initial field U = (ubulk, 0, 0); backflow > 0 reverses the upper
+    half of the last tenth of the channel to -backflow, so that the outlet starts with inflow faces.
+    Returns (mesh, case, U0)."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    m = vm.box_mesh((nx, ny, nz), hi=(4.0, 1.0, 0.1), two_d=True)
+    names = list(m["patch_names"])
+    nP = len(names)
+    u_type = np.array([{"xMin": 1, "xMax": 3}.get(nm, 1) for nm in names], np.int32)
+    p_type = np.array([1 if nm == "xMax" else 0 for nm in names], np.int32)
+    nI = m["n_internal_faces"]
+    nB = m["n_faces"] - nI
+    u_face = np.zeros((nB, 3))
+    q = names.index("xMin")
+    f = np.arange(m["patch_start"][q], m["patch_start"][q] + m["patch_size"][q])
+    s = (m["Cf"][f, 1] - 0.5) / 0.5
+    u_face[f - nI, 0] = 1.5 * ubulk * np.maximum(1.0 - s * s, 0.0)
+    case = dict(nu=nu, steady=True, div_scheme=1, ddt_scheme=0, n_outer=1, n_corr=1, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=0.7, alpha_p=0.3, u_type=u_type, u_value=np.zeros(3 * nP),
+                p_type=p_type, p_value=np.zeros(nP), u_face=u_face,
+                U=_ctl("PBiCGStab", "DILU", 1e-10, 0.1, 1000), p=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000),
+                pFinal=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000), p_ref_cell=0, p_ref_value=0.0)
+    U0 = np.zeros((m["n_cells"], 3))
+    U0[:, 0] = ubulk
+    if backflow > 0:
+        C = m["C"]
+        U0[(C[:, 0] > 3.6) & (C[:, 1] > 0.5), 0] = -backflow
+    return m, case, U0
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

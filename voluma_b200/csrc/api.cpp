@@ -750,6 +750,14 @@ vlm_status vlm_flow_set_state(vlm_flow* f, const double* U, const double* p) {
     });
 }
 
+vlm_status vlm_flow_set_boundary_values(vlm_flow* f, const double* u_face, const double* p_face) {
+    if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(f->mesh->ctx, [&] {
+        setDevice(f->mesh->ctx);
+        f->flow->setBoundaryValues(u_face, p_face);
+    });
+}
+
 vlm_status vlm_flow_step(vlm_flow* f, double dt, vlm_step_info* info) {
     if (!f) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
     return guarded(f->mesh->ctx, [&] {

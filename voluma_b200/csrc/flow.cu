@@ -42,13 +42,20 @@ __device__ __forceinline__ double tvd_limiter(int scheme, double k, double r) {
 // owner's; symmetry u - (n.u) n with n = S_f / |S_f| (SymmetryBC<Vec3>::evaluate, VolField.h:164-170)
 __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __restrict__ own,
                              const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
-                             const double* __restrict__ uValue, const double* __restrict__ Sf,
-                             const double* __restrict__ magSf, const double* __restrict__ U,
-                             double* __restrict__ Ub) {
+                             const double* __restrict__ uValueB, const double* __restrict__ Sf,
+                             const double* __restrict__ magSf, const double* __restrict__ ndc,
+                             const double* __restrict__ wIO, const double* __restrict__ U, double* __restrict__ Ub) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int q = bPatch[b];
     const int c = own[nI + b];
+    if (uType[q] == 3) {
+        // inletOutlet = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
+        const double w = wIO[b], dc = ndc[nI + b];
+        for (int k = 0; k < 3; ++k)
+            Ub[k * nB + b] = w * uValueB[k * nB + b] + (1.0 - w) * (U[k * nC + c] + 0.0 / dc);
+        return;
+    }
     if (uType[q] == 2) {
         const int f = nI + b;
         const double A = magSf[f];
@@ -58,7 +65,15 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
         for (int k = 0; k < 3; ++k) Ub[k * nB + b] = u[k] - dnu * n[k];
         return;
     }
-    for (int k = 0; k < 3; ++k) Ub[k * nB + b] = uType[q] == 1 ? uValue[3 * q + k] : U[k * nC + c];
+    for (int k = 0; k < 3; ++k) Ub[k * nB + b] = uType[q] == 1 ? uValueB[k * nB + b] : U[k * nC + c];
+}
+
+// inletOutlet value fractions at the start of a step (InletOutletBC::update, BoundaryCondition.h:277-282):
+// 1 where the face flux is inflow (phi < 0), else 0
+__global__ void k_io_fraction(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                              const double* __restrict__ phi, double* __restrict__ wIO) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nB && uType[bPatch[b]] == 3) wIO[b] = phi[nI + b] < 0 ? 1.0 : 0.0;
 }
 
 // ---------------------------------------------------------------- fvc::grad of U (Gauss linear)
@@ -210,7 +225,8 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
 // others 0 (BoundaryCondition.h:104-130).  UEqn = (0 + div) - laplacian.
 __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __restrict__ own,
                              const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
-                             const double* __restrict__ uValue, const double* __restrict__ Sf,
+                             const double* __restrict__ uValueB, const double* __restrict__ wIO,
+                             const double* __restrict__ Sf,
                              const double* __restrict__ magSf, const double* __restrict__ ndc,
                              const double* __restrict__ phi, double nu, const double* __restrict__ nuF,
                              const double* __restrict__ U, double* __restrict__ ic, double* __restrict__ bs) {
@@ -232,9 +248,17 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
         dnu = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
     }
     for (int k = 0; k < 3; ++k) {
-        const double val = fixedValue ? uValue[3 * q + k] : 0.0;
+        const double val = fixedValue ? uValueB[k * nB + b] : 0.0;
         double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
         double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
+        if (uType[q] == 3) {
+            // inletOutlet = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
+            const double w = wIO[b], rv = uValueB[k * nB + b], rg = 0.0;
+            vic = 1.0 - w;
+            vbc = w * rv + (1.0 - w) * (rg / dc);
+            gic = -w * dc;
+            gbc = w * dc * rv + (1.0 - w) * rg;
+        }
         if (symmetry) {
             const double nn = n[k] * n[k];
             vic = 1.0 - nn;
@@ -471,10 +495,10 @@ __global__ void k_grad_ls_cells(int nC, int nI, int nF, int nB, const int32_t* _
 // HbyA boundary values of the skew-corrected Rhie-Chow flux on fixes-flux faces: U_b + rAU_P grad p_P
 // (IncompressibleFlow.cpp:262-272); gp: 3 per cell
 __global__ void k_hbya_bval(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
-                            const int32_t* __restrict__ uType, const double* __restrict__ Ub,
+                            const int32_t* __restrict__ fixesFlux, const double* __restrict__ Ub,
                             const double* __restrict__ rAU, const double* __restrict__ gp, double* __restrict__ hB) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nB || uType[bPatch[b]] == 0) return;
+    if (b >= nB || !fixesFlux[bPatch[b]]) return;
     const int o = own[nI + b];
     for (int j = 0; j < 3; ++j) hB[size_t(j) * nB + b] = Ub[size_t(j) * nB + b] + rAU[o] * gp[3 * size_t(o) + j];
 }
@@ -512,7 +536,7 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     } else {
         const int b = f - nI;
         rAUf[f] = rAU[o];
-        if (uType[bPatch[b]] != 0)  // fixesFlux: fixedValue and symmetry (BoundaryCondition.h:76, 203)
+        if (uType[bPatch[b]] == 1 || uType[bPatch[b]] == 2)  // fixesFlux (BoundaryCondition.h:76, 203, 251)
             phiHbyA[f] = Ub[b] * S[0] + Ub[size_t(nB) + b] * S[1] + Ub[size_t(2) * nB + b] * S[2];
         else
             phiHbyA[f] = HbyA[o] * S[0] + HbyA[size_t(nC) + o] * S[1] + HbyA[size_t(2) * nC + o] * S[2];
@@ -607,7 +631,6 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     VLM_REQUIRE(ctrl_.div_scheme >= 0 && ctrl_.div_scheme <= 7, VLM_ERR_BAD_ARG, "unknown divergence scheme");
     if (ctrl_.div_coeff == 0) ctrl_.div_coeff = 1.0;
     VLM_REQUIRE(ctrl_.ddt_scheme >= 0 && ctrl_.ddt_scheme <= 2, VLM_ERR_BAD_ARG, "unknown ddt scheme");
-    VLM_REQUIRE(!ctrl_.steady || ctrl_.ddt_scheme == 0 || true, VLM_ERR_BAD_ARG, "");
     VLM_REQUIRE(ctrl_.nu > 0, VLM_ERR_BAD_ARG, "nu must be positive");
     VLM_REQUIRE(ctrl_.n_corr >= 1 && ctrl_.n_outer >= 1 && ctrl_.n_non_orth_corr >= 0, VLM_ERR_BAD_ARG,
                 "nOuter, nCorr must be >= 1 and nNonOrthCorr >= 0");
@@ -617,7 +640,8 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     uTypeHost_.assign(uType, uType + nP);
     pTypeHost_.assign(pType, pType + nP);
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 2, VLM_ERR_BAD_ARG, "U boundary type must be 0, 1 or 2");
+        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 3, VLM_ERR_BAD_ARG, "U boundary type must be 0, 1, 2 or 3");
+        if (uType[q] == 3) hasInletOutlet_ = true;
         VLM_REQUIRE(pType[q] >= 0 && pType[q] <= 2, VLM_ERR_BAD_ARG, "p boundary type must be 0, 1 or 2");
     }
     // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
@@ -629,11 +653,23 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     for (int k = 0; k < 3; ++k)
         if (!G_.twoD() || k != G_.emptyDir()) solved_.push_back(k);  // Mesh.cpp:642-644
     uType_.upload(uTypeHost_, s_);
-    uValue_.upload(uValue, size_t(3) * std::max(nP, 1), s_);
-    std::vector<double> pv(size_t(std::max(nB_, 1)), 0.0);
+    // fixesFlux per patch (BoundaryCondition.h:76, 203, 251): fixedValue and symmetry
+    std::vector<int32_t> fix(size_t(std::max(nP, 1)), 0);
+    for (int q = 0; q < nP; ++q) fix[q] = uType[q] == 1 || uType[q] == 2;
+    uFixesFlux_.upload(fix, s_);
+    // per boundary face: U values of fixedValue faces and inlet values of inletOutlet faces (SoA), p values
+    const size_t nBb = size_t(std::max(nB_, 1));
+    std::vector<double> uv(3 * nBb, 0.0), pv(nBb, 0.0);
     for (int q = 0; q < nP; ++q)
-        for (int i = 0; i < G_.patchSize()[q]; ++i) pv[size_t(G_.patchStart()[q] - nI_ + i)] = pValue[q];
+        for (int i = 0; i < G_.patchSize()[q]; ++i) {
+            const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
+            for (int k = 0; k < 3; ++k) uv[k * nBb + b] = uValue[3 * q + k];
+            pv[b] = pValue[q];
+        }
+    uValueB_.upload(uv, s_);
     pValueB_.upload(pv, s_);
+    wIO_.resize(nBb);
+    wIO_.zero(s_);
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1)), FI = size_t(std::max(nI_, 1)), F = size_t(nF_);
     for (DBuf<double>* b : {&U_, &U0_, &U00_, &src_, &msrc_, &HbyA_}) b->resize(3 * N);
     for (DBuf<double>* b : {&Ub_, &ic_, &bs_}) b->resize(3 * B);
@@ -712,7 +748,47 @@ bool DeviceFlow::componentBatch() {
 void DeviceFlow::boundaryU() {
     if (nB_ > 0)
         k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
-                                                uValue_.get(), G_.Sf(), G_.magSf(), U_.get(), Ub_.get()), ++launches_;
+                                                uValueB_.get(), G_.Sf(), G_.magSf(), G_.ndc(), wIO_.get(), U_.get(),
+                                                Ub_.get()), ++launches_;
+}
+
+void DeviceFlow::ioFractions() {
+    if (hasInletOutlet_ && nB_ > 0)
+        k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), phi_.get(), wIO_.get()),
+            ++launches_;
+}
+
+void DeviceFlow::setBoundaryValues(const double* uFace, const double* pFace) {
+    const size_t nBb = size_t(std::max(nB_, 1));
+    if (uFace && nB_ > 0) {
+        std::vector<double> uv(3 * nBb);
+        VLM_CUDA(cudaMemcpyAsync(uv.data(), uValueB_.get(), sizeof(double) * uv.size(), cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+        for (int q = 0; q < G_.nPatches(); ++q) {
+            if (uTypeHost_[q] != 1 && uTypeHost_[q] != 3) continue;
+            for (int i = 0; i < G_.patchSize()[q]; ++i) {
+                const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
+                for (int k = 0; k < 3; ++k) uv[k * nBb + b] = uFace[3 * b + k];
+            }
+        }
+        uValueB_.upload(uv, s_);
+    }
+    if (pFace && nB_ > 0) {
+        std::vector<double> pv(nBb);
+        VLM_CUDA(cudaMemcpyAsync(pv.data(), pValueB_.get(), sizeof(double) * pv.size(), cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+        for (int q = 0; q < G_.nPatches(); ++q) {
+            if (pTypeHost_[q] != 1) continue;
+            for (int i = 0; i < G_.patchSize()[q]; ++i) {
+                const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
+                pv[b] = pFace[b];
+            }
+        }
+        pValueB_.upload(pv, s_);
+    }
+    boundaryU();
+    boundaryP();
+    VLM_CUDA(cudaStreamSynchronize(s_));
 }
 
 void DeviceFlow::boundaryP() {
@@ -736,6 +812,7 @@ void DeviceFlow::setState(const double* U, const double* p) {
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
     if (p) p_.upload(p, size_t(nC_), s_);
+    wIO_.zero(s_);  // initialize(): no flux yet, every inletOutlet face evaluates as outflow
     boundaryU();
     boundaryP();
     if (G_.skewed()) gradU();
@@ -880,6 +957,7 @@ bool DeviceFlow::readRestart(const std::string& dir) {
         VLM_CUDA(cudaMemcpyAsync(forceState_.get(), &gp, sizeof(double), cudaMemcpyHostToDevice, s_));
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
+    ioFractions();  // markRestarted: updateBCs with the restart's flux
     boundaryU();
     boundaryP();
     VLM_CUDA(cudaStreamSynchronize(s_));
@@ -903,7 +981,7 @@ void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
                                               skewLin ? cSkew_.get() : nullptr, ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
-                                               uValue_.get(), G_.Sf(), G_.magSf(), G_.ndc(), phi_.get(), ctrl_.nu,
+                                               uValueB_.get(), wIO_.get(), G_.Sf(), G_.magSf(), G_.ndc(), phi_.get(), ctrl_.nu,
                                                nuF, U_.get(), ic_.get(), bs_.get()), ++launches_;
     // ddt coefficients (Schemes.h:70-86)
     double kc = 0, kc0 = 0, kc00 = 0;
@@ -997,7 +1075,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
         // boundaries; grad HbyA by least squares with the fixes-flux faces at U_b + rAU_P grad p_P
         G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
         if (nB_ > 0)
-            k_hbya_bval<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.own(), G_.bPatch(), uType_.get(), Ub_.get(),
+            k_hbya_bval<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.own(), G_.bPatch(), uFixesFlux_.get(), Ub_.get(),
                                                   rAU_.get(), gP_.get(), hB_.get()), ++launches_;
         k_grad_ls_cells<1><<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
                                                      G_.nei(), G_.Sf(), G_.magSf(), G_.d(), rAU_.get(), nullptr,
@@ -1005,7 +1083,8 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
             ++launches_;
         k_grad_ls_cells<3><<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
                                                      G_.nei(), G_.Sf(), G_.magSf(), G_.d(), HbyA_.get(), hB_.get(),
-                                                     G_.bPatch(), uType_.get(), G_.twoD(), G_.emptyDir(), gH_.get()),
+                                                     G_.bPatch(), uFixesFlux_.get(), G_.twoD(), G_.emptyDir(),
+                                                     gH_.get()),
             ++launches_;
     }
     k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
@@ -1061,6 +1140,7 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
         VLM_CUDA(cudaMemcpyAsync(U0_.get(), U_.get(), sizeof(double) * 3 * nC_, cudaMemcpyDeviceToDevice, s_));
         VLM_CUDA(cudaMemcpyAsync(phiOld_.get(), phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToDevice, s_));
     }
+    ioFractions();
     boundaryU();
     boundaryP();
     nSolves_ = 0;

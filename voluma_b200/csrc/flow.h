@@ -15,7 +15,8 @@
 //
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
 // linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients,
-// fixedValue, zeroGradient and symmetry boundary conditions for U and p, empty (2D) directions and
+// fixedValue (uniform or face by face), zeroGradient and symmetry boundary conditions for U and p and
+// inletOutlet for U, empty (2D) directions and
 // cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
 // Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
 // constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
@@ -44,6 +45,9 @@ public:
 
     // IncompressibleFlow::initialize (IncompressibleFlow.cpp:32-40) from host fields (U: 3 per cell)
     void setState(const double* U, const double* p);
+    // Per boundary face (index f - nInternal) values of the fixedValue / inletOutlet U faces (3 each,
+    // AoS) and of the fixedValue p faces; NULL keeps the current values.
+    void setBoundaryValues(const double* uFace, const double* pFace);
     // IncompressibleFlow::step(dt)
     vlm_step_info step(double dt);
     // fields to host (any pointer may be null)
@@ -60,6 +64,7 @@ public:
 
 private:
     void boundaryU();
+    void ioFractions();
     void boundaryP();
     void gradU();
     void assembleMomentum(double aU, bool haveGradU);
@@ -112,7 +117,10 @@ private:
     std::vector<int32_t> uTypeHost_, pTypeHost_;
     std::vector<int> solved_;
     DBuf<int32_t> uType_;
-    DBuf<double> uValue_, pValueB_;
+    DBuf<double> uValueB_, pValueB_;  // per boundary face: U values (SoA) / inlet values, p values
+    DBuf<double> wIO_;                // inletOutlet value fraction per boundary face (phi < 0 at step start)
+    DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry)
+    bool hasInletOutlet_ = false;
     // fields (vectors SoA: component k at [k * n])
     DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_, phiOld_, phiOldOld_;
     // momentum matrix: UEqn (diag, upper, lower, source, internalCoeffs, boundarySource)
