@@ -271,10 +271,14 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * registered with geometry (and C / Cf for linearUpwind or LUST); it must outlive the flow.
  * Boundary conditions per patch: 0 zeroGradient, 1 fixedValue (noSlip = fixedValue 0), 2 symmetry
  * (slip plane, SymmetryBC of field/BoundaryCondition.h:194-205: U_b = U_P - (n.U_P) n with the
- * normal part implicit and zero flux; for p the same as zeroGradient), and for U 3 inletOutlet
+ * normal part implicit and zero flux; for p the same as zeroGradient), 3 inletOutlet for U
  * (InletOutletBC, BoundaryCondition.h:263-287: inlet value u_value where the face flux at the start
- * of the step is inflow, zeroGradient elsewhere; the flux is not fixed).  Patch values are uniform;
- * vlm_flow_set_boundary_values sets them face by face (profiles such as a parabolic inlet).
+ * of the step is inflow, zeroGradient elsewhere; the flux is not fixed), 4 freestream (U: value
+ * fraction 1/2 - (U_inf.n)/(2|U_inf|) towards u_value = U_inf, BoundaryCondition.h:289-302; p:
+ * freestreamPressure towards p_value with fraction 1/2 + (U_inf.n)/(2|U_inf|), U_inf from the U
+ * freestream condition of the same patch, :304-320), 5 fixedGradient (the value is the normal
+ * gradient, :140-153).  Patch values are uniform; vlm_flow_set_boundary_values sets the fixedValue
+ * and inletOutlet values face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
  * reference's fields bit for bit. */
 typedef struct vlm_flow vlm_flow;

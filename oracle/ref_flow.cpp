@@ -37,7 +37,9 @@ struct RefSolverCtl {
 // 4 limitedLinear divK, 5 vanLeer, 6 MUSCL, 7 minmod;
 // ddt: 0 steadyState, 1 Euler, 2 backward); per patch (mesh patch order) U/p boundary type
 // 0 zeroGradient, 1 fixedValue with the given value, 2 symmetry, 3 inletOutlet with the given inlet
-// value (InletOutletBC on the flow's BCContext); uFace / pFace override the values face by face.
+// value (InletOutletBC on the flow's BCContext), 4 freestream (U: the free-stream velocity; p:
+// freestreamPressure with the p value and the U free-stream velocity of the patch), 5 fixedGradient
+// (the value is the gradient); uFace / pFace override the values face by face.
 struct RefFlowSpec {
     double nu;
     int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
@@ -155,6 +157,10 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 auto& bc = flow.U().set<InletOutletBC<Vec3>>(name, &flow.context(), uv);
                 if (sp->uFace)
                     for (label i = 0; i < size; ++i) bc.refValue()[i] = uFace(i);
+            } else if (sp->uType[q] == 4) {
+                flow.U().set<FreestreamVelocityBC>(name, uv);
+            } else if (sp->uType[q] == 5) {
+                flow.U().set<FixedGradientBC<Vec3>>(name, uv);
             } else {
                 flow.U().zeroGradient(name);
             }
@@ -166,6 +172,10 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.p().set<SymmetryBC<scalar>>(name);
             } else if (sp->pType[q] == 3) {
                 flow.p().set<InletOutletBC<scalar>>(name, &flow.context(), sp->pValue[q]);
+            } else if (sp->pType[q] == 4) {
+                flow.p().set<FreestreamPressureBC>(name, &flow.context(), sp->pValue[q], &uv);
+            } else if (sp->pType[q] == 5) {
+                flow.p().set<FixedGradientBC<scalar>>(name, sp->pValue[q]);
             } else {
                 flow.p().zeroGradient(name);
             }

@@ -11,7 +11,12 @@ CFD_REPRODUCIBLE mode:
   * inlet / inlet_backflow / inlet_transient: the 40 x 10 inlet-outlet channel (parabolic fixedValue
     inlet given face by face, inletOutlet outlet, InletOutletBC BoundaryCondition.h:263-287), steady
     SIMPLE 6 steps from U = (1, 0, 0) and from a field with backflow at the outlet, and transient
-    Euler (nCorr 2, 3 steps of dt 0.02) from the backflow field.
+    Euler (nCorr 2, 3 steps of dt 0.02) from the backflow field;
+  * freestream: a vortex carried through the 32 x 16 box with freestream U / freestreamPressure p on
+    every side (FreestreamVelocityBC, FreestreamPressureBC, BoundaryCondition.h:289-320), transient
+    Euler, 4 steps of dt 0.02;
+  * gradient: the inlet-outlet channel with fixedGradient p at the inlet and fixedGradient U at the
+    outlet (FixedGradientBC, BoundaryCondition.h:140-153), steady SIMPLE, 6 steps.
 Run where the reference sources are present:
     make -C oracle && python tests/golden/make_bc_golden.py
 """
@@ -65,6 +70,14 @@ def main():
         R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
         U, p, phi, hist = R.flow_run(tf(case), steps, dt=dt, U=U0, reproducible=True)
         out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
+    m, case, U0 = cases.freestream_box()
+    R = ref.RefMesh((32, 16, 1), hi=(2.0, 1.0, 0.1), two_d=True)
+    U, p, phi, hist = R.flow_run(case, 4, dt=0.02, U=U0, reproducible=True)
+    out.update(freestream_U=U, freestream_p=p, freestream_phi=phi, freestream_hist=hist)
+    m, case, U0 = cases.channel_gradient()
+    R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
+    U, p, phi, hist = R.flow_run(case, 6, U=U0, reproducible=True)
+    out.update(gradient_U=U, gradient_p=p, gradient_phi=phi, gradient_hist=hist)
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))
 

@@ -140,9 +140,44 @@ def test_inlet_outlet_channel_bitwise(gold, tag):
 @pytest.mark.gpu
 def test_flow_rejects_unknown_boundary_types():
     m, case, _ = cases.channel_inlet((8, 4, 1))
-    bad = dict(case, u_type=np.full(len(case["u_type"]), 4, np.int32))
+    bad = dict(case, u_type=np.full(len(case["u_type"]), 6, np.int32))
     with pytest.raises(vb.VlmError):
         vb.Flow(vb.Mesh.from_arrays(m), bad)
     bad = dict(case, p_type=np.full(len(case["p_type"]), 3, np.int32))
     with pytest.raises(vb.VlmError):
         vb.Flow(vb.Mesh.from_arrays(m), bad)
+    # freestreamPressure takes its direction from a freestream velocity on the same patch
+    bad = dict(case, p_type=np.full(len(case["p_type"]), 4, np.int32))
+    with pytest.raises(vb.VlmError):
+        vb.Flow(vb.Mesh.from_arrays(m), bad)
+
+
+def run_case(m, case, U0, steps, dt):
+    fl = vb.Flow(vb.Mesh.from_arrays(m), dict(case, reproducible=True))
+    fl.set_state(U0, None)
+    hist = []
+    for _ in range(steps):
+        i = fl.step(dt)
+        hist.append([i["UInitialResidual"], i["pInitialResidual"], i["continuityError"]])
+    U, p, phi = fl.state()
+    fl.close()
+    return U, p, phi, np.array(hist)
+
+
+@pytest.mark.gpu
+def test_freestream_box_bitwise(gold):
+    # freestream U / freestreamPressure p on every side, fractional value fractions on the oblique sides
+    m, case, U0 = cases.freestream_box()
+    U, p, phi, hist = run_case(m, case, U0, 4, 0.02)
+    assert np.array_equal(hist, gold["freestream_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"freestream_{k}"]), k
+
+
+@pytest.mark.gpu
+def test_fixed_gradient_channel_bitwise(gold):
+    m, case, U0 = cases.channel_gradient()
+    U, p, phi, hist = run_case(m, case, U0, 6, 1.0)
+    assert np.array_equal(hist, gold["gradient_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"gradient_{k}"]), k

@@ -252,6 +252,48 @@ def channel_inlet(n=(80, 20, 1), ubulk=1.0, nu=0.05, backflow=0.0):
     return m, case, U0
 
 
+def freestream_box(n=(32, 16, 1), uinf=(1.0, 0.2, 0.0), nu=0.01, vortex=0.5):
+    """A vortex carried through a 2D box 2 x 1 (0.1 deep) whose four sides are free-stream boundaries:
+    U freestream (FreestreamVelocityBC: inflow faces fixed at uinf, outflow faces zero gradient, with the
+    value fraction 1/2 - (uinf.n)/(2|uinf|)) and p freestreamPressure at 0 (fraction 1/2 + (uinf.n) /
+    (2|uinf|)); uinf oblique so that the side fractions are fractional.  Transient Euler PISO (nCorr 2),
+    linear divergence.  Initial field: uinf plus a Gaussian vortex of peak speed ~vortex at (0.6, 0.5).
+    Returns (mesh, case, U0)."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    m = vm.box_mesh((nx, ny, nz), hi=(2.0, 1.0, 0.1), two_d=True)
+    nP = len(m["patch_names"])
+    u_value = np.tile(np.asarray(uinf, np.float64), nP)
+    case = dict(nu=nu, steady=False, div_scheme=1, ddt_scheme=1, n_outer=1, n_corr=2, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=1.0, alpha_p=1.0, u_type=np.full(nP, 4, np.int32), u_value=u_value,
+                p_type=np.full(nP, 4, np.int32), p_value=np.zeros(nP),
+                U=_ctl("PBiCGStab", "DILU", 1e-10, 0.0, 1000), p=_ctl("PCG", "GAMG", 1e-10, 0.01, 2000),
+                pFinal=_ctl("PCG", "GAMG", 1e-10, 0.0, 2000), p_ref_cell=0, p_ref_value=0.0)
+    C = m["C"]
+    dx, dy = C[:, 0] - 0.6, C[:, 1] - 0.5
+    g = vortex * np.exp(-(dx * dx + dy * dy) / 0.02) / 0.14
+    U0 = np.zeros((m["n_cells"], 3))
+    U0[:, 0] = uinf[0] - g * dy
+    U0[:, 1] = uinf[1] + g * dx
+    return m, case, U0
+
+
+def channel_gradient(n=(40, 10, 1), ubulk=1.0, nu=0.05, dpdn=0.6, dudn=(0.05, 0.0, 0.0)):
+    """channel_inlet with fixedGradient conditions (FixedGradientBC): p at the inlet with the normal
+    gradient dpdn (the Poiseuille pressure drop -dp/dx = 12 nu ubulk / h^2 = 0.6 seen along the outward
+    normal -x) and U at the outlet with the normal gradient dudn.  Returns (mesh, case, U0)."""
+    m, case, U0 = channel_inlet(n, ubulk, nu)
+    names = list(m["patch_names"])
+    qi, qo = names.index("xMin"), names.index("xMax")
+    case = dict(case, u_type=case["u_type"].copy(), p_type=case["p_type"].copy(), u_value=case["u_value"].copy(),
+                p_value=case["p_value"].copy())
+    case["p_type"][qi] = 5
+    case["p_value"][qi] = dpdn
+    case["u_type"][qo] = 5
+    case["u_value"][3 * qo:3 * qo + 3] = dudn
+    return m, case, U0
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

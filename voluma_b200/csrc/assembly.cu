@@ -50,17 +50,28 @@ __global__ void k_face_gs(int nF, int nI, const double* __restrict__ gamma, cons
     if (f < nI) upper[f] = g * ndc[f];
 }
 
-// boundary coefficients of the laplacian (Fvm.h:171-180) for fixedValue / zeroGradient
+// boundary coefficients of the laplacian (Fvm.h:171-180): fixedValue (gic -dc, gbc dc v), mixed
+// (MixedBC, BoundaryCondition.h:240-243: -w dc, w dc v + (1 - w) g with g = 0), fixedGradient
+// (BoundaryCondition.h:147-148: 0, g), zeroGradient (0, 0)
 __global__ void k_lap_boundary(int nB, int nI, const double* __restrict__ gs, const double* __restrict__ ndc,
                                const int32_t* __restrict__ bPatch, const int32_t* __restrict__ bcType,
-                               const double* __restrict__ bcValue, double* __restrict__ ic, double* __restrict__ bs) {
+                               const double* __restrict__ bcValue, const double* __restrict__ frac,
+                               double* __restrict__ ic, double* __restrict__ bs) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int f = nI + b;
     double gic = 0.0, gbc = 0.0;
-    if (bcType[bPatch[b]] == 1) {
+    const int t = bcType[bPatch[b]];
+    const double v = bcValue ? bcValue[b] : 0.0;
+    if (t == 1) {
         gic = -ndc[f];
-        gbc = ndc[f] * (bcValue ? bcValue[b] : 0.0);
+        gbc = ndc[f] * v;
+    } else if (t == 4) {
+        const double w = frac[b], dc = ndc[f];
+        gic = -w * dc;
+        gbc = w * dc * v + (1.0 - w) * 0.0;
+    } else if (t == 5) {
+        gbc = v;
     }
     ic[b] = 0.0 + gs[f] * gic;
     bs[b] = 0.0 - gs[f] * gbc;
@@ -292,10 +303,21 @@ __global__ void k_set_references(const int32_t* __restrict__ cells, int n, doubl
 
 __global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
                              const int32_t* __restrict__ bcType, const double* __restrict__ bcValue,
+                             const double* __restrict__ frac, const double* __restrict__ ndc,
                              const double* __restrict__ psi, double* __restrict__ psiB) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
-    psiB[b] = bcType[bPatch[b]] == 1 ? (bcValue ? bcValue[b] : 0.0) : psi[own[nI + b]];
+    const int t = bcType[bPatch[b]];
+    const double v = bcValue ? bcValue[b] : 0.0;
+    const double pP = psi[own[nI + b]];
+    if (t == 1)
+        psiB[b] = v;
+    else if (t == 4)  // MixedBC::evaluate (BoundaryCondition.h:232-235), refGrad 0
+        psiB[b] = frac[b] * v + (1.0 - frac[b]) * (pP + 0.0 / ndc[nI + b]);
+    else if (t == 5)  // FixedGradientBC::evaluate (VolField.h:144-146)
+        psiB[b] = pP + v / ndc[nI + b];
+    else
+        psiB[b] = pP;
 }
 
 }  // namespace
@@ -398,12 +420,17 @@ void DeviceGeom::correctBoundary(const double* psi, const ScalarBC& bc, double* 
     uploadBCType(bc, s);
     const int nB = nBoundary();
     if (nB > 0)
-        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, psi, psiB), ++launches_;
+        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, bc.frac,
+                                              ndc_.get(), psi, psiB), ++launches_;
 }
 
 void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out,
                       cudaStream_t s) {
     uploadBCType(bc, s);
+    if (scheme == 1)
+        for (int32_t t : bcTypeHost_)
+            VLM_REQUIRE(t != 4 && t != 5, VLM_ERR_UNSUPPORTED,
+                        "the least-squares gradient supports zeroGradient and fixedValue boundaries only");
     if (scheme == 1)
         k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                             Sf_.get(), magSf_.get(), d_.get(), psi, psiB, bPatch_.get(), bcType_.get(),
@@ -429,7 +456,8 @@ void DeviceGeom::laplacian(const double* gamma, const double* psi, const double*
                                           source), ++launches_;
     const int nB = nBoundary();
     if (nB > 0)
-        k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value, ic, bs), ++launches_;
+        k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value,
+                                                bc.frac, ic, bs), ++launches_;
     if (hasFfc) *hasFfc = corr;
 }
 

@@ -12,11 +12,14 @@
 
 namespace vlm {
 
-// Scalar boundary conditions of one field: per patch 0 = zeroGradient, 1 = fixedValue
-// (values per boundary face, index f - nInternal).
+// Scalar boundary conditions of one field: per patch 0 = zeroGradient (also a scalar symmetry plane),
+// 1 = fixedValue, 4 = mixed with refGrad 0 (value fraction per face in `frac`, reference value in
+// `value`; freestreamPressure), 5 = fixedGradient (the gradient in `value`); values per boundary
+// face, index f - nInternal.  Types 4 and 5 are for the Gauss gradient and the laplacian only.
 struct ScalarBC {
     const int32_t* type = nullptr;  // host, nPatches
     const double* value = nullptr;  // device, nBoundary (may be null: 0)
+    const double* frac = nullptr;   // device, nBoundary: value fractions of type-4 faces
 };
 
 class DeviceGeom {

@@ -49,11 +49,16 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
     if (b >= nB) return;
     const int q = bPatch[b];
     const int c = own[nI + b];
-    if (uType[q] == 3) {
-        // inletOutlet = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
+    if (uType[q] == 3 || uType[q] == 4) {
+        // inletOutlet / freestream = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
         const double w = wIO[b], dc = ndc[nI + b];
         for (int k = 0; k < 3; ++k)
             Ub[k * nB + b] = w * uValueB[k * nB + b] + (1.0 - w) * (U[k * nC + c] + 0.0 / dc);
+        return;
+    }
+    if (uType[q] == 5) {  // fixedGradient (VolField.h:144-146): U_P + g / dc
+        const double dc = ndc[nI + b];
+        for (int k = 0; k < 3; ++k) Ub[k * nB + b] = U[k * nC + c] + uValueB[k * nB + b] / dc;
         return;
     }
     if (uType[q] == 2) {
@@ -68,12 +73,35 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
     for (int k = 0; k < 3; ++k) Ub[k * nB + b] = uType[q] == 1 ? uValueB[k * nB + b] : U[k * nC + c];
 }
 
+// freestream value fractions (constant): U w = clamp(1/2 - (U_inf.n)/(2|U_inf|), 0, 1)
+// (FreestreamVelocityBC, BoundaryCondition.h:291-302) and, on the same patch, p w = clamp(1/2 +
+// (U_inf.n)/(2|U_inf|), 0, 1) (FreestreamPressureBC::setDirection, BoundaryCondition.h:316-320)
+__global__ void k_freestream_fractions(int nB, int nI, int nF, const int32_t* __restrict__ bPatch,
+                                       const int32_t* __restrict__ uType, const int32_t* __restrict__ pType,
+                                       const double* __restrict__ uValueB, const double* __restrict__ Sf,
+                                       const double* __restrict__ magSf, double* __restrict__ wU,
+                                       double* __restrict__ wP) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB) return;
+    const int q = bPatch[b];
+    if (uType[q] != 4) return;
+    const int f = nI + b;
+    const double A = magSf[f];
+    const double n[3] = {Sf[f] / A, Sf[nF + f] / A, Sf[2 * size_t(nF) + f] / A};
+    const double u[3] = {uValueB[b], uValueB[size_t(nB) + b], uValueB[2 * size_t(nB) + b]};
+    const double mu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+    auto clamp01 = [](double v) { return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v); };
+    wU[b] = mu > 0 ? clamp01(0.5 - 0.5 * un / mu) : 1.0;
+    if (pType[q] == 4) wP[b] = mu > 0 ? clamp01(0.5 + 0.5 * un / mu) : 1.0;
+}
+
 // inletOutlet value fractions at the start of a step (InletOutletBC::update, BoundaryCondition.h:277-282):
-// 1 where the face flux is inflow (phi < 0), else 0
+// 1 where the face flux is inflow (phi < 0), else 0; phi == NULL (no flux yet) gives 0
 __global__ void k_io_fraction(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                               const double* __restrict__ phi, double* __restrict__ wIO) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < nB && uType[bPatch[b]] == 3) wIO[b] = phi[nI + b] < 0 ? 1.0 : 0.0;
+    if (b < nB && uType[bPatch[b]] == 3) wIO[b] = phi && phi[nI + b] < 0 ? 1.0 : 0.0;
 }
 
 // ---------------------------------------------------------------- fvc::grad of U (Gauss linear)
@@ -251,8 +279,15 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
         const double val = fixedValue ? uValueB[k * nB + b] : 0.0;
         double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
         double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
-        if (uType[q] == 3) {
-            // inletOutlet = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
+        if (uType[q] == 5) {  // fixedGradient (BoundaryCondition.h:145-148)
+            const double g = uValueB[k * nB + b];
+            vic = 1.0;
+            vbc = g / dc;
+            gic = 0.0;
+            gbc = g;
+        }
+        if (uType[q] == 3 || uType[q] == 4) {
+            // inletOutlet / freestream = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
             const double w = wIO[b], rv = uValueB[k * nB + b], rg = 0.0;
             vic = 1.0 - w;
             vbc = w * rv + (1.0 - w) * (rg / dc);
@@ -640,19 +675,21 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     uTypeHost_.assign(uType, uType + nP);
     pTypeHost_.assign(pType, pType + nP);
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 3, VLM_ERR_BAD_ARG, "U boundary type must be 0, 1, 2 or 3");
+        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 5, VLM_ERR_BAD_ARG, "U boundary type must be 0 to 5");
         if (uType[q] == 3) hasInletOutlet_ = true;
-        VLM_REQUIRE(pType[q] >= 0 && pType[q] <= 2, VLM_ERR_BAD_ARG, "p boundary type must be 0, 1 or 2");
+        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || pType[q] == 4 || pType[q] == 5,
+                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4 or 5");
+        VLM_REQUIRE(pType[q] != 4 || uType[q] == 4, VLM_ERR_BAD_ARG,
+                    "freestreamPressure needs the freestream velocity condition on the same patch");
     }
     // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
     needRef_ = true;
     for (int q = 0; q < nP; ++q)
         if (pType[q] == 1 && G_.patchSize()[q] > 0) needRef_ = false;
-    if (needRef_)
-        VLM_REQUIRE(ctrl_.p_ref_cell >= 0 && ctrl_.p_ref_cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
     for (int k = 0; k < 3; ++k)
         if (!G_.twoD() || k != G_.emptyDir()) solved_.push_back(k);  // Mesh.cpp:642-644
     uType_.upload(uTypeHost_, s_);
+    pType_.upload(pTypeHost_, s_);
     // fixesFlux per patch (BoundaryCondition.h:76, 203, 251): fixedValue and symmetry
     std::vector<int32_t> fix(size_t(std::max(nP, 1)), 0);
     for (int q = 0; q < nP; ++q) fix[q] = uType[q] == 1 || uType[q] == 2;
@@ -670,6 +707,25 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     pValueB_.upload(pv, s_);
     wIO_.resize(nBb);
     wIO_.zero(s_);
+    pFrac_.resize(nBb);
+    pFrac_.zero(s_);
+    bool freestream = false;
+    for (int q = 0; q < nP; ++q) freestream = freestream || uType[q] == 4;
+    if (freestream && nB_ > 0) {
+        k_freestream_fractions<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nF_, G_.bPatch(), uType_.get(), pType_.get(),
+                                                          uValueB_.get(), G_.Sf(), G_.magSf(), wIO_.get(),
+                                                          pFrac_.get()), ++launches_;
+        // a freestreamPressure patch fixes p where any of its faces has a positive value fraction
+        std::vector<double> pf(nBb);
+        VLM_CUDA(cudaMemcpyAsync(pf.data(), pFrac_.get(), sizeof(double) * nBb, cudaMemcpyDeviceToHost, s_));
+        VLM_CUDA(cudaStreamSynchronize(s_));
+        for (int q = 0; q < nP; ++q)
+            if (pType[q] == 4)
+                for (int i = 0; i < G_.patchSize()[q]; ++i)
+                    if (pf[size_t(G_.patchStart()[q] - nI_ + i)] > 0) needRef_ = false;
+    }
+    if (needRef_)
+        VLM_REQUIRE(ctrl_.p_ref_cell >= 0 && ctrl_.p_ref_cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1)), FI = size_t(std::max(nI_, 1)), F = size_t(nF_);
     for (DBuf<double>* b : {&U_, &U0_, &U00_, &src_, &msrc_, &HbyA_}) b->resize(3 * N);
     for (DBuf<double>* b : {&Ub_, &ic_, &bs_}) b->resize(3 * B);
@@ -795,6 +851,7 @@ void DeviceFlow::boundaryP() {
     ScalarBC bc;
     bc.type = pTypeHost_.data();
     bc.value = pValueB_.get();
+    bc.frac = pFrac_.get();
     G_.correctBoundary(p_.get(), bc, pB_.get(), s_);
 }
 
@@ -812,7 +869,10 @@ void DeviceFlow::setState(const double* U, const double* p) {
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
     if (p) p_.upload(p, size_t(nC_), s_);
-    wIO_.zero(s_);  // initialize(): no flux yet, every inletOutlet face evaluates as outflow
+    // initialize(): no flux yet, every inletOutlet face evaluates as outflow (the freestream fractions stay)
+    if (hasInletOutlet_ && nB_ > 0)
+        k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), nullptr, wIO_.get()),
+            ++launches_;
     boundaryU();
     boundaryP();
     if (G_.skewed()) gradU();
@@ -1015,6 +1075,7 @@ void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     ScalarBC pbc;
     pbc.type = pTypeHost_.data();
     pbc.value = pValueB_.get();
+    pbc.frac = pFrac_.get();
     G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
     k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get()), ++launches_;
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
@@ -1069,6 +1130,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     ScalarBC pbc;
     pbc.type = pTypeHost_.data();
     pbc.value = pValueB_.get();
+    pbc.frac = pFrac_.get();
     const bool skewed = G_.skewed();
     if (skewed) {
         // skewed mesh (IncompressibleFlow.cpp:252-275): grad rAU by least squares with zero-gradient

@@ -15,8 +15,8 @@
 //
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
 // linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients,
-// fixedValue (uniform or face by face), zeroGradient and symmetry boundary conditions for U and p and
-// inletOutlet for U, empty (2D) directions and
+// fixedValue (uniform or face by face), zeroGradient, symmetry, freestream / freestreamPressure and
+// fixedGradient boundary conditions for U and p and inletOutlet for U, empty (2D) directions and
 // cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
 // Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
 // constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
@@ -118,7 +118,10 @@ private:
     std::vector<int> solved_;
     DBuf<int32_t> uType_;
     DBuf<double> uValueB_, pValueB_;  // per boundary face: U values (SoA) / inlet values, p values
-    DBuf<double> wIO_;                // inletOutlet value fraction per boundary face (phi < 0 at step start)
+    DBuf<double> wIO_;                // mixed U value fraction per boundary face: inletOutlet (phi < 0 at
+                                      // step start), freestream (constant)
+    DBuf<double> pFrac_;              // freestreamPressure value fraction per boundary face
+    DBuf<int32_t> pType_;
     DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry)
     bool hasInletOutlet_ = false;
     // fields (vectors SoA: component k at [k * n])
