@@ -277,7 +277,9 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * fraction 1/2 - (U_inf.n)/(2|U_inf|) towards u_value = U_inf, BoundaryCondition.h:289-302; p:
  * freestreamPressure towards p_value with fraction 1/2 + (U_inf.n)/(2|U_inf|), U_inf from the U
  * freestream condition of the same patch, :304-320), 5 fixedGradient (the value is the normal
- * gradient, :140-153).  Patch values are uniform; vlm_flow_set_boundary_values sets the fixedValue
+ * gradient, :140-153), 6 fixedFluxPressure for p (the gradient that makes the boundary flux the
+ * boundary velocity's, set every corrector, :155-163 and IncompressibleFlow.cpp:17-29).  Patch
+ * values are uniform; vlm_flow_set_boundary_values sets the fixedValue
  * and inletOutlet values face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
  * reference's fields bit for bit. */

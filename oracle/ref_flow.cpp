@@ -39,7 +39,7 @@ struct RefSolverCtl {
 // 0 zeroGradient, 1 fixedValue with the given value, 2 symmetry, 3 inletOutlet with the given inlet
 // value (InletOutletBC on the flow's BCContext), 4 freestream (U: the free-stream velocity; p:
 // freestreamPressure with the p value and the U free-stream velocity of the patch), 5 fixedGradient
-// (the value is the gradient); uFace / pFace override the values face by face.
+// (the value is the gradient), 6 fixedFluxPressure (p); uFace / pFace override the values face by face.
 struct RefFlowSpec {
     double nu;
     int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
@@ -176,6 +176,8 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.p().set<FreestreamPressureBC>(name, &flow.context(), sp->pValue[q], &uv);
             } else if (sp->pType[q] == 5) {
                 flow.p().set<FixedGradientBC<scalar>>(name, sp->pValue[q]);
+            } else if (sp->pType[q] == 6) {
+                flow.p().set<FixedFluxPressureBC>(name);
             } else {
                 flow.p().zeroGradient(name);
             }

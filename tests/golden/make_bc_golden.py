@@ -16,7 +16,10 @@ CFD_REPRODUCIBLE mode:
     every side (FreestreamVelocityBC, FreestreamPressureBC, BoundaryCondition.h:289-320), transient
     Euler, 4 steps of dt 0.02;
   * gradient: the inlet-outlet channel with fixedGradient p at the inlet and fixedGradient U at the
-    outlet (FixedGradientBC, BoundaryCondition.h:140-153), steady SIMPLE, 6 steps.
+    outlet (FixedGradientBC, BoundaryCondition.h:140-153), steady SIMPLE, 6 steps;
+  * fluxp / fluxpo: the inlet-outlet channel with fixedFluxPressure p at the inlet / at the outlet
+    (FixedFluxPressureBC, BoundaryCondition.h:155-163; IncompressibleFlow.cpp:17-29), steady SIMPLE,
+    6 steps.
 Run where the reference sources are present:
     make -C oracle && python tests/golden/make_bc_golden.py
 """
@@ -78,6 +81,13 @@ def main():
     R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
     U, p, phi, hist = R.flow_run(case, 6, U=U0, reproducible=True)
     out.update(gradient_U=U, gradient_p=p, gradient_phi=phi, gradient_hist=hist)
+    m, case, U0 = cases.channel_flux_pressure()
+    R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
+    U, p, phi, hist = R.flow_run(case, 6, U=U0, reproducible=True)
+    out.update(fluxp_U=U, fluxp_p=p, fluxp_phi=phi, fluxp_hist=hist)
+    m, case, U0 = cases.channel_flux_pressure(patch="xMax")
+    U, p, phi, hist = R.flow_run(case, 6, U=U0, reproducible=True)
+    out.update(fluxpo_U=U, fluxpo_p=p, fluxpo_phi=phi, fluxpo_hist=hist)
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))
 

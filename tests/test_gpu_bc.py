@@ -175,6 +175,21 @@ def test_freestream_box_bitwise(gold):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("patch,tag", [("xMin", "fluxp"), ("xMax", "fluxpo")])
+def test_fixed_flux_pressure_channel_bitwise(gold, patch, tag):
+    m, case, U0 = cases.channel_flux_pressure(patch=patch)
+    U, p, phi, hist = run_case(m, case, U0, 6, 1.0)
+    assert np.array_equal(hist, gold[f"{tag}_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"{tag}_{k}"]), k
+
+
+def test_golden_outlet_flux_pressure_differs():
+    z = np.load(GOLD)
+    assert not np.array_equal(z["fluxpo_p"], z["inlet_p"])
+
+
+@pytest.mark.gpu
 def test_fixed_gradient_channel_bitwise(gold):
     m, case, U0 = cases.channel_gradient()
     U, p, phi, hist = run_case(m, case, U0, 6, 1.0)

@@ -294,6 +294,19 @@ def channel_gradient(n=(40, 10, 1), ubulk=1.0, nu=0.05, dpdn=0.6, dudn=(0.05, 0.
     return m, case, U0
 
 
+def channel_flux_pressure(n=(40, 10, 1), ubulk=1.0, nu=0.05, patch="xMin"):
+    """channel_inlet with fixedFluxPressure p on `patch` (FixedFluxPressureBC, whose gradient the
+    corrector sets so that the boundary flux is the boundary velocity's).  On the inlet
+    (cases/channelInlet/fixedFluxPressure.json) the fixed inlet velocity makes that gradient zero; on
+    the outlet, where the velocity is inletOutlet, it is not (and p then needs the reference cell).
+    Returns (mesh, case, U0)."""
+    m, case, U0 = channel_inlet(n, ubulk, nu)
+    q = list(m["patch_names"]).index(patch)
+    case = dict(case, p_type=case["p_type"].copy())
+    case["p_type"][q] = 6
+    return m, case, U0
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

@@ -578,6 +578,20 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     }
 }
 
+// constrainPressure (IncompressibleFlow.cpp:17-29): the fixedFluxPressure gradient that makes the
+// boundary flux the boundary velocity's, g = (phiHbyA - U_b.S) / (|S| rAUf)
+__global__ void k_flux_pressure(int nB, int nI, int nF, const int32_t* __restrict__ bPatch,
+                                const int32_t* __restrict__ pType, const double* __restrict__ phiHbyA,
+                                const double* __restrict__ Ub, const double* __restrict__ Sf,
+                                const double* __restrict__ magSf, const double* __restrict__ rAUf,
+                                double* __restrict__ pValueB) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB || pType[bPatch[b]] != 6) return;
+    const int f = nI + b;
+    const double ubS = Ub[b] * Sf[f] + Ub[size_t(nB) + b] * Sf[nF + f] + Ub[2 * size_t(nB) + b] * Sf[2 * size_t(nF) + f];
+    pValueB[b] = (phiHbyA[f] - ubS) / (magSf[f] * rAUf[f]);
+}
+
 // phi = phiHbyA - flux (IncompressibleFlow.cpp:337-340)
 __global__ void k_phi_update(int nF, const double* __restrict__ phiHbyA, const double* __restrict__ F,
                              double* __restrict__ phi) {
@@ -674,11 +688,19 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
                     "linearUpwind / LUST need the cell and face centres (vlm_mesh_desc.C, .Cf)");
     uTypeHost_.assign(uType, uType + nP);
     pTypeHost_.assign(pType, pType + nP);
+    // the types the assembly sees: fixedFluxPressure is a fixedGradient whose gradient the corrector sets
+    pTypeAsm_.assign(pType, pType + nP);
+    for (int32_t& t : pTypeAsm_)
+        if (t == 6) {
+            t = 5;
+            hasFluxPressure_ = true;
+        }
     for (int q = 0; q < nP; ++q) {
         VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 5, VLM_ERR_BAD_ARG, "U boundary type must be 0 to 5");
         if (uType[q] == 3) hasInletOutlet_ = true;
-        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || pType[q] == 4 || pType[q] == 5,
-                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4 or 5");
+        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || pType[q] == 4 || pType[q] == 5 ||
+                        pType[q] == 6,
+                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5 or 6");
         VLM_REQUIRE(pType[q] != 4 || uType[q] == 4, VLM_ERR_BAD_ARG,
                     "freestreamPressure needs the freestream velocity condition on the same patch");
     }
@@ -701,7 +723,7 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
         for (int i = 0; i < G_.patchSize()[q]; ++i) {
             const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
             for (int k = 0; k < 3; ++k) uv[k * nBb + b] = uValue[3 * q + k];
-            pv[b] = pValue[q];
+            pv[b] = pType[q] == 6 ? 0.0 : pValue[q];  // FixedFluxPressureBC starts with a zero gradient
         }
     uValueB_.upload(uv, s_);
     pValueB_.upload(pv, s_);
@@ -849,7 +871,7 @@ void DeviceFlow::setBoundaryValues(const double* uFace, const double* pFace) {
 
 void DeviceFlow::boundaryP() {
     ScalarBC bc;
-    bc.type = pTypeHost_.data();
+    bc.type = pTypeAsm_.data();
     bc.value = pValueB_.get();
     bc.frac = pFrac_.get();
     G_.correctBoundary(p_.get(), bc, pB_.get(), s_);
@@ -1073,7 +1095,7 @@ void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
 // Momentum predictor: M = UEqn + grad p, one solve per solved component (FvMatrix.h:144-175)
 void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     ScalarBC pbc;
-    pbc.type = pTypeHost_.data();
+    pbc.type = pTypeAsm_.data();
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
     G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
@@ -1128,7 +1150,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
                                        diag_.get(), upper_.get(), lower_.get(), ic_.get(), bs_.get(), src_.get(),
                                        U_.get(), G_.V(), rAU_.get(), HbyA_.get()), ++launches_;
     ScalarBC pbc;
-    pbc.type = pTypeHost_.data();
+    pbc.type = pTypeAsm_.data();
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
     const bool skewed = G_.skewed();
@@ -1153,6 +1175,9 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
                                          uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(),
                                          skewed ? G_.skew() : nullptr, gR_.get(), gH_.get(), rAUf_.get(),
                                          phiHbyA_.get()), ++launches_;
+    if (hasFluxPressure_ && nB_ > 0)
+        k_flux_pressure<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nF_, G_.bPatch(), pType_.get(), phiHbyA_.get(), Ub_.get(),
+                                                   G_.Sf(), G_.magSf(), rAUf_.get(), pValueB_.get()), ++launches_;
     G_.div(phiHbyA_.get(), divPhi_.get(), s_);
     if (ctrl_.steady) VLM_CUDA(cudaMemcpyAsync(pPrev_.get(), p_.get(), sizeof(double) * nC_, cudaMemcpyDeviceToDevice, s_));
     const int nNO = ctrl_.n_non_orth_corr;

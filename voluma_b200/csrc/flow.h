@@ -16,7 +16,8 @@
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
 // linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients,
 // fixedValue (uniform or face by face), zeroGradient, symmetry, freestream / freestreamPressure and
-// fixedGradient boundary conditions for U and p and inletOutlet for U, empty (2D) directions and
+// fixedGradient boundary conditions for U and p, inletOutlet for U and fixedFluxPressure for p,
+// empty (2D) directions and
 // cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
 // Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
 // constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
@@ -114,7 +115,8 @@ private:
     cudaStream_t s_;
     int nC_, nI_, nF_, nB_;
     bool needRef_ = false;
-    std::vector<int32_t> uTypeHost_, pTypeHost_;
+    std::vector<int32_t> uTypeHost_, pTypeHost_, pTypeAsm_;
+    bool hasFluxPressure_ = false;
     std::vector<int> solved_;
     DBuf<int32_t> uType_;
     DBuf<double> uValueB_, pValueB_;  // per boundary face: U values (SoA) / inlet values, p values
