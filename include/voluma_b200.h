@@ -277,8 +277,11 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * fraction 1/2 - (U_inf.n)/(2|U_inf|) towards u_value = U_inf, BoundaryCondition.h:289-302; p:
  * freestreamPressure towards p_value with fraction 1/2 + (U_inf.n)/(2|U_inf|), U_inf from the U
  * freestream condition of the same patch, :304-320), 5 fixedGradient (the value is the normal
- * gradient, :140-153), 6 fixedFluxPressure for p (the gradient that makes the boundary flux the
- * boundary velocity's, set every corrector, :155-163 and IncompressibleFlow.cpp:17-29).  Patch
+ * gradient, :140-153), 6 pressureInletOutletVelocity for U (u_value = the tangential inflow
+ * velocity, :343-364) and fixedFluxPressure for p (the gradient that makes the boundary flux the
+ * boundary velocity's, set every corrector, :155-163 and IncompressibleFlow.cpp:17-29), 7
+ * totalPressure for p (p_value = p0; p0 - |U_b|^2/2 on inflow faces, set at each step start,
+ * :325-341).  Patch
  * values are uniform; vlm_flow_set_boundary_values sets the fixedValue
  * and inletOutlet values face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the

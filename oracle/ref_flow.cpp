@@ -39,7 +39,9 @@ struct RefSolverCtl {
 // 0 zeroGradient, 1 fixedValue with the given value, 2 symmetry, 3 inletOutlet with the given inlet
 // value (InletOutletBC on the flow's BCContext), 4 freestream (U: the free-stream velocity; p:
 // freestreamPressure with the p value and the U free-stream velocity of the patch), 5 fixedGradient
-// (the value is the gradient), 6 fixedFluxPressure (p); uFace / pFace override the values face by face.
+// (the value is the gradient), 6 pressureInletOutletVelocity (U, the value is the tangential velocity)
+// and fixedFluxPressure (p), 7 totalPressure (p, the value is p0); uFace / pFace override the values
+// face by face.
 struct RefFlowSpec {
     double nu;
     int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
@@ -161,6 +163,8 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.U().set<FreestreamVelocityBC>(name, uv);
             } else if (sp->uType[q] == 5) {
                 flow.U().set<FixedGradientBC<Vec3>>(name, uv);
+            } else if (sp->uType[q] == 6) {
+                flow.U().set<PressureInletOutletVelocityBC>(name, &flow.context(), uv);
             } else {
                 flow.U().zeroGradient(name);
             }
@@ -178,6 +182,9 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.p().set<FixedGradientBC<scalar>>(name, sp->pValue[q]);
             } else if (sp->pType[q] == 6) {
                 flow.p().set<FixedFluxPressureBC>(name);
+            } else if (sp->pType[q] == 7) {
+                const double p0 = sp->pValue[q];
+                flow.p().set<TotalPressureBC>(name, &flow.context(), [p0](scalar) { return p0; });
             } else {
                 flow.p().zeroGradient(name);
             }

@@ -19,7 +19,9 @@ CFD_REPRODUCIBLE mode:
     outlet (FixedGradientBC, BoundaryCondition.h:140-153), steady SIMPLE, 6 steps;
   * fluxp / fluxpo: the inlet-outlet channel with fixedFluxPressure p at the inlet / at the outlet
     (FixedFluxPressureBC, BoundaryCondition.h:155-163; IncompressibleFlow.cpp:17-29), steady SIMPLE,
-    6 steps.
+    6 steps;
+  * totalp: the total-pressure inlet of cases/channelInlet/totalPressure.json (TotalPressureBC with
+    PressureInletOutletVelocityBC, BoundaryCondition.h:325-364), steady SIMPLE, 8 steps from rest.
 Run where the reference sources are present:
     make -C oracle && python tests/golden/make_bc_golden.py
 """
@@ -88,6 +90,9 @@ def main():
     m, case, U0 = cases.channel_flux_pressure(patch="xMax")
     U, p, phi, hist = R.flow_run(case, 6, U=U0, reproducible=True)
     out.update(fluxpo_U=U, fluxpo_p=p, fluxpo_phi=phi, fluxpo_hist=hist)
+    m, case, U0 = cases.channel_total_pressure()
+    U, p, phi, hist = R.flow_run(case, 8, U=U0, reproducible=True)
+    out.update(totalp_U=U, totalp_p=p, totalp_phi=phi, totalp_hist=hist)
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))
 

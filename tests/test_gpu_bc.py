@@ -140,7 +140,7 @@ def test_inlet_outlet_channel_bitwise(gold, tag):
 @pytest.mark.gpu
 def test_flow_rejects_unknown_boundary_types():
     m, case, _ = cases.channel_inlet((8, 4, 1))
-    bad = dict(case, u_type=np.full(len(case["u_type"]), 6, np.int32))
+    bad = dict(case, u_type=np.full(len(case["u_type"]), 7, np.int32))
     with pytest.raises(vb.VlmError):
         vb.Flow(vb.Mesh.from_arrays(m), bad)
     bad = dict(case, p_type=np.full(len(case["p_type"]), 3, np.int32))
@@ -187,6 +187,17 @@ def test_fixed_flux_pressure_channel_bitwise(gold, patch, tag):
 def test_golden_outlet_flux_pressure_differs():
     z = np.load(GOLD)
     assert not np.array_equal(z["fluxpo_p"], z["inlet_p"])
+
+
+@pytest.mark.gpu
+def test_total_pressure_inlet_bitwise(gold):
+    # totalPressure p (values from the inflow faces' velocity at each step start) with a
+    # pressureInletOutletVelocity inlet, slip walls and an inletOutlet outlet
+    m, case, U0 = cases.channel_total_pressure()
+    U, p, phi, hist = run_case(m, case, U0, 8, 1.0)
+    assert np.array_equal(hist, gold["totalp_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"totalp_{k}"]), k
 
 
 @pytest.mark.gpu

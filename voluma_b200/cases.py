@@ -307,6 +307,28 @@ def channel_flux_pressure(n=(40, 10, 1), ubulk=1.0, nu=0.05, patch="xMin"):
     return m, case, U0
 
 
+def channel_total_pressure(n=(40, 10, 1), p0=0.5, nu=0.01):
+    """The total-pressure inlet of cases/channelInlet/totalPressure.json: the 2D box 4 x 1 (0.1 deep) with
+    slip walls yMin / yMax, the xMin inlet with totalPressure p0 (TotalPressureBC: p0 - |U_b|^2/2 on inflow
+    faces) and pressureInletOutletVelocity U, the xMax outlet with inletOutlet U and fixedValue p = 0;
+    nu 0.01, steady SIMPLE with linearUpwind, alphaU 0.7, alphaP 0.3, from U = 0 (the exact solution is
+    U = (1, 0, 0), p = 0).  Returns (mesh, case, U0)."""
+    from . import mesh as vm
+    nx, ny, nz = (int(v) for v in n)
+    m = vm.box_mesh((nx, ny, nz), hi=(4.0, 1.0, 0.1), two_d=True)
+    names = list(m["patch_names"])
+    nP = len(names)
+    u_type = np.array([{"xMin": 6, "xMax": 3}.get(nm, 2) for nm in names], np.int32)
+    p_type = np.array([{"xMin": 7, "xMax": 1}.get(nm, 0) for nm in names], np.int32)
+    p_value = np.array([p0 if nm == "xMin" else 0.0 for nm in names])
+    case = dict(nu=nu, steady=True, div_scheme=2, ddt_scheme=0, n_outer=1, n_corr=1, n_non_orth_corr=0,
+                momentum_predictor=True, alpha_u=0.7, alpha_p=0.3, u_type=u_type, u_value=np.zeros(3 * nP),
+                p_type=p_type, p_value=p_value, U=_ctl("PBiCGStab", "DILU", 1e-10, 0.1, 1000),
+                p=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000), pFinal=_ctl("PCG", "GAMG", 1e-10, 0.05, 2000),
+                p_ref_cell=0, p_ref_value=0.0)
+    return m, case, np.zeros((m["n_cells"], 3))
+
+
 def taylor_green_flow(n=16, nu=1.0 / 1600, u0=1.0):
     """Taylor-Green vortex in the periodic box [0, 2pi]^3 (fvmFlow.cpp:76-89 initial condition
     U = u0 (sin x cos y cos z, -cos x sin y cos z, 0)); transient PIMPLE with the fvmFlow transient

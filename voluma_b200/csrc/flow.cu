@@ -44,7 +44,8 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
                              const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                              const double* __restrict__ uValueB, const double* __restrict__ Sf,
                              const double* __restrict__ magSf, const double* __restrict__ ndc,
-                             const double* __restrict__ wIO, const double* __restrict__ U, double* __restrict__ Ub) {
+                             const double* __restrict__ wIO, const double* __restrict__ phi,
+                             const double* __restrict__ U, double* __restrict__ Ub) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int q = bPatch[b];
@@ -54,6 +55,24 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
         const double w = wIO[b], dc = ndc[nI + b];
         for (int k = 0; k < 3; ++k)
             Ub[k * nB + b] = w * uValueB[k * nB + b] + (1.0 - w) * (U[k * nC + c] + 0.0 / dc);
+        return;
+    }
+    if (uType[q] == 6) {
+        // pressureInletOutletVelocity (VolField.h:204-212): outflow zero gradient; inflow the normal
+        // component of U_P and the tangential part of Ut; the current flux decides
+        double u[3];
+        for (int k = 0; k < 3; ++k) u[k] = U[k * nC + c];
+        if (phi[nI + b] >= 0) {
+            for (int k = 0; k < 3; ++k) Ub[k * nB + b] = u[k];
+            return;
+        }
+        const int f = nI + b;
+        const double A = magSf[f];
+        const double n[3] = {Sf[f] / A, Sf[nF + f] / A, Sf[2 * size_t(nF) + f] / A};
+        const double ut[3] = {uValueB[b], uValueB[size_t(nB) + b], uValueB[2 * size_t(nB) + b]};
+        const double nu_ = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+        const double nt = n[0] * ut[0] + n[1] * ut[1] + n[2] * ut[2];
+        for (int k = 0; k < 3; ++k) Ub[k * nB + b] = nu_ * n[k] + (ut[k] - nt * n[k]);
         return;
     }
     if (uType[q] == 5) {  // fixedGradient (VolField.h:144-146): U_P + g / dc
@@ -279,6 +298,31 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
         const double val = fixedValue ? uValueB[k * nB + b] : 0.0;
         double vic = fixedValue ? 0.0 : 1.0, vbc = fixedValue ? val : 0.0;
         double gic = fixedValue ? -dc : 0.0, gbc = fixedValue ? val * dc : 0.0;
+        if (uType[q] == 6) {
+            // pressureInletOutletVelocity (BoundaryCondition.h:351-360, VolField.h:204-215)
+            const int c = own[f];
+            const double uk = U[size_t(k) * nC + c];
+            double fv;
+            if (F >= 0) {
+                vic = 1.0;
+                fv = uk;
+            } else {
+                const double A = magSf[f];
+                double nn[3], uu[3], ut[3];
+                for (int j = 0; j < 3; ++j) {
+                    nn[j] = Sf[size_t(j) * nF + f] / A;
+                    uu[j] = U[size_t(j) * nC + c];
+                    ut[j] = uValueB[j * nB + b];
+                }
+                vic = nn[k] * nn[k];
+                const double nu_ = nn[0] * uu[0] + nn[1] * uu[1] + nn[2] * uu[2];
+                const double nt = nn[0] * ut[0] + nn[1] * ut[1] + nn[2] * ut[2];
+                fv = nu_ * nn[k] + (ut[k] - nt * nn[k]);
+            }
+            vbc = fv - vic * uk;
+            gic = dc * (vic - 1.0);
+            gbc = dc * vbc;
+        }
         if (uType[q] == 5) {  // fixedGradient (BoundaryCondition.h:145-148)
             const double g = uValueB[k * nB + b];
             vic = 1.0;
@@ -578,6 +622,21 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     }
 }
 
+// totalPressure values (TotalPressureBC::update, VolField.h:217-223): p0 - |U_b|^2 / 2 on inflow faces
+// (phi < 0), p0 elsewhere; phi == NULL (no flux yet) gives p0
+__global__ void k_total_pressure(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ pType,
+                                 const double* __restrict__ phi, const double* __restrict__ Ub,
+                                 const double* __restrict__ p0, double* __restrict__ pValueB) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB || pType[bPatch[b]] != 7) return;
+    if (phi && phi[nI + b] < 0) {
+        const double u0 = Ub[b], u1 = Ub[size_t(nB) + b], u2 = Ub[2 * size_t(nB) + b];
+        pValueB[b] = p0[b] - 0.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+    } else {
+        pValueB[b] = p0[b];
+    }
+}
+
 // constrainPressure (IncompressibleFlow.cpp:17-29): the fixedFluxPressure gradient that makes the
 // boundary flux the boundary velocity's, g = (phiHbyA - U_b.S) / (|S| rAUf)
 __global__ void k_flux_pressure(int nB, int nI, int nF, const int32_t* __restrict__ bPatch,
@@ -690,24 +749,27 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     pTypeHost_.assign(pType, pType + nP);
     // the types the assembly sees: fixedFluxPressure is a fixedGradient whose gradient the corrector sets
     pTypeAsm_.assign(pType, pType + nP);
+    // and totalPressure a fixedValue whose values the step start sets
     for (int32_t& t : pTypeAsm_)
         if (t == 6) {
             t = 5;
             hasFluxPressure_ = true;
+        } else if (t == 7) {
+            t = 1;
+            hasTotalPressure_ = true;
         }
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 5, VLM_ERR_BAD_ARG, "U boundary type must be 0 to 5");
+        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 6, VLM_ERR_BAD_ARG, "U boundary type must be 0 to 6");
         if (uType[q] == 3) hasInletOutlet_ = true;
-        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || pType[q] == 4 || pType[q] == 5 ||
-                        pType[q] == 6,
-                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5 or 6");
+        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || (pType[q] >= 4 && pType[q] <= 7),
+                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5, 6 or 7");
         VLM_REQUIRE(pType[q] != 4 || uType[q] == 4, VLM_ERR_BAD_ARG,
                     "freestreamPressure needs the freestream velocity condition on the same patch");
     }
     // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
     needRef_ = true;
     for (int q = 0; q < nP; ++q)
-        if (pType[q] == 1 && G_.patchSize()[q] > 0) needRef_ = false;
+        if ((pType[q] == 1 || pType[q] == 7) && G_.patchSize()[q] > 0) needRef_ = false;
     for (int k = 0; k < 3; ++k)
         if (!G_.twoD() || k != G_.emptyDir()) solved_.push_back(k);  // Mesh.cpp:642-644
     uType_.upload(uTypeHost_, s_);
@@ -727,6 +789,7 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
         }
     uValueB_.upload(uv, s_);
     pValueB_.upload(pv, s_);
+    if (hasTotalPressure_) pTotal_.upload(pv, s_);  // p0 per face
     wIO_.resize(nBb);
     wIO_.zero(s_);
     pFrac_.resize(nBb);
@@ -826,14 +889,20 @@ bool DeviceFlow::componentBatch() {
 void DeviceFlow::boundaryU() {
     if (nB_ > 0)
         k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
-                                                uValueB_.get(), G_.Sf(), G_.magSf(), G_.ndc(), wIO_.get(), U_.get(),
-                                                Ub_.get()), ++launches_;
+                                                uValueB_.get(), G_.Sf(), G_.magSf(), G_.ndc(), wIO_.get(),
+                                                phi_.get(), U_.get(), Ub_.get()), ++launches_;
 }
 
 void DeviceFlow::ioFractions() {
     if (hasInletOutlet_ && nB_ > 0)
         k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), phi_.get(), wIO_.get()),
             ++launches_;
+}
+
+void DeviceFlow::totalPressure(bool noFlux) {
+    if (hasTotalPressure_ && nB_ > 0)
+        k_total_pressure<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), pType_.get(), noFlux ? nullptr : phi_.get(),
+                                                    Ub_.get(), pTotal_.get(), pValueB_.get()), ++launches_;
 }
 
 void DeviceFlow::setBoundaryValues(const double* uFace, const double* pFace) {
@@ -895,6 +964,7 @@ void DeviceFlow::setState(const double* U, const double* p) {
     if (hasInletOutlet_ && nB_ > 0)
         k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), nullptr, wIO_.get()),
             ++launches_;
+    totalPressure(true);
     boundaryU();
     boundaryP();
     if (G_.skewed()) gradU();
@@ -1040,6 +1110,7 @@ bool DeviceFlow::readRestart(const std::string& dir) {
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
     ioFractions();  // markRestarted: updateBCs with the restart's flux
+    totalPressure(false);
     boundaryU();
     boundaryP();
     VLM_CUDA(cudaStreamSynchronize(s_));
@@ -1228,6 +1299,7 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
         VLM_CUDA(cudaMemcpyAsync(phiOld_.get(), phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToDevice, s_));
     }
     ioFractions();
+    totalPressure(false);  // p_.updateBCs reads U's boundary values of the previous step
     boundaryU();
     boundaryP();
     nSolves_ = 0;

@@ -16,8 +16,8 @@
 // Supported: steady SIMPLE and transient PIMPLE (Euler, backward), divergence schemes upwind /
 // linear / linearUpwind / LUST / limitedLinear / vanLeer / MUSCL / minmod, Gauss linear gradients,
 // fixedValue (uniform or face by face), zeroGradient, symmetry, freestream / freestreamPressure and
-// fixedGradient boundary conditions for U and p, inletOutlet for U and fixedFluxPressure for p,
-// empty (2D) directions and
+// fixedGradient boundary conditions for U and p, inletOutlet and pressureInletOutletVelocity for U,
+// fixedFluxPressure and totalPressure for p, empty (2D) directions and
 // cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
 // Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
 // constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
@@ -66,6 +66,7 @@ public:
 private:
     void boundaryU();
     void ioFractions();
+    void totalPressure(bool noFlux);
     void boundaryP();
     void gradU();
     void assembleMomentum(double aU, bool haveGradU);
@@ -116,13 +117,14 @@ private:
     int nC_, nI_, nF_, nB_;
     bool needRef_ = false;
     std::vector<int32_t> uTypeHost_, pTypeHost_, pTypeAsm_;
-    bool hasFluxPressure_ = false;
+    bool hasFluxPressure_ = false, hasTotalPressure_ = false;
     std::vector<int> solved_;
     DBuf<int32_t> uType_;
     DBuf<double> uValueB_, pValueB_;  // per boundary face: U values (SoA) / inlet values, p values
     DBuf<double> wIO_;                // mixed U value fraction per boundary face: inletOutlet (phi < 0 at
                                       // step start), freestream (constant)
     DBuf<double> pFrac_;              // freestreamPressure value fraction per boundary face
+    DBuf<double> pTotal_;             // totalPressure p0 per boundary face
     DBuf<int32_t> pType_;
     DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry)
     bool hasInletOutlet_ = false;
