@@ -300,6 +300,11 @@ typedef struct {
     double p_ref_value;
     vlm_solver_ctrl U, p, p_final;
     double div_coeff;            /* limitedLinear's k ("limitedLinear k"); 0 -> 1 */
+    int32_t grad_scheme;         /* IncompressibleFlow::gradScheme, also the mesh default (Mesh::setGradScheme)
+                                    that fvm::div and the laplacians' non-orthogonal correction use:
+                                    0 Gauss linear, 1 leastSquares */
+    int32_t grad_p_scheme;       /* IncompressibleFlow::gradPScheme (momentum source, U correction):
+                                    0 Gauss linear, 1 leastSquares, 2 GaussSkew (Fvc.h:233-262) */
 } vlm_flow_ctrl;
 
 typedef struct {

@@ -82,7 +82,8 @@ class RefFlowSpec(C.Structure):
                 ("uValue", C.c_void_p), ("pType", C.c_void_p), ("pValue", C.c_void_p), ("U", RefSolverCtl),
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
                 ("reproducible", C.c_int), ("residualTol", C.c_double), ("divK", C.c_double),
-                ("uFace", C.c_void_p), ("pFace", C.c_void_p)]
+                ("uFace", C.c_void_p), ("pFace", C.c_void_p), ("gradScheme", C.c_int),
+                ("gradPScheme", C.c_int)]
 
 
 class RefModelSpec(C.Structure):
@@ -200,6 +201,8 @@ class RefMesh:
         sp.reproducible = int(reproducible)
         sp.residualTol = residual_tol
         sp.divK = case.get("div_coeff", 1.0)
+        sp.gradScheme = int(case.get("grad_scheme", 0))
+        sp.gradPScheme = int(case.get("grad_p_scheme", 0))
         if case.get("u_face") is not None:  # face-by-face values (boundary faces in mesh order)
             keep.append(np.ascontiguousarray(case["u_face"], np.float64).reshape(-1))
             sp.uFace = _p(keep[-1])

@@ -59,6 +59,8 @@ struct RefFlowSpec {
     double divK;         // limitedLinear's k
     const double* uFace; // optional, 3 per boundary face: values of the fixedValue / inletOutlet U faces
     const double* pFace; // optional, 1 per boundary face: values of the fixedValue p faces
+    int gradScheme;      // IncompressibleFlow::gradScheme and the mesh default: 0 Gauss, 1 leastSquares
+    int gradPScheme;     // IncompressibleFlow::gradPScheme: 0 Gauss, 1 leastSquares, 2 GaussSkew
 };
 
 // Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
@@ -113,6 +115,12 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
         par::setReproducible(sp->reproducible != 0);
         const Mesh& m = *r->mesh;
         IncompressibleFlow flow(r->mesh, sp->nu);
+        // gradient schemes as fvmFlow sets them (fvmFlow.cpp:151-154); the mesh default follows gradScheme
+        flow.gradScheme = sp->gradScheme == 1 ? GradScheme::LeastSquares : GradScheme::GaussLinear;
+        r->mesh->setGradScheme(flow.gradScheme);
+        flow.gradPScheme = sp->gradPScheme == 1   ? GradScheme::LeastSquares
+                           : sp->gradPScheme == 2 ? GradScheme::GaussSkew
+                                                  : GradScheme::GaussLinear;
         PimpleControls& c = flow.controls;
         c.steady = sp->steady != 0;
         c.nOuter = sp->nOuter;

@@ -533,6 +533,8 @@ def _flow_ctrl(case: dict) -> _ffi.FlowCtrl:
     c.alpha_u, c.alpha_p = case["alpha_u"], case["alpha_p"]
     c.p_ref_cell, c.p_ref_value = case["p_ref_cell"], case["p_ref_value"]
     c.div_coeff = case.get("div_coeff", 1.0)
+    c.grad_scheme = int(case.get("grad_scheme", 0))
+    c.grad_p_scheme = int(case.get("grad_p_scheme", 0))
     repro = bool(case.get("reproducible", False))
     for name, key in (("U", "U"), ("p", "p"), ("p_final", "pFinal")):
         d = case[key]

@@ -56,7 +56,8 @@ class FlowCtrl(C.Structure):
                 ("n_outer", C.c_int32), ("n_corr", C.c_int32), ("n_non_orth_corr", C.c_int32),
                 ("momentum_predictor", C.c_int32), ("alpha_u", C.c_double), ("alpha_p", C.c_double),
                 ("p_ref_cell", C.c_int32), ("p_ref_value", C.c_double), ("U", SolverCtrl), ("p", SolverCtrl),
-                ("p_final", SolverCtrl), ("div_coeff", C.c_double)]
+                ("p_final", SolverCtrl), ("div_coeff", C.c_double), ("grad_scheme", C.c_int32),
+                ("grad_p_scheme", C.c_int32)]
 
 
 class StepInfo(C.Structure):

@@ -27,16 +27,36 @@ __device__ __forceinline__ double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.
 struct BFace {
     V3 de;
     bool value;
+    double nd;  // max(n.d, 0.05|d|) of a gradient constraint
 };
 
 __device__ __forceinline__ BFace lsBoundary(const double* Sf, const double* magSf, const double* d, int nF, int f,
                                             bool value) {
     const V3 dd = ld3(d, nF, f);
-    if (value) return BFace{dd, true};
+    if (value) return BFace{dd, true, 0.0};
     const double inv = 1.0 / magSf[f];
     const V3 n{Sf[f] * inv, Sf[nF + f] * inv, Sf[2 * nF + f] * inv};
     const double nd = fmax(dot3(n, dd), 0.05 * sqrt(dot3(dd, dd)));
-    return BFace{V3{n.x * nd, n.y * nd, n.z * nd}, false};
+    return BFace{V3{n.x * nd, n.y * nd, n.z * nd}, false, nd};
+}
+
+// The least-squares constraint kind of a boundary face: a value constraint where the patch's
+// condition fixes the value (lsFix per patch when given, else fixedValue), else a normal-gradient one
+__device__ __forceinline__ bool lsValue(const int32_t* bcType, const int32_t* lsFix, int p) {
+    return lsFix ? lsFix[p] != 0 : bcType[p] == 1;
+}
+
+// (gic psi_P + gbc) of a gradient-constrained face (Fvc.h:283-284): zeroGradient / symmetry 0, 0;
+// mixed -w dc, w dc v (refGrad 0); fixedGradient 0, g
+__device__ __forceinline__ double lsBoundaryGradient(int t, double psiP, double v, double w, double dc) {
+    double gic = 0.0, gbc = 0.0;
+    if (t == 4) {
+        gic = -w * dc;
+        gbc = w * dc * v + (1.0 - w) * 0.0;
+    } else if (t == 5) {
+        gbc = v;
+    }
+    return gic * psiP + gbc;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -75,6 +95,77 @@ __global__ void k_lap_boundary(int nB, int nI, const double* __restrict__ gs, co
     }
     ic[b] = 0.0 + gs[f] * gic;
     bs[b] = 0.0 - gs[f] * gbc;
+}
+
+// GaussSkew gradient (Fvc.h:233-262): Gauss with the face values w psi_P + (1-w) psi_N + (x_f - x'_f).
+// (w gls_P + (1-w) gls_N) on internal faces; on boundary faces the boundary value where the condition
+// fixes it, else psi_P + dt.gls_P + gb (n.d) with n.d unclipped, dt = d - n (n.d), gb = gic psi_P + gbc;
+// gls: the least-squares gradient (3 per cell)
+__global__ void k_grad_gauss_skew(int nC, int nI, int nF, const int32_t* __restrict__ cfOff,
+                                  const int32_t* __restrict__ cf, const int32_t* __restrict__ own,
+                                  const int32_t* __restrict__ nei, const double* __restrict__ w,
+                                  const double* __restrict__ Sf, const double* __restrict__ magSf,
+                                  const double* __restrict__ d, const double* __restrict__ V,
+                                  const double* __restrict__ skew, const double* __restrict__ ndc,
+                                  const double* __restrict__ psi, const double* __restrict__ psiB,
+                                  const double* __restrict__ gls, const int32_t* __restrict__ bPatch,
+                                  const int32_t* __restrict__ bcType, const int32_t* __restrict__ lsFix,
+                                  const double* __restrict__ bcValue, const double* __restrict__ frac, int twoD,
+                                  int emptyDir, double* __restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const uint32_t e = (uint32_t)cf[k];
+        const int f = (int)(e & 0x7fffffffu);
+        double phif;
+        if (f < nI) {
+            const int o = own[f], n = nei[f];
+            const double wf = w[f], wn = 1.0 - wf;
+            double gf[3];
+            for (int q = 0; q < 3; ++q) gf[q] = wf * gls[3 * o + q] + wn * gls[3 * n + q];
+            const double sk = skew[f] * gf[0] + skew[nF + f] * gf[1] + skew[2 * nF + f] * gf[2];
+            phif = (wf * psi[o] + wn * psi[n]) + sk;
+        } else {
+            const int b = f - nI, p = bPatch[b], o = own[f];
+            if (lsValue(bcType, lsFix, p)) {
+                phif = psiB[b];
+            } else {
+                const double inv = 1.0 / magSf[f];
+                const V3 n{Sf[f] * inv, Sf[nF + f] * inv, Sf[2 * nF + f] * inv};
+                const V3 dd = ld3(d, nF, f);
+                const double nd = dot3(n, dd);
+                const V3 dt{dd.x - n.x * nd, dd.y - n.y * nd, dd.z - n.z * nd};
+                const int t = bcType[p];
+                const double gb =
+                    lsBoundaryGradient(t, psi[o], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f]);
+                const double tg = dt.x * gls[3 * o] + dt.y * gls[3 * o + 1] + dt.z * gls[3 * o + 2];
+                phif = (psi[o] + tg) + gb * nd;
+            }
+        }
+        const double cx = Sf[f] * phif, cy = Sf[nF + f] * phif, cz = Sf[2 * nF + f] * phif;
+        if (e >> 31) {
+            gx -= cx;
+            gy -= cy;
+            gz -= cz;
+        } else {
+            gx += cx;
+            gy += cy;
+            gz += cz;
+        }
+    }
+    const double iv = 1.0 / V[c];
+    gx = gx * iv;
+    gy = gy * iv;
+    gz = gz * iv;
+    if (twoD) {
+        if (emptyDir == 0) gx = 0.0;
+        if (emptyDir == 1) gy = 0.0;
+        if (emptyDir == 2) gz = 0.0;
+    }
+    g[3 * c] = gx;
+    g[3 * c + 1] = gy;
+    g[3 * c + 2] = gz;
 }
 
 // diag[c] = -Σ upper; source[c] = Σ ∓ffc (Fvm.h:149-168), cell faces in ascending order
@@ -146,8 +237,10 @@ __global__ void k_grad_gauss(int nC, int nI, int nF, const int32_t* __restrict__
 __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cfOff, const int32_t* __restrict__ cf,
                           const int32_t* __restrict__ own, const int32_t* __restrict__ nei,
                           const double* __restrict__ Sf, const double* __restrict__ magSf, const double* __restrict__ d,
-                          const double* __restrict__ psi, const double* __restrict__ psiB,
-                          const int32_t* __restrict__ bPatch, const int32_t* __restrict__ bcType, int twoD,
+                          const double* __restrict__ ndc, const double* __restrict__ psi,
+                          const double* __restrict__ psiB, const int32_t* __restrict__ bPatch,
+                          const int32_t* __restrict__ bcType, const int32_t* __restrict__ lsFix,
+                          const double* __restrict__ bcValue, const double* __restrict__ frac, int twoD,
                           int emptyDir, double* __restrict__ g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
@@ -158,7 +251,7 @@ __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cf
         if (f < nI)
             v = ld3(d, nF, f);
         else
-            v = lsBoundary(Sf, magSf, d, nF, f, bcType[bPatch[f - nI]] == 1).de;
+            v = lsBoundary(Sf, magSf, d, nF, f, lsValue(bcType, lsFix, bPatch[f - nI])).de;
         const double s = 1.0 / dot3(v, v);
         const double o[9] = {v.x * v.x, v.x * v.y, v.x * v.z, v.y * v.x, v.y * v.y, v.y * v.z,
                              v.z * v.x, v.z * v.y, v.z * v.z};
@@ -188,15 +281,16 @@ __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cf
             v = ld3(d, nF, f);
             dp = psi[nei[f]] - psi[own[f]];
         } else {
-            const bool value = bcType[bPatch[f - nI]] == 1;
+            const int b = f - nI, p = bPatch[b];
+            const bool value = lsValue(bcType, lsFix, p);
             const BFace bfc = lsBoundary(Sf, magSf, d, nF, f, value);
             v = bfc.de;
             if (value) {
-                dp = psiB[f - nI] - psi[own[f]];
+                dp = psiB[b] - psi[own[f]];
             } else {
-                // zeroGradient: (gic psi_P + gbc)(n.d) with gic = gbc = 0
-                const double nd = sqrt(dot3(v, v));
-                dp = (0.0 * psi[own[f]] + 0.0) * nd;
+                const int t = bcType[p];
+                dp = lsBoundaryGradient(t, psi[own[f]], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f]) *
+                     bfc.nd;
             }
         }
         const double wgt = 1.0 / dot3(v, v);
@@ -392,7 +486,7 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
             skewMax = std::max(skewMax, sk);
         }
         skewed_ = skewMax > 1e-8;
-        if (skewed_) soa(skewVecs, skew_);
+        soa(skewVecs, skew_);  // kept on unskewed meshes too: the GaussSkew gradient reads them
     }
     // the correction is applied when any internal corrVec is non-zero (Fvm.h:156-158)
     for (int f = 0; f < nI_ && !nonOrth_; ++f) {
@@ -427,14 +521,23 @@ void DeviceGeom::correctBoundary(const double* psi, const ScalarBC& bc, double* 
 void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out,
                       cudaStream_t s) {
     uploadBCType(bc, s);
-    if (scheme == 1)
-        for (int32_t t : bcTypeHost_)
-            VLM_REQUIRE(t != 4 && t != 5, VLM_ERR_UNSUPPORTED,
-                        "the least-squares gradient supports zeroGradient and fixedValue boundaries only");
-    if (scheme == 1)
+    if (scheme == 2) {
+        VLM_REQUIRE(skew_.size() > 0, VLM_ERR_BAD_ARG, "the GaussSkew gradient needs the mesh's skew vectors");
+        scratchGls_.resize(size_t(3) * nC_);
         k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
-                                            Sf_.get(), magSf_.get(), d_.get(), psi, psiB, bPatch_.get(), bcType_.get(),
-                                            twoD_, emptyDir_, out), ++launches_;
+                                            Sf_.get(), magSf_.get(), d_.get(), ndc_.get(), psi, psiB, bPatch_.get(),
+                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_,
+                                            scratchGls_.get()), ++launches_;
+        k_grad_gauss_skew<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
+                                                    w_.get(), Sf_.get(), magSf_.get(), d_.get(), V_.get(), skew_.get(),
+                                                    ndc_.get(), psi, psiB, scratchGls_.get(), bPatch_.get(),
+                                                    bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_, out),
+            ++launches_;
+    } else if (scheme == 1)
+        k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
+                                            Sf_.get(), magSf_.get(), d_.get(), ndc_.get(), psi, psiB, bPatch_.get(),
+                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_, out),
+            ++launches_;
     else
         k_grad_gauss<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                                w_.get(), Sf_.get(), V_.get(), psi, psiB, twoD_, emptyDir_, out), ++launches_;

@@ -15,11 +15,13 @@ namespace vlm {
 // Scalar boundary conditions of one field: per patch 0 = zeroGradient (also a scalar symmetry plane),
 // 1 = fixedValue, 4 = mixed with refGrad 0 (value fraction per face in `frac`, reference value in
 // `value`; freestreamPressure), 5 = fixedGradient (the gradient in `value`); values per boundary
-// face, index f - nInternal.  Types 4 and 5 are for the Gauss gradient and the laplacian only.
+// face, index f - nInternal.
 struct ScalarBC {
     const int32_t* type = nullptr;  // host, nPatches
     const double* value = nullptr;  // device, nBoundary (may be null: 0)
     const double* frac = nullptr;   // device, nBoundary: value fractions of type-4 faces
+    const int32_t* lsFix = nullptr; // device, nPatches: least-squares value constraint (Fvc.h:267-287,
+                                    // bc.fixesValue()); null: the fixedValue patches
 };
 
 class DeviceGeom {
@@ -36,7 +38,8 @@ public:
     int nFaces() const { return nF_; }
     int nBoundary() const { return nF_ - nI_; }
     bool nonOrthogonal() const { return nonOrth_; }
-    bool skewed() const { return skewed_; }  // Mesh::skewed(); skew() is then the SoA x_f - x'_f
+    bool skewed() const { return skewed_; }
+    bool hasSkewVectors() const { return skew_.size() > 0; }  // Mesh::skewed(); skew() is then the SoA x_f - x'_f
 
     // fvm::laplacian(gamma, psi) for a scalar field (Fvm.h:141-182).  All pointers device.
     // gradScheme: 0 Gauss linear, 1 least squares.  ffc may be null when not needed.
@@ -44,7 +47,8 @@ public:
                    int gradScheme, double* diag, double* upper, double* source, double* ic, double* bs, double* ffc,
                    bool* hasFfc, cudaStream_t s);
 
-    // fvc::grad of a scalar (Fvc.h:209-291): out 3*nCells (x,y,z per cell).  psiB: boundary values.
+    // fvc::grad of a scalar (Fvc.h:209-291), scheme 0 Gauss linear, 1 leastSquares, 2 GaussSkew (needs
+    // the skew vectors): out 3*nCells (x,y,z per cell).  psiB: boundary values.
     void grad(const double* psi, const double* psiB, const ScalarBC& bc, int scheme, double* out, cudaStream_t s);
 
     // zeroGradient / fixedValue boundary values of a scalar field (correctBoundaryConditions)
@@ -85,7 +89,7 @@ public:
     const double* corr() const { return corr_.get(); }
     const double* C() const { return C_.size() ? C_.get() : nullptr; }
     const double* Cf() const { return Cf_.size() ? Cf_.get() : nullptr; }
-    const double* skew() const { return skew_.size() ? skew_.get() : nullptr; }
+    const double* skew() const { return skewed_ ? skew_.get() : nullptr; }  // null on unskewed meshes
     int twoD() const { return twoD_; }
     int64_t launches() const { return launches_; }  // kernels launched by the methods above
     int emptyDir() const { return emptyDir_; }
@@ -102,7 +106,7 @@ private:
     DBuf<double> magSf_, ndc_, V_, w_, Sf_, d_, corr_;  // vectors as SoA: [x(nF) y(nF) z(nF)]
     DBuf<double> C_, Cf_, skew_;                        // SoA; empty when not registered (skew_: not skewed)
     int64_t launches_ = 0;
-    DBuf<double> scratchG_, scratchGS_;
+    DBuf<double> scratchG_, scratchGS_, scratchGls_;
     void uploadBCType(const ScalarBC& bc, cudaStream_t s);
 };
 

@@ -571,6 +571,144 @@ __global__ void k_grad_ls_cells(int nC, int nI, int nF, int nB, const int32_t* _
             g[size_t(i * NC + j) * nC + c] = (twoD && i == emptyDir) ? 0.0 : acc[i * NC + j];
 }
 
+// (gic u_P + gbc) of component k of a U boundary face that the least-squares gradient constrains by its
+// normal gradient (Fvc.h:283-284): zeroGradient 0; symmetry -dc n_k^2 u_k + (-dc (n.u) n_k - gic u_k)
+// (VolField.h:183-191); mixed -w dc u_k + w dc v_k (refGrad 0); fixedGradient g_k;
+// pressureInletOutletVelocity dc (vic - 1) u_k + dc vbc (BoundaryCondition.h:357-360)
+__device__ __forceinline__ double u_ls_gradient(int t, int k, int b, int f, int c, int nB, int nC, int nF,
+                                                const double* __restrict__ Sf, const double* __restrict__ magSf,
+                                                double dc, const double* __restrict__ U,
+                                                const double* __restrict__ uValueB, const double* __restrict__ wIO,
+                                                const double* __restrict__ phi) {
+    const double uk = U[size_t(k) * nC + c];
+    double gic = 0.0, gbc = 0.0;
+    if (t == 2 || t == 6) {
+        const double A = magSf[f];
+        double n[3], u[3];
+        for (int j = 0; j < 3; ++j) {
+            n[j] = Sf[size_t(j) * nF + f] / A;
+            u[j] = U[size_t(j) * nC + c];
+        }
+        if (t == 2) {
+            const double dnu = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+            gic = -dc * (n[k] * n[k]);
+            gbc = (-dc * dnu) * n[k] - gic * uk;
+        } else {
+            double vic, fv;
+            if (phi[f] >= 0) {
+                vic = 1.0;
+                fv = uk;
+            } else {
+                double ut[3];
+                for (int j = 0; j < 3; ++j) ut[j] = uValueB[size_t(j) * nB + b];
+                vic = n[k] * n[k];
+                const double nu_ = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+                const double nt = n[0] * ut[0] + n[1] * ut[1] + n[2] * ut[2];
+                fv = nu_ * n[k] + (ut[k] - nt * n[k]);
+            }
+            const double vbc = fv - vic * uk;
+            gic = dc * (vic - 1.0);
+            gbc = dc * vbc;
+        }
+    } else if (t == 3 || t == 4) {
+        const double w = wIO[b];
+        gic = -w * dc;
+        gbc = w * dc * uValueB[size_t(k) * nB + b] + (1.0 - w) * 0.0;
+    } else if (t == 5) {
+        gbc = uValueB[size_t(k) * nB + b];
+    }
+    return gic * uk + gbc;
+}
+
+// grad U by least squares with U's boundary conditions (fvc::grad(U, leastSquares), Fvc.h:264-289 with
+// leastSquaresGrad :135-167 and finishGrad :169-181): value constraint (d, U_b - U_P) on the patches
+// whose condition fixes the value (uFix), else the normal-gradient constraint n max(n.d, 0.05|d|) with
+// (gic U_P + gbc) max(n.d, 0.05|d|).  Out: SoA rows 3 i + j = dU_j/dx_i.
+__global__ void k_grad_ls_u(int nC, int nI, int nF, int nB, const int32_t* __restrict__ cfOff,
+                            const int32_t* __restrict__ cf, const int32_t* __restrict__ own,
+                            const int32_t* __restrict__ nei, const double* __restrict__ Sf,
+                            const double* __restrict__ magSf, const double* __restrict__ d,
+                            const double* __restrict__ ndc, const double* __restrict__ U,
+                            const double* __restrict__ Ub, const int32_t* __restrict__ bPatch,
+                            const int32_t* __restrict__ uType, const int32_t* __restrict__ uFix,
+                            const double* __restrict__ uValueB, const double* __restrict__ wIO,
+                            const double* __restrict__ phi, int twoD, int emptyDir, double* __restrict__ G) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    // constraint vector of face f; nd set for a gradient constraint
+    auto faceVec = [&](int f, double v[3], double& nd) -> bool {
+        v[0] = d[f];
+        v[1] = d[nF + f];
+        v[2] = d[2 * size_t(nF) + f];
+        if (f < nI || uFix[bPatch[f - nI]]) return true;
+        const double inv = 1.0 / magSf[f];
+        const double n[3] = {Sf[f] * inv, Sf[nF + f] * inv, Sf[2 * size_t(nF) + f] * inv};
+        nd = fmax(n[0] * v[0] + n[1] * v[1] + n[2] * v[2], 0.05 * sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+        for (int k = 0; k < 3; ++k) v[k] = n[k] * nd;
+        return false;
+    };
+    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = int((uint32_t)cf[k] & 0x7fffffffu);
+        double v[3], nd = 0.0;
+        faceVec(f, v, nd);
+        const double s = 1.0 / (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double o[9] = {v[0] * v[0], v[0] * v[1], v[0] * v[2], v[1] * v[0], v[1] * v[1],
+                             v[1] * v[2], v[2] * v[0], v[2] * v[1], v[2] * v[2]};
+        for (int q = 0; q < 9; ++q) a[q] += o[q] * s;
+    }
+    if (twoD) a[4 * emptyDir] += 1.0;
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    double Gi[9];
+    Gi[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+    Gi[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+    Gi[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+    Gi[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+    Gi[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+    Gi[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+    Gi[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+    Gi[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+    Gi[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+    double acc[9];
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+    for (int k = cfOff[c]; k < cfOff[c + 1]; ++k) {
+        const int f = int((uint32_t)cf[k] & 0x7fffffffu);
+        double v[3], dp[3], nd = 0.0;
+        const bool value = faceVec(f, v, nd);
+        if (f < nI) {
+            for (int j = 0; j < 3; ++j) dp[j] = U[size_t(j) * nC + nei[f]] - U[size_t(j) * nC + own[f]];
+        } else if (value) {
+            for (int j = 0; j < 3; ++j) dp[j] = Ub[size_t(j) * nB + (f - nI)] - U[size_t(j) * nC + c];
+        } else {
+            const int b = f - nI, t = uType[bPatch[b]];
+            for (int j = 0; j < 3; ++j)
+                dp[j] = u_ls_gradient(t, j, b, f, c, nB, nC, nF, Sf, magSf, ndc[f], U, uValueB, wIO, phi) * nd;
+        }
+        const double wgt = 1.0 / (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double dw[3] = {v[0] * wgt, v[1] * wgt, v[2] * wgt};
+        const double Gd[3] = {Gi[0] * dw[0] + Gi[1] * dw[1] + Gi[2] * dw[2],
+                              Gi[3] * dw[0] + Gi[4] * dw[1] + Gi[5] * dw[2],
+                              Gi[6] * dw[0] + Gi[7] * dw[1] + Gi[8] * dw[2]};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) acc[3 * i + j] += Gd[i] * dp[j];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) G[size_t(3 * i + j) * nC + c] = (twoD && i == emptyDir) ? 0.0 : acc[3 * i + j];
+}
+
+__global__ void k_io_patch_reset(int nP, const int32_t* __restrict__ uType, int32_t* __restrict__ uFix) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nP && uType[q] == 3) uFix[q] = 0;
+}
+
+// inletOutlet patches fix U for the least-squares gradient while any face has inflow
+__global__ void k_io_patch_fix(int nB, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                               const double* __restrict__ wIO, int32_t* __restrict__ uFix) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nB && uType[bPatch[b]] == 3 && wIO[b] > 0) uFix[bPatch[b]] = 1;
+}
+
 // HbyA boundary values of the skew-corrected Rhie-Chow flux on fixes-flux faces: U_b + rAU_P grad p_P
 // (IncompressibleFlow.cpp:262-272); gp: 3 per cell
 __global__ void k_hbya_bval(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
@@ -738,6 +876,12 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     VLM_REQUIRE(batch_.plan().nsys == 1, VLM_ERR_UNSUPPORTED, "the device flow step runs on a single-system mesh");
     VLM_REQUIRE(ctrl_.div_scheme >= 0 && ctrl_.div_scheme <= 7, VLM_ERR_BAD_ARG, "unknown divergence scheme");
     if (ctrl_.div_coeff == 0) ctrl_.div_coeff = 1.0;
+    VLM_REQUIRE(ctrl_.grad_scheme == 0 || ctrl_.grad_scheme == 1, VLM_ERR_BAD_ARG,
+                "grad_scheme must be 0 (Gauss linear) or 1 (leastSquares)");
+    VLM_REQUIRE(ctrl_.grad_p_scheme >= 0 && ctrl_.grad_p_scheme <= 2, VLM_ERR_BAD_ARG,
+                "grad_p_scheme must be 0 (Gauss linear), 1 (leastSquares) or 2 (GaussSkew)");
+    VLM_REQUIRE(ctrl_.grad_p_scheme != 2 || G_.hasSkewVectors(), VLM_ERR_BAD_ARG,
+                "the GaussSkew pressure gradient needs the mesh registered with its skew vectors");
     VLM_REQUIRE(ctrl_.ddt_scheme >= 0 && ctrl_.ddt_scheme <= 2, VLM_ERR_BAD_ARG, "unknown ddt scheme");
     VLM_REQUIRE(ctrl_.nu > 0, VLM_ERR_BAD_ARG, "nu must be positive");
     VLM_REQUIRE(ctrl_.n_corr >= 1 && ctrl_.n_outer >= 1 && ctrl_.n_non_orth_corr >= 0, VLM_ERR_BAD_ARG,
@@ -811,6 +955,30 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     }
     if (needRef_)
         VLM_REQUIRE(ctrl_.p_ref_cell >= 0 && ctrl_.p_ref_cell < nC_, VLM_ERR_BAD_ARG, "reference cell out of range");
+    {
+        // the patches whose conditions fix the value, for the least-squares gradients (bc.fixesValue():
+        // fixedValue, totalPressure, and mixed conditions with a positive value fraction somewhere;
+        // inletOutlet's flags follow the flux at every gradient)
+        std::vector<double> wu(nBb, 0.0), wp(nBb, 0.0);
+        if (nB_ > 0) {
+            VLM_CUDA(cudaMemcpyAsync(wu.data(), wIO_.get(), sizeof(double) * nBb, cudaMemcpyDeviceToHost, s_));
+            VLM_CUDA(cudaMemcpyAsync(wp.data(), pFrac_.get(), sizeof(double) * nBb, cudaMemcpyDeviceToHost, s_));
+            VLM_CUDA(cudaStreamSynchronize(s_));
+        }
+        std::vector<int32_t> uf(size_t(std::max(nP, 1)), 0), pf(size_t(std::max(nP, 1)), 0);
+        for (int q = 0; q < nP; ++q) {
+            uf[q] = uType[q] == 1;
+            pf[q] = pType[q] == 1 || pType[q] == 7;
+            for (int i = 0; i < G_.patchSize()[q]; ++i) {
+                const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
+                if (uType[q] == 4 && wu[b] > 0) uf[q] = 1;
+                if (pType[q] == 4 && wp[b] > 0) pf[q] = 1;
+            }
+        }
+        uLsFix_.upload(uf, s_);
+        pLsFix_.upload(pf, s_);
+        VLM_CUDA(cudaStreamSynchronize(s_));
+    }
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1)), FI = size_t(std::max(nI_, 1)), F = size_t(nF_);
     for (DBuf<double>* b : {&U_, &U0_, &U00_, &src_, &msrc_, &HbyA_}) b->resize(3 * N);
     for (DBuf<double>* b : {&Ub_, &ic_, &bs_}) b->resize(3 * B);
@@ -943,10 +1111,24 @@ void DeviceFlow::boundaryP() {
     bc.type = pTypeAsm_.data();
     bc.value = pValueB_.get();
     bc.frac = pFrac_.get();
+    bc.lsFix = pLsFix_.get();
     G_.correctBoundary(p_.get(), bc, pB_.get(), s_);
 }
 
 void DeviceFlow::gradU() {
+    if (ctrl_.grad_scheme == 1) {
+        if (hasInletOutlet_ && nB_ > 0) {
+            k_io_patch_reset<<<nblk(G_.nPatches()), 256, 0, s_>>>(G_.nPatches(), uType_.get(), uLsFix_.get()),
+                ++launches_;
+            k_io_patch_fix<<<nblk(nB_), 256, 0, s_>>>(nB_, G_.bPatch(), uType_.get(), wIO_.get(), uLsFix_.get()),
+                ++launches_;
+        }
+        k_grad_ls_u<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
+                                               G_.nei(), G_.Sf(), G_.magSf(), G_.d(), G_.ndc(), U_.get(), Ub_.get(),
+                                               G_.bPatch(), uType_.get(), uLsFix_.get(), uValueB_.get(), wIO_.get(),
+                                               phi_.get(), G_.twoD(), G_.emptyDir(), gU_.get()), ++launches_;
+        return;
+    }
     k_grad_tensor<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, nF_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
                                             G_.w(), G_.Sf(), G_.V(), U_.get(), Ub_.get(), G_.twoD(), G_.emptyDir(),
                                             gU_.get()), ++launches_;
@@ -1169,7 +1351,8 @@ void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     pbc.type = pTypeAsm_.data();
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
-    G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+    pbc.lsFix = pLsFix_.get();
+    G_.grad(p_.get(), pB_.get(), pbc, ctrl_.grad_p_scheme, gP_.get(), s_);
     k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get()), ++launches_;
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
     if (componentBatch()) {
@@ -1224,11 +1407,12 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     pbc.type = pTypeAsm_.data();
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
+    pbc.lsFix = pLsFix_.get();
     const bool skewed = G_.skewed();
     if (skewed) {
         // skewed mesh (IncompressibleFlow.cpp:252-275): grad rAU by least squares with zero-gradient
         // boundaries; grad HbyA by least squares with the fixes-flux faces at U_b + rAU_P grad p_P
-        G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+        G_.grad(p_.get(), pB_.get(), pbc, ctrl_.grad_p_scheme, gP_.get(), s_);
         if (nB_ > 0)
             k_hbya_bval<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.own(), G_.bPatch(), uFixesFlux_.get(), Ub_.get(),
                                                   rAU_.get(), gP_.get(), hB_.get()), ++launches_;
@@ -1255,7 +1439,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     for (int no = 0; no <= nNO; ++no) {
         const bool finalNO = no == nNO;
         bool hasFfc = false;
-        G_.laplacian(rAUf_.get(), p_.get(), pB_.get(), pbc, true, 0, pdiag_.get(), pupper_.get(), psrc_.get(),
+        G_.laplacian(rAUf_.get(), p_.get(), pB_.get(), pbc, true, ctrl_.grad_scheme, pdiag_.get(), pupper_.get(), psrc_.get(),
                      pic_.get(), pbs_.get(), pffc_.get(), &hasFfc, s_);
         G_.addVolumeSource(psrc_.get(), divPhi_.get(), s_);
         if (needRef_) G_.setReference(ctrl_.p_ref_cell, ctrl_.p_ref_value, pdiag_.get(), psrc_.get(), s_);
@@ -1275,7 +1459,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
         k_p_relax<<<nblk(nC_), 256, 0, s_>>>(nC_, pPrev_.get(), ctrl_.alpha_p, p_.get()), ++launches_;
         boundaryP();
     }
-    G_.grad(p_.get(), pB_.get(), pbc, 0, gP_.get(), s_);
+    G_.grad(p_.get(), pB_.get(), pbc, ctrl_.grad_p_scheme, gP_.get(), s_);
     k_u_correct<<<nblk(nC_), 256, 0, s_>>>(nC_, HbyA_.get(), rAU_.get(), gP_.get(), G_.twoD(), G_.emptyDir(),
                                           U_.get()), ++launches_;
     boundaryU();

@@ -20,8 +20,9 @@
 // fixedFluxPressure and totalPressure for p, empty (2D) directions and
 // cyclic (internal) faces, skewed meshes (the skew corrections of linear / LUST div, rAUf, the
 // Rhie-Chow flux and the initial flux), the LES Smagorinsky model with Van Driest damping and
-// constant / mean-velocity momentum forcing (flow_les.cu).  Not supported: other turbulence models,
-// wall models, buoyancy body forces, ddtPhiCoeff, the leastSquares / GaussSkew gradient schemes.
+// constant / mean-velocity momentum forcing (flow_les.cu), Gauss or leastSquares mesh-default gradients
+// and Gauss / leastSquares / GaussSkew pressure gradients.  Not supported: other turbulence models,
+// wall models, buoyancy body forces, ddtPhiCoeff.
 #pragma once
 
 #include <cstdint>
@@ -125,6 +126,7 @@ private:
                                       // step start), freestream (constant)
     DBuf<double> pFrac_;              // freestreamPressure value fraction per boundary face
     DBuf<double> pTotal_;             // totalPressure p0 per boundary face
+    DBuf<int32_t> uLsFix_, pLsFix_;   // per patch: the condition fixes the value (least-squares gradients)
     DBuf<int32_t> pType_;
     DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry)
     bool hasInletOutlet_ = false;
