@@ -653,6 +653,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
                                                                  const double* __restrict__ inv, const T* r0, T* x0,
                                                                  T omega, const SysState* st, int flag, int jacobi0) {
     pdl_entry();
+    __shared__ T resS[kTailFullRows];  // one level's residuals (restriction)
     const TailSys& ts = tsys[blockIdx.x];
     if (st != nullptr && sys_idle(st[ts.sys], flag)) return;  // uniform over the CTA
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -715,20 +716,34 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
         }
         __syncthreads();
         }
-        // residual of each child computed where its aggregate sums it (k_residual + k_restrict)
+        // k_residual + k_restrict: every row's residual (one row per thread, into shared memory where
+        // the level fits), then each aggregate sums its children's residuals in child order
         T* rn = lev[k + 1].r;
         auto xr = [&](int j) -> T { return x[j]; };
         const int b0 = ts.rowStart[k + 1], b1 = b0 + ts.rowCount[k + 1];
-        for (int R = b0 + tid; R < b1; R += nthr) {
-            T s = T(0);
-            const int q1 = __ldg(L.cptr + R + 1);
-            for (int q = __ldg(L.cptr + R); q < q1; ++q) {
-                const int i = __ldg(L.child + q);
-                const T t = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
-                                                                               r[i] - __ldg(L.diag + i) * x[i]);
-                s += t;
+        if (a1 - a0 <= kTailFullRows) {
+            for (int i = a0 + tid; i < a1; i += nthr)
+                resS[i - a0] = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
+                                                                                 r[i] - __ldg(L.diag + i) * x[i]);
+            __syncthreads();
+            for (int R = b0 + tid; R < b1; R += nthr) {
+                T s = T(0);
+                const int q1 = __ldg(L.cptr + R + 1);
+                for (int q = __ldg(L.cptr + R); q < q1; ++q) s += resS[__ldg(L.child + q) - a0];
+                rn[R] = s;
             }
-            rn[R] = s;
+        } else {
+            for (int R = b0 + tid; R < b1; R += nthr) {
+                T s = T(0);
+                const int q1 = __ldg(L.cptr + R + 1);
+                for (int q = __ldg(L.cptr + R); q < q1; ++q) {
+                    const int i = __ldg(L.child + q);
+                    const T t = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
+                                                                                   r[i] - __ldg(L.diag + i) * x[i]);
+                    s += t;
+                }
+                rn[R] = s;
+            }
         }
         __syncthreads();
     }
