@@ -469,8 +469,18 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
             VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         } else {
-            VLM_LAUNCH((k_smooth_jacobi<T, 2>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
-                       om, agg, xc, st, flag);
+            if (k > 0) {
+                // coarse levels: the correction x += xc[agg] as its own coalesced pass, then a plain
+                // sweep (same values: the fused sweep adds xc[agg[j]] to every neighbour it reads, two
+                // more dependent loads per entry, and measured slower); level-0 chunks may be wider
+                // than k_prolong covers, so level 0 keeps the fused sweep
+                VLM_LAUNCH(k_prolong<T>, rows.n, kRowsPerCta, s, D.ch(rows), agg, xc, x, st, flag);
+                VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
+                           om, agg, xc, st, flag);
+            } else {
+                VLM_LAUNCH((k_smooth_jacobi<T, 2>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
+                           om, agg, xc, st, flag);
+            }
             VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         }
