@@ -786,13 +786,14 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
                 }
             continue;
         }
-        // post-sweep 1 with the coarse-grid correction fused in (MODE 2), into x2
-        auto xv = [&](int j) -> T {
-            T v = x[j];
-            const int a = __ldg(L.agg + j);
-            if (a >= 0) v += xc[a];
-            return v;
-        };
+        // the coarse-grid correction x += xc[agg] as its own phase, then post-sweep 1 into x2 (the same
+        // values as adding xc[agg[j]] to every neighbour read, without the two dependent loads per entry)
+        for (int i = a0 + tid; i < a1; i += nthr) {
+            const int a = __ldg(L.agg + i);
+            if (a >= 0) x[i] += xc[a];
+        }
+        __syncthreads();
+        auto xv = [&](int j) -> T { return x[j]; };
         for (int i = a0 + tid; i < a1; i += nthr) {
             const T s = row_accumulate<true, T, decltype(xv), kTailBatch>(L.S, L.val, xv, i, r[i]);
             const T v = s / __ldg(L.diag + i);

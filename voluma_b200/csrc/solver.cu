@@ -460,7 +460,7 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
     const T* xc = k + 1 < int(L_.size()) ? LV<T>::x(L_[k + 1]) : nullptr;
     const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
     if (jacobiHere) {
-        // Jacobi; pre: from zero, post: prolongation fused into the first sweep
+        // Jacobi; pre: from zero, post: after the ascent's prolongation pass
         const T om = T(jacobiOmega_);
         const ChunkList& rows = head ? D.headActive : D.active;
         if (pre) {
@@ -469,18 +469,11 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
             VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         } else {
-            if (k > 0) {
-                // coarse levels: the correction x += xc[agg] as its own coalesced pass, then a plain
-                // sweep (same values: the fused sweep adds xc[agg[j]] to every neighbour it reads, two
-                // more dependent loads per entry, and measured slower); level-0 chunks may be wider
-                // than k_prolong covers, so level 0 keeps the fused sweep
-                VLM_LAUNCH(k_prolong<T>, rows.n, kRowsPerCta, s, D.ch(rows), agg, xc, x, st, flag);
-                VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
-                           om, agg, xc, st, flag);
-            } else {
-                VLM_LAUNCH((k_smooth_jacobi<T, 2>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
-                           om, agg, xc, st, flag);
-            }
+            // the correction x += xc[agg] as its own coalesced pass (the ascent launches k_prolong), then
+            // plain sweeps: the same values as a first sweep that adds xc[agg[j]] to every neighbour it
+            // reads, which pays two more dependent loads per entry and measured slower
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
+                       om, agg, xc, st, flag);
             VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
                        om, agg, xc, st, flag);
         }
@@ -559,8 +552,11 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
     for (int k = headEnd - 1; k >= 0; --k) {
         DevLevel& D = L_[k];
         const bool jacobiHere = sm == SmootherKind::Jacobi || (sm == SmootherKind::MCGSJacobi && k > 0);
-        // block GS, Jacobi and two-colour GS fuse the prolongation into their first sweep
-        if (!jacobiHere && !D.blockGS && D.nSteps != 2) {
+        // block GS and two-colour GS fuse the prolongation into their first sweep (for two colours
+        // the separate pass measured no faster); Jacobi (on any level layout) and multicolour GS
+        // with more colours sweep after this pass (active chunks are at most kRowsPerCta rows, one
+        // per k_prolong thread)
+        if (jacobiHere || (!D.blockGS && D.nSteps != 2)) {
             const ChunkList& rows = tail ? D.headActive : D.active;
             VLM_LAUNCH(k_prolong<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.agg.get(), xx(k + 1), xx(k), st, flag);
         }
