@@ -191,7 +191,9 @@ vlm_status vlm_gamg_colours(vlm_mesh* mesh, int32_t level, int32_t* n_colours);
 
 /* ------------------------------------------------------------------ assembly */
 /* fvm::laplacian(gamma, psi, nonOrthCorr) for a scalar field with per-patch BCs
- * (bc_type[p]: 0 zeroGradient, 1 fixedValue with values bc_values[f - n_internal_faces]).
+ * (bc_type[p]: 0 zeroGradient, 1 fixedValue with values bc_values[f - n_internal_faces], 2 symmetry
+ * (zeroGradient for a scalar), 5 fixedGradient with the normal gradients in bc_values; other types
+ * are rejected with VLM_ERR_BAD_ARG).
  * grad_scheme for the non-orthogonal correction: 0 Gauss linear, 1 leastSquares.
  * Outputs (host): diag[n_cells], upper[n_internal], source[n_cells],
  * internal_coeffs[n_boundary], boundary_source[n_boundary], ffc[n_faces], *has_ffc. */

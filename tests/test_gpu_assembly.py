@@ -72,3 +72,23 @@ def test_pressure_loop_gamg(name):
     # both solutions satisfy relTol 1e-8; they agree to the solver tolerance
     assert rel(p, g["ps_p"]) <= 1e-5
     assert rel(flux, g["ps_flux"]) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_scalar_boundary_types_checked():
+    # a mixed boundary needs value fractions that only the flow step supplies, and unknown types are
+    # refused: neither reaches a kernel
+    from voluma_b200 import mesh as vm
+    M = vm.box_mesh((6, 5, 4))
+    m = vb.Mesh.from_arrays(M)
+    nP = len(M["patch_start"])
+    psi = np.linspace(0.0, 1.0, M["n_cells"])
+    for t in (3, 4, 9, -1):
+        with pytest.raises(vb.VlmError):
+            vb.grad(m, psi, np.full(nP, t, np.int32))
+        with pytest.raises(vb.VlmError):
+            vb.laplacian(m, np.ones(M["n_faces"]), psi, np.full(nP, t, np.int32))
+    # symmetry is a zero gradient for a scalar; a zero fixedGradient is too
+    g0 = vb.grad(m, psi, np.zeros(nP, np.int32))
+    assert np.array_equal(vb.grad(m, psi, np.full(nP, 2, np.int32)), g0)
+    assert np.array_equal(vb.grad(m, psi, np.full(nP, 5, np.int32), np.zeros(M["n_faces"] - M["n_internal_faces"])), g0)

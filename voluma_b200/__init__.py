@@ -410,7 +410,8 @@ def _bc(mesh: Mesh, bc_type, bc_values):
 
 def laplacian(mesh: Mesh, gamma, psi, bc_type=None, bc_values=None, non_orth_corr=True, grad_scheme=0):
     """fvm::laplacian(gamma, psi) (Fvm.h:141-182) of a scalar field: dict of diag, upper, source,
-    internalCoeffs, boundarySource, ffc, hasFfc.  bc_type per patch: 0 zeroGradient, 1 fixedValue."""
+    internalCoeffs, boundarySource, ffc, hasFfc.  bc_type per patch: 0 zeroGradient, 1 fixedValue,
+    2 symmetry (a zero gradient), 5 fixedGradient (bc_values are the gradients)."""
     nC, nI, nF = mesh.n_cells, mesh.n_internal_faces, mesh.n_faces
     out = dict(diag=np.zeros(nC), upper=np.zeros(nI), source=np.zeros(nC), internalCoeffs=np.zeros(nF - nI),
                boundarySource=np.zeros(nF - nI), ffc=np.zeros(nF))
@@ -425,7 +426,8 @@ def laplacian(mesh: Mesh, gamma, psi, bc_type=None, bc_values=None, non_orth_cor
 
 
 def grad(mesh: Mesh, psi, bc_type=None, bc_values=None, scheme=0):
-    """fvc::grad of a scalar (Fvc.h:209-291): (n_cells, 3); scheme 0 Gauss linear, 1 least squares."""
+    """fvc::grad of a scalar (Fvc.h:209-291): (n_cells, 3); scheme 0 Gauss linear, 1 least squares,
+    2 GaussSkew (the mesh registered with skewVecs)."""
     g = np.zeros((mesh.n_cells, 3))
     t, v = _bc(mesh, bc_type, bc_values)
     check(load().vlm_grad(mesh.ctx.handle, mesh.handle, _ptr(_f64(psi)), _ptr(t), _ptr(v), int(scheme), _ptr(g)),

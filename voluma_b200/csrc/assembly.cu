@@ -503,7 +503,12 @@ DeviceGeom::DeviceGeom(int nCells, int nInternal, int nFaces, const int32_t* own
 // from pageable memory waits for the stream, which would stall every assembly call).
 void DeviceGeom::uploadBCType(const ScalarBC& bc, cudaStream_t s) {
     std::vector<int32_t> t(bcType_.size(), 0);
-    for (size_t p = 0; p < patchStart_.size(); ++p) t[p] = bc.type ? bc.type[p] : 0;
+    for (size_t p = 0; p < patchStart_.size(); ++p) {
+        t[p] = bc.type ? bc.type[p] : 0;
+        VLM_REQUIRE(t[p] == 0 || t[p] == 1 || t[p] == 2 || t[p] == 4 || t[p] == 5, VLM_ERR_BAD_ARG,
+                    "scalar boundary type must be 0 zeroGradient, 1 fixedValue, 2 symmetry, 4 mixed or 5 fixedGradient");
+        VLM_REQUIRE(t[p] != 4 || bc.frac != nullptr, VLM_ERR_BAD_ARG, "a mixed boundary needs its value fractions");
+    }
     if (t == bcTypeHost_) return;
     VLM_CUDA(cudaMemcpyAsync(bcType_.get(), t.data(), sizeof(int32_t) * t.size(), cudaMemcpyHostToDevice, s));
     VLM_CUDA(cudaStreamSynchronize(s));  // t is a local
