@@ -258,6 +258,12 @@ vlm_status vlm_topology_levels(const vlm_topology* t, int32_t* n_levels);
 vlm_status vlm_topology_level(const vlm_topology* t, int32_t level, int32_t* sizes, int32_t* l, int32_t* u,
                               double* weight, int32_t* agg, int32_t* face_map, int8_t* face_flip,
                               int32_t* colour);
+/* Whether the mesh is a generateBox mesh (src/fvm/mesh/RawMesh.cpp:391-502), read from its face
+ * arrays: shape = {nx, ny, nz, periodic x, y, z, box layout}; nx = 0 when it is not a box.  The
+ * last entry is 1 when level 0 of its solves runs the structured box kernels (every periodic extent
+ * even and the natural-order colouring red-black).  No reference counterpart: the reference has no
+ * structured path. */
+vlm_status vlm_topology_box(const vlm_topology* t, int32_t* shape);
 vlm_status vlm_topology_destroy(vlm_topology* t);
 
 /* ------------------------------------------------------------------ reductions */

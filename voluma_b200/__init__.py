@@ -374,6 +374,28 @@ def topology(n_cells, owner, neighbour, magSf, ndc, merge_levels: int = 2):
         L.vlm_topology_destroy(h)
 
 
+def box_shape(n_cells, owner, neighbour, magSf=None, ndc=None):
+    """Whether the face arrays are those of a generateBox mesh (no GPU needed): a dict with the
+    shape n = (nx, ny, nz), the periodic flags and `layout` (level 0 of its solves runs the
+    structured box kernels), or None when the mesh is not a box."""
+    L = load()
+    own = np.ascontiguousarray(owner, np.int32)
+    nei = np.ascontiguousarray(neighbour, np.int32)
+    magSf = np.ones(nei.size) if magSf is None else magSf
+    ndc = np.ones(nei.size) if ndc is None else ndc
+    h = C.c_void_p()
+    check(L.vlm_topology_build(int(n_cells), nei.size, _ptr(own), _ptr(nei), _ptr(_f64(magSf)), _ptr(_f64(ndc)),
+                               2, C.byref(h)))
+    try:
+        s = np.zeros(7, np.int32)
+        check(L.vlm_topology_box(h, _ptr(s)))
+    finally:
+        L.vlm_topology_destroy(h)
+    if s[0] == 0:
+        return None
+    return dict(n=tuple(int(v) for v in s[:3]), periodic=tuple(bool(v) for v in s[3:6]), layout=bool(s[6]))
+
+
 def solve_ldu(mesh: Mesh, diag, upper, lower, b, x, ctrl: SolverControls) -> SolverPerformance:
     """solveLdu (LinearSolver.cpp:135): solves in place into x (float64 numpy array)."""
     if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):

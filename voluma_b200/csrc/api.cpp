@@ -26,6 +26,8 @@ struct vlm_topology {
     vlm::Hierarchy H;
     std::vector<std::vector<int>> colour;
     std::vector<int> nColours;
+    vlm::BoxShape box;   // n[0] == 0: not a box mesh
+    bool boxLayout = false;
 };
 
 struct vlm_mesh {
@@ -421,6 +423,11 @@ vlm_status vlm_topology_build(int32_t n_cells, int32_t n_internal_faces, const i
             t->colour.push_back(vlm::greedyColour(L, &nc));
             t->nColours.push_back(nc);
         }
+        if (vlm::detectBox(n_cells, n_internal_faces, owner, neighbour, &t->box))
+            t->boxLayout = t->H.levels.size() <= 1 ||
+                           vlm::boxParityColouring(t->box, t->colour[0].data(), t->nColours[0]);
+        else
+            t->box = vlm::BoxShape();
         *out = t.release();
     });
 }
@@ -448,6 +455,16 @@ vlm_status vlm_topology_level(const vlm_topology* t, int32_t level, int32_t* siz
     if (face_flip)
         for (size_t k = 0; k < L.faceFlip.size(); ++k) face_flip[k] = int8_t(L.faceFlip[k]);
     if (colour) std::copy(t->colour[level].begin(), t->colour[level].end(), colour);
+    return VLM_OK;
+}
+
+vlm_status vlm_topology_box(const vlm_topology* t, int32_t* shape) {
+    if (!t || !shape) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    for (int d = 0; d < 3; ++d) {
+        shape[d] = t->box.n[d];
+        shape[3 + d] = t->box.per[d];
+    }
+    shape[6] = t->boxLayout ? 1 : 0;
     return VLM_OK;
 }
 

@@ -50,7 +50,7 @@ void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slo
 
 }  // namespace
 
-BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
+BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox) {
     BatchPlan P;
     const int ns = int(systems.size());
     if (ns == 0) throw std::invalid_argument("empty batch");
@@ -112,6 +112,28 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
     const int Lmax = P.nLevels[0];
     P.levels.resize(Lmax);
 
+    // ---------------------------------------------------------------- box level 0
+    // Every system a box mesh with even periodic extents that smooths on level 0 (a one-level system
+    // solves level 0 directly, in natural row order), and its natural-order colouring the parity
+    // colouring: level 0 takes the box layout (box.h).
+    std::vector<BoxShape> shapes(ns);
+    bool boxMode = useBox;
+    for (int b = 0; b < ns && boxMode; ++b) {
+        const SysTopo& T = systems[P.order[b]];
+        BoxShape& S = shapes[b];
+        if (!detectBox(T.nCells, T.nInternal, T.own, T.nei, &S)) {
+            boxMode = false;
+            break;
+        }
+        for (int d = 0; d < 3; ++d)
+            if (S.per[d] && S.n[d] % 2 != 0) boxMode = false;
+        if (P.nLevels[b] <= 1) boxMode = false;
+        if (!boxMode) continue;
+        int nc = 0;
+        const std::vector<int> colour = greedyColour(P.H[b].levels[0], &nc);
+        boxMode = boxParityColouring(S, colour.data(), nc);
+    }
+
     // ---------------------------------------------------------------- row layout per level
     // rowOf[k][b][natural] -> solver row
     std::vector<std::vector<std::vector<int32_t>>> rowOf(Lmax, std::vector<std::vector<int32_t>>(ns));
@@ -122,6 +144,8 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
         int present = 0, active = 0;
         if (k > 0) {
             LP.blockGS = true;
+        } else if (boxMode) {
+            LP.box = true;
         } else {
             // level 0: global multicolour GS if every smoothing system needs few colours
             for (int b = 0; b < ns; ++b) {
@@ -158,7 +182,41 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
                     ++row;
                 }
             };
-            if (b < active && !LP.blockGS) {
+            if (LP.box) {
+                // colour groups in slot order (box.h); slots past the x-row's end are padding
+                const BoxShape& S = shapes[b];
+                const int nx = S.n[0], ny = S.n[1], nz = S.n[2], H = (nx + 1) / 2;
+                BoxSys bs;
+                bs.nx = nx;
+                bs.ny = ny;
+                bs.nz = nz;
+                bs.H = H;
+                bs.per = S.per[0] | S.per[1] << 1 | S.per[2] << 2;
+                bs.slots = H * ny * nz;
+                bs.divH = makeFastDiv(uint32_t(H));
+                bs.divNy = makeFastDiv(uint32_t(ny));
+                for (int C = 0; C < 2; ++C) {
+                    const int g0 = row;
+                    (C == 0 ? bs.base0 : bs.base1) = row;
+                    for (int q = 0; q < ny * nz; ++q) {
+                        const int j = q % ny, kk = q / ny;
+                        for (int m = 0; m < H; ++m) {
+                            const int i = 2 * m + ((j + kk + C) & 1);
+                            if (i < nx) {
+                                place(i + nx * q);
+                            } else {
+                                LP.natural.push_back(-1);
+                                LP.rowSys.push_back(-1);
+                                ++row;
+                            }
+                        }
+                    }
+                    pad();
+                    if (b < active) groups[k][b].push_back({g0, row - g0});
+                }
+                if (b < active) LP.maxColours = std::max(LP.maxColours, 2);
+                LP.boxes.push_back(bs);
+            } else if (b < active && !LP.blockGS) {
                 int nc = 0;
                 const std::vector<int> colour = greedyColour(L, &nc);
                 LP.maxColours = std::max(LP.maxColours, nc);
@@ -230,6 +288,35 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels) {
                     appendChunks(LP.rev[t], g[nc - 1 - t].first, g[nc - 1 - t].second, b, nullptr);
                 }
             }
+    }
+
+    // ---------------------------------------------------------------- box face map
+    if (P.levels[0].box) {
+        LevelPlan& LP = P.levels[0];
+        const size_t nr = size_t(LP.nrows);
+        LP.boxFace.assign(3 * nr, -1);
+        for (int b = 0; b < int(LP.sysRow.size()) - 1; ++b) {
+            const SysTopo& T = systems[P.order[b]];
+            const BoxShape& S = shapes[b];
+            const int nx = S.n[0], nxny = S.n[0] * S.n[1];
+            for (int f = 0; f < T.nInternal; ++f) {
+                const int o = T.own[f], n = T.nei[f];
+                const int io = o % nx, jo = (o / nx) % S.n[1], ko = o / nxny;
+                const int in = n % nx, jn = (n / nx) % S.n[1], kn = n / nxny;
+                int d, minus;
+                if (jo == jn && ko == kn) {
+                    d = 0;
+                    minus = in == io + 1 ? o : n;  // cyclic: the max-side cell is the minus side
+                } else if (io == in && ko == kn) {
+                    d = 1;
+                    minus = jn == jo + 1 ? o : n;
+                } else {
+                    d = 2;
+                    minus = kn == ko + 1 ? o : n;
+                }
+                LP.boxFace[size_t(d) * nr + size_t(rowOf[0][b][minus])] = LP.sysFace[b] + f;
+            }
+        }
     }
 
     // ---------------------------------------------------------------- SELL-32 structure

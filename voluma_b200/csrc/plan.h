@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "box.h"
 #include "common.h"
 #include "hierarchy.h"
 
@@ -54,6 +55,11 @@ struct LevelPlan {
     std::vector<int32_t> childPtr, child;         // next-level row -> rows, ascending natural index
     std::vector<int32_t> intraPtr, intraFace;     // next-level row -> this-level faces inside it
     std::vector<int32_t> cfacePtr, cfaceSrc;      // next-level face -> this-level faces | flip<<31
+    // level 0 of a batch of box meshes (box.h): per batch position its descriptor, and per
+    // direction d and solver row the user face to the row's +d neighbour (-1: none)
+    bool box = false;
+    std::vector<BoxSys> boxes;
+    std::vector<int32_t> boxFace;                 // [d * nrows + row]
 };
 
 struct CoarsePlan {
@@ -77,6 +83,8 @@ struct BatchPlan {
     int nSlots = 0;
 };
 
-BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels);
+// useBox: lay level 0 out for the structured box kernels when every system is a box mesh whose
+// natural-order colouring is the red-black parity colouring.
+BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox = true);
 
 }  // namespace vlm

@@ -12,6 +12,7 @@
 #include <set>
 #include <utility>
 
+#include "boxkernels.cuh"
 #include "dilu.cuh"
 #include "krylov.cuh"
 #include "solver.h"
@@ -123,6 +124,7 @@ template <> struct LV<double> {
     static double* x2(DevLevel& L) { return L.x2.get(); }
     static const double* val(const DevLevel& L) { return L.val.get(); }
     static const double* diag(const DevLevel& L) { return L.diag.get(); }
+    static const double* bcoef(const DevLevel& L) { return L.bcoef.get(); }
 };
 template <> struct LV<float> {
     static float* r(DevLevel& L) { return L.r32.get(); }
@@ -131,6 +133,7 @@ template <> struct LV<float> {
     static float* x2(DevLevel& L) { return L.x232.get(); }
     static const float* val(const DevLevel& L) { return L.val32.get(); }
     static const float* diag(const DevLevel& L) { return L.diag32.get(); }
+    static const float* bcoef(const DevLevel& L) { return L.bcoef32.get(); }
 };
 
 __global__ void k_set_cond(cudaGraphConditionalHandle h, int nsys, const SysState* st, int flag) {
@@ -158,7 +161,9 @@ std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
 // ====================================================================== construction
 DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
     : stream_(stream), topo_(systems), mergeLevels_(mergeLevels) {
-    plan_ = buildPlan(systems, mergeLevels);
+    // VLM_BOX=0 keeps box meshes on the general (SELL) level-0 layout
+    const char* bv = std::getenv("VLM_BOX");
+    plan_ = buildPlan(systems, mergeLevels, !(bv && bv[0] == '0'));
     const char* gv = std::getenv("VLM_GRAPH");
     useGraphs_ = !(gv && gv[0] == '0');
 
@@ -225,6 +230,13 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         D.blocks = add(P.blocks);
         D.chunks.upload(all, stream_);
         if (P.blockGS) D.rowColour.upload(P.rowColour, stream_);
+        if (P.box) {
+            D.box = true;
+            D.boxFace.upload(P.boxFace, stream_);
+            D.bcoef.resize(P.boxFace.size());
+            boxes_.upload(P.boxes, stream_);
+            std::vector<int32_t>().swap(P.boxFace);
+        }
         if (k + 1 < nL) {
             D.agg.upload(P.agg, stream_);
             D.childPtr.upload(P.childPtr, stream_);
@@ -390,6 +402,7 @@ void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
             D.x232.resize(size_t(D.nrows));
             D.t32.zero(stream_);
             D.x232.zero(stream_);
+            if (D.box) D.bcoef32.resize(D.bcoef.size());
         }
         if (tailOn_) buildTailTable<float>(tail32_);
     }
@@ -409,6 +422,13 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
     if (mixed) VLM_LAUNCH(k_gather_diag0<float>, nblk(D0.nrows), 256, s, D0.nrows, perm0_.get(), diag, D0.diag32.get());
     VLM_LAUNCH(k_materialize, nblk(D0.nent), 256, s, D0.nent, D0.src.get(), upper, lower, D0.val.get(),
                mixed ? D0.val32.get() : nullptr);
+    // the box kernels take each face coefficient once: symmetric matrices only
+    boxOn_ = D0.box && lower == upper;
+    if (boxOn_) {
+        const int n3 = int(D0.bcoef.size());
+        VLM_LAUNCH(k_box_coef, nblk(n3), 256, s, n3, D0.boxFace.get(), upper, D0.bcoef.get(),
+                   mixed ? D0.bcoef32.get() : nullptr);
+    }
     if (!gamg) return;
     const int nL = int(L_.size());
     for (int k = 0; k + 1 < nL; ++k) {
@@ -499,9 +519,24 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
         const bool two = D.nSteps == 2;
         const ChunkList& rows = head ? D.headActive : D.active;
         if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, rows.n, kRowsPerCta, s, D.ch(rows), x, st, flag);
+        const bool boxK = k == 0 && boxOn_;
+        const T* bc = LV<T>::bcoef(D);
+        const BoxSys* bx = boxes_.get();
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
                 const ChunkList& l = head ? (pre ? D.headFwd[t] : D.headRev[t]) : (pre ? D.fwd[t] : D.rev[t]);
+                if (boxK) {
+                    if (two && sweep == 0 && t == 0 && pre)
+                        VLM_LAUNCH((k_box_gs<T, 1>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
+                                   xc, st, flag);
+                    else if (two && sweep == 0 && t == 0)
+                        VLM_LAUNCH((k_box_gs<T, 2>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
+                                   xc, st, flag);
+                    else
+                        VLM_LAUNCH((k_box_gs<T, 0>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
+                                   xc, st, flag);
+                    continue;
+                }
                 if (two && sweep == 0 && t == 0 && pre)
                     VLM_LAUNCH((k_smooth_gs<T, 1>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
                                flag);
@@ -535,8 +570,12 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
         const ChunkList& rows = tail ? D.headActive : D.active;
         const ChunkList& next = tail ? N.headIn : N.all;
         recordSmooth<T>(k, rr(k), xx(k), sm, true, flag, tail);
-        VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
-                   rr(k), xx(k), LV<T>::t(D), st, flag);
+        if (k == 0 && boxOn_)
+            VLM_LAUNCH(k_box_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), (const BoxSys*)boxes_.get(),
+                       LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k), (const T*)xx(k), LV<T>::t(D), st, flag);
+        else
+            VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
+                       rr(k), xx(k), LV<T>::t(D), st, flag);
         VLM_LAUNCH(k_restrict<T>, next.n, kRowsPerCta, s, N.ch(next), D.childPtr.get(), D.child.get(), LV<T>::t(D),
                    LV<T>::r(N), st, flag);
     }
@@ -732,8 +771,13 @@ void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
                    st_.get());
         VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
     }
-    VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(),
-               p_.get(), Ap_.get(), red(), st_.get());
+    if (boxOn_)
+        VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, (const BoxSys*)boxes_.get(),
+                   (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)p_.get(),
+                   Ap_.get(), red(), st_.get());
+    else
+        VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(),
+                   D0.diag.get(), p_.get(), Ap_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_update<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, x_.get(), r_.get(), p_.get(),
                Ap_.get(), perm0_.get(), red(), st_.get(), dctrl_.get(), v32 ? r32_.get() : (float*)nullptr);
 }
@@ -752,8 +796,13 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
         throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs the GAMG or diagonal preconditioner");
     VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
-    VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), D0.diag32.get(),
-               p32_.get(), Ap32_.get(), red(), st_.get());
+    if (boxOn_)
+        VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, (const BoxSys*)boxes_.get(),
+                   (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)p32_.get(),
+                   Ap32_.get(), red(), st_.get());
+    else
+        VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(),
+                   D0.diag32.get(), p32_.get(), Ap32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_update<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
                Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get(), (float*)nullptr);
 }
@@ -1222,7 +1271,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
         Ay_.zero(s);
         p_.zero(s);
     }
-    const SolveKey key{sk, pk, sm, prec, exact_, relax ? ctrl.nSweeps : 0};
+    const SolveKey key{sk, pk, sm, prec, exact_, relax ? ctrl.nSweeps : 0, boxOn_};
     int64_t eagerLaunches = 0;
     GraphExec* Gp = nullptr;
     if (useGraphs_) {
@@ -1385,6 +1434,34 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
     if (name == "amul64") {
         run = [&] { VLM_LAUNCH(k_amul, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), x_.get(), w_.get()); };
         *bytesPerLaunch = sz * 3 * N + sz * F + 8 * F;
+    } else if ((name == "smooth64" || name == "smooth32") && boxOn_) {
+        // box level 0: each face coefficient once, no column indices
+        run = [&] {
+            for (int t = 0; t < D0.nSteps; ++t) {
+                if (f32)
+                    VLM_LAUNCH((k_box_gs<float, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), (const BoxSys*)boxes_.get(), (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr, (const SysState*)st_.get(), kFlagDone);
+                else
+                    VLM_LAUNCH((k_box_gs<double, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), (const int32_t*)nullptr, (const double*)nullptr, (const SysState*)st_.get(), kFlagDone);
+            }
+        };
+        *bytesPerLaunch = sz * 4 * N + sz * F;
+    } else if ((name == "residual64" || name == "residual32") && boxOn_) {
+        run = [&] {
+            if (f32)
+                VLM_LAUNCH(k_box_residual<float>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), (const BoxSys*)boxes_.get(), (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), (const float*)w32_.get(), D0.t32.get(), (const SysState*)st_.get(), kFlagDone);
+            else
+                VLM_LAUNCH(k_box_residual<double>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), (const double*)w_.get(), D0.t.get(), (const SysState*)st_.get(), kFlagDone);
+        };
+        *bytesPerLaunch = sz * 4 * N + sz * F;
+    } else if (name == "spmv64") {
+        // the PCG product with its fused dot (the FP64 Krylov recurrence's largest kernel)
+        run = [&] {
+            if (boxOn_)
+                VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
+            else
+                VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), red(), st_.get());
+        };
+        *bytesPerLaunch = boxOn_ ? 8.0 * 3 * N + 8.0 * F : 8.0 * 3 * N + 8.0 * F + 8.0 * F;
     } else if (name == "smooth64" || name == "smooth32") {
         run = [&] {
             for (int t = 0; t < D0.nSteps; ++t) {

@@ -30,6 +30,12 @@ struct DevLevel {
     std::vector<ChunkList> fwd, rev;
     DBuf<int32_t> agg, childPtr, child, intraPtr, intraFace, cfacePtr, cfaceSrc;
     ChunkList coarse;  // CoarseDev entries whose coarsest level is this one
+    // level 0 of box meshes (box.h): the face of each row's +x/+y/+z neighbour, and the
+    // per-direction coefficients materialised from it per solve
+    bool box = false;
+    DBuf<int32_t> boxFace;
+    DBuf<double> bcoef;
+    DBuf<float> bcoef32;
     // numeric, per solve
     DBuf<double> diag, val, up, lo;
     DBuf<float> diag32, val32;
@@ -55,9 +61,10 @@ struct SolveKey {
     Precision prec;
     bool exact;
     int nSweeps;  // relaxation solvers: sweeps per residual evaluation (0 for Krylov solvers)
+    bool box;     // level 0 runs the box kernels (box mesh, symmetric matrix)
     bool operator<(const SolveKey& o) const {
-        return std::tie(solver, precond, smoother, prec, exact, nSweeps) <
-               std::tie(o.solver, o.precond, o.smoother, o.prec, o.exact, o.nSweeps);
+        return std::tie(solver, precond, smoother, prec, exact, nSweeps, box) <
+               std::tie(o.solver, o.precond, o.smoother, o.prec, o.exact, o.nSweeps, o.box);
     }
 };
 
@@ -170,6 +177,8 @@ private:
     DBuf<CoarseDev> coarse_;
     DBuf<double> lu_, inv_;
     DBuf<int32_t> perm0_, sysCells_, slotBegin_, slotEnd_, counters_, status_;
+    DBuf<BoxSys> boxes_;     // per batch position, when level 0 has the box layout
+    bool boxOn_ = false;     // the current solve's matrix uses the box kernels on level 0
     DBuf<DD> partials_;
     DBuf<long long> xbins_;  // exact-sum partials (reproducible mode)
     bool exact_ = false;
