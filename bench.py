@@ -535,6 +535,135 @@ def run_channel(args, rank, world, local):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------------ TGV PIMPLE workload (config 2)
+TGV_METRIC = "Taylor-Green 3D PIMPLE: s/step (backward, dt 2e-3, nCorr 2, p PCG+GAMG 1e-8), FP64 vs mixed pressure"
+TGV_DT = 2e-3
+
+
+def tgv_config(args, world):
+    return {"workload": f"3D Taylor-Green vortex, periodic box [0,2pi]^3, {args.n}^3 hex ({args.n ** 3} cells), nu = 1/1600, "
+                        f"u0 = (sin x cos y cos z, -cos x sin y cos z, 0); transient PIMPLE backward, linear, dt = "
+                        f"{TGV_DT}, nOuter 1, nCorr 2; U PBiCGStab/DILU 1e-8, p PCG/GAMG 1e-8 relTol 0.01, "
+                        f"pFinal relTol 0", "cells": args.n ** 3, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (the step touches ~GBs)",
+            "steps_note": "the configuration's 200 steps are not run: s/step is timed over the steps given"}
+
+
+def _tgv_ref_step_time(n, steps):
+    """Seconds per step of the reference's own PIMPLE step (IncompressibleFlow, single-threaded) on the
+    n^3 TGV, over `steps` steps after one untimed step."""
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    from voluma_b200 import cases
+    m, case, U0 = cases.taylor_green_flow(n)
+    R = ref.RefMesh((n, n, n), hi=(2 * np.pi,) * 3, periodic=(1, 1, 1))
+    t0 = time.perf_counter()
+    R.flow_run(case, 1, dt=TGV_DT, U=U0)
+    t1 = time.perf_counter()
+    _, _, _, hist = R.flow_run(case, 1 + steps, dt=TGV_DT, U=U0)
+    t2 = time.perf_counter()
+    return ((t2 - t1) - (t1 - t0)) / steps, float(np.mean(hist[1:, 3]))
+
+
+def run_tgv_reference(args, rank, world):
+    """The reference's own PIMPLE step on the same TGV, one process (its MPI path is not built here);
+    s/step over 2 steps after an untimed one.  Higher is better is false: the metric is time."""
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvlmref.so was not built (make -C oracle)"}))
+        return
+    per, its = _tgv_ref_step_time(args.n, 2)
+    line = {"metric": TGV_METRIC, "impl": "reference", "value": per, "unit": "s/step", "n_gpus": args.gpus,
+            "steps": 2, "warmup": 1, "ms_per_step": 1e3 * per, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": tgv_config(args, 1),
+            "linear_iterations_per_step": its,
+            "cpu_baseline": {"value": per, "unit": "s/step", "cores": 1, "kind": "reference",
+                             "sample": f"2 PIMPLE steps of the {args.n}^3 TGV after one untimed step, 1 thread "
+                                       f"(reference IncompressibleFlow::step)"},
+            "e2e": {"value": per, "unit": "s/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_tgv(args, rank, world, local):
+    import torch
+    import voluma_b200 as vb
+    from voluma_b200 import cases
+    torch.cuda.set_device(local)
+    m, case0, U0 = cases.taylor_green_flow(args.n)
+    mesh = vb.Mesh.from_arrays(m, ctx=vb.Context(local))
+    st = torch.cuda.ExternalStream(mesh.ctx.stream())
+    modes = {}
+    sampler = ClockSampler(local)
+    clocks = None
+    fields = {}
+    for prec in ("mixed", "fp64"):
+        case = dict(case0, p=dict(case0["p"], precision=prec), pFinal=dict(case0["pFinal"], precision=prec))
+        fl = vb.Flow(mesh, case)
+        fl.set_state(U0, None)
+        for _ in range(args.warmup):
+            fl.step(TGV_DT)
+        l0 = fl.launches()
+        if prec == "mixed":
+            sampler.start()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its = 0
+        for _ in range(args.steps):
+            its += fl.step(TGV_DT)["iterations"]
+        e1.record(st)
+        torch.cuda.synchronize(local)
+        dev_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, torch.device("cuda", local))
+        launches = fl.launches() - l0
+        # end to end: every step also reads U and p back to the host
+        t = time.perf_counter()
+        ne = max(2, args.steps // 2)
+        for _ in range(ne):
+            fl.step(TGV_DT)
+            U, p, _ = fl.state()
+        e2e_s = max_over_ranks((time.perf_counter() - t) / ne, world, torch.device("cuda", local))
+        if prec == "mixed":
+            clocks = sampler.stop()
+        fields[prec] = (U, p)
+        fl.close()
+        modes[prec] = dict(value=dev_s / args.steps, ms_per_step=1e3 * dev_s / args.steps,
+                           linear_iterations_per_step=its / args.steps, e2e_s_per_step=e2e_s,
+                           gpu_launches=int(launches))
+    if rank != 0:
+        return
+    mx = modes["mixed"]
+    u64, p64 = fields["fp64"]
+    umx, pmx = fields["mixed"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            per, _ = _tgv_ref_step_time(min(args.n, 64), 2)
+            scale = (args.n / min(args.n, 64)) ** 3
+            cpu = {"value": per * scale, "unit": "s/step", "cores": 1, "kind": "reference",
+                   "sample": f"2 PIMPLE steps of the {min(args.n, 64)}^3 TGV after one untimed step, 1 thread, "
+                             f"scaled by cells to {args.n}^3"}
+    line = {"metric": TGV_METRIC, "value": mx["value"], "unit": "s/step", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (pressure V-cycle f32 in mixed)", "data": "synthetic",
+            "config": tgv_config(args, world),
+            "modes": {"mixed": mx, "fp64": modes["fp64"],
+                      "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"],
+                      "extrapolated_200_steps_s": {"mixed": 200 * mx["value"], "fp64": 200 * modes["fp64"]["value"]},
+                      "mixed_vs_fp64_after_steps": {
+                          "U_rel_l2": float(np.linalg.norm(umx - u64) / np.linalg.norm(u64)),
+                          "p_rel_l2": float(np.linalg.norm(pmx - p64) / np.linalg.norm(p64))}},
+            "e2e": {"value": mx["e2e_s_per_step"], "unit": "s/step", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * 4 * args.n ** 3,
+                    "note": "vlm_flow_step plus vlm_flow_get_state of U and p every step; the state stays resident"},
+            "roofline": None, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": mx["gpu_launches"]}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------------------ batch workload (config 3)
 BATCH_METRIC = ("batch of Poisson systems: systems solved/s (laplacian with LS non-orthogonal correction, "
                 "nNonOrthCorr 2, PCG+GAMG relTol 1e-8, FP32 V-cycles in FP64 PCG)")
@@ -682,6 +811,47 @@ def run_batch(args, rank, world, local):
                            ms_per_step=1e3 * dev_s / args.steps,
                            all_converged=bool(ok), iterations_max=int(max(max(r) for r in its)),
                            iterations_median=int(np.median([x for r in its for x in r])))
+    # plain FP64: every system registered on its own and solved one after another with the same
+    # corrector (the unbatched FP64 GPU path), registration untimed
+    if args.plain:
+        singles = [vb.Mesh.from_arrays(mm, ctx=ctx) for mm in meshes]
+        offs = np.cumsum([0] + [mm["n_cells"] for mm in meshes])
+        with torch.cuda.stream(st):
+            g1 = [torch.ones(mm["n_faces"], dtype=torch.float64, device=dev) for mm in meshes]
+            p1 = [torch.zeros(mm["n_cells"], dtype=torch.float64, device=dev) for mm in meshes]
+        ctrl64 = vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000)
+
+        def plain_pass():
+            its = []
+            for i, sm in enumerate(singles):
+                with torch.cuda.stream(st):
+                    p1[i].zero_()
+                perf = vb.pressure_solve_device(sm, g1[i].data_ptr(), div.data_ptr() + 8 * int(offs[i]),
+                                                p1[i].data_ptr(), ctrl64, ref_cell=0, n_non_orth=BATCH_NON_ORTH,
+                                                grad_scheme=1)
+                its.append(perf[-1][0].iterations)
+            return its
+        plain_pass()  # warm-up: every system's graphs
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its1 = plain_pass()
+        e1.record(st)
+        torch.cuda.synchronize(local)
+        plain_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
+        # the same systems' results as the batched FP64 solve
+        with torch.cuda.stream(st):
+            p.zero_()
+        vb.pressure_solve_device(B, gamma.data_ptr(), div.data_ptr(), p.data_ptr(),
+                                 vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000), ref_cell=refs,
+                                 n_non_orth=BATCH_NON_ORTH, grad_scheme=1)
+        torch.cuda.synchronize(local)
+        pb = p.cpu().numpy()
+        same = all(np.array_equal(p1[i].cpu().numpy(), pb[offs[i]:offs[i + 1]]) for i in range(len(singles)))
+        modes["fp64_plain"] = dict(value=aggregate_rate(args.systems, world, plain_s), ms_per_step=1e3 * plain_s,
+                                   iterations_median=int(np.median(its1)), iterations_max=int(max(its1)),
+                                   bitwise_equal_to_batched_fp64=bool(same))
+        del singles, g1, p1
     # end to end through the host-pointer corrector (H2D gamma, div, p; D2H p and the face flux)
     ctrl = vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000, precision="mixed")
     ph = np.zeros(B.n_cells)
@@ -705,8 +875,11 @@ def run_batch(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": mx["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic",
             "config": batch_config(args, world, nC),
-            "modes": {"mixed": mx, "fp64": modes["fp64"],
-                      "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"]},
+            "modes": dict({"mixed": mx, "fp64": modes["fp64"],
+                           "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"]},
+                          **({"fp64_plain": modes["fp64_plain"],
+                              "speedup_batched_mixed_vs_plain_fp64": modes["fp64_plain"]["ms_per_step"] /
+                              mx["ms_per_step"]} if "fp64_plain" in modes else {})),
             "setup_s": {"generate": t_gen, "register": t_reg},
             "e2e": {"value": e2e, "unit": "systems/s", "h2d_bytes_per_step": int(8 * (nF + 2 * nC)),
                     "d2h_bytes_per_step": int(8 * (nC + nF)),
@@ -869,9 +1042,11 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--smoother", default="")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving", "channel", "batch"])
+    ap.add_argument("--workload", default="pressure", choices=["pressure", "serving", "channel", "batch", "tgv"])
     ap.add_argument("--systems", type=int, default=256)
     ap.add_argument("--ref-systems", type=int, default=16)
+    ap.add_argument("--no-plain", dest="plain", action="store_false",
+                    help="batch workload: skip the unbatched FP64 arm (each system solved on its own)")
     ap.add_argument("--channel", default="256x192x128")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=4.0)
@@ -887,7 +1062,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         {"serving": run_serving_reference, "channel": run_channel_reference,
-         "batch": run_batch_reference}.get(args.workload, run_reference)(
+         "batch": run_batch_reference, "tgv": run_tgv_reference}.get(args.workload, run_reference)(
             args, rank, world)
         return
     if world > 1:
@@ -897,7 +1072,7 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        {"serving": run_serving, "channel": run_channel, "batch": run_batch}.get(args.workload, run_ours)(
+        {"serving": run_serving, "channel": run_channel, "batch": run_batch, "tgv": run_tgv}.get(args.workload, run_ours)(
             args, rank, world, local)
     finally:
         if world > 1:

@@ -266,6 +266,16 @@ vlm_status vlm_topology_level(const vlm_topology* t, int32_t level, int32_t* siz
 vlm_status vlm_topology_box(const vlm_topology* t, int32_t* shape);
 vlm_status vlm_topology_destroy(vlm_topology* t);
 
+/* ------------------------------------------------------------------ failure detection */
+/* Self-test of the bounded group barrier that the level-scheduled DIC/DILU and Gauss-Seidel kernels
+ * use when one system spans several CTAs (no reference counterpart: the reference is serial).  Runs
+ * `ctas` co-resident CTAs (1..64) through `rounds` barriers with each wait limited to `spin_limit`
+ * polls; CTA `absent_cta` (when in range; -1 for none) returns before its first arrival, so the other
+ * CTAs' wait runs out.  *barrier_status: 0, or VLM_ERR_TIMEOUT when a wait gave up (the kernel still
+ * ends, and the context stays usable); passed[b]: barriers CTA b passed before that. */
+vlm_status vlm_barrier_check(vlm_ctx* ctx, int32_t ctas, int64_t spin_limit, int32_t absent_cta, int32_t rounds,
+                             int32_t* passed, int32_t* barrier_status);
+
 /* ------------------------------------------------------------------ reductions */
 /* Order-independent exact sum of n doubles on the device (host pointer in, host result). */
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out);

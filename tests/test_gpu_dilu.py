@@ -158,3 +158,16 @@ def test_wide_system_uses_a_cooperative_group():
                       n_sweeps=2)
     assert p.iterations == po["iterations"] == 4
     assert np.array_equal(x, xo)
+
+
+def test_group_barrier_gives_up_when_a_cta_never_arrives():
+    """Failure path of the bounded group barrier (dilu.cuh group_sync): with every CTA present the
+    barriers all pass; with one CTA returning before its first arrival, the others' wait runs out
+    after the spin limit, the kernel ends with status TIMEOUT, and the context stays usable."""
+    st, passed = vb.barrier_check(6, 1 << 22, absent_cta=-1, rounds=5)
+    assert st == "OK" and np.all(passed == 5)
+    st, passed = vb.barrier_check(6, 2000, absent_cta=3, rounds=5)
+    assert st == "TIMEOUT"
+    assert np.all(passed == 0)  # nobody got through the first barrier
+    st, passed = vb.barrier_check(4, 1 << 22, absent_cta=-1, rounds=3)
+    assert st == "OK" and np.all(passed == 3)

@@ -117,3 +117,53 @@ def test_flow_rejects_bad_settings():
     with pytest.raises(vb.VlmError) as e:
         vb.Flow(mesh2, case)  # linearUpwind needs the cell and face centres
     assert e.value.name == "BAD_ARG"
+
+
+@pytest.fixture(scope="module")
+def cav64():
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "flow_cavity64.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def fnv1a(a):
+    """The reference's field checksum (fieldChecksum, VtkWriter.cpp:81-99): 64-bit FNV-1a over the
+    bytes of the doubles in cell order."""
+    h = 0xcbf29ce484222325
+    for byte in np.ascontiguousarray(a, np.float64).tobytes():
+        h ^= byte
+        h = (h * 0x100000001b3) & 0xffffffffffffffff
+    return h
+
+
+def test_cavity64_steady_like_reference(cav64):
+    """The lid-driven cavity of cases/cavity/case.json (64x64, Re 100, steady SIMPLE to residualTol
+    1e-6): the reference converges in 1161 iterations.  Default mode (device GAMG with its
+    multicolour smoother): the iteration count within +-2 % of the reference's and the converged
+    fields within 2e-5 (U) and 2e-4 (p, relative to its mean) of the reference's."""
+    m, case = cases.lid_cavity(64, 100.0)
+    mesh, fl = flow_for(m, case)
+    fl.set_state(None, None)
+    its, last = fl.run_steady(20000, 1e-6)
+    U, p, phi = fl.state()
+    fl.close()
+    ref_its = int(cav64["cav64_iters"])
+    assert ref_its == 1161
+    assert abs(its - ref_its) <= int(0.02 * ref_its)
+    assert last["UInitialResidual"] < 1e-6 and last["pInitialResidual"] < 1e-6
+    assert rel(U, cav64["cav64_U"]) < 2e-5
+    assert rel(p - p.mean(), cav64["cav64_p"] - cav64["cav64_p"].mean()) < 2e-4
+
+
+def test_cavity64_reproducible_to_convergence_bitwise(cav64):
+    """The same case in CFD_REPRODUCIBLE mode, run to convergence: the same iteration count and the
+    converged fields bit for bit (so the reference's field checksums too)."""
+    m, case = cases.lid_cavity(64, 100.0)
+    case["reproducible"] = True
+    mesh, fl = flow_for(m, case)
+    fl.set_state(None, None)
+    its, last = fl.run_steady(20000, 1e-6)
+    U, p, phi = fl.state()
+    fl.close()
+    assert its == int(cav64["cav64_repro_iters"])
+    assert np.array_equal(U, cav64["cav64_repro_U"]) and np.array_equal(p, cav64["cav64_repro_p"])
+    assert fnv1a(U) == fnv1a(cav64["cav64_repro_U"]) and fnv1a(p) == fnv1a(cav64["cav64_repro_p"])

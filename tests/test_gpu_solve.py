@@ -37,6 +37,18 @@ def ctrl(**kw):
     return vb.SolverControls(**base)
 
 
+def oracle_iterate(m, d, up, b, x0, xo, po, iterations, smoother="mcgs-jacobi"):
+    """The oracle's solution after exactly `iterations` PCG+GAMG iterations: its converged solution
+    when the counts agree, else the same schedule run to that count (tolerances 0).  Near relTol
+    1e-8 one iteration moves the solution by up to 2e-7 relative on these systems, so a +-1 count
+    is compared at equal work."""
+    if iterations == po["iterations"]:
+        return xo
+    xk, pk = ro.solve(m, d, up, None, b, x0, "PCG", "GAMG", 0.0, 0.0, iterations, smoother=smoother, coarse=1)
+    assert pk["iterations"] == iterations
+    return xk
+
+
 def true_residual(m, d, up, lo, b, x):
     return np.abs(b - ro.amul(m, d, up, lo, x)).sum()
 
@@ -131,7 +143,7 @@ def test_pcg_gamg_matches_oracle(name, smoother):
                       smoother=smoother, coarse=1)
     assert abs(p.iterations - po["iterations"]) <= 1
     assert p.converged and po["converged"]
-    assert rel(x, xo) <= 1e-10 if p.iterations == po["iterations"] else True
+    assert rel(x, oracle_iterate(g, g["diag"], g["upper"], g["b"], g["x0"], xo, po, p.iterations, smoother)) <= 1e-10
     # against the reference's sequential-GS GAMG: same tolerance reached, counts reported
     ref = perf_dict(g["pcg_gamg_perf"])
     assert true_residual(g, g["diag"], g["upper"], None, g["b"], x) <= 1e-8 * ref["residualSum"] * 1.0001
@@ -263,4 +275,30 @@ def test_64cubed_gamg_against_oracle():
     xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000,
                       smoother="mcgs-jacobi", coarse=1)
     assert abs(p.iterations - po["iterations"]) <= 1
-    assert rel(x, xo) <= 1e-9
+    assert rel(x, oracle_iterate(M, d, up, b, np.zeros(M["n_cells"]), xo, po, p.iterations)) <= 1e-10
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_box_level0_matches_general_layout(name, precision, monkeypatch):
+    """Every golden mesh is a box; level 0 runs the structured box kernels unless a periodic extent
+    is odd (stretched6x9x5: three colours, the general layout).  The same solve on the general SELL
+    layout (VLM_BOX=0 at registration) gives the same iterates - bit for bit where the two layouts
+    place the rows alike (even x extent), else to rounding (odd x extent: the box layout has padding
+    slots, so the reductions' partial sums are grouped differently)."""
+    g, m = device_mesh(name)
+    shape = vb.box_shape(g["n_cells"], g["owner"][:g["n_internal_faces"]], g["neighbour"][:g["n_internal_faces"]])
+    assert shape is not None
+    assert shape["layout"] == all(not p or n % 2 == 0 for n, p in zip(shape["n"], shape["periodic"]))
+    monkeypatch.setenv("VLM_BOX", "0")
+    m2 = vb.Mesh.from_arrays(g)
+    monkeypatch.delenv("VLM_BOX")
+    c = ctrl(preconditioner="GAMG", precision=precision)
+    x1, x2 = g["x0"].copy(), g["x0"].copy()
+    p1 = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x1, c)
+    p2 = vb.solve_ldu(m2, g["diag"], g["upper"], None, g["b"], x2, c)
+    assert p1.iterations == p2.iterations
+    if shape["n"][0] % 2 == 0 or not shape["layout"]:
+        assert np.array_equal(x1, x2) and p1.finalResidual == p2.finalResidual
+    else:
+        assert rel(x1, x2) <= 1e-12

@@ -374,6 +374,18 @@ def topology(n_cells, owner, neighbour, magSf, ndc, merge_levels: int = 2):
         L.vlm_topology_destroy(h)
 
 
+def barrier_check(ctas: int, spin_limit: int, absent_cta: int = -1, rounds: int = 4, ctx: "Context | None" = None):
+    """Runs the level-scheduled kernels' bounded group barrier on its own (vlm_barrier_check):
+    returns (status name, barriers passed per CTA); status "TIMEOUT" when a wait gave up."""
+    ctx = ctx or default_context()
+    L = load()
+    passed = np.zeros(int(ctas), np.int32)
+    st = C.c_int32()
+    check(L.vlm_barrier_check(ctx.handle, int(ctas), int(spin_limit), int(absent_cta), int(rounds), _ptr(passed),
+                              C.byref(st)), ctx.handle)
+    return _ffi.STATUS.get(st.value, str(st.value)), passed
+
+
 def box_shape(n_cells, owner, neighbour, magSf=None, ndc=None):
     """Whether the face arrays are those of a generateBox mesh (no GPU needed): a dict with the
     shape n = (nx, ny, nz), the periodic flags and `layout` (level 0 of its solves runs the

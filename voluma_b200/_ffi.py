@@ -15,7 +15,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_mesh_release", "vlm_amul", "vlm_ldu_solve", "vlm_ldu_solve_device", "vlm_gamg_apply",
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
-           "vlm_topology_box",
+           "vlm_topology_box", "vlm_barrier_check",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
            "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
@@ -147,6 +147,7 @@ def load():
     L.vlm_topology_level.argtypes = [P, i32, P, P, P, P, P, P, P, P]
     L.vlm_topology_destroy.argtypes = [P]
     L.vlm_topology_box.argtypes = [P, P]
+    L.vlm_barrier_check.argtypes = [P, i32, C.c_int64, i32, i32, P, C.POINTER(i32)]
     L.vlm_div.argtypes = [P, P, P, P]
     L.vlm_pressure_solve.argtypes = [P, P, P, P, P, P, P, i32, C.c_double, i32, i32, C.POINTER(SolverCtrl),
                                      C.POINTER(SolverCtrl), P, P]

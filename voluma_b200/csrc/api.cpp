@@ -724,6 +724,15 @@ vlm_status vlm_box_destroy(vlm_box* box) {
     return VLM_OK;
 }
 
+vlm_status vlm_barrier_check(vlm_ctx* ctx, int32_t ctas, int64_t spin_limit, int32_t absent_cta, int32_t rounds,
+                             int32_t* passed, int32_t* barrier_status) {
+    if (!ctx || !passed || !barrier_status) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(ctx, [&] {
+        setDevice(ctx);
+        *barrier_status = vlm::groupBarrierCheck(ctx->stream, ctas, spin_limit, absent_cta, rounds, passed);
+    });
+}
+
 vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* out) {
     if (!ctx || (!values && n > 0) || !out || n < 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
     return guarded(ctx, [&] {

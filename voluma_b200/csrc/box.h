@@ -21,6 +21,8 @@
 
 namespace vlm {
 
+struct Chunk;
+
 // Shape of a box mesh as its face arrays define it.
 struct BoxShape {
     int n[3] = {0, 0, 0};
@@ -54,6 +56,19 @@ struct BoxSys {
     int base0, base1;   // first solver row of colour group 0 and 1
     int slots;          // H * ny * nz
     FastDiv divH, divNy;
+};
+
+// Rows of one launch: a chunk list (any batch; CTA b takes chunk b, whose system gives the
+// descriptor, and skips systems that are done), or - a batch of one system - a row range taken by
+// arithmetic with the descriptor passed by value, so the first loads of a thread are its data.  The
+// range form skips the state check: the loop stops once its one system is done, and a V-cycle that
+// still runs in that last pass (after a breakdown found earlier in the pass) only rewrites the
+// preconditioner's scratch vectors, which nothing reads afterwards.
+struct BoxRows {
+    const Chunk* ch;  // null: the range form
+    const BoxSys* boxes;
+    BoxSys one;
+    int begin, end;
 };
 
 }  // namespace vlm

@@ -59,70 +59,91 @@ __device__ __forceinline__ BoxSys box_load(const BoxSys* __restrict__ boxes, int
     return BoxSys{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, FastDiv{unsigned(c.x), c.y}, FastDiv{unsigned(c.z), c.w}};
 }
 
-// s -= (MINUS) or += a_f X(nbr) over the faces of the row's cell in face order.  cx/cy/cz: the
-// per-direction coefficients in solver-row layout; xf(row) reads the neighbour's value.  All
-// coefficient and neighbour loads are issued before the arithmetic.
-template <bool MINUS, class T, class XF>
-__device__ __forceinline__ T box_accumulate(const BoxSys& B, int row, const T* __restrict__ cx,
-                                            const T* __restrict__ cy, const T* __restrict__ cz, XF xf, T s) {
-    int C, i, j, k, q;
-    if (!box_locate(B, row, C, i, j, k, q)) return s;
-    const int H = B.H, ny = B.ny, nx = B.nx, nz = B.nz;
-    const int o = C ? B.base0 : B.base1;  // the other colour's group: every face neighbour is there
-    const int ih = i >> 1;
-    const int xr = o + q * H;
-    const bool px = B.per & 1, py = B.per & 2, pz = B.per & 4;
-    // minus and plus neighbour of each direction (internal or cyclic), their rows and coefficients
-    const bool hmx = i > 0 || px, hpx = i < nx - 1 || px;
-    const bool hmy = j > 0 || py, hpy = j < ny - 1 || py;
-    const bool hmz = k > 0 || pz, hpz = k < nz - 1 || pz;
-    const int rmx = xr + (i > 0 ? (i - 1) >> 1 : (nx - 1) >> 1);
-    const int rpx = xr + (i < nx - 1 ? (i + 1) >> 1 : 0);
-    const int rmy = o + (j > 0 ? q - 1 : q + ny - 1) * H + ih;
-    const int rpy = o + (j < ny - 1 ? q + 1 : q - (ny - 1)) * H + ih;
-    const int rmz = o + (k > 0 ? q - ny : q + (nz - 1) * ny) * H + ih;
-    const int rpz = o + (k < nz - 1 ? q + ny : q - (nz - 1) * ny) * H + ih;
-    T amx = T(0), apx = T(0), amy = T(0), apy = T(0), amz = T(0), apz = T(0);
-    T vmx = T(0), vpx = T(0), vmy = T(0), vpy = T(0), vmz = T(0), vpz = T(0);
-    const uint64_t pol = l2_keep();
-    if (hmz) { amz = ld_keep(cz + rmz, pol); vmz = xf(rmz); }
-    if (hmy) { amy = ld_keep(cy + rmy, pol); vmy = xf(rmy); }
-    if (hmx) { amx = ld_keep(cx + rmx, pol); vmx = xf(rmx); }
-    if (hpx) { apx = ld_keep(cx + row, pol); vpx = xf(rpx); }
-    if (hpy) { apy = ld_keep(cy + row, pol); vpy = xf(rpy); }
-    if (hpz) { apz = ld_keep(cz + row, pol); vpz = xf(rpz); }
-    auto term = [&](T a, T v) {
-        if (MINUS)
-            s -= a * v;
-        else
-            s += a * v;
-    };
-    if (k > 0) term(amz, vmz);
-    if (j > 0) term(amy, vmy);
-    if (i > 0) term(amx, vmx);
-    if (i < nx - 1) term(apx, vpx);
-    if (j < ny - 1) term(apy, vpy);
-    if (k < nz - 1) term(apz, vpz);
-    if (px) {
-        if (i == 0)
-            term(amx, vmx);
-        else if (i == nx - 1)
-            term(apx, vpx);
+// One row's neighbours (rows and face coefficients, in the six directions) loaded ahead of the
+// gathers, before the kernel waits for its predecessor; accumulate() gathers X and sums the terms
+// s -= (MINUS) or += a_f X(nbr) in the cell's face order.  xf(row) reads a neighbour's value.
+template <class T>
+struct BoxRowPre {
+    bool valid = false;
+    int i, j, k, nx, ny, nz, per;
+    int rmx, rpx, rmy, rpy, rmz, rpz;
+    T amx, apx, amy, apy, amz, apz;
+    __device__ __forceinline__ void load(const BoxSys& B, int row, const T* __restrict__ cx, const T* __restrict__ cy,
+                                         const T* __restrict__ cz) {
+        int C, q;
+        valid = box_locate(B, row, C, i, j, k, q);
+        if (!valid) return;
+        const int H = B.H;
+        nx = B.nx;
+        ny = B.ny;
+        nz = B.nz;
+        per = B.per;
+        const int o = C ? B.base0 : B.base1;  // the other colour's group: every face neighbour is there
+        const int ih = i >> 1;
+        const int xr = o + q * H;
+        const bool px = per & 1, py = per & 2, pz = per & 4;
+        rmx = xr + (i > 0 ? (i - 1) >> 1 : (nx - 1) >> 1);
+        rpx = xr + (i < nx - 1 ? (i + 1) >> 1 : 0);
+        rmy = o + (j > 0 ? q - 1 : q + ny - 1) * H + ih;
+        rpy = o + (j < ny - 1 ? q + 1 : q - (ny - 1)) * H + ih;
+        rmz = o + (k > 0 ? q - ny : q + (nz - 1) * ny) * H + ih;
+        rpz = o + (k < nz - 1 ? q + ny : q - (nz - 1) * ny) * H + ih;
+        const uint64_t pol = l2_keep();
+        amx = apx = amy = apy = amz = apz = T(0);
+        if (k > 0 || pz) amz = ld_keep(cz + rmz, pol);
+        if (j > 0 || py) amy = ld_keep(cy + rmy, pol);
+        if (i > 0 || px) amx = ld_keep(cx + rmx, pol);
+        if (i < nx - 1 || px) apx = ld_keep(cx + row, pol);
+        if (j < ny - 1 || py) apy = ld_keep(cy + row, pol);
+        if (k < nz - 1 || pz) apz = ld_keep(cz + row, pol);
     }
-    if (py) {
-        if (j == 0)
-            term(amy, vmy);
-        else if (j == ny - 1)
-            term(apy, vpy);
+    template <bool MINUS, class XF>
+    __device__ __forceinline__ T accumulate(XF xf, T s) const {
+        if (!valid) return s;
+        const bool px = per & 1, py = per & 2, pz = per & 4;
+        const bool hmx = i > 0 || px, hpx = i < nx - 1 || px;
+        const bool hmy = j > 0 || py, hpy = j < ny - 1 || py;
+        const bool hmz = k > 0 || pz, hpz = k < nz - 1 || pz;
+        T vmx = T(0), vpx = T(0), vmy = T(0), vpy = T(0), vmz = T(0), vpz = T(0);
+        if (hmz) vmz = xf(rmz);
+        if (hmy) vmy = xf(rmy);
+        if (hmx) vmx = xf(rmx);
+        if (hpx) vpx = xf(rpx);
+        if (hpy) vpy = xf(rpy);
+        if (hpz) vpz = xf(rpz);
+        auto term = [&](T a, T v) {
+            if (MINUS)
+                s -= a * v;
+            else
+                s += a * v;
+        };
+        if (k > 0) term(amz, vmz);
+        if (j > 0) term(amy, vmy);
+        if (i > 0) term(amx, vmx);
+        if (i < nx - 1) term(apx, vpx);
+        if (j < ny - 1) term(apy, vpy);
+        if (k < nz - 1) term(apz, vpz);
+        if (px) {
+            if (i == 0)
+                term(amx, vmx);
+            else if (i == nx - 1)
+                term(apx, vpx);
+        }
+        if (py) {
+            if (j == 0)
+                term(amy, vmy);
+            else if (j == ny - 1)
+                term(apy, vpy);
+        }
+        if (pz) {
+            if (k == 0)
+                term(amz, vmz);
+            else if (k == nz - 1)
+                term(apz, vpz);
+        }
+        return s;
     }
-    if (pz) {
-        if (k == 0)
-            term(amz, vmz);
-        else if (k == nz - 1)
-            term(apz, vpz);
-    }
-    return s;
-}
+};
 
 // Coefficients of the box level 0 from the LDU face coefficients (symmetric: upper == lower):
 // coef[d * nrows + row] = upper[boxFace[...]] (0 where the cell has no +d face).
@@ -140,21 +161,46 @@ __global__ void k_box_coef(int n3, const int32_t* __restrict__ face, const doubl
 // Gauss-Seidel colour step (GAMG.cpp:368-380) on the rows of one colour; MODE as k_smooth_gs:
 // 0 plain, 1 first colour from x = 0 (x = r / D), 2 first colour of the first post-sweep with the
 // coarse-grid correction x + xc[agg] applied to the neighbours it reads.
+__device__ __forceinline__ bool box_rows(const BoxRows& R, const SysState* st, int flag, int& row, BoxSys& B,
+                                         bool& idle, int& sys) {
+    if (R.ch == nullptr) {
+        row = R.begin + int(blockIdx.x) * kRowsPerCta + int(threadIdx.x);
+        B = R.one;
+        idle = false;
+        sys = 0;
+        return row < R.end;
+    }
+    const Chunk c = R.ch[blockIdx.x];
+    row = c.start + int(threadIdx.x);
+    sys = c.sys;
+    if ((int)threadIdx.x >= c.count) return false;
+    B = box_load(R.boxes, c.sys);
+    idle = false;
+    return true;
+}
+
+// Gauss-Seidel colour step (GAMG.cpp:368-380) on the rows of one colour; MODE as k_smooth_gs:
+// 0 plain, 1 first colour from x = 0 (x = r / D), 2 first colour of the first post-sweep with the
+// coarse-grid correction x + xc[agg] applied to the neighbours it reads.
 template <class T, int MODE = 0>
-__global__ void __launch_bounds__(kRowsPerCta) k_box_gs(const Chunk* __restrict__ ch, const BoxSys* __restrict__ boxes,
-                                                        const T* __restrict__ coef, int nrows,
+__global__ void __launch_bounds__(kRowsPerCta) k_box_gs(BoxRows R, const T* __restrict__ coef, int nrows,
                                                         const T* __restrict__ diag, const T* __restrict__ r, T* x,
                                                         const int32_t* __restrict__ agg, const T* __restrict__ xc,
                                                         const SysState* st, int flag) {
-    pdl_entry();
-    const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
+    pdl_launch();
+    int row, sys;
+    BoxSys B;
+    bool idle;
+    if (!box_rows(R, st, flag, row, B, idle, sys)) return;
+    const T dg = ld_keep(diag + row, l2_keep());
+    BoxRowPre<T> pre;
+    if (MODE != 1) pre.load(B, row, coef, coef + nrows, coef + 2 * size_t(nrows));
+    pdl_wait();
+    if (R.ch != nullptr && sys_idle(st[sys], flag)) return;
     if (MODE == 1) {
-        x[row] = r[row] / diag[row];
+        x[row] = r[row] / dg;
         return;
     }
-    const BoxSys B = box_load(boxes, c.sys);
     auto xf = [&](int j) -> T {
         T v = __ldg(x + j);
         if (MODE == 2) {
@@ -163,27 +209,26 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_gs(const Chunk* __restrict_
         }
         return v;
     };
-    const T dg = ld_keep(diag + row, l2_keep());
-    const T s = box_accumulate<true>(B, row, coef, coef + nrows, coef + 2 * size_t(nrows), xf, r[row]);
-    x[row] = s / dg;
+    x[row] = pre.template accumulate<true>(xf, r[row]) / dg;
 }
 
 // res = r - A x (GAMG.cpp:387-401: diagonal first, then the faces in order)
 template <class T>
-__global__ void __launch_bounds__(kRowsPerCta) k_box_residual(const Chunk* __restrict__ ch,
-                                                              const BoxSys* __restrict__ boxes,
-                                                              const T* __restrict__ coef, int nrows,
+__global__ void __launch_bounds__(kRowsPerCta) k_box_residual(BoxRows R, const T* __restrict__ coef, int nrows,
                                                               const T* __restrict__ diag, const T* __restrict__ r,
                                                               const T* __restrict__ x, T* __restrict__ res,
                                                               const SysState* st, int flag) {
-    pdl_entry();
-    const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
-    const int row = c.start + threadIdx.x;
-    const BoxSys B = box_load(boxes, c.sys);
-    auto xf = [&](int j) -> T { return __ldg(x + j); };
-    res[row] = box_accumulate<true>(B, row, coef, coef + nrows, coef + 2 * size_t(nrows), xf,
-                                    r[row] - ld_keep(diag + row, l2_keep()) * x[row]);
+    pdl_launch();
+    int row, sys;
+    BoxSys B;
+    bool idle;
+    if (!box_rows(R, st, flag, row, B, idle, sys)) return;
+    const T dg = ld_keep(diag + row, l2_keep());
+    BoxRowPre<T> pre;
+    pre.load(B, row, coef, coef + nrows, coef + 2 * size_t(nrows));
+    pdl_wait();
+    if (R.ch != nullptr && sys_idle(st[sys], flag)) return;
+    res[row] = pre.template accumulate<true>([&](int j) { return __ldg(x + j); }, r[row] - dg * x[row]);
 }
 
 // Ap = A p ; wApA = sum Ap.p ; alpha = wArA / wApA (k_pcg_spmv on the box layout)
@@ -193,16 +238,19 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_pcg_spmv(const Chunk* __res
                                                               const T* __restrict__ coef, int nrows,
                                                               const T* __restrict__ diag, const T* __restrict__ p,
                                                               T* __restrict__ Ap, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    if (sys_idle(st[c.sys], FLAG)) return;
     const BoxSys B = box_load(boxes, c.sys);
+    pdl_wait();
+    if (sys_idle(st[c.sys], FLAG)) return;
     auto xf = [&](int j) -> T { return __ldg(p + j); };
     BlockSum<1, EXACT> acc;
     acc.begin();
     for (int row = c.start + (int)threadIdx.x; row < c.start + c.count; row += kRowsPerCta) {
         const T pr = p[row];
-        const T y = box_accumulate<false>(B, row, coef, coef + nrows, coef + 2 * size_t(nrows), xf, ld_keep(diag + row, l2_keep()) * pr);
+        BoxRowPre<T> pre;
+        pre.load(B, row, coef, coef + nrows, coef + 2 * size_t(nrows));
+        const T y = pre.template accumulate<false>(xf, ld_keep(diag + row, l2_keep()) * pr);
         Ap[row] = y;
         acc.add(0, (double)y * (double)pr);
     }

@@ -21,7 +21,8 @@ struct DiluBar {
     unsigned count, gen;
 };
 
-__device__ __forceinline__ void group_sync(DiluBar* bar, int G, int* err) {
+// spinLimit: polls before a wait gives up (kDiluSpinLimit in the solver kernels).
+__device__ __forceinline__ void group_sync(DiluBar* bar, int G, int* err, long long spinLimit = kDiluSpinLimit) {
     __syncthreads();
     if (G > 1) {
         if (threadIdx.x == 0) {
@@ -37,7 +38,7 @@ __device__ __forceinline__ void group_sync(DiluBar* bar, int G, int* err) {
                 long long it = 0;
                 while (*vg == g) {
                     if (*(volatile int*)err != 0) break;
-                    if (++it > kDiluSpinLimit) {
+                    if (++it > spinLimit) {
                         atomicExch(err, int(VLM_ERR_TIMEOUT));
                         break;
                     }
@@ -47,6 +48,20 @@ __device__ __forceinline__ void group_sync(DiluBar* bar, int G, int* err) {
             __threadfence();
         }
         __syncthreads();
+    }
+}
+
+// Self-test of the group barrier's failure path: G co-resident CTAs (cooperative launch) pass
+// `rounds` barriers; CTA `absent` (when 0 <= absent < G) returns before its first arrival, so the
+// others' first wait runs out after spinLimit polls, sets VLM_ERR_TIMEOUT in *err, and every later
+// wait returns at once: the kernel ends and the status reaches the host.  passed[b]: barriers CTA b
+// got through.
+__global__ void k_group_barrier_check(DiluBar* bar, int G, int* err, long long spinLimit, int absent, int rounds,
+                                      int* passed) {
+    if ((int)blockIdx.x == absent) return;
+    for (int q = 0; q < rounds; ++q) {
+        group_sync(bar, G, err, spinLimit);
+        if (threadIdx.x == 0 && *(volatile int*)err == 0) passed[blockIdx.x] = q + 1;
     }
 }
 

@@ -18,11 +18,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <thread>
 #include <vector>
 
 #include "exactsum.cuh"
 #include "flow.h"
+#include "walldist.h"
 
 namespace vlm {
 namespace {
@@ -268,109 +268,6 @@ __global__ void k_force_correct(int nC, const double* __restrict__ rAU, double d
     U[2 * size_t(nC) + c] += d2 * s;
 }
 
-// ---------------------------------------------------------------- nearest wall face (host)
-// The reference (WallDistance.cpp) takes, for every cell centre, the K = 8 wall faces whose centres are
-// nearest, measures the distance to each face approximated as a disc of the face's area, and keeps
-// the smallest (ties to the lower wall-face index).  A k-d tree over the face centres finds the K
-// nearest centres.
-struct WallDisc {
-    double c[3], n[3], r;
-};
-
-class NearestCentres {
-public:
-    static constexpr int K = 8;
-    explicit NearestCentres(const std::vector<WallDisc>& f) : f_(f), idx_(f.size()) {
-        for (size_t i = 0; i < idx_.size(); ++i) idx_[i] = int(i);
-        if (!f.empty()) build(0, int(f.size()));
-    }
-    // indices of the K (or fewer) nearest centres of x
-    int query(const double* x, int* out) const {
-        Best b;
-        if (!nodes_.empty()) search(0, x, b);
-        for (int k = 0; k < b.n; ++k) out[k] = b.id[k];
-        return b.n;
-    }
-
-private:
-    static constexpr int kLeaf = 8;
-    struct Node {
-        int b, e, axis = -1, left = -1, right = -1;
-        double split = 0;
-    };
-    struct Best {
-        int id[K];
-        double d2[K];
-        int n = 0;
-        double worst() const { return n < K ? 1e300 : d2[n - 1]; }
-        void insert(int i, double d) {
-            if (n == K && d >= d2[K - 1]) return;
-            int k = n < K ? n++ : K - 1;
-            while (k > 0 && d2[k - 1] > d) {
-                d2[k] = d2[k - 1];
-                id[k] = id[k - 1];
-                --k;
-            }
-            d2[k] = d;
-            id[k] = i;
-        }
-    };
-    int build(int b, int e) {
-        const int me = int(nodes_.size());
-        nodes_.push_back({b, e});
-        if (e - b <= kLeaf) return me;
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int i = b; i < e; ++i)
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = std::min(lo[a], f_[idx_[i]].c[a]);
-                hi[a] = std::max(hi[a], f_[idx_[i]].c[a]);
-            }
-        int axis = 0;
-        for (int a = 1; a < 3; ++a)
-            if (hi[a] - lo[a] > hi[axis] - lo[axis]) axis = a;
-        const int mid = (b + e) / 2;
-        std::nth_element(idx_.begin() + b, idx_.begin() + mid, idx_.begin() + e, [&](int x, int y) {
-            const double cx = f_[x].c[axis], cy = f_[y].c[axis];
-            return cx < cy || (cx == cy && x < y);
-        });
-        nodes_[me].axis = axis;
-        nodes_[me].split = f_[idx_[mid]].c[axis];
-        const int l = build(b, mid);
-        const int r = build(mid, e);
-        nodes_[me].left = l;
-        nodes_[me].right = r;
-        return me;
-    }
-    void search(int ni, const double* x, Best& best) const {
-        const Node& nd = nodes_[ni];
-        if (nd.axis < 0) {
-            for (int i = nd.b; i < nd.e; ++i) {
-                const WallDisc& w = f_[idx_[i]];
-                const double d[3] = {x[0] - w.c[0], x[1] - w.c[1], x[2] - w.c[2]};
-                best.insert(idx_[i], d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-            }
-            return;
-        }
-        const double dx = x[nd.axis] - nd.split;
-        const int first = dx < 0 ? nd.left : nd.right, second = dx < 0 ? nd.right : nd.left;
-        search(first, x, best);
-        if (dx * dx < best.worst()) search(second, x, best);
-    }
-    const std::vector<WallDisc>& f_;
-    std::vector<int> idx_;
-    std::vector<Node> nodes_;
-};
-
-// faceDistance (WallDistance.cpp): distance to the disc of centre c, normal n, radius r
-double discDistance(const WallDisc& w, const double* x) {
-    const double d[3] = {x[0] - w.c[0], x[1] - w.c[1], x[2] - w.c[2]};
-    const double dn = d[0] * w.n[0] + d[1] * w.n[1] + d[2] * w.n[2];
-    const double t[3] = {d[0] - dn * w.n[0], d[1] - dn * w.n[1], d[2] - dn * w.n[2]};
-    const double lat = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-    const double out = std::max(lat - w.r, 0.0);
-    return std::sqrt(dn * dn + out * out);
-}
-
 template <class T>
 std::vector<T> download(const T* d, size_t n) {
     std::vector<T> h(n);
@@ -479,34 +376,10 @@ void DeviceFlow::setModel(const vlm_flow_model& m) {
         uTau_.resize(size_t(nWall_));
     }
     if (vanDriest_ && nWall_ > 0) {
-        // nearest wall face and distance of every cell (WallDistance.cpp compute)
-        const NearestCentres tree(discs);
-        std::vector<double> yc(N);
-        std::vector<int32_t> nc(N);
-        auto work = [&](size_t c0, size_t c1) {
-            int ids[NearestCentres::K];
-            for (size_t c = c0; c < c1; ++c) {
-                const double x[3] = {C[c], C[N + c], C[2 * N + c]};
-                const int k = tree.query(x, ids);
-                double best = 1e300;
-                int bi = 0;
-                for (int j = 0; j < k; ++j) {
-                    const double d = discDistance(discs[size_t(ids[j])], x);
-                    if (d < best || (d == best && ids[j] < bi)) {
-                        best = d;
-                        bi = ids[j];
-                    }
-                }
-                yc[c] = best;
-                nc[c] = bi;
-            }
-        };
-        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nt; ++t) pool.emplace_back(work, N * t / nt, N * (t + 1) / nt);
-        for (auto& t : pool) t.join();
-        yWall_.upload(yc, s_);
-        nearest_.upload(nc, s_);
+        // nearest wall face and distance of every cell (WallDistance.cpp compute), on the device
+        yWall_.resize(N);
+        nearest_.resize(N);
+        wallNearestOnDevice(s_, nC_, G_.C(), discs, yWall_.get(), nearest_.get());
     } else {
         vanDriest_ = false;  // no walls: the damping is off (wd->hasWalls false)
     }

@@ -29,6 +29,14 @@ __device__ __forceinline__ void pdl_entry() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Split form for the row kernels of the solve loop: the kernel lets its successor launch at once,
+// loads what no earlier kernel of the loop writes (chunk descriptors, matrix structure, values and
+// diagonals, transfer maps: fixed for a whole solve) while its predecessor drains, and only then
+// waits for the predecessor's results.  On the small coarse levels this takes the dependent loads
+// of the row structure off the critical path.
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 
 constexpr double kVSMALL = 1.0e-300;  // core/Types.h VSMALL
 constexpr double kGREAT = 1.0e15;     // core/Types.h GREAT
@@ -232,8 +240,9 @@ template <int NV> struct BlockSum<NV, true> {
 // Exact sum of a plain array (vlm_exact_sum): one system, chunks of kRowsPerCta values.
 __global__ void __launch_bounds__(kRowsPerCta) k_exact_sum(const Chunk* __restrict__ ch, const double* __restrict__ v,
                                                            RedCtx R, double* out) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     DD a[1] = {DD{0.0, 0.0}};
     if ((int)threadIdx.x < c.count) a[0].hi = v[c.start + threadIdx.x];
     double o[1];
@@ -302,6 +311,52 @@ __device__ __forceinline__ T row_plus(const Sell& S, const T* __restrict__ val, 
     return row_accumulate<false>(S, val, [&](int j) { return __ldg(x + j); }, row, s);
 }
 
+// The first P entries of a SELL row (structure and values) loaded ahead of the gathers: before the
+// kernel waits for its predecessor.  accumulate() then gathers X and sums every entry in entry order
+// (entries past P are loaded there, in batches), the same arithmetic as row_accumulate.
+constexpr int kRowPre = 16;
+
+template <class T, int P = kRowPre>
+struct RowPre {
+    int len = 0, base = 0;
+    int col[P];
+    T a[P];
+    __device__ __forceinline__ void load(const Sell& S, const T* __restrict__ val, int row) {
+        len = __ldg(S.rlen + row);
+        base = sell_base(S, row);
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (q < len) {
+                const int e = base + (q << 5);
+                col[q] = __ldg(S.col + e);
+                a[q] = __ldg(val + e);
+            }
+    }
+    template <bool MINUS, class XF>
+    __device__ __forceinline__ T accumulate(const Sell& S, const T* __restrict__ val, XF xf, T s) const {
+        T xv[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (q < len) xv[q] = xf(col[q]);
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (q < len) {
+                if (MINUS)
+                    s -= a[q] * xv[q];
+                else
+                    s += a[q] * xv[q];
+            }
+        for (int k = P; k < len; ++k) {  // rows longer than P: one entry at a time
+            const int e = base + (k << 5);
+            if (MINUS)
+                s -= __ldg(val + e) * xf(__ldg(S.col + e));
+            else
+                s += __ldg(val + e) * xf(__ldg(S.col + e));
+        }
+        return s;
+    }
+};
+
 // Which SysState flag a kernel honours: the outer "done" or the inner-solve "innerDone".
 enum : int { kFlagDone = 0, kFlagInner = 1 };
 
@@ -317,8 +372,9 @@ __device__ __forceinline__ bool chunk_skip(const Chunk& c, const SysState* st, i
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_zero_rows(const Chunk* __restrict__ ch, T* __restrict__ x,
                                                            const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) x[row] = T(0);
 }
@@ -327,8 +383,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_zero_rows(const Chunk* __restri
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restrict__ ch, const T* __restrict__ r,
                                                            T* __restrict__ w, const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) w[row] = r[row];
 }
@@ -337,8 +394,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_copy_rows(const Chunk* __restri
 template <class From, class To>
 __global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restrict__ ch, const From* __restrict__ a,
                                                            To* __restrict__ b, const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (chunk_skip(c, st, flag)) return;
     for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) b[row] = (To)a[row];
 }
@@ -354,16 +412,21 @@ __global__ void __launch_bounds__(kRowsPerCta) k_cast_rows(const Chunk* __restri
 // gathers): the more rows in flight per SM the better.  Batches of 6 entries (one batch for the
 // rows of a hex mesh) fit 32 registers in FP32, so 8 CTAs of 256 threads stay resident.
 template <class T, int MODE = 0>
-__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 8 : 6) k_smooth_gs(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 6 : 4) k_smooth_gs(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                            const T* __restrict__ diag, const T* __restrict__ r, T* x,
                                                            const int32_t* __restrict__ agg, const T* __restrict__ xc,
                                                            const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
+    if ((int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
+    const T dg = __ldg(diag + row);
+    RowPre<T, 6> pre;
+    if (MODE != 1) pre.load(S, val, row);
+    pdl_wait();
+    if (chunk_skip(c, st, flag)) return;
     if (MODE == 1) {
-        x[row] = r[row] / diag[row];
+        x[row] = r[row] / dg;
         return;
     }
     auto xf = [&](int j) -> T {
@@ -374,8 +437,8 @@ __global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 8 : 6) k_smooth_
         }
         return v;
     };
-    const T s = row_accumulate<true, T, decltype(xf), 6>(S, val, xf, row, r[row]);
-    x[row] = s / diag[row];
+    const T s = pre.template accumulate<true>(S, val, xf, r[row]);
+    x[row] = s / dg;
 }
 
 // Block-hybrid Gauss-Seidel sweep.  One CTA per block of <= kBlockRows rows: the block's x lives
@@ -469,14 +532,24 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
 // FP32: 48 registers, 5 resident CTAs per SM (measured faster than 4 at 56 registers on the coarse
 // levels, whose rows of 11-19 entries take two or three batches); FP64 keeps the compiler's choice.
 template <class T, int MODE>
-__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 3 : 2) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
                                                                const T* __restrict__ val, const T* __restrict__ diag,
                                                                const T* __restrict__ r, const T* __restrict__ xi,
                                                                T* __restrict__ xo, T omega,
                                                                const int32_t* __restrict__ agg,
                                                                const T* __restrict__ xc, const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    // the thread's first row: structure, values and diagonal ahead of the wait
+    const int row0 = c.start + threadIdx.x;
+    const bool has = (int)threadIdx.x < c.count;
+    RowPre<T> pre;
+    T d0 = T(1);
+    if (has) {
+        d0 = __ldg(diag + row0);
+        if (MODE != 1) pre.load(S, val, row0);
+    }
+    pdl_wait();
     if (chunk_skip(c, st, flag)) return;
     auto xv = [&](int j) -> T {
         T v = __ldg(xi + j);
@@ -487,14 +560,19 @@ __global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_smooth_
         return v;
     };
     // chunks of up to kRowsPerCta rows (one pass), or wider level-0 chunks (strided)
-    for (int row = c.start + threadIdx.x; row < c.start + c.count; row += kRowsPerCta) {
+    T dg = d0;
+    for (int row = row0; row < c.start + c.count; row += kRowsPerCta) {
+        if (row != row0) {
+            dg = diag[row];
+            if (MODE != 1) pre.load(S, val, row);
+        }
         if (MODE == 1) {
-            const T v = r[row] / diag[row];
+            const T v = r[row] / dg;
             xo[row] = omega == T(1) ? v : omega * v;
             continue;
         }
-        const T s = row_accumulate<true>(S, val, xv, row, r[row]);
-        const T v = s / diag[row];
+        const T s = pre.template accumulate<true>(S, val, xv, r[row]);
+        const T v = s / dg;
         if (omega == T(1)) {
             xo[row] = v;
         } else {
@@ -506,29 +584,49 @@ __global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_smooth_
 
 // res = r - A x  (GAMG.cpp:387-401: diagonal first, then the faces in order)
 template <class T>
-__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 5 : 1) k_residual(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 4 : 2) k_residual(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                           const T* __restrict__ diag, const T* __restrict__ r,
                                                           const T* __restrict__ x, T* __restrict__ res,
                                                           const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
+    if ((int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
-    const T s = row_minus(S, val, x, row, r[row] - diag[row] * x[row]);
-    res[row] = s;
+    RowPre<T> pre;
+    pre.load(S, val, row);
+    const T dg = __ldg(diag + row);
+    pdl_wait();
+    if (chunk_skip(c, st, flag)) return;
+    res[row] = pre.template accumulate<true>(S, val, [&](int j) { return __ldg(x + j); }, r[row] - dg * x[row]);
 }
 
 // rc[R] = sum of res over the children of R in ascending natural order (GAMG.cpp:434-435)
+constexpr int kChildPre = 8;
+
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_restrict(const Chunk* __restrict__ ch, const int32_t* __restrict__ cptr,
                                                           const int32_t* __restrict__ child, const T* __restrict__ res,
                                                           T* __restrict__ rc, const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
+    if ((int)threadIdx.x >= c.count) return;
     const int R = c.start + threadIdx.x;
+    const int k0 = __ldg(cptr + R), k1 = __ldg(cptr + R + 1);
+    int kid[kChildPre];
+#pragma unroll
+    for (int q = 0; q < kChildPre; ++q)
+        if (k0 + q < k1) kid[q] = __ldg(child + k0 + q);
+    pdl_wait();
+    if (chunk_skip(c, st, flag)) return;
+    T v[kChildPre];
+#pragma unroll
+    for (int q = 0; q < kChildPre; ++q)
+        if (k0 + q < k1) v[q] = res[kid[q]];
     T s = T(0);
-    for (int k = cptr[R]; k < cptr[R + 1]; ++k) s += res[child[k]];
+#pragma unroll
+    for (int q = 0; q < kChildPre; ++q)
+        if (k0 + q < k1) s += v[q];
+    for (int k = k0 + kChildPre; k < k1; ++k) s += res[child[k]];
     rc[R] = s;
 }
 
@@ -536,11 +634,13 @@ __global__ void __launch_bounds__(kRowsPerCta) k_restrict(const Chunk* __restric
 template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_prolong(const Chunk* __restrict__ ch, const int32_t* __restrict__ agg,
                                                          const T* __restrict__ xc, T* __restrict__ x, const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    if (chunk_skip(c, st, flag) || (int)threadIdx.x >= c.count) return;
+    if ((int)threadIdx.x >= c.count) return;
     const int row = c.start + threadIdx.x;
-    const int a = agg[row];
+    const int a = __ldg(agg + row);
+    pdl_wait();
+    if (chunk_skip(c, st, flag)) return;
     if (a >= 0) x[row] += xc[a];
 }
 

@@ -24,8 +24,9 @@ __device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, doubl
 template <class T, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_sum_x(const Chunk* __restrict__ ch, const T* __restrict__ x, RedCtx R,
                                                        SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     BlockSum<1, EXACT> acc;
     acc.begin();
     VLM_ROWS(c) acc.add(0, (double)x[row]);
@@ -43,8 +44,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_init_residual(const Chunk* __re
                                                                const int32_t* __restrict__ perm, double* __restrict__ r,
                                                                float* __restrict__ r32, const int32_t* __restrict__ nCells,
                                                                RedCtx R, SysState* st, const DevCtrl* __restrict__ ctrlp) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     const double xRef = st[c.sys].s0 / (double)nCells[c.sys];
     BlockSum<2, EXACT> acc;
     acc.begin();
@@ -92,8 +94,9 @@ template <class T>
 __global__ void __launch_bounds__(kRowsPerCta) k_precond_diag(const Chunk* __restrict__ ch, const T* __restrict__ rD,
                                                               const T* __restrict__ r, T* __restrict__ w,
                                                               const SysState* st, int flag) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (sys_idle(st[c.sys], flag)) return;
     VLM_ROWS(c) w[row] = rD[row] * r[row];
 }
@@ -114,8 +117,9 @@ __global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* 
 template <class T, int FLAG, bool EXACT, class W = T>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restrict__ ch, const W* __restrict__ w,
                                                             const T* __restrict__ r, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
@@ -134,8 +138,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
 template <class T, int FLAG, class W = T>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__ ch, const W* __restrict__ w,
                                                        T* __restrict__ p, const SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     const SysState& s = st[c.sys];
     if (sys_idle(s, FLAG)) return;
     const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
@@ -152,8 +157,9 @@ template <class T, int FLAG, bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restrict__ ch, Sell S, const T* __restrict__ val,
                                                           const T* __restrict__ diag, const T* __restrict__ p,
                                                           T* __restrict__ Ap, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
@@ -185,8 +191,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
                                                             const T* __restrict__ p, const T* __restrict__ Ap,
                                                             const int32_t* __restrict__ perm, RedCtx R, SysState* st,
                                                             const DevCtrl* __restrict__ ctrlp, float* __restrict__ r32) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (sys_idle(st[c.sys], FLAG)) return;
     const T alpha = (T)st[c.sys].alpha;
     BlockSum<1, EXACT> acc;
@@ -243,8 +250,9 @@ __global__ void k_inner_begin(int nsys, SysState* st) {
 // x64 += e32 ; then r64 = b - A x64 in a second kernel (neighbours must be updated first)
 __global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                                const float* __restrict__ e, const SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     VLM_ROWS(c) x[row] += (double)e[row];
 }
@@ -257,8 +265,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
                                                                 const double* __restrict__ b, double* __restrict__ r,
                                                                 float* __restrict__ r32, RedCtx R, SysState* st,
                                                                 const DevCtrl* __restrict__ ctrlp) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     BlockSum<1, false> acc;
     acc.begin();
@@ -290,8 +299,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
 template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restrict__ ch, const double* __restrict__ r0,
                                                           const double* __restrict__ r, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
@@ -314,8 +324,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_rho(const Chunk* __restric
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_p(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ p,
                                                         const SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     const SysState& s = st[c.sys];
     if (s.done) return;
     if (s.iterations == 0) {
@@ -333,8 +344,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_alpha(const Chunk* __
                                                                  const double* __restrict__ diag,
                                                                  const double* __restrict__ y, double* __restrict__ Ay,
                                                                  const double* __restrict__ r0, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
@@ -358,8 +370,9 @@ template <bool EXACT>
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict__ ch, const double* __restrict__ r,
                                                         const double* __restrict__ Ay, double* __restrict__ sv, RedCtx R,
                                                         SysState* st, const DevCtrl* __restrict__ ctrlp) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha;
     BlockSum<1, EXACT> acc;
@@ -387,8 +400,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_s(const Chunk* __restrict_
 // early exit of LinearSolver.cpp:224-227
 __global__ void __launch_bounds__(kRowsPerCta) k_bicg_early(const Chunk* __restrict__ ch, double* __restrict__ x,
                                                             const double* __restrict__ y, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     SysState& s = st[c.sys];
     if (s.done || s.s1 == 0.0) return;
     const double alpha = s.alpha;
@@ -412,8 +426,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_spmv_omega(const Chunk* __
                                                                  const double* __restrict__ diag,
                                                                  const double* __restrict__ z, double* __restrict__ t,
                                                                  const double* __restrict__ sv, RedCtx R, SysState* st) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     BlockSum<2, EXACT> acc;
     acc.begin();
@@ -437,8 +452,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
                                                              const double* __restrict__ z, const double* __restrict__ sv,
                                                              const double* __restrict__ t, RedCtx R, SysState* st,
                                                              const DevCtrl* __restrict__ ctrlp) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     if (st[c.sys].done) return;
     const double alpha = st[c.sys].alpha, omega = st[c.sys].omega;
     BlockSum<1, EXACT> acc;
@@ -467,8 +483,9 @@ __global__ void __launch_bounds__(kRowsPerCta) k_bicg_update(const Chunk* __rest
 __global__ void __launch_bounds__(kRowsPerCta) k_amul(const Chunk* __restrict__ ch, Sell S, const double* __restrict__ val,
                                                       const double* __restrict__ diag, const double* __restrict__ x,
                                                       double* __restrict__ y) {
-    pdl_entry();
+    pdl_launch();
     const Chunk c = ch[blockIdx.x];
+    pdl_wait();
     VLM_ROWS(c) y[row] = row_plus(S, val, x, row, diag[row] * x[row]);
 }
 

@@ -80,9 +80,8 @@ constexpr int kCoarseSharedN = 80;
 thread_local int64_t tl_launches = 0;
 
 // Launch helper: skips empty grids (a zero-block launch is an error) and counts the launch.
-// Programmatic dependent launch for the solver kernels launched directly on a stream (VLM_PDL=0
-// turns it off).  Inside the captured solve graphs it measured no faster, so graph capture
-// records plain launches.
+// Programmatic dependent launch for the solver kernels (VLM_PDL=0 turns it off): each kernel loads
+// its fixed inputs while its predecessor drains (pdl_launch / pdl_wait).
 thread_local bool tl_capturing = false;
 
 bool pdlEnabled() {
@@ -90,7 +89,13 @@ bool pdlEnabled() {
         const char* v = std::getenv("VLM_PDL");
         return !(v && v[0] == '0');
     }();
-    return on && !tl_capturing;
+    // inside captured solve graphs too (programmatic edges between consecutive kernel nodes), unless
+    // VLM_PDL_GRAPH=0
+    static const bool inGraphs = [] {
+        const char* v = std::getenv("VLM_PDL_GRAPH");
+        return !(v && v[0] == '0');
+    }();
+    return on && (inGraphs || !tl_capturing);
 }
 
 template <class... Exp, class... Act>
@@ -229,6 +234,7 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
         D.blocks = add(P.blocks);
         D.chunks.upload(all, stream_);
+        D.hostChunks = all;
         if (P.blockGS) D.rowColour.upload(P.rowColour, stream_);
         if (P.box) {
             D.box = true;
@@ -408,6 +414,26 @@ void DeviceBatch::ensureVectors(bool mixed, bool bicg) {
     }
 }
 
+// The rows of a box-kernel launch: the range form for a batch of one system (its chunks are
+// consecutive), else the chunk list.  *grid: CTAs of the launch.
+BoxRows DeviceBatch::boxRows(const DevLevel& D, const ChunkList& l, int* grid) const {
+    BoxRows R = {};
+    if (plan_.nsys == 1 && l.n > 0) {
+        const Chunk& a = D.hostChunks[size_t(l.off)];
+        const Chunk& z = D.hostChunks[size_t(l.off + l.n - 1)];
+        R.ch = nullptr;
+        R.one = plan_.levels[0].boxes[0];
+        R.begin = a.start;
+        R.end = z.start + z.count;
+        *grid = (R.end - R.begin + kRowsPerCta - 1) / kRowsPerCta;
+    } else {
+        R.ch = D.ch(l);
+        R.boxes = boxes_.get();
+        *grid = l.n;
+    }
+    return R;
+}
+
 RedCtx DeviceBatch::red() const {
     return RedCtx{partials_.get(), xbins_.get(), counters_.get(), slotBegin_.get(), slotEnd_.get()};
 }
@@ -521,20 +547,18 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
         if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, rows.n, kRowsPerCta, s, D.ch(rows), x, st, flag);
         const bool boxK = k == 0 && boxOn_;
         const T* bc = LV<T>::bcoef(D);
-        const BoxSys* bx = boxes_.get();
         for (int sweep = 0; sweep < 2; ++sweep)
             for (int t = 0; t < D.nSteps; ++t) {
                 const ChunkList& l = head ? (pre ? D.headFwd[t] : D.headRev[t]) : (pre ? D.fwd[t] : D.rev[t]);
                 if (boxK) {
+                    int g = 0;
+                    const BoxRows R = boxRows(D, l, &g);
                     if (two && sweep == 0 && t == 0 && pre)
-                        VLM_LAUNCH((k_box_gs<T, 1>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
-                                   xc, st, flag);
+                        VLM_LAUNCH((k_box_gs<T, 1>), g, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc, st, flag);
                     else if (two && sweep == 0 && t == 0)
-                        VLM_LAUNCH((k_box_gs<T, 2>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
-                                   xc, st, flag);
+                        VLM_LAUNCH((k_box_gs<T, 2>), g, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc, st, flag);
                     else
-                        VLM_LAUNCH((k_box_gs<T, 0>), l.n, kRowsPerCta, s, D.ch(l), bx, bc, D.nrows, diag, r, x, agg,
-                                   xc, st, flag);
+                        VLM_LAUNCH((k_box_gs<T, 0>), g, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc, st, flag);
                     continue;
                 }
                 if (two && sweep == 0 && t == 0 && pre)
@@ -570,10 +594,12 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
         const ChunkList& rows = tail ? D.headActive : D.active;
         const ChunkList& next = tail ? N.headIn : N.all;
         recordSmooth<T>(k, rr(k), xx(k), sm, true, flag, tail);
-        if (k == 0 && boxOn_)
-            VLM_LAUNCH(k_box_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), (const BoxSys*)boxes_.get(),
-                       LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k), (const T*)xx(k), LV<T>::t(D), st, flag);
-        else
+        if (k == 0 && boxOn_) {
+            int g = 0;
+            const BoxRows R = boxRows(D, rows, &g);
+            VLM_LAUNCH(k_box_residual<T>, g, kRowsPerCta, s, R, LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k),
+                       (const T*)xx(k), LV<T>::t(D), st, flag);
+        } else
             VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
                        rr(k), xx(k), LV<T>::t(D), st, flag);
         VLM_LAUNCH(k_restrict<T>, next.n, kRowsPerCta, s, N.ch(next), D.childPtr.get(), D.child.get(), LV<T>::t(D),
@@ -1398,6 +1424,31 @@ void DeviceBatch::precondApply(const double* diag, const double* upper, const do
     if (dilu) checkLevelError();
 }
 
+int groupBarrierCheck(cudaStream_t s, int G, long long spinLimit, int absent, int rounds, int* passedOut) {
+    if (G < 1 || G > 64 || rounds < 1 || spinLimit < 1) throw Error(VLM_ERR_BAD_ARG, "barrier check: 1 <= ctas <= 64, rounds >= 1, spin limit >= 1");
+    DBuf<DiluBar> bar(1);
+    DBuf<int> err(1), passed(static_cast<size_t>(G));
+    bar.zero(s);
+    err.zero(s);
+    passed.zero(s);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(G));
+    cfg.blockDim = dim3(unsigned(kDiluThreads));
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    VLM_CUDA(cudaLaunchKernelEx(&cfg, k_group_barrier_check, bar.get(), G, err.get(), spinLimit, absent, rounds,
+                                passed.get()));
+    int h = 0;
+    VLM_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaMemcpyAsync(passedOut, passed.get(), sizeof(int) * size_t(G), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
 double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n) {
     if (n <= 0) return 0.0;
     std::vector<Chunk> ch;
@@ -1438,19 +1489,23 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
         // box level 0: each face coefficient once, no column indices
         run = [&] {
             for (int t = 0; t < D0.nSteps; ++t) {
+                int g = 0;
+                const BoxRows R = boxRows(D0, D0.fwd[t], &g);
                 if (f32)
-                    VLM_LAUNCH((k_box_gs<float, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), (const BoxSys*)boxes_.get(), (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr, (const SysState*)st_.get(), kFlagDone);
+                    VLM_LAUNCH((k_box_gs<float, 0>), g, kRowsPerCta, s, R, (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr, (const SysState*)st_.get(), kFlagDone);
                 else
-                    VLM_LAUNCH((k_box_gs<double, 0>), D0.fwd[t].n, kRowsPerCta, s, D0.ch(D0.fwd[t]), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), (const int32_t*)nullptr, (const double*)nullptr, (const SysState*)st_.get(), kFlagDone);
+                    VLM_LAUNCH((k_box_gs<double, 0>), g, kRowsPerCta, s, R, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), (const int32_t*)nullptr, (const double*)nullptr, (const SysState*)st_.get(), kFlagDone);
             }
         };
         *bytesPerLaunch = sz * 4 * N + sz * F;
     } else if ((name == "residual64" || name == "residual32") && boxOn_) {
         run = [&] {
+            int g = 0;
+            const BoxRows R = boxRows(D0, D0.active, &g);
             if (f32)
-                VLM_LAUNCH(k_box_residual<float>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), (const BoxSys*)boxes_.get(), (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), (const float*)w32_.get(), D0.t32.get(), (const SysState*)st_.get(), kFlagDone);
+                VLM_LAUNCH(k_box_residual<float>, g, kRowsPerCta, s, R, (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), (const float*)w32_.get(), D0.t32.get(), (const SysState*)st_.get(), kFlagDone);
             else
-                VLM_LAUNCH(k_box_residual<double>, D0.active.n, kRowsPerCta, s, D0.ch(D0.active), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), (const double*)w_.get(), D0.t.get(), (const SysState*)st_.get(), kFlagDone);
+                VLM_LAUNCH(k_box_residual<double>, g, kRowsPerCta, s, R, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), (const double*)w_.get(), D0.t.get(), (const SysState*)st_.get(), kFlagDone);
         };
         *bytesPerLaunch = sz * 4 * N + sz * F;
     } else if (name == "spmv64") {

@@ -24,6 +24,7 @@ struct DevLevel {
     DBuf<int8_t> rowColour;
     DBuf<int32_t> slPtr, rlen, col, src;
     DBuf<Chunk> chunks;
+    std::vector<Chunk> hostChunks;  // host copy of `chunks`
     ChunkList active, all;
     ChunkList headActive, headIn;  // coarse-tail mode: rows above each system's tail / restricted into
     std::vector<ChunkList> headFwd, headRev;  // coarse-tail mode: colour steps of the systems above the tail
@@ -170,6 +171,7 @@ private:
     void buildGraph(const SolveKey& key, GraphExec& g);
     void ensureVectors(bool mixed, bool bicg);
     RedCtx red() const;
+    BoxRows boxRows(const DevLevel& D, const ChunkList& l, int* grid) const;
 
     BatchPlan plan_;
     std::vector<DevLevel> L_;
@@ -213,6 +215,11 @@ private:
 
     friend struct StreamSwap;
 };
+
+// The level-scheduled kernels' bounded group barrier run on its own: G co-resident CTAs pass
+// `rounds` barriers, CTA `absent` (if in range) never arrives.  Returns the status word the barrier
+// left (0 or VLM_ERR_TIMEOUT); passed[b] = barriers CTA b got through before any wait gave up.
+int groupBarrierCheck(cudaStream_t s, int G, long long spinLimit, int absent, int rounds, int* passed);
 
 // Exact (order-independent) sum of n device doubles, ordered on stream s.
 double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n);
