@@ -121,6 +121,8 @@ vlm_status vlm_ctx_destroy(vlm_ctx* ctx);
 const char* vlm_last_error(const vlm_ctx* ctx); /* ctx may be NULL: last error of this thread */
 /* Stream the context orders its work on (a cudaStream_t). */
 void* vlm_ctx_stream(vlm_ctx* ctx);
+/* The context's device name (cudaDeviceProp::name), for per-device tuning tables. */
+vlm_status vlm_ctx_device_name(vlm_ctx* ctx, char* name, int32_t capacity);
 
 vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* desc, int32_t merge_levels, vlm_mesh** out);
 /* A batch of n_systems independent meshes registered as one device object (batched GAMG-PCG:
@@ -237,6 +239,15 @@ vlm_status vlm_pressure_solve_device(vlm_ctx* ctx, vlm_mesh* mesh, const double*
 
 /* Kernel launches executed on this mesh so far and its device memory footprint in bytes. */
 vlm_status vlm_mesh_stats(vlm_mesh* mesh, int64_t* launches, int64_t* device_bytes);
+/* Launch configuration of the coarse V-cycle tail (no reference counterpart: it only shapes
+ * launches and leaves every result bit for bit as it is): the levels of at most max_rows rows of a
+ * system (and the whole V-cycle of systems of at most full_rows level-0 rows) run in one launch on a
+ * thread-block cluster of `cluster` CTAs (1, 2, 4 or 8).  0 keeps a value; row limits left at 0 scale
+ * with the cluster.  Set it before the mesh's first solve or flow (recorded graphs are dropped; a
+ * flow created before keeps launching the old configuration).  The tuner (voluma_b200/tune.py)
+ * picks these per device and mesh size. */
+vlm_status vlm_mesh_set_tail(vlm_mesh* mesh, int32_t cluster, int64_t max_rows, int64_t full_rows);
+vlm_status vlm_mesh_get_tail(vlm_mesh* mesh, int32_t* cluster, int64_t* max_rows, int64_t* full_rows);
 /* Measurement hook: times `reps` back-to-back launches of one level-0 kernel on the matrix of
  * the last solve ("amul64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch
  * is one full multicolour sweep; "vcycle32" / "vcycle32_notail" one FP32 V-cycle with / without

@@ -26,7 +26,7 @@ def lib():
     global _lib
     if _lib is None:
         if not available():
-            raise RuntimeError(f"reference oracle not built: {LIB_PATH} (run make -C oracle)")
+            raise RuntimeError(f"reference oracle not built: {LIB_PATH} (run make -C oracle REF=<reference tree>)")
         L = C.CDLL(LIB_PATH)
         P = C.c_void_p
         dp = np.ctypeslib.ndpointer(np.float64, flags="C")

@@ -23,7 +23,7 @@ CFD_REPRODUCIBLE mode:
   * totalp: the total-pressure inlet of cases/channelInlet/totalPressure.json (TotalPressureBC with
     PressureInletOutletVelocityBC, BoundaryCondition.h:325-364), steady SIMPLE, 8 steps from rest.
 Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_bc_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_bc_golden.py
 """
 import os
 import sys

@@ -5,7 +5,7 @@ oracle/ref_flow.cpp) to residualTol 1e-6 as fvmFlow's steady loop stops it (fvmF
 in the default mode and in CFD_REPRODUCIBLE mode.  Stores the converged U, p, phi and the iteration
 counts, and the FNV-1a checksums the reference prints for U and p (VtkWriter.cpp:81-99).
 Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_cavity64_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_cavity64_golden.py
 """
 import os
 import sys

@@ -3,7 +3,7 @@ TVD-limited divergence schemes of fvm::div (Fvm.h:47-137: limitedLinear k, vanLe
 compiled into oracle/_ref/libvlmref.so and driven by oracle/ref_flow.cpp, in CFD_REPRODUCIBLE mode:
 the 16 x 16 lid cavity (6 SIMPLE steps) per scheme and the 12^3 Taylor-Green vortex with vanLeer
 (3 PIMPLE steps).  Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_div_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_div_golden.py
 """
 import os
 import sys

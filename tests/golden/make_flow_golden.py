@@ -2,7 +2,7 @@
 (solvers/IncompressibleFlow.cpp) compiled from the reference's own sources into oracle/_ref/libvlmref.so
 and driven by oracle/ref_flow.cpp, on the lid-driven cavity (cases/cavity/case.json settings) and the
 Taylor-Green vortex (fvmFlow transient defaults).  Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_flow_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_flow_golden.py
 """
 import os
 import sys

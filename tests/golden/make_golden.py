@@ -1,6 +1,6 @@
 """Generates the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a checkout where the reference sources are present:  make -C oracle && python
+Run where the reference sources are present:  make -C oracle REF=<reference tree> && python
 tests/golden/make_golden.py.  Every array comes from the unmodified reference compiled from its
 own sources (oracle/_ref/libvlmref.so through oracle/ref_driver.cpp): generateBox + Mesh::build
 meshes, the LDU pressure matrix of fvm::laplacian(1, p) + setReference(0), and the results of

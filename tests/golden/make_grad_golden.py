@@ -12,7 +12,7 @@ compiled into oracle/_ref/libvlmref.so and driven by oracle/ref_flow.cpp, in CFD
   * freestream_ls: the freestream vortex box with leastSquares + leastSquares, 3 steps of dt 0.02;
   * gradient_ls: the fixedGradient channel with leastSquares + GaussSkew, 6 steps.
 Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_grad_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_grad_golden.py
 """
 import os
 import sys

@@ -3,7 +3,7 @@ reference's Smagorinsky LES model (models/LESModels.cpp, built by TurbulenceMode
 "turbulence" dictionary) and its mean-velocity / constant momentum forcing, compiled from the reference's
 own sources into oracle/_ref/libvlmref.so and driven by oracle/ref_flow.cpp, on a small periodic channel
 (voluma_b200.cases.channel at 8 x 12 x 6).  Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_les_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_les_golden.py
 """
 import os
 import sys

@@ -10,7 +10,7 @@ oracle/ref_flow.cpp), in CFD_REPRODUCIBLE mode:
                                each directory
 
 Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_restart_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_restart_golden.py
 """
 import os
 import shutil

@@ -10,7 +10,7 @@ in CFD_REPRODUCIBLE mode:
     a smooth non-zero initial field;
   * skew2d_default: skew2d_lu in the reference's default (non-reproducible) mode.
 Run where the reference sources are present:
-    make -C oracle && python tests/golden/make_skew_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_skew_golden.py
 """
 import os
 import sys

@@ -302,3 +302,23 @@ def test_box_level0_matches_general_layout(name, precision, monkeypatch):
         assert np.array_equal(x1, x2) and p1.finalResidual == p2.finalResidual
     else:
         assert rel(x1, x2) <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["periodic24", "cavity16", "jitter10x8x6"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tail_launch_configurations_give_identical_results(name, precision):
+    """The coarse V-cycle tail (one CTA or a thread-block cluster of 2, 4 or 8 CTAs per system, taking
+    the levels below a row limit, or the whole V-cycle of a small system) only shapes launches: every
+    configuration gives the solution of the per-level launches bit for bit."""
+    g, _ = device_mesh(name)
+    m = vb.Mesh.from_arrays(g)
+    c = ctrl(preconditioner="GAMG", precision=precision)
+    ref = None
+    for cfg in [(1, 32, 1), (1, 256, 1), (1, 1, 4096), (2, 256, 1), (4, 1, 4096), (8, 4096, 1), (8, 1, 8192)]:
+        m.set_tail(*cfg)
+        x = g["x0"].copy()
+        p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, c)
+        if ref is None:
+            ref = (x, p.iterations)
+            assert p.converged
+        assert p.iterations == ref[1] and np.array_equal(x, ref[0]), cfg

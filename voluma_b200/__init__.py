@@ -108,6 +108,11 @@ class Context:
     def stream(self) -> int:
         return load().vlm_ctx_stream(self._h) or 0
 
+    def device_name(self) -> str:
+        buf = C.create_string_buffer(256)
+        check(load().vlm_ctx_device_name(self._h, buf, 256), self._h)
+        return buf.value.decode()
+
     def close(self):
         if getattr(self, "_h", None):
             load().vlm_ctx_destroy(self._h)
@@ -186,6 +191,15 @@ class Mesh:
         check(load().vlm_mesh_register(self.ctx.handle, C.byref(d), merge_levels, C.byref(h)), self.ctx.handle)
         self._h = h
         _live.add(self)
+        self._apply_tuning()
+
+    def _apply_tuning(self):
+        """The tuner's launch configuration for this device and mesh size (voluma_b200/tuning/);
+        VLM_TUNE=0 keeps the built-in defaults."""
+        if os.environ.get("VLM_TUNE", "1") == "0":
+            return
+        from . import tune
+        tune.apply(self)
 
     @classmethod
     def batch(cls, meshes: list, ctx: Context | None = None, merge_levels: int = 2) -> "Mesh":
@@ -230,6 +244,7 @@ class Mesh:
         self.cell_base = np.cumsum([0] + [int(m["n_cells"]) for m in meshes])
         self.face_base = np.cumsum([0] + [len(m["neighbour"]) for m in meshes])
         self.bface_base = np.cumsum([0] + [len(m["owner"]) - len(m["neighbour"]) for m in meshes])
+        self._apply_tuning()
         return self
 
     @classmethod
@@ -263,6 +278,17 @@ class Mesh:
         n, b = C.c_int64(), C.c_int64()
         check(load().vlm_mesh_stats(self._h, C.byref(n), C.byref(b)))
         return n.value, b.value
+
+    def set_tail(self, cluster: int = 0, max_rows: int = 0, full_rows: int = 0):
+        """Coarse V-cycle tail launch configuration (vlm_mesh_set_tail): cluster size 1/2/4/8, level
+        row limit, whole-V-cycle row limit; 0 keeps a value.  Results are unchanged bit for bit."""
+        check(load().vlm_mesh_set_tail(self._h, int(cluster), int(max_rows), int(full_rows)), self.ctx.handle)
+
+    def tail_config(self):
+        """(cluster, max_rows, full_rows) of the coarse tail; row limits 0 = scaled defaults."""
+        c, a, b = C.c_int32(), C.c_int64(), C.c_int64()
+        check(load().vlm_mesh_get_tail(self._h, C.byref(c), C.byref(a), C.byref(b)))
+        return c.value, a.value, b.value
 
     def profile_kernel(self, kernel: str, reps: int = 20):
         """(ms per launch, algorithmic bytes per launch) of a level-0 kernel on the last solve's matrix."""

@@ -15,7 +15,8 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_mesh_release", "vlm_amul", "vlm_ldu_solve", "vlm_ldu_solve_device", "vlm_gamg_apply",
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
-           "vlm_topology_box", "vlm_barrier_check",
+           "vlm_topology_box", "vlm_barrier_check", "vlm_mesh_set_tail", "vlm_mesh_get_tail",
+           "vlm_ctx_device_name",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
            "vlm_flow_step", "vlm_flow_run_steady", "vlm_flow_get_state", "vlm_flow_destroy", "vlm_flow_launches",
@@ -158,6 +159,9 @@ def load():
     L.vlm_pressure_solve_batch.argtypes = [P, P, P, P, P, P, P, P, C.c_double, i32, i32, C.POINTER(SolverCtrl),
                                            C.POINTER(SolverCtrl), P, P, i32]
     L.vlm_mesh_stats.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.vlm_mesh_set_tail.argtypes = [P, i32, C.c_int64, C.c_int64]
+    L.vlm_ctx_device_name.argtypes = [P, C.c_char_p, i32]
+    L.vlm_mesh_get_tail.argtypes = [P, C.POINTER(i32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.vlm_box_create.argtypes = [P, C.POINTER(BoxSpec), C.POINTER(P)]
     L.vlm_box_desc.argtypes = [P, C.POINTER(MeshDesc)]
     L.vlm_box_patch_sides.argtypes = [P, P]

@@ -171,6 +171,15 @@ const char* vlm_last_error(const vlm_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 void* vlm_ctx_stream(vlm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+vlm_status vlm_ctx_device_name(vlm_ctx* ctx, char* name, int32_t capacity) {
+    if (!ctx || !name || capacity <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    return guarded(ctx, [&] {
+        cudaDeviceProp p;
+        VLM_CUDA(cudaGetDeviceProperties(&p, ctx->device));
+        std::snprintf(name, size_t(capacity), "%s", p.name);
+    });
+}
+
 vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_desc* descs, int32_t mergeLevels,
                                    vlm_mesh** out) {
     if (!ctx || !descs || !out || nsys <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
@@ -397,6 +406,23 @@ vlm_status vlm_mesh_stats(vlm_mesh* m, int64_t* launches, int64_t* bytes) {
     if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
     if (launches) *launches = m->batch->launches();
     if (bytes) *bytes = int64_t(m->batch->deviceBytes());
+    return VLM_OK;
+}
+
+vlm_status vlm_mesh_set_tail(vlm_mesh* m, int32_t cluster, int64_t max_rows, int64_t full_rows) {
+    if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    if (cluster < 0 || max_rows < 0 || full_rows < 0) return fail(m->ctx, VLM_ERR_BAD_ARG, "negative tail setting");
+    return guarded(m->ctx, [&] {
+        setDevice(m->ctx);
+        m->batch->setTail(cluster, max_rows, full_rows);
+    });
+}
+
+vlm_status vlm_mesh_get_tail(vlm_mesh* m, int32_t* cluster, int64_t* max_rows, int64_t* full_rows) {
+    if (!m || !cluster || !max_rows || !full_rows) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    int c = 0;
+    m->batch->tailConfig(&c, max_rows, full_rows);
+    *cluster = c;
     return VLM_OK;
 }
 

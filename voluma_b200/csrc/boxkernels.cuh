@@ -231,31 +231,294 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_residual(BoxRows R, const T
     res[row] = pre.template accumulate<true>([&](int j) { return __ldg(x + j); }, r[row] - dg * x[row]);
 }
 
-// Ap = A p ; wApA = sum Ap.p ; alpha = wArA / wApA (k_pcg_spmv on the box layout)
+// ------------------------------------------------------------------ four slots per thread
+// Range form with H % 4 == 0: thread g takes the four consecutive slots 4g..4g+3 of its colour
+// group, which lie in one x-row (same j, k, colour) at x = i0, i0+2, i0+4, i0+6.  Their own arrays
+// (r, diagonal, +x/+y/+z coefficients) and their +-y and +-z neighbours in the other colour are
+// four consecutive, 16-byte aligned rows each (one vector load); the +-x neighbours are the other
+// colour's slots m0-1+p .. m0+4+p of the same x-row (one vector load and one scalar).  Index
+// arithmetic is paid once per four rows, and every row still sums its faces in its own face order.
+template <class T> struct V4 { T v[4]; };
+
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    return V4<float>{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ V4<float> ld4_keep(const float* p, uint64_t pol) {
+    float4 a;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w) : "l"(p), "l"(pol));
+    return V4<float>{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ V4<double> ld4_keep(const double* p, uint64_t pol) {
+    double2 a, b;
+    asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(a.x), "=d"(a.y) : "l"(p), "l"(pol));
+    asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(b.x), "=d"(b.y) : "l"(p + 2), "l"(pol));
+    return V4<double>{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// A four-slot group's geometry and fixed operands (coefficients, diagonal), loaded ahead of the wait.
+// Every neighbour row is formed with the periodic wrap (always a row of the other colour's group),
+// and per-row predicates say which faces the cell has and whether each is internal or cyclic, so
+// walls, cyclic faces and padding slots of odd x extents take the same instruction stream.
+template <class T>
+struct BoxGroup4 {
+    bool valid;     // not a padding group (slots past the colour group's cells)
+    int p;          // parity offset of the group's x-row: cell x = 2 (m0 + v) + p
+    int xr, xe, rmy, rpy, rmz, rpz;  // other colour: x-row at slot m0, the slot just outside, +-y, +-z
+    // per-row faces: bit 0..5 internal -z,-y,-x,+x,+y,+z; bit 6..11 cyclic -z,-y,-x,+x,+y,+z
+    int faces[4];
+    V4<T> dg, cpx, cpy, cpz, cmy, cmz, cmx;  // diagonal, own +d coefficients, neighbours' -d ones
+    T cme;          // the -x coefficient at slot xe (p == 0)
+
+    __device__ __forceinline__ void load(const BoxSys& B, int row, const T* __restrict__ cx,
+                                         const T* __restrict__ cy, const T* __restrict__ cz,
+                                         const T* __restrict__ diag) {
+        const int C = row >= B.base1 ? 1 : 0;
+        const int s = row - (C ? B.base1 : B.base0);
+        valid = s < B.slots;
+        if (!valid) return;
+        const int H = B.H, nx = B.nx, ny = B.ny, nz = B.nz;
+        const int q = fast_div(s, B.divH);
+        const int m0 = s - q * H;
+        const int k = fast_div(q, B.divNy);
+        const int j = q - k * ny;
+        p = (j + k + C) & 1;
+        const bool px = B.per & 1, py = B.per & 2, pz = B.per & 4;
+        const int o = C ? B.base0 : B.base1;
+        const int x0 = o + q * H;  // the other colour's x-row
+        xr = x0 + m0;
+        // the slot just outside the vector: p == 0 -> m0 - 1 (wrapping to H - 1), p == 1 -> m0 + 4 (to 0)
+        xe = p == 0 ? (m0 > 0 ? xr - 1 : x0 + H - 1) : (m0 + 4 < H ? xr + 4 : x0);
+        rmy = o + (j > 0 ? q - 1 : q + ny - 1) * H + m0;
+        rpy = o + (j < ny - 1 ? q + 1 : q - (ny - 1)) * H + m0;
+        rmz = o + (k > 0 ? q - ny : q + (nz - 1) * ny) * H + m0;
+        rpz = o + (k < nz - 1 ? q + ny : q - (nz - 1) * ny) * H + m0;
+        const int fy = (j > 0 ? 2 : (py ? 2 << 6 : 0)) | (j < ny - 1 ? 16 : (py ? 16 << 6 : 0));
+        const int fz = (k > 0 ? 1 : (pz ? 1 << 6 : 0)) | (k < nz - 1 ? 32 : (pz ? 32 << 6 : 0));
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int i = 2 * (m0 + v) + p;
+            const int fx = (i > 0 ? 4 : (px ? 4 << 6 : 0)) | (i < nx - 1 ? 8 : (px ? 8 << 6 : 0));
+            faces[v] = i < nx ? (fx | fy | fz) : 0;  // i >= nx: a padding slot (odd nx)
+        }
+        const uint64_t pol = l2_keep();
+        dg = ld4_keep(diag + row, pol);
+        cpx = ld4_keep(cx + row, pol);
+        cpy = ld4_keep(cy + row, pol);
+        cmy = ld4_keep(cy + rmy, pol);
+        if (nz > 1) {
+            cpz = ld4_keep(cz + row, pol);
+            cmz = ld4_keep(cz + rmz, pol);
+        }
+        cmx = ld4_keep(cx + xr, pol);  // p == 1: the -x neighbours are slots m0..m0+3
+        cme = p == 0 ? ld_keep(cx + xe, pol) : T(0);
+    }
+
+    // s[v] (op)= a_f X(neighbour) over the faces of row v in face order: internal -z, -y, -x, +x, +y,
+    // +z, then the cyclic faces of x, y, z.  xv4(row): four neighbour values; xv1(row): one.
+    template <bool MINUS, bool Z, class XV4, class XV1>
+    __device__ __forceinline__ void accumulate(XV4 xv4, XV1 xv1, T (&s)[4]) const {
+        const V4<T> xmy = xv4(rmy), xpy = xv4(rpy), xrow = xv4(xr);
+        V4<T> xmz, xpz;
+        if (Z) {
+            xmz = xv4(rmz);
+            xpz = xv4(rpz);
+        }
+        const T vx = xv1(xe);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            // p == 0: -x is slot m0+v-1, +x slot m0+v; p == 1: -x slot m0+v, +x slot m0+v+1
+            const T am = p == 0 ? (v == 0 ? cme : cmx.v[v - 1]) : cmx.v[v];
+            const T vm = p == 0 ? (v == 0 ? vx : xrow.v[v - 1]) : xrow.v[v];
+            const T vp = p == 0 ? xrow.v[v] : (v == 3 ? vx : xrow.v[v + 1]);
+            const int f = faces[v];
+            T a = s[v];
+            auto term = [&](int bit, T c, T x) {
+                if (f & bit) {
+                    if (MINUS)
+                        a -= c * x;
+                    else
+                        a += c * x;
+                }
+            };
+            if (Z) term(1, cmz.v[v], xmz.v[v]);
+            term(2, cmy.v[v], xmy.v[v]);
+            term(4, am, vm);
+            term(8, cpx.v[v], vp);
+            term(16, cpy.v[v], xpy.v[v]);
+            if (Z) term(32, cpz.v[v], xpz.v[v]);
+            term(4 << 6, am, vm);
+            term(8 << 6, cpx.v[v], vp);
+            term(2 << 6, cmy.v[v], xmy.v[v]);
+            term(16 << 6, cpy.v[v], xpy.v[v]);
+            if (Z) {
+                term(1 << 6, cmz.v[v], xmz.v[v]);
+                term(32 << 6, cpz.v[v], xpz.v[v]);
+            }
+            s[v] = a;
+        }
+    }
+};
+
+// Gauss-Seidel colour step, four slots per thread (range form, H % 4 == 0); MODE as k_box_gs.
+template <class T, int MODE = 0>
+__global__ void __launch_bounds__(kRowsPerCta) k_box_gs4(BoxRows R, const T* __restrict__ coef, int nrows,
+                                                         const T* __restrict__ diag, const T* __restrict__ r, T* x,
+                                                         const int32_t* __restrict__ agg, const T* __restrict__ xc) {
+    pdl_launch();
+    const int row0 = R.begin + 4 * (int(blockIdx.x) * kRowsPerCta + int(threadIdx.x));
+    if (row0 >= R.end) return;
+    const BoxSys& B = R.one;
+    const T* cx = coef;
+    const T* cy = coef + nrows;
+    const T* cz = coef + 2 * size_t(nrows);
+    if (MODE == 1) {
+        const V4<T> dg = ld4_keep(diag + row0, l2_keep());
+        pdl_wait();
+        const V4<T> rv = ld4(r + row0);
+        T out[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) out[v] = rv.v[v] / dg.v[v];
+        st4(x + row0, out);
+        return;
+    }
+    BoxGroup4<T> G;
+    G.load(B, row0, cx, cy, cz, diag);
+    if (!G.valid) {
+        // padding slots past the colour group's cells: x = r / D as for any padding row
+        pdl_wait();
+        for (int v = 0; v < 4; ++v) x[row0 + v] = r[row0 + v] / diag[row0 + v];
+        return;
+    }
+    pdl_wait();
+    // the other colour's values (x, plus the coarse-grid correction for MODE 2)
+    auto xv4 = [&](int j) -> V4<T> {
+        V4<T> a = ld4(x + j);
+        if (MODE == 2) {
+            const int4 g = __ldg(reinterpret_cast<const int4*>(agg + j));
+            const int gi[4] = {g.x, g.y, g.z, g.w};
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (gi[v] >= 0) a.v[v] += __ldg(xc + gi[v]);
+        }
+        return a;
+    };
+    auto xv1 = [&](int j) -> T {
+        T a = __ldg(x + j);
+        if (MODE == 2) {
+            const int g = __ldg(agg + j);
+            if (g >= 0) a += __ldg(xc + g);
+        }
+        return a;
+    };
+    const V4<T> rv = ld4(r + row0);
+    T s[4] = {rv.v[0], rv.v[1], rv.v[2], rv.v[3]};
+    if (B.nz > 1)
+        G.template accumulate<true, true>(xv4, xv1, s);
+    else
+        G.template accumulate<true, false>(xv4, xv1, s);
+    T out[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) out[v] = s[v] / G.dg.v[v];
+    st4(x + row0, out);
+}
+
+// res = r - A x, four slots per thread (range form, H % 4 == 0)
+template <class T>
+__global__ void __launch_bounds__(kRowsPerCta) k_box_residual4(BoxRows R, const T* __restrict__ coef, int nrows,
+                                                               const T* __restrict__ diag, const T* __restrict__ r,
+                                                               const T* __restrict__ x, T* __restrict__ res) {
+    pdl_launch();
+    const int row0 = R.begin + 4 * (int(blockIdx.x) * kRowsPerCta + int(threadIdx.x));
+    if (row0 >= R.end) return;
+    const BoxSys& B = R.one;
+    const T* cx = coef;
+    const T* cy = coef + nrows;
+    const T* cz = coef + 2 * size_t(nrows);
+    BoxGroup4<T> G;
+    G.load(B, row0, cx, cy, cz, diag);
+    auto xf = [&](int j) -> T { return __ldg(x + j); };
+    if (!G.valid) {
+        pdl_wait();
+        for (int v = 0; v < 4; ++v) res[row0 + v] = r[row0 + v] - diag[row0 + v] * x[row0 + v];
+        return;
+    }
+    pdl_wait();
+    const V4<T> rv = ld4(r + row0), xo = ld4(x + row0);
+    T s[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) s[v] = rv.v[v] - G.dg.v[v] * xo.v[v];
+    auto xv4 = [&](int j) { return ld4(x + j); };
+    if (B.nz > 1)
+        G.template accumulate<true, true>(xv4, xf, s);
+    else
+        G.template accumulate<true, false>(xv4, xf, s);
+    st4(res + row0, s);
+}
+
+// Ap = A p ; wApA = sum Ap.p ; alpha = wArA / wApA (k_pcg_spmv on the box layout).  Rows of a chunk
+// are taken four consecutive rows per thread (the mapping of k_pcg_spmv, so both products add the
+// same partial sums); with the range form and H % 4 == 0 interior groups take the vector path.
 template <class T, int FLAG, bool EXACT>
-__global__ void __launch_bounds__(kRowsPerCta) k_box_pcg_spmv(const Chunk* __restrict__ ch,
-                                                              const BoxSys* __restrict__ boxes,
+__global__ void __launch_bounds__(kRowsPerCta) k_box_pcg_spmv(const Chunk* __restrict__ ch, BoxRows R,
                                                               const T* __restrict__ coef, int nrows,
                                                               const T* __restrict__ diag, const T* __restrict__ p,
-                                                              T* __restrict__ Ap, RedCtx R, SysState* st) {
+                                                              T* __restrict__ Ap, RedCtx Rc, SysState* st) {
     pdl_launch();
     const Chunk c = ch[blockIdx.x];
-    const BoxSys B = box_load(boxes, c.sys);
+    const BoxSys B = R.ch == nullptr ? R.one : box_load(R.boxes, c.sys);
+    const T* cx = coef;
+    const T* cy = coef + nrows;
+    const T* cz = coef + 2 * size_t(nrows);
+    const int row0 = c.start + 4 * int(threadIdx.x);
+    const bool vec = R.ch == nullptr && B.H % 4 == 0 && row0 + 3 < c.start + c.count;
+    BoxGroup4<T> G;
+    G.valid = false;
+    if (vec) G.load(B, row0, cx, cy, cz, diag);
     pdl_wait();
     if (sys_idle(st[c.sys], FLAG)) return;
     auto xf = [&](int j) -> T { return __ldg(p + j); };
     BlockSum<1, EXACT> acc;
     acc.begin();
-    for (int row = c.start + (int)threadIdx.x; row < c.start + c.count; row += kRowsPerCta) {
-        const T pr = p[row];
-        BoxRowPre<T> pre;
-        pre.load(B, row, coef, coef + nrows, coef + 2 * size_t(nrows));
-        const T y = pre.template accumulate<false>(xf, ld_keep(diag + row, l2_keep()) * pr);
-        Ap[row] = y;
-        acc.add(0, (double)y * (double)pr);
+    if (G.valid) {
+        const V4<T> pv = ld4(p + row0);
+        T s[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) s[v] = G.dg.v[v] * pv.v[v];
+        auto xv4 = [&](int j) { return ld4(p + j); };
+        if (B.nz > 1)
+            G.template accumulate<false, true>(xv4, xf, s);
+        else
+            G.template accumulate<false, false>(xv4, xf, s);
+        st4(Ap + row0, s);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc.add(0, (double)s[v] * (double)pv.v[v]);
+    } else {
+        for (int v = 0; v < 4; ++v) {
+            const int row = row0 + v;
+            if (row >= c.start + c.count) break;
+            const T pr = p[row];
+            BoxRowPre<T> pre;
+            pre.load(B, row, cx, cy, cz);
+            const T y = pre.template accumulate<false>(xf, ld_keep(diag + row, l2_keep()) * pr);
+            Ap[row] = y;
+            acc.add(0, (double)y * (double)pr);
+        }
     }
     double out[1];
-    if (acc.finish(c, R, out)) {
+    if (acc.finish(c, Rc, out)) {
         SysState& s = st[c.sys];
         if (fabs(out[0]) < kVSMALL) {
             if (FLAG == kFlagDone) {

@@ -747,16 +747,36 @@ constexpr int kTailBatch = 4;      // entries in flight per row (64 registers at
 constexpr int kTailMaxRows = 1024;  // levels at most this many rows (padded) go to the tail
 constexpr int kTailFullRows = 2048;  // systems at most this many level-0 rows run the whole V-cycle there
 
-template <class T>
+// CL: CTAs of the thread-block cluster that runs one system's tail (CL == 1: one CTA).  With CL > 1
+// the rows of each step are spread over the cluster's threads and the steps are separated by the
+// cluster's hardware barrier (barrier.cluster arrive.release / wait.acquire); vectors that other CTAs
+// of the cluster write are read through L2, and the restriction's residuals go through the level's
+// x2 scratch vector (free while the V-cycle descends) instead of shared memory.
+template <int CL>
+__device__ __forceinline__ void tail_sync() {
+    if (CL == 1) {
+        __syncthreads();
+    } else {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+}
+
+template <class T, int CL>
+__device__ __forceinline__ T tail_ld(const T* p) {
+    if (CL == 1) return *p;
+    return __ldcg(p);
+}
+
+template <class T, int CL = 1>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* __restrict__ tsys,
                                                                  const TailLevel<T>* __restrict__ lev,
                                                                  const double* __restrict__ inv, const T* r0, T* x0,
                                                                  T omega, const SysState* st, int flag, int jacobi0) {
     pdl_entry();
-    __shared__ T resS[kTailFullRows];  // one level's residuals (restriction)
-    const TailSys& ts = tsys[blockIdx.x];
-    if (st != nullptr && sys_idle(st[ts.sys], flag)) return;  // uniform over the CTA
-    const int tid = threadIdx.x, nthr = blockDim.x;
+    __shared__ T resS[CL == 1 ? kTailFullRows : 1];  // one level's residuals (restriction), one CTA
+    const TailSys& ts = tsys[blockIdx.x / CL];
+    if (st != nullptr && sys_idle(st[ts.sys], flag)) return;  // uniform over the CTA / cluster
+    const int tid = int(blockIdx.x % CL) * int(blockDim.x) + int(threadIdx.x), nthr = CL * int(blockDim.x);
     const int c = ts.coarsest;
     auto rOf = [&](int k) -> const T* { return k == 0 ? r0 : lev[k].r; };
     auto xOf = [&](int k) -> T* { return k == 0 ? x0 : lev[k].x; };
@@ -765,18 +785,18 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
     auto gsRows = [&](const TailLevel<T>& L, const T* r, T* x, int g0, int g1, int mode, const T* xc) {
         for (int i = g0 + tid; i < g1; i += nthr) {
             if (mode == 1) {
-                x[i] = r[i] / __ldg(L.diag + i);
+                x[i] = tail_ld<T, CL>(r + i) / __ldg(L.diag + i);
                 continue;
             }
             auto xf = [&](int j) -> T {
-                T v = x[j];
+                T v = tail_ld<T, CL>(x + j);
                 if (mode == 2) {
                     const int a = __ldg(L.agg + j);
-                    if (a >= 0) v += xc[a];
+                    if (a >= 0) v += tail_ld<T, CL>(xc + a);
                 }
                 return v;
             };
-            const T s = row_accumulate<true, T, decltype(xf), kTailBatch>(L.S, L.val, xf, i, r[i]);
+            const T s = row_accumulate<true, T, decltype(xf), kTailBatch>(L.S, L.val, xf, i, tail_ld<T, CL>(r + i));
             x[i] = s / __ldg(L.diag + i);
         }
     };
@@ -789,23 +809,23 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
             const int nc = ts.nColours;
             if (!ts.two) {
                 for (int i = a0 + tid; i < a1; i += nthr) x[i] = T(0);
-                __syncthreads();
+                tail_sync<CL>();
             }
             for (int sweep = 0; sweep < 2; ++sweep)
                 for (int t = 0; t < nc; ++t) {
                     gsRows(L, r, x, ts.grpStart[t], ts.grpStart[t] + ts.grpCount[t],
                            (ts.two && sweep == 0 && t == 0) ? 1 : 0, nullptr);
-                    __syncthreads();
+                    tail_sync<CL>();
                 }
         } else {
         // two pre-sweeps from zero; the first sweep's value of a neighbour is recomputed where
         // the second sweep needs it (MODE 1 then MODE 0 of k_smooth_jacobi)
         auto first = [&](int j) -> T {
-            const T v = r[j] / __ldg(L.diag + j);
+            const T v = tail_ld<T, CL>(r + j) / __ldg(L.diag + j);
             return omega == T(1) ? v : omega * v;
         };
         for (int i = a0 + tid; i < a1; i += nthr) {
-            const T s = row_accumulate<true, T, decltype(first), kTailBatch>(L.S, L.val, first, i, r[i]);
+            const T s = row_accumulate<true, T, decltype(first), kTailBatch>(L.S, L.val, first, i, tail_ld<T, CL>(r + i));
             const T v = s / __ldg(L.diag + i);
             if (omega == T(1)) {
                 x[i] = v;
@@ -814,18 +834,30 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
                 x[i] = xv + omega * (v - xv);
             }
         }
-        __syncthreads();
+        tail_sync<CL>();
         }
         // k_residual + k_restrict: every row's residual (one row per thread, into shared memory where
         // the level fits), then each aggregate sums its children's residuals in child order
         T* rn = lev[k + 1].r;
-        auto xr = [&](int j) -> T { return x[j]; };
+        auto xr = [&](int j) -> T { return tail_ld<T, CL>(x + j); };
         const int b0 = ts.rowStart[k + 1], b1 = b0 + ts.rowCount[k + 1];
-        if (a1 - a0 <= kTailFullRows) {
+        if (CL > 1) {
+            T* res = L.x2;  // free while descending
+            for (int i = a0 + tid; i < a1; i += nthr)
+                res[i] = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
+                                                                           tail_ld<T, CL>(r + i) - __ldg(L.diag + i) * tail_ld<T, CL>(x + i));
+            tail_sync<CL>();
+            for (int R = b0 + tid; R < b1; R += nthr) {
+                T s = T(0);
+                const int q1 = __ldg(L.cptr + R + 1);
+                for (int q = __ldg(L.cptr + R); q < q1; ++q) s += __ldcg(res + __ldg(L.child + q));
+                rn[R] = s;
+            }
+        } else if (a1 - a0 <= kTailFullRows) {
             for (int i = a0 + tid; i < a1; i += nthr)
                 resS[i - a0] = row_accumulate<true, T, decltype(xr), kTailBatch>(L.S, L.val, xr, i,
                                                                                  r[i] - __ldg(L.diag + i) * x[i]);
-            __syncthreads();
+            tail_sync<CL>();
             for (int R = b0 + tid; R < b1; R += nthr) {
                 T s = T(0);
                 const int q1 = __ldg(L.cptr + R + 1);
@@ -845,7 +877,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
                 rn[R] = s;
             }
         }
-        __syncthreads();
+        tail_sync<CL>();
     }
     {
         // coarsest level: x = inv * r (k_coarse_apply)
@@ -855,12 +887,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
         const double* X = inv + ts.invOffset;
         for (int i = tid; i < n; i += nthr) {
             double g = 0.0;
-            for (int j = 0; j < n; ++j) g += __ldg(X + (size_t)i * n + j) * (double)r[rs + j];
+            for (int j = 0; j < n; ++j) g += __ldg(X + (size_t)i * n + j) * (double)tail_ld<T, CL>(r + rs + j);
             x[rs + i] = (T)g;
         }
     }
     for (int k = c - 1; k >= ts.first; --k) {
-        __syncthreads();
+        tail_sync<CL>();
         const TailLevel<T>& L = lev[k];
         const T* r = rOf(k);
         T* x = xOf(k);
@@ -873,16 +905,16 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
             if (!ts.two) {
                 for (int i = a0 + tid; i < a1; i += nthr) {
                     const int a = __ldg(L.agg + i);
-                    if (a >= 0) x[i] += xc[a];
+                    if (a >= 0) x[i] += tail_ld<T, CL>(xc + a);
                 }
-                __syncthreads();
+                tail_sync<CL>();
             }
             for (int sweep = 0; sweep < 2; ++sweep)
                 for (int t = 0; t < nc; ++t) {
                     const int q = nc - 1 - t;
                     gsRows(L, r, x, ts.grpStart[q], ts.grpStart[q] + ts.grpCount[q],
                            (ts.two && sweep == 0 && t == 0) ? 2 : 0, xc);
-                    if (sweep + 1 < 2 || t + 1 < nc) __syncthreads();
+                    if (sweep + 1 < 2 || t + 1 < nc) tail_sync<CL>();
                 }
             continue;
         }
@@ -890,12 +922,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
         // values as adding xc[agg[j]] to every neighbour read, without the two dependent loads per entry)
         for (int i = a0 + tid; i < a1; i += nthr) {
             const int a = __ldg(L.agg + i);
-            if (a >= 0) x[i] += xc[a];
+            if (a >= 0) x[i] += tail_ld<T, CL>(xc + a);
         }
-        __syncthreads();
-        auto xv = [&](int j) -> T { return x[j]; };
+        tail_sync<CL>();
+        auto xv = [&](int j) -> T { return tail_ld<T, CL>(x + j); };
         for (int i = a0 + tid; i < a1; i += nthr) {
-            const T s = row_accumulate<true, T, decltype(xv), kTailBatch>(L.S, L.val, xv, i, r[i]);
+            const T s = row_accumulate<true, T, decltype(xv), kTailBatch>(L.S, L.val, xv, i, tail_ld<T, CL>(r + i));
             const T v = s / __ldg(L.diag + i);
             if (omega == T(1)) {
                 x2[i] = v;
@@ -904,16 +936,16 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
                 x2[i] = x0v + omega * (v - x0v);
             }
         }
-        __syncthreads();
+        tail_sync<CL>();
         // post-sweep 2 (MODE 0), back into x
         for (int i = a0 + tid; i < a1; i += nthr) {
-            auto x2f = [&](int j) -> T { return x2[j]; };
-            const T s = row_accumulate<true, T, decltype(x2f), kTailBatch>(L.S, L.val, x2f, i, r[i]);
+            auto x2f = [&](int j) -> T { return tail_ld<T, CL>(x2 + j); };
+            const T s = row_accumulate<true, T, decltype(x2f), kTailBatch>(L.S, L.val, x2f, i, tail_ld<T, CL>(r + i));
             const T v = s / __ldg(L.diag + i);
             if (omega == T(1)) {
                 x[i] = v;
             } else {
-                const T x0v = x2[i];
+                const T x0v = tail_ld<T, CL>(x2 + i);
                 x[i] = x0v + omega * (v - x0v);
             }
         }

@@ -11,6 +11,8 @@
 
 namespace vlm {
 
+static_assert(kWideRows == 4 * kRowsPerCta, "the level-0 products take four rows per thread");
+
 #define VLM_ROWS(c) for (int row = (c).start + (int)threadIdx.x; row < (c).start + (c).count; row += kRowsPerCta)
 
 // converged() of LinearSolver.cpp:114-117
@@ -163,7 +165,10 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_spmv(const Chunk* __restric
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
-    VLM_ROWS(c) {
+    // four consecutive rows per thread (the box layout's product adds the same partial sums)
+    for (int v = 0; v < 4; ++v) {
+        const int row = c.start + 4 * int(threadIdx.x) + v;
+        if (row >= c.start + c.count) break;
         const T y = row_plus(S, val, p, row, diag[row] * p[row]);
         Ap[row] = y;
         acc.add(0, (double)y * (double)p[row]);

@@ -185,7 +185,11 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         L_[k].coarse.n = int(cds.size()) - L_[k].coarse.off;
     }
     coarse_.upload(cds, stream_);
+    if (const char* cl = std::getenv("VLM_TAIL_CLUSTER")) tailCl_ = std::atoi(cl);
+    if (const char* mr = std::getenv("VLM_TAIL_ROWS")) tailMaxRows_ = std::atoll(mr);
+    if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) tailFullRows_ = std::atoll(fr);
     planTail();
+    buildChunkLists();
     for (int k = 0; k < nL; ++k) {
         LevelPlan& P = plan_.levels[k];
         DevLevel& D = L_[k];
@@ -202,39 +206,6 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
         D.rlen.upload(P.rlen, stream_);
         D.col.upload(P.col, stream_);
         D.src.upload(P.src, stream_);
-        std::vector<Chunk> all;
-        auto add = [&](const std::vector<Chunk>& v) {
-            ChunkList l{int(all.size()), int(v.size())};
-            all.insert(all.end(), v.begin(), v.end());
-            return l;
-        };
-        D.active = add(P.active);
-        D.all = add(P.all);
-        if (tailOn_) {
-            // coarse-tail mode: rows still smoothed by per-level launches, and the rows the last
-            // of those restrictions writes (systems whose tail starts at or below this level)
-            std::vector<Chunk> head, in;
-            for (const Chunk& c : P.active)
-                if (tailFirst_[c.sys] > k) head.push_back(c);
-            for (const Chunk& c : P.all)
-                if (k > 0 && tailFirst_[c.sys] >= k) in.push_back(c);
-            D.headActive = add(head);
-            D.headIn = add(in);
-            for (int t = 0; t < P.nSteps; ++t) {
-                std::vector<Chunk> hf, hr;
-                for (const Chunk& c : P.fwd[t])
-                    if (tailFirst_[c.sys] > k) hf.push_back(c);
-                for (const Chunk& c : P.rev[t])
-                    if (tailFirst_[c.sys] > k) hr.push_back(c);
-                D.headFwd.push_back(add(hf));
-                D.headRev.push_back(add(hr));
-            }
-        }
-        for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
-        for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
-        D.blocks = add(P.blocks);
-        D.chunks.upload(all, stream_);
-        D.hostChunks = all;
         if (P.blockGS) D.rowColour.upload(P.rowColour, stream_);
         if (P.box) {
             D.box = true;
@@ -293,6 +264,70 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     }
     hostState_.resize(size_t(plan_.nsys));
     if (tailOn_) buildTailTable<double>(tail64_);
+    VLM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// Row chunk lists of every level (uploaded): all rows, smoothing rows, colour steps, blocks and,
+// with the coarse tail on, the rows still handled by per-level launches.
+void DeviceBatch::buildChunkLists() {
+    for (int k = 0; k < int(L_.size()); ++k) {
+        const LevelPlan& P = plan_.levels[k];
+        DevLevel& D = L_[k];
+        D.headFwd.clear();
+        D.headRev.clear();
+        D.fwd.clear();
+        D.rev.clear();
+        std::vector<Chunk> all;
+        auto add = [&](const std::vector<Chunk>& v) {
+            ChunkList l{int(all.size()), int(v.size())};
+            all.insert(all.end(), v.begin(), v.end());
+            return l;
+        };
+        D.active = add(P.active);
+        D.all = add(P.all);
+        if (tailOn_) {
+            // coarse-tail mode: rows still smoothed by per-level launches, and the rows the last
+            // of those restrictions writes (systems whose tail starts at or below this level)
+            std::vector<Chunk> head, in;
+            for (const Chunk& c : P.active)
+                if (tailFirst_[c.sys] > k) head.push_back(c);
+            for (const Chunk& c : P.all)
+                if (k > 0 && tailFirst_[c.sys] >= k) in.push_back(c);
+            D.headActive = add(head);
+            D.headIn = add(in);
+            for (int t = 0; t < P.nSteps; ++t) {
+                std::vector<Chunk> hf, hr;
+                for (const Chunk& c : P.fwd[t])
+                    if (tailFirst_[c.sys] > k) hf.push_back(c);
+                for (const Chunk& c : P.rev[t])
+                    if (tailFirst_[c.sys] > k) hr.push_back(c);
+                D.headFwd.push_back(add(hf));
+                D.headRev.push_back(add(hr));
+            }
+        }
+        for (int t = 0; t < P.nSteps; ++t) D.fwd.push_back(add(P.fwd[t]));
+        for (int t = 0; t < P.nSteps; ++t) D.rev.push_back(add(P.rev[t]));
+        D.blocks = add(P.blocks);
+        D.chunks.upload(all, stream_);
+        D.hostChunks = all;
+    }
+}
+
+// Re-plans the coarse tail (cluster size, level row limit, whole-V-cycle row limit; 0 keeps the
+// current value) on a registered batch: chunk lists, tail tables, and the recorded graphs.
+void DeviceBatch::setTail(int cluster, int64_t maxRows, int64_t fullRows) {
+    if (cluster != 0) tailCl_ = cluster;
+    if (maxRows != 0) tailMaxRows_ = maxRows;
+    if (fullRows != 0) tailFullRows_ = fullRows;
+    VLM_CUDA(cudaStreamSynchronize(stream_));
+    graphs_.clear();
+    tailOn_ = false;
+    planTail();
+    buildChunkLists();
+    if (tailOn_) {
+        buildTailTable<double>(tail64_);
+        if (e32_.size() == size_t(L_[0].nrows)) buildTailTable<float>(tail32_);
+    }
     VLM_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -553,6 +588,17 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
                 if (boxK) {
                     int g = 0;
                     const BoxRows R = boxRows(D, l, &g);
+                    if (R.ch == nullptr && R.one.H % 4 == 0) {
+                        // four slots per thread
+                        const int g4 = (R.end - R.begin + 4 * kRowsPerCta - 1) / (4 * kRowsPerCta);
+                        if (two && sweep == 0 && t == 0 && pre)
+                            VLM_LAUNCH((k_box_gs4<T, 1>), g4, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc);
+                        else if (two && sweep == 0 && t == 0)
+                            VLM_LAUNCH((k_box_gs4<T, 2>), g4, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc);
+                        else
+                            VLM_LAUNCH((k_box_gs4<T, 0>), g4, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc);
+                        continue;
+                    }
                     if (two && sweep == 0 && t == 0 && pre)
                         VLM_LAUNCH((k_box_gs<T, 1>), g, kRowsPerCta, s, R, bc, D.nrows, diag, r, x, agg, xc, st, flag);
                     else if (two && sweep == 0 && t == 0)
@@ -597,8 +643,13 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
         if (k == 0 && boxOn_) {
             int g = 0;
             const BoxRows R = boxRows(D, rows, &g);
-            VLM_LAUNCH(k_box_residual<T>, g, kRowsPerCta, s, R, LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k),
-                       (const T*)xx(k), LV<T>::t(D), st, flag);
+            if (R.ch == nullptr && R.one.H % 4 == 0)
+                VLM_LAUNCH(k_box_residual4<T>, (R.end - R.begin + 4 * kRowsPerCta - 1) / (4 * kRowsPerCta),
+                           kRowsPerCta, s, R, LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k), (const T*)xx(k),
+                           LV<T>::t(D));
+            else
+                VLM_LAUNCH(k_box_residual<T>, g, kRowsPerCta, s, R, LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k),
+                           (const T*)xx(k), LV<T>::t(D), st, flag);
         } else
             VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
                        rr(k), xx(k), LV<T>::t(D), st, flag);
@@ -634,8 +685,39 @@ void DeviceBatch::recordTail(const T* r0, T* x0, int flag, bool jacobi0) {
     const TailLevel<T>* tab = std::is_same<T, float>::value ? (const TailLevel<T>*)tail32_.get()
                                                              : (const TailLevel<T>*)tail64_.get();
     if (!tab) throw Error(VLM_ERR_CUDA, "internal: coarse-tail table missing");
-    VLM_LAUNCH(k_vcycle_tail<T>, int(tailSys_.size()), kTailThreads, stream_, (const TailSys*)tailSys_.get(), tab,
-               (const double*)inv_.get(), r0, x0, T(jacobiOmega_), (const SysState*)st_.get(), flag, jacobi0 ? 1 : 0);
+    // one CTA, or one thread-block cluster of tailCl_ CTAs, per system
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(tailSys_.size()) * unsigned(tailCl_));
+    cfg.blockDim = dim3(unsigned(kTailThreads));
+    cfg.stream = stream_;
+    cudaLaunchAttribute at[2];
+    int na = 0;
+    if (tailCl_ > 1) {
+        at[na].id = cudaLaunchAttributeClusterDimension;
+        at[na].val.clusterDim.x = unsigned(tailCl_);
+        at[na].val.clusterDim.y = 1;
+        at[na].val.clusterDim.z = 1;
+        ++na;
+    }
+    if (pdlEnabled()) {
+        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    cfg.attrs = at;
+    cfg.numAttrs = unsigned(na);
+    auto launch = [&](auto kernel) {
+        VLM_CUDA(cudaLaunchKernelEx(&cfg, kernel, (const TailSys*)tailSys_.get(), tab, (const double*)inv_.get(), r0, x0,
+                                    T(jacobiOmega_), (const SysState*)st_.get(), flag, jacobi0 ? 1 : 0));
+    };
+    switch (tailCl_) {
+    case 1: launch(k_vcycle_tail<T, 1>); break;
+    case 2: launch(k_vcycle_tail<T, 2>); break;
+    case 4: launch(k_vcycle_tail<T, 4>); break;
+    case 8: launch(k_vcycle_tail<T, 8>); break;
+    default: throw Error(VLM_ERR_BAD_ARG, "coarse-tail cluster size must be 1, 2, 4 or 8");
+    }
+    ++tl_launches;
 }
 
 // Per system: the first level of the single-CTA tail = the first level (below level 0) whose
@@ -646,9 +728,12 @@ void DeviceBatch::planTail() {
     if (tv && tv[0] == '0') return;
     const int ns = plan_.nsys;
     if (ns == 0) return;
-    int64_t maxRows = kTailMaxRows, fullRows = kTailFullRows;
-    if (const char* mr = std::getenv("VLM_TAIL_ROWS")) maxRows = std::atoll(mr);
-    if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) fullRows = std::atoll(fr);
+    // the tail runs on one CTA or on a cluster of tailCl_ CTAs; unset row limits (0) scale with it
+    if (tailCl_ != 1 && tailCl_ != 2 && tailCl_ != 4 && tailCl_ != 8)
+        throw Error(VLM_ERR_BAD_ARG, "the coarse-tail cluster size must be 1, 2, 4 or 8");
+    const int64_t maxRows = tailMaxRows_ > 0 ? tailMaxRows_ : int64_t(kTailMaxRows) * tailCl_;
+    const int64_t fullRows =
+        tailFullRows_ > 0 ? tailFullRows_ : (tailCl_ == 1 ? int64_t(kTailFullRows) : int64_t(kTailMaxRows) * tailCl_);
     const LevelPlan& L0 = plan_.levels[0];
     tailFirst_.assign(size_t(ns), 0);
     std::vector<TailSys> ts(static_cast<size_t>(ns));
@@ -797,10 +882,12 @@ void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
                    st_.get());
         VLM_LAUNCH((k_pcg_p<double, kFlagDone>), nb, kRowsPerCta, s, ch, w_.get(), p_.get(), st_.get());
     }
-    if (boxOn_)
-        VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, (const BoxSys*)boxes_.get(),
+    if (boxOn_) {
+        int g = 0;
+        VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, boxRows(D0, D0.all, &g),
                    (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)p_.get(),
                    Ap_.get(), red(), st_.get());
+    }
     else
         VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(),
                    D0.diag.get(), p_.get(), Ap_.get(), red(), st_.get());
@@ -822,10 +909,12 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
         throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs the GAMG or diagonal preconditioner");
     VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
-    if (boxOn_)
-        VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, (const BoxSys*)boxes_.get(),
+    if (boxOn_) {
+        int g = 0;
+        VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, boxRows(D0, D0.all, &g),
                    (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)p32_.get(),
                    Ap32_.get(), red(), st_.get());
+    }
     else
         VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(),
                    D0.diag32.get(), p32_.get(), Ap32_.get(), red(), st_.get());
@@ -1491,6 +1580,14 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
             for (int t = 0; t < D0.nSteps; ++t) {
                 int g = 0;
                 const BoxRows R = boxRows(D0, D0.fwd[t], &g);
+                if (R.ch == nullptr && R.one.H % 4 == 0) {
+                    const int g4 = (R.end - R.begin + 4 * kRowsPerCta - 1) / (4 * kRowsPerCta);
+                    if (f32)
+                        VLM_LAUNCH((k_box_gs4<float, 0>), g4, kRowsPerCta, s, R, (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr);
+                    else
+                        VLM_LAUNCH((k_box_gs4<double, 0>), g4, kRowsPerCta, s, R, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), (const int32_t*)nullptr, (const double*)nullptr);
+                    continue;
+                }
                 if (f32)
                     VLM_LAUNCH((k_box_gs<float, 0>), g, kRowsPerCta, s, R, (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)r32_.get(), w32_.get(), (const int32_t*)nullptr, (const float*)nullptr, (const SysState*)st_.get(), kFlagDone);
                 else
@@ -1511,8 +1608,9 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
     } else if (name == "spmv64") {
         // the PCG product with its fused dot (the FP64 Krylov recurrence's largest kernel)
         run = [&] {
+            int g = 0;
             if (boxOn_)
-                VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), (const BoxSys*)boxes_.get(), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
+                VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), boxRows(D0, D0.all, &g), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
             else
                 VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), red(), st_.get());
         };

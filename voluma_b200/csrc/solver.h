@@ -139,6 +139,14 @@ public:
     const std::vector<SysTopo>& topology() const { return topo_; }
     int mergeLevels() const { return mergeLevels_; }
     size_t deviceBytes() const;
+    // Coarse-tail configuration (tuning): cluster size 1/2/4/8, level row limit, whole-V-cycle row
+    // limit (0 keeps a value); re-plans the batch's launches, same results.
+    void setTail(int cluster, int64_t maxRows, int64_t fullRows);
+    void tailConfig(int* cluster, int64_t* maxRows, int64_t* fullRows) const {
+        *cluster = tailCl_;
+        *maxRows = tailMaxRows_;
+        *fullRows = tailFullRows_;
+    }
     int64_t launches() const { return launches_; }
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
     // solve); returns ms per launch and the algorithmic bytes one launch moves.
@@ -151,6 +159,7 @@ private:
     template <class T> void recordTail(const T* r0, T* x0, int flag, bool jacobi0);
     template <class T> void buildTailTable(DBuf<TailLevel<T>>& out);
     void planTail();
+    void buildChunkLists();
     void ensureDilu();
     void recordDiluApply(const double* r, double* w);
     void diluFactor(const double* upper, const double* lower);
@@ -198,6 +207,9 @@ private:
     int tailMaxFirst_ = 0;      // head levels: k < tailMaxFirst_
     std::vector<int> tailFirst_;
     DBuf<TailSys> tailSys_;
+    int tailCl_ = 1;                     // CTAs of the cluster that runs one system's tail (the tuner may widen it)
+    int64_t tailMaxRows_ = 0;            // levels of at most this many rows go to the tail (0: scaled default)
+    int64_t tailFullRows_ = 0;           // systems of at most this many level-0 rows: whole V-cycle there
     std::vector<SysTopo> topo_;          // host topology (owned by the caller for the batch's lifetime)
     int mergeLevels_ = 2;
     std::unique_ptr<DiluDev> dilu_;      // built on the first DIC/DILU/Gauss-Seidel solve
