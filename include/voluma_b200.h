@@ -310,7 +310,8 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * velocity, :343-364) and fixedFluxPressure for p (the gradient that makes the boundary flux the
  * boundary velocity's, set every corrector, :155-163 and IncompressibleFlow.cpp:17-29), 7
  * totalPressure for p (p_value = p0; p0 - |U_b|^2/2 on inflow faces, set at each step start,
- * :325-341).  Patch
+ * :325-341), 8 Robin a phi + b dphi/dn = c (:166-192, coefficients in vlm_flow_ctrl u_robin /
+ * p_robin; it fixes the value when a != 0).  Patch
  * values are uniform; vlm_flow_set_boundary_values sets the fixedValue
  * and inletOutlet values face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
@@ -334,6 +335,10 @@ typedef struct {
                                     0 Gauss linear, 1 leastSquares */
     int32_t grad_p_scheme;       /* IncompressibleFlow::gradPScheme (momentum source, U correction):
                                     0 Gauss linear, 1 leastSquares, 2 GaussSkew (Fvc.h:233-262) */
+    const double* u_robin;       /* boundary type 8, Robin a U + b dU/dn = c (RobinBC, field/BoundaryCondition.h:
+                                    166-192): {a, b} per patch (host array, 2 x patches), c = the patch's
+                                    u_value; NULL when no U patch is Robin */
+    const double* p_robin;       /* the same for p: {a, b} per patch, c = p_value; NULL when none */
 } vlm_flow_ctrl;
 
 typedef struct {

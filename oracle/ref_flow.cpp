@@ -40,8 +40,8 @@ struct RefSolverCtl {
 // value (InletOutletBC on the flow's BCContext), 4 freestream (U: the free-stream velocity; p:
 // freestreamPressure with the p value and the U free-stream velocity of the patch), 5 fixedGradient
 // (the value is the gradient), 6 pressureInletOutletVelocity (U, the value is the tangential velocity)
-// and fixedFluxPressure (p), 7 totalPressure (p, the value is p0); uFace / pFace override the values
-// face by face.
+// and fixedFluxPressure (p), 7 totalPressure (p, the value is p0), 8 Robin a phi + b dphi/dn = value
+// with {a, b} per patch in uRobin / pRobin; uFace / pFace override the values face by face.
 struct RefFlowSpec {
     double nu;
     int steady, divScheme, ddtScheme, nOuter, nCorr, nNonOrthCorr, momentumPredictor;
@@ -61,6 +61,8 @@ struct RefFlowSpec {
     const double* pFace; // optional, 1 per boundary face: values of the fixedValue p faces
     int gradScheme;      // IncompressibleFlow::gradScheme and the mesh default: 0 Gauss, 1 leastSquares
     int gradPScheme;     // IncompressibleFlow::gradPScheme: 0 Gauss, 1 leastSquares, 2 GaussSkew
+    const double* uRobin;  // optional, {a, b} per patch: Robin U patches
+    const double* pRobin;  // optional, {a, b} per patch: Robin p patches
 };
 
 // Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
@@ -173,6 +175,8 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.U().set<FixedGradientBC<Vec3>>(name, uv);
             } else if (sp->uType[q] == 6) {
                 flow.U().set<PressureInletOutletVelocityBC>(name, &flow.context(), uv);
+            } else if (sp->uType[q] == 8) {
+                flow.U().set<RobinBC<Vec3>>(name, sp->uRobin[2 * q], sp->uRobin[2 * q + 1], uv);
             } else {
                 flow.U().zeroGradient(name);
             }
@@ -193,6 +197,8 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
             } else if (sp->pType[q] == 7) {
                 const double p0 = sp->pValue[q];
                 flow.p().set<TotalPressureBC>(name, &flow.context(), [p0](scalar) { return p0; });
+            } else if (sp->pType[q] == 8) {
+                flow.p().set<RobinBC<scalar>>(name, sp->pRobin[2 * q], sp->pRobin[2 * q + 1], sp->pValue[q]);
             } else {
                 flow.p().zeroGradient(name);
             }

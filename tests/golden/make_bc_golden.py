@@ -21,7 +21,11 @@ CFD_REPRODUCIBLE mode:
     (FixedFluxPressureBC, BoundaryCondition.h:155-163; IncompressibleFlow.cpp:17-29), steady SIMPLE,
     6 steps;
   * totalp: the total-pressure inlet of cases/channelInlet/totalPressure.json (TotalPressureBC with
-    PressureInletOutletVelocityBC, BoundaryCondition.h:325-364), steady SIMPLE, 8 steps from rest.
+    PressureInletOutletVelocityBC, BoundaryCondition.h:325-364), steady SIMPLE, 8 steps from rest;
+  * robin / robin_walls / robin_gradient: the inlet-outlet channel with Robin U and p at the outlet
+    (RobinBC, BoundaryCondition.h:166-192), also with Robin (partial-slip-like) U walls, and with a
+    pure-gradient Robin (a = 0) outlet; steady SIMPLE, 6 steps; robin_transient: Euler, nCorr 2,
+    3 steps of dt 0.02.
 Run where the reference sources are present:
     make -C oracle REF=<reference tree> && python tests/golden/make_bc_golden.py
 """
@@ -93,6 +97,13 @@ def main():
     m, case, U0 = cases.channel_total_pressure()
     U, p, phi, hist = R.flow_run(case, 8, U=U0, reproducible=True)
     out.update(totalp_U=U, totalp_p=p, totalp_phi=phi, totalp_hist=hist)
+    for tag, kw, tf, steps, dt in (("robin", {}, dict, 6, 1.0), ("robin_walls", {"wall_ab": (2.0, 0.05)}, dict, 6, 1.0),
+                                   ("robin_gradient", {"u_ab": (0.0, 1.0), "u_c": (0.02, 0.0, 0.0),
+                                                       "p_ab": (0.0, 1.0), "p_c": 0.3}, dict, 6, 1.0),
+                                   ("robin_transient", {}, transient, 3, 0.02)):
+        m, case, U0 = cases.channel_robin(**kw)
+        U, p, phi, hist = R.flow_run(tf(case), steps, dt=dt, U=U0, reproducible=True)
+        out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))
 

@@ -79,3 +79,24 @@ def test_batch_ldu_solve_matches_solo(systems):
         ps = vb.solve_ldu(M, mats[i][0], mats[i][1], None, bs[i], xs, vb.SolverControls("PCG", "GAMG", 0.0, 1e-9, 500))
         assert ps.iterations == perf[i].iterations
         assert np.array_equal(x[B.cell_base[i]:B.cell_base[i + 1]], xs)
+
+
+@pytest.mark.parametrize("precision", ["", "mixed"])
+def test_pressure_corrector_graph_replays_the_direct_run(systems, precision):
+    """The batched pressure corrector runs its first call directly and every later call of the same
+    configuration as one captured graph (the passes' assembly kernels and solve loops in one launch):
+    the replayed calls give the direct call's fields, flux and solver records bit for bit."""
+    meshes = [m for m, _ in systems]
+    B = vb.Mesh.batch(meshes)
+    gamma = cases.batch_face_array(meshes, [np.ones(m["n_faces"]) for m in meshes])
+    div = np.concatenate([d for _, d in systems])
+    ctrl = vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 500, precision=precision)
+    runs = []
+    for _ in range(3):
+        p = np.zeros(B.n_cells)
+        perf, flux = vb.pressure_solve(B, gamma, div, p, ctrl, ref_cell=[0] * len(meshes), n_non_orth=2,
+                                       grad_scheme=1)
+        runs.append((p, flux, [[(q.iterations, q.finalResidual, q.initialResidual) for q in row] for row in perf]))
+    for p, flux, rec in runs[1:]:
+        assert np.array_equal(p, runs[0][0]) and np.array_equal(flux, runs[0][1])
+        assert rec == runs[0][2]

@@ -207,3 +207,35 @@ def test_fixed_gradient_channel_bitwise(gold):
     assert np.array_equal(hist, gold["gradient_hist"][:, :3])
     for k, v in (("U", U), ("p", p), ("phi", phi)):
         assert np.array_equal(v, gold[f"gradient_{k}"]), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag,kw,transient,steps,dt", [
+    ("robin", {}, False, 6, 1.0),
+    ("robin_walls", {"wall_ab": (2.0, 0.05)}, False, 6, 1.0),
+    ("robin_gradient", {"u_ab": (0.0, 1.0), "u_c": (0.02, 0.0, 0.0), "p_ab": (0.0, 1.0), "p_c": 0.3}, False, 6, 1.0),
+    ("robin_transient", {}, True, 3, 0.02),
+])
+def test_robin_channel_bitwise(gold, tag, kw, transient, steps, dt):
+    """Robin a phi + b dphi/dn = c (RobinBC, BoundaryCondition.h:166-192) for U and p at the channel
+    outlet, on the walls as a partial-slip U condition, and as a pure-gradient condition (a = 0, which
+    then fixes neither the value nor the flux): the reference's fields and residual history bit for
+    bit in reproducible mode."""
+    m, case, U0 = cases.channel_robin(**kw)
+    if transient:
+        case = dict(case, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0)
+    U, p, phi, hist = run_case(m, case, U0, steps, dt)
+    assert np.array_equal(hist, gold[f"{tag}_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"{tag}_{k}"]), k
+
+
+@pytest.mark.gpu
+def test_robin_needs_its_coefficients():
+    m, case, U0 = cases.channel_robin()
+    mesh = vb.Mesh.from_arrays(m)
+    for bad in (dict(case, u_robin=None), dict(case, p_robin=None),
+                dict(case, u_robin=np.zeros_like(case["u_robin"]))):
+        with pytest.raises(vb.VlmError) as e:
+            vb.Flow(mesh, bad)
+        assert e.value.name == "BAD_ARG"

@@ -597,6 +597,12 @@ def _flow_ctrl(case: dict) -> _ffi.FlowCtrl:
     c.div_coeff = case.get("div_coeff", 1.0)
     c.grad_scheme = int(case.get("grad_scheme", 0))
     c.grad_p_scheme = int(case.get("grad_p_scheme", 0))
+    c._keep = []
+    for key in ("u_robin", "p_robin"):  # Robin {a, b} per patch (type 8), copied by vlm_flow_create
+        if case.get(key) is not None:
+            a = np.ascontiguousarray(case[key], np.float64).reshape(-1)
+            c._keep.append(a)
+            setattr(c, key, a.ctypes.data)
     repro = bool(case.get("reproducible", False))
     for name, key in (("U", "U"), ("p", "p"), ("p_final", "pFinal")):
         d = case[key]

@@ -294,6 +294,36 @@ def channel_gradient(n=(40, 10, 1), ubulk=1.0, nu=0.05, dpdn=0.6, dudn=(0.05, 0.
     return m, case, U0
 
 
+def channel_robin(n=(40, 10, 1), ubulk=1.0, nu=0.05, u_ab=(1.0, 0.4), p_ab=(1.0, 0.25), u_c=(0.9, 0.0, 0.0),
+                  p_c=0.05, wall_ab=None):
+    """channel_inlet with Robin conditions a phi + b dphi/dn = c (RobinBC, BoundaryCondition.h:166-192):
+    U at the outlet ({a, b} = u_ab, c = u_c) and p at the outlet (p_ab, c = p_c); wall_ab: also a Robin
+    (partial-slip-like) U condition on the walls with c = 0.  Returns (mesh, case, U0)."""
+    m, case, U0 = channel_inlet(n, ubulk, nu)
+    names = list(m["patch_names"])
+    nP = len(names)
+    qo = names.index("xMax")
+    case = dict(case, u_type=case["u_type"].copy(), p_type=case["p_type"].copy(), u_value=case["u_value"].copy(),
+                p_value=case["p_value"].copy())
+    ur = np.zeros(2 * nP)
+    pr = np.zeros(2 * nP)
+    case["u_type"][qo] = 8
+    case["u_value"][3 * qo:3 * qo + 3] = u_c
+    ur[2 * qo:2 * qo + 2] = u_ab
+    case["p_type"][qo] = 8
+    case["p_value"][qo] = p_c
+    pr[2 * qo:2 * qo + 2] = p_ab
+    if wall_ab is not None:
+        for nm in ("yMin", "yMax"):
+            q = names.index(nm)
+            case["u_type"][q] = 8
+            case["u_value"][3 * q:3 * q + 3] = 0.0
+            ur[2 * q:2 * q + 2] = wall_ab
+    case["u_robin"] = ur
+    case["p_robin"] = pr
+    return m, case, U0
+
+
 def channel_flux_pressure(n=(40, 10, 1), ubulk=1.0, nu=0.05, patch="xMin"):
     """channel_inlet with fixedFluxPressure p on `patch` (FixedFluxPressureBC, whose gradient the
     corrector sets so that the boundary flux is the boundary velocity's).  On the inlet

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -45,6 +46,28 @@ struct vlm_mesh {
     vlm::DBuf<double> diag, upper, lower, b, x;
     // pressure-equation work arrays
     vlm::DBuf<double> gamma, su, p, pB, pdiag, pupper, psource, ic, bs, ffc, fd, fb, flux, bcv, grad;
+    // the pressure corrector as one captured graph per configuration (pointers, passes, controls):
+    // its solves write their records here, read back once per call
+    struct PGraph {
+        std::vector<int64_t> key;
+        int runs = 0;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        ~PGraph() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+        }
+    };
+    std::vector<std::unique_ptr<PGraph>> pgraphs;
+    std::vector<int32_t> refsHost;
+    vlm::DBuf<vlm::SysState> pstate;
+    vlm::DBuf<int> pstatus;
+    void* pinned = nullptr;
+    size_t pinnedBytes = 0;
+    ~vlm_mesh() {
+        pgraphs.clear();
+        if (pinned) cudaFreeHost(pinned);
+    }
 };
 
 namespace {
@@ -529,12 +552,53 @@ void ensureWork(vlm_mesh* m) {
     m->grad.resize(3 * nC);
 }
 
-// Device-pointer pressure corrector loop; bcv: device boundary values or null.
+// The corrector passes (IncompressibleFlow.cpp:322-341) on the stream: boundary values, laplacian with
+// the explicit non-orthogonal correction, source, references, fold, solve (deferred: its records go to
+// m->pstate / m->pstatus), and the face flux of the last pass.
+void pressurePasses(vlm_mesh* m, const double* gamma, const double* divPhi, double* p, const vlm::ScalarBC& bc,
+                    int nRefs, double refValue, int nNonOrth, int gradScheme, const vlm_solver_ctrl& ctrl,
+                    const vlm_solver_ctrl& finalCtrl, double* flux) {
+    vlm::DeviceGeom& G = geomOf(m);
+    cudaStream_t s = m->ctx->stream;
+    for (int no = 0; no <= nNonOrth; ++no) {
+        const bool last = no == nNonOrth;
+        G.correctBoundary(p, bc, m->pB.get(), s);
+        bool hasFfc = false;
+        G.laplacian(gamma, p, m->pB.get(), bc, true, gradScheme, m->pdiag.get(), m->pupper.get(), m->psource.get(),
+                    m->ic.get(), m->bs.get(), m->ffc.get(), &hasFfc, s);
+        G.addVolumeSource(m->psource.get(), divPhi, s);
+        if (nRefs > 0) G.setReferences(m->refCells.get(), nRefs, refValue, m->pdiag.get(), m->psource.get(), s);
+        G.fold(m->pdiag.get(), m->psource.get(), m->ic.get(), m->bs.get(), m->fd.get(), m->fb.get(), s);
+        std::vector<vlm_solver_perf> pf;
+        m->batch->deferNextSolve(m->pstate.get() + size_t(no) * m->nsys, m->pstatus.get() + 2 * no);
+        m->batch->solve(m->fd.get(), m->pupper.get(), m->pupper.get(), m->fb.get(), p, last ? finalCtrl : ctrl, pf);
+        if (last && flux) G.flux(m->pupper.get(), p, m->ic.get(), m->bs.get(), hasFfc ? m->ffc.get() : nullptr, flux, s);
+    }
+    G.correctBoundary(p, bc, m->pB.get(), s);
+}
+
+std::vector<int64_t> ctrlKey(const vlm_solver_ctrl& c) {
+    std::vector<int64_t> k;
+    for (const char* t : {c.solver, c.preconditioner, c.smoother, c.precision}) k.push_back(int64_t(std::hash<std::string>()(t)));
+    double d[4] = {c.tolerance, c.relTol, c.innerRelTol, 0.0};
+    for (double v : d) {
+        int64_t b;
+        std::memcpy(&b, &v, sizeof b);
+        k.push_back(b);
+    }
+    for (int v : {int(c.maxIter), int(c.minIter), int(c.nSweeps), int(c.reproducible), int(c.mergeLevels)}) k.push_back(v);
+    return k;
+}
+
+// Device-pointer pressure corrector; bcv: device boundary values or null.  The first call of a
+// configuration runs the passes directly (creating every lazily built resource and the solves'
+// graphs); from the second call on the passes are one captured graph: one launch per call.  The
+// solver records of every pass are read back once at the end.
 void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double* p, const int32_t* bcType,
                   const double* bcv, const int32_t* refCells, double refValue, int nNonOrth, int gradScheme,
                   const vlm_solver_ctrl& ctrl, const vlm_solver_ctrl& finalCtrl, vlm_solver_perf* perf, double* flux) {
-    vlm::DeviceGeom& G = geomOf(m);
     cudaStream_t s = m->ctx->stream;
+    geomOf(m);
     ensureWork(m);
     // global reference cells (-1: none)
     std::vector<int32_t> refs;
@@ -544,26 +608,102 @@ void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double
         VLM_REQUIRE(refCells[q] < cellsOfSystem, VLM_ERR_BAD_ARG, "reference cell out of range");
         refs.push_back(int32_t(m->cellBase[q] + refCells[q]));
     }
-    if (!refs.empty()) m->refCells.upload(refs, s);
+    if (!refs.empty() && refs != m->refsHost) {
+        m->refCells.upload(refs, s);
+        m->refsHost = refs;
+        m->pgraphs.clear();  // the graphs hold the old reference-cell array
+    }
+    const size_t nRec = size_t(nNonOrth + 1) * size_t(m->nsys);
+    if (m->pstate.size() < nRec) {
+        VLM_CUDA(cudaStreamSynchronize(s));
+        m->pgraphs.clear();
+        m->pstate.resize(nRec);
+        m->pstatus.resize(2 * size_t(nNonOrth + 1));
+    }
+    const size_t need = sizeof(vlm::SysState) * nRec + sizeof(int) * 2 * size_t(nNonOrth + 1);
+    if (m->pinnedBytes < need) {
+        if (m->pinned) cudaFreeHost(m->pinned);
+        m->pinned = nullptr;
+        VLM_CUDA(cudaMallocHost(&m->pinned, need));
+        m->pinnedBytes = need;
+    }
     vlm::ScalarBC bc;
     bc.type = bcType;
     bc.value = bcv;
-    for (int no = 0; no <= nNonOrth; ++no) {
-        const bool last = no == nNonOrth;
-        G.correctBoundary(p, bc, m->pB.get(), s);
-        bool hasFfc = false;
-        G.laplacian(gamma, p, m->pB.get(), bc, true, gradScheme, m->pdiag.get(), m->pupper.get(), m->psource.get(),
-                    m->ic.get(), m->bs.get(), m->ffc.get(), &hasFfc, s);
-        G.addVolumeSource(m->psource.get(), divPhi, s);
-        if (!refs.empty())
-            G.setReferences(m->refCells.get(), int(refs.size()), refValue, m->pdiag.get(), m->psource.get(), s);
-        G.fold(m->pdiag.get(), m->psource.get(), m->ic.get(), m->bs.get(), m->fd.get(), m->fb.get(), s);
-        std::vector<vlm_solver_perf> pf;
-        m->batch->solve(m->fd.get(), m->pupper.get(), m->pupper.get(), m->fb.get(), p, last ? finalCtrl : ctrl, pf);
-        if (perf) std::copy(pf.begin(), pf.end(), perf + size_t(no) * m->nsys);
-        if (last && flux) G.flux(m->pupper.get(), p, m->ic.get(), m->bs.get(), hasFfc ? m->ffc.get() : nullptr, flux, s);
+    std::vector<int64_t> key = {int64_t(gamma), int64_t(divPhi), int64_t(p), int64_t(bcType), int64_t(bcv),
+                                int64_t(flux), int64_t(refs.size()), nNonOrth, gradScheme};
+    {
+        int64_t b;
+        std::memcpy(&b, &refValue, sizeof b);
+        key.push_back(b);
+        const auto k1 = ctrlKey(ctrl), k2 = ctrlKey(finalCtrl);
+        key.insert(key.end(), k1.begin(), k1.end());
+        key.insert(key.end(), k2.begin(), k2.end());
     }
-    G.correctBoundary(p, bc, m->pB.get(), s);
+    const char* gv = std::getenv("VLM_GRAPH");
+    const bool graphs = !(gv && gv[0] == '0') && m->batch->embeddable();
+    vlm_mesh::PGraph* g = nullptr;
+    for (auto& q : m->pgraphs)
+        if (q->key == key) g = q.get();
+    if (!g) {
+        m->pgraphs.push_back(std::make_unique<vlm_mesh::PGraph>());
+        g = m->pgraphs.back().get();
+        g->key = key;
+    }
+    const int nRefs = int(refs.size());
+    if (graphs && g->runs >= 1 && !g->exec) {
+        VLM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        m->batch->beginEmbedding();
+        try {
+            pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux);
+        } catch (...) {
+            m->batch->endEmbedding();
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        m->batch->endEmbedding();
+        VLM_CUDA(cudaStreamEndCapture(s, &g->graph));
+        VLM_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    }
+    if (g->exec)
+        VLM_CUDA(cudaGraphLaunch(g->exec, s));
+    else
+        pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux);
+    ++g->runs;
+    // every pass's solver records, read once
+    vlm::SysState* hs = static_cast<vlm::SysState*>(m->pinned);
+    int* hst = reinterpret_cast<int*>(hs + nRec);
+    VLM_CUDA(cudaMemcpyAsync(hs, m->pstate.get(), sizeof(vlm::SysState) * nRec, cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaMemcpyAsync(hst, m->pstatus.get(), sizeof(int) * 2 * size_t(nNonOrth + 1), cudaMemcpyDeviceToHost, s));
+    VLM_CUDA(cudaStreamSynchronize(s));
+    const auto& order = m->batch->plan().order;
+    for (int no = 0; no <= nNonOrth; ++no) {
+        if (hst[2 * no + 1] != 0) {
+            m->batch->clearLevelError();
+            throw vlm::Error(VLM_ERR_TIMEOUT, "level-scheduled sweep: a group barrier wait gave up");
+        }
+        if (hst[2 * no] == VLM_ERR_SINGULAR) throw vlm::Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
+        const vlm_solver_ctrl& c = no == nNonOrth ? finalCtrl : ctrl;
+        if (!perf) continue;
+        for (int b = 0; b < m->nsys; ++b) {
+            const vlm::SysState& q = hs[size_t(no) * m->nsys + b];
+            vlm_solver_perf r = {};
+            r.initialResidual = q.initialResidual;
+            r.finalResidual = q.finalResidual;
+            r.residualSum = q.residualSum;
+            r.normFactor = q.normFactor;
+            r.iterations = q.iterations;
+            r.outerIterations = q.outer;
+            r.status = q.status;
+            // converged() evaluated once more at exit (LinearSolver.cpp:283)
+            r.converged = (r.iterations >= c.minIter) &&
+                          (r.finalResidual < c.tolerance || (c.relTol > 0 && r.finalResidual < c.relTol * r.initialResidual));
+            std::snprintf(r.solver, sizeof(r.solver), "%s", c.solver);
+            perf[size_t(no) * m->nsys + size_t(order[b])] = r;
+        }
+    }
 }
 
 }  // namespace
@@ -646,13 +786,14 @@ vlm_status vlm_pressure_solve_batch(vlm_ctx* ctx, vlm_mesh* m, const double* gam
         setDevice(ctx);
         cudaStream_t s = ctx->stream;
         if (devicePointers) {
-            vlm::DBuf<double> bcvd;
             const int nB = m->nFaces - m->nInternal;
+            const double* bcvd = nullptr;
             if (bcValues && nB > 0) {
-                bcvd.resize(size_t(nB));
-                VLM_CUDA(cudaMemcpyAsync(bcvd.get(), bcValues, sizeof(double) * nB, cudaMemcpyDeviceToDevice, s));
+                m->bcv.resize(size_t(nB));
+                VLM_CUDA(cudaMemcpyAsync(m->bcv.get(), bcValues, sizeof(double) * nB, cudaMemcpyDeviceToDevice, s));
+                bcvd = m->bcv.get();
             }
-            pressureLoop(m, gamma, divPhi, p, bcType, bcvd.get(), refCells, refValue, nNonOrth, gradScheme, *ctrl,
+            pressureLoop(m, gamma, divPhi, p, bcType, bcvd, refCells, refValue, nNonOrth, gradScheme, *ctrl,
                          finalCtrl ? *finalCtrl : *ctrl, perf, flux);
             VLM_CUDA(cudaStreamSynchronize(s));
             return;

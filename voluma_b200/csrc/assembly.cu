@@ -42,19 +42,34 @@ __device__ __forceinline__ BFace lsBoundary(const double* Sf, const double* magS
 
 // The least-squares constraint kind of a boundary face: a value constraint where the patch's
 // condition fixes the value (lsFix per patch when given, else fixedValue), else a normal-gradient one
-__device__ __forceinline__ bool lsValue(const int32_t* bcType, const int32_t* lsFix, int p) {
-    return lsFix ? lsFix[p] != 0 : bcType[p] == 1;
+__device__ __forceinline__ bool lsValue(const int32_t* bcType, const int32_t* lsFix, const double* robin, int p) {
+    return lsFix ? lsFix[p] != 0 : (bcType[p] == 1 || (bcType[p] == 8 && robin[2 * p] != 0.0));
+}
+
+// Robin a phi + b dphi/dn = c (RobinBC, BoundaryCondition.h:166-192): the gradient coefficients
+// gic = dc (b dc / (a + b dc) - 1), gbc = dc (c / (a + b dc)), the face value (c + b dc phi_P) / (a + b dc)
+__device__ __forceinline__ void robinGradient(const double* ab, double c, double dc, double& gic, double& gbc) {
+    const double a = ab[0], b = ab[1];
+    gic = dc * (b * dc / (a + b * dc) - 1.0);
+    gbc = dc * (c / (a + b * dc));
+}
+__device__ __forceinline__ double robinValue(const double* ab, double c, double dc, double psiP) {
+    const double bd = ab[1] * dc;
+    return (c + bd * psiP) / (ab[0] + bd);
 }
 
 // (gic psi_P + gbc) of a gradient-constrained face (Fvc.h:283-284): zeroGradient / symmetry 0, 0;
-// mixed -w dc, w dc v (refGrad 0); fixedGradient 0, g
-__device__ __forceinline__ double lsBoundaryGradient(int t, double psiP, double v, double w, double dc) {
+// mixed -w dc, w dc v (refGrad 0); fixedGradient 0, g; Robin (rob = the patch's {a, b})
+__device__ __forceinline__ double lsBoundaryGradient(int t, double psiP, double v, double w, double dc,
+                                                     const double* rob) {
     double gic = 0.0, gbc = 0.0;
     if (t == 4) {
         gic = -w * dc;
         gbc = w * dc * v + (1.0 - w) * 0.0;
     } else if (t == 5) {
         gbc = v;
+    } else if (t == 8) {
+        robinGradient(rob, v, dc, gic, gbc);
     }
     return gic * psiP + gbc;
 }
@@ -75,7 +90,7 @@ __global__ void k_face_gs(int nF, int nI, const double* __restrict__ gamma, cons
 // (BoundaryCondition.h:147-148: 0, g), zeroGradient (0, 0)
 __global__ void k_lap_boundary(int nB, int nI, const double* __restrict__ gs, const double* __restrict__ ndc,
                                const int32_t* __restrict__ bPatch, const int32_t* __restrict__ bcType,
-                               const double* __restrict__ bcValue, const double* __restrict__ frac,
+                               const double* __restrict__ bcValue, const double* __restrict__ frac, const double* __restrict__ robin,
                                double* __restrict__ ic, double* __restrict__ bs) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
@@ -92,6 +107,8 @@ __global__ void k_lap_boundary(int nB, int nI, const double* __restrict__ gs, co
         gbc = w * dc * v + (1.0 - w) * 0.0;
     } else if (t == 5) {
         gbc = v;
+    } else if (t == 8) {
+        robinGradient(robin + 2 * bPatch[b], v, ndc[f], gic, gbc);
     }
     ic[b] = 0.0 + gs[f] * gic;
     bs[b] = 0.0 - gs[f] * gbc;
@@ -110,7 +127,7 @@ __global__ void k_grad_gauss_skew(int nC, int nI, int nF, const int32_t* __restr
                                   const double* __restrict__ psi, const double* __restrict__ psiB,
                                   const double* __restrict__ gls, const int32_t* __restrict__ bPatch,
                                   const int32_t* __restrict__ bcType, const int32_t* __restrict__ lsFix,
-                                  const double* __restrict__ bcValue, const double* __restrict__ frac, int twoD,
+                                  const double* __restrict__ bcValue, const double* __restrict__ frac, const double* __restrict__ robin, int twoD,
                                   int emptyDir, double* __restrict__ g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
@@ -128,7 +145,7 @@ __global__ void k_grad_gauss_skew(int nC, int nI, int nF, const int32_t* __restr
             phif = (wf * psi[o] + wn * psi[n]) + sk;
         } else {
             const int b = f - nI, p = bPatch[b], o = own[f];
-            if (lsValue(bcType, lsFix, p)) {
+            if (lsValue(bcType, lsFix, robin, p)) {
                 phif = psiB[b];
             } else {
                 const double inv = 1.0 / magSf[f];
@@ -138,7 +155,8 @@ __global__ void k_grad_gauss_skew(int nC, int nI, int nF, const int32_t* __restr
                 const V3 dt{dd.x - n.x * nd, dd.y - n.y * nd, dd.z - n.z * nd};
                 const int t = bcType[p];
                 const double gb =
-                    lsBoundaryGradient(t, psi[o], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f]);
+                    lsBoundaryGradient(t, psi[o], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f],
+                                       robin ? robin + 2 * p : nullptr);
                 const double tg = dt.x * gls[3 * o] + dt.y * gls[3 * o + 1] + dt.z * gls[3 * o + 2];
                 phif = (psi[o] + tg) + gb * nd;
             }
@@ -240,7 +258,7 @@ __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cf
                           const double* __restrict__ ndc, const double* __restrict__ psi,
                           const double* __restrict__ psiB, const int32_t* __restrict__ bPatch,
                           const int32_t* __restrict__ bcType, const int32_t* __restrict__ lsFix,
-                          const double* __restrict__ bcValue, const double* __restrict__ frac, int twoD,
+                          const double* __restrict__ bcValue, const double* __restrict__ frac, const double* __restrict__ robin, int twoD,
                           int emptyDir, double* __restrict__ g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
@@ -251,7 +269,7 @@ __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cf
         if (f < nI)
             v = ld3(d, nF, f);
         else
-            v = lsBoundary(Sf, magSf, d, nF, f, lsValue(bcType, lsFix, bPatch[f - nI])).de;
+            v = lsBoundary(Sf, magSf, d, nF, f, lsValue(bcType, lsFix, robin, bPatch[f - nI])).de;
         const double s = 1.0 / dot3(v, v);
         const double o[9] = {v.x * v.x, v.x * v.y, v.x * v.z, v.y * v.x, v.y * v.y, v.y * v.z,
                              v.z * v.x, v.z * v.y, v.z * v.z};
@@ -282,14 +300,15 @@ __global__ void k_grad_ls(int nC, int nI, int nF, const int32_t* __restrict__ cf
             dp = psi[nei[f]] - psi[own[f]];
         } else {
             const int b = f - nI, p = bPatch[b];
-            const bool value = lsValue(bcType, lsFix, p);
+            const bool value = lsValue(bcType, lsFix, robin, p);
             const BFace bfc = lsBoundary(Sf, magSf, d, nF, f, value);
             v = bfc.de;
             if (value) {
                 dp = psiB[b] - psi[own[f]];
             } else {
                 const int t = bcType[p];
-                dp = lsBoundaryGradient(t, psi[own[f]], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f]) *
+                dp = lsBoundaryGradient(t, psi[own[f]], bcValue ? bcValue[b] : 0.0, t == 4 ? frac[b] : 0.0, ndc[f],
+                                        robin ? robin + 2 * p : nullptr) *
                      bfc.nd;
             }
         }
@@ -397,7 +416,7 @@ __global__ void k_set_references(const int32_t* __restrict__ cells, int n, doubl
 
 __global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, const int32_t* __restrict__ bPatch,
                              const int32_t* __restrict__ bcType, const double* __restrict__ bcValue,
-                             const double* __restrict__ frac, const double* __restrict__ ndc,
+                             const double* __restrict__ frac, const double* __restrict__ robin, const double* __restrict__ ndc,
                              const double* __restrict__ psi, double* __restrict__ psiB) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
@@ -410,6 +429,8 @@ __global__ void k_correct_bc(int nB, int nI, const int32_t* __restrict__ own, co
         psiB[b] = frac[b] * v + (1.0 - frac[b]) * (pP + 0.0 / ndc[nI + b]);
     else if (t == 5)  // FixedGradientBC::evaluate (VolField.h:144-146)
         psiB[b] = pP + v / ndc[nI + b];
+    else if (t == 8)  // RobinBC::evaluate (VolField.h:148-153)
+        psiB[b] = robinValue(robin + 2 * bPatch[b], v, ndc[nI + b], pP);
     else
         psiB[b] = pP;
 }
@@ -505,8 +526,10 @@ void DeviceGeom::uploadBCType(const ScalarBC& bc, cudaStream_t s) {
     std::vector<int32_t> t(bcType_.size(), 0);
     for (size_t p = 0; p < patchStart_.size(); ++p) {
         t[p] = bc.type ? bc.type[p] : 0;
-        VLM_REQUIRE(t[p] == 0 || t[p] == 1 || t[p] == 2 || t[p] == 4 || t[p] == 5, VLM_ERR_BAD_ARG,
-                    "scalar boundary type must be 0 zeroGradient, 1 fixedValue, 2 symmetry, 4 mixed or 5 fixedGradient");
+        VLM_REQUIRE(t[p] == 0 || t[p] == 1 || t[p] == 2 || t[p] == 4 || t[p] == 5 || (t[p] == 8 && bc.robin),
+                    VLM_ERR_BAD_ARG,
+                    "scalar boundary type must be 0 zeroGradient, 1 fixedValue, 2 symmetry, 4 mixed or 5 fixedGradient "
+                    "(8 Robin inside a flow, which carries its coefficients)");
         VLM_REQUIRE(t[p] != 4 || bc.frac != nullptr, VLM_ERR_BAD_ARG, "a mixed boundary needs its value fractions");
     }
     if (t == bcTypeHost_) return;
@@ -519,7 +542,7 @@ void DeviceGeom::correctBoundary(const double* psi, const ScalarBC& bc, double* 
     uploadBCType(bc, s);
     const int nB = nBoundary();
     if (nB > 0)
-        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, bc.frac,
+        k_correct_bc<<<nblk(nB), 256, 0, s>>>(nB, nI_, own_.get(), bPatch_.get(), bcType_.get(), bc.value, bc.frac, bc.robin,
                                               ndc_.get(), psi, psiB), ++launches_;
 }
 
@@ -531,17 +554,17 @@ void DeviceGeom::grad(const double* psi, const double* psiB, const ScalarBC& bc,
         scratchGls_.resize(size_t(3) * nC_);
         k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                             Sf_.get(), magSf_.get(), d_.get(), ndc_.get(), psi, psiB, bPatch_.get(),
-                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_,
+                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, bc.robin, twoD_, emptyDir_,
                                             scratchGls_.get()), ++launches_;
         k_grad_gauss_skew<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                                     w_.get(), Sf_.get(), magSf_.get(), d_.get(), V_.get(), skew_.get(),
                                                     ndc_.get(), psi, psiB, scratchGls_.get(), bPatch_.get(),
-                                                    bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_, out),
+                                                    bcType_.get(), bc.lsFix, bc.value, bc.frac, bc.robin, twoD_, emptyDir_, out),
             ++launches_;
     } else if (scheme == 1)
         k_grad_ls<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
                                             Sf_.get(), magSf_.get(), d_.get(), ndc_.get(), psi, psiB, bPatch_.get(),
-                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, twoD_, emptyDir_, out),
+                                            bcType_.get(), bc.lsFix, bc.value, bc.frac, bc.robin, twoD_, emptyDir_, out),
             ++launches_;
     else
         k_grad_gauss<<<nblk(nC_), 256, 0, s>>>(nC_, nI_, nF_, cfOff_.get(), cfList_.get(), own_.get(), nei_.get(),
@@ -565,7 +588,7 @@ void DeviceGeom::laplacian(const double* gamma, const double* psi, const double*
     const int nB = nBoundary();
     if (nB > 0)
         k_lap_boundary<<<nblk(nB), 256, 0, s>>>(nB, nI_, gs, ndc_.get(), bPatch_.get(), bcType_.get(), bc.value,
-                                                bc.frac, ic, bs), ++launches_;
+                                                bc.frac, bc.robin, ic, bs), ++launches_;
     if (hasFfc) *hasFfc = corr;
 }
 

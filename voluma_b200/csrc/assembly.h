@@ -21,7 +21,8 @@ struct ScalarBC {
     const double* value = nullptr;  // device, nBoundary (may be null: 0)
     const double* frac = nullptr;   // device, nBoundary: value fractions of type-4 faces
     const int32_t* lsFix = nullptr; // device, nPatches: least-squares value constraint (Fvc.h:267-287,
-                                    // bc.fixesValue()); null: the fixedValue patches
+                                    // bc.fixesValue()); null: the fixedValue patches (and Robin with a != 0)
+    const double* robin = nullptr;  // device, nPatches x {a, b}: Robin (type 8) a phi + b dphi/dn = value
 };
 
 class DeviceGeom {

@@ -45,11 +45,18 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
                              const double* __restrict__ uValueB, const double* __restrict__ Sf,
                              const double* __restrict__ magSf, const double* __restrict__ ndc,
                              const double* __restrict__ wIO, const double* __restrict__ phi,
-                             const double* __restrict__ U, double* __restrict__ Ub) {
+                             const double* __restrict__ uRobin, const double* __restrict__ U,
+                             double* __restrict__ Ub) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nB) return;
     const int q = bPatch[b];
     const int c = own[nI + b];
+    if (uType[q] == 8) {
+        // RobinBC<Vec3>::evaluate (VolField.h:148-153): (c + b dc U_P) / (a + b dc)
+        const double bd = uRobin[2 * q + 1] * ndc[nI + b];
+        for (int k = 0; k < 3; ++k) Ub[k * nB + b] = (uValueB[k * nB + b] + bd * U[k * nC + c]) / (uRobin[2 * q] + bd);
+        return;
+    }
     if (uType[q] == 3 || uType[q] == 4) {
         // inletOutlet / freestream = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
         const double w = wIO[b], dc = ndc[nI + b];
@@ -273,7 +280,7 @@ __global__ void k_mom_faces(int nI, int nC, int nF, const int32_t* __restrict__ 
 __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __restrict__ own,
                              const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                              const double* __restrict__ uValueB, const double* __restrict__ wIO,
-                             const double* __restrict__ Sf,
+                             const double* __restrict__ uRobin, const double* __restrict__ Sf,
                              const double* __restrict__ magSf, const double* __restrict__ ndc,
                              const double* __restrict__ phi, double nu, const double* __restrict__ nuF,
                              const double* __restrict__ U, double* __restrict__ ic, double* __restrict__ bs) {
@@ -329,6 +336,14 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
             vbc = g / dc;
             gic = 0.0;
             gbc = g;
+        }
+        if (uType[q] == 8) {  // Robin (BoundaryCondition.h:170-184)
+            const double a = uRobin[2 * q], rb = uRobin[2 * q + 1], cv = uValueB[k * nB + b];
+            const double bd = rb * dc;
+            vic = bd / (a + bd);
+            vbc = cv / (a + rb * dc);
+            gic = dc * (rb * dc / (a + rb * dc) - 1.0);
+            gbc = dc * (cv / (a + rb * dc));
         }
         if (uType[q] == 3 || uType[q] == 4) {
             // inletOutlet / freestream = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
@@ -579,7 +594,7 @@ __device__ __forceinline__ double u_ls_gradient(int t, int k, int b, int f, int 
                                                 const double* __restrict__ Sf, const double* __restrict__ magSf,
                                                 double dc, const double* __restrict__ U,
                                                 const double* __restrict__ uValueB, const double* __restrict__ wIO,
-                                                const double* __restrict__ phi) {
+                                                const double* __restrict__ phi, const double* __restrict__ rob) {
     const double uk = U[size_t(k) * nC + c];
     double gic = 0.0, gbc = 0.0;
     if (t == 2 || t == 6) {
@@ -616,6 +631,10 @@ __device__ __forceinline__ double u_ls_gradient(int t, int k, int b, int f, int 
         gbc = w * dc * uValueB[size_t(k) * nB + b] + (1.0 - w) * 0.0;
     } else if (t == 5) {
         gbc = uValueB[size_t(k) * nB + b];
+    } else if (t == 8) {
+        const double a = rob[0], rb = rob[1], cv = uValueB[size_t(k) * nB + b];
+        gic = dc * (rb * dc / (a + rb * dc) - 1.0);
+        gbc = dc * (cv / (a + rb * dc));
     }
     return gic * uk + gbc;
 }
@@ -632,7 +651,8 @@ __global__ void k_grad_ls_u(int nC, int nI, int nF, int nB, const int32_t* __res
                             const double* __restrict__ Ub, const int32_t* __restrict__ bPatch,
                             const int32_t* __restrict__ uType, const int32_t* __restrict__ uFix,
                             const double* __restrict__ uValueB, const double* __restrict__ wIO,
-                            const double* __restrict__ phi, int twoD, int emptyDir, double* __restrict__ G) {
+                            const double* __restrict__ phi, const double* __restrict__ uRobin, int twoD, int emptyDir,
+                            double* __restrict__ G) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
     // constraint vector of face f; nd set for a gradient constraint
@@ -683,7 +703,8 @@ __global__ void k_grad_ls_u(int nC, int nI, int nF, int nB, const int32_t* __res
         } else {
             const int b = f - nI, t = uType[bPatch[b]];
             for (int j = 0; j < 3; ++j)
-                dp[j] = u_ls_gradient(t, j, b, f, c, nB, nC, nF, Sf, magSf, ndc[f], U, uValueB, wIO, phi) * nd;
+                dp[j] = u_ls_gradient(t, j, b, f, c, nB, nC, nF, Sf, magSf, ndc[f], U, uValueB, wIO, phi,
+                                      uRobin ? uRobin + 2 * bPatch[b] : nullptr) * nd;
         }
         const double wgt = 1.0 / (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         const double dw[3] = {v[0] * wgt, v[1] * wgt, v[2] * wgt};
@@ -723,7 +744,7 @@ __global__ void k_hbya_bval(int nB, int nI, const int32_t* __restrict__ own, con
 // rAUf = interpolate(rAU) (Fvc.h:24-32) and phiHbyA (IncompressibleFlow.cpp:258-281)
 __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __restrict__ own,
                            const int32_t* __restrict__ nei, const double* __restrict__ w, const double* __restrict__ Sf,
-                           const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                           const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uFixesFlux,
                            const double* __restrict__ rAU, const double* __restrict__ HbyA,
                            const double* __restrict__ Ub, const double* __restrict__ skew,
                            const double* __restrict__ gR, const double* __restrict__ gH, double* __restrict__ rAUf,
@@ -753,7 +774,7 @@ __global__ void k_phi_hbya(int nF, int nI, int nB, int nC, const int32_t* __rest
     } else {
         const int b = f - nI;
         rAUf[f] = rAU[o];
-        if (uType[bPatch[b]] == 1 || uType[bPatch[b]] == 2)  // fixesFlux (BoundaryCondition.h:76, 203, 251)
+        if (uFixesFlux[bPatch[b]])  // fixesFlux (BoundaryCondition.h:76, 203, 251)
             phiHbyA[f] = Ub[b] * S[0] + Ub[size_t(nB) + b] * S[1] + Ub[size_t(2) * nB + b] * S[2];
         else
             phiHbyA[f] = HbyA[o] * S[0] + HbyA[size_t(nC) + o] * S[1] + HbyA[size_t(2) * nC + o] * S[2];
@@ -902,25 +923,47 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
             t = 1;
             hasTotalPressure_ = true;
         }
+    // Robin coefficients {a, b} per patch (a phi + b dphi/dn = c); c is the patch value
+    uRobinH_.assign(size_t(2) * std::max(nP, 1), 0.0);
+    pRobinH_.assign(size_t(2) * std::max(nP, 1), 0.0);
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE(uType[q] >= 0 && uType[q] <= 6, VLM_ERR_BAD_ARG, "U boundary type must be 0 to 6");
+        VLM_REQUIRE((uType[q] >= 0 && uType[q] <= 6) || uType[q] == 8, VLM_ERR_BAD_ARG,
+                    "U boundary type must be 0 to 6 or 8");
         if (uType[q] == 3) hasInletOutlet_ = true;
-        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || (pType[q] >= 4 && pType[q] <= 7),
-                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5, 6 or 7");
+        VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || (pType[q] >= 4 && pType[q] <= 8),
+                    VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5, 6, 7 or 8");
+        for (int side = 0; side < 2; ++side) {
+            const bool rob = (side == 0 ? uType[q] : pType[q]) == 8;
+            if (!rob) continue;
+            const double* src = side == 0 ? ctrl_.u_robin : ctrl_.p_robin;
+            VLM_REQUIRE(src != nullptr, VLM_ERR_BAD_ARG, "a Robin boundary needs its {a, b} coefficients (u_robin / p_robin)");
+            const double a = src[2 * q], b = src[2 * q + 1];
+            VLM_REQUIRE(std::isfinite(a) && std::isfinite(b) && (a != 0.0 || b != 0.0), VLM_ERR_BAD_ARG,
+                        "Robin coefficients a and b must be finite and not both zero");
+            std::vector<double>& dst = side == 0 ? uRobinH_ : pRobinH_;
+            dst[2 * q] = a;
+            dst[2 * q + 1] = b;
+        }
         VLM_REQUIRE(pType[q] != 4 || uType[q] == 4, VLM_ERR_BAD_ARG,
                     "freestreamPressure needs the freestream velocity condition on the same patch");
     }
-    // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p
+    // the stored controls do not keep the caller's Robin arrays
+    ctrl_.u_robin = nullptr;
+    ctrl_.p_robin = nullptr;
+    uRobin_.upload(uRobinH_, s_);
+    pRobin_.upload(pRobinH_, s_);
+    // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p (Robin fixes it when a != 0)
     needRef_ = true;
     for (int q = 0; q < nP; ++q)
-        if ((pType[q] == 1 || pType[q] == 7) && G_.patchSize()[q] > 0) needRef_ = false;
+        if ((pType[q] == 1 || pType[q] == 7 || (pType[q] == 8 && pRobinH_[2 * q] != 0.0)) && G_.patchSize()[q] > 0)
+            needRef_ = false;
     for (int k = 0; k < 3; ++k)
         if (!G_.twoD() || k != G_.emptyDir()) solved_.push_back(k);  // Mesh.cpp:642-644
     uType_.upload(uTypeHost_, s_);
     pType_.upload(pTypeHost_, s_);
     // fixesFlux per patch (BoundaryCondition.h:76, 203, 251): fixedValue and symmetry
     std::vector<int32_t> fix(size_t(std::max(nP, 1)), 0);
-    for (int q = 0; q < nP; ++q) fix[q] = uType[q] == 1 || uType[q] == 2;
+    for (int q = 0; q < nP; ++q) fix[q] = uType[q] == 1 || uType[q] == 2 || (uType[q] == 8 && uRobinH_[2 * q] != 0.0);
     uFixesFlux_.upload(fix, s_);
     // per boundary face: U values of fixedValue faces and inlet values of inletOutlet faces (SoA), p values
     const size_t nBb = size_t(std::max(nB_, 1));
@@ -967,8 +1010,8 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
         }
         std::vector<int32_t> uf(size_t(std::max(nP, 1)), 0), pf(size_t(std::max(nP, 1)), 0);
         for (int q = 0; q < nP; ++q) {
-            uf[q] = uType[q] == 1;
-            pf[q] = pType[q] == 1 || pType[q] == 7;
+            uf[q] = uType[q] == 1 || (uType[q] == 8 && uRobinH_[2 * q] != 0.0);
+            pf[q] = pType[q] == 1 || pType[q] == 7 || (pType[q] == 8 && pRobinH_[2 * q] != 0.0);
             for (int i = 0; i < G_.patchSize()[q]; ++i) {
                 const size_t b = size_t(G_.patchStart()[q] - nI_ + i);
                 if (uType[q] == 4 && wu[b] > 0) uf[q] = 1;
@@ -1058,7 +1101,7 @@ void DeviceFlow::boundaryU() {
     if (nB_ > 0)
         k_u_boundary<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
                                                 uValueB_.get(), G_.Sf(), G_.magSf(), G_.ndc(), wIO_.get(),
-                                                phi_.get(), U_.get(), Ub_.get()), ++launches_;
+                                                phi_.get(), uRobin_.get(), U_.get(), Ub_.get()), ++launches_;
 }
 
 void DeviceFlow::ioFractions() {
@@ -1112,6 +1155,7 @@ void DeviceFlow::boundaryP() {
     bc.value = pValueB_.get();
     bc.frac = pFrac_.get();
     bc.lsFix = pLsFix_.get();
+    bc.robin = pRobin_.get();
     G_.correctBoundary(p_.get(), bc, pB_.get(), s_);
 }
 
@@ -1126,7 +1170,8 @@ void DeviceFlow::gradU() {
         k_grad_ls_u<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nF_, nB_, G_.cellFaceOff(), G_.cellFaces(), G_.own(),
                                                G_.nei(), G_.Sf(), G_.magSf(), G_.d(), G_.ndc(), U_.get(), Ub_.get(),
                                                G_.bPatch(), uType_.get(), uLsFix_.get(), uValueB_.get(), wIO_.get(),
-                                               phi_.get(), G_.twoD(), G_.emptyDir(), gU_.get()), ++launches_;
+                                               phi_.get(), uRobin_.get(), G_.twoD(), G_.emptyDir(), gU_.get()),
+            ++launches_;
         return;
     }
     k_grad_tensor<<<nblk(nC_), 256, 0, s_>>>(nC_, nI_, nB_, nF_, G_.cellFaceOff(), G_.cellFaces(), G_.own(), G_.nei(),
@@ -1316,7 +1361,8 @@ void DeviceFlow::assembleMomentum(double aU, bool haveGradU) {
                                               skewLin ? cSkew_.get() : nullptr, ffc_.get()), ++launches_;
     if (nB_ > 0)
         k_mom_bfaces<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, nC_, nF_, G_.own(), G_.bPatch(), uType_.get(),
-                                               uValueB_.get(), wIO_.get(), G_.Sf(), G_.magSf(), G_.ndc(), phi_.get(), ctrl_.nu,
+                                               uValueB_.get(), wIO_.get(), uRobin_.get(), G_.Sf(), G_.magSf(), G_.ndc(),
+                                               phi_.get(), ctrl_.nu,
                                                nuF, U_.get(), ic_.get(), bs_.get()), ++launches_;
     // ddt coefficients (Schemes.h:70-86)
     double kc = 0, kc0 = 0, kc00 = 0;
@@ -1352,6 +1398,7 @@ void DeviceFlow::solveMomentum(vlm_step_info& info, bool first) {
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
     pbc.lsFix = pLsFix_.get();
+    pbc.robin = pRobin_.get();
     G_.grad(p_.get(), pB_.get(), pbc, ctrl_.grad_p_scheme, gP_.get(), s_);
     k_mom_gradp<<<nblk(nC_), 256, 0, s_>>>(nC_, src_.get(), gP_.get(), G_.V(), msrc_.get()), ++launches_;
     const size_t N = size_t(nC_), B = size_t(std::max(nB_, 1));
@@ -1408,6 +1455,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
     pbc.value = pValueB_.get();
     pbc.frac = pFrac_.get();
     pbc.lsFix = pLsFix_.get();
+    pbc.robin = pRobin_.get();
     const bool skewed = G_.skewed();
     if (skewed) {
         // skewed mesh (IncompressibleFlow.cpp:252-275): grad rAU by least squares with zero-gradient
@@ -1427,7 +1475,7 @@ void DeviceFlow::correctPressure(bool finalCorr, bool first, vlm_step_info& info
             ++launches_;
     }
     k_phi_hbya<<<nblk(nF_), 256, 0, s_>>>(nF_, nI_, nB_, nC_, G_.own(), G_.nei(), G_.w(), G_.Sf(), G_.bPatch(),
-                                         uType_.get(), rAU_.get(), HbyA_.get(), Ub_.get(),
+                                         uFixesFlux_.get(), rAU_.get(), HbyA_.get(), Ub_.get(),
                                          skewed ? G_.skew() : nullptr, gR_.get(), gH_.get(), rAUf_.get(),
                                          phiHbyA_.get()), ++launches_;
     if (hasFluxPressure_ && nB_ > 0)

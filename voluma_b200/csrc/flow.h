@@ -128,7 +128,9 @@ private:
     DBuf<double> pTotal_;             // totalPressure p0 per boundary face
     DBuf<int32_t> uLsFix_, pLsFix_;   // per patch: the condition fixes the value (least-squares gradients)
     DBuf<int32_t> pType_;
-    DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry)
+    DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry, Robin a != 0)
+    std::vector<double> uRobinH_, pRobinH_;  // per patch {a, b} of Robin conditions (0 elsewhere)
+    DBuf<double> uRobin_, pRobin_;
     bool hasInletOutlet_ = false;
     // fields (vectors SoA: component k at [k * n])
     DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_, phiOld_, phiOldOld_;
