@@ -311,7 +311,11 @@ vlm_status vlm_exact_sum(vlm_ctx* ctx, const double* values, int64_t n, double* 
  * boundary velocity's, set every corrector, :155-163 and IncompressibleFlow.cpp:17-29), 7
  * totalPressure for p (p_value = p0; p0 - |U_b|^2/2 on inflow faces, set at each step start,
  * :325-341), 8 Robin a phi + b dphi/dn = c (:166-192, coefficients in vlm_flow_ctrl u_robin /
- * p_robin; it fixes the value when a != 0).  Patch
+ * p_robin; it fixes the value when a != 0), 9 advective for U (AdvectiveBC, :389-414 and
+ * field/VolField.h:235-264: the outflow wave equation dU/dt + U_n dU/dn = 0 discretised with the
+ * step's Euler / backward coefficients, a mixed condition with value fraction c / (c + U_n dc) towards
+ * the boundary's own history; zero gradient when steady; optional far-field relaxation in
+ * vlm_flow_ctrl u_advective).  Patch
  * values are uniform; vlm_flow_set_boundary_values sets the fixedValue
  * and inletOutlet values face by face (profiles such as a parabolic inlet).
  * In CFD_REPRODUCIBLE mode (reproducible = 1 in all three solver controls) a step reproduces the
@@ -339,6 +343,9 @@ typedef struct {
                                     166-192): {a, b} per patch (host array, 2 x patches), c = the patch's
                                     u_value; NULL when no U patch is Robin */
     const double* p_robin;       /* the same for p: {a, b} per patch, c = p_value; NULL when none */
+    const double* u_advective;   /* boundary type 9: {lInf, fieldInf x, y, z} per patch (host array, 4 x
+                                    patches); lInf > 0 relaxes towards fieldInf over the length lInf
+                                    (AdvectiveBC's fieldInf / lInf), lInf = 0 none; NULL: no far field */
 } vlm_flow_ctrl;
 
 typedef struct {

@@ -83,7 +83,8 @@ class RefFlowSpec(C.Structure):
                 ("p", RefSolverCtl), ("pFinal", RefSolverCtl), ("pRefCell", C.c_int), ("pRefValue", C.c_double),
                 ("reproducible", C.c_int), ("residualTol", C.c_double), ("divK", C.c_double),
                 ("uFace", C.c_void_p), ("pFace", C.c_void_p), ("gradScheme", C.c_int),
-                ("gradPScheme", C.c_int), ("uRobin", C.c_void_p), ("pRobin", C.c_void_p)]
+                ("gradPScheme", C.c_int), ("uRobin", C.c_void_p), ("pRobin", C.c_void_p),
+                ("uAdv", C.c_void_p)]
 
 
 class RefModelSpec(C.Structure):
@@ -209,7 +210,8 @@ class RefMesh:
         if case.get("p_face") is not None:
             keep.append(np.ascontiguousarray(case["p_face"], np.float64).reshape(-1))
             sp.pFace = _p(keep[-1])
-        for key, field in (("u_robin", "uRobin"), ("p_robin", "pRobin")):  # Robin {a, b} per patch
+        # Robin {a, b} per patch, advective {lInf, fieldInf} per patch
+        for key, field in (("u_robin", "uRobin"), ("p_robin", "pRobin"), ("u_advective", "uAdv")):
             if case.get(key) is not None:
                 keep.append(np.ascontiguousarray(case[key], np.float64).reshape(-1))
                 setattr(sp, field, _p(keep[-1]))

@@ -63,6 +63,7 @@ struct RefFlowSpec {
     int gradPScheme;     // IncompressibleFlow::gradPScheme: 0 Gauss, 1 leastSquares, 2 GaussSkew
     const double* uRobin;  // optional, {a, b} per patch: Robin U patches
     const double* pRobin;  // optional, {a, b} per patch: Robin p patches
+    const double* uAdv;    // optional, {lInf, fieldInf x, y, z} per patch: advective U patches
 };
 
 // Turbulence model and momentum forcing, as fvmFlow.cpp:182-194, 234 sets them from a case file:
@@ -177,6 +178,11 @@ int runFlow(const RefMesh* r, const RefFlowSpec* sp, const RefModelSpec* model, 
                 flow.U().set<PressureInletOutletVelocityBC>(name, &flow.context(), uv);
             } else if (sp->uType[q] == 8) {
                 flow.U().set<RobinBC<Vec3>>(name, sp->uRobin[2 * q], sp->uRobin[2 * q + 1], uv);
+            } else if (sp->uType[q] == 9) {
+                const double* a = sp->uAdv ? sp->uAdv + 4 * q : nullptr;
+                const bool inf = a && a[0] > 0;
+                flow.U().set<AdvectiveBC<Vec3>>(name, &flow.context(), inf, inf ? Vec3{a[1], a[2], a[3]} : Vec3{},
+                                                inf ? a[0] : 0.0);
             } else {
                 flow.U().zeroGradient(name);
             }

@@ -25,7 +25,11 @@ CFD_REPRODUCIBLE mode:
   * robin / robin_walls / robin_gradient: the inlet-outlet channel with Robin U and p at the outlet
     (RobinBC, BoundaryCondition.h:166-192), also with Robin (partial-slip-like) U walls, and with a
     pure-gradient Robin (a = 0) outlet; steady SIMPLE, 6 steps; robin_transient: Euler, nCorr 2,
-    3 steps of dt 0.02.
+    3 steps of dt 0.02;
+  * adv_euler / adv_backward / adv_far / adv_steady: the inlet-outlet channel with an advective U
+    outlet (AdvectiveBC, BoundaryCondition.h:389-414, VolField.h:235-264) and p fixed there: PISO
+    (nCorr 2) Euler 4 steps and backward 5 steps of dt 0.02, backward with the far-field relaxation
+    (lInf 0.5 towards (0.8, 0.05, 0)), and steady SIMPLE 3 steps (zero gradient).
 Run where the reference sources are present:
     make -C oracle REF=<reference tree> && python tests/golden/make_bc_golden.py
 """
@@ -60,6 +64,19 @@ INLET = {
     "inlet_transient": (0.5, lambda c: dict(c, steady=False, ddt_scheme=1, n_corr=2, alpha_u=1.0, alpha_p=1.0), 3,
                         0.02),
 }
+
+
+# tag, steps, dt of the advective-outlet channels (advective_case builds them)
+ADVECTIVE = (("adv_euler", 4, 0.02), ("adv_backward", 5, 0.02), ("adv_far", 5, 0.02), ("adv_steady", 3, 1.0))
+
+
+def advective_case(tag):
+    kw = {"adv_euler": dict(ddt_scheme=1), "adv_backward": dict(ddt_scheme=2),
+          "adv_far": dict(ddt_scheme=2, far_field=(0.5, (0.8, 0.05, 0.0))), "adv_steady": dict(ddt_scheme=0)}[tag]
+    m, case, U0 = cases.channel_advective(**kw)
+    if tag == "adv_steady":
+        case = dict(case, steady=True, n_corr=1, alpha_u=0.7, alpha_p=0.3)
+    return m, case, U0
 
 
 def main():
@@ -103,6 +120,10 @@ def main():
                                    ("robin_transient", {}, transient, 3, 0.02)):
         m, case, U0 = cases.channel_robin(**kw)
         U, p, phi, hist = R.flow_run(tf(case), steps, dt=dt, U=U0, reproducible=True)
+        out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
+    for tag, steps, dt in ADVECTIVE:
+        m, case, U0 = advective_case(tag)
+        U, p, phi, hist = R.flow_run(case, steps, dt=dt, U=U0, reproducible=True)
         out.update({f"{tag}_U": U, f"{tag}_p": p, f"{tag}_phi": phi, f"{tag}_hist": hist})
     np.savez_compressed(os.path.join(HERE, "flow_bc_cases.npz"), **out)
     print(sorted(out))

@@ -6,6 +6,9 @@ oracle/ref_flow.cpp), in CFD_REPRODUCIBLE mode:
                                PIMPLE backward) after 3 steps: U, U_0, U_00, p, phi, phi_0, phi_00, nut,
                                state.txt
   tests/golden/restart_cav/    the 16 x 16 lid cavity (steady SIMPLE) after 4 steps: U, p, phi, state.txt
+  tests/golden/restart_adv/    the 40 x 10 channel with an advective U outlet (PISO backward, dt 0.02)
+                               after 3 steps: U, U_0, U_00, p, phi, phi_0, phi_00, state.txt (the
+                               outlet condition's own history is not part of a restart)
   tests/golden/flow_restart_cases.npz   U, p, phi (and gradP) of the reference continuing 2 steps from
                                each directory
 
@@ -47,8 +50,16 @@ def main():
     R.flow_run(case, 4, reproducible=True, write_restart=d)
     U, p, phi, _, _, _ = R.flow_run(case, 2, reproducible=True, read_restart=d)
     out.update(cav_U=U, cav_p=p, cav_phi=phi)
+    # advective outlet: restart::read gives a fresh condition (markRestarted, IncompressibleFlow.cpp:41-47)
+    m, case, U0 = cases.channel_advective(ddt_scheme=2)
+    R = ref.RefMesh((40, 10, 1), hi=(4.0, 1.0, 0.1), two_d=True)
+    d = os.path.join(HERE, "restart_adv")
+    shutil.rmtree(d, ignore_errors=True)
+    R.flow_run(case, 3, dt=0.02, U=U0, reproducible=True, write_restart=d)
+    U, p, phi, _, _, _ = R.flow_run(case, 2, dt=0.02, U=U0, reproducible=True, read_restart=d)
+    out.update(adv_U=U, adv_p=p, adv_phi=phi)
     np.savez_compressed(os.path.join(HERE, "flow_restart_cases.npz"), **out)
-    for name in ("restart_chan", "restart_cav"):
+    for name in ("restart_chan", "restart_cav", "restart_adv"):
         print(name, sorted(os.listdir(os.path.join(HERE, name))))
 
 

@@ -239,3 +239,46 @@ def test_robin_needs_its_coefficients():
         with pytest.raises(vb.VlmError) as e:
             vb.Flow(mesh, bad)
         assert e.value.name == "BAD_ARG"
+
+
+# tag, steps, dt, channel_advective arguments, steady (the cases of flow_bc_cases.npz)
+ADVECTIVE = [
+    ("adv_euler", 4, 0.02, dict(ddt_scheme=1), False),
+    ("adv_backward", 5, 0.02, dict(ddt_scheme=2), False),
+    ("adv_far", 5, 0.02, dict(ddt_scheme=2, far_field=(0.5, (0.8, 0.05, 0.0))), False),
+    ("adv_steady", 3, 1.0, dict(ddt_scheme=0), True),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag,steps,dt,kw,steady", ADVECTIVE)
+def test_advective_outlet_bitwise(gold, tag, steps, dt, kw, steady):
+    """Advective U outlet (AdvectiveBC, BoundaryCondition.h:389-414; VolField.h:235-264): the
+    condition's own boundary history, shifted at each new time index, Euler and backward
+    coefficients (backward from the third level on), the far-field relaxation, and the steady zero
+    gradient; the later steps replay the captured step graph.  The reference's fields and residual
+    history bit for bit."""
+    m, case, U0 = cases.channel_advective(**kw)
+    if steady:
+        case = dict(case, steady=True, n_corr=1, alpha_u=0.7, alpha_p=0.3)
+    U, p, phi, hist = run_case(m, case, U0, steps, dt)
+    assert np.array_equal(hist, gold[f"{tag}_hist"][:, :3])
+    for k, v in (("U", U), ("p", p), ("phi", phi)):
+        assert np.array_equal(v, gold[f"{tag}_{k}"]), k
+
+
+def test_golden_advective_cases_differ():
+    # the far field and the time scheme change the outlet's fields
+    z = np.load(GOLD)
+    assert not np.array_equal(z["adv_far_U"], z["adv_backward_U"])
+    assert not np.array_equal(z["adv_euler_U"], z["inlet_transient_U"])
+    names_ok = [k for k in z.files if k.startswith("adv_")]
+    assert len(names_ok) == 16
+
+
+@pytest.mark.gpu
+def test_advective_far_field_checked():
+    m, case, U0 = cases.channel_advective(far_field=(-1.0, (1.0, 0.0, 0.0)))
+    with pytest.raises(vb.VlmError) as e:
+        vb.Flow(vb.Mesh.from_arrays(m), case)
+    assert e.value.name == "BAD_ARG"

@@ -7,7 +7,8 @@ restart::write / restart::read (io/Restart.cpp), fixtures from tests/golden/make
   bit for bit;
 * write -> read -> continue equals the uninterrupted run; a directory of another mesh is refused.
 All in CFD_REPRODUCIBLE mode: the graded LES channel with mean-velocity forcing (transient, two old
-time levels, nu_t) and the steady lid cavity."""
+time levels, nu_t), the steady lid cavity, and the channel with an advective outlet (whose
+condition restarts without its history, as the reference's markRestarted gives it)."""
 import os
 
 import numpy as np
@@ -45,7 +46,15 @@ def cavity_flow():
     return fl, 1.0
 
 
-FLOWS = {"chan": (channel_flow, 3), "cav": (cavity_flow, 4)}
+def advective_flow():
+    m, case, U0 = cases.channel_advective(ddt_scheme=2)
+    case["reproducible"] = True
+    fl = vb.Flow(vb.Mesh.from_arrays(m), case)
+    fl.set_state(U0, None)
+    return fl, 0.02
+
+
+FLOWS = {"chan": (channel_flow, 3), "cav": (cavity_flow, 4), "adv": (advective_flow, 3)}
 
 
 def same_files(a, b):
@@ -56,7 +65,7 @@ def same_files(a, b):
             assert fa.read() == fb.read(), n
 
 
-@pytest.mark.parametrize("case", ["chan", "cav"])
+@pytest.mark.parametrize("case", ["chan", "cav", "adv"])
 def test_write_matches_reference_bytes(tmp_path, case):
     make, steps = FLOWS[case]
     fl, dt = make()
@@ -67,7 +76,7 @@ def test_write_matches_reference_bytes(tmp_path, case):
     same_files(tmp_path / "r", os.path.join(HERE, f"restart_{case}"))
 
 
-@pytest.mark.parametrize("case", ["chan", "cav"])
+@pytest.mark.parametrize("case", ["chan", "cav", "adv"])
 def test_continue_from_reference_restart(gold, case):
     make, _ = FLOWS[case]
     fl, dt = make()

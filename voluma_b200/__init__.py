@@ -598,7 +598,8 @@ def _flow_ctrl(case: dict) -> _ffi.FlowCtrl:
     c.grad_scheme = int(case.get("grad_scheme", 0))
     c.grad_p_scheme = int(case.get("grad_p_scheme", 0))
     c._keep = []
-    for key in ("u_robin", "p_robin"):  # Robin {a, b} per patch (type 8), copied by vlm_flow_create
+    # Robin {a, b} per patch (type 8), advective {lInf, fieldInf} per patch (type 9); copied by vlm_flow_create
+    for key in ("u_robin", "p_robin", "u_advective"):
         if case.get(key) is not None:
             a = np.ascontiguousarray(case[key], np.float64).reshape(-1)
             c._keep.append(a)

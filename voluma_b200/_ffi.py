@@ -59,7 +59,8 @@ class FlowCtrl(C.Structure):
                 ("momentum_predictor", C.c_int32), ("alpha_u", C.c_double), ("alpha_p", C.c_double),
                 ("p_ref_cell", C.c_int32), ("p_ref_value", C.c_double), ("U", SolverCtrl), ("p", SolverCtrl),
                 ("p_final", SolverCtrl), ("div_coeff", C.c_double), ("grad_scheme", C.c_int32),
-                ("grad_p_scheme", C.c_int32), ("u_robin", C.c_void_p), ("p_robin", C.c_void_p)]
+                ("grad_p_scheme", C.c_int32), ("u_robin", C.c_void_p), ("p_robin", C.c_void_p),
+                ("u_advective", C.c_void_p)]
 
 
 class StepInfo(C.Structure):

@@ -324,6 +324,26 @@ def channel_robin(n=(40, 10, 1), ubulk=1.0, nu=0.05, u_ab=(1.0, 0.4), p_ab=(1.0,
     return m, case, U0
 
 
+def channel_advective(n=(40, 10, 1), ubulk=1.0, nu=0.05, ddt_scheme=2, far_field=None):
+    """channel_inlet, transient (PISO, nCorr 2, ddt_scheme 1 Euler or 2 backward), with an advective
+    U outlet (AdvectiveBC, BoundaryCondition.h:389-414; VolField.h:235-264) and p fixed at 0 there;
+    far_field = (lInf, (Ux, Uy, Uz)) adds the relaxation towards that far-field velocity.  Returns
+    (mesh, case, U0)."""
+    m, case, U0 = channel_inlet(n, ubulk, nu)
+    names = list(m["patch_names"])
+    nP = len(names)
+    qo = names.index("xMax")
+    case = dict(case, u_type=case["u_type"].copy(), steady=False, ddt_scheme=ddt_scheme, n_corr=2, alpha_u=1.0,
+                alpha_p=1.0)
+    case["u_type"][qo] = 9
+    if far_field is not None:
+        adv = np.zeros(4 * nP)
+        adv[4 * qo] = far_field[0]
+        adv[4 * qo + 1:4 * qo + 4] = far_field[1]
+        case["u_advective"] = adv
+    return m, case, U0
+
+
 def channel_flux_pressure(n=(40, 10, 1), ubulk=1.0, nu=0.05, patch="xMin"):
     """channel_inlet with fixedFluxPressure p on `patch` (FixedFluxPressureBC, whose gradient the
     corrector sets so that the boundary flux is the boundary velocity's).  On the inlet

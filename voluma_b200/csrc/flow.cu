@@ -57,8 +57,8 @@ __global__ void k_u_boundary(int nB, int nI, int nC, int nF, const int32_t* __re
         for (int k = 0; k < 3; ++k) Ub[k * nB + b] = (uValueB[k * nB + b] + bd * U[k * nC + c]) / (uRobin[2 * q] + bd);
         return;
     }
-    if (uType[q] == 3 || uType[q] == 4) {
-        // inletOutlet / freestream = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
+    if (uType[q] == 3 || uType[q] == 4 || uType[q] == 9) {
+        // inletOutlet / freestream / advective = mixed with refGrad 0 (MixedBC::evaluate, BoundaryCondition.h:232-235)
         const double w = wIO[b], dc = ndc[nI + b];
         for (int k = 0; k < 3; ++k)
             Ub[k * nB + b] = w * uValueB[k * nB + b] + (1.0 - w) * (U[k * nC + c] + 0.0 / dc);
@@ -128,6 +128,53 @@ __global__ void k_io_fraction(int nB, int nI, const int32_t* __restrict__ bPatch
                               const double* __restrict__ phi, double* __restrict__ wIO) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < nB && uType[bPatch[b]] == 3) wIO[b] = phi && phi[nI + b] < 0 ? 1.0 : 0.0;
+}
+
+// advective outflow (AdvectiveBC::update, VolField.h:235-264).  On a new time
+// index the current boundary values become the old level (and the old one the old-old level when
+// shiftOldOld); fromZero takes zeros instead (a freshly constructed field, whose boundary values are 0).
+// Then w = c / (c + max(phi/|S|, 0) dc) and refValue = (c0 U_b^0 - c00 U_b^00) / c with the step's ddt
+// coefficients; phi == nullptr is a zero flux.  The face evaluates as a mixed condition with refGrad 0.
+__global__ void k_adv_update(int nB, int nI, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                             const double* __restrict__ phi, const double* __restrict__ magSf,
+                             const double* __restrict__ ndc, const double* __restrict__ Ub, double* __restrict__ old,
+                             double* __restrict__ oldOld, const double* __restrict__ adv, int shift,
+                             int shiftOldOld, int fromZero, double c, double c0, double c00,
+                             double* __restrict__ wIO, double* __restrict__ uValueB) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nB || uType[bPatch[b]] != 9) return;
+    if (shift)
+        for (int k = 0; k < 3; ++k) {
+            const size_t e = size_t(k) * nB + b;
+            if (shiftOldOld) oldOld[e] = old[e];
+            old[e] = fromZero ? 0.0 : Ub[e];
+        }
+    const int f = nI + b;
+    const double un = phi ? fmax(phi[f] / magSf[f], 0.0) : 0.0;
+    const double a = un * ndc[f];
+    const double* inf = adv + 4 * bPatch[b];
+    if (inf[0] > 0.0) {
+        // relaxation towards the far field: + (U_n / lInf)(U_b - fieldInf)
+        const double kk = un / inf[0];
+        for (int k = 0; k < 3; ++k) {
+            const size_t e = size_t(k) * nB + b;
+            uValueB[e] = ((c0 * old[e] - c00 * oldOld[e]) + kk * inf[1 + k]) / (c + kk);
+        }
+        wIO[b] = (c + kk) / (c + a + kk);
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            const size_t e = size_t(k) * nB + b;
+            uValueB[e] = (c0 * old[e] - c00 * oldOld[e]) / c;
+        }
+        wIO[b] = c / (c + a);
+    }
+}
+
+// steady (or no positive time step): zero gradient
+__global__ void k_adv_steady(int nB, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
+                             double* __restrict__ wIO) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nB && uType[bPatch[b]] == 9) wIO[b] = 0.0;
 }
 
 // ---------------------------------------------------------------- fvc::grad of U (Gauss linear)
@@ -345,8 +392,8 @@ __global__ void k_mom_bfaces(int nB, int nI, int nC, int nF, const int32_t* __re
             gic = dc * (rb * dc / (a + rb * dc) - 1.0);
             gbc = dc * (cv / (a + rb * dc));
         }
-        if (uType[q] == 3 || uType[q] == 4) {
-            // inletOutlet / freestream = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
+        if (uType[q] == 3 || uType[q] == 4 || uType[q] == 9) {
+            // inletOutlet / freestream / advective = mixed (MixedBC, BoundaryCondition.h:236-243) with refGrad 0
             const double w = wIO[b], rv = uValueB[k * nB + b], rg = 0.0;
             vic = 1.0 - w;
             vbc = w * rv + (1.0 - w) * (rg / dc);
@@ -625,7 +672,7 @@ __device__ __forceinline__ double u_ls_gradient(int t, int k, int b, int f, int 
             gic = dc * (vic - 1.0);
             gbc = dc * vbc;
         }
-    } else if (t == 3 || t == 4) {
+    } else if (t == 3 || t == 4 || t == 9) {
         const double w = wIO[b];
         gic = -w * dc;
         gbc = w * dc * uValueB[size_t(k) * nB + b] + (1.0 - w) * 0.0;
@@ -720,14 +767,15 @@ __global__ void k_grad_ls_u(int nC, int nI, int nF, int nB, const int32_t* __res
 
 __global__ void k_io_patch_reset(int nP, const int32_t* __restrict__ uType, int32_t* __restrict__ uFix) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < nP && uType[q] == 3) uFix[q] = 0;
+    if (q < nP && (uType[q] == 3 || uType[q] == 9)) uFix[q] = 0;
 }
 
-// inletOutlet patches fix U for the least-squares gradient while any face has inflow
+// inletOutlet and advective patches fix U for the least-squares gradient while any face has a positive
+// value fraction (MixedBC::fixesValue, BoundaryCondition.h:246-250): inflow, or a transient advective step
 __global__ void k_io_patch_fix(int nB, const int32_t* __restrict__ bPatch, const int32_t* __restrict__ uType,
                                const double* __restrict__ wIO, int32_t* __restrict__ uFix) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < nB && uType[bPatch[b]] == 3 && wIO[b] > 0) uFix[bPatch[b]] = 1;
+    if (b < nB && (uType[bPatch[b]] == 3 || uType[bPatch[b]] == 9) && wIO[b] > 0) uFix[bPatch[b]] = 1;
 }
 
 // HbyA boundary values of the skew-corrected Rhie-Chow flux on fixes-flux faces: U_b + rAU_P grad p_P
@@ -927,9 +975,18 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     uRobinH_.assign(size_t(2) * std::max(nP, 1), 0.0);
     pRobinH_.assign(size_t(2) * std::max(nP, 1), 0.0);
     for (int q = 0; q < nP; ++q) {
-        VLM_REQUIRE((uType[q] >= 0 && uType[q] <= 6) || uType[q] == 8, VLM_ERR_BAD_ARG,
-                    "U boundary type must be 0 to 6 or 8");
+        VLM_REQUIRE((uType[q] >= 0 && uType[q] <= 6) || uType[q] == 8 || uType[q] == 9, VLM_ERR_BAD_ARG,
+                    "U boundary type must be 0 to 6, 8 or 9");
         if (uType[q] == 3) hasInletOutlet_ = true;
+        if (uType[q] == 9) {
+            hasAdvective_ = true;
+            if (ctrl_.u_advective) {
+                const double* a = ctrl_.u_advective + 4 * q;
+                VLM_REQUIRE(std::isfinite(a[0]) && a[0] >= 0.0 && std::isfinite(a[1]) && std::isfinite(a[2]) &&
+                                std::isfinite(a[3]),
+                            VLM_ERR_BAD_ARG, "advective far field: lInf must be finite and not negative");
+            }
+        }
         VLM_REQUIRE(pType[q] == 0 || pType[q] == 1 || pType[q] == 2 || (pType[q] >= 4 && pType[q] <= 8),
                     VLM_ERR_BAD_ARG, "p boundary type must be 0, 1, 2, 4, 5, 6, 7 or 8");
         for (int side = 0; side < 2; ++side) {
@@ -947,9 +1004,17 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
         VLM_REQUIRE(pType[q] != 4 || uType[q] == 4, VLM_ERR_BAD_ARG,
                     "freestreamPressure needs the freestream velocity condition on the same patch");
     }
-    // the stored controls do not keep the caller's Robin arrays
+    if (hasAdvective_) {
+        std::vector<double> adv(size_t(4) * std::max(nP, 1), 0.0);
+        for (int q = 0; q < nP; ++q)
+            if (uType[q] == 9 && ctrl_.u_advective)
+                for (int k = 0; k < 4; ++k) adv[4 * q + k] = ctrl_.u_advective[4 * q + k];
+        uAdv_.upload(adv, s_);
+    }
+    // the stored controls do not keep the caller's Robin and advective arrays
     ctrl_.u_robin = nullptr;
     ctrl_.p_robin = nullptr;
+    ctrl_.u_advective = nullptr;
     uRobin_.upload(uRobinH_, s_);
     pRobin_.upload(pRobinH_, s_);
     // pressureNeedsReference (IncompressibleFlow.cpp:109-113): no patch fixes p (Robin fixes it when a != 0)
@@ -979,6 +1044,12 @@ DeviceFlow::DeviceFlow(DeviceBatch& batch, DeviceGeom& geom, const vlm_flow_ctrl
     if (hasTotalPressure_) pTotal_.upload(pv, s_);  // p0 per face
     wIO_.resize(nBb);
     wIO_.zero(s_);
+    if (hasAdvective_) {
+        advOld_.resize(3 * nBb);
+        advOld_.zero(s_);
+        advOldOld_.resize(3 * nBb);
+        advOldOld_.zero(s_);
+    }
     pFrac_.resize(nBb);
     pFrac_.zero(s_);
     bool freestream = false;
@@ -1104,6 +1175,45 @@ void DeviceFlow::boundaryU() {
                                                 phi_.get(), uRobin_.get(), U_.get(), Ub_.get()), ++launches_;
 }
 
+void DeviceFlow::advectiveAdvance(int ddt, bool fromZero, bool noFlux) {
+    adv_ = AdvStep{};
+    if (!hasAdvective_ || nB_ == 0) return;
+    adv_.on = true;
+    if (ddt == 0 || !(dt_ > 0)) return;  // w = 0
+    adv_.fromZero = fromZero;
+    adv_.noFlux = noFlux;
+    if (timeIndex_ != advLastTI_) {
+        adv_.shift = true;
+        adv_.shiftOldOld = advN_ >= 1;
+        advN_ = std::min(advN_ + 1, 2);
+        advLastTI_ = timeIndex_;
+    }
+    // ddtCoeffs (Schemes.h:71-86) with the condition's own old-old level
+    const double rDt = 1.0 / dt_;
+    if (ddt == 2 && advN_ >= 2 && dt0_ > 0) {
+        const double ct = 1.0 + dt_ / (dt_ + dt0_);
+        const double ct00 = dt_ * dt_ / (dt0_ * (dt_ + dt0_));
+        adv_.c = ct * rDt;
+        adv_.c0 = (ct + ct00) * rDt;
+        adv_.c00 = ct00 * rDt;
+    } else {
+        adv_.c = adv_.c0 = rDt;
+    }
+}
+
+void DeviceFlow::advectiveApply() {
+    if (!adv_.on) return;
+    if (adv_.c == 0.0) {
+        k_adv_steady<<<nblk(nB_), 256, 0, s_>>>(nB_, G_.bPatch(), uType_.get(), wIO_.get()), ++launches_;
+        return;
+    }
+    k_adv_update<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), adv_.noFlux ? nullptr : phi_.get(),
+                                            G_.magSf(), G_.ndc(), Ub_.get(), advOld_.get(), advOldOld_.get(),
+                                            uAdv_.get(), adv_.shift ? 1 : 0, adv_.shiftOldOld ? 1 : 0, adv_.fromZero ? 1 : 0,
+                                            adv_.c, adv_.c0, adv_.c00, wIO_.get(), uValueB_.get()),
+        ++launches_;
+}
+
 void DeviceFlow::ioFractions() {
     if (hasInletOutlet_ && nB_ > 0)
         k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), phi_.get(), wIO_.get()),
@@ -1161,7 +1271,7 @@ void DeviceFlow::boundaryP() {
 
 void DeviceFlow::gradU() {
     if (ctrl_.grad_scheme == 1) {
-        if (hasInletOutlet_ && nB_ > 0) {
+        if ((hasInletOutlet_ || hasAdvective_) && nB_ > 0) {
             k_io_patch_reset<<<nblk(G_.nPatches()), 256, 0, s_>>>(G_.nPatches(), uType_.get(), uLsFix_.get()),
                 ++launches_;
             k_io_patch_fix<<<nblk(nB_), 256, 0, s_>>>(nB_, G_.bPatch(), uType_.get(), wIO_.get(), uLsFix_.get()),
@@ -1191,6 +1301,12 @@ void DeviceFlow::setState(const double* U, const double* p) {
     if (hasInletOutlet_ && nB_ > 0)
         k_io_fraction<<<nblk(nB_), 256, 0, s_>>>(nB_, nI_, G_.bPatch(), uType_.get(), nullptr, wIO_.get()),
             ++launches_;
+    // advective faces: a fresh condition (no history) on a fresh field (boundary values 0), updated
+    // with the context's initial Euler scheme and no flux
+    advN_ = 0;
+    advLastTI_ = -1;
+    advectiveAdvance(1, true, true);
+    advectiveApply();
     totalPressure(true);
     boundaryU();
     boundaryP();
@@ -1337,6 +1453,11 @@ bool DeviceFlow::readRestart(const std::string& dir) {
         VLM_CUDA(cudaStreamSynchronize(s_));
     }
     ioFractions();  // markRestarted: updateBCs with the restart's flux
+    // a fresh advective condition on a fresh field, with the context's initial Euler scheme
+    advN_ = 0;
+    advLastTI_ = -1;
+    advectiveAdvance(1, true, false);
+    advectiveApply();
     totalPressure(false);
     boundaryU();
     boundaryP();
@@ -1531,6 +1652,7 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
         VLM_CUDA(cudaMemcpyAsync(phiOld_.get(), phi_.get(), sizeof(double) * nF_, cudaMemcpyDeviceToDevice, s_));
     }
     ioFractions();
+    advectiveApply();
     totalPressure(false);  // p_.updateBCs reads U's boundary values of the previous step
     boundaryU();
     boundaryP();
@@ -1562,7 +1684,8 @@ void DeviceFlow::stepWork(bool copyOld, bool copyOldOld) {
 // One step's device work captured into a graph (the solves' iteration loops embedded as conditional
 // nodes); returns null when the capture is not possible, and the step then runs directly.
 DeviceFlow::StepGraph* DeviceFlow::stepGraph(bool copyOld, bool copyOldOld) {
-    const StepKey key{ctrl_.steady != 0, dt_, dt0_, copyOld, copyOldOld};
+    const StepKey key{ctrl_.steady != 0, dt_,         dt0_,     copyOld,   copyOldOld, adv_.shift,
+                      adv_.shiftOldOld,  adv_.c, adv_.c0, adv_.c00};
     for (auto& g : stepGraphs_)
         if (g->key == key) return g.get();
     auto g = std::make_unique<StepGraph>();
@@ -1621,6 +1744,7 @@ vlm_step_info DeviceFlow::step(double dt) {
         time_ += 1.0;
         ++timeIndex_;
     }
+    advectiveAdvance(steady ? 0 : ctrl_.ddt_scheme, false, false);
     // The first step runs directly (it creates every lazily built resource); later steps replay one
     // captured graph per (steady, dt, old-time-level) configuration: one launch per step.
     StepGraph* sg = nullptr;

@@ -86,9 +86,12 @@ private:
         bool steady;
         double dt, dt0;
         bool copyOld, copyOldOld;
+        bool advShift, advShiftOldOld;
+        double advC, advC0, advC00;
         bool operator==(const StepKey& o) const {
             return steady == o.steady && dt == o.dt && dt0 == o.dt0 && copyOld == o.copyOld &&
-                   copyOldOld == o.copyOldOld;
+                   copyOldOld == o.copyOldOld && advShift == o.advShift && advShiftOldOld == o.advShiftOldOld &&
+                   advC == o.advC && advC0 == o.advC0 && advC00 == o.advC00;
         }
     };
     struct StepGraph {
@@ -131,6 +134,20 @@ private:
     DBuf<int32_t> uFixesFlux_;        // per patch: the U condition fixes the flux (fixedValue, symmetry, Robin a != 0)
     std::vector<double> uRobinH_, pRobinH_;  // per patch {a, b} of Robin conditions (0 elsewhere)
     DBuf<double> uRobin_, pRobin_;
+    // advective outflow (type 9): the condition keeps its own history of boundary values, advanced
+    // when the time index changes (AdvectiveBC::update, VolField.h:235-264)
+    bool hasAdvective_ = false;
+    DBuf<double> advOld_, advOldOld_;  // boundary values at the old / old-old time levels (3 x nB)
+    DBuf<double> uAdv_;                // per patch {lInf, fieldInf x, y, z}; lInf 0: no far field
+    int advN_ = 0, advLastTI_ = -1;    // levels held (0..2) and the time index of the last shift
+    struct AdvStep {
+        bool on = false, shift = false, shiftOldOld = false, fromZero = false, noFlux = false;
+        double c = 0, c0 = 0, c00 = 0;
+    } adv_;
+    // one update of the condition's state on the host (ddt: 0 steady, 1 Euler, 2 backward); the
+    // launch that applies it is advectiveApply
+    void advectiveAdvance(int ddt, bool fromZero, bool noFlux);
+    void advectiveApply();
     bool hasInletOutlet_ = false;
     // fields (vectors SoA: component k at [k * n])
     DBuf<double> U_, Ub_, p_, pB_, phi_, U0_, U00_, phiOld_, phiOldOld_;

@@ -35,7 +35,7 @@ struct Request {
     int64_t id = 0;
     int32_t nCells = 0, nInternal = 0, nFaces = 0, nPatches = 0, twoD = 0, emptyDir = 0;
     std::vector<int32_t> own, nei, patchStart, patchSize, uType, pType;
-    std::vector<double> magSf, ndc, V, Sf, d, w, corr, C, Cf, skew, uValue, pValue, U0, p0, uRobin, pRobin;
+    std::vector<double> magSf, ndc, V, Sf, d, w, corr, C, Cf, skew, uValue, pValue, U0, p0, uRobin, pRobin, uAdv;
     vlm_flow_ctrl ctrl{};
     int32_t steady = 1, nSteps = 0, maxIter = 0;
     double dt = 1.0, tol = 1e-6, arrival = 0;
@@ -272,6 +272,8 @@ vlm_status vlm_server_submit(vlm_server* s, const vlm_flow_request* r, int64_t* 
     q->pRobin = copyOf(r->ctrl->p_robin, 2 * nPb);
     q->ctrl.u_robin = q->uRobin.empty() ? nullptr : q->uRobin.data();
     q->ctrl.p_robin = q->pRobin.empty() ? nullptr : q->pRobin.data();
+    q->uAdv = copyOf(r->ctrl->u_advective, 4 * nPb);
+    q->ctrl.u_advective = q->uAdv.empty() ? nullptr : q->uAdv.data();
     q->steady = r->ctrl->steady;
     q->nSteps = r->n_steps;
     q->dt = r->dt;
