@@ -248,12 +248,21 @@ vlm_status vlm_mesh_stats(vlm_mesh* mesh, int64_t* launches, int64_t* device_byt
  * picks these per device and mesh size. */
 vlm_status vlm_mesh_set_tail(vlm_mesh* mesh, int32_t cluster, int64_t max_rows, int64_t full_rows);
 vlm_status vlm_mesh_get_tail(vlm_mesh* mesh, int32_t* cluster, int64_t* max_rows, int64_t* full_rows);
-/* Measurement hook: times `reps` back-to-back launches of one level-0 kernel on the matrix of
- * the last solve ("amul64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch
- * is one full multicolour sweep; "vcycle32" / "vcycle32_notail" one FP32 V-cycle with / without
- * the single-CTA coarse tail, "tail32" the tail alone, bytes 0) with CUDA events on the context
- * stream, from a fixed state (right-hand side b, zero iterate).  Outputs the mean ms per launch
- * and the algorithmic bytes of one launch (values + int32 addressing, each array once). */
+/* Fused launches on the V-cycle's Jacobi levels (no reference counterpart; results bit for bit as
+ * unfused): on levels of at most pre_rows rows (all systems of the mesh) both pre-sweeps from zero
+ * run as one pass, on levels of at most restrict_rows rows the residual and the restriction, and on
+ * levels of at most post_rows rows the prolongation runs inside the first post-sweep.  A negative
+ * value keeps a setting; 0 (the default) fuses nowhere.  Same timing rules as vlm_mesh_set_tail. */
+vlm_status vlm_mesh_set_fusion(vlm_mesh* mesh, int64_t pre_rows, int64_t restrict_rows, int64_t post_rows);
+vlm_status vlm_mesh_get_fusion(vlm_mesh* mesh, int64_t* pre_rows, int64_t* restrict_rows, int64_t* post_rows);
+/* Measurement hook: times `reps` launches of one level-0 kernel on the matrix of the last solve
+ * ("amul64", "spmv64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch is one
+ * full multicolour sweep; "vcycle32" / "vcycle32_notail" one FP32 V-cycle with / without the
+ * coarse tail, "tail32" the tail alone, bytes 0) with CUDA events on the context stream, from a
+ * fixed state (right-hand side b, zero iterate).  Each launch is timed on its own after a read of a
+ * 256 MB buffer has evicted its operands from the L2 cache; the suffix ":warm" times the launches
+ * back to back instead (operands that fit stay in L2).  Outputs the mean ms per launch and the
+ * algorithmic bytes of one launch (values + int32 addressing, each array once). */
 vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* mesh, const char* kernel, int32_t reps, double* ms,
                               double* bytes);
 
@@ -463,8 +472,8 @@ vlm_status vlm_server_destroy(vlm_server* server);
  * device pointers; the work is ordered on `stream` (a cudaStream_t, NULL = default stream) and the
  * call returns before it completes.  Scratch: one fixed 299,016-byte __device__ array per device,
  * held until the process exits and shared by all calls; calls that overlap on the GPU race on it,
- * so order them on one stream.  The first call on a device looks the array up and clears it
- * (make that first call before any stream capture).  n <= 2^31-1, else VLM_ERR_BAD_ARG; the
+ * so order them on one stream.  The first call on a device looks the array up; every call clears
+ * its counter on `stream` before the sum.  n <= 2^31-1, else VLM_ERR_BAD_ARG; the
  * message is available from vlm_last_error(NULL). */
 vlm_status vlm_exact_sum_noalloc(const double* values, int64_t n, double* out, void* stream);
 

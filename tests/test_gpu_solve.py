@@ -322,3 +322,29 @@ def test_tail_launch_configurations_give_identical_results(name, precision):
             ref = (x, p.iterations)
             assert p.converged
         assert p.iterations == ref[1] and np.array_equal(x, ref[0]), cfg
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["periodic24", "stretched6x9x5"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_coarse_launches_give_identical_results(name, precision):
+    """The fused Jacobi-level launches (both pre-sweeps in one pass, residual with restriction,
+    prolongation inside the first post-sweep) perform the unfused launches' row operations in the
+    same order: every combination gives the unfused solution bit for bit, with and without the
+    coarse tail."""
+    g, _ = device_mesh(name)
+    m = vb.Mesh.from_arrays(g)
+    c = ctrl(preconditioner="GAMG", precision=precision)
+    ref = None
+    big = 1 << 40
+    for tail in [(1, 32, 1), (1, 1, 1 << 30)]:
+        m.set_tail(*tail)
+        for fuse in [(0, 0, 0), (big, 0, 0), (0, big, 0), (0, 0, big), (big, big, big), (64, 64, 64)]:
+            m.set_fusion(*fuse)
+            assert m.fusion_config() == fuse
+            x = g["x0"].copy()
+            p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, c)
+            if ref is None:
+                ref = (x, p.iterations)
+                assert p.converged
+            assert p.iterations == ref[1] and np.array_equal(x, ref[0]), (tail, fuse)

@@ -290,6 +290,18 @@ class Mesh:
         check(load().vlm_mesh_get_tail(self._h, C.byref(c), C.byref(a), C.byref(b)))
         return c.value, a.value, b.value
 
+    def set_fusion(self, pre_rows: int = -1, restrict_rows: int = -1, post_rows: int = -1):
+        """Row limits of the fused Jacobi-level launches (vlm_mesh_set_fusion): both pre-sweeps in one
+        pass, residual with restriction, prolongation inside the first post-sweep; negative keeps a
+        value, 0 fuses nowhere.  Results are unchanged bit for bit."""
+        check(load().vlm_mesh_set_fusion(self._h, int(pre_rows), int(restrict_rows), int(post_rows)), self.ctx.handle)
+
+    def fusion_config(self):
+        """(pre_rows, restrict_rows, post_rows) of the fused Jacobi-level launches."""
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().vlm_mesh_get_fusion(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def profile_kernel(self, kernel: str, reps: int = 20):
         """(ms per launch, algorithmic bytes per launch) of a level-0 kernel on the last solve's matrix."""
         ms, by = C.c_double(), C.c_double()

@@ -449,6 +449,20 @@ vlm_status vlm_mesh_get_tail(vlm_mesh* m, int32_t* cluster, int64_t* max_rows, i
     return VLM_OK;
 }
 
+vlm_status vlm_mesh_set_fusion(vlm_mesh* m, int64_t pre_rows, int64_t restrict_rows, int64_t post_rows) {
+    if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(m->ctx, [&] {
+        setDevice(m->ctx);
+        m->batch->setFusion(pre_rows, restrict_rows, post_rows);
+    });
+}
+
+vlm_status vlm_mesh_get_fusion(vlm_mesh* m, int64_t* pre_rows, int64_t* restrict_rows, int64_t* post_rows) {
+    if (!m || !pre_rows || !restrict_rows || !post_rows) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    m->batch->fusionConfig(pre_rows, restrict_rows, post_rows);
+    return VLM_OK;
+}
+
 vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* m, const char* kernel, int32_t reps, double* ms, double* bytes) {
     if (!ctx || !m || !kernel || !ms || !bytes || reps <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
     return guarded(ctx, [&] {

@@ -528,9 +528,10 @@ __global__ void __launch_bounds__(kBlockRows, 1) k_smooth_bgs(const Chunk* __res
 }
 
 // Jacobi sweep xo = (r - offdiag*xi)/D.  MODE 0: plain; MODE 1: xi == 0 (first pre-sweep);
-// MODE 2: xi + xc[agg] (the coarse-grid correction, GAMG.cpp:437-438, fused in).
-// FP32: 48 registers, 5 resident CTAs per SM (measured faster than 4 at 56 registers on the coarse
-// levels, whose rows of 11-19 entries take two or three batches); FP64 keeps the compiler's choice.
+// MODE 2: xi + xc[agg] (the coarse-grid correction, GAMG.cpp:437-438, fused in); MODE 3: both
+// pre-sweeps from zero in one pass (the neighbours' first-sweep values recomputed from r and D).
+// Launch bounds: 3 resident CTAs per SM for FP32 (at most 80 registers: the 16 preloaded entries of
+// RowPre), 2 for FP64.
 template <class T, int MODE>
 __global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 3 : 2) k_smooth_jacobi(const Chunk* __restrict__ ch, Sell S,
                                                                const T* __restrict__ val, const T* __restrict__ diag,
@@ -552,6 +553,11 @@ __global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 3 : 2) k_smooth_
     pdl_wait();
     if (chunk_skip(c, st, flag)) return;
     auto xv = [&](int j) -> T {
+        if (MODE == 3) {
+            // the first sweep from zero, recomputed where the second reads it (the MODE 1 value)
+            const T v = __ldg(r + j) / __ldg(diag + j);
+            return omega == T(1) ? v : omega * v;
+        }
         T v = __ldg(xi + j);
         if (MODE == 2) {
             const int a = __ldg(agg + j);
@@ -627,6 +633,47 @@ __global__ void __launch_bounds__(kRowsPerCta) k_restrict(const Chunk* __restric
     for (int q = 0; q < kChildPre; ++q)
         if (k0 + q < k1) s += v[q];
     for (int k = k0 + kChildPre; k < k1; ++k) s += res[child[k]];
+    rc[R] = s;
+}
+
+// k_residual and k_restrict in one pass over the coarse rows: each aggregate computes its
+// children's residuals (the same row operations as k_residual) and sums them in child order, as
+// k_restrict sums the stored ones.  For coarse levels, where a launch costs more than the
+// scattered row reads it saves.
+template <class T>
+__global__ void __launch_bounds__(kRowsPerCta) k_residual_restrict(const Chunk* __restrict__ ch, Sell S,
+                                                                   const T* __restrict__ val,
+                                                                   const T* __restrict__ diag, const T* __restrict__ r,
+                                                                   const T* __restrict__ x,
+                                                                   const int32_t* __restrict__ cptr,
+                                                                   const int32_t* __restrict__ child,
+                                                                   T* __restrict__ rc, const SysState* st, int flag) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    if ((int)threadIdx.x >= c.count) return;
+    const int R = c.start + threadIdx.x;
+    const int k0 = __ldg(cptr + R), k1 = __ldg(cptr + R + 1);
+    int i0 = 0;
+    RowPre<T, 8> pre;
+    T dg = T(1);
+    if (k0 < k1) {  // the first child's structure, values and diagonal ahead of the wait
+        i0 = __ldg(child + k0);
+        pre.load(S, val, i0);
+        dg = __ldg(diag + i0);
+    }
+    pdl_wait();
+    if (chunk_skip(c, st, flag)) return;
+    auto xf = [&](int j) { return __ldg(x + j); };
+    T s = T(0);
+    for (int k = k0; k < k1; ++k) {
+        int i = i0;
+        if (k != k0) {
+            i = __ldg(child + k);
+            pre.load(S, val, i);
+            dg = __ldg(diag + i);
+        }
+        s += pre.template accumulate<true>(S, val, xf, r[i] - dg * x[i]);
+    }
     rc[R] = s;
 }
 

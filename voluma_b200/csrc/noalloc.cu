@@ -107,12 +107,7 @@ vlm_status scratchForCurrentDevice(long long** out, std::string* err) {
             *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
             return VLM_ERR_CUDA;
         }
-        e = cudaMemset(p + kCounterWord, 0, sizeof(long long));
-        if (e != cudaSuccess) {
-            *err = std::string("cudaMemset: ") + cudaGetErrorString(e);
-            return VLM_ERR_CUDA;
-        }
-        g_scratchAddr[dev] = p;
+        g_scratchAddr[dev] = p;  // every call clears the counter on its own stream
     }
     *out = g_scratchAddr[dev];
     return VLM_OK;

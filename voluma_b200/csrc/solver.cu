@@ -188,6 +188,9 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     if (const char* cl = std::getenv("VLM_TAIL_CLUSTER")) tailCl_ = std::atoi(cl);
     if (const char* mr = std::getenv("VLM_TAIL_ROWS")) tailMaxRows_ = std::atoll(mr);
     if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) tailFullRows_ = std::atoll(fr);
+    if (const char* f = std::getenv("VLM_FUSE_PRE")) fusePre_ = std::atoll(f);
+    if (const char* f = std::getenv("VLM_FUSE_RESTRICT")) fuseRestrict_ = std::atoll(f);
+    if (const char* f = std::getenv("VLM_FUSE_POST")) fusePost_ = std::atoll(f);
     planTail();
     buildChunkLists();
     for (int k = 0; k < nL; ++k) {
@@ -252,6 +255,7 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     counters_.resize(size_t(plan_.nsys));
     counters_.zero(stream_);
     status_.resize(1);
+    status_.zero(stream_);
     partials_.resize(size_t(plan_.nSlots) * 2);
     st_.resize(size_t(plan_.nsys));
     st_.zero(stream_);
@@ -315,6 +319,15 @@ void DeviceBatch::buildChunkLists() {
 
 // Re-plans the coarse tail (cluster size, level row limit, whole-V-cycle row limit; 0 keeps the
 // current value) on a registered batch: chunk lists, tail tables, and the recorded graphs.
+// Row limits of the fused coarse-level launches (negative keeps a value); the recorded graphs go.
+void DeviceBatch::setFusion(int64_t pre, int64_t restrict, int64_t post) {
+    VLM_CUDA(cudaStreamSynchronize(stream_));
+    if (pre >= 0) fusePre_ = pre;
+    if (restrict >= 0) fuseRestrict_ = restrict;
+    if (post >= 0) fusePost_ = post;
+    graphs_.clear();
+}
+
 void DeviceBatch::setTail(int cluster, int64_t maxRows, int64_t fullRows) {
     if (cluster != 0) tailCl_ = cluster;
     if (maxRows != 0) tailMaxRows_ = maxRows;
@@ -544,7 +557,17 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
         // Jacobi; pre: from zero, post: after the ascent's prolongation pass
         const T om = T(jacobiOmega_);
         const ChunkList& rows = head ? D.headActive : D.active;
-        if (pre) {
+        if (pre && fusedLevel(k, fusePre_)) {
+            // both sweeps from zero in one pass
+            VLM_LAUNCH((k_smooth_jacobi<T, 3>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r,
+                       (const T*)nullptr, x, om, agg, xc, st, flag);
+        } else if (!pre && fusedLevel(k, fusePost_)) {
+            // the coarse-grid correction inside the first sweep (no k_prolong pass)
+            VLM_LAUNCH((k_smooth_jacobi<T, 2>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x, x2,
+                       om, agg, xc, st, flag);
+            VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
+                       om, agg, xc, st, flag);
+        } else if (pre) {
             VLM_LAUNCH((k_smooth_jacobi<T, 1>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r,
                        (const T*)nullptr, x2, om, agg, xc, st, flag);
             VLM_LAUNCH((k_smooth_jacobi<T, 0>), rows.n, kRowsPerCta, s, D.ch(rows), S, val, diag, r, x2, x,
@@ -650,6 +673,10 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
             else
                 VLM_LAUNCH(k_box_residual<T>, g, kRowsPerCta, s, R, LV<T>::bcoef(D), D.nrows, LV<T>::diag(D), rr(k),
                            (const T*)xx(k), LV<T>::t(D), st, flag);
+        } else if (fusedLevel(k, fuseRestrict_)) {
+            VLM_LAUNCH(k_residual_restrict<T>, next.n, kRowsPerCta, s, N.ch(next), D.sell(), LV<T>::val(D),
+                       LV<T>::diag(D), rr(k), (const T*)xx(k), D.childPtr.get(), D.child.get(), LV<T>::r(N), st, flag);
+            continue;
         } else
             VLM_LAUNCH(k_residual<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.sell(), LV<T>::val(D), LV<T>::diag(D),
                        rr(k), xx(k), LV<T>::t(D), st, flag);
@@ -672,7 +699,8 @@ void DeviceBatch::recordVcycle(const T* r0, T* x0, SmootherKind sm, int flag, bo
         // the separate pass measured no faster); Jacobi (on any level layout) and multicolour GS
         // with more colours sweep after this pass (active chunks are at most kRowsPerCta rows, one
         // per k_prolong thread)
-        if (jacobiHere || (!D.blockGS && D.nSteps != 2)) {
+        const bool fusedProlong = jacobiHere && fusedLevel(k, fusePost_);
+        if (!fusedProlong && (jacobiHere || (!D.blockGS && D.nSteps != 2))) {
             const ChunkList& rows = tail ? D.headActive : D.active;
             VLM_LAUNCH(k_prolong<T>, rows.n, kRowsPerCta, s, D.ch(rows), D.agg.get(), xx(k + 1), xx(k), st, flag);
         }
@@ -1411,7 +1439,11 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
         lastDeferred_.pre = Gp ? Gp->preK : 0;
         lastDeferred_.body = Gp ? Gp->bodyK : 0;
         VLM_CUDA(cudaMemcpyAsync(so, st_.get(), sizeof(SysState) * plan_.nsys, cudaMemcpyDeviceToDevice, s));
-        VLM_CUDA(cudaMemcpyAsync(sto, status_.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
+        // the coarse-factor status belongs to GAMG solves only (status_ is not reset for the others)
+        if (pk == PrecondKind::GAMG)
+            VLM_CUDA(cudaMemcpyAsync(sto, status_.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
+        else
+            VLM_CUDA(cudaMemsetAsync(sto, 0, sizeof(int), s));
         if (levelSchedule)
             VLM_CUDA(cudaMemcpyAsync(sto + 1, dilu_->err.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
         else
@@ -1560,8 +1592,24 @@ double exactSumOnDevice(cudaStream_t s, const double* v, int64_t n) {
     return h;
 }
 
-double DeviceBatch::profileKernel(const std::string& name, int reps, double* bytesPerLaunch) {
+// Reads a buffer larger than the L2 cache so that the next launch finds none of its operands there
+// (clean lines: no write-backs compete with the timed kernel).  The buffer is zero, so the store
+// never happens; it keeps the loads.
+__global__ void k_l2_flush(const int4* __restrict__ buf, size_t n, int* __restrict__ sink) {
+    int acc = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const int4 v = buf[i];
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if (acc == 0x5eed1234) *sink = acc;
+}
+
+double DeviceBatch::profileKernel(const std::string& fullName, int reps, double* bytesPerLaunch) {
     cudaStream_t s = stream_;
+    const std::string warmSuffix = ":warm";
+    const bool warm = fullName.size() > warmSuffix.size() &&
+                      fullName.compare(fullName.size() - warmSuffix.size(), warmSuffix.size(), warmSuffix) == 0;
+    const std::string name = warm ? fullName.substr(0, fullName.size() - warmSuffix.size()) : fullName;
     DevLevel& D0 = L_[0];
     const double N = double(plan_.userCells), F = double(plan_.userFaces);
     cudaEvent_t e0, e1;
@@ -1657,15 +1705,37 @@ double DeviceBatch::profileKernel(const std::string& name, int reps, double* byt
     w_.zero(s);
     if (w32_.size() == size_t(D0.nrows)) w32_.zero(s);
     run();
-    VLM_CUDA(cudaEventRecord(e0, s));
-    for (int i = 0; i < reps; ++i) run();
-    VLM_CUDA(cudaEventRecord(e1, s));
-    VLM_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    VLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    double total = 0.0;
+    if (warm) {
+        VLM_CUDA(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; ++i) run();
+        VLM_CUDA(cudaEventRecord(e1, s));
+        VLM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        total = ms;
+    } else {
+        constexpr size_t kFlushBytes = size_t(256) << 20;  // twice the B200's 126 MB L2
+        if (flush_.size() == 0) {
+            flush_.resize(kFlushBytes / sizeof(int4));
+            flush_.zero(s);
+            flushSink_.resize(1);
+        }
+        for (int i = 0; i < reps; ++i) {
+            k_l2_flush<<<1184, 256, 0, s>>>(flush_.get(), flush_.size(), flushSink_.get());
+            VLM_CUDA(cudaGetLastError());
+            VLM_CUDA(cudaEventRecord(e0, s));
+            run();
+            VLM_CUDA(cudaEventRecord(e1, s));
+            VLM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            VLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            total += ms;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return double(ms) / reps;
+    return total / reps;
 }
 
 template void DeviceBatch::recordVcycle<double>(const double*, double*, SmootherKind, int, bool);

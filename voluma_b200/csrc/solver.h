@@ -142,6 +142,12 @@ public:
     // Coarse-tail configuration (tuning): cluster size 1/2/4/8, level row limit, whole-V-cycle row
     // limit (0 keeps a value); re-plans the batch's launches, same results.
     void setTail(int cluster, int64_t maxRows, int64_t fullRows);
+    void setFusion(int64_t pre, int64_t restrict, int64_t post);
+    void fusionConfig(int64_t* pre, int64_t* restrict, int64_t* post) const {
+        *pre = fusePre_;
+        *restrict = fuseRestrict_;
+        *post = fusePost_;
+    }
     void tailConfig(int* cluster, int64_t* maxRows, int64_t* fullRows) const {
         *cluster = tailCl_;
         *maxRows = tailMaxRows_;
@@ -151,6 +157,8 @@ public:
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
     // solve); returns ms per launch and the algorithmic bytes one launch moves.
     double profileKernel(const std::string& name, int reps, double* bytesPerLaunch);
+    DBuf<int4> flush_;       // profileKernel's L2-evicting read buffer (allocated on first use)
+    DBuf<int> flushSink_;
 
 
 private:
@@ -210,6 +218,12 @@ private:
     int tailCl_ = 1;                     // CTAs of the cluster that runs one system's tail (the tuner may widen it)
     int64_t tailMaxRows_ = 0;            // levels of at most this many rows go to the tail (0: scaled default)
     int64_t tailFullRows_ = 0;           // systems of at most this many level-0 rows: whole V-cycle there
+    // fused coarse-level launches on levels of at most this many rows (all systems): both Jacobi
+    // pre-sweeps in one pass, residual with restriction, prolongation inside the first post-sweep.
+    // Off by default: at 128^3 each fusion measured slower than its separate launches (inside the
+    // captured graph a launch costs less than the longer dependent-load chain of the fused kernel).
+    int64_t fusePre_ = 0, fuseRestrict_ = 0, fusePost_ = 0;
+    bool fusedLevel(int k, int64_t limit) const { return int64_t(L_[k].nrows) <= limit; }
     std::vector<SysTopo> topo_;          // host topology (owned by the caller for the batch's lifetime)
     int mergeLevels_ = 2;
     std::unique_ptr<DiluDev> dilu_;      // built on the first DIC/DILU/Gauss-Seidel solve
