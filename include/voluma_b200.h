@@ -254,6 +254,12 @@ vlm_status vlm_mesh_get_tail(vlm_mesh* mesh, int32_t* cluster, int64_t* max_rows
  * levels of at most post_rows rows the prolongation runs inside the first post-sweep.  A negative
  * value keeps a setting; 0 (the default) fuses nowhere.  Same timing rules as vlm_mesh_set_tail. */
 vlm_status vlm_mesh_set_fusion(vlm_mesh* mesh, int64_t pre_rows, int64_t restrict_rows, int64_t post_rows);
+/* Measurement hook (no reference counterpart): with `on`, the mesh's solves run their launches
+ * directly (no graph) with a CUDA event pair around every level-0 smoothing sweep, in the solve's
+ * own order; vlm_mesh_sweep_time returns the summed event times (ms) and the number of sweeps since
+ * timing was switched on.  Results are unchanged. */
+vlm_status vlm_mesh_time_sweeps(vlm_mesh* mesh, int32_t on);
+vlm_status vlm_mesh_sweep_time(vlm_mesh* mesh, double* ms_total, int64_t* sweeps);
 vlm_status vlm_mesh_get_fusion(vlm_mesh* mesh, int64_t* pre_rows, int64_t* restrict_rows, int64_t* post_rows);
 /* Measurement hook: times `reps` launches of one level-0 kernel on the matrix of the last solve
  * ("amul64", "spmv64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch is one

@@ -348,3 +348,43 @@ def test_fused_coarse_launches_give_identical_results(name, precision):
                 ref = (x, p.iterations)
                 assert p.converged
             assert p.iterations == ref[1] and np.array_equal(x, ref[0]), (tail, fuse)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["periodic24", "walls7x5x3"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_box_sweep_matches_colour_launches(name, precision, monkeypatch):
+    """A box level-0 red-black sweep as one launch (first-colour pieces, then second-colour pieces
+    that wait for the planes they read, across the periodic wrap) performs the two colour launches'
+    row operations: the same solution bit for bit."""
+    g, _ = device_mesh(name)
+    out = []
+    for fused in ("0", "1"):
+        monkeypatch.setenv("VLM_BOX_FUSED", fused)
+        m = vb.Mesh.from_arrays(g)
+        x = g["x0"].copy()
+        p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, ctrl(preconditioner="GAMG", precision=precision))
+        out.append((x, p.iterations))
+        m.close()
+    assert out[0][1] == out[1][1] and np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["periodic24", "jitter10x8x6", "stretched6x9x5"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_shared_memory_tail_matches_global_tail(name, precision, monkeypatch):
+    """The coarse tail with every operand in shared memory performs the global-memory tail's row
+    operations in the same order: bit for bit, for tails that start at several levels."""
+    g, _ = device_mesh(name)
+    c = ctrl(preconditioner="GAMG", precision=precision)
+    for rows in (32, 256, 1024):
+        out = []
+        for smem in ("0", "1"):
+            monkeypatch.setenv("VLM_TAIL_SMEM", smem)
+            m = vb.Mesh.from_arrays(g)
+            m.set_tail(1, rows, 1)
+            x = g["x0"].copy()
+            p = vb.solve_ldu(m, g["diag"], g["upper"], None, g["b"], x, c)
+            out.append((x, p.iterations))
+            m.close()
+        assert out[0][1] == out[1][1] and np.array_equal(out[0][0], out[1][0]), rows

@@ -302,6 +302,17 @@ class Mesh:
         check(load().vlm_mesh_get_fusion(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
 
+    def time_sweeps(self, on: bool = True):
+        """Live level-0 sweep timing (vlm_mesh_time_sweeps): solves run eagerly with CUDA events
+        around every level-0 sweep."""
+        check(load().vlm_mesh_time_sweeps(self._h, int(bool(on))), self.ctx.handle)
+
+    def sweep_time(self):
+        """(summed ms, sweeps) of the level-0 sweeps timed since time_sweeps(True)."""
+        ms, n = C.c_double(), C.c_int64()
+        check(load().vlm_mesh_sweep_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def profile_kernel(self, kernel: str, reps: int = 20):
         """(ms per launch, algorithmic bytes per launch) of a level-0 kernel on the last solve's matrix."""
         ms, by = C.c_double(), C.c_double()

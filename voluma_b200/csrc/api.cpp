@@ -449,6 +449,20 @@ vlm_status vlm_mesh_get_tail(vlm_mesh* m, int32_t* cluster, int64_t* max_rows, i
     return VLM_OK;
 }
 
+vlm_status vlm_mesh_time_sweeps(vlm_mesh* m, int32_t on) {
+    if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    return guarded(m->ctx, [&] {
+        setDevice(m->ctx);
+        m->batch->setSweepTiming(on != 0);
+    });
+}
+
+vlm_status vlm_mesh_sweep_time(vlm_mesh* m, double* ms_total, int64_t* sweeps) {
+    if (!m || !ms_total || !sweeps) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    m->batch->sweepTiming(ms_total, sweeps);
+    return VLM_OK;
+}
+
 vlm_status vlm_mesh_set_fusion(vlm_mesh* m, int64_t pre_rows, int64_t restrict_rows, int64_t post_rows) {
     if (!m) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
     return guarded(m->ctx, [&] {

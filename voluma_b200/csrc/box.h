@@ -64,6 +64,12 @@ struct BoxSys {
 // range form skips the state check: the loop stops once its one system is done, and a V-cycle that
 // still runs in that last pass (after a breakdown found earlier in the pass) only rewrites the
 // preconditioner's scratch vectors, which nothing reads afterwards.
+// Counters of the fused two-colour level-0 sweep: piece tickets, finished CTAs, launch epoch, and an
+// error word for a wait that gave up.
+struct SweepSync {
+    unsigned ticket, finished, epoch, err;
+};
+
 struct BoxRows {
     const Chunk* ch;  // null: the range form
     const BoxSys* boxes;

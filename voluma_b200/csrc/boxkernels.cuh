@@ -372,40 +372,40 @@ struct BoxGroup4 {
     }
 };
 
-// Gauss-Seidel colour step, four slots per thread (range form, H % 4 == 0); MODE as k_box_gs.
-template <class T, int MODE = 0>
-__global__ void __launch_bounds__(kRowsPerCta) k_box_gs4(BoxRows R, const T* __restrict__ coef, int nrows,
-                                                         const T* __restrict__ diag, const T* __restrict__ r, T* x,
-                                                         const int32_t* __restrict__ agg, const T* __restrict__ xc) {
-    pdl_launch();
-    const int row0 = R.begin + 4 * (int(blockIdx.x) * kRowsPerCta + int(threadIdx.x));
-    if (row0 >= R.end) return;
-    const BoxSys& B = R.one;
-    const T* cx = coef;
-    const T* cy = coef + nrows;
-    const T* cz = coef + 2 * size_t(nrows);
+// Coherent (L2) vector loads: values that other CTAs of the same launch write (the fused sweep).
+__device__ __forceinline__ V4<float> ld4_cg(const float* p) {
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    return V4<float>{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ V4<double> ld4_cg(const double* p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p)), b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>{{a.x, a.y, b.x, b.y}};
+}
+
+// One four-slot group of a Gauss-Seidel colour step after its fixed operands are loaded (G.load):
+// MODE 0 plain, 1 from a zero iterate (x = r / D), 2 with the coarse-grid correction x + xc[agg] of the
+// neighbours read (the prolongation fused into the first post-smoothing step).  COH: the other colour
+// was written by this launch (coherent loads) instead of by an earlier one.
+template <class T, int MODE, bool COH>
+__device__ __forceinline__ void box_gs4_group(const BoxGroup4<T>& G, const BoxSys& B, int row0,
+                                              const T* __restrict__ diag, const T* __restrict__ r, T* x,
+                                              const int32_t* __restrict__ agg, const T* __restrict__ xc) {
     if (MODE == 1) {
-        const V4<T> dg = ld4_keep(diag + row0, l2_keep());
-        pdl_wait();
         const V4<T> rv = ld4(r + row0);
         T out[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = rv.v[v] / dg.v[v];
+        for (int v = 0; v < 4; ++v) out[v] = rv.v[v] / G.dg.v[v];
         st4(x + row0, out);
         return;
     }
-    BoxGroup4<T> G;
-    G.load(B, row0, cx, cy, cz, diag);
     if (!G.valid) {
         // padding slots past the colour group's cells: x = r / D as for any padding row
-        pdl_wait();
         for (int v = 0; v < 4; ++v) x[row0 + v] = r[row0 + v] / diag[row0 + v];
         return;
     }
-    pdl_wait();
     // the other colour's values (x, plus the coarse-grid correction for MODE 2)
     auto xv4 = [&](int j) -> V4<T> {
-        V4<T> a = ld4(x + j);
+        V4<T> a = COH ? ld4_cg(x + j) : ld4(x + j);
         if (MODE == 2) {
             const int4 g = __ldg(reinterpret_cast<const int4*>(agg + j));
             const int gi[4] = {g.x, g.y, g.z, g.w};
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_gs4(BoxRows R, const T* __r
         return a;
     };
     auto xv1 = [&](int j) -> T {
-        T a = __ldg(x + j);
+        T a = COH ? __ldcg(x + j) : __ldg(x + j);
         if (MODE == 2) {
             const int g = __ldg(agg + j);
             if (g >= 0) a += __ldg(xc + g);
@@ -433,6 +433,132 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_gs4(BoxRows R, const T* __r
 #pragma unroll
     for (int v = 0; v < 4; ++v) out[v] = s[v] / G.dg.v[v];
     st4(x + row0, out);
+}
+
+// Gauss-Seidel colour step, four slots per thread (range form, H % 4 == 0); MODE as k_box_gs.
+template <class T, int MODE = 0>
+__global__ void __launch_bounds__(kRowsPerCta) k_box_gs4(BoxRows R, const T* __restrict__ coef, int nrows,
+                                                         const T* __restrict__ diag, const T* __restrict__ r, T* x,
+                                                         const int32_t* __restrict__ agg, const T* __restrict__ xc) {
+    pdl_launch();
+    const int row0 = R.begin + 4 * (int(blockIdx.x) * kRowsPerCta + int(threadIdx.x));
+    if (row0 >= R.end) return;
+    const BoxSys& B = R.one;
+    BoxGroup4<T> G;
+    if (MODE == 1)
+        G.dg = ld4_keep(diag + row0, l2_keep());
+    else
+        G.load(B, row0, coef, coef + nrows, coef + 2 * size_t(nrows), diag);
+    pdl_wait();
+    box_gs4_group<T, MODE, false>(G, B, row0, diag, r, x, agg, xc);
+}
+
+// ---------------------------------------------------------------- fused two-colour sweep
+// Both colour steps of a red-black sweep in one launch.  Pieces of kSweepPiece slots are taken in
+// ticket order from a device counter: first every piece of the first colour, then every piece of the
+// second; a second-colour piece starts once the first-colour pieces it reads (its z-planes and the two
+// next to them, across the periodic wrap) carry this launch's done stamp.  A piece only waits for
+// lower tickets, which CTAs that are already running hold, so the waits end without any guarantee
+// of co-residency; each is still bounded (spin limit, then an error word and no wait).  The last CTA
+// resets the counters and advances the launch epoch that the stamps compare against.
+constexpr int kSweepPiece = 4 * kRowsPerCta;
+constexpr long long kSweepSpinLimit = 1ll << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Lanes of one warp wait until stamps[lo..hi] all equal `want` (bounded).
+__device__ __forceinline__ void sweep_wait_range(const unsigned* stamps, int lo, int hi, unsigned want,
+                                                 SweepSync* sync) {
+    for (int i = lo + int(threadIdx.x & 31); i <= hi; i += 32) {
+        long long n = 0;
+        while (ld_acquire_u32(stamps + i) != want) {
+            if (++n > kSweepSpinLimit) {
+                atomicOr(&sync->err, 1u);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+}
+
+// Launch bounds: the colour step's register budget (4 resident CTAs per SM in FP32, 2 in FP64).
+template <class T, int MODE1>
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 4 ? 4 : 2) k_box_sweep4(BoxSys B, int beginA, int endA, int beginB, int endB,
+                                                            const T* __restrict__ coef, int nrows,
+                                                            const T* __restrict__ diag, const T* __restrict__ r, T* x,
+                                                            const int32_t* __restrict__ agg, const T* __restrict__ xc,
+                                                            SweepSync* sync, unsigned* done) {
+    pdl_launch();
+    pdl_wait();
+    __shared__ int sTicket;
+    __shared__ unsigned sEpoch;
+    if (threadIdx.x == 0) sEpoch = ld_acquire_u32(&sync->epoch);
+    const T* cx = coef;
+    const T* cy = coef + nrows;
+    const T* cz = coef + 2 * size_t(nrows);
+    const int nA = (endA - beginA + kSweepPiece - 1) / kSweepPiece;
+    const int nB = (endB - beginB + kSweepPiece - 1) / kSweepPiece;
+    const int plane = B.H * B.ny;  // slots of one colour in one z-plane
+    const bool perZ = (B.per & 4) != 0;
+    __syncthreads();
+    const unsigned stamp = sEpoch + 1u;
+    for (;;) {
+        if (threadIdx.x == 0) sTicket = int(atomicAdd(&sync->ticket, 1u));
+        __syncthreads();
+        const int t = sTicket;
+        __syncthreads();
+        if (t >= nA + nB) break;
+        const bool first = t < nA;
+        const int q = first ? t : t - nA;
+        if (!first && threadIdx.x < 32) {
+            // the first colour's slots this piece reads: its z-planes and one more on each side
+            const int s0 = q * kSweepPiece, s1 = min((q + 1) * kSweepPiece, endB - beginB);
+            const int k0 = s0 / plane, k1 = (s1 - 1) / plane;
+            const int lo = max(k0 - 1, 0) * plane, hi = min(k1 + 2, B.nz) * plane;
+            sweep_wait_range(done, lo / kSweepPiece, min((hi - 1) / kSweepPiece, nA - 1), stamp, sync);
+            if (perZ && k0 == 0) sweep_wait_range(done, ((B.nz - 1) * plane) / kSweepPiece, nA - 1, stamp, sync);
+            if (perZ && k1 == B.nz - 1) sweep_wait_range(done, 0, min((plane - 1) / kSweepPiece, nA - 1), stamp, sync);
+        }
+        if (!first) __syncthreads();
+        const int row0 = (first ? beginA : beginB) + q * kSweepPiece + 4 * int(threadIdx.x);
+        if (row0 < (first ? endA : endB)) {
+            BoxGroup4<T> G;
+            if (MODE1 != 0 && first) {
+                if (MODE1 == 1)
+                    G.dg = ld4_keep(diag + row0, l2_keep());
+                else
+                    G.load(B, row0, cx, cy, cz, diag);
+                box_gs4_group<T, MODE1, false>(G, B, row0, diag, r, x, agg, xc);
+            } else {
+                // the other colour: written by an earlier launch (first colour) or by this one
+                G.load(B, row0, cx, cy, cz, diag);
+                box_gs4_group<T, 0, true>(G, B, row0, diag, r, x, agg, xc);
+            }
+        }
+        if (first) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                st_release_u32(done + t, stamp);
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&sync->finished, 1u) == gridDim.x - 1) {
+            sync->ticket = 0u;
+            sync->finished = 0u;
+            __threadfence();
+            st_release_u32(&sync->epoch, stamp);
+        }
+    }
 }
 
 // res = r - A x, four slots per thread (range form, H % 4 == 0)
@@ -529,6 +655,62 @@ __global__ void __launch_bounds__(kRowsPerCta) k_box_pcg_spmv(const Chunk* __res
             }
         } else {
             s.alpha = s.wArA / out[0];
+        }
+    }
+}
+
+// k_box_pcg_spmv for a single box system with H % 4 == 0 (every group of four slots takes the
+// vector path): no per-row fallback, so FP64 fits three resident CTAs per SM instead of two (the
+// exact-sum form, with its larger accumulator, keeps two).
+template <class T, int FLAG, bool EXACT>
+__global__ void __launch_bounds__(kRowsPerCta, sizeof(T) == 8 ? (EXACT ? 2 : 3) : 4) k_box_pcg_spmv4(
+    const Chunk* __restrict__ ch, BoxSys B, const T* __restrict__ coef, int nrows, const T* __restrict__ diag,
+    const T* __restrict__ p, T* __restrict__ Ap, RedCtx Rc, SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    const int row0 = c.start + 4 * int(threadIdx.x);
+    const bool has = row0 < c.start + c.count;
+    BoxGroup4<T> G;
+    G.valid = false;
+    if (has) G.load(B, row0, coef, coef + nrows, coef + 2 * size_t(nrows), diag);
+    pdl_wait();
+    if (sys_idle(st[c.sys], FLAG)) return;
+    BlockSum<1, EXACT> acc;
+    acc.begin();
+    if (has) {
+        const V4<T> pv = ld4(p + row0);
+        T s[4];
+        if (G.valid) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s[v] = G.dg.v[v] * pv.v[v];
+            auto xv4 = [&](int j) { return ld4(p + j); };
+            auto xf = [&](int j) -> T { return __ldg(p + j); };
+            if (B.nz > 1)
+                G.template accumulate<false, true>(xv4, xf, s);
+            else
+                G.template accumulate<false, false>(xv4, xf, s);
+        } else {
+            // padding slots past the colour group's cells: a diagonal-only row
+            const V4<T> dg = ld4(diag + row0);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s[v] = dg.v[v] * pv.v[v];
+        }
+        st4(Ap + row0, s);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc.add(0, (double)s[v] * (double)pv.v[v]);
+    }
+    double out[1];
+    if (acc.finish(c, Rc, out)) {
+        SysState& q = st[c.sys];
+        if (fabs(out[0]) < kVSMALL) {
+            if (FLAG == kFlagDone) {
+                q.done = 1;
+            } else {
+                q.innerDone = 1;
+                q.s1 = 1.0;
+            }
+        } else {
+            q.alpha = q.wArA / out[0];
         }
     }
 }

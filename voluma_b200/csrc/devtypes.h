@@ -75,4 +75,32 @@ struct TailSys {
     int grpStart[4], grpCount[4];
 };
 
+// One system's coarse tail in shared memory (k_vcycle_tail_smem): the Jacobi levels first..coarsest-1
+// as ELL rows with 16-bit local columns, the coarsest level's dense inverse, and every level's
+// vectors.  t* are element offsets into the T region of shared memory (the value image, then the
+// vectors), u* into the uint16 region (structure image).
+#ifdef __CUDACC__
+#define VLM_HD __host__ __device__
+#else
+#define VLM_HD
+#endif
+VLM_HD constexpr size_t tail_align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+// Shared-memory bytes of one system's tail: the T region, the coarsest inverse (doubles), the
+// uint16 region, each starting on a 16-byte boundary.
+VLM_HD inline size_t tail_smem_bytes(size_t tsize, int tCount, int nc, int strCount) {
+    return tail_align16(size_t(tCount) * tsize) + tail_align16(size_t(nc) * nc * sizeof(double)) +
+           tail_align16(size_t(strCount) * sizeof(uint16_t));
+}
+
+struct TailImg {
+    int sys, first, coarsest, nc, invOffset;
+    int valOff, strOff;              // offsets of this system's images in the batch's image buffers
+    int valCount, tCount, strCount;  // value-image T count; T count in shared memory; uint16 count
+    int n[kTailMaxLevels], W[kTailMaxLevels], rowStart[kTailMaxLevels];
+    int tDiag[kTailMaxLevels], tVal[kTailMaxLevels], tR[kTailMaxLevels], tX[kTailMaxLevels], tX2[kTailMaxLevels];
+    int uRlen[kTailMaxLevels], uCol[kTailMaxLevels], uAgg[kTailMaxLevels], uCptr[kTailMaxLevels],
+        uChild[kTailMaxLevels];
+};
+
 }  // namespace vlm

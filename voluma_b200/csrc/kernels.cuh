@@ -999,6 +999,160 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const TailSys* 
     }
 }
 
+// ------------------------------------------------------------------ shared-memory coarse tail
+// The value image of the shared-memory tail, gathered once per solve: code < 0 -> 0, else level
+// code >> 26, diagonal when bit 25 is set, index code & 0x1ffffff into that level's values.
+template <class T>
+__global__ void k_tail_values(int count, const int32_t* __restrict__ codes, const TailLevel<T>* __restrict__ lev,
+                              T* __restrict__ img) {
+    pdl_entry();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= count) return;
+    const int c = codes[v];
+    T a = T(0);
+    if (c >= 0) {
+        const TailLevel<T>& L = lev[c >> 26];
+        const int i = c & 0x1ffffff;
+        a = (c >> 25) & 1 ? L.diag[i] : L.val[i];
+    }
+    img[v] = a;
+}
+
+// The coarse tail of k_vcycle_tail (levels first..coarsest of one system, one CTA) with every
+// operand in shared memory: the images are copied in while the predecessor drains, then each step
+// (Jacobi sweep, residual, restriction, coarse solve, prolongation) reads shared memory only and ends
+// at a CTA barrier.  The row arithmetic is k_vcycle_tail's, term for term, so the results are the
+// same bit for bit; the first-sweep values are stored instead of recomputed.
+template <class T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail_smem(const TailImg* __restrict__ imgs,
+                                                                      const T* __restrict__ vimg,
+                                                                      const uint16_t* __restrict__ simg,
+                                                                      const TailLevel<T>* __restrict__ lev,
+                                                                      const double* __restrict__ inv, T omega,
+                                                                      const SysState* st, int flag) {
+    pdl_launch();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ __align__(16) TailImg I;  // the descriptor, read at every step
+    {
+        static_assert(sizeof(TailImg) % 4 == 0, "TailImg is copied as words");
+        const int* src = reinterpret_cast<const int*>(imgs + blockIdx.x);
+        int* dst = reinterpret_cast<int*>(&I);
+        for (int i = threadIdx.x; i < int(sizeof(TailImg) / 4); i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    const int nc = I.nc;
+    T* t = reinterpret_cast<T*>(smraw);
+    double* sinv = reinterpret_cast<double*>(smraw + tail_align16(size_t(I.tCount) * sizeof(T)));
+    uint16_t* u = reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(sinv) +
+                                              tail_align16(size_t(nc) * nc * sizeof(double)));
+    // images (fixed for the solve) while the predecessor drains: 16-byte copies (both images are
+    // padded to whole 16-byte words), the inverse by doubles
+    {
+        const int4* vs = reinterpret_cast<const int4*>(vimg + I.valOff);
+        int4* vd = reinterpret_cast<int4*>(t);
+        const int nv = int(size_t(I.valCount) * sizeof(T) / 16);
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) vd[i] = __ldg(vs + i);
+        const int4* ss = reinterpret_cast<const int4*>(simg + I.strOff);
+        int4* sd = reinterpret_cast<int4*>(u);
+        const int ns = int(size_t(I.strCount) * sizeof(uint16_t) / 16);
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) sd[i] = __ldg(ss + i);
+        const double* X = inv + I.invOffset;
+        for (int i = threadIdx.x; i < nc * nc; i += blockDim.x) sinv[i] = __ldg(X + i);
+    }
+    pdl_wait();
+    if (st != nullptr && sys_idle(st[I.sys], flag)) return;  // uniform over the CTA
+    const int f = I.first, c = I.coarsest;
+    {
+        const T* rg = lev[f].r + I.rowStart[f];
+        T* r = t + I.tR[f];
+        for (int i = threadIdx.x; i < I.n[f]; i += blockDim.x) r[i] = __ldcg(rg + i);
+    }
+    __syncthreads();
+    // s -= a_ij v_j over row i's entries in order (ELL, column-major, local columns)
+    auto rowMinus = [](const T* A, const uint16_t* col, int len, int n, int i, const T* v, T s) -> T {
+        for (int q = 0; q < len; ++q) s -= A[q * n + i] * v[col[q * n + i]];
+        return s;
+    };
+    for (int k = f; k < c; ++k) {
+        const int n = I.n[k];
+        const T* A = t + I.tVal[k];
+        const uint16_t* col = u + I.uCol[k];
+        const uint16_t* rl = u + I.uRlen[k];
+        const T* D = t + I.tDiag[k];
+        const T* r = t + I.tR[k];
+        T* x = t + I.tX[k];
+        T* x2 = t + I.tX2[k];
+        // two pre-sweeps from zero (k_smooth_jacobi MODE 1, then MODE 0)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const T v = r[i] / D[i];
+            x2[i] = omega == T(1) ? v : omega * v;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const T v = rowMinus(A, col, rl[i], n, i, x2, r[i]) / D[i];
+            x[i] = omega == T(1) ? v : x2[i] + omega * (v - x2[i]);
+        }
+        __syncthreads();
+        // residual (k_residual) into x2, then the restriction (k_restrict) into the next level's r
+        for (int i = threadIdx.x; i < n; i += blockDim.x) x2[i] = rowMinus(A, col, rl[i], n, i, x, r[i] - D[i] * x[i]);
+        __syncthreads();
+        const uint16_t* cp = u + I.uCptr[k];
+        const uint16_t* ch = u + I.uChild[k];
+        T* rn = t + I.tR[k + 1];
+        for (int R = threadIdx.x; R < I.n[k + 1]; R += blockDim.x) {
+            T s = T(0);
+            for (int q = cp[R]; q < cp[R + 1]; ++q) s += x2[ch[q]];
+            rn[R] = s;
+        }
+        __syncthreads();
+    }
+    {
+        // coarsest level: x = inv * r (k_coarse_apply)
+        const T* r = t + I.tR[c];
+        T* x = t + I.tX[c];
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            double g = 0.0;
+            for (int j = 0; j < nc; ++j) g += sinv[i * nc + j] * (double)r[j];
+            x[i] = (T)g;
+        }
+        for (int i = nc + threadIdx.x; i < I.n[c]; i += blockDim.x) x[i] = T(0);
+    }
+    for (int k = c - 1; k >= f; --k) {
+        __syncthreads();
+        const int n = I.n[k];
+        const T* D = t + I.tDiag[k];
+        const T* A = t + I.tVal[k];
+        const uint16_t* col = u + I.uCol[k];
+        const uint16_t* rl = u + I.uRlen[k];
+        const T* r = t + I.tR[k];
+        T* x = t + I.tX[k];
+        T* x2 = t + I.tX2[k];
+        const uint16_t* agg = u + I.uAgg[k];
+        const T* xc = t + I.tX[k + 1];
+        // the coarse-grid correction, then the two post-sweeps (x -> x2 -> x)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int a = agg[i];
+            if (a != 0xffff) x[i] += xc[a];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const T v = rowMinus(A, col, rl[i], n, i, x, r[i]) / D[i];
+            x2[i] = omega == T(1) ? v : x[i] + omega * (v - x[i]);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const T v = rowMinus(A, col, rl[i], n, i, x2, r[i]) / D[i];
+            x[i] = omega == T(1) ? v : x2[i] + omega * (v - x2[i]);
+        }
+    }
+    __syncthreads();
+    {
+        T* xg = lev[f].x + I.rowStart[f];
+        const T* x = t + I.tX[f];
+        for (int i = threadIdx.x; i < I.n[f]; i += blockDim.x) xg[i] = x[i];
+    }
+}
+
 // ------------------------------------------------------------------ per-solve setup
 // Level-0 diagonal in solver order (padding rows get 1 so smoothers leave them at 0).
 template <class T>

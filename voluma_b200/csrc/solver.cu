@@ -16,6 +16,7 @@
 #include "dilu.cuh"
 #include "krylov.cuh"
 #include "solver.h"
+#include "tailplan.h"
 
 namespace vlm {
 
@@ -188,6 +189,10 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     if (const char* cl = std::getenv("VLM_TAIL_CLUSTER")) tailCl_ = std::atoi(cl);
     if (const char* mr = std::getenv("VLM_TAIL_ROWS")) tailMaxRows_ = std::atoll(mr);
     if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) tailFullRows_ = std::atoll(fr);
+    // VLM_BOX_FUSED=1: a box level-0 sweep as one fused launch instead of the two colour launches
+    if (const char* f = std::getenv("VLM_BOX_FUSED")) sweepFused_ = f[0] == '1';
+    // VLM_TAIL_SMEM=0: the coarse tail reads its operands from global memory
+    if (const char* f = std::getenv("VLM_TAIL_SMEM")) tailSmemAllowed_ = f[0] != '0';
     if (const char* f = std::getenv("VLM_FUSE_PRE")) fusePre_ = std::atoll(f);
     if (const char* f = std::getenv("VLM_FUSE_RESTRICT")) fuseRestrict_ = std::atoll(f);
     if (const char* f = std::getenv("VLM_FUSE_POST")) fusePost_ = std::atoll(f);
@@ -242,8 +247,13 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
             D.r.zero(stream_);
             D.x.zero(stream_);
         }
-        // host-side plan data no longer needed on the device path
-        std::vector<int32_t>().swap(P.col);
+        // host-side plan data no longer needed on the device path; the column indices of levels a
+        // shared-memory tail may take (below level 0, every system under 16-bit local indices) stay
+        // for re-planning the tail (setTail)
+        bool tailLevel = k > 0;
+        for (size_t b = 0; tailLevel && b + 1 < P.sysRow.size(); ++b)
+            if (P.sysRow[b + 1] - P.sysRow[b] >= 0xffff) tailLevel = false;
+        if (!tailLevel) std::vector<int32_t>().swap(P.col);
         std::vector<int32_t>().swap(P.src);
     }
     lu_.resize(size_t(std::max(plan_.invTotal, 1)));
@@ -538,6 +548,13 @@ void DeviceBatch::setupMatrix(const double* diag, const double* upper, const dou
         VLM_CUDA(cudaGetLastError());
         ++tl_launches;
     }
+    if (tailOn_ && tailSmem_) {
+        // the shared-memory tail's value images of this solve's coarse levels
+        const int nv = int(tailCodes_.size());
+        VLM_LAUNCH(k_tail_values<double>, nblk(nv), 256, s, nv, tailCodes_.get(), tail64_.get(), tailVal64_.get());
+        if (mixed && tail32_.size() != 0)
+            VLM_LAUNCH(k_tail_values<float>, nblk(nv), 256, s, nv, tailCodes_.get(), tail32_.get(), tailVal32_.get());
+    }
 }
 
 // ====================================================================== V-cycle
@@ -605,7 +622,31 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
         if (pre && !two) VLM_LAUNCH(k_zero_rows<T>, rows.n, kRowsPerCta, s, D.ch(rows), x, st, flag);
         const bool boxK = k == 0 && boxOn_;
         const T* bc = LV<T>::bcoef(D);
-        for (int sweep = 0; sweep < 2; ++sweep)
+        // live sweep timing (eager solves only): an event pair around each level-0 sweep
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (timeSweeps_ && k == 0) VLM_CUDA(cudaStreamIsCapturing(s, &cap));
+        const bool timed = timeSweeps_ && k == 0 && cap == cudaStreamCaptureStatusNone;
+        cudaEvent_t te0 = nullptr;
+        auto sweepEnd = [&] {
+            if (!timed) return;
+            cudaEvent_t te1 = nullptr;
+            VLM_CUDA(cudaEventCreate(&te1));
+            VLM_CUDA(cudaEventRecord(te1, s));
+            sweepEvents_.push_back({te0, te1});
+        };
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            if (timed) {
+                VLM_CUDA(cudaEventCreate(&te0));
+                VLM_CUDA(cudaEventRecord(te0, s));
+            }
+            if (boxK && two) {
+                const ChunkList& la = head ? (pre ? D.headFwd[0] : D.headRev[0]) : (pre ? D.fwd[0] : D.rev[0]);
+                const ChunkList& lb = head ? (pre ? D.headFwd[1] : D.headRev[1]) : (pre ? D.fwd[1] : D.rev[1]);
+                if (recordFusedSweep<T>(la, lb, r, x, pre, sweep, agg, xc)) {
+                    sweepEnd();
+                    continue;
+                }
+            }
             for (int t = 0; t < D.nSteps; ++t) {
                 const ChunkList& l = head ? (pre ? D.headFwd[t] : D.headRev[t]) : (pre ? D.fwd[t] : D.rev[t]);
                 if (boxK) {
@@ -640,6 +681,85 @@ void DeviceBatch::recordSmooth(int k, const T* r, T* x, SmootherKind sm, bool pr
                     VLM_LAUNCH((k_smooth_gs<T, 0>), l.n, kRowsPerCta, s, D.ch(l), S, val, diag, r, x, agg, xc, st,
                                flag);
             }
+            sweepEnd();
+        }
+    }
+}
+
+void DeviceBatch::setSweepTiming(bool on) {
+    VLM_CUDA(cudaStreamSynchronize(stream_));
+    collectSweepTimes();
+    timeSweeps_ = on;
+    sweepMs_ = 0.0;
+    sweepCount_ = 0;
+}
+
+// Adds the recorded level-0 sweep times (the stream has been synchronised) and frees the events.
+void DeviceBatch::collectSweepTimes() {
+    for (auto& e : sweepEvents_) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) {
+            sweepMs_ += ms;
+            ++sweepCount_;
+        }
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    sweepEvents_.clear();
+}
+
+// One red-black sweep of a single box system's level 0 as one launch (k_box_sweep4): forward colours
+// for pre-smoothing, reversed for post-smoothing; the first sweep starts from zero (pre) or carries
+// the coarse-grid correction (post).  False when the layout does not qualify (the caller then
+// launches the two colour steps).
+template <class T>
+bool DeviceBatch::recordFusedSweep(const ChunkList& la, const ChunkList& lb, const T* r, T* x, bool pre, int sweep,
+                                   const int32_t* agg, const T* xc) {
+    DevLevel& D = L_[0];
+    if (!sweepFused_ || plan_.nsys != 1 || D.nSteps != 2 || la.n == 0 || lb.n == 0) return false;
+    int g = 0;
+    const BoxRows RA = boxRows(D, la, &g);
+    const BoxRows RB = boxRows(D, lb, &g);
+    if (RA.ch != nullptr || RB.ch != nullptr || RA.one.H % 4 != 0) return false;
+    const int nA = (RA.end - RA.begin + kSweepPiece - 1) / kSweepPiece;
+    const int nB = (RB.end - RB.begin + kSweepPiece - 1) / kSweepPiece;
+    if (sweepSync_.size() == 0) {
+        int dev = 0, sms = 0, per = 0;
+        VLM_CUDA(cudaGetDevice(&dev));
+        VLM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_box_sweep4<T, 0>, kRowsPerCta, 0));
+        sweepGrid_ = sms * std::max(1, per);
+        sweepSync_.resize(1);
+        sweepSync_.zero(stream_);
+        sweepDone_.resize(size_t(std::max(nA, nB)));
+        sweepDone_.zero(stream_);
+    }
+    if (sweepDone_.size() < size_t(std::max(nA, nB))) return false;
+    const int grid = std::min(sweepGrid_, nA + nB);
+    const T* bc = LV<T>::bcoef(D);
+    cudaStream_t s = stream_;
+    const int mode = sweep == 0 ? (pre ? 1 : 2) : 0;
+    if (mode == 1)
+        VLM_LAUNCH((k_box_sweep4<T, 1>), grid, kRowsPerCta, s, RA.one, RA.begin, RA.end, RB.begin, RB.end, bc, D.nrows,
+                   LV<T>::diag(D), r, x, agg, xc, sweepSync_.get(), sweepDone_.get());
+    else if (mode == 2)
+        VLM_LAUNCH((k_box_sweep4<T, 2>), grid, kRowsPerCta, s, RA.one, RA.begin, RA.end, RB.begin, RB.end, bc, D.nrows,
+                   LV<T>::diag(D), r, x, agg, xc, sweepSync_.get(), sweepDone_.get());
+    else
+        VLM_LAUNCH((k_box_sweep4<T, 0>), grid, kRowsPerCta, s, RA.one, RA.begin, RA.end, RB.begin, RB.end, bc, D.nrows,
+                   LV<T>::diag(D), r, x, agg, xc, sweepSync_.get(), sweepDone_.get());
+    return true;
+}
+
+// A wait of the fused sweep that gave up leaves a non-zero error word.
+void DeviceBatch::checkSweepError() {
+    if (sweepSync_.size() == 0) return;
+    SweepSync h = {};
+    VLM_CUDA(cudaMemcpy(&h, sweepSync_.get(), sizeof h, cudaMemcpyDeviceToHost));
+    if (h.err != 0) {
+        VLM_CUDA(cudaMemsetAsync(&sweepSync_.get()->err, 0, sizeof(unsigned), stream_));
+        VLM_CUDA(cudaStreamSynchronize(stream_));
+        throw Error(VLM_ERR_TIMEOUT, "fused level-0 sweep: a wait for another CTA's piece gave up");
     }
 }
 
@@ -713,6 +833,29 @@ void DeviceBatch::recordTail(const T* r0, T* x0, int flag, bool jacobi0) {
     const TailLevel<T>* tab = std::is_same<T, float>::value ? (const TailLevel<T>*)tail32_.get()
                                                              : (const TailLevel<T>*)tail64_.get();
     if (!tab) throw Error(VLM_ERR_CUDA, "internal: coarse-tail table missing");
+    if (tailSmem_) {
+        // every operand in shared memory, one CTA per system
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(tailImg_.size()));
+        cfg.blockDim = dim3(unsigned(kTailThreads));
+        cfg.dynamicSmemBytes = std::is_same<T, float>::value ? tailSmem32_ : tailSmem64_;
+        cfg.stream = stream_;
+        cudaLaunchAttribute at[1];
+        int na = 0;
+        if (pdlEnabled()) {
+            at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[na].val.programmaticStreamSerializationAllowed = 1;
+            ++na;
+        }
+        cfg.attrs = at;
+        cfg.numAttrs = unsigned(na);
+        const T* vimg = std::is_same<T, float>::value ? (const T*)tailVal32_.get() : (const T*)tailVal64_.get();
+        VLM_CUDA(cudaLaunchKernelEx(&cfg, k_vcycle_tail_smem<T>, (const TailImg*)tailImg_.get(), vimg,
+                                    (const uint16_t*)tailStr_.get(), tab, (const double*)inv_.get(), T(jacobiOmega_),
+                                    (const SysState*)st_.get(), flag));
+        ++tl_launches;
+        return;
+    }
     // one CTA, or one thread-block cluster of tailCl_ CTAs, per system
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(tailSys_.size()) * unsigned(tailCl_));
@@ -813,6 +956,35 @@ void DeviceBatch::planTail() {
     }
     tailSys_.upload(ts, stream_);
     tailOn_ = true;
+    planTailSmem(ts);
+}
+
+// Images of the shared-memory tail (buildTailImages): used when every tail system qualifies.
+void DeviceBatch::planTailSmem(const std::vector<TailSys>& ts) {
+    tailSmem_ = false;
+    if (!tailSmemAllowed_ || tailCl_ != 1) return;
+    int dev = 0, optin = 0;
+    VLM_CUDA(cudaGetDevice(&dev));
+    VLM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int budget = optin - int(sizeof(TailImg)) - 256;  // the kernel's static descriptor copy
+    TailImages im;
+    if (!buildTailImages(plan_, ts, size_t(budget), im)) return;
+    tailImg_.upload(im.imgs, stream_);
+    tailCodes_.upload(im.codes, stream_);
+    tailStr_.upload(im.str, stream_);
+    tailVal64_.resize(im.codes.size());
+    tailVal32_.resize(im.codes.size());
+    tailSmem64_ = im.bytes64;
+    tailSmem32_ = im.bytes32;
+    // the opt-in limit is a per-function setting: raised once to what the kernels may use
+    static const bool raised = [budget] {
+        VLM_CUDA(cudaFuncSetAttribute(k_vcycle_tail_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+        VLM_CUDA(cudaFuncSetAttribute(k_vcycle_tail_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+        return true;
+    }();
+    (void)raised;
+    VLM_CUDA(cudaStreamSynchronize(stream_));  // the host vectors are locals
+    tailSmem_ = true;
 }
 
 void DeviceBatch::recordPrecond(PrecondKind pk, SmootherKind sm, const double* r, double* w, bool f32) {
@@ -912,9 +1084,15 @@ void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
     }
     if (boxOn_) {
         int g = 0;
-        VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, boxRows(D0, D0.all, &g),
-                   (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)p_.get(),
-                   Ap_.get(), red(), st_.get());
+        const BoxRows R = boxRows(D0, D0.all, &g);
+        if (R.ch == nullptr && R.one.H % 4 == 0)
+            VLM_LAUNCH((k_box_pcg_spmv4<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, R.one,
+                       (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(),
+                       (const double*)p_.get(), Ap_.get(), red(), st_.get());
+        else
+            VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, R,
+                       (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(),
+                       (const double*)p_.get(), Ap_.get(), red(), st_.get());
     }
     else
         VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(),
@@ -939,9 +1117,15 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
     VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
     if (boxOn_) {
         int g = 0;
-        VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, boxRows(D0, D0.all, &g),
-                   (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(), (const float*)p32_.get(),
-                   Ap32_.get(), red(), st_.get());
+        const BoxRows R = boxRows(D0, D0.all, &g);
+        if (R.ch == nullptr && R.one.H % 4 == 0)
+            VLM_LAUNCH((k_box_pcg_spmv4<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, R.one,
+                       (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(),
+                       (const float*)p32_.get(), Ap32_.get(), red(), st_.get());
+        else
+            VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, R,
+                       (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(),
+                       (const float*)p32_.get(), Ap32_.get(), red(), st_.get());
     }
     else
         VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(),
@@ -1096,6 +1280,7 @@ void DeviceBatch::diluFactor(const double* upper, const double* lower) {
 }
 
 void DeviceBatch::clearLevelError() {
+    if (sweepSync_.size() != 0) VLM_CUDA(cudaMemsetAsync(&sweepSync_.get()->err, 0, sizeof(unsigned), stream_));
     if (!dilu_) return;
     dilu_->err.zero(stream_);
     dilu_->bars.zero(stream_);
@@ -1417,7 +1602,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     const SolveKey key{sk, pk, sm, prec, exact_, relax ? ctrl.nSweeps : 0, boxOn_};
     int64_t eagerLaunches = 0;
     GraphExec* Gp = nullptr;
-    if (useGraphs_) {
+    if (useGraphs_ && !(timeSweeps_ && !embedding_)) {
         Gp = &graphFor(key);
         if (embedding_)
             embedSolve(key);
@@ -1446,6 +1631,8 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
             VLM_CUDA(cudaMemsetAsync(sto, 0, sizeof(int), s));
         if (levelSchedule)
             VLM_CUDA(cudaMemcpyAsync(sto + 1, dilu_->err.get(), sizeof(int), cudaMemcpyDeviceToDevice, s));
+        else if (sweepSync_.size() != 0)
+            VLM_CUDA(cudaMemcpyAsync(sto + 1, &sweepSync_.get()->err, sizeof(int), cudaMemcpyDeviceToDevice, s));
         else
             VLM_CUDA(cudaMemsetAsync(sto + 1, 0, sizeof(int), s));
         return;
@@ -1467,6 +1654,8 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     if (pk == PrecondKind::GAMG && coarseStatus == VLM_ERR_SINGULAR)
         throw Error(VLM_ERR_SINGULAR, "GAMG: singular coarsest matrix");
     if (levelSchedule) checkLevelError();
+    checkSweepError();
+    collectSweepTimes();
     perfOut.resize(size_t(plan_.nsys));
     for (int bpos = 0; bpos < plan_.nsys; ++bpos) {
         const SysState& q = hostState_[bpos];
@@ -1615,16 +1804,29 @@ double DeviceBatch::profileKernel(const std::string& fullName, int reps, double*
     cudaEvent_t e0, e1;
     VLM_CUDA(cudaEventCreate(&e0));
     VLM_CUDA(cudaEventCreate(&e1));
-    const bool f32 = name.size() > 2 && name.substr(name.size() - 2) == "32";
+    // "<kernel>_steps": a box level-0 sweep as its two colour launches instead of the fused launch
+    const std::string stepsSuffix = "_steps";
+    const bool steps = name.size() > stepsSuffix.size() &&
+                       name.compare(name.size() - stepsSuffix.size(), stepsSuffix.size(), stepsSuffix) == 0;
+    const std::string base = steps ? name.substr(0, name.size() - stepsSuffix.size()) : name;
+    const bool f32 = base.size() > 2 && base.substr(base.size() - 2) == "32";
     const double sz = f32 ? 4.0 : 8.0;
     if (f32 && D0.val32.size() == 0) throw Error(VLM_ERR_BAD_ARG, "run a mixed-precision solve first");
     std::function<void()> run;
     if (name == "amul64") {
         run = [&] { VLM_LAUNCH(k_amul, D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), x_.get(), w_.get()); };
         *bytesPerLaunch = sz * 3 * N + sz * F + 8 * F;
-    } else if ((name == "smooth64" || name == "smooth32") && boxOn_) {
-        // box level 0: each face coefficient once, no column indices
+    } else if ((base == "smooth64" || base == "smooth32") && boxOn_) {
+        // box level 0: each face coefficient once, no column indices; one fused launch per sweep
+        // unless "_steps" asks for the colour launches
         run = [&] {
+            if (!steps) {
+                const bool done = f32 ? recordFusedSweep<float>(D0.fwd[0], D0.fwd[1], r32_.get(), w32_.get(), true, 1,
+                                                                nullptr, nullptr)
+                                      : recordFusedSweep<double>(D0.fwd[0], D0.fwd[1], r_.get(), w_.get(), true, 1,
+                                                                 nullptr, nullptr);
+                if (done) return;
+            }
             for (int t = 0; t < D0.nSteps; ++t) {
                 int g = 0;
                 const BoxRows R = boxRows(D0, D0.fwd[t], &g);
@@ -1657,8 +1859,11 @@ double DeviceBatch::profileKernel(const std::string& fullName, int reps, double*
         // the PCG product with its fused dot (the FP64 Krylov recurrence's largest kernel)
         run = [&] {
             int g = 0;
-            if (boxOn_)
-                VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), boxRows(D0, D0.all, &g), (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
+            const BoxRows R = boxOn_ ? boxRows(D0, D0.all, &g) : BoxRows{};
+            if (boxOn_ && R.ch == nullptr && R.one.H % 4 == 0)
+                VLM_LAUNCH((k_box_pcg_spmv4<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), R.one, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
+            else if (boxOn_)
+                VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), R, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
             else
                 VLM_LAUNCH((k_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), D0.sell(), D0.val.get(), D0.diag.get(), r_.get(), w_.get(), red(), st_.get());
         };

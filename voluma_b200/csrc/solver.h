@@ -157,6 +157,34 @@ public:
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
     // solve); returns ms per launch and the algorithmic bytes one launch moves.
     double profileKernel(const std::string& name, int reps, double* bytesPerLaunch);
+    // fused two-colour level-0 sweep (k_box_sweep4): ticket counters and per-piece done stamps.
+    // Off by default: at 128^3 one fused launch measured 33 us per sweep against 17 us for the two
+    // colour launches (each CTA serialises ticket, dependency wait and fence per piece)
+    bool sweepFused_ = false;
+    int sweepGrid_ = 0;
+    DBuf<SweepSync> sweepSync_;
+    DBuf<unsigned> sweepDone_;
+    template <class T>
+    bool recordFusedSweep(const ChunkList& la, const ChunkList& lb, const T* r, T* x, bool pre, int sweep,
+                          const int32_t* agg, const T* xc);
+    void checkSweepError();
+    // live timing of the level-0 sweeps: solves run eagerly with CUDA events around every level-0
+    // sweep (setSweepTiming); the stream's own order, so each sweep meets the cache state the solve
+    // leaves it
+    bool timeSweeps_ = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sweepEvents_;
+    double sweepMs_ = 0.0;
+    int64_t sweepCount_ = 0;
+    void collectSweepTimes();
+
+public:
+    void setSweepTiming(bool on);
+    void sweepTiming(double* msTotal, int64_t* count) const {
+        *msTotal = sweepMs_;
+        *count = sweepCount_;
+    }
+
+private:
     DBuf<int4> flush_;       // profileKernel's L2-evicting read buffer (allocated on first use)
     DBuf<int> flushSink_;
 
@@ -215,6 +243,15 @@ private:
     int tailMaxFirst_ = 0;      // head levels: k < tailMaxFirst_
     std::vector<int> tailFirst_;
     DBuf<TailSys> tailSys_;
+    // shared-memory tail (k_vcycle_tail_smem): used when every tail system's levels fit
+    bool tailSmem_ = false, tailSmemAllowed_ = true;
+    DBuf<TailImg> tailImg_;
+    DBuf<int32_t> tailCodes_;            // value-image gather codes (k_tail_values)
+    DBuf<uint16_t> tailStr_;             // structure images
+    DBuf<double> tailVal64_;
+    DBuf<float> tailVal32_;
+    size_t tailSmem64_ = 0, tailSmem32_ = 0;  // dynamic shared memory per CTA
+    void planTailSmem(const std::vector<TailSys>& ts);
     int tailCl_ = 1;                     // CTAs of the cluster that runs one system's tail (the tuner may widen it)
     int64_t tailMaxRows_ = 0;            // levels of at most this many rows go to the tail (0: scaled default)
     int64_t tailFullRows_ = 0;           // systems of at most this many level-0 rows: whole V-cycle there
