@@ -914,10 +914,10 @@ def run_ours(args, rank, world, local):
         return vb.SolverControls("PCG", "GAMG", 0.0, REL_TOL, 1000, smoother=args.smoother,
                                  precision="mixed" if prec == "mixed" else "")
 
-    def device_solve(prec):
+    def device_solve(prec, on=None):
         with torch.cuda.stream(ext):
             d_x.zero_()
-        return vb.solve_ldu_device(mesh, d_diag.data_ptr(), d_up.data_ptr(), 0, d_b.data_ptr(), d_x.data_ptr(),
+        return vb.solve_ldu_device(on or mesh, d_diag.data_ptr(), d_up.data_ptr(), 0, d_b.data_ptr(), d_x.data_ptr(),
                                    ctrl(prec))
 
     def barrier():
@@ -959,6 +959,33 @@ def run_ours(args, rank, world, local):
     device_solve("fp64")
     x64 = d_x.cpu().numpy()
     err_vs_fp64 = float(np.linalg.norm(x_mixed - x64) / np.linalg.norm(x64))
+
+    # the same solves on the device-built hierarchy (parallel matching, vlm_mesh_register_ex):
+    # registration time and the solve rates beside the reference hierarchy's
+    barrier()
+    t_reg = time.perf_counter()
+    mesh_dev = vb.Mesh.from_arrays(m, ctx=ctx, agglomeration="device")
+    t_reg = time.perf_counter() - t_reg
+    dev_modes = {"registration_s": t_reg}
+    for prec in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            device_solve(prec, mesh_dev)
+        barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        perfs = []
+        for e0, e1 in ev:
+            with torch.cuda.stream(ext):
+                d_x.zero_()
+            e0.record(ext)
+            perfs.append(vb.solve_ldu_device(mesh_dev, d_diag.data_ptr(), d_up.data_ptr(), 0, d_b.data_ptr(),
+                                             d_x.data_ptr(), ctrl(prec)))
+            e1.record(ext)
+        barrier()
+        tot = max_over_ranks(float(sum(e0.elapsed_time(e1) for e0, e1 in ev)), world, dev)
+        dev_modes[prec] = dict(value=aggregate_rate(args.steps, world, tot / 1e3), ms_per_step=tot / args.steps,
+                               iterations=int(np.median([p.iterations for p in perfs])),
+                               converged=all(p.converged for p in perfs))
+    mesh_dev.close()
 
     # e2e: host pinned buffers through vlm_ldu_solve (H2D diag/upper/b/x, D2H x inside the timed region)
     h_diag = torch.from_numpy(diag).pin_memory().numpy()
@@ -1009,7 +1036,8 @@ def run_ours(args, rank, world, local):
         "config": pressure_config(args.n, world, args.smoother),
         "modes": {"mixed": mx, "fp64": modes["fp64"],
                   "speedup_mixed_vs_fp64": modes["fp64"]["ms_per_step"] / mx["ms_per_step"],
-                  "mixed_rel_l2_vs_fp64": err_vs_fp64},
+                  "mixed_rel_l2_vs_fp64": err_vs_fp64,
+                  "device_agglomeration": dev_modes},
         "e2e": {"value": world * args.steps / (e2e_tot / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(8 * (n + nI + n + n)), "d2h_bytes_per_step": int(8 * n),
                 "p99_ms": float(np.percentile(e2e_ms, 99))},

@@ -133,6 +133,17 @@ vlm_status vlm_mesh_register(vlm_ctx* ctx, const vlm_mesh_desc* desc, int32_t me
  * followed by every system's boundary faces; perf outputs have n_systems entries (per pass). */
 vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t n_systems, const vlm_mesh_desc* descs,
                                    int32_t merge_levels, vlm_mesh** out);
+/* Registration flags (the _ex forms; 0 = the plain entry points).
+ * VLM_MESH_DEVICE_AGGLOMERATION: the GAMG hierarchy is built on the device by a parallel handshake
+ * matching of the heaviest couplings (magSf*ndc, GAMG.cpp:215) in place of the reference's
+ * sequential pairwise pass (GAMG.cpp:40-94, buildHierarchy): the same level structure, other
+ * aggregates (so iteration counts differ from the reference's by the aggregation's quality), for
+ * meshes whose registration time matters (serving unseen sizes).  No reference counterpart. */
+#define VLM_MESH_DEVICE_AGGLOMERATION 1
+vlm_status vlm_mesh_register_ex(vlm_ctx* ctx, const vlm_mesh_desc* desc, int32_t merge_levels, int32_t flags,
+                                vlm_mesh** out);
+vlm_status vlm_mesh_register_batch_ex(vlm_ctx* ctx, int32_t n_systems, const vlm_mesh_desc* descs,
+                                      int32_t merge_levels, int32_t flags, vlm_mesh** out);
 vlm_status vlm_mesh_systems(vlm_mesh* mesh, int32_t* n_systems, int64_t* n_cells, int64_t* n_internal_faces,
                             int64_t* n_faces);
 vlm_status vlm_mesh_release(vlm_mesh* mesh);
@@ -449,6 +460,8 @@ typedef struct {
     double residual_tol;        /* steady: convergence tolerance (fvmFlow residualTol) */
     double arrival;             /* server clock (s) at which the request arrives */
     int64_t device_bytes;       /* admission estimate (0: vlm_flow_request_bytes) */
+    int32_t mesh_flags;         /* registration flags of the request's mesh (vlm_mesh_register_ex): 0, or
+                                   VLM_MESH_DEVICE_AGGLOMERATION to build its GAMG hierarchy on the device */
 } vlm_flow_request;
 
 typedef struct {

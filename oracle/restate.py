@@ -17,7 +17,8 @@ _lib = None
 
 
 class GamgOpts(C.Structure):
-    _fields_ = [("smoother", C.c_int), ("omega", C.c_double), ("coarse", C.c_int), ("mergeLevels", C.c_int)]
+    _fields_ = [("smoother", C.c_int), ("omega", C.c_double), ("coarse", C.c_int), ("mergeLevels", C.c_int),
+                ("matching", C.c_int)]
 
 
 def build():
@@ -36,6 +37,8 @@ def lib():
         L.vo_amul.argtypes = [C.c_int, C.c_int, P, P, P, P, P, P, P]
         L.vo_hier_build.restype = P
         L.vo_hier_build.argtypes = [C.c_int, C.c_int, P, P, P, P, C.c_int, C.c_int]
+        L.vo_hier_build_matching.restype = P
+        L.vo_hier_build_matching.argtypes = [C.c_int, C.c_int, P, P, P, P, C.c_int, C.c_int]
         L.vo_hier_free.argtypes = [P]
         L.vo_hier_nlevels.argtypes = [P]
         L.vo_hier_level.argtypes = [P, C.c_int, P, P, P, P, P, P, P]
@@ -62,8 +65,9 @@ def _i(a):
     return np.ascontiguousarray(a, np.int32)
 
 
-def opts(smoother="gs", omega=1.0, coarse=0, merge=2):
-    return GamgOpts(SMOOTHERS[smoother] if isinstance(smoother, str) else smoother, omega, coarse, merge)
+def opts(smoother="gs", omega=1.0, coarse=0, merge=2, matching=False):
+    return GamgOpts(SMOOTHERS[smoother] if isinstance(smoother, str) else smoother, omega, coarse, merge,
+                    int(matching))
 
 
 def exact_sum(v) -> float:
@@ -79,12 +83,14 @@ def amul(m, diag, upper, lower, x):
     return y
 
 
-def hierarchy(m, merge=2, n_coarsest=64, colours=False):
-    """buildHierarchy restated: list of dicts n, l, u, weight, agg, faceMap, faceFlip (+colour)."""
+def hierarchy(m, merge=2, n_coarsest=64, colours=False, matching=False):
+    """buildHierarchy restated (matching: the device agglomeration's parallel matching): list of
+    dicts n, l, u, weight, agg, faceMap, faceFlip (+colour)."""
     L = lib()
     nI = len(m["neighbour"])
-    h = L.vo_hier_build(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(m["magSf"])),
-                        _p(_d(m["ndc"])), merge, n_coarsest)
+    build = L.vo_hier_build_matching if matching else L.vo_hier_build
+    h = build(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(m["magSf"])),
+              _p(_d(m["ndc"])), merge, n_coarsest)
     out = []
     try:
         for k in range(L.vo_hier_nlevels(h)):
@@ -119,12 +125,12 @@ def gamg_apply(m, diag, upper, lower, r, smoother="gs", omega=1.0, coarse=0, mer
 
 
 def solve(m, diag, upper, lower, b, x0, solver="PCG", precond="diagonal", tol=0.0, rel_tol=1e-8, max_iter=1000,
-          min_iter=0, exact=False, smoother="gs", omega=1.0, coarse=0, merge=2, n_sweeps=1):
+          min_iter=0, exact=False, smoother="gs", omega=1.0, coarse=0, merge=2, n_sweeps=1, matching=False):
     """solveLdu restated (PCG, PBiCGStab, GaussSeidel, symGaussSeidel, Jacobi). Returns (x, perf dict)."""
     nI = len(m["neighbour"])
     x = np.ascontiguousarray(x0, np.float64).copy()
     perf = np.zeros(6)
-    o = opts(smoother, omega, coarse, merge)
+    o = opts(smoother, omega, coarse, merge, matching)
     st = lib().vo_solve_ex(m["n_cells"], nI, _p(_i(m["owner"][:nI])), _p(_i(m["neighbour"])), _p(_d(m["magSf"])),
                            _p(_d(m["ndc"])), _p(_d(diag)), _p(_d(upper)), _p(_d(lower)), _p(_d(b)), _p(x),
                            solver.encode(), precond.encode(), tol, rel_tol, max_iter, min_iter, n_sweeps, int(exact),

@@ -294,8 +294,156 @@ static vo_level agglomerate(vo_level* L) {
     return C;
 }
 
+/* The device agglomeration's parallel handshake matching (voluma_b200/csrc/aggl.cu), restated
+ * with synchronous rounds: every unpaired cell names its heaviest unpaired neighbour (weight, then
+ * the SplitMix64 hash of the cell pair, Steele, Lea and Flood, OOPSLA 2014), mutual names pair up,
+ * until no pair forms; a cell left alone joins its heaviest neighbour's aggregate, a cell without
+ * neighbours is an aggregate of its own; aggregates numbered by their first cell; coarse faces in
+ * (lower, upper) order with weights summed in fine-face order. */
+static uint64_t pair_hash(int a, int b) {
+    const uint32_t lo = (uint32_t)(a < b ? a : b), hi = (uint32_t)(a < b ? b : a);
+    uint64_t z = (((uint64_t)lo << 32) | hi) + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+static int heavier(double w, uint64_t h, double bw, uint64_t bh) { return w > bw || (w == bw && h > bh); }
+
+typedef struct {
+    uint64_t key;
+    int face;
+} keyface_t;
+
+static int cmp_keyface(const void* a, const void* b) {
+    const keyface_t* x = (const keyface_t*)a;
+    const keyface_t* y = (const keyface_t*)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->face < y->face ? -1 : (x->face > y->face ? 1 : 0);
+}
+
+static vo_level agglomerate_matching(vo_level* L) {
+    const int n = L->n;
+    int* match = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* pref = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int i = 0; i < n; ++i) match[i] = -1;
+    for (;;) {
+        for (int i = 0; i < n; ++i) {
+            int best = -1;
+            double bw = 0.0;
+            uint64_t bh = 0;
+            if (match[i] < 0)
+                for (int k = L->off[i]; k < L->off[i + 1]; ++k) {
+                    const int j = L->adjCell[k];
+                    if (match[j] >= 0) continue;
+                    const double w = L->weight[L->adjFace[k]];
+                    const uint64_t h = pair_hash(i, j);
+                    if (best < 0 || heavier(w, h, bw, bh)) {
+                        best = j;
+                        bw = w;
+                        bh = h;
+                    }
+                }
+            pref[i] = best;
+        }
+        int paired = 0;
+        for (int i = 0; i < n; ++i)
+            if (match[i] < 0 && pref[i] >= 0 && pref[pref[i]] == i) {
+                match[i] = pref[i];
+                ++paired;
+            }
+        if (paired == 0) break;
+    }
+    int* id = (int*)malloc(sizeof(int) * (size_t)(n + 1));
+    int nc = 0;
+    for (int i = 0; i < n; ++i) {
+        id[i] = nc;
+        const int lead = match[i] >= 0 ? (i < match[i]) : (L->off[i + 1] == L->off[i]);
+        nc += lead;
+    }
+    free(L->agg);
+    L->agg = (int*)malloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int i = 0; i < n; ++i) {
+        const int m = match[i];
+        if (m >= 0) {
+            L->agg[i] = id[i < m ? i : m];
+        } else if (L->off[i + 1] == L->off[i]) {
+            L->agg[i] = id[i];
+        } else {
+            int best = -1;
+            double bw = 0.0;
+            uint64_t bh = 0;
+            for (int k = L->off[i]; k < L->off[i + 1]; ++k) {
+                const int j = L->adjCell[k];
+                const double w = L->weight[L->adjFace[k]];
+                const uint64_t h = pair_hash(i, j);
+                if (best < 0 || heavier(w, h, bw, bh)) {
+                    best = j;
+                    bw = w;
+                    bh = h;
+                }
+            }
+            const int mb = match[best];
+            L->agg[i] = id[best < mb ? best : mb];
+        }
+    }
+    free(match);
+    free(pref);
+    free(id);
+    vo_level C;
+    memset(&C, 0, sizeof C);
+    C.n = nc;
+    free(L->faceMap);
+    free(L->faceFlip);
+    const size_t nfa = (size_t)(L->nf ? L->nf : 1);
+    L->faceMap = (int*)malloc(sizeof(int) * nfa);
+    L->faceFlip = (signed char*)calloc(nfa, 1);
+    C.l = (int*)malloc(sizeof(int) * nfa);
+    C.u = (int*)malloc(sizeof(int) * nfa);
+    C.weight = (double*)malloc(sizeof(double) * nfa);
+    keyface_t* kf = (keyface_t*)malloc(sizeof(keyface_t) * nfa);
+    int m = 0;
+    for (int f = 0; f < L->nf; ++f) {
+        L->faceMap[f] = -1;
+        const int a = L->agg[L->l[f]], b = L->agg[L->u[f]];
+        if (a == b) continue;
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        kf[m].key = ((uint64_t)(uint32_t)lo << 32) | (uint64_t)(uint32_t)hi;
+        kf[m].face = f;
+        ++m;
+    }
+    qsort(kf, (size_t)m, sizeof(keyface_t), cmp_keyface);
+    for (int k = 0; k < m; ++k) {
+        if (k == 0 || kf[k].key != kf[k - 1].key) {
+            C.l[C.nf] = (int)(kf[k].key >> 32);
+            C.u[C.nf] = (int)(kf[k].key & 0xffffffffu);
+            C.weight[C.nf] = 0.0;
+            C.nf++;
+        }
+        const int cf = C.nf - 1, f = kf[k].face;
+        L->faceMap[f] = cf;
+        L->faceFlip[f] = (signed char)(L->agg[L->l[f]] != C.l[cf]);
+        C.weight[cf] += L->weight[f];
+    }
+    free(kf);
+    return C;
+}
+
+static vo_hier* hier_build(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
+                           int mergeLevels, int nCoarsest, vo_level (*pass)(vo_level*));
+
 vo_hier* vo_hier_build(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
                        int mergeLevels, int nCoarsest) {
+    return hier_build(n, nf, own, nei, magSf, ndc, mergeLevels, nCoarsest, agglomerate);
+}
+
+vo_hier* vo_hier_build_matching(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
+                                int mergeLevels, int nCoarsest) {
+    return hier_build(n, nf, own, nei, magSf, ndc, mergeLevels, nCoarsest, agglomerate_matching);
+}
+
+static vo_hier* hier_build(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
+                           int mergeLevels, int nCoarsest, vo_level (*pass)(vo_level*)) {
     if (mergeLevels < 1) mergeLevels = 1;
     if (nCoarsest <= 0) nCoarsest = 64;
     vo_hier* H = (vo_hier*)calloc(1, sizeof(vo_hier));
@@ -320,10 +468,10 @@ vo_hier* vo_hier_build(int n, int nf, const int* own, const int* nei, const doub
         vo_level* F = &H->lev[H->nL - 1];
         const int nF = F->n;
         if (nF <= nCoarsest) break;
-        vo_level C = agglomerate(F);
+        vo_level C = pass(F);
         for (int k = 1; k < mergeLevels && C.n > nCoarsest; ++k) {
             build_adjacency(&C);
-            vo_level C2 = agglomerate(&C);
+            vo_level C2 = pass(&C);
             for (int i = 0; i < F->n; ++i) F->agg[i] = C.agg[F->agg[i]];
             for (int f = 0; f < F->nf; ++f) {
                 const int cf = F->faceMap[f];
@@ -708,7 +856,8 @@ static void gamg_vcycle(gamg_t* g, int lev, const double* r, double* x) {
 int vo_gamg_apply(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
                   const double* diag, const double* upper, const double* lower, const double* r, double* w,
                   const vo_gamg_opts* opt) {
-    vo_hier* H = vo_hier_build(n, nf, own, nei, magSf, ndc, opt->mergeLevels ? opt->mergeLevels : 2, 64);
+    vo_hier* H = (opt->matching ? vo_hier_build_matching : vo_hier_build)(n, nf, own, nei, magSf, ndc,
+                                                                           opt->mergeLevels ? opt->mergeLevels : 2, 64);
     gamg_t g;
     const int st = gamg_init(&g, H, diag, upper, lower ? lower : upper, opt);
     if (st == 0) gamg_vcycle(&g, 0, r, w);
@@ -927,7 +1076,8 @@ int vo_solve_ex(int n, int nf, const int* own, const int* nei, const double* mag
             P.rD = (double*)malloc(sizeof(double) * (size_t)n);
             for (int c = 0; c < n; ++c) P.rD[c] = 1.0 / diag[c];
         } else if (P.kind == 2) {
-            P.H = vo_hier_build(n, nf, own, nei, magSf, ndc, opt->mergeLevels ? opt->mergeLevels : 2, 64);
+            P.H = (opt->matching ? vo_hier_build_matching : vo_hier_build)(n, nf, own, nei, magSf, ndc,
+                                                                           opt->mergeLevels ? opt->mergeLevels : 2, 64);
             status = gamg_init(&P.g, P.H, diag, upper, lower, opt);
         } else if (P.kind == 3) {
             dilu_init(&P.d, n, nf, own, nei, diag, upper, lower);

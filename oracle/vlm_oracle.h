@@ -22,6 +22,9 @@ void vo_amul(int n, int nf, const int* own, const int* nei, const double* diag, 
 
 /* buildHierarchy (src/fvm/linalg/GAMG.cpp:15-94, 206-261), serial */
 typedef struct vo_hier vo_hier;
+/* the device agglomeration's parallel matching (voluma_b200/csrc/aggl.cu), restated */
+vo_hier* vo_hier_build_matching(int n, int nf, const int* own, const int* nei, const double* magSf,
+                                const double* ndc, int mergeLevels, int nCoarsest);
 vo_hier* vo_hier_build(int n, int nf, const int* own, const int* nei, const double* magSf, const double* ndc,
                        int mergeLevels, int nCoarsest);
 void vo_hier_free(vo_hier* h);
@@ -44,6 +47,7 @@ typedef struct {
     double omega;
     int coarse;
     int mergeLevels;
+    int matching;  /* 1: the hierarchy of the device agglomeration's parallel matching */
 } vo_gamg_opts;
 
 /* One V-cycle w = M^-1 r (GamgPreconditioner ctor + apply, GAMG.cpp:263-353, 403-449).

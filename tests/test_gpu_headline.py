@@ -36,3 +36,27 @@ def test_tgv128_gamg_pcg_matches_oracle(tgv128, precision):
     assert p.converged and po["converged"]
     assert abs(p.iterations - po["iterations"]) <= 1
     assert rel(x, oracle_iterate(m, d, up, b, x0, xo, po, p.iterations)) <= 1e-10
+
+
+@pytest.fixture(scope="module")
+def tgv128_device_agglomeration(tgv128):
+    m, d, up, b, x0 = tgv128[:5]
+    xo, po = ro.solve(m, d, up, None, b, x0, "PCG", "GAMG", 0.0, 1e-8, 1000, smoother="mcgs-jacobi", coarse=1,
+                      matching=True)
+    return xo, po, vb.Mesh.from_arrays(m, agglomeration="device")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tgv128_device_agglomeration_matches_oracle(tgv128, tgv128_device_agglomeration, precision):
+    """The same system on the device-built hierarchy (parallel matching) against the restatement of
+    that hierarchy and schedule: iterations +-1 (42 on both), relative L2 1e-10 at equal work."""
+    m, d, up, b, x0 = tgv128[:5]
+    xo, po, mesh = tgv128_device_agglomeration
+    x = x0.copy()
+    p = vb.solve_ldu(mesh, d, up, None, b, x, vb.SolverControls("PCG", "GAMG", 0.0, 1e-8, 1000, precision=precision))
+    assert p.converged and po["converged"]
+    assert abs(p.iterations - po["iterations"]) <= 1
+    if p.iterations != po["iterations"]:
+        xo, _ = ro.solve(m, d, up, None, b, x0, "PCG", "GAMG", 0.0, 0.0, p.iterations, smoother="mcgs-jacobi",
+                         coarse=1, matching=True)
+    assert rel(x, xo) <= 1e-10

@@ -79,3 +79,30 @@ def test_budget_serialises_and_slots_overlap():
     spans = sorted((res[i]["admitted"], res[i]["finished"]) for i in ids)
     assert spans[1][0] < spans[0][1] and spans[2][0] < spans[0][1]
     assert all(res[i]["status"] == 0 for i in ids)
+
+
+def test_device_agglomeration_requests_alone_and_in_the_mix():
+    """Requests whose meshes build their GAMG hierarchy on the device (mesh_flags): the same result
+    alone, in a mix with host-agglomerated requests, and as a Flow on a mesh registered the same way."""
+    n, re = SPECS[2]
+    m, case = cases.lid_cavity(n, re)
+    s = vb.Server(max_active=1)
+    rid = s.submit(m, case, max_iter=60, residual_tol=1e-12, agglomeration="device")
+    assert drain(s, 1)[rid]["status"] == 0
+    alone = s.fields(rid)
+    s.close()
+    s = vb.Server(max_active=3)
+    ids = submit_all(s)
+    did = s.submit(m, case, max_iter=60, residual_tol=1e-12, agglomeration="device")
+    res = drain(s, 4)
+    assert all(r["status"] == 0 for r in res.values())
+    for a, b in zip(s.fields(did), alone):
+        assert np.array_equal(a, b)
+    s.close()
+    fl = vb.Flow(vb.Mesh.from_arrays(m, agglomeration="device"), case)
+    fl.set_state(None, None)
+    for _ in range(60):
+        fl.step()
+    for a, b in zip(fl.state(), alone):
+        assert np.array_equal(a, b)
+    fl.close()

@@ -1,11 +1,15 @@
 """The oracle pinned against the reference: the C restatement (oracle/vlm_oracle.c) must reproduce
 the reference's own outputs stored in tests/golden/ bit for bit, and, where the reference library
 was built here (oracle/_ref), agree with it live on fresh inputs."""
+import os
+
 import numpy as np
 import pytest
 
 from conftest import golden_hierarchy, perf_dict
 from oracle import restate as ro
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def test_exact_sum_properties():
@@ -105,3 +109,34 @@ def test_oracle_live_against_reference():
         xr, pr = R.solve(d, up, None, b, np.zeros(M["n_cells"]), "PCG", prec, 0.0, 1e-9, 500)
         xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", prec, 0.0, 1e-9, 500)
         assert np.array_equal(xr, xo) and pr == po
+
+
+@pytest.mark.parametrize("name", ["periodic8", "walls7x5x3", "cavity16", "jitter10x8x6", "periodic24"])
+def test_matching_hierarchy_is_a_maximal_pairing(name):
+    """The parallel matching's restatement (the device agglomeration's definition): on every level
+    of every pass each aggregate is a pair of neighbours or a pair with cells that had no unpaired
+    neighbour left, every cell has one aggregate, coarse faces are the distinct aggregate pairs in
+    (lower, upper) order, and the coarse weights are the fine weights' sums."""
+    z = dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+    z["n_cells"] = int(z["sizes"][0])
+    H = ro.hierarchy(z, matching=True, merge=1)
+    for k in range(len(H) - 1):
+        L, C = H[k], H[k + 1]
+        agg = L["agg"]
+        assert agg.min() == 0 and agg.max() == C["n"] - 1
+        sizes = np.bincount(agg, minlength=C["n"])
+        assert sizes.min() >= 1
+        # coarse faces: sorted distinct pairs
+        keys = C["l"].astype(np.int64) * (1 << 32) + C["u"]
+        assert np.all(np.diff(keys) > 0) and np.all(C["l"] < C["u"])
+        a, b = agg[L["l"]], agg[L["u"]]
+        inter = a != b
+        pairs = set(zip(np.minimum(a, b)[inter].tolist(), np.maximum(a, b)[inter].tolist()))
+        assert pairs == set(zip(C["l"].tolist(), C["u"].tolist()))
+        w = np.zeros(len(C["l"]))
+        np.add.at(w, L["faceMap"][inter], L["weight"][inter])
+        assert np.allclose(w, C["weight"], rtol=1e-14, atol=0)
+        # the cells paired in the matching: a pair shares a face
+        for c in np.nonzero(sizes == 2)[0][:200]:
+            i, j = np.nonzero(agg == c)[0]
+            assert np.any((L["l"] == i) & (L["u"] == j))

@@ -153,7 +153,9 @@ class Mesh:
     agglomeration weights and (optionally) the geometry the assembly kernels read."""
 
     def __init__(self, n_cells, owner, neighbour, magSf, ndc, n_faces=None, ctx: Context | None = None,
-                 merge_levels: int = 2, geometry: dict | None = None):
+                 merge_levels: int = 2, geometry: dict | None = None, agglomeration: str = "host"):
+        """agglomeration: "host" (the reference's sequential pairwise pass) or "device" (the parallel
+        matching of vlm_mesh_register_ex with VLM_MESH_DEVICE_AGGLOMERATION)."""
         self.ctx = ctx or default_context()
         self.n_systems = 1
         self.owner = np.ascontiguousarray(owner, np.int32)
@@ -187,8 +189,12 @@ class Mesh:
             d.patch_size = pz.ctypes.data
         d.two_d = int(self.geometry.get("two_d", 0))
         d.empty_dir = int(self.geometry.get("empty_dir", -1))
+        if agglomeration not in ("host", "device"):
+            raise ValueError(f"agglomeration must be 'host' or 'device', not {agglomeration!r}")
         h = C.c_void_p()
-        check(load().vlm_mesh_register(self.ctx.handle, C.byref(d), merge_levels, C.byref(h)), self.ctx.handle)
+        flags = 1 if agglomeration == "device" else 0
+        check(load().vlm_mesh_register_ex(self.ctx.handle, C.byref(d), merge_levels, flags, C.byref(h)),
+              self.ctx.handle)
         self._h = h
         _live.add(self)
         self._apply_tuning()
@@ -770,8 +776,10 @@ class Server:
         return load().vlm_server_clock(self._h)
 
     def submit(self, mesh: dict, case: dict, arrival: float = 0.0, max_iter: int = 5000, residual_tol: float = 1e-6,
-               n_steps: int = 0, dt: float = 1.0, U0=None, p0=None, device_bytes: int = 0) -> int:
-        """mesh: cfd::Mesh arrays with geometry (voluma_b200.mesh.box_mesh); case: Flow case dict."""
+               n_steps: int = 0, dt: float = 1.0, U0=None, p0=None, device_bytes: int = 0,
+               agglomeration: str = "host") -> int:
+        """mesh: cfd::Mesh arrays with geometry (voluma_b200.mesh.box_mesh); case: Flow case dict;
+        agglomeration "device" builds the request mesh's GAMG hierarchy on the device."""
         arrs = {}
         d = _ffi.MeshDesc()
         own = np.ascontiguousarray(mesh["owner"], np.int32)
@@ -793,6 +801,7 @@ class Server:
         bc = [np.ascontiguousarray(case["u_type"], np.int32), _f64(case["u_value"]),
               np.ascontiguousarray(case["p_type"], np.int32), _f64(case["p_value"])]
         r = _ffi.FlowRequest()
+        r.mesh_flags = 1 if agglomeration == "device" else 0
         r.mesh, r.ctrl = C.addressof(d), C.addressof(ctrl)
         r.u_type, r.u_value, r.p_type, r.p_value = (a.ctypes.data for a in bc)
         if U0 is not None:

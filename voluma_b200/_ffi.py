@@ -17,6 +17,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_topology_box", "vlm_barrier_check", "vlm_mesh_set_tail", "vlm_mesh_get_tail",
            "vlm_mesh_set_fusion", "vlm_mesh_get_fusion", "vlm_mesh_time_sweeps", "vlm_mesh_sweep_time",
+           "vlm_mesh_register_ex", "vlm_mesh_register_batch_ex",
            "vlm_ctx_device_name",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
            "vlm_mesh_register_batch", "vlm_mesh_systems", "vlm_pressure_solve_batch", "vlm_exact_sum_noalloc", "vlm_precond_apply", "vlm_flow_create", "vlm_flow_set_state",
@@ -81,7 +82,7 @@ class FlowRequest(C.Structure):
     _fields_ = [("mesh", C.c_void_p), ("ctrl", C.c_void_p), ("u_type", C.c_void_p), ("u_value", C.c_void_p),
                 ("p_type", C.c_void_p), ("p_value", C.c_void_p), ("U0", C.c_void_p), ("p0", C.c_void_p),
                 ("n_steps", C.c_int32), ("dt", C.c_double), ("max_iter", C.c_int32), ("residual_tol", C.c_double),
-                ("arrival", C.c_double), ("device_bytes", C.c_int64)]
+                ("arrival", C.c_double), ("device_bytes", C.c_int64), ("mesh_flags", C.c_int32)]
 
 
 class FlowResult(C.Structure):
@@ -111,6 +112,8 @@ def load():
     L.vlm_ctx_stream.restype = P
     L.vlm_ctx_stream.argtypes = [P]
     L.vlm_mesh_register.argtypes = [P, C.POINTER(MeshDesc), i32, C.POINTER(P)]
+    L.vlm_mesh_register_ex.argtypes = [P, C.POINTER(MeshDesc), i32, i32, C.POINTER(P)]
+    L.vlm_mesh_register_batch_ex.argtypes = [P, i32, P, i32, i32, C.POINTER(P)]
     L.vlm_mesh_release.argtypes = [P]
     L.vlm_amul.argtypes = [P, P, P, P, P, P, P]
     L.vlm_ldu_solve.argtypes = [P, P, P, P, P, P, P, C.POINTER(SolverCtrl), C.POINTER(SolverPerf)]

@@ -205,7 +205,19 @@ vlm_status vlm_ctx_device_name(vlm_ctx* ctx, char* name, int32_t capacity) {
 
 vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_desc* descs, int32_t mergeLevels,
                                    vlm_mesh** out) {
+    return vlm_mesh_register_batch_ex(ctx, nsys, descs, mergeLevels, 0, out);
+}
+
+vlm_status vlm_mesh_register_ex(vlm_ctx* ctx, const vlm_mesh_desc* d, int32_t mergeLevels, int32_t flags,
+                                vlm_mesh** out) {
+    if (!ctx || !d || !out) return fail(ctx, VLM_ERR_BAD_ARG, "NULL argument");
+    return vlm_mesh_register_batch_ex(ctx, 1, d, mergeLevels, flags, out);
+}
+
+vlm_status vlm_mesh_register_batch_ex(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_desc* descs, int32_t mergeLevels,
+                                      int32_t flags, vlm_mesh** out) {
     if (!ctx || !descs || !out || nsys <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
+    if ((flags & ~int32_t(VLM_MESH_DEVICE_AGGLOMERATION)) != 0) return fail(ctx, VLM_ERR_BAD_ARG, "unknown mesh flags");
     *out = nullptr;
     return guarded(ctx, [&] {
         bool geometry = true;
@@ -253,7 +265,8 @@ vlm_status vlm_mesh_register_batch(vlm_ctx* ctx, int32_t nsys, const vlm_mesh_de
             fb += d->n_internal_faces;
             bb += d->n_faces - d->n_internal_faces;
         }
-        m->batch = std::make_unique<vlm::DeviceBatch>(topo, mergeLevels > 0 ? mergeLevels : 2, ctx->stream);
+        m->batch = std::make_unique<vlm::DeviceBatch>(topo, mergeLevels > 0 ? mergeLevels : 2, ctx->stream,
+                                                      (flags & VLM_MESH_DEVICE_AGGLOMERATION) != 0);
         if (geometry) {
             // the union mesh: every system's internal faces, then every system's boundary faces
             const size_t F = static_cast<size_t>(nF), NI = static_cast<size_t>(std::max<int64_t>(nI, 1)),

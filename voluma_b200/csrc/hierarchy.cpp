@@ -13,8 +13,6 @@
 
 namespace vlm {
 
-namespace {
-
 // Row adjacency in face order: each face f adds (l -> u) then (u -> l)  (GAMG.cpp:15-37).
 void makeAdjacency(HLevel& L) {
     const size_t nf = L.l.size();
@@ -40,6 +38,8 @@ void makeAdjacency(HLevel& L) {
         L.adjIsL[k] = 0;
     }
 }
+
+namespace {
 
 // One pairwise pass; fills L.agg/faceMap/faceFlip and returns the coarse level's faces and
 // weights (no adjacency yet)  (GAMG.cpp:40-94).

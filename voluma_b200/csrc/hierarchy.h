@@ -30,6 +30,9 @@ struct Hierarchy {
 Hierarchy buildHierarchy(int nCells, int nInternal, const int32_t* own, const int32_t* nei, const double* magSf,
                          const double* ndc, int mergeLevels, int nCoarsest = 64);
 
+// Row adjacency (off/adjCell/adjFace/adjIsL) of a level from its faces, in face order.
+void makeAdjacency(HLevel& L);
+
 // Greedy colouring in natural order (smallest colour unused by already coloured neighbours).
 std::vector<int> greedyColour(const HLevel& L, int* nColours);
 

@@ -50,7 +50,8 @@ void appendChunks(std::vector<Chunk>& out, int start, int len, int sys, int* slo
 
 }  // namespace
 
-BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox) {
+BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox,
+                    const std::function<Hierarchy(const SysTopo&)>& hierarchy) {
     BatchPlan P;
     const int ns = int(systems.size());
     if (ns == 0) throw std::invalid_argument("empty batch");
@@ -69,9 +70,11 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool u
     std::vector<Hierarchy> Hin(ns);
     for (int s = 0; s < ns; ++s)
         if (systems[s].nCells <= 0) throw std::invalid_argument("system with no cells");
+    if (hierarchy) {
+        for (int s = 0; s < ns; ++s) Hin[s] = hierarchy(systems[s]);
+    } else {
     // the systems' hierarchies are independent: built by a pool of host threads, each taking the
     // next system (largest first keeps the pool busy to the end)
-    {
         std::vector<int> byCells(ns);
         std::iota(byCells.begin(), byCells.end(), 0);
         std::stable_sort(byCells.begin(), byCells.end(),

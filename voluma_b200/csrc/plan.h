@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "box.h"
@@ -85,6 +86,9 @@ struct BatchPlan {
 
 // useBox: lay level 0 out for the structured box kernels when every system is a box mesh whose
 // natural-order colouring is the red-black parity colouring.
-BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox = true);
+// hierarchy: builds one system's agglomeration hierarchy instead of buildHierarchy (the device
+// agglomeration; called for one system at a time).
+BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool useBox = true,
+                    const std::function<Hierarchy(const SysTopo&)>& hierarchy = {});
 
 }  // namespace vlm

@@ -39,6 +39,7 @@ struct Request {
     vlm_flow_ctrl ctrl{};
     int32_t steady = 1, nSteps = 0, maxIter = 0;
     double dt = 1.0, tol = 1e-6, arrival = 0;
+    int32_t meshFlags = 0;
     int64_t bytes = 0;
 };
 
@@ -169,7 +170,7 @@ struct vlm_server {
         m.skewVecs = q.skew.empty() ? nullptr : q.skew.data();
         vlm_mesh* mesh = nullptr;
         vlm_flow* flow = nullptr;
-        vlm_status st = vlm_mesh_register(ctx, &m, 0, &mesh);
+        vlm_status st = vlm_mesh_register_ex(ctx, &m, 0, q.meshFlags, &mesh);
         if (st == VLM_OK)
             st = vlm_flow_create(ctx, mesh, &q.ctrl, q.uType.data(), q.uValue.data(), q.pType.data(), q.pValue.data(),
                                  &flow);
@@ -280,6 +281,7 @@ vlm_status vlm_server_submit(vlm_server* s, const vlm_flow_request* r, int64_t* 
     q->maxIter = r->max_iter;
     q->tol = r->residual_tol;
     q->arrival = r->arrival;
+    q->meshFlags = r->mesh_flags;
     q->bytes = r->device_bytes > 0 ? r->device_bytes : vlm_flow_request_bytes(m.n_cells, m.n_faces);
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -15,6 +15,7 @@
 #include "boxkernels.cuh"
 #include "dilu.cuh"
 #include "krylov.cuh"
+#include "aggl.h"
 #include "solver.h"
 #include "tailplan.h"
 
@@ -165,11 +166,17 @@ std::vector<cudaGraphNode_t> nodesOf(cudaGraph_t g) {
 }  // namespace
 
 // ====================================================================== construction
-DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream)
+DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream,
+                         bool deviceAgglomeration)
     : stream_(stream), topo_(systems), mergeLevels_(mergeLevels) {
     // VLM_BOX=0 keeps box meshes on the general (SELL) level-0 layout
     const char* bv = std::getenv("VLM_BOX");
-    plan_ = buildPlan(systems, mergeLevels, !(bv && bv[0] == '0'));
+    std::function<Hierarchy(const SysTopo&)> hier;
+    if (deviceAgglomeration)
+        hier = [&](const SysTopo& t) {
+            return buildHierarchyDevice(stream, t.nCells, t.nInternal, t.own, t.nei, t.magSf, t.ndc, mergeLevels);
+        };
+    plan_ = buildPlan(systems, mergeLevels, !(bv && bv[0] == '0'), hier);
     const char* gv = std::getenv("VLM_GRAPH");
     useGraphs_ = !(gv && gv[0] == '0');
 

@@ -81,7 +81,10 @@ struct GraphExec {
 // A batch of systems resident on one device (a single-system mesh is a batch of one).
 class DeviceBatch {
 public:
-    DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream);
+    // deviceAgglomeration: the GAMG hierarchy from the device's parallel matching (aggl.h) instead
+    // of the host's sequential pass
+    DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, cudaStream_t stream,
+                bool deviceAgglomeration = false);
     ~DeviceBatch();
 
     const BatchPlan& plan() const { return plan_; }
