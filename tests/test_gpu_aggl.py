@@ -81,3 +81,42 @@ def test_unknown_registration_flag():
     g = golden("periodic8")
     with pytest.raises(ValueError):
         vb.Mesh.from_arrays(g, agglomeration="elsewhere")
+
+
+def test_device_hierarchy_disconnected_and_isolated_cells():
+    """Two disconnected boxes and a cell without faces: the matching never pairs across components,
+    the isolated cell is an aggregate of its own on every level, and the hierarchy equals the
+    restatement's."""
+    a = vm.box_mesh((9, 7, 1), two_d=True)
+    b = vm.box_mesh((6, 5, 4))
+    na, nb = a["n_cells"], b["n_cells"]
+    nIa, nIb = len(a["neighbour"]), len(b["neighbour"])
+    own = np.concatenate([a["owner"][:nIa], b["owner"][:nIb] + na]).astype(np.int32)
+    nei = np.concatenate([a["neighbour"], b["neighbour"] + na]).astype(np.int32)
+    magSf = np.concatenate([a["magSf"][:nIa], b["magSf"][:nIb]])
+    ndc = np.concatenate([a["ndc"][:nIa], b["ndc"][:nIb]])
+    m = dict(n_cells=na + nb + 1, owner=own, neighbour=nei, magSf=magSf, ndc=ndc)
+    mesh = vb.Mesh(m["n_cells"], own, nei, magSf, ndc, agglomeration="device")
+    H = ro.hierarchy(m, matching=True)
+    same_hierarchy(mesh, H)
+    for k in range(len(H) - 1):
+        agg = H[k]["agg"]
+        n = H[k]["n"]
+        # the last cell of every level is the isolated one (numbered by its first cell, it comes last)
+        assert np.count_nonzero(agg == agg[n - 1]) == 1
+    # a Poisson-like system on it: every component solvable (diagonal dominance for the isolated cell)
+    up = -magSf * ndc
+    d = np.zeros(m["n_cells"])
+    np.add.at(d, own, -up)
+    np.add.at(d, nei, -up)
+    d[0] *= 2.0
+    d[na] *= 2.0
+    d[-1] = 1.0
+    rng = np.random.default_rng(3)
+    bvec = rng.standard_normal(m["n_cells"])
+    x = np.zeros(m["n_cells"])
+    p = vb.solve_ldu(mesh, d, up, None, bvec, x, ctrl())
+    xo, po = ro.solve(m, d, up, None, bvec, np.zeros(m["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000,
+                      smoother="mcgs-jacobi", coarse=1, matching=True)
+    assert p.converged and abs(p.iterations - po["iterations"]) <= 1
+    mesh.close()
