@@ -376,38 +376,61 @@ BatchPlan buildPlan(const std::vector<SysTopo>& systems, int mergeLevels, bool u
         LP.childPtr.assign(size_t(NP.nrows) + 1, 0);
         LP.intraPtr.assign(size_t(NP.nrows) + 1, 0);
         LP.cfacePtr.assign(size_t(NP.nfaces) + 1, 0);
-        std::vector<std::vector<int32_t>> kids(size_t(NP.nrows)), intra(size_t(NP.nrows)),
-            cf(size_t(NP.nfaces));
         const int activeSys = int(NP.sysRow.size()) - 1;  // systems present on k+1 = active on k
-        for (int b = 0; b < activeSys; ++b) {
-            const HLevel& L = P.H[b].levels[k];
-            const int32_t fb = LP.sysFace[b], nfb = NP.sysFace[b];
-            for (int i = 0; i < L.n; ++i) {
-                const int R = rowOf[k + 1][b][L.agg[i]];
-                LP.agg[rowOf[k][b][i]] = R;
-                kids[R].push_back(rowOf[k][b][i]);
+        // CSR lists by counting sort: a counting pass, prefix sums, then a filling pass in the same
+        // order (systems, cells / faces ascending), so each list keeps that order
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int32_t> ck, ci, cc;  // fill cursors
+            if (pass == 1) {
+                for (int R = 0; R < NP.nrows; ++R) {
+                    LP.childPtr[R + 1] += LP.childPtr[R];
+                    LP.intraPtr[R + 1] += LP.intraPtr[R];
+                }
+                for (int c = 0; c < NP.nfaces; ++c) LP.cfacePtr[c + 1] += LP.cfacePtr[c];
+                LP.child.resize(size_t(LP.childPtr[NP.nrows]));
+                LP.intraFace.resize(size_t(LP.intraPtr[NP.nrows]));
+                LP.cfaceSrc.resize(size_t(LP.cfacePtr[NP.nfaces]));
+                ck.assign(LP.childPtr.begin(), LP.childPtr.end() - 1);
+                ci.assign(LP.intraPtr.begin(), LP.intraPtr.end() - 1);
+                cc.assign(LP.cfacePtr.begin(), LP.cfacePtr.end() - 1);
             }
-            const bool lev0 = k == 0;
-            for (size_t f = 0; f < L.l.size(); ++f) {
-                const int c = L.faceMap[f];
-                const int32_t g = fb + int32_t(f);
-                if (c < 0) {
-                    intra[rowOf[k + 1][b][L.agg[L.l[f]]]].push_back(g);
-                } else {
-                    bool flip = L.faceFlip[f] != 0;
-                    if (lev0 && !P.H[b].ownerIsL[f]) flip = !flip;
-                    cf[size_t(nfb + c)].push_back(int32_t(uint32_t(g) | (flip ? 0x80000000u : 0u)));
+            for (int b = 0; b < activeSys; ++b) {
+                const HLevel& L = P.H[b].levels[k];
+                const int32_t fb = LP.sysFace[b], nfb = NP.sysFace[b];
+                const std::vector<int32_t>& rk = rowOf[k][b];
+                const std::vector<int32_t>& rk1 = rowOf[k + 1][b];
+                for (int i = 0; i < L.n; ++i) {
+                    const int R = rk1[L.agg[i]];
+                    if (pass == 0) {
+                        LP.agg[rk[i]] = R;
+                        ++LP.childPtr[R + 1];
+                    } else {
+                        LP.child[size_t(ck[R]++)] = rk[i];
+                    }
+                }
+                const bool lev0 = k == 0;
+                for (size_t f = 0; f < L.l.size(); ++f) {
+                    const int c = L.faceMap[f];
+                    const int32_t g = fb + int32_t(f);
+                    if (c < 0) {
+                        const int R = rk1[L.agg[L.l[f]]];
+                        if (pass == 0)
+                            ++LP.intraPtr[R + 1];
+                        else
+                            LP.intraFace[size_t(ci[R]++)] = g;
+                    } else {
+                        const size_t C = size_t(nfb + c);
+                        if (pass == 0) {
+                            ++LP.cfacePtr[C + 1];
+                        } else {
+                            bool flip = L.faceFlip[f] != 0;
+                            if (lev0 && !P.H[b].ownerIsL[f]) flip = !flip;
+                            LP.cfaceSrc[size_t(cc[C]++)] = int32_t(uint32_t(g) | (flip ? 0x80000000u : 0u));
+                        }
+                    }
                 }
             }
         }
-        for (int R = 0; R < NP.nrows; ++R) {
-            LP.childPtr[R + 1] = LP.childPtr[R] + int(kids[R].size());
-            LP.intraPtr[R + 1] = LP.intraPtr[R] + int(intra[R].size());
-        }
-        for (int c = 0; c < NP.nfaces; ++c) LP.cfacePtr[c + 1] = LP.cfacePtr[c] + int(cf[c].size());
-        for (auto& v : kids) LP.child.insert(LP.child.end(), v.begin(), v.end());
-        for (auto& v : intra) LP.intraFace.insert(LP.intraFace.end(), v.begin(), v.end());
-        for (auto& v : cf) LP.cfaceSrc.insert(LP.cfaceSrc.end(), v.begin(), v.end());
     }
 
     // ---------------------------------------------------------------- coarse solves, level-0 map
