@@ -1053,10 +1053,24 @@ def run_ours(args, rank, world, local):
                      "ms_per_launch_l2_cold": k_ms_cold, "ms_per_launch_l2_warm": k_ms_warm,
                      "ms_per_sweep_as_two_colour_launches": k_ms_steps},
         "clocks": clocks, "gpu_launches": mx["gpu_launches"],
+        "launch_configuration": launch_configuration(mesh),
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, diag, upper, b)
     print(json.dumps(line))
+
+
+def launch_configuration(mesh):
+    """The V-cycle launch shape the mesh ran with: coarse tail (from the tuner's table, or the
+    built-in default with VLM_TUNE=0) and the fusion row limits."""
+    from voluma_b200 import tune
+    cl, max_rows, full_rows = mesh.tail_config()
+    entry = tune.lookup(tune.load_table(mesh.ctx.device_name()), int(mesh.n_cells), 1) \
+        if os.environ.get("VLM_TUNE", "1") != "0" else None
+    return {"tail_cluster": cl, "tail_max_rows": max_rows, "tail_full_rows": full_rows,
+            "tuning_entry": entry["case"] if entry else None,
+            "tuning_table": os.path.relpath(tune.table_path(mesh.ctx.device_name()), ROOT) if entry else None,
+            "fusion_rows": list(mesh.fusion_config())}
 
 
 def cpu_baseline(n, diag, upper, b):
