@@ -272,6 +272,12 @@ vlm_status vlm_mesh_set_fusion(vlm_mesh* mesh, int64_t pre_rows, int64_t restric
 vlm_status vlm_mesh_time_sweeps(vlm_mesh* mesh, int32_t on);
 vlm_status vlm_mesh_sweep_time(vlm_mesh* mesh, double* ms_total, int64_t* sweeps);
 vlm_status vlm_mesh_get_fusion(vlm_mesh* mesh, int64_t* pre_rows, int64_t* restrict_rows, int64_t* post_rows);
+/* Launch shape of the plane-streamed level-0 FP64 product of a box system, planned at registration:
+ * pencil height in x-rows, shared-memory plane stages, CTAs; all 0 where it does not apply (more than
+ * one system, an x extent not a multiple of 8, fewer than 3 planes, or VLM_BOX_STREAM=0 in the
+ * environment at registration), and the four-slot kernel runs instead.  Results are the same bit
+ * for bit either way. */
+vlm_status vlm_mesh_get_stream(vlm_mesh* mesh, int32_t* pencil_rows, int32_t* stages, int32_t* ctas);
 /* Measurement hook: times `reps` launches of one level-0 kernel on the matrix of the last solve
  * ("amul64", "spmv64", "smooth64", "smooth32", "residual64", "residual32"; a smooth launch is one
  * full multicolour sweep; "vcycle32" / "vcycle32_notail" one FP32 V-cycle with / without the

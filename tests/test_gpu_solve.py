@@ -388,3 +388,33 @@ def test_shared_memory_tail_matches_global_tail(name, precision, monkeypatch):
             out.append((x, p.iterations))
             m.close()
         assert out[0][1] == out[1][1] and np.array_equal(out[0][0], out[1][0]), rows
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,periodic", [((32, 16, 8), (1, 1, 1)), ((64, 16, 6), (0, 0, 0)),
+                                            ((32, 32, 12), (1, 0, 1)), ((64, 24, 4), (1, 1, 1))])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_streamed_product_matches_four_slot_kernel(shape, periodic, precision, monkeypatch):
+    """The plane-streamed level-0 FP64 product (y-pencils of x-rows, z-planes staged in shared
+    memory by bulk copies, runs of planes split across CTAs, periodic and wall boundaries) forms
+    every row's terms in the four-slot kernel's order, and its dot differs only in how the per-CTA
+    double-double partials are grouped: the same PCG iterates bit for bit, with GAMG and with the
+    diagonal preconditioner."""
+    M = vm.box_mesh(shape, hi=(1.0, 0.7, 0.5), periodic=periodic)
+    d, up = vm.poisson_matrix(M)
+    b = np.random.default_rng(3).standard_normal(M["n_cells"])
+    b -= b.mean()
+    out = {}
+    for on in ("0", "1"):
+        monkeypatch.setenv("VLM_BOX_STREAM", on)
+        m = vb.Mesh.from_arrays(M)
+        assert (m.stream_config()[2] > 0) == (on == "1")
+        for pc in ("GAMG", "diagonal"):
+            x = np.zeros(M["n_cells"])
+            p = vb.solve_ldu(m, d, up, None, b, x, ctrl(preconditioner=pc, precision=precision))
+            assert p.converged
+            out[on, pc] = (x, p.iterations)
+        m.close()
+    for pc in ("GAMG", "diagonal"):
+        assert out["0", pc][1] == out["1", pc][1]
+        assert np.array_equal(out["0", pc][0], out["1", pc][0])

@@ -308,6 +308,13 @@ class Mesh:
         check(load().vlm_mesh_get_fusion(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
 
+    def stream_config(self):
+        """(pencil_rows, stages, ctas) of the plane-streamed level-0 FP64 product
+        (vlm_mesh_get_stream); zeros where the four-slot kernel runs instead."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(load().vlm_mesh_get_stream(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def time_sweeps(self, on: bool = True):
         """Live level-0 sweep timing (vlm_mesh_time_sweeps): solves run eagerly with CUDA events
         around every level-0 sweep."""

@@ -16,7 +16,7 @@ EXPORTS = ["vlm_ctx_create", "vlm_ctx_destroy", "vlm_last_error", "vlm_ctx_strea
            "vlm_gamg_levels", "vlm_gamg_level", "vlm_gamg_colours", "vlm_laplacian", "vlm_grad", "vlm_exact_sum",
            "vlm_topology_build", "vlm_topology_levels", "vlm_topology_level", "vlm_topology_destroy",
            "vlm_topology_box", "vlm_barrier_check", "vlm_mesh_set_tail", "vlm_mesh_get_tail",
-           "vlm_mesh_set_fusion", "vlm_mesh_get_fusion", "vlm_mesh_time_sweeps", "vlm_mesh_sweep_time",
+           "vlm_mesh_set_fusion", "vlm_mesh_get_fusion", "vlm_mesh_get_stream", "vlm_mesh_time_sweeps", "vlm_mesh_sweep_time",
            "vlm_mesh_register_ex", "vlm_mesh_register_batch_ex",
            "vlm_ctx_device_name",
            "vlm_mesh_stats", "vlm_profile_kernel", "vlm_div", "vlm_pressure_solve", "vlm_pressure_solve_device",
@@ -169,6 +169,7 @@ def load():
     L.vlm_mesh_time_sweeps.argtypes = [P, i32]
     L.vlm_mesh_sweep_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.vlm_mesh_get_fusion.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.vlm_mesh_get_stream.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.vlm_ctx_device_name.argtypes = [P, C.c_char_p, i32]
     L.vlm_mesh_get_tail.argtypes = [P, C.POINTER(i32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.vlm_box_create.argtypes = [P, C.POINTER(BoxSpec), C.POINTER(P)]

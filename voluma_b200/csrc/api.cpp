@@ -490,6 +490,12 @@ vlm_status vlm_mesh_get_fusion(vlm_mesh* m, int64_t* pre_rows, int64_t* restrict
     return VLM_OK;
 }
 
+vlm_status vlm_mesh_get_stream(vlm_mesh* m, int32_t* pencil_rows, int32_t* stages, int32_t* ctas) {
+    if (!m || !pencil_rows || !stages || !ctas) return fail(nullptr, VLM_ERR_BAD_ARG, "NULL argument");
+    m->batch->streamConfig(pencil_rows, stages, ctas);
+    return VLM_OK;
+}
+
 vlm_status vlm_profile_kernel(vlm_ctx* ctx, vlm_mesh* m, const char* kernel, int32_t reps, double* ms, double* bytes) {
     if (!ctx || !m || !kernel || !ms || !bytes || reps <= 0) return fail(ctx, VLM_ERR_BAD_ARG, "invalid arguments");
     return guarded(ctx, [&] {

@@ -282,6 +282,20 @@ struct BoxGroup4 {
     V4<T> dg, cpx, cpy, cpz, cmy, cmz, cmx;  // diagonal, own +d coefficients, neighbours' -d ones
     T cme;          // the -x coefficient at slot xe (p == 0)
 
+    // faces[] of the group's rows (x-row j, plane k, slots m0.., parity p already set)
+    __device__ __forceinline__ void set_faces(const BoxSys& B, int j, int k, int m0) {
+        const int nx = B.nx, ny = B.ny, nz = B.nz;
+        const bool px = B.per & 1, py = B.per & 2, pz = B.per & 4;
+        const int fy = (j > 0 ? 2 : (py ? 2 << 6 : 0)) | (j < ny - 1 ? 16 : (py ? 16 << 6 : 0));
+        const int fz = (k > 0 ? 1 : (pz ? 1 << 6 : 0)) | (k < nz - 1 ? 32 : (pz ? 32 << 6 : 0));
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int i = 2 * (m0 + v) + p;
+            const int fx = (i > 0 ? 4 : (px ? 4 << 6 : 0)) | (i < nx - 1 ? 8 : (px ? 8 << 6 : 0));
+            faces[v] = i < nx ? (fx | fy | fz) : 0;  // i >= nx: a padding slot (odd nx)
+        }
+    }
+
     __device__ __forceinline__ void load(const BoxSys& B, int row, const T* __restrict__ cx,
                                          const T* __restrict__ cy, const T* __restrict__ cz,
                                          const T* __restrict__ diag) {
@@ -289,13 +303,12 @@ struct BoxGroup4 {
         const int s = row - (C ? B.base1 : B.base0);
         valid = s < B.slots;
         if (!valid) return;
-        const int H = B.H, nx = B.nx, ny = B.ny, nz = B.nz;
+        const int H = B.H, ny = B.ny, nz = B.nz;
         const int q = fast_div(s, B.divH);
         const int m0 = s - q * H;
         const int k = fast_div(q, B.divNy);
         const int j = q - k * ny;
         p = (j + k + C) & 1;
-        const bool px = B.per & 1, py = B.per & 2, pz = B.per & 4;
         const int o = C ? B.base0 : B.base1;
         const int x0 = o + q * H;  // the other colour's x-row
         xr = x0 + m0;
@@ -305,14 +318,7 @@ struct BoxGroup4 {
         rpy = o + (j < ny - 1 ? q + 1 : q - (ny - 1)) * H + m0;
         rmz = o + (k > 0 ? q - ny : q + (nz - 1) * ny) * H + m0;
         rpz = o + (k < nz - 1 ? q + ny : q - (nz - 1) * ny) * H + m0;
-        const int fy = (j > 0 ? 2 : (py ? 2 << 6 : 0)) | (j < ny - 1 ? 16 : (py ? 16 << 6 : 0));
-        const int fz = (k > 0 ? 1 : (pz ? 1 << 6 : 0)) | (k < nz - 1 ? 32 : (pz ? 32 << 6 : 0));
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int i = 2 * (m0 + v) + p;
-            const int fx = (i > 0 ? 4 : (px ? 4 << 6 : 0)) | (i < nx - 1 ? 8 : (px ? 8 << 6 : 0));
-            faces[v] = i < nx ? (fx | fy | fz) : 0;  // i >= nx: a padding slot (odd nx)
-        }
+        set_faces(B, j, k, m0);
         const uint64_t pol = l2_keep();
         dg = ld4_keep(diag + row, pol);
         cpx = ld4_keep(cx + row, pol);

@@ -60,9 +60,9 @@ __device__ __forceinline__ DD dd_shfl_down(DD v, int o) {
 }
 
 // Reduces NV values over the CTA (fixed tree), returns the totals in thread 0.
-template <int NV>
+template <int NV, int MAXW = kRowsPerCta / 32>
 __device__ __forceinline__ void block_reduce(DD (&v)[NV]) {
-    __shared__ DD sm[NV][kRowsPerCta / 32];
+    __shared__ DD sm[NV][MAXW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
@@ -82,24 +82,23 @@ __device__ __forceinline__ void block_reduce(DD (&v)[NV]) {
 }
 
 
-// Writes this CTA's partials; returns true in thread 0 of the CTA that completes the
-// system, with the system totals (summed over slots in a fixed order) in `out`.
-template <int NV>
-__device__ bool reduce_dd(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
-    block_reduce<NV>(v);
+// Writes this CTA's partials into `slot`; returns true in thread 0 of the CTA that completes
+// system `sys`, whose CTAs write the slots [b, e), with the totals (summed over the slots in a
+// fixed order) in `out`.
+template <int NV, int MAXW = kRowsPerCta / 32>
+__device__ bool reduce_dd_span(DD (&v)[NV], int slot, int sys, int b, int e, const RedCtx& R, double (&out)[NV]) {
+    block_reduce<NV, MAXW>(v);
     __shared__ int isLast;
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) R.partials[(size_t)c.slot * NV + q] = v[q];
+        for (int q = 0; q < NV; ++q) R.partials[(size_t)slot * NV + q] = v[q];
         __threadfence();
-        const int nslots = R.slotEnd[c.sys] - R.slotBegin[c.sys];
-        const int ticket = atomicAdd(&R.counters[c.sys], 1);
-        isLast = ticket == nslots - 1;
+        const int ticket = atomicAdd(&R.counters[sys], 1);
+        isLast = ticket == e - b - 1;
     }
     __syncthreads();
     if (!isLast) return false;
     __threadfence();
-    const int b = R.slotBegin[c.sys], e = R.slotEnd[c.sys];
     DD acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = DD{0.0, 0.0};
@@ -124,12 +123,18 @@ __device__ bool reduce_dd(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (
             acc[q] = dd_add(acc[q], DD{w.x, w.y});
         }
     __syncthreads();  // the shared tree below is reused
-    block_reduce<NV>(acc);
+    block_reduce<NV, MAXW>(acc);
     if (threadIdx.x != 0) return false;
-    R.counters[c.sys] = 0;
+    R.counters[sys] = 0;
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = acc[q].hi + acc[q].lo;
     return true;
+}
+
+// reduce_dd_span over the slots of chunk c's system, one slot per chunk.
+template <int NV>
+__device__ bool reduce_dd(DD (&v)[NV], const Chunk& c, const RedCtx& R, double (&out)[NV]) {
+    return reduce_dd_span<NV>(v, c.slot, c.sys, R.slotBegin[c.sys], R.slotEnd[c.sys], R, out);
 }
 
 // Writes this CTA's exact bins as its partial; the last CTA of the system adds every partial

@@ -13,6 +13,7 @@
 #include <utility>
 
 #include "boxkernels.cuh"
+#include "boxstream.cuh"
 #include "dilu.cuh"
 #include "krylov.cuh"
 #include "aggl.h"
@@ -101,11 +102,11 @@ bool pdlEnabled() {
 }
 
 template <class... Exp, class... Act>
-void launchK(void (*kernel)(Exp...), int grid, int block, cudaStream_t s, Act&&... args) {
+void launchKS(void (*kernel)(Exp...), int grid, int block, size_t smem, cudaStream_t s, Act&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(grid));
     cfg.blockDim = dim3(unsigned(block));
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -115,12 +116,26 @@ void launchK(void (*kernel)(Exp...), int grid, int block, cudaStream_t s, Act&&.
     VLM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
 }
 
+template <class... Exp, class... Act>
+void launchK(void (*kernel)(Exp...), int grid, int block, cudaStream_t s, Act&&... args) {
+    launchKS(kernel, grid, block, 0, s, std::forward<Act>(args)...);
+}
+
 #define VLM_LAUNCH(kernel, grid, block, stream, ...)                    \
     do {                                                                \
         if ((grid) > 0) {                                               \
             launchK(kernel, (grid), (block), (stream), __VA_ARGS__);    \
             ++tl_launches;                                              \
         }                                                               \
+    } while (0)
+
+// VLM_LAUNCH with dynamic shared memory
+#define VLM_LAUNCH_SMEM(kernel, grid, block, smem, stream, ...)                 \
+    do {                                                                        \
+        if ((grid) > 0) {                                                       \
+            launchKS(kernel, (grid), (block), (smem), (stream), __VA_ARGS__);   \
+            ++tl_launches;                                                      \
+        }                                                                       \
     } while (0)
 
 template <class T> struct LV;
@@ -198,6 +213,8 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     if (const char* fr = std::getenv("VLM_TAIL_FULL_ROWS")) tailFullRows_ = std::atoll(fr);
     // VLM_BOX_FUSED=1: a box level-0 sweep as one fused launch instead of the two colour launches
     if (const char* f = std::getenv("VLM_BOX_FUSED")) sweepFused_ = f[0] == '1';
+    // VLM_BOX_STREAM=0: level 0 of box systems without the plane-streamed kernels
+    if (const char* f = std::getenv("VLM_BOX_STREAM")) streamAllowed_ = f[0] != '0';
     // VLM_TAIL_SMEM=0: the coarse tail reads its operands from global memory
     if (const char* f = std::getenv("VLM_TAIL_SMEM")) tailSmemAllowed_ = f[0] != '0';
     if (const char* f = std::getenv("VLM_FUSE_PRE")) fusePre_ = std::atoll(f);
@@ -285,6 +302,12 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     }
     hostState_.resize(size_t(plan_.nsys));
     if (tailOn_) buildTailTable<double>(tail64_);
+    // launch shapes of the plane-streamed level-0 kernels, planned before any stream capture
+    if (L_[0].box && plan_.nsys == 1) {
+        int g = 0;
+        const BoxRows R = boxRows(L_[0], L_[0].all, &g);
+        planStream<double>(R);
+    }
     VLM_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -497,6 +520,80 @@ BoxRows DeviceBatch::boxRows(const DevLevel& D, const ChunkList& l, int* grid) c
         *grid = l.n;
     }
     return R;
+}
+
+// Launch shape of the streamed level-0 kernels (boxstream.cuh) for this batch's box system in
+// elements of T, planned at registration (streamShape: null where they do not apply and the
+// four-slot kernels run; VLM_BOX_STREAM=0 at registration: never).  They need a batch of one
+// system in the range form, H % 4 == 0 (16-byte rows), colour
+// groups and coefficient arrays on 16-byte boundaries, at least 3 planes, and a pencil height TY
+// (8, 4 or 2 x-rows) dividing ny with 2 * TY * H / N consumer threads (N slots of one colour, 16
+// bytes, each) a whole number of warps, at most 256.  The ring takes as many plane stages (3..8)
+// as the opt-in shared memory holds; the grid is one wave.
+template <class T>
+void DeviceBatch::planStream(const BoxRows& R) {
+    StreamShape& sh = sizeof(T) == 8 ? stream64_ : stream32_;
+    sh = StreamShape{};
+    if (!streamAllowed_ || R.ch != nullptr || plan_.nsys != 1) return;
+    const BoxSys& B = R.one;
+    if (B.H % 4 != 0 || B.nz < 3 || B.base0 % 4 != 0 || B.base1 % 4 != 0 || L_[0].nrows % 4 != 0) return;
+    auto kernel = k_box_pcg_spmv_stream<T, kFlagDone>;
+    int dev = 0, optin = 0, perSm = 0, sms = 0;
+    VLM_CUDA(cudaGetDevice(&dev));
+    VLM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    VLM_CUDA(cudaDeviceGetAttribute(&perSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    VLM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaFuncAttributes fa = {};
+    VLM_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    // the most resident warps per SM over pencil heights and CTAs per SM, with at least 4 stages
+    // (two read, two in flight); VLM_STREAM_TY / VLM_STREAM_CTAS pin a choice
+    const int pinTY = std::getenv("VLM_STREAM_TY") ? std::atoi(std::getenv("VLM_STREAM_TY")) : 0;
+    const int pinCtas = std::getenv("VLM_STREAM_CTAS") ? std::atoi(std::getenv("VLM_STREAM_CTAS")) : 0;
+    int TY = 0, S = 0, bestWarps = 0;
+    for (int t : {8, 4, 2}) {
+        const int consumers = 2 * t * B.H / SG<T>::N;
+        if (B.ny % t != 0 || consumers % 32 != 0 || consumers > kStreamMaxThreads - 32) continue;
+        if (pinTY && t != pinTY) continue;
+        const size_t stage = size_t(stream_stage_elems(B.H, t)) * sizeof(T);
+        for (int c = 1; c <= 3; ++c) {
+            if (pinCtas && c != pinCtas) continue;
+            const size_t budget = std::min<size_t>(size_t(optin), size_t(perSm) / c - 1024);
+            if (budget < fa.sharedSizeBytes + 128 + 4 * stage) continue;
+            const int s = int(std::min<size_t>(8, (budget - fa.sharedSizeBytes - 128) / stage));
+            const int warps = c * (consumers / 32 + 1);
+            if (warps > bestWarps || (warps == bestWarps && s > S)) {
+                bestWarps = warps;
+                TY = t;
+                S = s;
+            }
+        }
+    }
+    if (TY == 0) return;
+    const size_t smem = 128 + size_t(S) * size_t(stream_stage_elems(B.H, TY)) * sizeof(T);
+    // the attribute belongs to the kernel, not to this mesh: allow the most any mesh's launch asks
+    VLM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - int(fa.sharedSizeBytes)));
+    int per = 0;
+    const int threads = 32 + 2 * TY * B.H / SG<T>::N;  // the producer warp and the consumers
+    VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+    if (per < 1) return;
+    const int W = (B.ny / TY) * B.nz;
+    const int slots = plan_.sysSlotEnd[0] - plan_.sysSlotBegin[0];
+    if (sweepSync_.size() == 0) {
+        sweepSync_.resize(1);
+        sweepSync_.zero(stream_);
+    }
+    sh.TY = TY;
+    sh.S = S;
+    sh.threads = threads;
+    sh.smem = smem;
+    sh.grid = std::min({sms * per, W, slots});
+}
+
+template <class T>
+const DeviceBatch::StreamShape* DeviceBatch::streamShape(const BoxRows& R) const {
+    const StreamShape& sh = sizeof(T) == 8 ? stream64_ : stream32_;
+    return sh.grid > 0 && R.ch == nullptr ? &sh : nullptr;
 }
 
 RedCtx DeviceBatch::red() const {
@@ -730,14 +827,16 @@ bool DeviceBatch::recordFusedSweep(const ChunkList& la, const ChunkList& lb, con
     if (RA.ch != nullptr || RB.ch != nullptr || RA.one.H % 4 != 0) return false;
     const int nA = (RA.end - RA.begin + kSweepPiece - 1) / kSweepPiece;
     const int nB = (RB.end - RB.begin + kSweepPiece - 1) / kSweepPiece;
-    if (sweepSync_.size() == 0) {
+    if (sweepDone_.size() == 0) {
         int dev = 0, sms = 0, per = 0;
         VLM_CUDA(cudaGetDevice(&dev));
         VLM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         VLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_box_sweep4<T, 0>, kRowsPerCta, 0));
         sweepGrid_ = sms * std::max(1, per);
-        sweepSync_.resize(1);
-        sweepSync_.zero(stream_);
+        if (sweepSync_.size() == 0) {
+            sweepSync_.resize(1);
+            sweepSync_.zero(stream_);
+        }
         sweepDone_.resize(size_t(std::max(nA, nB)));
         sweepDone_.zero(stream_);
     }
@@ -758,7 +857,8 @@ bool DeviceBatch::recordFusedSweep(const ChunkList& la, const ChunkList& lb, con
     return true;
 }
 
-// A wait of the fused sweep that gave up leaves a non-zero error word.
+// A wait of the fused sweep (bit 0) or of a streamed kernel (bit 1) that gave up leaves a non-zero
+// error word.
 void DeviceBatch::checkSweepError() {
     if (sweepSync_.size() == 0) return;
     SweepSync h = {};
@@ -766,7 +866,8 @@ void DeviceBatch::checkSweepError() {
     if (h.err != 0) {
         VLM_CUDA(cudaMemsetAsync(&sweepSync_.get()->err, 0, sizeof(unsigned), stream_));
         VLM_CUDA(cudaStreamSynchronize(stream_));
-        throw Error(VLM_ERR_TIMEOUT, "fused level-0 sweep: a wait for another CTA's piece gave up");
+        throw Error(VLM_ERR_TIMEOUT, (h.err & 1u) ? "fused level-0 sweep: a wait for another CTA's piece gave up"
+                                                  : "streamed level-0 kernel: a plane stage never arrived");
     }
 }
 
@@ -1092,7 +1193,12 @@ void DeviceBatch::recordPcgIterT(PrecondKind pk, SmootherKind sm, bool f32) {
     if (boxOn_) {
         int g = 0;
         const BoxRows R = boxRows(D0, D0.all, &g);
-        if (R.ch == nullptr && R.one.H % 4 == 0)
+        const StreamShape* sh = EXACT ? nullptr : streamShape<double>(R);
+        if (sh)
+            VLM_LAUNCH_SMEM((k_box_pcg_spmv_stream<double, kFlagDone>), sh->grid, sh->threads, sh->smem, s, R.one,
+                            sh->TY, sh->S, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(),
+                            (const double*)p_.get(), Ap_.get(), red(), st_.get(), &sweepSync_.get()->err);
+        else if (R.ch == nullptr && R.one.H % 4 == 0)
             VLM_LAUNCH((k_box_pcg_spmv4<double, kFlagDone, EXACT>), nb, kRowsPerCta, s, ch, R.one,
                        (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(),
                        (const double*)p_.get(), Ap_.get(), red(), st_.get());
@@ -1867,7 +1973,12 @@ double DeviceBatch::profileKernel(const std::string& fullName, int reps, double*
         run = [&] {
             int g = 0;
             const BoxRows R = boxOn_ ? boxRows(D0, D0.all, &g) : BoxRows{};
-            if (boxOn_ && R.ch == nullptr && R.one.H % 4 == 0)
+            const StreamShape* sh = boxOn_ ? streamShape<double>(R) : nullptr;
+            if (sh)
+                VLM_LAUNCH_SMEM((k_box_pcg_spmv_stream<double, kFlagDone>), sh->grid, sh->threads, sh->smem, s, R.one,
+                                sh->TY, sh->S, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(),
+                                (const double*)r_.get(), w_.get(), red(), st_.get(), &sweepSync_.get()->err);
+            else if (boxOn_ && R.ch == nullptr && R.one.H % 4 == 0)
                 VLM_LAUNCH((k_box_pcg_spmv4<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), R.one, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());
             else if (boxOn_)
                 VLM_LAUNCH((k_box_pcg_spmv<double, kFlagDone, false>), D0.all.n, kRowsPerCta, s, D0.ch(D0.all), R, (const double*)D0.bcoef.get(), D0.nrows, (const double*)D0.diag.get(), (const double*)r_.get(), w_.get(), red(), st_.get());

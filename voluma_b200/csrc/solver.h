@@ -146,6 +146,11 @@ public:
     // limit (0 keeps a value); re-plans the batch's launches, same results.
     void setTail(int cluster, int64_t maxRows, int64_t fullRows);
     void setFusion(int64_t pre, int64_t restrict, int64_t post);
+    void streamConfig(int32_t* ty, int32_t* stages, int32_t* ctas) const {
+        *ty = stream64_.grid > 0 ? stream64_.TY : 0;
+        *stages = stream64_.grid > 0 ? stream64_.S : 0;
+        *ctas = stream64_.grid;
+    }
     void fusionConfig(int64_t* pre, int64_t* restrict, int64_t* post) const {
         *pre = fusePre_;
         *restrict = fuseRestrict_;
@@ -171,6 +176,15 @@ public:
     bool recordFusedSweep(const ChunkList& la, const ChunkList& lb, const T* r, T* x, bool pre, int sweep,
                           const int32_t* agg, const T* xc);
     void checkSweepError();
+    // streamed level-0 kernels (boxstream.cuh): launch shape per element size, planned once
+    struct StreamShape {
+        int TY = 0, S = 0, threads = 0, grid = 0;  // grid 0: the kernels do not apply
+        size_t smem = 0;
+    };
+    StreamShape stream64_, stream32_;
+    bool streamAllowed_ = true;
+    template <class T> void planStream(const BoxRows& R);
+    template <class T> const StreamShape* streamShape(const BoxRows& R) const;
     // live timing of the level-0 sweeps: solves run eagerly with CUDA events around every level-0
     // sweep (setSweepTiming); the stream's own order, so each sweep meets the cache state the solve
     // leaves it
