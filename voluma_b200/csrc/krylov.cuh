@@ -15,6 +15,11 @@ static_assert(kWideRows == 4 * kRowsPerCta, "the level-0 products take four rows
 
 #define VLM_ROWS(c) for (int row = (c).start + (int)threadIdx.x; row < (c).start + (c).count; row += kRowsPerCta)
 
+// A full level-0 chunk (kWideRows rows): this thread's four rows t, t + 256, ... in VLM_ROWS order,
+// so a kernel can issue every row's loads before its arithmetic.
+#define VLM_FULL(c) ((c).count == kWideRows)
+__device__ __forceinline__ int full_row(const Chunk& c, int q) { return c.start + int(threadIdx.x) + q * kRowsPerCta; }
+
 // converged() of LinearSolver.cpp:114-117
 __device__ __forceinline__ bool dev_converged(const DevCtrl& c, int iters, double finalRes, double initRes) {
     if (iters < c.minIter) return false;
@@ -125,7 +130,19 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
     if (sys_idle(st[c.sys], FLAG)) return;
     BlockSum<1, EXACT> acc;
     acc.begin();
-    VLM_ROWS(c) acc.add(0, (double)w[row] * (double)r[row]);
+    if (VLM_FULL(c)) {
+        W wv[4];
+        T rv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            wv[q] = w[full_row(c, q)];
+            rv[q] = r[full_row(c, q)];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc.add(0, (double)wv[q] * (double)rv[q]);
+    } else {
+        VLM_ROWS(c) acc.add(0, (double)w[row] * (double)r[row]);
+    }
     double out[1];
     if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
@@ -149,6 +166,16 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_p(const Chunk* __restrict__
     const T beta = (T)s.beta;
     if (it == 0) {
         VLM_ROWS(c) p[row] = (T)w[row];
+    } else if (VLM_FULL(c)) {
+        W wv[4];
+        T pv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            wv[q] = w[full_row(c, q)];
+            pv[q] = p[full_row(c, q)];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) p[full_row(c, q)] = (T)wv[q] + beta * pv[q];
     } else {
         VLM_ROWS(c) p[row] = (T)w[row] + beta * p[row];
     }
@@ -203,12 +230,33 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_update(const Chunk* __restr
     const T alpha = (T)st[c.sys].alpha;
     BlockSum<1, EXACT> acc;
     acc.begin();
-    VLM_ROWS(c) {
-        x[row] += alpha * p[row];
-        const T rr = r[row] - alpha * Ap[row];
-        r[row] = rr;
-        if (r32 != nullptr) r32[row] = (float)rr;
-        acc.add(0, fabs((double)rr));
+    if (VLM_FULL(c)) {
+        T xv[4], pv[4], rv[4], av[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int row = full_row(c, q);
+            xv[q] = x[row];
+            pv[q] = p[row];
+            rv[q] = r[row];
+            av[q] = Ap[row];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int row = full_row(c, q);
+            x[row] = xv[q] + alpha * pv[q];
+            const T rr = rv[q] - alpha * av[q];
+            r[row] = rr;
+            if (r32 != nullptr) r32[row] = (float)rr;
+            acc.add(0, fabs((double)rr));
+        }
+    } else {
+        VLM_ROWS(c) {
+            x[row] += alpha * p[row];
+            const T rr = r[row] - alpha * Ap[row];
+            r[row] = rr;
+            if (r32 != nullptr) r32[row] = (float)rr;
+            acc.add(0, fabs((double)rr));
+        }
     }
     double out[1];
     if (acc.finish(c, R, out)) {
