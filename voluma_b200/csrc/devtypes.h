@@ -12,8 +12,13 @@ struct SysState {
     double normFactor, initialResidual, finalResidual, residualSum;
     double wArA, wArAold, alpha, beta, omega, rho, rhoOld, s0, s1;
     double innerInit, innerFinal;  // mixed precision inner solve (FP32 L1 norms)
+    // defect correction around a reference row (the one row of A with a non-zero row sum): A =
+    // L + refC e_ref e_ref^T with L's rows summing to zero; sumR = sum of the outer residual,
+    // innerMu = mean of the inner iteration's preconditioned residual
+    double refC, sumR, innerMu;
     int iterations, converged, done, status;
     int innerIterations, innerDone, outer, pad;
+    int refRow, refCount;  // refRow < 0: no single reference row (no projection)
 };
 
 // Solve controls as seen by the device.

@@ -117,6 +117,16 @@ __global__ void k_recip_diag(int n, const int32_t* __restrict__ valid, const T* 
     rD[i] = valid[i] >= 0 ? T(1) / d[i] : T(0);
 }
 
+// wArA = sum w.r of the iteration and beta = wArA / wArAold (0 on the first), in the CTA that
+// completes the reduction.
+template <int FLAG>
+__device__ __forceinline__ void pcg_dot_wr_done(SysState& s, double wr) {
+    const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
+    s.wArAold = s.wArA;
+    s.wArA = wr;
+    s.beta = it == 0 ? 0.0 : s.wArA / s.wArAold;
+}
+
 // ------------------------------------------------------------------ PCG (LinearSolver.cpp:176-201)
 // wArA = Σ w·r ; beta = wArA / wArAold
 // W: type of the preconditioned residual w (float when an FP32 V-cycle produced it; widening it
@@ -144,13 +154,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_pcg_dot_wr(const Chunk* __restr
         VLM_ROWS(c) acc.add(0, (double)w[row] * (double)r[row]);
     }
     double out[1];
-    if (acc.finish(c, R, out)) {
-        SysState& s = st[c.sys];
-        const int it = FLAG == kFlagDone ? s.iterations : s.innerIterations;
-        s.wArAold = s.wArA;
-        s.wArA = out[0];
-        s.beta = it == 0 ? 0.0 : s.wArA / s.wArAold;
-    }
+    if (acc.finish(c, R, out)) pcg_dot_wr_done<FLAG>(st[c.sys], out[0]);
 }
 
 // p = w (first iteration) or w + beta p
@@ -300,17 +304,150 @@ __global__ void k_inner_begin(int nsys, SysState* st) {
     q.wArA = kGREAT;
 }
 
-// x64 += e32 ; then r64 = b - A x64 in a second kernel (neighbours must be updated first)
-__global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
-                                                               const float* __restrict__ e, const SysState* st) {
+// ---- reference row of the defect correction
+// A pressure matrix with setReference (FvMatrix.h:134-141) is A = L + refC e_ref e_ref^T: L, the
+// pure-Neumann operator, has rows that sum to zero, so its constant vector is a null mode and A's
+// smallest eigenvalue is about refC / N, which FP32 cannot resolve.  The defect correction then
+// solves L y = r - (sum r) e_ref in FP32 with the constant mode projected out of each preconditioned
+// residual (well conditioned on the complement), and restores the constant in FP64:
+// e = y + ((sum r) / refC - y_ref) 1, which makes A e = r.  The reference row is the one row whose
+// sum exceeds 1e-9 of its diagonal; with none or several (Dirichlet rows), nothing is projected.
+__global__ void k_ref_reset(int nsys, SysState* st) {
+    pdl_entry();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    st[s].refRow = -1;
+    st[s].refCount = 0;
+    st[s].refC = 0.0;
+    st[s].sumR = 0.0;
+    st[s].innerMu = 0.0;
+}
+
+__global__ void __launch_bounds__(kRowsPerCta) k_ref_detect(const Chunk* __restrict__ ch, Sell S,
+                                                            const double* __restrict__ val,
+                                                            const double* __restrict__ diag,
+                                                            const int32_t* __restrict__ perm, SysState* st) {
     pdl_launch();
     const Chunk c = ch[blockIdx.x];
     pdl_wait();
-    if (st[c.sys].done) return;
-    VLM_ROWS(c) x[row] += (double)e[row];
+    VLM_ROWS(c) {
+        if (perm[row] < 0) continue;
+        const double d = diag[row];
+        const double sum = row_accumulate<false>(S, val, [](int) { return 1.0; }, row, d);
+        if (fabs(sum) > 1e-9 * fabs(d)) {
+            if (atomicAdd(&st[c.sys].refCount, 1) == 0) {
+                st[c.sys].refRow = row;
+                st[c.sys].refC = sum;
+            }
+        }
+    }
 }
 
-// FP64 defect: r = b - A x (exact FP64 matrix), r32 = (float) r, finalResidual = Σ|r| / nf
+__global__ void k_ref_finish(int nsys, SysState* st) {
+    pdl_entry();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    if (st[s].refCount != 1) st[s].refRow = -1;
+}
+
+// FP32 diagonal of the inner operator: A's, with refC taken off the reference row (L)
+__global__ void __launch_bounds__(kRowsPerCta) k_ref_diag32(const Chunk* __restrict__ ch,
+                                                            const double* __restrict__ diag, float* __restrict__ dL,
+                                                            const SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    pdl_wait();
+    const int ref = st[c.sys].refRow;
+    const double rc = st[c.sys].refC;
+    VLM_ROWS(c) dL[row] = (float)(row == ref ? diag[row] - rc : diag[row]);
+}
+
+// sumR = sum of the initial residual
+__global__ void __launch_bounds__(kRowsPerCta) k_ref_sum_r(const Chunk* __restrict__ ch, const double* __restrict__ r,
+                                                           RedCtx R, SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    pdl_wait();
+    BlockSum<1, false> acc;
+    acc.begin();
+    VLM_ROWS(c) acc.add(0, r[row]);
+    double out[1];
+    if (acc.finish(c, R, out)) st[c.sys].sumR = out[0];
+}
+
+// the inner right-hand side r - (sum r) e_ref: only the reference row's FP32 value changes
+__global__ void k_ref_rhs(int nsys, const double* __restrict__ r, float* __restrict__ r32, const SysState* st) {
+    pdl_entry();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const SysState& q = st[s];
+    if (q.refRow >= 0 && !q.done) r32[q.refRow] = (float)(r[q.refRow] - q.sumR);
+}
+
+// wArA = (z - mu) . r, mu = the mean of z over the system's cells (with a reference row), and beta
+// for the inner recurrence; padding rows are left out of the sums
+__global__ void __launch_bounds__(kRowsPerCta) k_inner_dot_wr(const Chunk* __restrict__ ch, const float* __restrict__ z,
+                                                              const float* __restrict__ r,
+                                                              const int32_t* __restrict__ perm,
+                                                              const int* __restrict__ sysCells, RedCtx R, SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    pdl_wait();
+    if (sys_idle(st[c.sys], kFlagInner)) return;
+    BlockSum<3, false> acc;
+    acc.begin();
+    VLM_ROWS(c) {
+        if (perm[row] < 0) continue;
+        const double zv = (double)z[row], rv = (double)r[row];
+        acc.add(0, zv * rv);
+        acc.add(1, zv);
+        acc.add(2, rv);
+    }
+    double out[3];
+    if (acc.finish(c, R, out)) {
+        SysState& s = st[c.sys];
+        const double mu = s.refRow >= 0 ? out[1] / double(sysCells[c.sys]) : 0.0;
+        s.innerMu = mu;
+        pcg_dot_wr_done<kFlagInner>(s, out[0] - mu * out[2]);
+    }
+}
+
+// p = (z - mu) or (z - mu) + beta p on the system's cells
+__global__ void __launch_bounds__(kRowsPerCta) k_inner_p(const Chunk* __restrict__ ch, const float* __restrict__ z,
+                                                         float* __restrict__ p, const int32_t* __restrict__ perm,
+                                                         const SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    pdl_wait();
+    const SysState& s = st[c.sys];
+    if (sys_idle(s, kFlagInner)) return;
+    const float mu = (float)s.innerMu, beta = (float)s.beta;
+    const bool first = s.innerIterations == 0;
+    VLM_ROWS(c) {
+        if (perm[row] < 0) continue;
+        const float v = z[row] - mu;
+        p[row] = first ? v : v + beta * p[row];
+    }
+}
+
+// x64 += e32 (+ the constant that restores A e = r around a reference row) ; then r64 = b - A x64
+// in a second kernel (neighbours must be updated first)
+__global__ void __launch_bounds__(kRowsPerCta) k_mixed_correct(const Chunk* __restrict__ ch, double* __restrict__ x,
+                                                               const float* __restrict__ e,
+                                                               const int32_t* __restrict__ perm, const SysState* st) {
+    pdl_launch();
+    const Chunk c = ch[blockIdx.x];
+    pdl_wait();
+    const SysState& s = st[c.sys];
+    if (s.done) return;
+    const double a = s.refRow >= 0 ? s.sumR / s.refC - (double)e[s.refRow] : 0.0;
+    VLM_ROWS(c) {
+        if (perm[row] < 0) continue;
+        x[row] += (double)e[row] + a;
+    }
+}
+
+// FP64 defect: r = b - A x (exact FP64 matrix), r32 = (float) r, finalResidual = Σ|r| / nf, sumR = Σ r
 __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __restrict__ ch, Sell S,
                                                                 const double* __restrict__ val,
                                                                 const double* __restrict__ diag,
@@ -322,7 +459,7 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
     const Chunk c = ch[blockIdx.x];
     pdl_wait();
     if (st[c.sys].done) return;
-    BlockSum<1, false> acc;
+    BlockSum<2, false> acc;
     acc.begin();
     VLM_ROWS(c) {
         const double wA = row_plus(S, val, x, row, diag[row] * x[row]);
@@ -330,10 +467,12 @@ __global__ void __launch_bounds__(kRowsPerCta) k_mixed_residual(const Chunk* __r
         r[row] = rr;
         r32[row] = (float)rr;
         acc.add(0, fabs(rr));
+        acc.add(1, rr);
     }
-    double out[1];
+    double out[2];
     if (acc.finish(c, R, out)) {
         SysState& s = st[c.sys];
+        s.sumR = out[1];
         s.finalResidual = out[0] / s.normFactor;
         s.innerInit = out[0];
         s.outer += 1;

@@ -290,7 +290,7 @@ DeviceBatch::DeviceBatch(const std::vector<SysTopo>& systems, int mergeLevels, c
     counters_.zero(stream_);
     status_.resize(1);
     status_.zero(stream_);
-    partials_.resize(size_t(plan_.nSlots) * 2);
+    partials_.resize(size_t(plan_.nSlots) * 3);  // up to three sums per reduction (k_inner_dot_wr)
     st_.resize(size_t(plan_.nsys));
     st_.zero(stream_);
     dctrl_.resize(1);
@@ -1157,10 +1157,38 @@ void DeviceBatch::runEager(const SolveKey& key, int maxIter) {
         VLM_LAUNCH(k_inner_begin, nblk(plan_.nsys), 256, s, plan_.nsys, st_.get());
         VLM_LAUNCH(k_zero_rows<float>, nb, kRowsPerCta, s, ch, e32_.get(), st_.get(), kFlagInner);
         for (int it = 0; it < cap && anyActive(kFlagInner); ++it) recordInnerPcgIter(key.precond, key.smoother);
-        VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), e32_.get(), st_.get());
-        VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
-                   b_.get(), r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
+        recordMixedTail();
     }
+}
+
+void DeviceBatch::recordRefSetup() {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    if (dL32_.size() != size_t(D0.nrows)) dL32_.resize(size_t(D0.nrows));
+    VLM_LAUNCH(k_ref_reset, nblk(plan_.nsys), 256, s, plan_.nsys, st_.get());
+    VLM_LAUNCH(k_ref_detect, nb, kRowsPerCta, s, ch, D0.sell(), (const double*)D0.val.get(),
+               (const double*)D0.diag.get(), (const int32_t*)perm0_.get(), st_.get());
+    VLM_LAUNCH(k_ref_finish, nblk(plan_.nsys), 256, s, plan_.nsys, st_.get());
+    VLM_LAUNCH(k_ref_diag32, nb, kRowsPerCta, s, ch, (const double*)D0.diag.get(), dL32_.get(),
+               (const SysState*)st_.get());
+    VLM_LAUNCH(k_ref_sum_r, nb, kRowsPerCta, s, ch, (const double*)r_.get(), red(), st_.get());
+    VLM_LAUNCH(k_ref_rhs, nblk(plan_.nsys), 256, s, plan_.nsys, (const double*)r_.get(), r32_.get(),
+               (const SysState*)st_.get());
+}
+
+void DeviceBatch::recordMixedTail() {
+    DevLevel& D0 = L_[0];
+    cudaStream_t s = stream_;
+    const Chunk* ch = D0.ch(D0.all);
+    const int nb = D0.all.n;
+    VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), (const float*)e32_.get(),
+               (const int32_t*)perm0_.get(), (const SysState*)st_.get());
+    VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(), b_.get(),
+               r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
+    VLM_LAUNCH(k_ref_rhs, nblk(plan_.nsys), 256, s, plan_.nsys, (const double*)r_.get(), r32_.get(),
+               (const SysState*)st_.get());
 }
 
 void DeviceBatch::recordPcgIter(PrecondKind pk, SmootherKind sm, bool f32) {
@@ -1226,23 +1254,28 @@ void DeviceBatch::recordInnerPcgIter(PrecondKind pk, SmootherKind sm) {
                    kFlagInner);
     else
         throw Error(VLM_ERR_UNSUPPORTED, "mixed precision needs the GAMG or diagonal preconditioner");
-    VLM_LAUNCH((k_pcg_dot_wr<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, w32_.get(), r32_.get(), red(), st_.get());
-    VLM_LAUNCH((k_pcg_p<float, kFlagInner>), nb, kRowsPerCta, s, ch, w32_.get(), p32_.get(), st_.get());
+    // the inner operator is L (A without the reference row's refC) and the constant mode is projected
+    // out of the preconditioned residual; without a reference row both reduce to A and no projection
+    VLM_LAUNCH(k_inner_dot_wr, nb, kRowsPerCta, s, ch, (const float*)w32_.get(), (const float*)r32_.get(),
+               (const int32_t*)perm0_.get(), (const int*)sysCells_.get(), red(), st_.get());
+    VLM_LAUNCH(k_inner_p, nb, kRowsPerCta, s, ch, (const float*)w32_.get(), p32_.get(), (const int32_t*)perm0_.get(),
+               (const SysState*)st_.get());
+    const float* dL = dL32_.get();
     if (boxOn_) {
         int g = 0;
         const BoxRows R = boxRows(D0, D0.all, &g);
         if (R.ch == nullptr && R.one.H % 4 == 0)
             VLM_LAUNCH((k_box_pcg_spmv4<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, R.one,
-                       (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(),
-                       (const float*)p32_.get(), Ap32_.get(), red(), st_.get());
+                       (const float*)D0.bcoef32.get(), D0.nrows, dL, (const float*)p32_.get(), Ap32_.get(), red(),
+                       st_.get());
         else
             VLM_LAUNCH((k_box_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, R,
-                       (const float*)D0.bcoef32.get(), D0.nrows, (const float*)D0.diag32.get(),
-                       (const float*)p32_.get(), Ap32_.get(), red(), st_.get());
+                       (const float*)D0.bcoef32.get(), D0.nrows, dL, (const float*)p32_.get(), Ap32_.get(), red(),
+                       st_.get());
     }
     else
-        VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(),
-                   D0.diag32.get(), p32_.get(), Ap32_.get(), red(), st_.get());
+        VLM_LAUNCH((k_pcg_spmv<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, D0.sell(), D0.val32.get(), dL,
+                   p32_.get(), Ap32_.get(), red(), st_.get());
     VLM_LAUNCH((k_pcg_update<float, kFlagInner, false>), nb, kRowsPerCta, s, ch, e32_.get(), r32_.get(), p32_.get(),
                Ap32_.get(), perm0_.get(), red(), st_.get(), dctrl_.get(), (float*)nullptr);
 }
@@ -1567,9 +1600,7 @@ void DeviceBatch::buildGraph(const SolveKey& key, GraphExec& G) {
         });
         G.innerK = segment();
         captureInto(s, outer, {w}, [&] {
-            VLM_LAUNCH(k_mixed_correct, nb, kRowsPerCta, s, ch, x_.get(), e32_.get(), st_.get());
-            VLM_LAUNCH(k_mixed_residual, nb, kRowsPerCta, s, ch, D0.sell(), D0.val.get(), D0.diag.get(), x_.get(),
-                       b_.get(), r_.get(), r32_.get(), red(), st_.get(), dctrl_.get());
+            recordMixedTail();
             recordSetCond(ho, kFlagDone);
         });
         G.bodyK += segment();
@@ -1707,6 +1738,7 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
                    D0.diag.get(), x_.get(), b_.get(), perm0_.get(), r_.get(), r32first ? r32_.get() : nullptr,
                    sysCells_.get(), red(), st_.get(), dctrl_.get());
     }
+    if (dc) recordRefSetup();
     if (sk == SolverKind::PBiCGStab) {
         VLM_CUDA(cudaMemcpyAsync(r0_.get(), r_.get(), sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
         Ay_.zero(s);

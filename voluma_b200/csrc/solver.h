@@ -252,6 +252,9 @@ private:
     // Krylov vectors, level-0 solver order
     DBuf<double> x_, b_, r_, w_, p_, Ap_, rD_, r0_, y_, Ay_, s_, z_, t_;
     DBuf<float> e32_, r32_, w32_, p32_, Ap32_, rD32_;
+    DBuf<float> dL32_;  // defect correction: FP32 diagonal of the inner operator (reference row's refC removed)
+    void recordRefSetup();   // reference row, inner diagonal, inner right-hand side (mixed-dc)
+    void recordMixedTail();  // outer correction, FP64 defect, next inner right-hand side (mixed-dc)
     std::map<SolveKey, std::unique_ptr<GraphExec>> graphs_;
     std::vector<SysState> hostState_;
     double jacobiOmega_ = 1.0;
