@@ -19,6 +19,10 @@
 struct vlm_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // uploads of a solve's right-hand side and initial guess, behind the matrix upload and beside
+    // the matrix set-up (vlm_ldu_solve)
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t matrixSent = nullptr, inputsSent = nullptr;
     std::string err;
     int refs = 1;  // the handle itself + one per registered mesh
 };
@@ -176,6 +180,12 @@ namespace {
 void ctxUnref(vlm_ctx* ctx) {
     if (--ctx->refs > 0) return;
     cudaSetDevice(ctx->device);
+    if (ctx->copyStream) {
+        cudaStreamSynchronize(ctx->copyStream);
+        cudaStreamDestroy(ctx->copyStream);
+    }
+    if (ctx->matrixSent) cudaEventDestroy(ctx->matrixSent);
+    if (ctx->inputsSent) cudaEventDestroy(ctx->inputsSent);
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
@@ -372,8 +382,21 @@ vlm_status vlm_ldu_solve(vlm_ctx* ctx, vlm_mesh* m, const double* diag, const do
         cudaStream_t s = ctx->stream;
         const double *dd, *du, *dl;
         stageCoeffs(m, diag, upper, lower, &dd, &du, &dl);
-        m->b.upload(b, size_t(m->nCells), s);
-        m->x.upload(x, size_t(m->nCells), s);
+        // b and x cross the bus after the matrix (which the set-up needs first) on a second stream,
+        // while the device builds the hierarchy's matrices
+        if (!ctx->copyStream) {
+            VLM_CUDA(cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking));
+            VLM_CUDA(cudaEventCreateWithFlags(&ctx->matrixSent, cudaEventDisableTiming));
+            VLM_CUDA(cudaEventCreateWithFlags(&ctx->inputsSent, cudaEventDisableTiming));
+        }
+        m->b.resize(size_t(m->nCells));
+        m->x.resize(size_t(m->nCells));
+        VLM_CUDA(cudaEventRecord(ctx->matrixSent, s));
+        VLM_CUDA(cudaStreamWaitEvent(ctx->copyStream, ctx->matrixSent, 0));
+        m->b.upload(b, size_t(m->nCells), ctx->copyStream);
+        m->x.upload(x, size_t(m->nCells), ctx->copyStream);
+        VLM_CUDA(cudaEventRecord(ctx->inputsSent, ctx->copyStream));
+        m->batch->inputsAfter(ctx->inputsSent);
         std::vector<vlm_solver_perf> p;
         m->batch->solve(dd, du, dl, m->b.get(), m->x.get(), *ctrl, p);
         VLM_CUDA(cudaMemcpyAsync(x, m->x.get(), sizeof(double) * size_t(m->nCells), cudaMemcpyDeviceToHost, s));

@@ -1718,6 +1718,11 @@ void DeviceBatch::solve(const double* diag, const double* upper, const double* l
     hc.maxInner = ctrl.maxIter;
     VLM_LAUNCH(k_set_ctrl, 1, 1, s, dctrl_.get(), hc);
     st_.zero(s);
+    // b and x may still be arriving on another stream while the matrix was set up
+    if (inputsReady_) {
+        VLM_CUDA(cudaStreamWaitEvent(s, inputsReady_, 0));
+        inputsReady_ = nullptr;
+    }
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), x, x_.get());
     VLM_LAUNCH(k_to_solver<double>, nblk(n0), 256, s, n0, perm0_.get(), b, b_.get());
     exact_ = ctrl.reproducible != 0;

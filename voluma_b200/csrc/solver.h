@@ -146,6 +146,9 @@ public:
     // limit (0 keeps a value); re-plans the batch's launches, same results.
     void setTail(int cluster, int64_t maxRows, int64_t fullRows);
     void setFusion(int64_t pre, int64_t restrict, int64_t post);
+    // The next solve() reads b and x only after `ev` (their upload on another stream), so the
+    // upload overlaps the matrix set-up.
+    void inputsAfter(cudaEvent_t ev) { inputsReady_ = ev; }
     void streamConfig(int32_t* ty, int32_t* stages, int32_t* ctas) const {
         *ty = stream64_.grid > 0 ? stream64_.TY : 0;
         *stages = stream64_.grid > 0 ? stream64_.S : 0;
@@ -183,6 +186,7 @@ public:
     };
     StreamShape stream64_, stream32_;
     bool streamAllowed_ = true;
+    cudaEvent_t inputsReady_ = nullptr;
     template <class T> void planStream(const BoxRows& R);
     template <class T> const StreamShape* streamShape(const BoxRows& R) const;
     // live timing of the level-0 sweeps: solves run eagerly with CUDA events around every level-0
