@@ -725,8 +725,10 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
     }
     __syncthreads();
     // LU without pivoting, one pivot at a time: multipliers of column k, then the trailing block
-    // element-parallel (each element receives its updates in the order k = 0, 1, ...)
+    // element-parallel (each element receives its updates in the order k = 0, 1, ...).  The block
+    // loops run over a (blockDim.x / 32) x 32 grid of rows x columns (no index division).
     const int nt = blockDim.x;
+    const int tx = int(threadIdx.x) & 31, ty = int(threadIdx.x) >> 5, ny = nt >> 5;
     for (int k = 0; k < n; ++k) {
         const double piv = A[(size_t)k * n + k];
         if (fabs(piv) < kVSMALL) {  // uniform: every thread reads the same pivot
@@ -735,23 +737,22 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
         }
         for (int i = k + 1 + threadIdx.x; i < n; i += nt) A[(size_t)i * n + k] /= piv;
         __syncthreads();
-        const int m = n - k - 1;
-        for (int q = threadIdx.x; q < m * m; q += nt) {
-            const int i = k + 1 + q / m, j = k + 1 + q % m;
+        for (int i = k + 1 + ty; i < n; i += ny) {
             const double fct = A[(size_t)i * n + k];
-            if (fct != 0.0) A[(size_t)i * n + j] -= fct * A[(size_t)k * n + j];
+            if (fct == 0.0) continue;
+            for (int j = k + 1 + tx; j < n; j += 32) A[(size_t)i * n + j] -= fct * A[(size_t)k * n + j];
         }
         __syncthreads();
     }
     // inverse = U^-1 L^-1, all columns at once.  Forward (unit L): X = I, then for k ascending
     // X[i][j] -= L[i][k] X[k][j] for i > k (X[k][j] = 0 for j > k, so j <= k).
-    for (int q = threadIdx.x; q < n * n; q += nt) X[q] = (q / n == q % n) ? 1.0 : 0.0;
+    for (int i = ty; i < n; i += ny)
+        for (int j = tx; j < n; j += 32) X[(size_t)i * n + j] = i == j ? 1.0 : 0.0;
     __syncthreads();
     for (int k = 0; k + 1 < n; ++k) {
-        const int m = n - k - 1, w = k + 1;
-        for (int q = threadIdx.x; q < m * w; q += nt) {
-            const int i = k + 1 + q / w, j = q % w;
-            X[(size_t)i * n + j] -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
+        for (int i = k + 1 + ty; i < n; i += ny) {
+            const double l = A[(size_t)i * n + k];
+            for (int j = tx; j <= k; j += 32) X[(size_t)i * n + j] -= l * X[(size_t)k * n + j];
         }
         __syncthreads();
     }
@@ -760,9 +761,9 @@ __global__ void k_coarse_factor(const CoarseDev* __restrict__ cs, Sell S, const 
         const double ukk = A[(size_t)k * n + k];
         for (int j = threadIdx.x; j < n; j += nt) X[(size_t)k * n + j] /= ukk;
         __syncthreads();
-        for (int q = threadIdx.x; q < k * n; q += nt) {
-            const int i = q / n, j = q % n;
-            X[(size_t)i * n + j] -= A[(size_t)i * n + k] * X[(size_t)k * n + j];
+        for (int i = ty; i < k; i += ny) {
+            const double u = A[(size_t)i * n + k];
+            for (int j = tx; j < n; j += 32) X[(size_t)i * n + j] -= u * X[(size_t)k * n + j];
         }
         __syncthreads();
     }
