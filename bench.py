@@ -121,6 +121,9 @@ def ref_mesh_arrays(n):
 
 # ------------------------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi's clock and throttle-reason record during a timed region: one nvidia-smi process
+    streaming a line every 20 ms (-lms), started before the region (start() returns once the first
+    line has arrived) and ended after it by its own PID."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
@@ -128,38 +131,49 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
+        self._first = threading.Event()
 
     def start(self):
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                           "--format=csv,noheader,nounits", "-lms", "20"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
+            return
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        self._first.wait(timeout=5.0)
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([v.strip() for v in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        for line in self._proc.stdout:
+            out = line.strip()
+            if out:
+                self.samples.append([v.strip() for v in out.split(",")])
+                self._first.set()
 
     def stop(self):
-        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except Exception:
+                self._proc.kill()
         if self._t:
             self._t.join(timeout=10)
-        if not self.samples:
+        # the samples of the timed region: drop the one that start() waited for
+        samples = self.samples[1:] if len(self.samples) > 1 else self.samples
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in samples if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and
+        reasons = sorted({names[i] for s in samples for i in range(4) if len(s) > 4 + i and
                           s[4 + i].lower().startswith("active")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def measured_peak_gbs():
