@@ -811,18 +811,20 @@ def run_batch(args, rank, world, local):
             torch.distributed.barrier()
         torch.cuda.synchronize(local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = B.stats()[0]
         e0.record(st)
         for _ in range(args.steps):
             perf = one()
         e1.record(st)
         torch.cuda.synchronize(local)
+        launches = B.stats()[0] - l0
         dev_s = e0.elapsed_time(e1) / 1e3
         ok = all(r.converged for row in perf for r in row)
         if prec == "mixed":
             clocks = sampler.stop()
         dev_s = max_over_ranks(dev_s, world, dev)
         modes[prec] = dict(value=aggregate_rate(args.systems * args.steps, world, dev_s),
-                           ms_per_step=1e3 * dev_s / args.steps,
+                           ms_per_step=1e3 * dev_s / args.steps, gpu_launches=int(launches),
                            all_converged=bool(ok), iterations_max=int(max(max(r) for r in its)),
                            iterations_median=int(np.median([x for r in its for x in r])))
     # plain FP64: every system registered on its own and solved one after another with the same
@@ -899,7 +901,7 @@ def run_batch(args, rank, world, local):
                     "d2h_bytes_per_step": int(8 * (nC + nF)),
                     "note": "vlm_pressure_solve_batch with host arrays: H2D gamma, divPhi, p; D2H p and flux"},
             "roofline": None, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": None}
+            "gpu_launches": modes["mixed"]["gpu_launches"]}
     print(json.dumps(line))
 
 

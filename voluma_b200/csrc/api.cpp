@@ -57,6 +57,10 @@ struct vlm_mesh {
         int runs = 0;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
+        // kernels one call launches: the geometry kernels, and per pass the deferred solve's counts
+        // (eager set-up, loop entry, one loop pass), recorded when the passes were issued
+        int64_t geomK = 0;
+        std::vector<vlm::DeviceBatch::LaunchCount> solveK;
         ~PGraph() {
             if (exec) cudaGraphExecDestroy(exec);
             if (graph) cudaGraphDestroy(graph);
@@ -627,9 +631,11 @@ void ensureWork(vlm_mesh* m) {
 // m->pstate / m->pstatus), and the face flux of the last pass.
 void pressurePasses(vlm_mesh* m, const double* gamma, const double* divPhi, double* p, const vlm::ScalarBC& bc,
                     int nRefs, double refValue, int nNonOrth, int gradScheme, const vlm_solver_ctrl& ctrl,
-                    const vlm_solver_ctrl& finalCtrl, double* flux) {
+                    const vlm_solver_ctrl& finalCtrl, double* flux, vlm_mesh::PGraph* g) {
     vlm::DeviceGeom& G = geomOf(m);
     cudaStream_t s = m->ctx->stream;
+    const int64_t geom0 = G.launches();
+    g->solveK.clear();
     for (int no = 0; no <= nNonOrth; ++no) {
         const bool last = no == nNonOrth;
         G.correctBoundary(p, bc, m->pB.get(), s);
@@ -642,9 +648,11 @@ void pressurePasses(vlm_mesh* m, const double* gamma, const double* divPhi, doub
         std::vector<vlm_solver_perf> pf;
         m->batch->deferNextSolve(m->pstate.get() + size_t(no) * m->nsys, m->pstatus.get() + 2 * no);
         m->batch->solve(m->fd.get(), m->pupper.get(), m->pupper.get(), m->fb.get(), p, last ? finalCtrl : ctrl, pf);
+        g->solveK.push_back(m->batch->lastDeferred());
         if (last && flux) G.flux(m->pupper.get(), p, m->ic.get(), m->bs.get(), hasFfc ? m->ffc.get() : nullptr, flux, s);
     }
     G.correctBoundary(p, bc, m->pB.get(), s);
+    g->geomK = G.launches() - geom0;
 }
 
 std::vector<int64_t> ctrlKey(const vlm_solver_ctrl& c) {
@@ -725,7 +733,7 @@ void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double
         VLM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
         m->batch->beginEmbedding();
         try {
-            pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux);
+            pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux, g);
         } catch (...) {
             m->batch->endEmbedding();
             cudaGraph_t junk = nullptr;
@@ -740,7 +748,7 @@ void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double
     if (g->exec)
         VLM_CUDA(cudaGraphLaunch(g->exec, s));
     else
-        pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux);
+        pressurePasses(m, gamma, divPhi, p, bc, nRefs, refValue, nNonOrth, gradScheme, ctrl, finalCtrl, flux, g);
     ++g->runs;
     // every pass's solver records, read once
     vlm::SysState* hs = static_cast<vlm::SysState*>(m->pinned);
@@ -748,6 +756,16 @@ void pressureLoop(vlm_mesh* m, const double* gamma, const double* divPhi, double
     VLM_CUDA(cudaMemcpyAsync(hs, m->pstate.get(), sizeof(vlm::SysState) * nRec, cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaMemcpyAsync(hst, m->pstatus.get(), sizeof(int) * 2 * size_t(nNonOrth + 1), cudaMemcpyDeviceToHost, s));
     VLM_CUDA(cudaStreamSynchronize(s));
+    // executed kernels: the geometry kernels and, per pass, the solve's set-up, loop entry and one
+    // loop body per pass of its WHILE loop (the most iterations over the batch's systems)
+    int64_t executed = g->geomK;
+    for (int no = 0; no <= nNonOrth && no < int(g->solveK.size()); ++no) {
+        int64_t its = 0;
+        for (int b = 0; b < m->nsys; ++b) its = std::max<int64_t>(its, hs[size_t(no) * m->nsys + b].iterations);
+        const auto& k = g->solveK[size_t(no)];
+        executed += k.eager + k.pre + its * k.body;
+    }
+    m->batch->countLaunches(executed);
     const auto& order = m->batch->plan().order;
     for (int no = 0; no <= nNonOrth; ++no) {
         if (hst[2 * no + 1] != 0) {

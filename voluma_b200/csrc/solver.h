@@ -165,6 +165,7 @@ public:
         *fullRows = tailFullRows_;
     }
     int64_t launches() const { return launches_; }
+    void countLaunches(int64_t n) { launches_ += n; }  // kernels of deferred solves, counted by the caller
     // Times `reps` back-to-back launches of one level-0 kernel on the current matrix (after a
     // solve); returns ms per launch and the algorithmic bytes one launch moves.
     double profileKernel(const std::string& name, int reps, double* bytesPerLaunch);
