@@ -95,7 +95,12 @@ typedef struct {
                                  Gauss-Seidel, forward colours pre / reversed post; Jacobi on the
                                  coarser levels) | "mcgs" (block-hybrid Gauss-Seidel on the coarser
                                  levels) | "jacobi" (every level) */
-    char precision[16];       /* "" or "fp64" | "mixed" (FP32 inner PCG+GAMG in FP64 defect correction) */
+    char precision[16];       /* "" or "fp64" | "mixed" (FP32 GAMG V-cycle inside the FP64 PCG
+                                 recurrence) | "mixed-dc" (FP32 inner PCG+GAMG inside FP64 defect
+                                 correction; with a single reference row - the one row of A with a
+                                 non-zero row sum, as setReference leaves it - the inner solve runs on
+                                 the pure-Neumann operator with the constant mode projected out and
+                                 the correction restores that mode) */
     int32_t reproducible;     /* 1: CFD_REPRODUCIBLE semantics: preconditioner -> diagonal,
                                  GS -> Jacobi, exact (order-independent) global sums */
     int32_t mergeLevels;      /* GAMG pairwise merges per level; 0 -> 2 (GAMG.cpp:96-99) */
