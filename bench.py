@@ -1061,6 +1061,10 @@ def run_ours(args, rank, world, local):
     k_ms_cold, k_bytes = mesh.profile_kernel("smooth32", 20)
     k_ms_warm, _ = mesh.profile_kernel("smooth32:warm", 20)
     k_ms_steps, _ = mesh.profile_kernel("smooth32_steps", 20)
+    # the FP64 Krylov product of the same system (plane-streamed where the mesh allows it)
+    p_ms_cold, p_bytes = mesh.profile_kernel("spmv64", 20)
+    p_ms_warm, _ = mesh.profile_kernel("spmv64:warm", 20)
+    streamed = mesh.stream_config()[2] > 0
     peak, peak_kind = measured_peak_gbs()
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
     traffic = ncu_traffic("smooth32", args.n)
@@ -1081,6 +1085,14 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": world * args.steps / (e2e_tot / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(8 * (n + nI + n + n)), "d2h_bytes_per_step": int(8 * n),
                 "p99_ms": float(np.percentile(e2e_ms, 99))},
+        "fp64_product": {"kernel": ("k_box_pcg_spmv_stream<double>" if streamed else "k_box_pcg_spmv4<double>") +
+                                    " level 0 (PCG product Ap = A p with the fused p.Ap)",
+                         "alg_bytes_per_launch": p_bytes, "ms_per_launch_l2_cold": p_ms_cold,
+                         "ms_per_launch_l2_warm": p_ms_warm, "peak": peak, "unit": "GB/s",
+                         "frac_cold": p_bytes / (p_ms_cold * 1e-3) / 1e9 / peak,
+                         "frac_warm": p_bytes / (p_ms_warm * 1e-3) / 1e9 / peak,
+                         "timing": "CUDA events around single launches after an L2-evicting 256 MB read (cold) "
+                                   "and around back-to-back launches (warm)"},
         "roofline": {"kernel": ("k_box_sweep4<float> level 0 (one full red-black Gauss-Seidel sweep, one launch)"
                                 if os.environ.get("VLM_BOX_FUSED") == "1" else
                                 "k_box_gs4<float> level 0 (one full red-black Gauss-Seidel sweep: two colour launches)"),
