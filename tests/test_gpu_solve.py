@@ -460,3 +460,24 @@ def test_mixed_defect_correction_without_reference_row():
     assert p.converged and p.outerIterations >= 1
     r = np.abs(b - ro.amul(M, d, up, None, x)).sum()
     assert r / p.normFactor < 1e-8 * p.initialResidual * 1.0001
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,periodic", [((20, 16, 8), (1, 1, 1)), ((32, 16, 2), (0, 0, 0)), ((32, 9, 6), (0, 0, 0))])
+def test_streamed_product_not_planned_where_it_cannot_apply(shape, periodic):
+    """x rows of 10 slots (not whole 16-byte words), fewer than 3 planes, or no pencil height that
+    divides ny (9): no streamed shape is planned, the four-slot product runs, and the solve matches
+    the oracle's."""
+    M = vm.box_mesh(shape, hi=(1.0, 0.7, 0.5), periodic=periodic)
+    d, up = vm.poisson_matrix(M)
+    b = np.random.default_rng(4).standard_normal(M["n_cells"])
+    b -= b.mean()
+    m = vb.Mesh.from_arrays(M)
+    assert m.stream_config() == (0, 0, 0)
+    x = np.zeros(M["n_cells"])
+    p = vb.solve_ldu(m, d, up, None, b, x, ctrl(preconditioner="GAMG"))
+    m.close()
+    xo, po = ro.solve(M, d, up, None, b, np.zeros(M["n_cells"]), "PCG", "GAMG", 0.0, 1e-8, 2000,
+                      smoother="mcgs-jacobi", coarse=1)
+    assert p.converged and abs(p.iterations - po["iterations"]) <= 1
+    assert rel(x, oracle_iterate(M, d, up, b, np.zeros(M["n_cells"]), xo, po, p.iterations)) <= 1e-10
